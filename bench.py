@@ -1,0 +1,320 @@
+#!/usr/bin/env python
+"""Benchmark: batched VMC electron moves per second on one B200 (per GPU, weak scaling).
+
+Workload (default): the C2-like pseudopotential dimer (8 electrons, 60 contracted
+Gaussians, one determinant, e-e/e-n/e-e-n Jastrow, 12-point nonlocal quadrature) with
+8192 walkers in one launch, mixed precision.  A step is one VMC sweep over all walkers:
+8 single-electron Metropolis proposals per walker (ratio, accept, Sherman-Morrison and
+Jastrow-table update) plus one full local-energy evaluation per walker, including the
+nonlocal pseudopotential quadrature.  e-moves/s = walkers x electrons x steps / time.
+
+Output: one JSON line (rank 0).  --impl reference times the CPU restatement of the
+reference algorithm (the reference itself is Fortran and cannot be built here) on the
+host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "e-moves/s & param-grad samples/s: mixed vs FP64, 1 B200, |ΔE_L|≤1e-6 Ha"
+UNIT = "e-moves/s"
+SEED = 20261203
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--system", type=int, default=2)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--walkers", type=int, default=0)
+    ap.add_argument("--step-size", type=float, default=0.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-arm", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.idx), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            p = [q.strip() for q in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def state_bytes(system, precision):
+    """Algorithmic HBM bytes per walker per sweep: the persistent walker state (positions,
+    reference-determinant inverses, Jastrow pair table, ln|D|, sign, J) read and written once."""
+    N, nup = system.nelec, system.nup
+    ndn = N - nup
+    t = 8 if precision == "fp64" else 4
+    b = 8 * 3 * N + 8 * (nup * nup + ndn * ndn) + t * N * N + 8 * 3
+    return 2 * b
+
+
+def cpu_baseline_sample(system, seconds=12.0):
+    """Oracle (CPU restatement, OpenMP over walkers, all host threads) on a bounded sample."""
+    from oracle.oracle import Oracle
+    o = Oracle(system)
+    ncores = os.cpu_count() or 1
+    nw = max(ncores * 4, 32)
+    x = system_walkers(system, nw, seed=3)
+    t0 = time.perf_counter()
+    o.vmc(x, 1, seed=SEED, sweep0=0, step=step_size(system), nthreads=ncores)
+    dt1 = max(time.perf_counter() - t0, 1e-3)
+    nsw = max(1, int(seconds / dt1))
+    t0 = time.perf_counter()
+    o.vmc(x, nsw, seed=SEED, sweep0=1, step=step_size(system), nthreads=ncores)
+    dt = time.perf_counter() - t0
+    v = nw * system.nelec * nsw / dt
+    return {"value": v, "unit": UNIT, "cores": ncores, "kind": "port",
+            "sample": f"{nw} walkers x {nsw} sweeps of {system.name} on the FP64 oracle ({dt:.1f} s)"}
+
+
+def system_walkers(system, nw, seed):
+    from champ_b200.system import initial_walkers
+    return initial_walkers(system, nw, seed=seed)
+
+
+def step_size(system):
+    return ARGS.step_size if ARGS.step_size > 0 else system.step
+
+
+def dist_setup(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def run_reference(args, system, rank, world):
+    if rank != 0:
+        return
+    from oracle.oracle import Oracle
+    o = Oracle(system)
+    ncores = os.cpu_count() or 1
+    nw = max(ncores * 4, 32)
+    x = system_walkers(system, nw, seed=3)
+    for i in range(args.warmup):
+        r = o.vmc(x, 1, seed=SEED, sweep0=i, step=step_size(system), nthreads=ncores)
+        x = r["x"]
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        r = o.vmc(x, 1, seed=SEED, sweep0=args.warmup + k, step=step_size(system), nthreads=ncores)
+        x = r["x"]
+    dt = time.perf_counter() - t0
+    v = nw * system.nelec * args.steps / dt
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": config_of(system, nw, "fp64"),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": ncores, "kind": "port",
+                             "sample": f"{nw} walkers per step, 1 sweep each, FP64 CPU restatement of the reference "
+                                       f"algorithm (the Fortran reference cannot be compiled here)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def config_of(system, nw, prec):
+    return {"workload": f"{system.name}: VMC sweeps, {system.nelec} electrons, {system.nbasis} basis functions, "
+                        f"{system.ndet} determinant(s), {system.ncent} centres, "
+                        f"{'12-point NLPP quadrature' if system.nloc else 'all-electron'}",
+            "walkers_per_gpu": nw, "electrons": system.nelec, "precision": prec,
+            "step": "one sweep: N single-electron proposals per walker + full E_L",
+            "l2": "flushed between timed steps (256 MB write)"}
+
+
+def time_engine(eng, system, args, nsteps, nwarm, flush, torch, sweep_base):
+    st = step_size(system)
+    for i in range(nwarm):
+        eng.vmc_sweeps(1, SEED, sweep0=sweep_base + i, step=st, stats=False)
+    torch.cuda.synchronize()
+    evs = []
+    for k in range(nsteps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        eng.vmc_sweeps(1, SEED, sweep0=sweep_base + nwarm + k, step=st, stats=False)
+        e1.record()
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in evs)  # ms
+
+
+def main():
+    global ARGS
+    args = ARGS = parse()
+    from champ_b200 import system as S
+    system = S.get_system(args.system)
+    rank, world, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        run_reference(args, system, rank, world)
+        return
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    from champ_b200.engine import Engine
+    nw = args.walkers or system.walkers
+    prec = args.precision
+    eng = Engine(system, nw, prec)
+    x0 = system_walkers(system, nw, seed=1000 + rank)
+    eng.set_walkers(x0)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    # equilibration (untimed)
+    eng.vmc_sweeps(10, SEED + rank, sweep0=0, step=step_size(system), stats=False)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    t_wall = time.perf_counter()
+    ms = time_engine(eng, system, args, args.steps, args.warmup, flush, torch, 100)
+    t_wall = time.perf_counter() - t_wall
+    clocks = clk.stop()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+        ms = float(t.item())
+    total_moves = nw * world * system.nelec * args.steps
+    value = total_moves / (ms * 1e-3)
+    ms_step = ms / args.steps
+    # roofline of the dominant kernel (the fused sweep kernel, one launch per step)
+    peaks, peak_kind = measured_peaks()
+    alg_bytes = state_bytes(system, prec) * nw
+    achieved = alg_bytes / (ms_step * 1e-3) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_source": peak_kind,
+            "kernel": "k_vmc (fused sweep)",
+            "note": "algorithmic bytes = persistent walker state read+written once per sweep; the kernel is "
+                    "CUDA-core bound (see profiles/), so this fraction is small by construction"}
+    # FP64 arm of the same workload (the metric compares mixed with FP64)
+    fp64 = None
+    if prec == "mixed" and not args.no_fp64_arm:
+        eng64 = Engine(system, nw, "fp64")
+        eng64.set_walkers(eng.get_walkers())
+        ms64 = time_engine(eng64, system, args, max(3, args.steps // 4), 2, flush, torch, 10000)
+        if world > 1:
+            t = torch.tensor([ms64], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms64 = float(t.item())
+        v64 = nw * world * system.nelec * max(3, args.steps // 4) / (ms64 * 1e-3)
+        fp64 = {"value": v64, "unit": UNIT, "ms_per_step": ms64 / max(3, args.steps // 4),
+                "mixed_over_fp64": value / v64}
+        eng64.close()
+    # end to end through the host-facing call: walkers in from pinned host memory, one sweep,
+    # E_L and walkers back to host memory, every step
+    xh = torch.empty((nw, system.nelec, 3), dtype=torch.float64, pin_memory=True)
+    xh.copy_(torch.from_numpy(eng.get_walkers()))
+    elh = torch.empty((nw,), dtype=torch.float64, pin_memory=True)
+    import ctypes as C
+    from champ_b200.engine import load_library
+    lib = load_library()
+    px = C.cast(xh.data_ptr(), C.POINTER(C.c_double))
+    pel = C.cast(elh.data_ptr(), C.POINTER(C.c_double))
+    for i in range(2):
+        eng._check(lib.champ_vmc_run_host(eng.h, nw, px, 1, SEED, 20000 + i, step_size(system), pel))
+    if world > 1:
+        dist.barrier()
+    ne2e = max(3, args.steps // 2)
+    t0 = time.perf_counter()
+    for k in range(ne2e):
+        eng._check(lib.champ_vmc_run_host(eng.h, nw, px, 1, SEED, 20010 + k, step_size(system), pel))
+    te2e = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([te2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        te2e = float(t.item())
+    e2e = {"value": nw * world * system.nelec * ne2e / te2e, "unit": UNIT,
+           "h2d_bytes_per_step": nw * system.nelec * 3 * 8, "d2h_bytes_per_step": nw * system.nelec * 3 * 8 + nw * 8,
+           "call": "champ_vmc_run_host (walkers host->device, state rebuild, 1 sweep, E_L and walkers device->host)"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(system)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32+f64" if prec == "mixed" else "f64", "data": "synthetic",
+                "config": config_of(system, nw, prec), "clocks": clocks, "gpu_launches": args.steps,
+                "roofline": roof, "fp64_arm": fp64, "e2e": e2e, "cpu_baseline": cpu,
+                "wall_s_timed_region": t_wall}
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,467 @@
+// device_math.cuh -- per-walker wave-function arithmetic shared by the engine's kernels.
+//
+// Every function here is warp-cooperative (one warp owns one walker) or per-lane scalar.
+// T is the compute type of basis functions, orbitals, Jastrow and the nonlocal
+// quadrature (double in FP64 mode, float in mixed mode); inverses, log-determinants,
+// the accepted-move Sherman-Morrison update and energy sums are always double.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace champ {
+
+constexpr int MAXCT = 4;     // centre types
+constexpr int MAXORD = 8;    // norda, nordb <= 7
+constexpr int MAXT = 24;     // e-e-n terms (nordc <= 5)
+constexpr int MG = 4;        // Gaussian terms per pseudopotential channel
+constexpr int MAXLCH = 5;    // pseudopotential channels
+constexpr int MAXQ = 12;     // quadrature points
+constexpr double HB = 0.5;   // hbar^2 / 2m
+
+// ---------------------------------------------------------------------------------------
+// parameters (copied once per block into shared memory)
+// ---------------------------------------------------------------------------------------
+template <class T>
+struct JasPar {
+  T scalek;
+  int norda, nordb, nspin2b, nct;
+  T a4[MAXCT][MAXORD];
+  T b[2][MAXORD];
+  T c[MAXCT][MAXT];
+  T asymp_a[MAXCT];
+  T asymp_b[2];
+};
+
+struct EcpPar {
+  int npotd[MAXCT], lpotp1[MAXCT], nterm[MAXCT][MAXLCH];
+  double coef[MAXCT][MAXLCH][MG], expo[MAXCT][MAXLCH][MG];
+  int pw[MAXCT][MAXLCH][MG];
+  double znuc[MAXCT];
+  double q0[MAXQ][3], wq[MAXQ];
+  int nquad;
+};
+
+// System data in device memory (pointers into one allocation).
+template <class T>
+struct Sys {
+  int N, nup, ndn, C, nct, nshell, nbasis, nmax, nloc, nordc;
+  double pecent;
+  const double *cent;   // [C][3]
+  const int *ctype;     // [C]
+  const double *zc;     // [C] charge of centre
+  const int4 *shell;    // [nshell]: centre, n, l, kind
+  const int2 *shprim;   // [nshell]: first primitive, count
+  const int *shb0;      // [nshell] first basis function
+  const T *pz, *pc;     // primitive exponent, normalised weight
+  const int *bm;        // [nbasis] m
+  const T *cref[2];     // [nbasis][n_s] reference-determinant orbital coefficients
+  const JasPar<T> *jas;
+  const EcpPar *ecp;
+};
+
+// ---------------------------------------------------------------------------------------
+// small helpers
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ double texp(double x) { return exp(x); }
+__device__ __forceinline__ float texp(float x) { return expf(x); }
+__device__ __forceinline__ double tsqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float tsqrt(float x) { return sqrtf(x); }
+
+template <class V>
+__device__ __forceinline__ V warp_sum(V v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <class T>
+__device__ __forceinline__ T ipow(T r, int n) {
+  T p = 1;
+  for (int i = 0; i < n; i++) p *= r;
+  return p;
+}
+
+// ---------------------------------------------------------------------------------------
+// Philox4x32-10 counter-based generator (Salmon et al., SC'11) and the draws the
+// movers use: the same definition as the CPU checker.
+// ---------------------------------------------------------------------------------------
+__host__ __device__ inline void philox(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                       uint32_t *out) {
+  uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+    uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    uint32_t n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
+    c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+    k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+__host__ __device__ inline double u53(uint32_t a, uint32_t b) {
+  return ((double)(((uint64_t)(a >> 5) << 26) | (b >> 6)) + 0.5) * (1.0 / 9007199254740992.0);
+}
+__host__ __device__ inline double u32d(uint32_t a) { return ((double)a + 0.5) * (1.0 / 4294967296.0); }
+
+// Gaussian displacement (3) and accept uniform for (seed, walker, sweep, electron).
+__device__ inline void move_randoms(uint64_t seed, uint32_t w, uint64_t sweep, uint32_t e, double *g, double *ua) {
+  uint32_t a[4], b[4];
+  philox(seed, w, (uint32_t)sweep, (uint32_t)(sweep >> 32), 2u * e, a);
+  philox(seed, w, (uint32_t)sweep, (uint32_t)(sweep >> 32), 2u * e + 1u, b);
+  const double tp = 6.283185307179586;
+  double u1 = u53(a[0], a[1]), u2 = u53(a[2], a[3]);
+  double u3 = u53(b[0], b[1]), u4 = u32d(b[2]);
+  double r1 = sqrt(-2.0 * log(u1)), r2 = sqrt(-2.0 * log(u3));
+  double s2, c2, s4, c4;
+  sincos(tp * u2, &s2, &c2);
+  sincos(tp * u4, &s4, &c4);
+  g[0] = r1 * c2;
+  g[1] = r1 * s2;
+  g[2] = r2 * c4;
+  *ua = u32d(b[3]);
+}
+
+// Uniform random rotation (Shoemake's quaternion method) for (seed, walker, sweep).
+__device__ inline void random_rotation(uint64_t seed, uint32_t w, uint64_t sweep, double *R) {
+  uint32_t o[4];
+  philox(seed, w, (uint32_t)sweep, (uint32_t)(sweep >> 32), 0xFFFFFFFFu, o);
+  double u1 = u53(o[0], o[1]), u2 = u32d(o[2]), u3 = u32d(o[3]);
+  const double tp = 6.283185307179586;
+  double s1 = sqrt(1.0 - u1), s2 = sqrt(u1);
+  double sa, ca, sb, cb;
+  sincos(tp * u2, &sa, &ca);
+  sincos(tp * u3, &sb, &cb);
+  double qx = s1 * sa, qy = s1 * ca, qz = s2 * sb, qw = s2 * cb;
+  R[0] = 1 - 2 * (qy * qy + qz * qz); R[1] = 2 * (qx * qy - qz * qw); R[2] = 2 * (qx * qz + qy * qw);
+  R[3] = 2 * (qx * qy + qz * qw); R[4] = 1 - 2 * (qx * qx + qz * qz); R[5] = 2 * (qy * qz - qx * qw);
+  R[6] = 2 * (qx * qz - qy * qw); R[7] = 2 * (qy * qz + qx * qw); R[8] = 1 - 2 * (qx * qx + qy * qy);
+}
+
+// ---------------------------------------------------------------------------------------
+// Basis functions: radial shell x real solid harmonic (basis_fns.f90:38-474)
+// ---------------------------------------------------------------------------------------
+// S_lm = r^l C_lm(rhat) with the reference's normalisation and sign, and grad S.
+template <class T>
+__device__ __forceinline__ void solid_harm(int l, int m, T x, T y, T z, T &S, T *g) {
+  T x2 = x * x, y2 = y * y, z2 = z * z, rho2 = x2 + y2;
+  g[0] = g[1] = g[2] = T(0);
+  switch (l) {
+  case 0: S = T(1); return;
+  case 1:
+    if (m == 1) { S = x; g[0] = 1; }
+    else if (m == -1) { S = y; g[1] = 1; }
+    else { S = z; g[2] = 1; }
+    return;
+  case 2: {
+    const T s3 = T(1.7320508075688772);
+    if (m == 0) { S = T(0.5) * (2 * z2 - rho2); g[0] = -x; g[1] = -y; g[2] = 2 * z; }
+    else if (m == 1) { S = s3 * x * z; g[0] = s3 * z; g[2] = s3 * x; }
+    else if (m == -1) { S = s3 * y * z; g[1] = s3 * z; g[2] = s3 * y; }
+    else if (m == 2) { S = T(0.5) * s3 * (x2 - y2); g[0] = s3 * x; g[1] = -s3 * y; }
+    else { S = s3 * x * y; g[0] = s3 * y; g[1] = s3 * x; }
+    return;
+  }
+  case 3: {
+    const T c1 = T(0.61237243569579452), c2 = T(1.9364916731037085), c3 = T(0.79056941504209483);
+    if (m == 0) { S = z * z2 - T(1.5) * z * rho2; g[0] = -3 * x * z; g[1] = -3 * y * z; g[2] = 3 * z2 - T(1.5) * rho2; }
+    else if (m == 1) { S = c1 * x * (4 * z2 - rho2); g[0] = c1 * (4 * z2 - 3 * x2 - y2); g[1] = -2 * c1 * x * y; g[2] = 8 * c1 * x * z; }
+    else if (m == -1) { S = c1 * y * (4 * z2 - rho2); g[0] = -2 * c1 * x * y; g[1] = c1 * (4 * z2 - x2 - 3 * y2); g[2] = 8 * c1 * y * z; }
+    else if (m == 2) { S = c2 * z * (x2 - y2); g[0] = 2 * c2 * x * z; g[1] = -2 * c2 * y * z; g[2] = c2 * (x2 - y2); }
+    else if (m == -2) { S = 2 * c2 * x * y * z; g[0] = 2 * c2 * y * z; g[1] = 2 * c2 * x * z; g[2] = 2 * c2 * x * y; }
+    else if (m == 3) { S = c3 * (x * x2 - 3 * x * y2); g[0] = 3 * c3 * (x2 - y2); g[1] = -6 * c3 * x * y; }
+    else { S = c3 * (3 * x2 * y - y * y2); g[0] = 6 * c3 * x * y; g[1] = 3 * c3 * (x2 - y2); }
+    return;
+  }
+  default: {
+    const T c1 = T(0.79056941504209483), c2 = T(0.55901699437494742), c3 = T(2.0916500663351889),
+            c4 = T(0.73950997288745201);
+    if (m == 0) {
+      S = z2 * z2 - 3 * rho2 * z2 + T(0.375) * rho2 * rho2;
+      g[0] = -6 * x * z2 + T(1.5) * rho2 * x; g[1] = -6 * y * z2 + T(1.5) * rho2 * y; g[2] = 4 * z * z2 - 6 * rho2 * z;
+    } else if (m == 1) {
+      S = c1 * x * z * (4 * z2 - 3 * rho2);
+      g[0] = c1 * (4 * z * z2 - 9 * x2 * z - 3 * y2 * z); g[1] = -6 * c1 * x * y * z; g[2] = c1 * (12 * x * z2 - 3 * x * x2 - 3 * x * y2);
+    } else if (m == -1) {
+      S = c1 * y * z * (4 * z2 - 3 * rho2);
+      g[0] = -6 * c1 * x * y * z; g[1] = c1 * (4 * z * z2 - 3 * x2 * z - 9 * y2 * z); g[2] = c1 * (12 * y * z2 - 3 * x2 * y - 3 * y * y2);
+    } else if (m == 2) {
+      T P = 6 * z2 - rho2, Q = x2 - y2;
+      S = c2 * P * Q; g[0] = 2 * c2 * x * (P - Q); g[1] = -2 * c2 * y * (P + Q); g[2] = 12 * c2 * z * Q;
+    } else if (m == -2) {
+      T P = 6 * z2 - rho2;
+      S = 2 * c2 * P * x * y; g[0] = 2 * c2 * y * (P - 2 * x2); g[1] = 2 * c2 * x * (P - 2 * y2); g[2] = 24 * c2 * x * y * z;
+    } else if (m == 3) {
+      S = c3 * z * (x * x2 - 3 * x * y2); g[0] = 3 * c3 * z * (x2 - y2); g[1] = -6 * c3 * x * y * z; g[2] = c3 * (x * x2 - 3 * x * y2);
+    } else if (m == -3) {
+      S = c3 * z * (3 * x2 * y - y * y2); g[0] = 6 * c3 * x * y * z; g[1] = 3 * c3 * z * (x2 - y2); g[2] = c3 * (3 * x2 * y - y * y2);
+    } else if (m == 4) {
+      S = c4 * (x2 * x2 - 6 * x2 * y2 + y2 * y2); g[0] = c4 * (4 * x * x2 - 12 * x * y2); g[1] = c4 * (4 * y * y2 - 12 * x2 * y);
+    } else {
+      S = 4 * c4 * (x * x2 * y - x * y * y2); g[0] = c4 * (12 * x2 * y - 4 * y * y2); g[1] = c4 * (4 * x * x2 - 12 * x * y2);
+    }
+    return;
+  }
+  }
+}
+
+// Radial function R, R', R'' of one shell at distance r (wfv(1..3), basis_fns.f90:118-157).
+template <class T, bool DERIV>
+__device__ __forceinline__ void shell_radial(const Sys<T> &s, int ish, T r, T *R) {
+  int4 sh = s.shell[ish];
+  int2 pr = s.shprim[ish];
+  int n = sh.y;
+  T rn = T(n);
+  T rm1 = ipow(r, n - 1);
+  T ri = T(1) / r;
+  T rm2 = rm1 * ri, rm3 = rm2 * ri;
+  R[0] = R[1] = R[2] = T(0);
+  for (int p = pr.x; p < pr.x + pr.y; p++) {
+    T z = s.pz[p], w = s.pc[p];
+    if (sh.w == 0) {
+      T zr = z * r, ex = w * texp(-zr);
+      R[0] += rm1 * ex;
+      if (DERIV) {
+        R[1] += rm2 * ((rn - 1) - zr) * ex;
+        R[2] += rm3 * ((rn - 1) * (rn - 2 - zr) - (rn - 1 - zr) * zr) * ex;
+      }
+    } else {
+      T zr = 2 * z * r * r, ex = w * texp(T(-0.5) * zr);
+      R[0] += rm1 * ex;
+      if (DERIV) {
+        R[1] += rm2 * ((rn - 1) - zr) * ex;
+        R[2] += rm3 * ((rn - 1) * (rn - 2) - (2 * rn - 1 - zr) * zr) * ex;
+      }
+    }
+  }
+}
+
+// All basis functions of one shell at point pt; NCH=1 values, NCH=5 value, grad, laplacian.
+// out[b*NCH + ch] for the shell's basis functions b.
+template <class T, int NCH>
+__device__ __forceinline__ void shell_eval(const Sys<T> &s, int ish, const double *pt, T *out) {
+  int4 sh = s.shell[ish];
+  int c = sh.x, l = sh.z;
+  T d0 = T(pt[0] - s.cent[3 * c]), d1 = T(pt[1] - s.cent[3 * c + 1]), d2 = T(pt[2] - s.cent[3 * c + 2]);
+  T r2 = d0 * d0 + d1 * d1 + d2 * d2;
+  T r = tsqrt(r2);
+  if (r == T(0)) { r = T(1e-30); d0 = r; }
+  T R[3];
+  shell_radial<T, NCH == 5>(s, ish, r, R);
+  T ri = T(1) / r;
+  T ril = ipow(ri, l);
+  int b0 = s.shb0[ish];
+  for (int im = 0; im < 2 * l + 1; im++) {
+    int b = b0 + im;
+    T S, g[3];
+    solid_harm<T>(l, s.bm[b], d0, d1, d2, S, g);
+    T Y = S * ril;
+    out[b * NCH] = Y * R[0];
+    if (NCH == 5) {
+      T lr = T(l) * S * ril * ri * ri;
+      T dd[3] = {d0, d1, d2};
+#pragma unroll
+      for (int k = 0; k < 3; k++) out[b * NCH + 1 + k] = Y * dd[k] * ri * R[1] + (g[k] * ril - lr * dd[k]) * R[0];
+      out[b * NCH + 4] = Y * (R[2] + 2 * ri * R[1] - T(l * (l + 1)) * ri * ri * R[0]);
+    }
+  }
+}
+
+// Warp: all basis functions at pt into phi (shared memory).
+template <class T, int NCH>
+__device__ __forceinline__ void warp_basis(const Sys<T> &s, const double *pt, T *phi, int lane) {
+  for (int ish = lane; ish < s.nshell; ish += 32) shell_eval<T, NCH>(s, ish, pt, phi);
+  __syncwarp();
+}
+
+// Warp: orbitals o_m = sum_b coef[b][m] phi[b] for m < n (orbitals_loc_ana.f90:50-64).
+// Lanes are split into LM lanes along m and 32/LM along b, reduced by shuffles.
+// out[ch*ostride + m].
+template <class T, int NCH>
+__device__ __forceinline__ void warp_orbitals(const T *phi, const T *coef, int nbasis, int n, T *out, int ostride,
+                                              int lane) {
+  int LM = 1;
+  while (LM < n && LM < 32) LM <<= 1;
+  int LB = 32 / LM;
+  int lm = lane & (LM - 1), lb = lane / LM;
+  for (int m0 = 0; m0 < n; m0 += LM) {
+    int m = m0 + lm;
+    T acc[NCH];
+#pragma unroll
+    for (int ch = 0; ch < NCH; ch++) acc[ch] = T(0);
+    if (m < n) {
+      for (int b = lb; b < nbasis; b += LB) {
+        T cf = coef[b * n + m];
+#pragma unroll
+        for (int ch = 0; ch < NCH; ch++) acc[ch] += cf * phi[b * NCH + ch];
+      }
+    }
+    for (int o = LM; o < 32; o <<= 1)
+#pragma unroll
+      for (int ch = 0; ch < NCH; ch++) acc[ch] += __shfl_xor_sync(0xffffffffu, acc[ch], o);
+    if (lb == 0 && m < n)
+#pragma unroll
+      for (int ch = 0; ch < NCH; ch++) out[ch * ostride + m] = acc[ch];
+  }
+  __syncwarp();
+}
+
+// ---------------------------------------------------------------------------------------
+// Jastrow ijas=4, isc=4 (jastrow4.f90, scale_dist.f90:644-648, 857-884)
+// ---------------------------------------------------------------------------------------
+struct Terms {
+  int n;
+  int k[64], l[64], m[64];
+};
+__host__ __device__ constexpr Terms make_terms(int nord) {
+  Terms t{};
+  int i = 0;
+  for (int n = 2; n <= nord; n++)
+    for (int k = n - 1; k >= 0; k--) {
+      int l_hi = (k == 0) ? n - k - 2 : n - k;
+      for (int l = l_hi; l >= 0; l--) {
+        int m = (n - k - l) / 2;
+        if (2 * m == n - k - l) { t.k[i] = k; t.l[i] = l; t.m[i] = m; i++; }
+      }
+    }
+  t.n = i;
+  return t;
+}
+
+// spin class of pair (i,j): parallel spins use b set 2 (nspin2b=2) or 1/2 on b1.
+template <class T>
+__device__ __forceinline__ void pair_class(const JasPar<T> &J, int nup, int i, int j, int &isb, T &ss, int &ipar) {
+  bool par = (i < nup) == (j < nup);
+  ipar = par ? 1 : 0;
+  isb = (par && J.nspin2b == 2) ? 1 : 0;
+  ss = (par && J.nspin2b == 1) ? T(0.5) : T(1);
+}
+
+// e-e term: f, f'/r, f'' (jastrow4.f90:63-156)
+template <class T, bool DERIV>
+__device__ __forceinline__ T jas_ee(const JasPar<T> &J, int isb, T ss, int ipar, T rij, T &fu, T &fuu) {
+  T deni = T(1) / (T(1) + J.scalek * rij);
+  T u = rij * deni, dd1 = deni * deni, dd2 = -2 * J.scalek * deni * dd1;
+  T b1 = J.b[isb][0], b2 = J.b[isb][1];
+  T bot = T(1) + b2 * u;
+  T top = ss * b1 * u;
+  T f = top / bot - J.asymp_b[ipar];
+  T feeu = 0, feeuu = 0;
+  if (DERIV) {
+    feeu = ss * b1 / (bot * bot);
+    feeuu = -2 * feeu * b2 / bot;
+  }
+  T up = u, upm1 = T(1), upm2 = T(0);
+  for (int iord = 2; iord <= J.nordb; iord++) {
+    upm2 = upm1; upm1 = up; up = up * u;
+    T bb = J.b[isb][iord];
+    f += bb * up;
+    if (DERIV) {
+      feeu += bb * iord * upm1;
+      feeuu += bb * iord * (iord - 1) * upm2;
+    }
+  }
+  if (DERIV) {
+    fuu = feeuu * dd1 * dd1 + feeu * dd2;
+    fu = feeu * dd1 / rij;
+  }
+  return f;
+}
+
+// e-n term: f, f'/r, f'' (jastrow4.f90:354-455)
+template <class T, bool DERIV>
+__device__ __forceinline__ T jas_en(const JasPar<T> &J, int it, T ri, T &fi, T &fii) {
+  T deni = T(1) / (T(1) + J.scalek * ri);
+  T rr = ri * deni, dd7 = deni * deni, dd9 = -2 * J.scalek * deni * dd7;
+  T a1 = J.a4[it][0], a2 = J.a4[it][1];
+  T bot = T(1) + a2 * rr;
+  T f = a1 * rr / bot - J.asymp_a[it];
+  T feni = 0, fenii = 0;
+  if (DERIV) {
+    feni = a1 / (bot * bot);
+    fenii = -2 * feni * a2 / bot;
+  }
+  T p = rr, pm1 = T(1), pm2 = T(0);
+  for (int iord = 2; iord <= J.norda; iord++) {
+    pm2 = pm1; pm1 = p; p = p * rr;
+    T aa = J.a4[it][iord];
+    f += aa * p;
+    if (DERIV) {
+      feni += aa * iord * pm1;
+      fenii += aa * iord * (iord - 1) * pm2;
+    }
+  }
+  if (DERIV) {
+    fii = fenii * dd7 * dd7 + feni * dd9;
+    fi = feni * dd7 / ri;
+  }
+  return f;
+}
+
+template <class T>
+struct Een {
+  T fc, fu, fuu, fi, fii, fj, fjj, fui, fuj;
+};
+
+// e-e-n term for one centre (jastrow4.f90:159-336).  LEVEL 0: value, 1: + first
+// derivatives (fu, fi, fj), 2: everything.  Power tables carry two zero entries below 0.
+template <class T, int NORD, int LEVEL>
+__device__ __forceinline__ void jas_een(const JasPar<T> &J, int it, T rij, T ri, T rj, Een<T> &o) {
+  constexpr Terms tl = make_terms(NORD);
+  T sk = J.scalek;
+  T di = T(1) / (T(1) + sk * rij), dI = T(1) / (T(1) + sk * ri), dJ = T(1) / (T(1) + sk * rj);
+  // switched scaled distances 1 - k r/(1+k r) and their derivatives (switch_scale2)
+  T u1 = T(1) - sk * (rij * di), dd1 = -sk * di * di, dd2 = 2 * sk * sk * di * di * di;
+  T ri1 = T(1) - sk * (ri * dI), dd7 = -sk * dI * dI, dd9 = 2 * sk * sk * dI * dI * dI;
+  T rj1 = T(1) - sk * (rj * dJ), dd8 = -sk * dJ * dJ, dd10 = 2 * sk * sk * dJ * dJ * dJ;
+  T uu[NORD + 3], rri[NORD + 3], rrj[NORD + 3], ssv[NORD + 3], ttv[NORD + 3];
+  uu[0] = uu[1] = rri[0] = rri[1] = rrj[0] = rrj[1] = ssv[0] = ssv[1] = ttv[0] = ttv[1] = T(0);
+  uu[2] = 1; ssv[2] = 2; ttv[2] = 1; rri[2] = 1; rrj[2] = 1;
+#pragma unroll
+  for (int i = 1; i <= NORD; i++) {
+    uu[i + 2] = uu[i + 1] * u1;
+    rri[i + 2] = rri[i + 1] * ri1;
+    rrj[i + 2] = rrj[i + 1] * rj1;
+    ssv[i + 2] = rri[i + 2] + rrj[i + 2];
+    ttv[i + 2] = rri[i + 2] * rrj[i + 2];
+  }
+  T fc = 0, fu = 0, fuu = 0, fi = 0, fii = 0, fj = 0, fjj = 0, fui = 0, fuj = 0;
+  const T *c = J.c[it];
+#pragma unroll
+  for (int ll = 0; ll < tl.n; ll++) {
+    const int k = tl.k[ll], l = tl.l[ll], m = tl.m[ll];
+    T cc = c[ll];
+    T st = ssv[l + 2] * ttv[m + 2];
+    fc += cc * uu[k + 2] * st;
+    if (LEVEL >= 1) {
+      T pi_ = T(l + m) * rri[l + m + 1] * rrj[m + 2] + T(m) * rri[m + 1] * rrj[l + m + 2];
+      T pj_ = T(l + m) * rrj[l + m + 1] * rri[m + 2] + T(m) * rrj[m + 1] * rri[l + m + 2];
+      fu += cc * T(k) * uu[k + 1] * st;
+      fi += cc * uu[k + 2] * pi_;
+      fj += cc * uu[k + 2] * pj_;
+      if (LEVEL >= 2) {
+        fuu += cc * T(k * (k - 1)) * uu[k] * st;
+        fii += cc * uu[k + 2] * (T((l + m) * (l + m - 1)) * rri[l + m] * rrj[m + 2] + T(m * (m - 1)) * rri[m] * rrj[l + m + 2]);
+        fjj += cc * uu[k + 2] * (T((l + m) * (l + m - 1)) * rrj[l + m] * rri[m + 2] + T(m * (m - 1)) * rrj[m] * rri[l + m + 2]);
+        fui += cc * T(k) * uu[k + 1] * pi_;
+        fuj += cc * T(k) * uu[k + 1] * pj_;
+      }
+    }
+  }
+  o.fc = fc;
+  if (LEVEL >= 2) {
+    o.fuu = fuu * dd1 * dd1 + fu * dd2;
+    o.fui = fui * dd1 * dd7;
+    o.fuj = fuj * dd1 * dd8;
+    o.fii = fii * dd7 * dd7 + fi * dd9;
+    o.fjj = fjj * dd8 * dd8 + fj * dd10;
+  }
+  if (LEVEL >= 1) {
+    o.fu = fu * dd1 / rij;
+    o.fi = fi * dd7 / ri;
+    o.fj = fj * dd8 / rj;
+  }
+}
+
+}  // namespace champ

@@ -1,0 +1,179 @@
+"""ctypes binding of the engine's C ABI (include/champ_b200.h).
+
+``Engine`` mirrors the reference's per-walker interface for all walkers at once:
+``eval_full`` ~ hpsi, ``propose_1e`` ~ hpsie, ``accept_1e`` ~ jassav+detsav+dete_save,
+``grad_1e`` ~ eval_grad, ``set_walkers`` ~ psi_at, ``vmc_sweeps`` ~ the metrop sweep loop.
+Errors raise ``ChampError`` carrying the library's message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .system import System
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libchamp_b200.so")
+
+EXPORTED_SYMBOLS = [
+    "champ_last_error", "champ_version", "champ_create", "champ_destroy", "champ_nparam",
+    "champ_set_walkers", "champ_get_walkers", "champ_set_quadrature_rotation", "champ_eval_full",
+    "champ_propose_1e", "champ_accept_1e", "champ_grad_1e", "champ_vmc_sweeps", "champ_vmc_run_host",
+    "champ_walker_status", "champ_synchronize",
+]
+
+PREC = {"fp64": 0, "mixed": 1}
+
+_lib = None
+
+
+class ChampError(RuntimeError):
+    pass
+
+
+class EvalOut(C.Structure):
+    _fields_ = [(n, C.POINTER(C.c_double)) for n in
+                ("lnpsi", "sign", "psij", "velocity", "div_v", "d2lnpsi", "pe", "pe_ee", "pe_nonloc", "energy")]
+
+
+class VmcStats(C.Structure):
+    _fields_ = [(n, C.POINTER(C.c_double)) for n in ("esum", "e2sum", "accept", "elast")]
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the CUDA engine.  Raises if the library has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ChampError(f"engine library not built: {path} (run python -m champ_b200.build)")
+    L = C.CDLL(path)
+    vp, i32, dp, u64 = C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.c_uint64
+    L.champ_last_error.restype = C.c_char_p
+    L.champ_version.restype = C.c_char_p
+    L.champ_create.argtypes = [vp, i32, i32, vp, C.POINTER(vp)]
+    L.champ_destroy.argtypes = [vp]
+    L.champ_nparam.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
+    L.champ_set_walkers.argtypes = [vp, i32, dp]
+    L.champ_get_walkers.argtypes = [vp, dp]
+    L.champ_set_quadrature_rotation.argtypes = [vp, dp]
+    L.champ_eval_full.argtypes = [vp, C.POINTER(EvalOut)]
+    L.champ_propose_1e.argtypes = [vp, i32, dp, dp, dp]
+    L.champ_accept_1e.argtypes = [vp, i32, C.POINTER(C.c_uint8)]
+    L.champ_grad_1e.argtypes = [vp, i32, dp]
+    L.champ_vmc_sweeps.argtypes = [vp, i32, u64, u64, C.c_double, C.POINTER(VmcStats)]
+    L.champ_vmc_run_host.argtypes = [vp, i32, dp, i32, u64, u64, C.c_double, dp]
+    L.champ_walker_status.argtypes = [vp, C.POINTER(C.c_uint32)]
+    L.champ_synchronize.argtypes = [vp]
+    for n in EXPORTED_SYMBOLS:
+        if n not in ("champ_last_error", "champ_version"):
+            getattr(L, n).restype = C.c_int
+    _lib = L
+    return L
+
+
+def _p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Engine:
+    """One engine context (one system, up to w_max walkers, one precision)."""
+
+    def __init__(self, system: System, w_max: int, precision: str = "fp64", stream: int = 0):
+        self.lib = load_library()
+        self.system = system
+        self.N = system.nelec
+        self.w_max = w_max
+        self._cs, self._keep = system.to_c()
+        h = C.c_void_p()
+        self._check(self.lib.champ_create(C.byref(self._cs), w_max, PREC[precision], C.c_void_p(stream), C.byref(h)))
+        self.h = h
+        self.nw = 0
+
+    def _check(self, rc):
+        if rc != 0:
+            raise ChampError(f"champ error {rc}: {self.lib.champ_last_error().decode()}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.champ_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- walkers
+    def set_walkers(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        self.nw = x.shape[0]
+        self._check(self.lib.champ_set_walkers(self.h, self.nw, _p(x)))
+
+    def get_walkers(self):
+        x = np.zeros((self.nw, self.N, 3))
+        self._check(self.lib.champ_get_walkers(self.h, _p(x)))
+        return x
+
+    def set_rotation(self, rot=None):
+        if rot is None:
+            self._check(self.lib.champ_set_quadrature_rotation(self.h, None))
+        else:
+            r = np.ascontiguousarray(rot, np.float64)
+            self._check(self.lib.champ_set_quadrature_rotation(self.h, _p(r)))
+
+    # -- hpsi
+    def eval_full(self):
+        nw, N = self.nw, self.N
+        out = {k: np.zeros(nw) for k in ("lnpsi", "sign", "psij", "d2lnpsi", "pe", "pe_ee", "pe_nonloc", "energy")}
+        out["velocity"] = np.zeros((nw, N, 3))
+        out["div_v"] = np.zeros((nw, N))
+        eo = EvalOut(**{k: _p(v) for k, v in out.items()})
+        self._check(self.lib.champ_eval_full(self.h, C.byref(eo)))
+        return out
+
+    # -- single-electron moves
+    def propose_1e(self, iel, xnew, grad=False):
+        xnew = np.ascontiguousarray(xnew, np.float64).reshape(self.nw, 3)
+        ratio = np.zeros(self.nw)
+        g = np.zeros((self.nw, 3)) if grad else None
+        self._check(self.lib.champ_propose_1e(self.h, iel, _p(xnew), _p(ratio), _p(g) if grad else None))
+        return (ratio, g) if grad else ratio
+
+    def accept_1e(self, iel, accept):
+        a = np.ascontiguousarray(accept, np.uint8)
+        self._check(self.lib.champ_accept_1e(self.h, iel, a.ctypes.data_as(C.POINTER(C.c_uint8))))
+
+    def grad_1e(self, iel):
+        g = np.zeros((self.nw, 3))
+        self._check(self.lib.champ_grad_1e(self.h, iel, _p(g)))
+        return g
+
+    # -- VMC
+    def vmc_sweeps(self, nsweep, seed, sweep0=0, step=0.5, stats=True):
+        if not stats:
+            self._check(self.lib.champ_vmc_sweeps(self.h, nsweep, seed, sweep0, step, None))
+            return None
+        out = {k: np.zeros(self.nw) for k in ("esum", "e2sum", "accept", "elast")}
+        st = VmcStats(**{k: _p(v) for k, v in out.items()})
+        self._check(self.lib.champ_vmc_sweeps(self.h, nsweep, seed, sweep0, step, C.byref(st)))
+        return out
+
+    def vmc_run_host(self, x, nsweep, seed, sweep0=0, step=0.5):
+        x = np.ascontiguousarray(x, np.float64).copy()
+        nw = x.shape[0]
+        el = np.zeros(nw)
+        self._check(self.lib.champ_vmc_run_host(self.h, nw, _p(x), nsweep, seed, sweep0, step, _p(el)))
+        self.nw = nw
+        return x, el
+
+    def walker_status(self):
+        f = np.zeros(self.nw, np.uint32)
+        self._check(self.lib.champ_walker_status(self.h, f.ctypes.data_as(C.POINTER(C.c_uint32))))
+        return f
+
+    def synchronize(self):
+        self._check(self.lib.champ_synchronize(self.h))

@@ -1,0 +1,197 @@
+/*
+ * champ_b200.h -- C ABI of the walker-batched Slater-Jastrow engine.
+ *
+ * The engine evaluates, for all walkers at once on one B200, what CHAMP's
+ * per-walker wave-function routines evaluate one walker at a time:
+ *
+ *   champ_eval_full   <->  hpsi            (qmc/vmc/hpsi.f90:2)
+ *   champ_propose_1e  <->  hpsie           (qmc/vmc/hpsie.f90:1)
+ *   champ_accept_1e   <->  jassav + detsav + dete_save
+ *                          (qmc/vmc/jassav.f90:1, qmc/vmc/detsav.f90:1, qmc/dete_mod.f90:75)
+ *   champ_grad_1e     <->  eval_grad / calc_1e_derivatives
+ *                          (qmc/dete_mod.f90:249, qmc/psi_utils_mod.f90:457)
+ *   champ_set_walkers <->  psi_at for every walker (qmc/psi_utils_mod.f90:13)
+ *   champ_vmc_sweeps  <->  the metrop_mov1 sweep loop + hpsi per sweep
+ *                          (qmc/vmc/metrop_mov1.f90:64-296, qmc/vmc/vmc.f90:250-331)
+ *   champ_dmc_steps   <->  rundmc walker/electron loops (qmc/rundmc_mod.f90:123-365)
+ *   champ_param_grad  <->  dpsi_bld / deloc_bld (qmc/deriv_mod.f90:248,437)
+ *   champ_accumulate_oh <-> dpsi_dpsi / dpsi_deloc / dpsi_dpsi_eloc averages
+ *                          (qmc/deriv_mod.f90:683,1375,898)
+ *
+ * Conventions
+ *   - All indices are 0-based.  Electrons 0..nup-1 are spin up, nup..nelec-1 spin down.
+ *   - Host arrays are C row-major.  Walker arrays are walker-major: x[w][e][k].
+ *   - Every entry point returns 0 on success and a positive CHAMP_E* code on error;
+ *     champ_last_error() gives a message.  Nothing calls exit() or traps.
+ *   - A context owns its device buffers and works on the CUDA stream given at create.
+ */
+#ifndef CHAMP_B200_H
+#define CHAMP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CHAMP_OK 0
+#define CHAMP_EINVAL 1      /* bad argument or size beyond the compiled limits */
+#define CHAMP_ECUDA 2       /* CUDA runtime error */
+#define CHAMP_ENOMEM 3      /* device allocation failed */
+#define CHAMP_ESTATE 4      /* call out of order (e.g. propose before set_walkers) */
+#define CHAMP_ESINGULAR 5   /* a walker hit a singular Slater matrix (see champ_walker_status) */
+
+#define CHAMP_PREC_FP64 0   /* every step in FP64 */
+#define CHAMP_PREC_MIXED 1  /* orbitals, Jastrow, NLPP quadrature in FP32; inverse, log-det,
+                               accepted Sherman-Morrison update and E_L sums in FP64 */
+
+/* Per-walker status bits (champ_walker_status). */
+#define CHAMP_WS_SINGULAR 1u   /* Slater matrix singular at the last full evaluation */
+#define CHAMP_WS_NONFINITE 2u  /* non-finite E_L or ln|psi| */
+
+/* Maximum sizes the kernels are compiled for. */
+#define CHAMP_MAX_ELEC 256
+#define CHAMP_MAX_SPIN 64      /* electrons of one spin */
+#define CHAMP_MAX_L 4
+#define CHAMP_MAX_CTYPE 8
+#define CHAMP_MAX_NORD 7
+#define CHAMP_MAX_LCHAN 5      /* pseudopotential l channels (npotd) */
+
+/*
+ * System descriptor: everything the reference reads from its input menus
+ * (nuclei, basis, orbitals, csfs, jastrow, pseudo blocks).  Pointers are host
+ * pointers; they are copied at champ_create and may be freed afterwards.
+ */
+typedef struct champ_system {
+  int32_t nelec, nup;
+  int32_t ncent, nctype;
+  const double *cent;          /* [ncent][3] */
+  const int32_t *iwctype;      /* [ncent] centre type */
+  const double *znuc;          /* [nctype] nuclear (or pseudo-atom) charge */
+
+  /* Basis (qmc/vmc/basis_fns.f90:38-474): a shell is one radial function on one centre,
+     R(r) = sum_p coef_p * N(n,l,zeta_p) * r^(n-1) * exp(-zeta_p r)     (Slater, kind 0)
+                                          * exp(-zeta_p r^2)   (Gaussian, kind 1)
+     N is the reference normalisation (qmc/vmc/basis_norm.f90), including sqrt((2l+1)/4pi).
+     Basis function b = R_shell(b)(r) * C_{l,m}(rhat), C the real harmonics of basis_fns. */
+  int32_t nshell;
+  const int32_t *shell_cent;   /* [nshell] */
+  const int32_t *shell_n;      /* [nshell] */
+  const int32_t *shell_l;      /* [nshell] 0..4 */
+  const int32_t *shell_kind;   /* [nshell] 0 Slater, 1 Gaussian */
+  const int32_t *shell_nprim;  /* [nshell] */
+  const double *prim_zeta;     /* [sum nprim] */
+  const double *prim_coef;     /* [sum nprim] contraction weights */
+  int32_t nbasis;
+  const int32_t *basis_shell;  /* [nbasis] shell of basis function; shells contiguous */
+  const int32_t *basis_m;      /* [nbasis] m in -l..l (x=+1, y=-1, z=0 for l=1) */
+
+  /* Orbitals: orb_i = sum_b coef[i][b] * basis_b  (coef(ibasis,iorb) in the reference). */
+  int32_t norb;
+  const double *coef;          /* [norb][nbasis] */
+
+  /* Determinants and CSFs (qmc/csfs_mod.f90, qmc/deriv_fast_mod.f90:144). */
+  int32_t ndet;
+  const int32_t *det_orb;      /* [ndet][nelec] orbital in column j (iworbd) */
+  int32_t ncsf;
+  const double *csf_coef;      /* [ncsf] */
+  const int32_t *csf_ndet;     /* [ncsf] */
+  const int32_t *csf_det;      /* [sum csf_ndet] determinant index */
+  const double *csf_det_coef;  /* [sum csf_ndet] (cdet_in_csf) */
+
+  /* Jastrow ijas=4, isc=4 (qmc/vmc/jastrow4.f90, qmc/vmc/scale_dist.f90). */
+  double scalek;
+  int32_t norda, nordb, nordc;
+  int32_t nspin2b;             /* 1: one b set (parallel spins get 1/2 on b1); 2: separate sets */
+  int32_t een_cusp;            /* nonzero: dependent e-e-n coefficients are set from the
+                                  cusp conditions (qmc/fit/cuspinit4.f90, cuspexact4.f90) */
+  const double *a4;            /* [nctype][norda+1] */
+  const double *b;             /* [nspin2b][nordb+1] */
+  const double *c;             /* [nctype][nterms4(nordc)] */
+
+  /* Pseudopotential (nloc=6: Gaussian ECP, qmc/vmc/readps_gauss.f90:126-165). */
+  int32_t nloc;                /* 0 all-electron, 6 Gaussian ECP */
+  int32_t nquad;               /* 12 (icosahedral rule of qmc/vmc/rotqua.f90) */
+  int32_t mgauss;              /* max terms per channel */
+  const int32_t *npotd;        /* [nctype] number of l channels */
+  const int32_t *lpotp1;       /* [nctype] 1-based local channel */
+  const int32_t *necp_term;    /* [nctype][CHAMP_MAX_LCHAN] terms of channel l (0-based l) */
+  const int32_t *necp_power;   /* [nctype][CHAMP_MAX_LCHAN][mgauss] */
+  const double *ecp_coef;      /* [nctype][CHAMP_MAX_LCHAN][mgauss] */
+  const double *ecp_exponent;  /* [nctype][CHAMP_MAX_LCHAN][mgauss] */
+} champ_system;
+
+/* Outputs of a full evaluation (hpsi).  Host pointers; any may be NULL. */
+typedef struct champ_eval_out {
+  double *lnpsi;     /* [nw] ln|psi| = ln|D| + J */
+  double *sign;      /* [nw] sign of D */
+  double *psij;      /* [nw] J = ln(Jastrow) */
+  double *velocity;  /* [nw][nelec][3] grad ln psi */
+  double *div_v;     /* [nw][nelec] */
+  double *d2lnpsi;   /* [nw] sum_i lap_i ln psi */
+  double *pe;        /* [nw] total potential energy (local + nonlocal + e-e + n-n) */
+  double *pe_ee;     /* [nw] e-e Coulomb energy (pei) */
+  double *pe_nonloc; /* [nw] nonlocal pseudopotential energy */
+  double *energy;    /* [nw] local energy E_L */
+} champ_eval_out;
+
+/* Per-walker VMC accumulators (acues1 in the reference).  Host pointers; any may be NULL. */
+typedef struct champ_vmc_stats {
+  double *esum;      /* [nw] sum of E_L over the sweeps of the call */
+  double *e2sum;     /* [nw] sum of E_L^2 */
+  double *accept;    /* [nw] accepted single-electron moves */
+  double *elast;     /* [nw] E_L after the last sweep */
+} champ_vmc_stats;
+
+typedef struct champ_ctx champ_ctx;
+
+const char *champ_last_error(void);
+const char *champ_version(void);
+
+/* Context. precision = CHAMP_PREC_*; stream = cudaStream_t (NULL: default stream). */
+int champ_create(const champ_system *sys, int32_t w_max, int32_t precision, void *stream,
+                 champ_ctx **out);
+int champ_destroy(champ_ctx *ctx);
+int champ_nparam(const champ_ctx *ctx, int32_t *nparm_jas, int32_t *nparm_csf, int32_t *nparm_orb);
+
+/* Walker positions.  psi_at for every walker: sets x and runs a full evaluation,
+   rebuilding inverses and Jastrow tables (qmc/psi_utils_mod.f90:13). */
+int champ_set_walkers(champ_ctx *ctx, int32_t nw, const double *x /* host [nw][nelec][3] */);
+int champ_get_walkers(champ_ctx *ctx, double *x /* host [nw][nelec][3] */);
+
+/* Rotation applied to the nonlocal quadrature grid (rotqua, qmc/vmc/rotqua.f90:621).
+   rot = row-major 3x3 orthogonal matrix; NULL resets to the identity. */
+int champ_set_quadrature_rotation(champ_ctx *ctx, const double *rot);
+
+/* hpsi for all walkers at their current positions. */
+int champ_eval_full(champ_ctx *ctx, const champ_eval_out *out);
+
+/* hpsie: psi(x with electron iel at xnew)/psi(x) for every walker, and grad ln psi of
+   electron iel at the new position (grad_new may be NULL). */
+int champ_propose_1e(champ_ctx *ctx, int32_t iel, const double *xnew /* [nw][3] */,
+                     double *ratio /* [nw] */, double *grad_new /* [nw][3] or NULL */);
+/* Accept the last proposal of electron iel where accept[w] != 0. */
+int champ_accept_1e(champ_ctx *ctx, int32_t iel, const uint8_t *accept /* [nw] */);
+/* grad ln psi of electron iel at the current positions. */
+int champ_grad_1e(champ_ctx *ctx, int32_t iel, double *grad /* [nw][3] */);
+
+/* Fused VMC: nsweep sweeps of single-electron Metropolis moves (Gaussian proposal of
+   width step), with a full E_L evaluation after every sweep, all on the device.
+   Random numbers come from a counter-based generator keyed by (seed, walker, sweep). */
+int champ_vmc_sweeps(champ_ctx *ctx, int32_t nsweep, uint64_t seed, uint64_t sweep0,
+                     double step, const champ_vmc_stats *stats);
+
+/* Same as champ_vmc_sweeps, but the walkers come from and go back to host memory and
+   the per-walker E_L of the last sweep is copied back (the call a host driver makes). */
+int champ_vmc_run_host(champ_ctx *ctx, int32_t nw, double *x /* host [nw][nelec][3], in/out */,
+                       int32_t nsweep, uint64_t seed, uint64_t sweep0, double step,
+                       double *eloc /* host [nw] */);
+
+int champ_walker_status(champ_ctx *ctx, uint32_t *flags /* [nw] */);
+int champ_synchronize(champ_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CHAMP_B200_H */
