@@ -45,7 +45,7 @@ struct EcpPar {
 template <class T>
 struct Sys {
   int N, nup, ndn, C, nct, nshell, nbasis, nmax, nloc, nordc;
-  double pecent;
+  double pecent, scalek;
   const double *cent;   // [C][3]
   const int *ctype;     // [C]
   const double *zc;     // [C] charge of centre
@@ -53,8 +53,9 @@ struct Sys {
   const int2 *shprim;   // [nshell]: first primitive, count
   const int *shb0;      // [nshell] first basis function
   const T *pz, *pc;     // primitive exponent, normalised weight
-  const int *bm;        // [nbasis] m
-  const T *cref[2];     // [nbasis][n_s] reference-determinant orbital coefficients
+  const T *cref[2];     // [nbasis][n_s] reference-determinant orbital coefficients; rows in the
+                        // internal basis order (each shell's functions in harmonic-slot order
+                        // m = 0, 1, -1, 2, -2, ...)
   const JasPar<T> *jas;
   const EcpPar *ecp;
 };
@@ -142,64 +143,73 @@ __device__ inline void random_rotation(uint64_t seed, uint32_t w, uint64_t sweep
 // ---------------------------------------------------------------------------------------
 // Basis functions: radial shell x real solid harmonic (basis_fns.f90:38-474)
 // ---------------------------------------------------------------------------------------
-// S_lm = r^l C_lm(rhat) with the reference's normalisation and sign, and grad S.
-template <class T>
-__device__ __forceinline__ void solid_harm(int l, int m, T x, T y, T z, T &S, T *g) {
+// All 2l+1 solid harmonics of degree l at once, in slot order m = 0, 1, -1, 2, -2, ...
+// (slot(m) = 0, 2m-1 for m > 0, -2m for m < 0), with gradients if GRAD.
+template <class T, bool GRAD>
+__device__ __forceinline__ void solid_all(int l, T x, T y, T z, T *S, T (*G)[3]) {
   T x2 = x * x, y2 = y * y, z2 = z * z, rho2 = x2 + y2;
-  g[0] = g[1] = g[2] = T(0);
+  if (GRAD)
+    for (int i = 0; i < 2 * l + 1; i++) G[i][0] = G[i][1] = G[i][2] = T(0);
   switch (l) {
-  case 0: S = T(1); return;
+  case 0:
+    S[0] = T(1);
+    return;
   case 1:
-    if (m == 1) { S = x; g[0] = 1; }
-    else if (m == -1) { S = y; g[1] = 1; }
-    else { S = z; g[2] = 1; }
+    S[0] = z; S[1] = x; S[2] = y;
+    if (GRAD) { G[0][2] = 1; G[1][0] = 1; G[2][1] = 1; }
     return;
   case 2: {
     const T s3 = T(1.7320508075688772);
-    if (m == 0) { S = T(0.5) * (2 * z2 - rho2); g[0] = -x; g[1] = -y; g[2] = 2 * z; }
-    else if (m == 1) { S = s3 * x * z; g[0] = s3 * z; g[2] = s3 * x; }
-    else if (m == -1) { S = s3 * y * z; g[1] = s3 * z; g[2] = s3 * y; }
-    else if (m == 2) { S = T(0.5) * s3 * (x2 - y2); g[0] = s3 * x; g[1] = -s3 * y; }
-    else { S = s3 * x * y; g[0] = s3 * y; g[1] = s3 * x; }
+    S[0] = T(0.5) * (2 * z2 - rho2); S[1] = s3 * x * z; S[2] = s3 * y * z;
+    S[3] = T(0.5) * s3 * (x2 - y2); S[4] = s3 * x * y;
+    if (GRAD) {
+      G[0][0] = -x; G[0][1] = -y; G[0][2] = 2 * z;
+      G[1][0] = s3 * z; G[1][2] = s3 * x;
+      G[2][1] = s3 * z; G[2][2] = s3 * y;
+      G[3][0] = s3 * x; G[3][1] = -s3 * y;
+      G[4][0] = s3 * y; G[4][1] = s3 * x;
+    }
     return;
   }
   case 3: {
     const T c1 = T(0.61237243569579452), c2 = T(1.9364916731037085), c3 = T(0.79056941504209483);
-    if (m == 0) { S = z * z2 - T(1.5) * z * rho2; g[0] = -3 * x * z; g[1] = -3 * y * z; g[2] = 3 * z2 - T(1.5) * rho2; }
-    else if (m == 1) { S = c1 * x * (4 * z2 - rho2); g[0] = c1 * (4 * z2 - 3 * x2 - y2); g[1] = -2 * c1 * x * y; g[2] = 8 * c1 * x * z; }
-    else if (m == -1) { S = c1 * y * (4 * z2 - rho2); g[0] = -2 * c1 * x * y; g[1] = c1 * (4 * z2 - x2 - 3 * y2); g[2] = 8 * c1 * y * z; }
-    else if (m == 2) { S = c2 * z * (x2 - y2); g[0] = 2 * c2 * x * z; g[1] = -2 * c2 * y * z; g[2] = c2 * (x2 - y2); }
-    else if (m == -2) { S = 2 * c2 * x * y * z; g[0] = 2 * c2 * y * z; g[1] = 2 * c2 * x * z; g[2] = 2 * c2 * x * y; }
-    else if (m == 3) { S = c3 * (x * x2 - 3 * x * y2); g[0] = 3 * c3 * (x2 - y2); g[1] = -6 * c3 * x * y; }
-    else { S = c3 * (3 * x2 * y - y * y2); g[0] = 6 * c3 * x * y; g[1] = 3 * c3 * (x2 - y2); }
+    T q = 4 * z2 - rho2;
+    S[0] = z * z2 - T(1.5) * z * rho2; S[1] = c1 * x * q; S[2] = c1 * y * q;
+    S[3] = c2 * z * (x2 - y2); S[4] = 2 * c2 * x * y * z;
+    S[5] = c3 * (x * x2 - 3 * x * y2); S[6] = c3 * (3 * x2 * y - y * y2);
+    if (GRAD) {
+      G[0][0] = -3 * x * z; G[0][1] = -3 * y * z; G[0][2] = 3 * z2 - T(1.5) * rho2;
+      G[1][0] = c1 * (4 * z2 - 3 * x2 - y2); G[1][1] = -2 * c1 * x * y; G[1][2] = 8 * c1 * x * z;
+      G[2][0] = -2 * c1 * x * y; G[2][1] = c1 * (4 * z2 - x2 - 3 * y2); G[2][2] = 8 * c1 * y * z;
+      G[3][0] = 2 * c2 * x * z; G[3][1] = -2 * c2 * y * z; G[3][2] = c2 * (x2 - y2);
+      G[4][0] = 2 * c2 * y * z; G[4][1] = 2 * c2 * x * z; G[4][2] = 2 * c2 * x * y;
+      G[5][0] = 3 * c3 * (x2 - y2); G[5][1] = -6 * c3 * x * y;
+      G[6][0] = 6 * c3 * x * y; G[6][1] = 3 * c3 * (x2 - y2);
+    }
     return;
   }
   default: {
     const T c1 = T(0.79056941504209483), c2 = T(0.55901699437494742), c3 = T(2.0916500663351889),
             c4 = T(0.73950997288745201);
-    if (m == 0) {
-      S = z2 * z2 - 3 * rho2 * z2 + T(0.375) * rho2 * rho2;
-      g[0] = -6 * x * z2 + T(1.5) * rho2 * x; g[1] = -6 * y * z2 + T(1.5) * rho2 * y; g[2] = 4 * z * z2 - 6 * rho2 * z;
-    } else if (m == 1) {
-      S = c1 * x * z * (4 * z2 - 3 * rho2);
-      g[0] = c1 * (4 * z * z2 - 9 * x2 * z - 3 * y2 * z); g[1] = -6 * c1 * x * y * z; g[2] = c1 * (12 * x * z2 - 3 * x * x2 - 3 * x * y2);
-    } else if (m == -1) {
-      S = c1 * y * z * (4 * z2 - 3 * rho2);
-      g[0] = -6 * c1 * x * y * z; g[1] = c1 * (4 * z * z2 - 3 * x2 * z - 9 * y2 * z); g[2] = c1 * (12 * y * z2 - 3 * x2 * y - 3 * y * y2);
-    } else if (m == 2) {
-      T P = 6 * z2 - rho2, Q = x2 - y2;
-      S = c2 * P * Q; g[0] = 2 * c2 * x * (P - Q); g[1] = -2 * c2 * y * (P + Q); g[2] = 12 * c2 * z * Q;
-    } else if (m == -2) {
-      T P = 6 * z2 - rho2;
-      S = 2 * c2 * P * x * y; g[0] = 2 * c2 * y * (P - 2 * x2); g[1] = 2 * c2 * x * (P - 2 * y2); g[2] = 24 * c2 * x * y * z;
-    } else if (m == 3) {
-      S = c3 * z * (x * x2 - 3 * x * y2); g[0] = 3 * c3 * z * (x2 - y2); g[1] = -6 * c3 * x * y * z; g[2] = c3 * (x * x2 - 3 * x * y2);
-    } else if (m == -3) {
-      S = c3 * z * (3 * x2 * y - y * y2); g[0] = 6 * c3 * x * y * z; g[1] = 3 * c3 * z * (x2 - y2); g[2] = c3 * (3 * x2 * y - y * y2);
-    } else if (m == 4) {
-      S = c4 * (x2 * x2 - 6 * x2 * y2 + y2 * y2); g[0] = c4 * (4 * x * x2 - 12 * x * y2); g[1] = c4 * (4 * y * y2 - 12 * x2 * y);
-    } else {
-      S = 4 * c4 * (x * x2 * y - x * y * y2); g[0] = c4 * (12 * x2 * y - 4 * y * y2); g[1] = c4 * (4 * x * x2 - 12 * x * y2);
+    T P = 6 * z2 - rho2, Q = x2 - y2, q = 4 * z2 - 3 * rho2;
+    S[0] = z2 * z2 - 3 * rho2 * z2 + T(0.375) * rho2 * rho2;
+    S[1] = c1 * x * z * q; S[2] = c1 * y * z * q;
+    S[3] = c2 * P * Q; S[4] = 2 * c2 * P * x * y;
+    S[5] = c3 * z * (x * x2 - 3 * x * y2); S[6] = c3 * z * (3 * x2 * y - y * y2);
+    S[7] = c4 * (x2 * x2 - 6 * x2 * y2 + y2 * y2); S[8] = 4 * c4 * (x * x2 * y - x * y * y2);
+    if (GRAD) {
+      G[0][0] = -6 * x * z2 + T(1.5) * rho2 * x; G[0][1] = -6 * y * z2 + T(1.5) * rho2 * y;
+      G[0][2] = 4 * z * z2 - 6 * rho2 * z;
+      G[1][0] = c1 * (4 * z * z2 - 9 * x2 * z - 3 * y2 * z); G[1][1] = -6 * c1 * x * y * z;
+      G[1][2] = c1 * (12 * x * z2 - 3 * x * x2 - 3 * x * y2);
+      G[2][0] = -6 * c1 * x * y * z; G[2][1] = c1 * (4 * z * z2 - 3 * x2 * z - 9 * y2 * z);
+      G[2][2] = c1 * (12 * y * z2 - 3 * x2 * y - 3 * y * y2);
+      G[3][0] = 2 * c2 * x * (P - Q); G[3][1] = -2 * c2 * y * (P + Q); G[3][2] = 12 * c2 * z * Q;
+      G[4][0] = 2 * c2 * y * (P - 2 * x2); G[4][1] = 2 * c2 * x * (P - 2 * y2); G[4][2] = 24 * c2 * x * y * z;
+      G[5][0] = 3 * c3 * z * (x2 - y2); G[5][1] = -6 * c3 * x * y * z; G[5][2] = c3 * (x * x2 - 3 * x * y2);
+      G[6][0] = 6 * c3 * x * y * z; G[6][1] = 3 * c3 * z * (x2 - y2); G[6][2] = c3 * (3 * x2 * y - y * y2);
+      G[7][0] = c4 * (4 * x * x2 - 12 * x * y2); G[7][1] = c4 * (4 * y * y2 - 12 * x2 * y);
+      G[8][0] = c4 * (12 * x2 * y - 4 * y * y2); G[8][1] = c4 * (4 * x * x2 - 12 * x * y2);
     }
     return;
   }
@@ -251,21 +261,47 @@ __device__ __forceinline__ void shell_eval(const Sys<T> &s, int ish, const doubl
   shell_radial<T, NCH == 5>(s, ish, r, R);
   T ri = T(1) / r;
   T ril = ipow(ri, l);
+  T S[9], G[9][3];
+  solid_all<T, NCH == 5>(l, d0, d1, d2, S, G);
+  // the shell's basis functions are stored in harmonic-slot order: b = b0 + slot
   int b0 = s.shb0[ish];
-  for (int im = 0; im < 2 * l + 1; im++) {
-    int b = b0 + im;
-    T S, g[3];
-    solid_harm<T>(l, s.bm[b], d0, d1, d2, S, g);
-    T Y = S * ril;
-    out[b * NCH] = Y * R[0];
-    if (NCH == 5) {
-      T lr = T(l) * S * ril * ri * ri;
-      T dd[3] = {d0, d1, d2};
+  const int nm = 2 * l + 1;
 #pragma unroll
-      for (int k = 0; k < 3; k++) out[b * NCH + 1 + k] = Y * dd[k] * ri * R[1] + (g[k] * ril - lr * dd[k]) * R[0];
-      out[b * NCH + 4] = Y * (R[2] + 2 * ri * R[1] - T(l * (l + 1)) * ri * ri * R[0]);
+  for (int sl = 0; sl < 9; sl++) {
+    if (sl < nm) {
+      int b = b0 + sl;
+      T Y = S[sl] * ril;
+      out[b * NCH] = Y * R[0];
+      if (NCH == 5) {
+        T lr = T(l) * S[sl] * ril * ri * ri;
+        out[b * NCH + 1] = Y * d0 * ri * R[1] + (G[sl][0] * ril - lr * d0) * R[0];
+        out[b * NCH + 2] = Y * d1 * ri * R[1] + (G[sl][1] * ril - lr * d1) * R[0];
+        out[b * NCH + 3] = Y * d2 * ri * R[1] + (G[sl][2] * ril - lr * d2) * R[0];
+        out[b * NCH + 4] = Y * (R[2] + 2 * ri * R[1] - T(l * (l + 1)) * ri * ri * R[0]);
+      }
     }
   }
+}
+
+// Values of all basis functions of one shell at pt contracted with g: sum_b phi_b(pt) g_b.
+template <class T>
+__device__ __forceinline__ T shell_dot(const Sys<T> &s, int ish, const double *pt, const T *g) {
+  int4 sh = s.shell[ish];
+  int c = sh.x, l = sh.z;
+  T d0 = T(pt[0] - s.cent[3 * c]), d1 = T(pt[1] - s.cent[3 * c + 1]), d2 = T(pt[2] - s.cent[3 * c + 2]);
+  T r = tsqrt(d0 * d0 + d1 * d1 + d2 * d2);
+  if (r == T(0)) { r = T(1e-30); d0 = r; }
+  T R[3];
+  shell_radial<T, false>(s, ish, r, R);
+  T S[9], G[9][3];
+  solid_all<T, false>(l, d0, d1, d2, S, G);
+  int b0 = s.shb0[ish];
+  const int nm = 2 * l + 1;
+  T acc = 0;
+#pragma unroll
+  for (int sl = 0; sl < 9; sl++)
+    if (sl < nm) acc += S[sl] * g[b0 + sl];
+  return acc * ipow(T(1) / r, l) * R[0];
 }
 
 // Warp: all basis functions at pt into phi (shared memory).
@@ -338,15 +374,17 @@ __device__ __forceinline__ void pair_class(const JasPar<T> &J, int nup, int i, i
   ss = (par && J.nspin2b == 1) ? T(0.5) : T(1);
 }
 
+// In all Jastrow terms d = 1/(1 + scalek r) is passed in: the isc=4 scaled distance is
+// r d (scale_dist2, scale_dist.f90:644-648) and the switched one used by the e-e-n term
+// is 1 - scalek r d = d (switch_scale2, scale_dist.f90:857-884).
+
 // e-e term: f, f'/r, f'' (jastrow4.f90:63-156)
 template <class T, bool DERIV>
-__device__ __forceinline__ T jas_ee(const JasPar<T> &J, int isb, T ss, int ipar, T rij, T &fu, T &fuu) {
-  T deni = T(1) / (T(1) + J.scalek * rij);
-  T u = rij * deni, dd1 = deni * deni, dd2 = -2 * J.scalek * deni * dd1;
+__device__ __forceinline__ T jas_ee(const JasPar<T> &J, int isb, T ss, int ipar, T rij, T deni, T &fu, T &fuu) {
+  T u = rij * deni;
   T b1 = J.b[isb][0], b2 = J.b[isb][1];
   T bot = T(1) + b2 * u;
-  T top = ss * b1 * u;
-  T f = top / bot - J.asymp_b[ipar];
+  T f = ss * b1 * u / bot - J.asymp_b[ipar];
   T feeu = 0, feeuu = 0;
   if (DERIV) {
     feeu = ss * b1 / (bot * bot);
@@ -363,6 +401,7 @@ __device__ __forceinline__ T jas_ee(const JasPar<T> &J, int isb, T ss, int ipar,
     }
   }
   if (DERIV) {
+    T dd1 = deni * deni, dd2 = -2 * J.scalek * deni * dd1;
     fuu = feeuu * dd1 * dd1 + feeu * dd2;
     fu = feeu * dd1 / rij;
   }
@@ -371,9 +410,8 @@ __device__ __forceinline__ T jas_ee(const JasPar<T> &J, int isb, T ss, int ipar,
 
 // e-n term: f, f'/r, f'' (jastrow4.f90:354-455)
 template <class T, bool DERIV>
-__device__ __forceinline__ T jas_en(const JasPar<T> &J, int it, T ri, T &fi, T &fii) {
-  T deni = T(1) / (T(1) + J.scalek * ri);
-  T rr = ri * deni, dd7 = deni * deni, dd9 = -2 * J.scalek * deni * dd7;
+__device__ __forceinline__ T jas_en(const JasPar<T> &J, int it, T ri, T deni, T &fi, T &fii) {
+  T rr = ri * deni;
   T a1 = J.a4[it][0], a2 = J.a4[it][1];
   T bot = T(1) + a2 * rr;
   T f = a1 * rr / bot - J.asymp_a[it];
@@ -393,6 +431,7 @@ __device__ __forceinline__ T jas_en(const JasPar<T> &J, int it, T ri, T &fi, T &
     }
   }
   if (DERIV) {
+    T dd7 = deni * deni, dd9 = -2 * J.scalek * deni * dd7;
     fii = fenii * dd7 * dd7 + feni * dd9;
     fi = feni * dd7 / ri;
   }
@@ -407,14 +446,11 @@ struct Een {
 // e-e-n term for one centre (jastrow4.f90:159-336).  LEVEL 0: value, 1: + first
 // derivatives (fu, fi, fj), 2: everything.  Power tables carry two zero entries below 0.
 template <class T, int NORD, int LEVEL>
-__device__ __forceinline__ void jas_een(const JasPar<T> &J, int it, T rij, T ri, T rj, Een<T> &o) {
+__device__ __forceinline__ void jas_een(const JasPar<T> &J, int it, T rij, T du, T ri, T di, T rj, T dj,
+                                        Een<T> &o) {
   constexpr Terms tl = make_terms(NORD);
   T sk = J.scalek;
-  T di = T(1) / (T(1) + sk * rij), dI = T(1) / (T(1) + sk * ri), dJ = T(1) / (T(1) + sk * rj);
-  // switched scaled distances 1 - k r/(1+k r) and their derivatives (switch_scale2)
-  T u1 = T(1) - sk * (rij * di), dd1 = -sk * di * di, dd2 = 2 * sk * sk * di * di * di;
-  T ri1 = T(1) - sk * (ri * dI), dd7 = -sk * dI * dI, dd9 = 2 * sk * sk * dI * dI * dI;
-  T rj1 = T(1) - sk * (rj * dJ), dd8 = -sk * dJ * dJ, dd10 = 2 * sk * sk * dJ * dJ * dJ;
+  T u1 = du, ri1 = di, rj1 = dj;
   T uu[NORD + 3], rri[NORD + 3], rrj[NORD + 3], ssv[NORD + 3], ttv[NORD + 3];
   uu[0] = uu[1] = rri[0] = rri[1] = rrj[0] = rrj[1] = ssv[0] = ssv[1] = ttv[0] = ttv[1] = T(0);
   uu[2] = 1; ssv[2] = 2; ttv[2] = 1; rri[2] = 1; rrj[2] = 1;
@@ -450,14 +486,17 @@ __device__ __forceinline__ void jas_een(const JasPar<T> &J, int it, T rij, T ri,
     }
   }
   o.fc = fc;
-  if (LEVEL >= 2) {
-    o.fuu = fuu * dd1 * dd1 + fu * dd2;
-    o.fui = fui * dd1 * dd7;
-    o.fuj = fuj * dd1 * dd8;
-    o.fii = fii * dd7 * dd7 + fi * dd9;
-    o.fjj = fjj * dd8 * dd8 + fj * dd10;
-  }
   if (LEVEL >= 1) {
+    // derivatives of the switched scaled distances: -k d^2 and 2 k^2 d^3
+    T dd1 = -sk * du * du, dd7 = -sk * di * di, dd8 = -sk * dj * dj;
+    if (LEVEL >= 2) {
+      T dd2 = 2 * sk * sk * du * du * du, dd9 = 2 * sk * sk * di * di * di, dd10 = 2 * sk * sk * dj * dj * dj;
+      o.fuu = fuu * dd1 * dd1 + fu * dd2;
+      o.fui = fui * dd1 * dd7;
+      o.fuj = fuj * dd1 * dd8;
+      o.fii = fii * dd7 * dd7 + fi * dd9;
+      o.fjj = fjj * dd8 * dd8 + fj * dd10;
+    }
     o.fu = fu * dd1 / rij;
     o.fi = fi * dd7 / ri;
     o.fj = fj * dd8 / rj;

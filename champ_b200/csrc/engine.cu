@@ -30,6 +30,7 @@ struct State {
   double *x;       // [W][N][3]
   double *ainv;    // [W][astride]; spin-up block at 0 (nup x nup), spin-down at nup*nup
   T *fso;          // [W][N][N]
+  T *ren;          // [W][N][C][2]: r_en and 1/(1 + scalek r_en)
   double *fsum, *lnd, *sgn;
   uint32_t *status;
   T *pf;           // [W][N] proposed pair values
@@ -47,41 +48,107 @@ struct State {
 };
 constexpr int NLT = 2 + MAXLCH;  // task record: (e*C+c), r, vps[0..MAXLCH-1]
 
-// Per-warp shared-memory layout.
+// Per-warp shared-memory layout, computed on the host.  When `resident` is set the
+// walker's whole state and scratch live in shared memory for the life of a kernel
+// (small systems); otherwise they stay in HBM.
+struct Layout {
+  size_t phi, arow, xs, vacc, divj, colb, vb, perm, rnew;  // always in shared memory
+  size_t ainv, fso, ren, pf, orb5, gproj, nlt;             // resident mode only
+  size_t bytes;
+  int resident;
+};
+
+// Per-walker view: where this walker's arrays live for the current kernel.
 template <class T>
-struct WarpMem {
-  T *phi;        // [nbasis*5]
-  T *arow;       // [5*nmax]
-  double *xs;    // [N*3]
-  double *vacc;  // [N*3]
-  double *divj;  // [N]
-  double *colb;  // [nmax]
-  double *vb;    // [nmax]
-  int *perm;     // [nmax]
+struct View {
+  T *phi, *arow;
+  double *xs, *vacc, *divj, *colb, *vb;
+  int *perm;
+  T *rnew;         // [C][2] proposed electron's distances to the centres
+  double *ainv;
+  T *fso, *ren, *pf, *orb5, *gproj;
+  double *nlt;
 };
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
 
 template <class T>
-__host__ __device__ inline size_t warp_smem_bytes(int N, int nbasis, int nmax) {
-  return align16(sizeof(T) * nbasis * 5) + align16(sizeof(T) * 5 * nmax) + 3 * align16(sizeof(double) * N * 3) +
-         align16(sizeof(double) * N) + 2 * align16(sizeof(double) * nmax) + align16(sizeof(int) * nmax);
+static Layout make_layout(int N, int C, int nbasis, int nmax, int astride, bool nl, size_t resident_limit) {
+  Layout L;
+  size_t o = 0;
+  auto take = [&](size_t b) { size_t r = o; o += align16(b); return r; };
+  L.phi = take(sizeof(T) * nbasis * 5);
+  L.arow = take(sizeof(T) * 5 * nmax);
+  L.xs = take(sizeof(double) * N * 3);
+  L.vacc = take(sizeof(double) * N * 3);
+  L.divj = take(sizeof(double) * N);
+  L.colb = take(sizeof(double) * nmax);
+  L.vb = take(sizeof(double) * nmax);
+  L.perm = take(sizeof(int) * nmax);
+  L.rnew = take(sizeof(T) * C * 2);
+  size_t base = o;
+  L.ainv = take(sizeof(double) * astride);
+  L.fso = take(sizeof(T) * N * N);
+  L.ren = take(sizeof(T) * N * C * 2);
+  L.pf = take(sizeof(T) * N);
+  L.orb5 = take(sizeof(T) * N * 5 * nmax);
+  L.gproj = nl ? take(sizeof(T) * N * nbasis) : 0;
+  L.nlt = nl ? take(sizeof(double) * N * C * NLT) : 0;
+  L.resident = (o <= resident_limit) ? 1 : 0;
+  L.bytes = L.resident ? o : base;
+  return L;
 }
 
 template <class T>
-__device__ inline WarpMem<T> carve(char *base, int N, int nbasis, int nmax) {
-  WarpMem<T> m;
-  char *p = base;
-  m.phi = (T *)p; p += align16(sizeof(T) * nbasis * 5);
-  m.arow = (T *)p; p += align16(sizeof(T) * 5 * nmax);
-  m.xs = (double *)p; p += align16(sizeof(double) * N * 3);
-  m.vacc = (double *)p; p += align16(sizeof(double) * N * 3);
-  p += align16(sizeof(double) * N * 3);  // spare (det gradients are reduced in registers)
-  m.divj = (double *)p; p += align16(sizeof(double) * N);
-  m.colb = (double *)p; p += align16(sizeof(double) * nmax);
-  m.vb = (double *)p; p += align16(sizeof(double) * nmax);
-  m.perm = (int *)p;
-  return m;
+__device__ inline View<T> make_view(char *base, const Layout &L, const State<T> &st, int w, int N, int C, int nbasis,
+                                    int nmax, bool resident) {
+  View<T> v;
+  v.phi = (T *)(base + L.phi);
+  v.arow = (T *)(base + L.arow);
+  v.xs = (double *)(base + L.xs);
+  v.vacc = (double *)(base + L.vacc);
+  v.divj = (double *)(base + L.divj);
+  v.colb = (double *)(base + L.colb);
+  v.vb = (double *)(base + L.vb);
+  v.perm = (int *)(base + L.perm);
+  v.rnew = (T *)(base + L.rnew);
+  if (resident) {
+    v.ainv = (double *)(base + L.ainv);
+    v.fso = (T *)(base + L.fso);
+    v.ren = (T *)(base + L.ren);
+    v.pf = (T *)(base + L.pf);
+    v.orb5 = (T *)(base + L.orb5);
+    v.gproj = (T *)(base + L.gproj);
+    v.nlt = (double *)(base + L.nlt);
+  } else {
+    v.ainv = st.ainv + (size_t)w * st.astride;
+    v.fso = st.fso + (size_t)w * N * N;
+    v.ren = st.ren + (size_t)w * N * C * 2;
+    v.pf = st.pf + (size_t)w * N;
+    v.orb5 = st.orb5 + (size_t)w * N * 5 * nmax;
+    v.gproj = st.gproj ? st.gproj + (size_t)w * N * nbasis : nullptr;
+    v.nlt = st.nlt ? st.nlt + (size_t)w * N * C * NLT : nullptr;
+  }
+  return v;
+}
+
+// Copy a walker's persistent state between HBM and its resident view.
+template <class T>
+__device__ inline void view_load(const View<T> &v, const State<T> &st, int w, int N, int C, int lane) {
+  for (int i = lane; i < 3 * N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * N + i];
+  for (int i = lane; i < st.astride; i += 32) v.ainv[i] = st.ainv[(size_t)w * st.astride + i];
+  for (int i = lane; i < N * N; i += 32) v.fso[i] = st.fso[(size_t)w * N * N + i];
+  for (int i = lane; i < N * C * 2; i += 32) v.ren[i] = st.ren[(size_t)w * N * C * 2 + i];
+  __syncwarp();
+}
+template <class T>
+__device__ inline void view_store(const View<T> &v, const State<T> &st, int w, int N, int C, int lane) {
+  __syncwarp();
+  for (int i = lane; i < 3 * N; i += 32) st.x[(size_t)w * 3 * N + i] = v.xs[i];
+  for (int i = lane; i < st.astride; i += 32) st.ainv[(size_t)w * st.astride + i] = v.ainv[i];
+  for (int i = lane; i < N * N; i += 32) st.fso[(size_t)w * N * N + i] = v.fso[i];
+  for (int i = lane; i < N * C * 2; i += 32) st.ren[(size_t)w * N * C * 2 + i] = v.ren[i];
+  __syncwarp();
 }
 
 // ---------------------------------------------------------------------------------------
@@ -174,50 +241,40 @@ __device__ __forceinline__ void ecp_vps(const EcpPar &E, int it, double r, doubl
   }
 }
 
-// Jastrow value (and gradient wrt the first electron) of pair (e at xe, j at xj).
+// distance of point p to centre c and 1/(1 + scalek r)
+template <class T>
+__device__ __forceinline__ void cen_dist(const Sys<T> &s, T sk, const double *p, int c, T &r, T &d) {
+  const double *cc = s.cent + 3 * c;
+  T a = T(p[0] - cc[0]), b = T(p[1] - cc[1]), e = T(p[2] - cc[2]);
+  r = tsqrt(a * a + b * b + e * e);
+  d = T(1) / (T(1) + sk * r);
+}
+
+// Jastrow pair term (e-e + e-e-n) for electron e at xe (distances re[c][2]) and
+// electron j at xj (distances rj[c][2]); gradient wrt xe if GRAD.
 template <class T, int NORD, bool GRAD>
 __device__ __forceinline__ T pair_value(const Sys<T> &s, const JasPar<T> &J, int e, int j, const double *xe,
-                                        const double *xj, T *g) {
+                                        const T *re, const double *xj, const T *rj, T *g) {
   int isb, ipar;
   T ss;
   pair_class(J, s.nup, e, j, isb, ss, ipar);
   T rv[3] = {T(xe[0] - xj[0]), T(xe[1] - xj[1]), T(xe[2] - xj[2])};
   T rij = tsqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
+  T du = T(1) / (T(1) + J.scalek * rij);
   T fu = 0, fuu = 0;
-  T f = jas_ee<T, GRAD>(J, isb, ss, ipar, rij, fu, fuu);
+  T f = jas_ee<T, GRAD>(J, isb, ss, ipar, rij, du, fu, fuu);
   if (GRAD) { g[0] = fu * rv[0]; g[1] = fu * rv[1]; g[2] = fu * rv[2]; }
   if (NORD > 1) {
     for (int c = 0; c < s.C; c++) {
-      const double *cc = s.cent + 3 * c;
-      T rvi[3] = {T(xe[0] - cc[0]), T(xe[1] - cc[1]), T(xe[2] - cc[2])};
-      T rvj[3] = {T(xj[0] - cc[0]), T(xj[1] - cc[1]), T(xj[2] - cc[2])};
-      T ri = tsqrt(rvi[0] * rvi[0] + rvi[1] * rvi[1] + rvi[2] * rvi[2]);
-      T rj = tsqrt(rvj[0] * rvj[0] + rvj[1] * rvj[1] + rvj[2] * rvj[2]);
       Een<T> o;
-      jas_een<T, NORD, GRAD ? 1 : 0>(J, s.ctype[c], rij, ri, rj, o);
+      jas_een<T, NORD, GRAD ? 1 : 0>(J, s.ctype[c], rij, du, re[2 * c], re[2 * c + 1], rj[2 * c], rj[2 * c + 1], o);
       f += o.fc;
-      if (GRAD)
+      if (GRAD) {
+        const double *cc = s.cent + 3 * c;
 #pragma unroll
-        for (int k = 0; k < 3; k++) g[k] += o.fi * rvi[k] + o.fu * rv[k];
+        for (int k = 0; k < 3; k++) g[k] += o.fi * T(xe[k] - cc[k]) + o.fu * rv[k];
+      }
     }
-  }
-  return f;
-}
-
-// e-n Jastrow sum over centres handled by this lane (c = lane, lane+32, ...).
-template <class T, bool GRAD>
-__device__ __forceinline__ T en_partial(const Sys<T> &s, const JasPar<T> &J, const double *xe, T *g, int lane) {
-  T f = 0;
-  if (GRAD) g[0] = g[1] = g[2] = T(0);
-  for (int c = lane; c < s.C; c += 32) {
-    const double *cc = s.cent + 3 * c;
-    T rv[3] = {T(xe[0] - cc[0]), T(xe[1] - cc[1]), T(xe[2] - cc[2])};
-    T r = tsqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
-    T fi = 0, fii = 0;
-    f += jas_en<T, GRAD>(J, s.ctype[c], r, fi, fii);
-    if (GRAD)
-#pragma unroll
-      for (int k = 0; k < 3; k++) g[k] += fi * rv[k];
   }
   return f;
 }
@@ -232,14 +289,23 @@ struct EvalRes {
 
 template <class T, int NORD>
 __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, const State<T> &st, int w,
-                          const WarpMem<T> &sm, const double *R, int lane, bool outputs, EvalRes &res) {
+                          const View<T> &v, const double *R, int lane, bool outputs, EvalRes &res) {
   const int N = s.N, C = s.C, nmax = s.nmax;
-  const double *xs = sm.xs;
-  T *fso = st.fso + (size_t)w * N * N;
-  // --- Jastrow (jastrow4.f90) and e-e Coulomb (distances.f90:131-158)
-  for (int i = lane; i < 3 * N; i += 32) sm.vacc[i] = 0;
-  for (int i = lane; i < N; i += 32) sm.divj[i] = 0;
+  const double *xs = v.xs;
+  T *fso = v.fso;
+  const T sk = J.scalek;
+  // --- electron-nucleus distance table (distances.f90:16-27)
+  for (int i = lane; i < N * C; i += 32) {
+    int e = i / C, c = i - e * C;
+    T r, d;
+    cen_dist(s, sk, xs + 3 * e, c, r, d);
+    v.ren[2 * i] = r;
+    v.ren[2 * i + 1] = d;
+  }
+  for (int i = lane; i < 3 * N; i += 32) v.vacc[i] = 0;
+  for (int i = lane; i < N; i += 32) v.divj[i] = 0;
   __syncwarp();
+  // --- Jastrow (jastrow4.f90) and e-e Coulomb (distances.f90:131-158)
   double fsum = 0, d2j = 0, pe_ee = 0, pe_en = 0;
   const int npair = N * (N - 1) / 2;
   for (int p = lane; p < npair; p += 32) {
@@ -251,31 +317,30 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
     int isb, ipar;
     T ss;
     pair_class(J, s.nup, i, j, isb, ss, ipar);
-    T rv[3] = {T(xi[0] - xj[0]), T(xi[1] - xj[1]), T(xi[2] - xj[2])};
-    T rij = tsqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
-    double rijd = sqrt((xi[0] - xj[0]) * (xi[0] - xj[0]) + (xi[1] - xj[1]) * (xi[1] - xj[1]) +
-                       (xi[2] - xj[2]) * (xi[2] - xj[2]));
+    double dx = xi[0] - xj[0], dy = xi[1] - xj[1], dz = xi[2] - xj[2];
+    double rijd = sqrt(dx * dx + dy * dy + dz * dz);
     pe_ee += 1.0 / rijd;
+    T rv[3] = {T(dx), T(dy), T(dz)};
+    T rij = tsqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
+    T du = T(1) / (T(1) + sk * rij);
     T fu, fuu;
-    T f = jas_ee<T, true>(J, isb, ss, ipar, rij, fu, fuu);
+    T f = jas_ee<T, true>(J, isb, ss, ipar, rij, du, fu, fuu);
     T gi[3], gj[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) { gi[k] = fu * rv[k]; gj[k] = -fu * rv[k]; }
     T d2 = 2 * (fuu + 2 * fu);
     if (NORD > 1) {
+      const T *ri_ = v.ren + 2 * C * i, *rj_ = v.ren + 2 * C * j;
       for (int c = 0; c < C; c++) {
         const double *cc = s.cent + 3 * c;
-        T rvi[3] = {T(xi[0] - cc[0]), T(xi[1] - cc[1]), T(xi[2] - cc[2])};
-        T rvj[3] = {T(xj[0] - cc[0]), T(xj[1] - cc[1]), T(xj[2] - cc[2])};
-        T ri = tsqrt(rvi[0] * rvi[0] + rvi[1] * rvi[1] + rvi[2] * rvi[2]);
-        T rj = tsqrt(rvj[0] * rvj[0] + rvj[1] * rvj[1] + rvj[2] * rvj[2]);
+        T ri = ri_[2 * c], rj = rj_[2 * c];
         Een<T> o;
-        jas_een<T, NORD, 2>(J, s.ctype[c], rij, ri, rj, o);
+        jas_een<T, NORD, 2>(J, s.ctype[c], rij, du, ri, ri_[2 * c + 1], rj, rj_[2 * c + 1], o);
         f += o.fc;
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-          gi[k] += o.fi * rvi[k] + o.fu * rv[k];
-          gj[k] += o.fj * rvj[k] - o.fu * rv[k];
+          gi[k] += o.fi * T(xi[k] - cc[k]) + o.fu * rv[k];
+          gj[k] += o.fj * T(xj[k] - cc[k]) - o.fu * rv[k];
         }
         T sp = ri + rj, tm = ri - rj;
         d2 += 2 * (2 * o.fu + o.fi + o.fj) + 2 * o.fuu + o.fii + o.fjj + o.fui * (rij * rij + sp * tm) / (ri * rij) +
@@ -286,11 +351,11 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
     d2j += (double)d2;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-      atomicAdd(&sm.vacc[3 * i + k], (double)gi[k]);
-      atomicAdd(&sm.vacc[3 * j + k], (double)gj[k]);
+      atomicAdd(&v.vacc[3 * i + k], (double)gi[k]);
+      atomicAdd(&v.vacc[3 * j + k], (double)gj[k]);
     }
-    atomicAdd(&sm.divj[i], 0.5 * (double)d2);
-    atomicAdd(&sm.divj[j], 0.5 * (double)d2);
+    atomicAdd(&v.divj[i], 0.5 * (double)d2);
+    atomicAdd(&v.divj[j], 0.5 * (double)d2);
     fso[i * N + j] = f;
     fso[j * N + i] = f;
   }
@@ -300,12 +365,11 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
     T f = 0, d2 = 0, g[3] = {0, 0, 0};
     for (int c = 0; c < C; c++) {
       const double *cc = s.cent + 3 * c;
-      T rv[3] = {T(xi[0] - cc[0]), T(xi[1] - cc[1]), T(xi[2] - cc[2])};
-      T r = tsqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
+      T r = v.ren[2 * (i * C + c)], dn = v.ren[2 * (i * C + c) + 1];
       T fi, fii;
-      f += jas_en<T, true>(J, s.ctype[c], r, fi, fii);
+      f += jas_en<T, true>(J, s.ctype[c], r, dn, fi, fii);
 #pragma unroll
-      for (int k = 0; k < 3; k++) g[k] += fi * rv[k];
+      for (int k = 0; k < 3; k++) g[k] += fi * T(xi[k] - cc[k]);
       d2 += fii + 2 * fi;
       if (s.nloc == 0) {
         double rd = sqrt((xi[0] - cc[0]) * (xi[0] - cc[0]) + (xi[1] - cc[1]) * (xi[1] - cc[1]) +
@@ -316,8 +380,8 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
     fsum += (double)f;
     d2j += (double)d2;
 #pragma unroll
-    for (int k = 0; k < 3; k++) sm.vacc[3 * i + k] += (double)g[k];
-    sm.divj[i] += (double)d2;
+    for (int k = 0; k < 3; k++) v.vacc[3 * i + k] += (double)g[k];
+    v.divj[i] += (double)d2;
     fso[i * N + i] = f;
   }
   fsum = warp_sum(fsum);
@@ -327,14 +391,14 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
   __syncwarp();
 
   // --- orbitals of every electron, Slater matrices (determinant.f90:36-42, t_bld)
-  double *ainv = st.ainv + (size_t)w * st.astride;
-  T *orb5 = st.orb5 + (size_t)w * N * 5 * nmax;
+  double *ainv = v.ainv;
+  T *orb5 = v.orb5;
   for (int e = 0; e < N; e++) {
     int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
     double *A = ainv + (sp ? s.nup * s.nup : 0);
-    warp_basis<T, 5>(s, xs + 3 * e, sm.phi, lane);
+    warp_basis<T, 5>(s, xs + 3 * e, v.phi, lane);
     T *oe = orb5 + (size_t)e * 5 * nmax;
-    warp_orbitals<T, 5>(sm.phi, s.cref[sp], s.nbasis, n, oe, nmax, lane);
+    warp_orbitals<T, 5>(v.phi, s.cref[sp], s.nbasis, n, oe, nmax, lane);
     for (int k = lane; k < n; k += 32) A[eo * n + k] = (double)oe[k];
   }
   __syncwarp();
@@ -344,7 +408,7 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
     int n = sp ? s.ndn : s.nup;
     if (n == 0) continue;
     double l1, s1;
-    bool o1 = warp_gj(ainv + (sp ? s.nup * s.nup : 0), n, sm.perm, l1, s1, lane);
+    bool o1 = warp_gj(ainv + (sp ? s.nup * s.nup : 0), n, v.perm, l1, s1, lane);
     ok = ok && o1;
     lnd += l1;
     sgn *= s1;
@@ -366,12 +430,12 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
     g0 = warp_sum(g0); g1 = warp_sum(g1); g2 = warp_sum(g2); lp = warp_sum(lp);
     double dvd = lp - (g0 * g0 + g1 * g1 + g2 * g2);
     d2lnd += dvd;
-    double vx = sm.vacc[3 * e] + g0, vy = sm.vacc[3 * e + 1] + g1, vz = sm.vacc[3 * e + 2] + g2;
+    double vx = v.vacc[3 * e] + g0, vy = v.vacc[3 * e + 1] + g1, vz = v.vacc[3 * e + 2] + g2;
     v2 += vx * vx + vy * vy + vz * vz;
     if (outputs && lane == 0) {
       double *ov = st.o_vel + ((size_t)w * N + e) * 3;
       ov[0] = vx; ov[1] = vy; ov[2] = vz;
-      st.o_divv[(size_t)w * N + e] = sm.divj[e] + dvd;
+      st.o_divv[(size_t)w * N + e] = v.divj[e] + dvd;
     }
   }
 
@@ -379,7 +443,8 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
   double vloc = 0, vnl = 0;
   if (s.nloc > 0 && ok) {
     const int B = s.nbasis;
-    T *gp = st.gproj + (size_t)w * N * B;
+    T *gp = v.gproj;
+    // G projected onto the basis: g_e[b] = sum_k coef[b][k] Ainv[k][e] (psp_nonloc_pot_bld)
     for (int e = 0; e < N; e++) {
       int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
       const double *A = ainv + (sp ? s.nup * s.nup : 0);
@@ -390,15 +455,15 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
         gp[(size_t)e * B + b] = (T)acc;
       }
     }
-    double *tl = st.nlt + (size_t)w * N * C * NLT;
+    double *tl = v.nlt;
     int ntask = 0;
     for (int base = 0; base < N * C; base += 32) {
       int idx = base + lane;
       bool nl = false;
       double vps[MAXLCH], r = 0;
-      int e = 0, c = 0;
+      int c = 0;
       if (idx < N * C) {
-        e = idx / C;
+        int e = idx / C;
         c = idx - e * C;
         const double *cc = s.cent + 3 * c, *xe = xs + 3 * e;
         r = sqrt((xe[0] - cc[0]) * (xe[0] - cc[0]) + (xe[1] - cc[1]) * (xe[1] - cc[1]) +
@@ -433,46 +498,42 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
       for (int k = 0; k < 3; k++) qv[k] = R[3 * k] * E.q0[q][0] + R[3 * k + 1] * E.q0[q][1] + R[3 * k + 2] * E.q0[q][2];
       double costh = ((xe[0] - cc[0]) * qv[0] + (xe[1] - cc[1]) * qv[1] + (xe[2] - cc[2]) * qv[2]) / r;
       double xn[3] = {cc[0] + r * qv[0], cc[1] + r * qv[1], cc[2] + r * qv[2]};
-      // determinant ratio: orbitals at the point contracted with G (psp_nonloc_pot_bld)
+      // determinant ratio: orbitals at the point contracted with G
       const T *ge = gp + (size_t)e * B;
       T dr = 0;
-      for (int ish = 0; ish < s.nshell; ish++) {
-        int4 sh = s.shell[ish];
-        int cs = sh.x, l = sh.z;
-        T d0 = T(xn[0] - s.cent[3 * cs]), d1 = T(xn[1] - s.cent[3 * cs + 1]), d2 = T(xn[2] - s.cent[3 * cs + 2]);
-        T rr = tsqrt(d0 * d0 + d1 * d1 + d2 * d2);
-        if (rr == T(0)) { rr = T(1e-30); d0 = rr; }
-        T Rv[3];
-        shell_radial<T, false>(s, ish, rr, Rv);
-        T ril = ipow(T(1) / rr, l);
-        int b0 = s.shb0[ish];
-        T acc = 0;
-        for (int im = 0; im < 2 * l + 1; im++) {
-          T S, g[3];
-          solid_harm<T>(l, s.bm[b0 + im], d0, d1, d2, S, g);
-          acc += S * ge[b0 + im];
-        }
-        dr += acc * ril * Rv[0];
-      }
-      // Jastrow ratio (nonlocj)
+      for (int ish = 0; ish < s.nshell; ish++) dr += shell_dot<T>(s, ish, xn, ge);
+      // Jastrow ratio (nonlocj, nonloc.f90:432-522)
       double dj = 0;
       for (int j = 0; j < N; j++) {
         if (j == e) continue;
-        T g3[3];
-        T f = pair_value<T, NORD, false>(s, J, e, j, xn, xs + 3 * j, g3);
+        int isb, ipar;
+        T ss;
+        pair_class(J, s.nup, e, j, isb, ss, ipar);
+        const double *xj = xs + 3 * j;
+        T a0 = T(xn[0] - xj[0]), a1 = T(xn[1] - xj[1]), a2 = T(xn[2] - xj[2]);
+        T rij = tsqrt(a0 * a0 + a1 * a1 + a2 * a2);
+        T du = T(1) / (T(1) + sk * rij);
+        T fu, fuu;
+        T f = jas_ee<T, false>(J, isb, ss, ipar, rij, du, fu, fuu);
+        if (NORD > 1) {
+          const T *rj_ = v.ren + 2 * C * j;
+          for (int c2 = 0; c2 < C; c2++) {
+            T ri, di;
+            cen_dist(s, sk, xn, c2, ri, di);
+            Een<T> o;
+            jas_een<T, NORD, 0>(J, s.ctype[c2], rij, du, ri, di, rj_[2 * c2], rj_[2 * c2 + 1], o);
+            f += o.fc;
+          }
+        }
         dj += (double)f - (double)fso[e * N + j];
       }
       {
-        T g3[3];
         T f = 0;
         for (int c2 = 0; c2 < C; c2++) {
-          const double *c2p = s.cent + 3 * c2;
-          T rv[3] = {T(xn[0] - c2p[0]), T(xn[1] - c2p[1]), T(xn[2] - c2p[2])};
-          T rr = tsqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
-          T fi, fii;
-          f += jas_en<T, false>(J, s.ctype[c2], rr, fi, fii);
+          T ri, di, fi, fii;
+          cen_dist(s, sk, xn, c2, ri, di);
+          f += jas_en<T, false>(J, s.ctype[c2], ri, di, fi, fii);
         }
-        (void)g3;
         dj += (double)f - (double)fso[e * N + e];
       }
       int it = s.ctype[c];
@@ -522,44 +583,58 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
 // single-electron proposal (hpsie, qmc/vmc/hpsie.f90) and acceptance (jassav/detsav)
 // ---------------------------------------------------------------------------------------
 template <class T, int NORD, bool GRAD>
-__device__ void propose(const Sys<T> &s, const JasPar<T> &J, const State<T> &st, int w, const WarpMem<T> &sm, int e,
+__device__ void propose(const Sys<T> &s, const JasPar<T> &J, const State<T> &st, int w, const View<T> &v, int e,
                         const double *xn, int lane, double &rho, double &dj, double *grad) {
-  const int N = s.N, nmax = s.nmax;
+  const int N = s.N, C = s.C, nmax = s.nmax;
   int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
-  const double *A = st.ainv + (size_t)w * st.astride + (sp ? s.nup * s.nup : 0);
+  const double *A = v.ainv + (sp ? s.nup * s.nup : 0);
   constexpr int NCH = GRAD ? 5 : 1;
-  warp_basis<T, NCH>(s, xn, sm.phi, lane);
-  warp_orbitals<T, NCH>(sm.phi, s.cref[sp], s.nbasis, n, sm.arow, nmax, lane);
+  for (int c = lane; c < C; c += 32) {
+    T r, d;
+    cen_dist(s, J.scalek, xn, c, r, d);
+    v.rnew[2 * c] = r;
+    v.rnew[2 * c + 1] = d;
+  }
+  warp_basis<T, NCH>(s, xn, v.phi, lane);
+  warp_orbitals<T, NCH>(v.phi, s.cref[sp], s.nbasis, n, v.arow, nmax, lane);
   double r0 = 0, g0 = 0, g1 = 0, g2 = 0;
   for (int k = lane; k < n; k += 32) {
     double a = A[k * n + eo];
-    r0 += a * (double)sm.arow[k];
+    r0 += a * (double)v.arow[k];
     if (GRAD) {
-      g0 += a * (double)sm.arow[nmax + k];
-      g1 += a * (double)sm.arow[2 * nmax + k];
-      g2 += a * (double)sm.arow[3 * nmax + k];
+      g0 += a * (double)v.arow[nmax + k];
+      g1 += a * (double)v.arow[2 * nmax + k];
+      g2 += a * (double)v.arow[3 * nmax + k];
     }
   }
   rho = warp_sum(r0);
-  const T *fso = st.fso + (size_t)w * N * N;
-  T *pf = st.pf + (size_t)w * N;
+  const T *fso = v.fso;
+  T *pf = v.pf;
   double d = 0, gj0 = 0, gj1 = 0, gj2 = 0;
   for (int j = lane; j < N; j += 32) {
     if (j == e) continue;
     T g[3];
-    T f = pair_value<T, NORD, GRAD>(s, J, e, j, xn, sm.xs + 3 * j, g);
+    T f = pair_value<T, NORD, GRAD>(s, J, e, j, xn, v.rnew, v.xs + 3 * j, v.ren + 2 * C * j, g);
     d += (double)f - (double)fso[e * N + j];
     pf[j] = f;
     if (GRAD) { gj0 += g[0]; gj1 += g[1]; gj2 += g[2]; }
   }
-  T ge[3];
-  T fen = en_partial<T, GRAD>(s, J, xn, ge, lane);
+  T fen = 0;
+  for (int c = lane; c < C; c += 32) {
+    T fi = 0, fii = 0;
+    fen += jas_en<T, GRAD>(J, s.ctype[c], v.rnew[2 * c], v.rnew[2 * c + 1], fi, fii);
+    if (GRAD) {
+      const double *cc = s.cent + 3 * c;
+      gj0 += fi * T(xn[0] - cc[0]);
+      gj1 += fi * T(xn[1] - cc[1]);
+      gj2 += fi * T(xn[2] - cc[2]);
+    }
+  }
   double fent = warp_sum((double)fen);
   if (lane == 0) {
     pf[e] = (T)fent;
     d += fent - (double)fso[e * N + e];
   }
-  if (GRAD) { gj0 += ge[0]; gj1 += ge[1]; gj2 += ge[2]; }
   dj = warp_sum(d);
   if (GRAD) {
     g0 = warp_sum(g0); g1 = warp_sum(g1); g2 = warp_sum(g2);
@@ -573,33 +648,33 @@ __device__ void propose(const Sys<T> &s, const JasPar<T> &J, const State<T> &st,
 
 // Sherman-Morrison update of the inverse and Jastrow tables after accepting electron e
 // at xn (dete_update/detsav, qmc/dete_mod.f90:165-190; jassav.f90).  The proposed orbital
-// row is sm.arow (channel 0), the proposed pair values st.pf.
+// row is v.arow (channel 0), the proposed pair values v.pf, distances v.rnew.
 template <class T>
-__device__ void accept_move(const Sys<T> &s, const State<T> &st, int w, const WarpMem<T> &sm, int e, const double *xn,
+__device__ void accept_move(const Sys<T> &s, const State<T> &st, int w, const View<T> &v, int e, const double *xn,
                             double dj, double rho, int lane) {
-  const int N = s.N;
+  const int N = s.N, C = s.C;
   int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
-  double *A = st.ainv + (size_t)w * st.astride + (sp ? s.nup * s.nup : 0);
-  for (int k = lane; k < n; k += 32) sm.colb[k] = A[k * n + eo];
+  double *A = v.ainv + (sp ? s.nup * s.nup : 0);
+  for (int k = lane; k < n; k += 32) v.colb[k] = A[k * n + eo];
   for (int j = lane; j < n; j += 32) {
-    double v = 0;
-    for (int k = 0; k < n; k++) v += (double)sm.arow[k] * A[k * n + j];
-    sm.vb[j] = v - (j == eo ? 1.0 : 0.0);
+    double a = 0;
+    for (int k = 0; k < n; k++) a += (double)v.arow[k] * A[k * n + j];
+    v.vb[j] = a - (j == eo ? 1.0 : 0.0);
   }
   __syncwarp();
-  double rinv = 1.0 / (sm.vb[eo] + 1.0);
+  double rinv = 1.0 / (v.vb[eo] + 1.0);
   for (int idx = lane; idx < n * n; idx += 32) {
     int k = idx / n, j = idx - k * n;
-    A[idx] -= sm.colb[k] * sm.vb[j] * rinv;
+    A[idx] -= v.colb[k] * v.vb[j] * rinv;
   }
-  T *fso = st.fso + (size_t)w * N * N;
-  const T *pf = st.pf + (size_t)w * N;
+  T *fso = v.fso;
   for (int j = lane; j < N; j += 32) {
-    T f = pf[j];
+    T f = v.pf[j];
     fso[e * N + j] = f;
     fso[j * N + e] = f;
   }
-  if (lane < 3) sm.xs[3 * e + lane] = xn[lane];
+  for (int i = lane; i < 2 * C; i += 32) v.ren[2 * C * e + i] = v.rnew[i];
+  if (lane < 3) v.xs[3 * e + lane] = xn[lane];
   if (lane == 0) {
     st.fsum[w] += dj;
     st.lnd[w] += log(fabs(rho));
@@ -623,45 +698,47 @@ __device__ inline void load_params(const Sys<T> &s, JasPar<T> &J, EcpPar &E) {
 }
 
 template <class T, int NORD>
-__global__ void k_eval(Sys<T> s, State<T> st, double r0, double r1, double r2, double r3, double r4, double r5,
-                       double r6, double r7, double r8, int outputs) {
+__global__ void __launch_bounds__(128, 4) k_eval(Sys<T> s, State<T> st, Layout L, double r0, double r1, double r2,
+                                                 double r3, double r4, double r5, double r6, double r7, double r8,
+                                                 int outputs) {
   __shared__ JasPar<T> J;
   __shared__ EcpPar E;
   extern __shared__ __align__(16) char dsm[];
   load_params(s, J, E);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  const size_t wb = warp_smem_bytes<T>(s.N, s.nbasis, s.nmax);
-  WarpMem<T> sm = carve<T>(dsm + wb * wib, s.N, s.nbasis, s.nmax);
   const double R[9] = {r0, r1, r2, r3, r4, r5, r6, r7, r8};
   for (int w = blockIdx.x * wpb + wib; w < st.W; w += gridDim.x * wpb) {
-    for (int i = lane; i < 3 * s.N; i += 32) sm.xs[i] = st.x[(size_t)w * 3 * s.N + i];
+    View<T> v = make_view<T>(dsm + L.bytes * wib, L, st, w, s.N, s.C, s.nbasis, s.nmax, L.resident != 0);
+    for (int i = lane; i < 3 * s.N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * s.N + i];
     __syncwarp();
     EvalRes res;
-    full_eval<T, NORD>(s, J, E, st, w, sm, R, lane, outputs != 0, res);
+    full_eval<T, NORD>(s, J, E, st, w, v, R, lane, outputs != 0, res);
+    if (L.resident) view_store(v, st, w, s.N, s.C, lane);
   }
 }
 
+// The per-call proposal/accept kernels always work on the HBM copy of the state.
 template <class T, int NORD>
-__global__ void k_propose(Sys<T> s, State<T> st, int e, const double *xnew, double *ratio, double *grad) {
+__global__ void __launch_bounds__(128, 4) k_propose(Sys<T> s, State<T> st, Layout L, int e, const double *xnew,
+                                                    double *ratio, double *grad) {
   __shared__ JasPar<T> J;
   __shared__ EcpPar E;
   extern __shared__ __align__(16) char dsm[];
   load_params(s, J, E);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  const size_t wb = warp_smem_bytes<T>(s.N, s.nbasis, s.nmax);
-  WarpMem<T> sm = carve<T>(dsm + wb * wib, s.N, s.nbasis, s.nmax);
   const int nmax = s.nmax;
   for (int w = blockIdx.x * wpb + wib; w < st.W; w += gridDim.x * wpb) {
-    for (int i = lane; i < 3 * s.N; i += 32) sm.xs[i] = st.x[(size_t)w * 3 * s.N + i];
+    View<T> v = make_view<T>(dsm + L.bytes * wib, L, st, w, s.N, s.C, s.nbasis, s.nmax, false);
+    for (int i = lane; i < 3 * s.N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * s.N + i];
     __syncwarp();
     double xn[3] = {xnew[3 * w], xnew[3 * w + 1], xnew[3 * w + 2]};
     double rho, dj, g[3];
     if (grad)
-      propose<T, NORD, true>(s, J, st, w, sm, e, xn, lane, rho, dj, g);
+      propose<T, NORD, true>(s, J, st, w, v, e, xn, lane, rho, dj, g);
     else
-      propose<T, NORD, false>(s, J, st, w, sm, e, xn, lane, rho, dj, g);
+      propose<T, NORD, false>(s, J, st, w, v, e, xn, lane, rho, dj, g);
     int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup;
-    for (int k = lane; k < n; k += 32) st.pa[(size_t)w * nmax + k] = (double)sm.arow[k];
+    for (int k = lane; k < n; k += 32) st.pa[(size_t)w * nmax + k] = (double)v.arow[k];
     if (lane == 0) {
       st.pdj[w] = dj;
       st.prho[w] = rho;
@@ -675,20 +752,28 @@ __global__ void k_propose(Sys<T> s, State<T> st, int e, const double *xnew, doub
 }
 
 template <class T>
-__global__ void k_accept(Sys<T> s, State<T> st, int e, const uint8_t *mask) {
+__global__ void __launch_bounds__(128, 4) k_accept(Sys<T> s, State<T> st, Layout L, int e, const uint8_t *mask) {
   extern __shared__ __align__(16) char dsm[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  const size_t wb = warp_smem_bytes<T>(s.N, s.nbasis, s.nmax);
-  WarpMem<T> sm = carve<T>(dsm + wb * wib, s.N, s.nbasis, s.nmax);
-  const int nmax = s.nmax;
+  const int nmax = s.nmax, C = s.C;
   for (int w = blockIdx.x * wpb + wib; w < st.W; w += gridDim.x * wpb) {
     if (!mask[w] || st.piel[w] != e) continue;
+    View<T> v = make_view<T>(dsm + L.bytes * wib, L, st, w, s.N, s.C, s.nbasis, s.nmax, false);
     int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup;
-    for (int k = lane; k < n; k += 32) sm.arow[k] = (T)st.pa[(size_t)w * nmax + k];
-    for (int i = lane; i < 3 * s.N; i += 32) sm.xs[i] = st.x[(size_t)w * 3 * s.N + i];
-    __syncwarp();
+    for (int k = lane; k < n; k += 32) v.arow[k] = (T)st.pa[(size_t)w * nmax + k];
+    for (int i = lane; i < 3 * s.N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * s.N + i];
     double xn[3] = {st.pxn[3 * w], st.pxn[3 * w + 1], st.pxn[3 * w + 2]};
-    accept_move<T>(s, st, w, sm, e, xn, st.pdj[w], st.prho[w], lane);
+    for (int c = lane; c < C; c += 32) {
+      T r, d;
+      const double *cc = s.cent + 3 * c;
+      T a = T(xn[0] - cc[0]), b = T(xn[1] - cc[1]), z = T(xn[2] - cc[2]);
+      r = tsqrt(a * a + b * b + z * z);
+      d = T(1) / (T(1) + (T)s.scalek * r);
+      v.rnew[2 * c] = r;
+      v.rnew[2 * c + 1] = d;
+    }
+    __syncwarp();
+    accept_move<T>(s, st, w, v, e, xn, st.pdj[w], st.prho[w], lane);
     if (lane < 3) st.x[(size_t)w * 3 * s.N + 3 * e + lane] = xn[lane];
     if (lane == 0) st.piel[w] = -1;
     __syncwarp();
@@ -697,42 +782,50 @@ __global__ void k_accept(Sys<T> s, State<T> st, int e, const uint8_t *mask) {
 
 // Fused VMC: nsweep sweeps of single-electron Metropolis moves plus E_L after each sweep.
 template <class T, int NORD>
-__global__ void k_vmc(Sys<T> s, State<T> st, int nsweep, uint64_t seed, uint64_t sweep0, double step) {
+__global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L, int nsweep, uint64_t seed,
+                                                uint64_t sweep0, double step) {
   __shared__ JasPar<T> J;
   __shared__ EcpPar E;
   extern __shared__ __align__(16) char dsm[];
   load_params(s, J, E);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  const size_t wb = warp_smem_bytes<T>(s.N, s.nbasis, s.nmax);
-  WarpMem<T> sm = carve<T>(dsm + wb * wib, s.N, s.nbasis, s.nmax);
   const int N = s.N;
   for (int w = blockIdx.x * wpb + wib; w < st.W; w += gridDim.x * wpb) {
-    for (int i = lane; i < 3 * N; i += 32) sm.xs[i] = st.x[(size_t)w * 3 * N + i];
-    __syncwarp();
+    View<T> v = make_view<T>(dsm + L.bytes * wib, L, st, w, s.N, s.C, s.nbasis, s.nmax, L.resident != 0);
+    if (L.resident) {
+      view_load(v, st, w, N, s.C, lane);
+    } else {
+      for (int i = lane; i < 3 * N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * N + i];
+      __syncwarp();
+    }
     double es = 0, e2 = 0, acc = 0, el = 0;
     for (int isw = 0; isw < nsweep; isw++) {
       uint64_t sweep = sweep0 + (uint64_t)isw;
       for (int e = 0; e < N; e++) {
         double g[3], ua;
         move_randoms(seed, (uint32_t)w, sweep, (uint32_t)e, g, &ua);
-        double xn[3] = {sm.xs[3 * e] + step * g[0], sm.xs[3 * e + 1] + step * g[1], sm.xs[3 * e + 2] + step * g[2]};
+        double xn[3] = {v.xs[3 * e] + step * g[0], v.xs[3 * e + 1] + step * g[1], v.xs[3 * e + 2] + step * g[2]};
         double rho, dj, gr[3];
-        propose<T, NORD, false>(s, J, st, w, sm, e, xn, lane, rho, dj, gr);
+        propose<T, NORD, false>(s, J, st, w, v, e, xn, lane, rho, dj, gr);
         double p = rho * rho * exp(2.0 * dj);
         if (ua < p) {
-          accept_move<T>(s, st, w, sm, e, xn, dj, rho, lane);
+          accept_move<T>(s, st, w, v, e, xn, dj, rho, lane);
           acc += 1;
         }
       }
       double R[9];
       random_rotation(seed, (uint32_t)w, sweep, R);
       EvalRes res;
-      full_eval<T, NORD>(s, J, E, st, w, sm, R, lane, false, res);
+      full_eval<T, NORD>(s, J, E, st, w, v, R, lane, false, res);
       el = res.eloc;
       es += el;
       e2 += el * el;
     }
-    for (int i = lane; i < 3 * N; i += 32) st.x[(size_t)w * 3 * N + i] = sm.xs[i];
+    if (L.resident) {
+      view_store(v, st, w, N, s.C, lane);
+    } else {
+      for (int i = lane; i < 3 * N; i += 32) st.x[(size_t)w * 3 * N + i] = v.xs[i];
+    }
     if (lane == 0) {
       st.s_esum[w] = es;
       st.s_e2sum[w] = e2;
@@ -757,6 +850,10 @@ static int fail(int code, const std::string &msg) {
     if (e_ != cudaSuccess) return fail(CHAMP_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
+// Largest per-warp shared-memory footprint for which a walker's state stays resident in
+// shared memory inside the fused kernels (keeps >= 16 warps per SM).
+constexpr size_t RESIDENT_LIMIT = 12 * 1024;
+
 struct champ_ctx {
   int prec = 0;
   cudaStream_t stream = nullptr;
@@ -771,6 +868,7 @@ struct champ_ctx {
   bool have_walkers = false;
   int wpb = 4;
   size_t smem = 0;
+  Layout lay;
   // device staging for per-call host arrays
   double *d_in = nullptr, *d_out = nullptr;
   uint8_t *d_mask = nullptr;
@@ -843,6 +941,7 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
                      const double *asymp_a, const double *asymp_b, const EcpPar &ecp, double pecent, Sys<T> &s) {
   s.N = c->N; s.nup = c->nup; s.ndn = c->ndn; s.C = c->C; s.nct = c->nct; s.nshell = c->nshell;
   s.nbasis = c->nbasis; s.nmax = c->nmax; s.nloc = c->nloc; s.nordc = c->nordc; s.pecent = pecent;
+  s.scalek = d->scalek;
   double *cent = dalloc<double>(c, 3 * c->C);
   int *ctype = dalloc<int>(c, c->C);
   double *zc = dalloc<double>(c, c->C);
@@ -851,25 +950,38 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
   int *shb0 = dalloc<int>(c, c->nshell);
   int nprim = (int)pcn.size();
   T *pz = dalloc<T>(c, nprim), *pc = dalloc<T>(c, nprim);
-  int *bm = dalloc<int>(c, c->nbasis);
   T *cr0 = dalloc<T>(c, (size_t)c->nbasis * std::max(1, c->nup));
   T *cr1 = dalloc<T>(c, (size_t)c->nbasis * std::max(1, c->ndn));
   JasPar<T> *jp = dalloc<JasPar<T>>(c, 1);
   EcpPar *ep = dalloc<EcpPar>(c, 1);
-  if (!cent || !ctype || !zc || !sh || !shp || !shb0 || !pz || !pc || !bm || !cr0 || !cr1 || !jp || !ep)
+  if (!cent || !ctype || !zc || !sh || !shp || !shb0 || !pz || !pc || !cr0 || !cr1 || !jp || !ep)
     return fail(CHAMP_ENOMEM, "device allocation of the system data failed");
   std::vector<double> zcv(c->C);
   for (int i = 0; i < c->C; i++) zcv[i] = d->znuc[d->iwctype[i]];
   std::vector<int4> shv(c->nshell);
   std::vector<int2> shpv(c->nshell);
-  std::vector<int> shb0v(c->nshell, -1);
+  // internal basis order: shells in input order, each shell's 2l+1 functions in
+  // harmonic-slot order (slot(m) = 0, 2m-1 for m > 0, -2m for m < 0)
+  std::vector<int> shb0v(c->nshell, 0), perm_b(c->nbasis, -1);
+  {
+    int b0 = 0;
+    for (int i = 0; i < c->nshell; i++) { shb0v[i] = b0; b0 += 2 * d->shell_l[i] + 1; }
+    if (b0 != c->nbasis) return fail(CHAMP_EINVAL, "nbasis differs from the sum over shells of 2l+1");
+    for (int b = 0; b < c->nbasis; b++) {
+      int m = d->basis_m[b], ish = d->basis_shell[b];
+      if (ish < 0 || ish >= c->nshell || m < -d->shell_l[ish] || m > d->shell_l[ish])
+        return fail(CHAMP_EINVAL, "basis function with bad shell or m");
+      int ib = shb0v[ish] + (m > 0 ? 2 * m - 1 : -2 * m);
+      if (perm_b[ib] >= 0) return fail(CHAMP_EINVAL, "two basis functions with the same shell and m");
+      perm_b[ib] = b;  // internal index ib holds input basis function b
+    }
+  }
   int p0 = 0;
   for (int i = 0; i < c->nshell; i++) {
     shv[i] = make_int4(d->shell_cent[i], d->shell_n[i], d->shell_l[i], d->shell_kind[i]);
     shpv[i] = make_int2(p0, d->shell_nprim[i]);
     p0 += d->shell_nprim[i];
   }
-  for (int b = c->nbasis - 1; b >= 0; b--) shb0v[d->basis_shell[b]] = b;
   std::vector<T> pzv(nprim), pcv(nprim);
   for (int i = 0; i < nprim; i++) { pzv[i] = (T)d->prim_zeta[i]; pcv[i] = (T)pcn[i]; }
   std::vector<T> crv[2];
@@ -878,7 +990,7 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
     crv[sp].assign((size_t)c->nbasis * std::max(1, n), T(0));
     for (int k = 0; k < n; k++) {
       int o = d->det_orb[off + k];
-      for (int b = 0; b < c->nbasis; b++) crv[sp][(size_t)b * n + k] = (T)d->coef[(size_t)o * c->nbasis + b];
+      for (int b = 0; b < c->nbasis; b++) crv[sp][(size_t)b * n + k] = (T)d->coef[(size_t)o * c->nbasis + perm_b[b]];
     }
   }
   JasPar<T> J;
@@ -894,7 +1006,6 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
     for (int k = 0; k <= d->nordb; k++) J.b[is][k] = (T)d->b[is * (d->nordb + 1) + k];
   J.asymp_b[0] = (T)asymp_b[0]; J.asymp_b[1] = (T)asymp_b[1];
   std::vector<int> ctv(d->iwctype, d->iwctype + c->C);
-  std::vector<int> bmv(d->basis_m, d->basis_m + c->nbasis);
   CK(cudaMemcpy(cent, d->cent, sizeof(double) * 3 * c->C, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(ctype, ctv.data(), sizeof(int) * c->C, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(zc, zcv.data(), sizeof(double) * c->C, cudaMemcpyHostToDevice));
@@ -903,13 +1014,12 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
   CK(cudaMemcpy(shb0, shb0v.data(), sizeof(int) * c->nshell, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(pz, pzv.data(), sizeof(T) * nprim, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(pc, pcv.data(), sizeof(T) * nprim, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(bm, bmv.data(), sizeof(int) * c->nbasis, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(cr0, crv[0].data(), sizeof(T) * crv[0].size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(cr1, crv[1].data(), sizeof(T) * crv[1].size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(jp, &J, sizeof J, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(ep, &ecp, sizeof ecp, cudaMemcpyHostToDevice));
   s.cent = cent; s.ctype = ctype; s.zc = zc; s.shell = sh; s.shprim = shp; s.shb0 = shb0;
-  s.pz = pz; s.pc = pc; s.bm = bm; s.cref[0] = cr0; s.cref[1] = cr1; s.jas = jp; s.ecp = ep;
+  s.pz = pz; s.pc = pc; s.cref[0] = cr0; s.cref[1] = cr1; s.jas = jp; s.ecp = ep;
   return CHAMP_OK;
 }
 
@@ -921,6 +1031,7 @@ static int build_state(champ_ctx *c, State<T> &st) {
   st.x = dalloc<double>(c, W * N * 3);
   st.ainv = dalloc<double>(c, W * st.astride);
   st.fso = dalloc<T>(c, W * N * N);
+  st.ren = dalloc<T>(c, W * N * c->C * 2);
   st.fsum = dalloc<double>(c, W); st.lnd = dalloc<double>(c, W); st.sgn = dalloc<double>(c, W);
   st.status = dalloc<uint32_t>(c, W);
   st.pf = dalloc<T>(c, W * N);
@@ -936,7 +1047,7 @@ static int build_state(champ_ctx *c, State<T> &st) {
   st.o_eloc = dalloc<double>(c, W);
   st.s_esum = dalloc<double>(c, W); st.s_e2sum = dalloc<double>(c, W); st.s_acc = dalloc<double>(c, W);
   st.s_elast = dalloc<double>(c, W);
-  if (!st.x || !st.ainv || !st.fso || !st.orb5 || !st.s_elast || (c->nloc > 0 && (!st.gproj || !st.nlt)))
+  if (!st.x || !st.ainv || !st.fso || !st.ren || !st.orb5 || !st.s_elast || (c->nloc > 0 && (!st.gproj || !st.nlt)))
     return fail(CHAMP_ENOMEM, "device allocation of the walker state failed");
   return CHAMP_OK;
 }
@@ -949,6 +1060,11 @@ static int set_smem_attrs(champ_ctx *c) {
   CK(cudaFuncSetAttribute(k_propose<T, NORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   CK(cudaFuncSetAttribute(k_accept<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   CK(cudaFuncSetAttribute(k_vmc<T, NORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  const int co = cudaSharedmemCarveoutMaxShared;
+  CK(cudaFuncSetAttribute(k_eval<T, NORD>, cudaFuncAttributePreferredSharedMemoryCarveout, co));
+  CK(cudaFuncSetAttribute(k_propose<T, NORD>, cudaFuncAttributePreferredSharedMemoryCarveout, co));
+  CK(cudaFuncSetAttribute(k_accept<T>, cudaFuncAttributePreferredSharedMemoryCarveout, co));
+  CK(cudaFuncSetAttribute(k_vmc<T, NORD>, cudaFuncAttributePreferredSharedMemoryCarveout, co));
   return CHAMP_OK;
 }
 
@@ -988,18 +1104,18 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
   switch (op) {
   case Op::Eval:
   case Op::EvalOut:
-    k_eval<T, NORD><<<grid, block, c->smem, c->stream>>>(s, st, R[0], R[1], R[2], R[3], R[4], R[5], R[6], R[7], R[8],
+    k_eval<T, NORD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, R[0], R[1], R[2], R[3], R[4], R[5], R[6], R[7], R[8],
                                                        op == Op::EvalOut ? 1 : 0);
     break;
   case Op::Propose:
   case Op::ProposeGrad:
-    k_propose<T, NORD><<<grid, block, c->smem, c->stream>>>(s, st, a.e, a.xnew, a.ratio, op == Op::ProposeGrad ? a.grad : nullptr);
+    k_propose<T, NORD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, a.e, a.xnew, a.ratio, op == Op::ProposeGrad ? a.grad : nullptr);
     break;
   case Op::Accept:
-    k_accept<T><<<grid, block, c->smem, c->stream>>>(s, st, a.e, a.mask);
+    k_accept<T><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, a.e, a.mask);
     break;
   case Op::Vmc:
-    k_vmc<T, NORD><<<grid, block, c->smem, c->stream>>>(s, st, a.nsweep, a.seed, a.sweep0, a.step);
+    k_vmc<T, NORD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, a.nsweep, a.seed, a.sweep0, a.step);
     break;
   }
   CK(cudaGetLastError());
@@ -1165,15 +1281,17 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
   if (precision == CHAMP_PREC_FP64) {
     rc = build_sys<double>(c, d, pcn, cfull, asa, asb, ecp, pecent, c->sd);
     if (!rc) rc = build_state<double>(c, c->std_);
-    c->smem = warp_smem_bytes<double>(c->N, c->nbasis, c->nmax);
+    c->lay = make_layout<double>(c->N, c->C, c->nbasis, c->nmax, c->std_.astride, c->nloc > 0, RESIDENT_LIMIT);
+    c->smem = c->lay.bytes;
   } else {
     rc = build_sys<float>(c, d, pcn, cfull, asa, asb, ecp, pecent, c->sf);
     if (!rc) rc = build_state<float>(c, c->stf);
-    c->smem = warp_smem_bytes<float>(c->N, c->nbasis, c->nmax);
+    c->lay = make_layout<float>(c->N, c->C, c->nbasis, c->nmax, c->stf.astride, c->nloc > 0, RESIDENT_LIMIT);
+    c->smem = c->lay.bytes;
   }
   if (rc) { champ_destroy(c); return rc; }
   // warps per block: up to 8, keeping the block's dynamic shared memory under 96 KB
-  c->wpb = 8;
+  c->wpb = 4;  // 128-thread blocks (the kernels' launch bounds)
   while (c->wpb > 1 && c->smem * c->wpb > 96 * 1024) c->wpb >>= 1;
   if (c->smem * c->wpb > 200 * 1024) { champ_destroy(c); return fail(CHAMP_EINVAL, "system too large for the per-warp shared memory"); }
   c->smem *= c->wpb;
