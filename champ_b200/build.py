@@ -1,17 +1,25 @@
-"""Builds the engine's shared library in-tree with nvcc for sm_100a."""
+"""Builds the engine's shared library in-tree with nvcc for sm_100a.
+
+The kernels are instantiated in two translation units (FP32 and FP64 compute types)
+compiled in parallel with the C-ABI unit, then linked into libchamp_b200.so.
+"""
 from __future__ import annotations
 
+import glob
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = [os.path.join(HERE, "csrc", "engine.cu")]
-DEPS = SRC + [os.path.join(HERE, "csrc", "device_math.cuh"), os.path.join(HERE, "..", "include", "champ_b200.h")]
+CSRC = os.path.join(HERE, "csrc")
+UNITS = ["host.cu", "inst_f32.cu", "inst_f64.cu"]
+DEPS = [os.path.join(HERE, "..", "include", "champ_b200.h")] + glob.glob(os.path.join(CSRC, "*"))
 LIB = os.path.join(HERE, "libchamp_b200.so")
+OBJDIR = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-         "-Xcompiler", "-fPIC", "-shared"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
 
 
 def needs_build() -> bool:
@@ -22,9 +30,19 @@ def needs_build() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    if force or needs_build():
-        cmd = [NVCC] + FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-o", LIB] + SRC
+    if not (force or needs_build()):
+        return LIB
+    os.makedirs(OBJDIR, exist_ok=True)
+
+    def compile_unit(u):
+        obj = os.path.join(OBJDIR, u.replace(".cu", ".o"))
+        cmd = [NVCC] + FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", os.path.join(CSRC, u), "-o", obj]
         subprocess.check_call(cmd)
+        return obj
+
+    with ThreadPoolExecutor(len(UNITS)) as ex:
+        objs = list(ex.map(compile_unit, UNITS))
+    subprocess.check_call([NVCC] + ARCH + ["-shared", "-o", LIB] + objs)
     return LIB
 
 

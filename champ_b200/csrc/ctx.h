@@ -1,0 +1,86 @@
+// ctx.h -- host-side context of the engine, shared by the C-ABI translation unit and
+// the per-precision kernel instantiation units.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+int champ_fail(int code, const std::string &msg);
+#define CK(call)                                                                                          \
+  do {                                                                                                    \
+    cudaError_t e_ = (call);                                                                              \
+    if (e_ != cudaSuccess) return champ_fail(CHAMP_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// Occupied orbitals and determinant tables of the wave function (occ_bld, excit_bld,
+// cdet_in_wf_bld: deriv_fast_mod.f90:144-300), built once on the host.
+struct MultiDet {
+  int multidet = 0, ndet = 0;
+  int nocc[2] = {0, 0}, nvirt[2] = {0, 0}, ndu[2] = {0, 0};
+  std::vector<int> occ[2];              // orbital index of each occupied column
+  std::vector<int> dk[2], dh[2], dp[2];  // per unique determinant: order, holes[4], particles[4]
+  std::vector<double> dsg[2];
+  std::vector<int> ciu, cid;
+  std::vector<double> ccoef;
+};
+
+// Largest per-warp shared-memory footprint for which a walker's state stays resident in
+// shared memory inside the fused kernels (keeps >= 16 warps per SM).
+constexpr size_t RESIDENT_LIMIT = 12 * 1024;
+
+struct champ_ctx {
+  int prec = 0;
+  cudaStream_t stream = nullptr;
+  int wmax = 0, W = 0;
+  int N = 0, nup = 0, ndn = 0, C = 0, nct = 0, nshell = 0, nbasis = 0, nmax = 0, nordc = 0, nloc = 0;
+  int nomax = 1;
+  MultiDet md;
+  std::vector<void *> allocs;
+  Sys<double> sd;
+  Sys<float> sf;
+  State<double> std_;
+  State<float> stf;
+  double rot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  bool have_walkers = false;
+  int wpb = 4;
+  size_t smem = 0;
+  Layout lay;
+  // device staging for per-call host arrays
+  double *d_in = nullptr, *d_out = nullptr;
+  uint8_t *d_mask = nullptr;
+  int nparm_jas = 0;
+};
+
+template <class T>
+inline Sys<T> &sysof(champ_ctx *c);
+template <>
+inline Sys<double> &sysof<double>(champ_ctx *c) { return c->sd; }
+template <>
+inline Sys<float> &sysof<float>(champ_ctx *c) { return c->sf; }
+template <class T>
+inline State<T> &stof(champ_ctx *c);
+template <>
+inline State<double> &stof<double>(champ_ctx *c) { return c->std_; }
+template <>
+inline State<float> &stof<float>(champ_ctx *c) { return c->stf; }
+
+inline int nblocks(champ_ctx *c) { return (c->W + c->wpb - 1) / c->wpb; }
+
+enum class Op { Eval, EvalOut, Propose, ProposeGrad, Accept, Vmc };
+struct OpArgs {
+  int e = 0;
+  const double *xnew = nullptr;
+  double *ratio = nullptr, *grad = nullptr;
+  const uint8_t *mask = nullptr;
+  int nsweep = 0;
+  uint64_t seed = 0, sweep0 = 0;
+  double step = 0;
+};
+
+
+// per-precision kernel launchers (inst_f32.cu, inst_f64.cu)
+int launch_f32(champ_ctx *c, Op op, const OpArgs &a);
+int launch_f64(champ_ctx *c, Op op, const OpArgs &a);
+int attrs_f32(champ_ctx *c);
+int attrs_f64(champ_ctx *c);

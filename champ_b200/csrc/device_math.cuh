@@ -53,9 +53,20 @@ struct Sys {
   const int2 *shprim;   // [nshell]: first primitive, count
   const int *shb0;      // [nshell] first basis function
   const T *pz, *pc;     // primitive exponent, normalised weight
-  const T *cref[2];     // [nbasis][n_s] reference-determinant orbital coefficients; rows in the
-                        // internal basis order (each shell's functions in harmonic-slot order
-                        // m = 0, 1, -1, 2, -2, ...)
+  // occupied orbitals of each spin: det-0 (reference) orbitals in column order, then the
+  // other orbitals any determinant of that spin uses ("virtuals"), ascending
+  int nocc[2], nvirt[2], nomax, nvmax;
+  const T *cocc[2];     // [nbasis][nocc_s] orbital coefficients; rows in the internal basis
+                        // order (each shell's functions in harmonic-slot order m = 0, 1, -1, ...)
+  // multi-determinant tables (deriv_fast_mod.f90:261 excit_bld): unique determinants per
+  // spin as excitations of the reference, and the (up, down, coefficient) combinations
+  int multidet, ndet, ndu[2];
+  const int *dk[2];       // [ndu_s] excitation order
+  const int *dh[2];       // [ndu_s][4] hole: reference column
+  const int *dpart[2];    // [ndu_s][4] particle: virtual index
+  const double *dsg[2];   // [ndu_s] sign of det(T[:, L]) / det(alpha)
+  const int *ciu, *cid;   // [ndet] unique up / down determinant of each determinant
+  const double *ccoef;    // [ndet] determinant coefficient (csf coefficients folded in)
   const JasPar<T> *jas;
   const EcpPar *ecp;
 };

@@ -1,0 +1,689 @@
+// host.cu -- the engine's C ABI: system set-up, walker state, dispatch.
+//
+// One warp owns one walker.  Walker state lives in HBM, walker-major:
+//   x[w][e][3] (double), ainv[w][spin block][k][e] (double, reference-determinant inverse),
+//   fso[w][i][j] (T, Jastrow pair table: i != j pair term incl. e-e-n, i == j e-n term),
+//   ln|D|, sign, J per walker.
+// Per-warp scratch (basis values, proposed orbital row, gradient accumulators) lives in
+// shared memory; larger per-walker scratch (orbitals of all electrons, projected
+// coefficients, pseudopotential task lists) in HBM.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/champ_b200.h"
+#include "ctx.h"
+
+using namespace champ;
+
+// ---------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------
+static thread_local std::string g_err;
+int champ_fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+static int fail(int code, const std::string &msg) { return champ_fail(code, msg); }
+
+
+static double host_det(std::vector<double> a, int n) {
+  double d = 1;
+  for (int c = 0; c < n; c++) {
+    int p = c;
+    for (int i = c + 1; i < n; i++)
+      if (std::fabs(a[i * n + c]) > std::fabs(a[p * n + c])) p = i;
+    if (a[p * n + c] == 0) return 0;
+    if (p != c) {
+      d = -d;
+      for (int j = 0; j < n; j++) std::swap(a[c * n + j], a[p * n + j]);
+    }
+    d *= a[c * n + c];
+    for (int i = c + 1; i < n; i++) {
+      double f = a[i * n + c] / a[c * n + c];
+      for (int j = c; j < n; j++) a[i * n + j] -= f * a[c * n + j];
+    }
+  }
+  return d;
+}
+
+static int build_multidet(const champ_system *d, MultiDet &md) {
+  const int N = d->nelec, nup = d->nup;
+  md.ndet = d->ndet;
+  md.ciu.assign(d->ndet, 0);
+  md.cid.assign(d->ndet, 0);
+  md.ccoef.assign(d->ndet, 0.0);
+  for (int icsf = 0, off = 0; icsf < d->ncsf; icsf++)
+    for (int i = 0; i < d->csf_ndet[icsf]; i++, off++) {
+      int I = d->csf_det[off];
+      if (I < 0 || I >= d->ndet) return fail(CHAMP_EINVAL, "csf_det index out of range");
+      md.ccoef[I] += d->csf_det_coef[off] * d->csf_coef[icsf];
+    }
+  uint64_t lcg = 88172645463325252ull;
+  auto rnd = [&]() { lcg = lcg * 6364136223846793005ull + 1442695040888963407ull; return 0.5 + (double)(lcg >> 11) / 9007199254740992.0; };
+  for (int sp = 0; sp < 2; sp++) {
+    const int n = sp ? N - nup : nup, o0 = sp ? nup : 0;
+    std::vector<int> R(d->det_orb + o0, d->det_orb + o0 + n);
+    std::vector<int> used;
+    for (int I = 0; I < d->ndet; I++)
+      for (int j = 0; j < n; j++) {
+        int o = d->det_orb[I * N + o0 + j];
+        if (o < 0 || o >= d->norb) return fail(CHAMP_EINVAL, "det_orb orbital index out of range");
+        if (std::find(R.begin(), R.end(), o) == R.end() && std::find(used.begin(), used.end(), o) == used.end())
+          used.push_back(o);
+      }
+    std::sort(used.begin(), used.end());
+    md.occ[sp] = R;
+    md.occ[sp].insert(md.occ[sp].end(), used.begin(), used.end());
+    md.nocc[sp] = (int)md.occ[sp].size();
+    md.nvirt[sp] = (int)used.size();
+    const int no = md.nocc[sp];
+    auto col = [&](int o) { return (int)(std::find(md.occ[sp].begin(), md.occ[sp].end(), o) - md.occ[sp].begin()); };
+    // a random T with T[:, reference] = 1 fixes each determinant's sign relative to det(alpha)
+    std::vector<double> Tr((size_t)n * std::max(no, 1));
+    for (int k = 0; k < n; k++)
+      for (int m = 0; m < no; m++) Tr[(size_t)k * no + m] = (m < n) ? (m == k ? 1.0 : 0.0) : rnd();
+    std::vector<std::vector<int>> uniq;
+    for (int I = 0; I < d->ndet; I++) {
+      std::vector<int> L(d->det_orb + I * N + o0, d->det_orb + I * N + o0 + n);
+      int u = -1;
+      for (size_t q = 0; q < uniq.size(); q++)
+        if (uniq[q] == L) { u = (int)q; break; }
+      if (u < 0) {
+        u = (int)uniq.size();
+        uniq.push_back(L);
+        std::vector<int> holes, parts;
+        for (int k = 0; k < n; k++)
+          if (std::find(L.begin(), L.end(), R[k]) == L.end()) holes.push_back(k);
+        for (int j = 0; j < n; j++)
+          if (col(L[j]) >= n) parts.push_back(col(L[j]) - n);
+        for (int j = 0; j < n; j++)
+          for (int j2 = j + 1; j2 < n; j2++)
+            if (L[j] == L[j2]) return fail(CHAMP_EINVAL, "determinant with a repeated orbital");
+        if (holes.size() != parts.size() || holes.size() > 4)
+          return fail(CHAMP_EINVAL, "determinant more than 4 excitations away from the reference");
+        int k = (int)holes.size();
+        std::vector<double> M((size_t)n * n), a((size_t)k * k);
+        for (int r = 0; r < n; r++)
+          for (int j = 0; j < n; j++) M[(size_t)r * n + j] = Tr[(size_t)r * no + col(L[j])];
+        for (int ia = 0; ia < k; ia++)
+          for (int ib = 0; ib < k; ib++) a[(size_t)ia * k + ib] = Tr[(size_t)holes[ia] * no + n + parts[ib]];
+        double dm = host_det(M, n), da = k ? host_det(a, k) : 1.0;
+        double sg = dm / da;
+        if (!(std::fabs(std::fabs(sg) - 1.0) < 1e-6)) return fail(CHAMP_EINVAL, "could not fix a determinant's sign");
+        md.dk[sp].push_back(k);
+        for (int i = 0; i < 4; i++) {
+          md.dh[sp].push_back(i < k ? holes[i] : 0);
+          md.dp[sp].push_back(i < k ? parts[i] : 0);
+        }
+        md.dsg[sp].push_back(sg > 0 ? 1.0 : -1.0);
+      }
+      (sp ? md.cid : md.ciu)[I] = u;
+    }
+    md.ndu[sp] = (int)uniq.size();
+  }
+  md.multidet = (d->ndet > 1 || md.nvirt[0] > 0 || md.nvirt[1] > 0) ? 1 : 0;
+  if (!md.multidet && md.ccoef[0] == 0.0) return fail(CHAMP_EINVAL, "zero determinant coefficient");
+  return CHAMP_OK;
+}
+
+
+template <class T>
+static T *dalloc(champ_ctx *c, size_t n) {
+  void *p = nullptr;
+  if (cudaMalloc(&p, sizeof(T) * (n ? n : 1)) != cudaSuccess) return nullptr;
+  cudaMemset(p, 0, sizeof(T) * (n ? n : 1));
+  c->allocs.push_back(p);
+  return (T *)p;
+}
+
+static double host_fact(int n) {
+  double f = 1;
+  for (int i = 2; i <= n; i++) f *= i;
+  return f;
+}
+// basis_norm.f90:53-60 (with sqrt((2l+1)/4pi))
+static double host_anorm(int kind, int n, int l, double z) {
+  const double pi = 3.141592653589793;
+  if (kind == 0) return std::sqrt(std::pow(2 * z, 2 * n + 1) * (2 * l + 1) / (host_fact(2 * n) * 4 * pi));
+  double g = std::sqrt(pi);
+  for (int i = 1; i <= n; i++) g *= (i - 0.5);
+  return std::sqrt(2 * std::pow(2 * z, n + 0.5) * (2 * l + 1) / (g * 4 * pi));
+}
+
+// cuspinit4 + cuspexact4 (qmc/fit/cuspinit4.f90:1-60, qmc/fit/cuspexact4.f90:14-40)
+static void host_een_cusp(int nordc, int nct, int nt, std::vector<double> &c) {
+  if (nordc <= 1) return;
+  int neq = 2 * (nordc - 1);
+  std::vector<double> d((size_t)neq * nt, 0.0);
+  std::vector<int> iwc(neq, 0);
+  int i = 0;
+  for (int n = 2; n <= nordc; n++)
+    for (int k = n - 1; k >= 0; k--) {
+      int l_hi = (k == 0) ? n - k - 2 : n - k;
+      for (int l = l_hi; l >= 0; l--) {
+        int m = (n - k - l) / 2;
+        if (2 * m != n - k - l) continue;
+        i++;
+        if (k == 1 && iwc[n - 2] == 0) iwc[n - 2] = i;
+        if (k == 0 && iwc[n + nordc - 3] == 0) iwc[n + nordc - 3] = i;
+        int iord = l + 2 * m;
+        d[(size_t)(iord - 1) * nt + i - 1] -= 2 * k;
+        if (l + m > 0) { iord = nordc - 1 + k + m; d[(size_t)(iord - 1) * nt + i - 1] -= (l + m); }
+        if (m > 0) { iord = nordc - 1 + k + l + m; d[(size_t)(iord - 1) * nt + i - 1] -= m; }
+      }
+    }
+  std::vector<int> order;
+  for (int e = 1; e <= nordc - 1; e++) order.push_back(e);
+  for (int e = nordc + 1; e <= neq; e++) order.push_back(e);
+  order.push_back(nordc);
+  for (int it = 0; it < nct; it++) {
+    double *cc = c.data() + (size_t)it * nt;
+    for (int e : order) {
+      int jd = iwc[e - 1];
+      double sum = 0;
+      for (int j = 1; j <= nt; j++)
+        if (j != jd) sum += d[(size_t)(e - 1) * nt + j - 1] * cc[j - 1];
+      cc[jd - 1] = -sum / d[(size_t)(e - 1) * nt + jd - 1];
+    }
+  }
+}
+
+template <class T>
+static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<double> &pcn, const std::vector<double> &cfull,
+                     const double *asymp_a, const double *asymp_b, const EcpPar &ecp, double pecent, Sys<T> &s) {
+  s.N = c->N; s.nup = c->nup; s.ndn = c->ndn; s.C = c->C; s.nct = c->nct; s.nshell = c->nshell;
+  s.nbasis = c->nbasis; s.nmax = c->nmax; s.nloc = c->nloc; s.nordc = c->nordc; s.pecent = pecent;
+  s.scalek = d->scalek;
+  double *cent = dalloc<double>(c, 3 * c->C);
+  int *ctype = dalloc<int>(c, c->C);
+  double *zc = dalloc<double>(c, c->C);
+  int4 *sh = dalloc<int4>(c, c->nshell);
+  int2 *shp = dalloc<int2>(c, c->nshell);
+  int *shb0 = dalloc<int>(c, c->nshell);
+  int nprim = (int)pcn.size();
+  T *pz = dalloc<T>(c, nprim), *pc = dalloc<T>(c, nprim);
+  const MultiDet &md = c->md;
+  T *cr0 = dalloc<T>(c, (size_t)c->nbasis * std::max(1, md.nocc[0]));
+  T *cr1 = dalloc<T>(c, (size_t)c->nbasis * std::max(1, md.nocc[1]));
+  JasPar<T> *jp = dalloc<JasPar<T>>(c, 1);
+  EcpPar *ep = dalloc<EcpPar>(c, 1);
+  if (!cent || !ctype || !zc || !sh || !shp || !shb0 || !pz || !pc || !cr0 || !cr1 || !jp || !ep)
+    return fail(CHAMP_ENOMEM, "device allocation of the system data failed");
+  std::vector<double> zcv(c->C);
+  for (int i = 0; i < c->C; i++) zcv[i] = d->znuc[d->iwctype[i]];
+  std::vector<int4> shv(c->nshell);
+  std::vector<int2> shpv(c->nshell);
+  // internal basis order: shells in input order, each shell's 2l+1 functions in
+  // harmonic-slot order (slot(m) = 0, 2m-1 for m > 0, -2m for m < 0)
+  std::vector<int> shb0v(c->nshell, 0), perm_b(c->nbasis, -1);
+  {
+    int b0 = 0;
+    for (int i = 0; i < c->nshell; i++) { shb0v[i] = b0; b0 += 2 * d->shell_l[i] + 1; }
+    if (b0 != c->nbasis) return fail(CHAMP_EINVAL, "nbasis differs from the sum over shells of 2l+1");
+    for (int b = 0; b < c->nbasis; b++) {
+      int m = d->basis_m[b], ish = d->basis_shell[b];
+      if (ish < 0 || ish >= c->nshell || m < -d->shell_l[ish] || m > d->shell_l[ish])
+        return fail(CHAMP_EINVAL, "basis function with bad shell or m");
+      int ib = shb0v[ish] + (m > 0 ? 2 * m - 1 : -2 * m);
+      if (perm_b[ib] >= 0) return fail(CHAMP_EINVAL, "two basis functions with the same shell and m");
+      perm_b[ib] = b;  // internal index ib holds input basis function b
+    }
+  }
+  int p0 = 0;
+  for (int i = 0; i < c->nshell; i++) {
+    shv[i] = make_int4(d->shell_cent[i], d->shell_n[i], d->shell_l[i], d->shell_kind[i]);
+    shpv[i] = make_int2(p0, d->shell_nprim[i]);
+    p0 += d->shell_nprim[i];
+  }
+  std::vector<T> pzv(nprim), pcv(nprim);
+  for (int i = 0; i < nprim; i++) { pzv[i] = (T)d->prim_zeta[i]; pcv[i] = (T)pcn[i]; }
+  std::vector<T> crv[2];
+  for (int sp = 0; sp < 2; sp++) {
+    int no = md.nocc[sp];
+    crv[sp].assign((size_t)c->nbasis * std::max(1, no), T(0));
+    for (int k = 0; k < no; k++) {
+      int o = md.occ[sp][k];
+      for (int b = 0; b < c->nbasis; b++) crv[sp][(size_t)b * no + k] = (T)d->coef[(size_t)o * c->nbasis + perm_b[b]];
+    }
+  }
+  // determinant tables
+  s.multidet = md.multidet;
+  s.ndet = md.ndet;
+  s.nomax = c->nomax;
+  s.nvmax = std::max(md.nvirt[0], md.nvirt[1]);
+  for (int sp = 0; sp < 2; sp++) {
+    s.nocc[sp] = md.nocc[sp];
+    s.nvirt[sp] = md.nvirt[sp];
+    s.ndu[sp] = md.ndu[sp];
+    int nd = std::max(1, md.ndu[sp]);
+    int *dk = dalloc<int>(c, nd), *dh = dalloc<int>(c, 4 * nd), *dpp = dalloc<int>(c, 4 * nd);
+    double *dsg = dalloc<double>(c, nd);
+    if (!dk || !dh || !dpp || !dsg) return fail(CHAMP_ENOMEM, "device allocation of determinant tables failed");
+    if (md.ndu[sp]) {
+      CK(cudaMemcpy(dk, md.dk[sp].data(), sizeof(int) * md.ndu[sp], cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(dh, md.dh[sp].data(), sizeof(int) * 4 * md.ndu[sp], cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(dpp, md.dp[sp].data(), sizeof(int) * 4 * md.ndu[sp], cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(dsg, md.dsg[sp].data(), sizeof(double) * md.ndu[sp], cudaMemcpyHostToDevice));
+    }
+    s.dk[sp] = dk; s.dh[sp] = dh; s.dpart[sp] = dpp; s.dsg[sp] = dsg;
+  }
+  {
+    int nd = std::max(1, md.ndet);
+    int *ciu = dalloc<int>(c, nd), *cid = dalloc<int>(c, nd);
+    double *cc = dalloc<double>(c, nd);
+    if (!ciu || !cid || !cc) return fail(CHAMP_ENOMEM, "device allocation of determinant tables failed");
+    CK(cudaMemcpy(ciu, md.ciu.data(), sizeof(int) * md.ndet, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(cid, md.cid.data(), sizeof(int) * md.ndet, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(cc, md.ccoef.data(), sizeof(double) * md.ndet, cudaMemcpyHostToDevice));
+    s.ciu = ciu; s.cid = cid; s.ccoef = cc;
+  }
+  JasPar<T> J;
+  memset(&J, 0, sizeof J);
+  J.scalek = (T)d->scalek; J.norda = d->norda; J.nordb = d->nordb; J.nspin2b = d->nspin2b; J.nct = c->nct;
+  int nt = (int)(cfull.size() / std::max(1, c->nct));
+  for (int it = 0; it < c->nct; it++) {
+    for (int k = 0; k <= d->norda; k++) J.a4[it][k] = (T)d->a4[it * (d->norda + 1) + k];
+    for (int k = 0; k < nt; k++) J.c[it][k] = (T)cfull[(size_t)it * nt + k];
+    J.asymp_a[it] = (T)asymp_a[it];
+  }
+  for (int is = 0; is < d->nspin2b; is++)
+    for (int k = 0; k <= d->nordb; k++) J.b[is][k] = (T)d->b[is * (d->nordb + 1) + k];
+  J.asymp_b[0] = (T)asymp_b[0]; J.asymp_b[1] = (T)asymp_b[1];
+  std::vector<int> ctv(d->iwctype, d->iwctype + c->C);
+  CK(cudaMemcpy(cent, d->cent, sizeof(double) * 3 * c->C, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctype, ctv.data(), sizeof(int) * c->C, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(zc, zcv.data(), sizeof(double) * c->C, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sh, shv.data(), sizeof(int4) * c->nshell, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(shp, shpv.data(), sizeof(int2) * c->nshell, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(shb0, shb0v.data(), sizeof(int) * c->nshell, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(pz, pzv.data(), sizeof(T) * nprim, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(pc, pcv.data(), sizeof(T) * nprim, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(cr0, crv[0].data(), sizeof(T) * crv[0].size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(cr1, crv[1].data(), sizeof(T) * crv[1].size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(jp, &J, sizeof J, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ep, &ecp, sizeof ecp, cudaMemcpyHostToDevice));
+  s.cent = cent; s.ctype = ctype; s.zc = zc; s.shell = sh; s.shprim = shp; s.shb0 = shb0;
+  s.pz = pz; s.pc = pc; s.cocc[0] = cr0; s.cocc[1] = cr1; s.jas = jp; s.ecp = ep;
+  return CHAMP_OK;
+}
+
+template <class T>
+static int build_state(champ_ctx *c, State<T> &st) {
+  size_t W = c->wmax, N = c->N;
+  st.W = 0;
+  st.astride = c->nup * c->nup + c->ndn * c->ndn;
+  const MultiDet &md = c->md;
+  st.tvstride = std::max(1, c->nup * md.nvirt[0] + c->ndn * md.nvirt[1]);
+  st.gstride = md.multidet ? md.nocc[0] * c->nup + md.nocc[1] * c->ndn : 1;
+  st.wstride = md.multidet ? 2 * (md.ndu[0] + md.ndu[1]) : 1;
+  st.x = dalloc<double>(c, W * N * 3);
+  st.ainv = dalloc<double>(c, W * st.astride);
+  st.fso = dalloc<T>(c, W * N * N);
+  st.ren = dalloc<T>(c, W * N * c->C * 2);
+  st.fsum = dalloc<double>(c, W); st.lnd = dalloc<double>(c, W); st.sgn = dalloc<double>(c, W);
+  st.status = dalloc<uint32_t>(c, W);
+  st.pf = dalloc<T>(c, W * N);
+  st.pa = dalloc<double>(c, W * c->nomax);
+  st.pdj = dalloc<double>(c, W); st.prho = dalloc<double>(c, W); st.pxn = dalloc<double>(c, 3 * W);
+  st.piel = dalloc<int>(c, W);
+  st.orb5 = dalloc<T>(c, W * N * 5 * c->nomax);
+  st.tv = dalloc<double>(c, W * st.tvstride);
+  st.gam = dalloc<double>(c, W * st.gstride);
+  st.ymd = dalloc<double>(c, W * st.tvstride);
+  st.wdet = dalloc<double>(c, W * st.wstride);
+  if (!st.tv || !st.gam || !st.ymd || !st.wdet) return fail(CHAMP_ENOMEM, "device allocation of the walker state failed");
+  st.gproj = c->nloc > 0 ? dalloc<T>(c, W * N * c->nbasis) : nullptr;
+  st.nlt = c->nloc > 0 ? dalloc<double>(c, W * N * c->C * NLT) : nullptr;
+  st.o_lnpsi = dalloc<double>(c, W); st.o_sign = dalloc<double>(c, W); st.o_psij = dalloc<double>(c, W);
+  st.o_vel = dalloc<double>(c, W * N * 3); st.o_divv = dalloc<double>(c, W * N); st.o_d2 = dalloc<double>(c, W);
+  st.o_pe = dalloc<double>(c, W); st.o_peee = dalloc<double>(c, W); st.o_penl = dalloc<double>(c, W);
+  st.o_eloc = dalloc<double>(c, W);
+  st.s_esum = dalloc<double>(c, W); st.s_e2sum = dalloc<double>(c, W); st.s_acc = dalloc<double>(c, W);
+  st.s_elast = dalloc<double>(c, W);
+  if (!st.x || !st.ainv || !st.fso || !st.ren || !st.orb5 || !st.s_elast || (c->nloc > 0 && (!st.gproj || !st.nlt)))
+    return fail(CHAMP_ENOMEM, "device allocation of the walker state failed");
+  return CHAMP_OK;
+}
+
+static int launch(champ_ctx *c, Op op, const OpArgs &a = OpArgs()) {
+  return c->prec == CHAMP_PREC_FP64 ? launch_f64(c, op, a) : launch_f32(c, op, a);
+}
+// ---------------------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------------------
+template <class T>
+static int copy_eval_out(champ_ctx *c, const champ_eval_out *o) {
+  State<T> &st = stof<T>(c);
+  size_t W = c->W, N = c->N;
+  struct { double *h; double *d; size_t n; } m[] = {
+      {o->lnpsi, st.o_lnpsi, W}, {o->sign, st.o_sign, W}, {o->psij, st.o_psij, W}, {o->velocity, st.o_vel, W * N * 3},
+      {o->div_v, st.o_divv, W * N}, {o->d2lnpsi, st.o_d2, W}, {o->pe, st.o_pe, W}, {o->pe_ee, st.o_peee, W},
+      {o->pe_nonloc, st.o_penl, W}, {o->energy, st.o_eloc, W}};
+  for (auto &e : m)
+    if (e.h) CK(cudaMemcpyAsync(e.h, e.d, sizeof(double) * e.n, cudaMemcpyDeviceToHost, c->stream));
+  return CHAMP_OK;
+}
+
+template <class T>
+static int copy_stats(champ_ctx *c, const champ_vmc_stats *s) {
+  State<T> &st = stof<T>(c);
+  size_t W = c->W;
+  if (s->esum) CK(cudaMemcpyAsync(s->esum, st.s_esum, sizeof(double) * W, cudaMemcpyDeviceToHost, c->stream));
+  if (s->e2sum) CK(cudaMemcpyAsync(s->e2sum, st.s_e2sum, sizeof(double) * W, cudaMemcpyDeviceToHost, c->stream));
+  if (s->accept) CK(cudaMemcpyAsync(s->accept, st.s_acc, sizeof(double) * W, cudaMemcpyDeviceToHost, c->stream));
+  if (s->elast) CK(cudaMemcpyAsync(s->elast, st.s_elast, sizeof(double) * W, cudaMemcpyDeviceToHost, c->stream));
+  return CHAMP_OK;
+}
+
+extern "C" {
+
+const char *champ_last_error(void) { return g_err.c_str(); }
+const char *champ_version(void) { return "champ_b200 0.1 (sm_100a)"; }
+
+int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *stream, champ_ctx **out) {
+  if (!d || !out || w_max <= 0) return fail(CHAMP_EINVAL, "null argument or w_max <= 0");
+  *out = nullptr;
+  if (d->nelec < 1 || d->nelec > CHAMP_MAX_ELEC) return fail(CHAMP_EINVAL, "nelec out of range");
+  if (d->nup < 0 || d->nup > d->nelec) return fail(CHAMP_EINVAL, "nup out of range");
+  if (d->nup > CHAMP_MAX_SPIN || d->nelec - d->nup > CHAMP_MAX_SPIN) return fail(CHAMP_EINVAL, "more than 64 electrons of one spin");
+  if (d->nctype < 1 || d->nctype > MAXCT) return fail(CHAMP_EINVAL, "nctype must be 1..4");
+  if (d->ncent < 1) return fail(CHAMP_EINVAL, "ncent < 1");
+  if (d->ndet < 1 || d->ndet > 65536) return fail(CHAMP_EINVAL, "ndet out of range");
+  if (d->norda > MAXORD - 1 || d->nordb > MAXORD - 1) return fail(CHAMP_EINVAL, "norda/nordb > 7");
+  if (!(d->nordc == 0 || d->nordc == 1 || d->nordc == 4 || d->nordc == 5)) return fail(CHAMP_EINVAL, "nordc must be 0, 1, 4 or 5");
+  if (d->nloc != 0 && d->nloc != 6) return fail(CHAMP_EINVAL, "nloc must be 0 or 6");
+  if (d->nloc == 6 && d->nquad != 12) return fail(CHAMP_EINVAL, "nquad must be 12");
+  if (d->nloc == 6 && d->mgauss > MG) return fail(CHAMP_EINVAL, "more than 4 Gaussian terms per channel");
+  if (precision != CHAMP_PREC_FP64 && precision != CHAMP_PREC_MIXED) return fail(CHAMP_EINVAL, "bad precision");
+  for (int i = 0; i < d->nshell; i++)
+    if (d->shell_l[i] < 0 || d->shell_l[i] > CHAMP_MAX_L || d->shell_n[i] < 1) return fail(CHAMP_EINVAL, "shell with bad n or l");
+  champ_ctx *c = new champ_ctx();
+  c->prec = precision;
+  c->stream = (cudaStream_t)stream;
+  c->wmax = w_max;
+  c->N = d->nelec; c->nup = d->nup; c->ndn = d->nelec - d->nup; c->C = d->ncent; c->nct = d->nctype;
+  c->nshell = d->nshell; c->nbasis = d->nbasis; c->nmax = std::max(1, std::max(c->nup, c->ndn));
+  c->nordc = d->nordc; c->nloc = d->nloc;
+  {
+    int rc0 = build_multidet(d, c->md);
+    if (rc0) { delete c; return rc0; }
+    c->nomax = std::max(1, std::max(c->md.nocc[0], c->md.nocc[1]));
+    if (c->nomax > 256) { delete c; return fail(CHAMP_EINVAL, "more than 256 occupied orbitals of one spin"); }
+  }
+  // normalised primitive weights (basis_norm)
+  std::vector<double> pcn;
+  for (int i = 0, p = 0; i < d->nshell; i++)
+    for (int q = 0; q < d->shell_nprim[i]; q++, p++)
+      pcn.push_back(d->prim_coef[p] * host_anorm(d->shell_kind[i], d->shell_n[i], d->shell_l[i], d->prim_zeta[p]));
+  // e-e-n coefficients with the cusp conditions applied
+  int nt = 0;
+  for (int n = 2; n <= d->nordc; n++)
+    for (int k = n - 1; k >= 0; k--) {
+      int l_hi = (k == 0) ? n - k - 2 : n - k;
+      for (int l = l_hi; l >= 0; l--) if (((n - k - l) & 1) == 0) nt++;
+    }
+  std::vector<double> cfull((size_t)d->nctype * std::max(nt, 1), 0.0);
+  if (nt) memcpy(cfull.data(), d->c, sizeof(double) * d->nctype * nt);
+  if (d->een_cusp) host_een_cusp(d->nordc, d->nctype, nt, cfull);
+  if (nt == 0) cfull.assign(d->nctype, 0.0);
+  // asymptotic values for isc=4 (set_scale_dist, scale_dist.f90:147-225)
+  double ar = 1.0 / d->scalek, asa[MAXCT] = {0}, asb[2] = {0, 0};
+  for (int it = 0; it < d->nctype; it++) {
+    const double *a = d->a4 + it * (d->norda + 1);
+    double v = a[0] * ar / (1 + a[1] * ar);
+    for (int k = 2; k <= d->norda; k++) v += a[k] * std::pow(ar, k);
+    asa[it] = v;
+  }
+  for (int i = 0; i < 2; i++) {
+    double ss = (i == 1 && d->nspin2b == 1) ? 0.5 : 1.0;
+    int isp = (i == 1) ? d->nspin2b - 1 : 0;
+    const double *b = d->b + isp * (d->nordb + 1);
+    double v = ss * b[0] * ar / (1 + b[1] * ar);
+    for (int k = 2; k <= d->nordb; k++) v += b[k] * std::pow(ar, k);
+    asb[i] = v;
+  }
+  // pseudopotential and quadrature (rotqua.f90 icosahedral rule)
+  EcpPar ecp;
+  memset(&ecp, 0, sizeof ecp);
+  ecp.nquad = 12;
+  for (int it = 0; it < d->nctype; it++) ecp.znuc[it] = d->znuc[it];
+  if (d->nloc == 6) {
+    for (int it = 0; it < d->nctype; it++) {
+      ecp.npotd[it] = d->npotd[it];
+      ecp.lpotp1[it] = d->lpotp1[it];
+      if (d->npotd[it] < 1 || d->npotd[it] > MAXLCH || d->lpotp1[it] < 1 || d->lpotp1[it] > d->npotd[it]) {
+        delete c;
+        return fail(CHAMP_EINVAL, "bad npotd/lpotp1");
+      }
+      for (int l = 0; l < MAXLCH; l++) {
+        int ntm = d->necp_term[it * MAXLCH + l];
+        if (ntm > MG) { delete c; return fail(CHAMP_EINVAL, "too many ECP terms"); }
+        ecp.nterm[it][l] = ntm;
+        for (int i = 0; i < ntm; i++) {
+          size_t o = ((size_t)it * MAXLCH + l) * d->mgauss + i;
+          ecp.coef[it][l][i] = d->ecp_coef[o];
+          ecp.expo[it][l][i] = d->ecp_exponent[o];
+          ecp.pw[it][l][i] = d->necp_power[o];
+        }
+      }
+    }
+  }
+  {
+    const double pi = 3.141592653589793, zr = 1.0 / std::sqrt(5.0), rr = 2.0 / std::sqrt(5.0);
+    ecp.q0[0][0] = 0; ecp.q0[0][1] = 0; ecp.q0[0][2] = 1;
+    ecp.q0[1][0] = 0; ecp.q0[1][1] = 0; ecp.q0[1][2] = -1;
+    for (int k = 0; k < 5; k++) {
+      double a = 2 * pi * k / 5.0, b = a + pi / 5.0;
+      ecp.q0[2 + k][0] = rr * std::cos(a); ecp.q0[2 + k][1] = rr * std::sin(a); ecp.q0[2 + k][2] = zr;
+      ecp.q0[7 + k][0] = rr * std::cos(b); ecp.q0[7 + k][1] = rr * std::sin(b); ecp.q0[7 + k][2] = -zr;
+    }
+    for (int k = 0; k < 12; k++) ecp.wq[k] = 1.0 / 12.0;
+  }
+  double pecent = 0;
+  for (int i = 0; i < d->ncent; i++)
+    for (int j = 0; j < i; j++) {
+      double dx = d->cent[3 * i] - d->cent[3 * j], dy = d->cent[3 * i + 1] - d->cent[3 * j + 1],
+             dz = d->cent[3 * i + 2] - d->cent[3 * j + 2];
+      pecent += d->znuc[d->iwctype[i]] * d->znuc[d->iwctype[j]] / std::sqrt(dx * dx + dy * dy + dz * dz);
+    }
+  int rc;
+  if (precision == CHAMP_PREC_FP64) {
+    rc = build_sys<double>(c, d, pcn, cfull, asa, asb, ecp, pecent, c->sd);
+    if (!rc) rc = build_state<double>(c, c->std_);
+    c->lay = make_layout<double>(c->N, c->C, c->nbasis, c->nmax, c->nomax, c->std_.astride, c->std_.tvstride,
+                                 c->std_.gstride, c->std_.wstride, c->nloc > 0, RESIDENT_LIMIT);
+    c->smem = c->lay.bytes;
+  } else {
+    rc = build_sys<float>(c, d, pcn, cfull, asa, asb, ecp, pecent, c->sf);
+    if (!rc) rc = build_state<float>(c, c->stf);
+    c->lay = make_layout<float>(c->N, c->C, c->nbasis, c->nmax, c->nomax, c->stf.astride, c->stf.tvstride,
+                                c->stf.gstride, c->stf.wstride, c->nloc > 0, RESIDENT_LIMIT);
+    c->smem = c->lay.bytes;
+  }
+  if (rc) { champ_destroy(c); return rc; }
+  // warps per block: up to 8, keeping the block's dynamic shared memory under 96 KB
+  c->wpb = 4;  // 128-thread blocks (the kernels' launch bounds)
+  while (c->wpb > 1 && c->smem * c->wpb > 96 * 1024) c->wpb >>= 1;
+  if (c->smem * c->wpb > 200 * 1024) { champ_destroy(c); return fail(CHAMP_EINVAL, "system too large for the per-warp shared memory"); }
+  c->smem *= c->wpb;
+  rc = c->prec == CHAMP_PREC_FP64 ? attrs_f64(c) : attrs_f32(c);
+  if (rc) { champ_destroy(c); return rc; }
+  c->d_in = dalloc<double>(c, (size_t)w_max * 3 * c->N);
+  c->d_out = dalloc<double>(c, (size_t)w_max * 4 * c->N);
+  c->d_mask = dalloc<uint8_t>(c, w_max);
+  if (!c->d_in || !c->d_out || !c->d_mask) { champ_destroy(c); return fail(CHAMP_ENOMEM, "staging allocation failed"); }
+  *out = c;
+  return CHAMP_OK;
+}
+
+int champ_destroy(champ_ctx *c) {
+  if (!c) return CHAMP_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  else cudaDeviceSynchronize();
+  for (void *p : c->allocs) cudaFree(p);
+  delete c;
+  return CHAMP_OK;
+}
+
+int champ_nparam(const champ_ctx *c, int32_t *nj, int32_t *ncsf, int32_t *norb) {
+  if (!c) return fail(CHAMP_EINVAL, "null context");
+  if (nj) *nj = c->nparm_jas;
+  if (ncsf) *ncsf = 0;
+  if (norb) *norb = 0;
+  return CHAMP_OK;
+}
+
+static double *state_x(champ_ctx *c) { return c->prec == CHAMP_PREC_FP64 ? c->std_.x : c->stf.x; }
+
+int champ_set_walkers(champ_ctx *c, int32_t nw, const double *x) {
+  if (!c || !x) return fail(CHAMP_EINVAL, "null argument");
+  if (nw < 1 || nw > c->wmax) return fail(CHAMP_EINVAL, "nw out of range");
+  c->W = nw;
+  CK(cudaMemcpyAsync(state_x(c), x, sizeof(double) * nw * 3 * c->N, cudaMemcpyHostToDevice, c->stream));
+  int *piel = c->prec == CHAMP_PREC_FP64 ? c->std_.piel : c->stf.piel;
+  CK(cudaMemsetAsync(piel, 0xFF, sizeof(int) * nw, c->stream));
+  int rc = launch(c, Op::Eval);
+  if (rc) return rc;
+  c->have_walkers = true;
+  CK(cudaStreamSynchronize(c->stream));
+  return CHAMP_OK;
+}
+
+int champ_get_walkers(champ_ctx *c, double *x) {
+  if (!c || !x) return fail(CHAMP_EINVAL, "null argument");
+  if (!c->have_walkers) return fail(CHAMP_ESTATE, "no walkers set");
+  CK(cudaMemcpyAsync(x, state_x(c), sizeof(double) * c->W * 3 * c->N, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return CHAMP_OK;
+}
+
+int champ_set_quadrature_rotation(champ_ctx *c, const double *rot) {
+  if (!c) return fail(CHAMP_EINVAL, "null context");
+  static const double I[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  memcpy(c->rot, rot ? rot : I, sizeof(double) * 9);
+  return CHAMP_OK;
+}
+
+
+int champ_eval_full(champ_ctx *c, const champ_eval_out *o) {
+  if (!c) return fail(CHAMP_EINVAL, "null context");
+  if (!c->have_walkers) return fail(CHAMP_ESTATE, "no walkers set");
+  int rc = launch(c, Op::EvalOut);
+  if (rc) return rc;
+  if (o) {
+    rc = c->prec == CHAMP_PREC_FP64 ? copy_eval_out<double>(c, o) : copy_eval_out<float>(c, o);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return CHAMP_OK;
+}
+
+int champ_propose_1e(champ_ctx *c, int32_t iel, const double *xnew, double *ratio, double *grad_new) {
+  if (!c || !xnew || !ratio) return fail(CHAMP_EINVAL, "null argument");
+  if (!c->have_walkers) return fail(CHAMP_ESTATE, "no walkers set");
+  if (iel < 0 || iel >= c->N) return fail(CHAMP_EINVAL, "iel out of range");
+  size_t W = c->W;
+  CK(cudaMemcpyAsync(c->d_in, xnew, sizeof(double) * 3 * W, cudaMemcpyHostToDevice, c->stream));
+  OpArgs a;
+  a.e = iel;
+  a.xnew = c->d_in;
+  a.ratio = c->d_out;
+  a.grad = c->d_out + W;
+  int rc = launch(c, grad_new ? Op::ProposeGrad : Op::Propose, a);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(ratio, c->d_out, sizeof(double) * W, cudaMemcpyDeviceToHost, c->stream));
+  if (grad_new) CK(cudaMemcpyAsync(grad_new, c->d_out + W, sizeof(double) * 3 * W, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return CHAMP_OK;
+}
+
+int champ_accept_1e(champ_ctx *c, int32_t iel, const uint8_t *accept) {
+  if (!c || !accept) return fail(CHAMP_EINVAL, "null argument");
+  if (!c->have_walkers) return fail(CHAMP_ESTATE, "no walkers set");
+  if (iel < 0 || iel >= c->N) return fail(CHAMP_EINVAL, "iel out of range");
+  CK(cudaMemcpyAsync(c->d_mask, accept, c->W, cudaMemcpyHostToDevice, c->stream));
+  OpArgs a;
+  a.e = iel;
+  a.mask = c->d_mask;
+  int rc = launch(c, Op::Accept, a);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  return CHAMP_OK;
+}
+
+int champ_grad_1e(champ_ctx *c, int32_t iel, double *grad) {
+  if (!c || !grad) return fail(CHAMP_EINVAL, "null argument");
+  if (!c->have_walkers) return fail(CHAMP_ESTATE, "no walkers set");
+  if (iel < 0 || iel >= c->N) return fail(CHAMP_EINVAL, "iel out of range");
+  // a proposal at the current position: ratio 1, gradient of the current configuration
+  std::vector<double> x((size_t)c->W * 3 * c->N), xn((size_t)c->W * 3), r(c->W);
+  int rc = champ_get_walkers(c, x.data());
+  if (rc) return rc;
+  for (int w = 0; w < c->W; w++)
+    for (int k = 0; k < 3; k++) xn[3 * w + k] = x[((size_t)w * c->N + iel) * 3 + k];
+  return champ_propose_1e(c, iel, xn.data(), r.data(), grad);
+}
+
+
+int champ_vmc_sweeps(champ_ctx *c, int32_t nsweep, uint64_t seed, uint64_t sweep0, double step,
+                     const champ_vmc_stats *stats) {
+  if (!c) return fail(CHAMP_EINVAL, "null context");
+  if (!c->have_walkers) return fail(CHAMP_ESTATE, "no walkers set");
+  if (nsweep < 0) return fail(CHAMP_EINVAL, "nsweep < 0");
+  OpArgs a;
+  a.nsweep = nsweep;
+  a.seed = seed;
+  a.sweep0 = sweep0;
+  a.step = step;
+  int rc = launch(c, Op::Vmc, a);
+  if (rc) return rc;
+  if (stats) {
+    rc = c->prec == CHAMP_PREC_FP64 ? copy_stats<double>(c, stats) : copy_stats<float>(c, stats);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  return CHAMP_OK;
+}
+
+int champ_vmc_run_host(champ_ctx *c, int32_t nw, double *x, int32_t nsweep, uint64_t seed, uint64_t sweep0,
+                       double step, double *eloc) {
+  if (!c || !x || !eloc) return fail(CHAMP_EINVAL, "null argument");
+  if (nw < 1 || nw > c->wmax) return fail(CHAMP_EINVAL, "nw out of range");
+  c->W = nw;
+  CK(cudaMemcpyAsync(state_x(c), x, sizeof(double) * nw * 3 * c->N, cudaMemcpyHostToDevice, c->stream));
+  int rc = launch(c, Op::Eval);
+  if (rc) return rc;
+  c->have_walkers = true;
+  champ_vmc_stats st = {nullptr, nullptr, nullptr, nullptr};
+  rc = champ_vmc_sweeps(c, nsweep, seed, sweep0, step, &st);
+  if (rc) return rc;
+  double *el = c->prec == CHAMP_PREC_FP64 ? c->std_.s_elast : c->stf.s_elast;
+  CK(cudaMemcpyAsync(eloc, el, sizeof(double) * nw, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(x, state_x(c), sizeof(double) * nw * 3 * c->N, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return CHAMP_OK;
+}
+
+int champ_walker_status(champ_ctx *c, uint32_t *flags) {
+  if (!c || !flags) return fail(CHAMP_EINVAL, "null argument");
+  uint32_t *s = c->prec == CHAMP_PREC_FP64 ? c->std_.status : c->stf.status;
+  CK(cudaMemcpyAsync(flags, s, sizeof(uint32_t) * c->W, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return CHAMP_OK;
+}
+
+int champ_synchronize(champ_ctx *c) {
+  if (!c) return fail(CHAMP_EINVAL, "null context");
+  CK(cudaStreamSynchronize(c->stream));
+  return CHAMP_OK;
+}
+
+}  // extern "C"

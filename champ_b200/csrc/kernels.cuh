@@ -1,0 +1,1029 @@
+// kernels.cuh -- walker-batched Slater-Jastrow engine: state layout and kernels.
+//
+// One warp owns one walker.  Walker state lives in HBM, walker-major:
+//   x[w][e][3] (double), ainv[w][spin block][k][e] (double, reference-determinant inverse),
+//   fso[w][i][j] (T, Jastrow pair table: i != j pair term incl. e-e-n, i == j e-n term),
+//   ln|D|, sign, J per walker.
+// Per-warp scratch (basis values, proposed orbital row, gradient accumulators) lives in
+// shared memory; larger per-walker scratch (orbitals of all electrons, projected
+// coefficients, pseudopotential task lists) in HBM.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/champ_b200.h"
+#include "device_math.cuh"
+
+using namespace champ;
+
+// ---------------------------------------------------------------------------------------
+// state
+// ---------------------------------------------------------------------------------------
+template <class T>
+struct State {
+  int W;
+  double *x;       // [W][N][3]
+  double *ainv;    // [W][astride]; spin-up block at 0 (nup x nup), spin-down at nup*nup
+  T *fso;          // [W][N][N]
+  T *ren;          // [W][N][C][2]: r_en and 1/(1 + scalek r_en)
+  double *fsum, *lnd, *sgn;
+  uint32_t *status;
+  T *pf;           // [W][N] proposed pair values
+  double *pa;      // [W][nomax] proposed orbital row (occupied orbitals)
+  double *pdj, *prho, *pxn;  // [W], [W], [W][3]
+  int *piel;       // [W]
+  T *orb5;         // [W][N][5][nomax]
+  T *gproj;        // [W][N][nbasis]
+  double *nlt;     // [W][N*C][NLT]
+  double *tv;      // [W][tvstride] T = Ainv Atilde restricted to the virtual orbitals, per spin [k][p]
+  double *gam;     // [W][gstride] G matrix per spin [m][e] (multi-determinant only)
+  double *ymd;     // [W][tvstride] Y scratch [p][k]
+  double *wdet;    // [W][2*(ndu0+ndu1)] alpha determinants, then determinant weights
+  int astride, tvstride, gstride, wstride;
+  // outputs of a full evaluation
+  double *o_lnpsi, *o_sign, *o_psij, *o_vel, *o_divv, *o_d2, *o_pe, *o_peee, *o_penl, *o_eloc;
+  // VMC accumulators
+  double *s_esum, *s_e2sum, *s_acc, *s_elast;
+};
+constexpr int NLT = 2 + MAXLCH;  // task record: (e*C+c), r, vps[0..MAXLCH-1]
+
+// Per-warp shared-memory layout, computed on the host.  When `resident` is set the
+// walker's whole state and scratch live in shared memory for the life of a kernel
+// (small systems); otherwise they stay in HBM.
+struct Layout {
+  size_t phi, arow, xs, vacc, divj, colb, vb, perm, rnew;  // always in shared memory
+  size_t ainv, fso, ren, pf, orb5, gproj, nlt, tv, gam, ymd, wdet;  // resident mode only
+  size_t bytes;
+  int resident;
+};
+
+// Per-walker view: where this walker's arrays live for the current kernel.
+template <class T>
+struct View {
+  T *phi, *arow;
+  double *xs, *vacc, *divj, *colb, *vb;
+  int *perm;
+  T *rnew;         // [C][2] proposed electron's distances to the centres
+  double *ainv;
+  T *fso, *ren, *pf, *orb5, *gproj;
+  double *nlt, *tv, *gam, *ymd, *wdet;
+};
+
+__host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+template <class T>
+static Layout make_layout(int N, int C, int nbasis, int nmax, int nomax, int astride, int tvstride, int gstride,
+                          int wstride, bool nl, size_t resident_limit) {
+  Layout L;
+  size_t o = 0;
+  auto take = [&](size_t b) { size_t r = o; o += align16(b); return r; };
+  L.phi = take(sizeof(T) * nbasis * 5);
+  L.arow = take(sizeof(T) * 5 * nomax);
+  L.xs = take(sizeof(double) * N * 3);
+  L.vacc = take(sizeof(double) * N * 3);
+  L.divj = take(sizeof(double) * N);
+  L.colb = take(sizeof(double) * nmax);
+  L.vb = take(sizeof(double) * nmax);
+  L.perm = take(sizeof(int) * nmax);
+  L.rnew = take(sizeof(T) * C * 2);
+  size_t base = o;
+  L.ainv = take(sizeof(double) * astride);
+  L.fso = take(sizeof(T) * N * N);
+  L.ren = take(sizeof(T) * N * C * 2);
+  L.pf = take(sizeof(T) * N);
+  L.orb5 = take(sizeof(T) * N * 5 * nomax);
+  L.gproj = nl ? take(sizeof(T) * N * nbasis) : 0;
+  L.nlt = nl ? take(sizeof(double) * N * C * NLT) : 0;
+  L.tv = take(sizeof(double) * tvstride);
+  L.gam = take(sizeof(double) * gstride);
+  L.ymd = take(sizeof(double) * tvstride);
+  L.wdet = take(sizeof(double) * wstride);
+  L.resident = (o <= resident_limit) ? 1 : 0;
+  L.bytes = L.resident ? o : base;
+  return L;
+}
+
+template <class T>
+__device__ inline View<T> make_view(char *base, const Layout &L, const State<T> &st, int w, int N, int C, int nbasis,
+                                    int nomax, bool resident) {
+  View<T> v;
+  v.phi = (T *)(base + L.phi);
+  v.arow = (T *)(base + L.arow);
+  v.xs = (double *)(base + L.xs);
+  v.vacc = (double *)(base + L.vacc);
+  v.divj = (double *)(base + L.divj);
+  v.colb = (double *)(base + L.colb);
+  v.vb = (double *)(base + L.vb);
+  v.perm = (int *)(base + L.perm);
+  v.rnew = (T *)(base + L.rnew);
+  if (resident) {
+    v.ainv = (double *)(base + L.ainv);
+    v.fso = (T *)(base + L.fso);
+    v.ren = (T *)(base + L.ren);
+    v.pf = (T *)(base + L.pf);
+    v.orb5 = (T *)(base + L.orb5);
+    v.gproj = (T *)(base + L.gproj);
+    v.nlt = (double *)(base + L.nlt);
+    v.tv = (double *)(base + L.tv);
+    v.gam = (double *)(base + L.gam);
+    v.ymd = (double *)(base + L.ymd);
+    v.wdet = (double *)(base + L.wdet);
+  } else {
+    v.ainv = st.ainv + (size_t)w * st.astride;
+    v.fso = st.fso + (size_t)w * N * N;
+    v.ren = st.ren + (size_t)w * N * C * 2;
+    v.pf = st.pf + (size_t)w * N;
+    v.orb5 = st.orb5 + (size_t)w * N * 5 * nomax;
+    v.gproj = st.gproj ? st.gproj + (size_t)w * N * nbasis : nullptr;
+    v.nlt = st.nlt ? st.nlt + (size_t)w * N * C * NLT : nullptr;
+    v.tv = st.tv + (size_t)w * st.tvstride;
+    v.gam = st.gam + (size_t)w * st.gstride;
+    v.ymd = st.ymd + (size_t)w * st.tvstride;
+    v.wdet = st.wdet + (size_t)w * st.wstride;
+  }
+  return v;
+}
+
+// Copy a walker's persistent state between HBM and its resident view.
+template <class T>
+__device__ inline void view_load(const View<T> &v, const State<T> &st, int w, int N, int C, int lane) {
+  for (int i = lane; i < 3 * N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * N + i];
+  for (int i = lane; i < st.astride; i += 32) v.ainv[i] = st.ainv[(size_t)w * st.astride + i];
+  for (int i = lane; i < N * N; i += 32) v.fso[i] = st.fso[(size_t)w * N * N + i];
+  for (int i = lane; i < N * C * 2; i += 32) v.ren[i] = st.ren[(size_t)w * N * C * 2 + i];
+  for (int i = lane; i < st.tvstride; i += 32) v.tv[i] = st.tv[(size_t)w * st.tvstride + i];
+  for (int i = lane; i < st.gstride; i += 32) v.gam[i] = st.gam[(size_t)w * st.gstride + i];
+  __syncwarp();
+}
+template <class T>
+__device__ inline void view_store(const View<T> &v, const State<T> &st, int w, int N, int C, int lane) {
+  __syncwarp();
+  for (int i = lane; i < 3 * N; i += 32) st.x[(size_t)w * 3 * N + i] = v.xs[i];
+  for (int i = lane; i < st.astride; i += 32) st.ainv[(size_t)w * st.astride + i] = v.ainv[i];
+  for (int i = lane; i < N * N; i += 32) st.fso[(size_t)w * N * N + i] = v.fso[i];
+  for (int i = lane; i < N * C * 2; i += 32) st.ren[(size_t)w * N * C * 2 + i] = v.ren[i];
+  for (int i = lane; i < st.tvstride; i += 32) st.tv[(size_t)w * st.tvstride + i] = v.tv[i];
+  for (int i = lane; i < st.gstride; i += 32) st.gam[(size_t)w * st.gstride + i] = v.gam[i];
+  __syncwarp();
+}
+
+// ---------------------------------------------------------------------------------------
+// warp Gauss-Jordan inversion with partial pivoting, in place (matinv, qmc/vmc/matinv.f90).
+// A is row-major n x n (electron row, orbital column); on return it holds the inverse
+// indexed [orbital][electron].  Returns false if a pivot is exactly zero.
+// ---------------------------------------------------------------------------------------
+static __device__ bool warp_gj(double *A, int n, int *perm, double &lnd, double &sg, int lane) {
+  lnd = 0;
+  sg = 1;
+  for (int k = 0; k < n; k++) {
+    double best = -1.0;
+    int bi = k;
+    for (int i = k + lane; i < n; i += 32) {
+      double v = fabs(A[i * n + k]);
+      if (v > best) { best = v; bi = i; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+    }
+    if (!(best > 0.0)) return false;
+    if (bi != k) {
+      for (int j = lane; j < n; j += 32) {
+        double t = A[k * n + j];
+        A[k * n + j] = A[bi * n + j];
+        A[bi * n + j] = t;
+      }
+      sg = -sg;
+    }
+    if (lane == 0) perm[k] = bi;
+    __syncwarp();
+    double piv = A[k * n + k];
+    lnd += log(fabs(piv));
+    if (piv < 0) sg = -sg;
+    double pinv = 1.0 / piv;
+    __syncwarp();
+    for (int j = lane; j < n; j += 32) A[k * n + j] = (j == k) ? pinv : A[k * n + j] * pinv;
+    __syncwarp();
+    for (int idx = lane; idx < n * n; idx += 32) {
+      int i = idx / n, j = idx - i * n;
+      if (i != k && j != k) A[idx] -= A[i * n + k] * A[k * n + j];
+    }
+    __syncwarp();
+    for (int i = lane; i < n; i += 32)
+      if (i != k) A[i * n + k] = -A[i * n + k] * pinv;
+    __syncwarp();
+  }
+  for (int k = n - 1; k >= 0; k--) {
+    int p = perm[k];
+    if (p != k)
+      for (int i = lane; i < n; i += 32) {
+        double t = A[i * n + k];
+        A[i * n + k] = A[i * n + p];
+        A[i * n + p] = t;
+      }
+    __syncwarp();
+  }
+  return true;
+}
+
+// (2L+1) P_L(x) (yl0, qmc/vmc/nonloc.f90:249-274)
+static __device__ __forceinline__ double yl0(int L, double x) {
+  if (L == 0) return 1.0;
+  double p0 = 1, p1 = x;
+  for (int n = 1; n < L; n++) {
+    double p2 = ((2 * n + 1) * x * p1 - n * p0) / (n + 1);
+    p0 = p1;
+    p1 = p2;
+  }
+  return (2 * L + 1) * p1;
+}
+
+// Gaussian pseudopotential channels at r (getvps_gauss/gauss_pot, readps_gauss.f90:126-165)
+static __device__ __forceinline__ void ecp_vps(const EcpPar &E, int it, double r, double *vps) {
+  r = r > 1e-10 ? r : 1e-10;
+  double rsq = r * r;
+  for (int l = 0; l < E.npotd[it]; l++) {
+    double v = 0;
+    for (int i = 0; i < E.nterm[it][l]; i++) {
+      int pw = E.pw[it][l][i];
+      double p = 1.0;
+      if (pw != 2) p = pow(r, (double)(pw - 2));
+      v += p * E.coef[it][l][i] * exp(-E.expo[it][l][i] * rsq);
+    }
+    if (l + 1 == E.lpotp1[it]) v -= E.znuc[it] / r;
+    vps[l] = v;
+  }
+}
+
+// distance of point p to centre c and 1/(1 + scalek r)
+template <class T>
+__device__ __forceinline__ void cen_dist(const Sys<T> &s, T sk, const double *p, int c, T &r, T &d) {
+  const double *cc = s.cent + 3 * c;
+  T a = T(p[0] - cc[0]), b = T(p[1] - cc[1]), e = T(p[2] - cc[2]);
+  r = tsqrt(a * a + b * b + e * e);
+  d = T(1) / (T(1) + sk * r);
+}
+
+// Jastrow pair term (e-e + e-e-n) for electron e at xe (distances re[c][2]) and
+// electron j at xj (distances rj[c][2]); gradient wrt xe if GRAD.
+template <class T, int NORD, bool GRAD>
+__device__ __forceinline__ T pair_value(const Sys<T> &s, const JasPar<T> &J, int e, int j, const double *xe,
+                                        const T *re, const double *xj, const T *rj, T *g) {
+  int isb, ipar;
+  T ss;
+  pair_class(J, s.nup, e, j, isb, ss, ipar);
+  T rv[3] = {T(xe[0] - xj[0]), T(xe[1] - xj[1]), T(xe[2] - xj[2])};
+  T rij = tsqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
+  T du = T(1) / (T(1) + J.scalek * rij);
+  T fu = 0, fuu = 0;
+  T f = jas_ee<T, GRAD>(J, isb, ss, ipar, rij, du, fu, fuu);
+  if (GRAD) { g[0] = fu * rv[0]; g[1] = fu * rv[1]; g[2] = fu * rv[2]; }
+  if (NORD > 1) {
+    for (int c = 0; c < s.C; c++) {
+      Een<T> o;
+      jas_een<T, NORD, GRAD ? 1 : 0>(J, s.ctype[c], rij, du, re[2 * c], re[2 * c + 1], rj[2 * c], rj[2 * c + 1], o);
+      f += o.fc;
+      if (GRAD) {
+        const double *cc = s.cent + 3 * c;
+#pragma unroll
+        for (int k = 0; k < 3; k++) g[k] += o.fi * T(xe[k] - cc[k]) + o.fu * rv[k];
+      }
+    }
+  }
+  return f;
+}
+
+// ---------------------------------------------------------------------------------------
+// multi-determinant G matrix (deriv_fast_mod.f90: alpha_bld :427, eval_y :545, g_bld :600)
+// ---------------------------------------------------------------------------------------
+// Determinant (and inverse, row-major, if inv != nullptr) of a k x k matrix, k <= 4.
+static __device__ inline double small_det_inv(const double *a0, int k, double *inv) {
+  double m[4][8];
+  for (int i = 0; i < k; i++)
+    for (int j = 0; j < k; j++) {
+      m[i][j] = a0[i * k + j];
+      m[i][k + j] = (i == j) ? 1.0 : 0.0;
+    }
+  double det = 1.0;
+  for (int c = 0; c < k; c++) {
+    int p = c;
+    for (int i = c + 1; i < k; i++)
+      if (fabs(m[i][c]) > fabs(m[p][c])) p = i;
+    if (m[p][c] == 0.0) {
+      if (inv)
+        for (int i = 0; i < k * k; i++) inv[i] = 0.0;
+      return 0.0;
+    }
+    if (p != c) {
+      det = -det;
+      for (int j = 0; j < 2 * k; j++) { double t = m[c][j]; m[c][j] = m[p][j]; m[p][j] = t; }
+    }
+    double pv = m[c][c];
+    det *= pv;
+    double pi = 1.0 / pv;
+    for (int j = 0; j < 2 * k; j++) m[c][j] *= pi;
+    for (int i = 0; i < k; i++) {
+      if (i == c) continue;
+      double f = m[i][c];
+      if (f != 0.0)
+        for (int j = 0; j < 2 * k; j++) m[i][j] -= f * m[c][j];
+    }
+  }
+  if (inv)
+    for (int i = 0; i < k; i++)
+      for (int j = 0; j < k; j++) inv[i * k + j] = m[i][k + j];
+  return det;
+}
+
+template <class T, bool MD>
+__device__ __forceinline__ double *gam_ptr(const Sys<T> &s, const View<T> &v, int sp) {
+  if (MD) return v.gam + (sp ? s.nocc[0] * s.nup : 0);
+  return v.ainv + (sp ? s.nup * s.nup : 0);
+}
+
+// alpha_I = T[holes, particles] for unique determinant I of spin sp
+template <class T>
+__device__ __forceinline__ int load_alpha(const Sys<T> &s, const View<T> &v, int sp, int I, double *a) {
+  const int nv = s.nvirt[sp];
+  const double *Tv = v.tv + (sp ? s.nup * s.nvirt[0] : 0);
+  int k = s.dk[sp][I];
+  for (int ia = 0; ia < k; ia++)
+    for (int ib = 0; ib < k; ib++) a[ia * k + ib] = Tv[s.dh[sp][4 * I + ia] * nv + s.dpart[sp][4 * I + ib]];
+  return k;
+}
+
+// From the reference inverses (v.ainv) and T (v.tv): chi = sum_I c_I s_I det(alpha_I^up) det(alpha_I^dn),
+// Y = sum_I (c_I s_I det det / chi) alpha_I^-1 scattered to (particle, hole), and
+// G = [Ainv - T Y Ainv ; Y Ainv] for both spins.  Returns ln|chi| and sign(chi).
+template <class T>
+__device__ void build_gamma(const Sys<T> &s, const View<T> &v, int lane, double &lnchi, double &sgnchi) {
+  const int nd0 = s.ndu[0], nd1 = s.ndu[1];
+  double *wd = v.wdet, *wg = v.wdet + nd0 + nd1;
+  for (int sp = 0; sp < 2; sp++)
+    for (int I = lane; I < s.ndu[sp]; I += 32) {
+      double a[16];
+      int k = load_alpha(s, v, sp, I, a);
+      wd[(sp ? nd0 : 0) + I] = s.dsg[sp][I] * (k ? small_det_inv(a, k, nullptr) : 1.0);
+    }
+  for (int i = lane; i < nd0 + nd1; i += 32) wg[i] = 0.0;
+  __syncwarp();
+  double chi = 0;
+  for (int I = lane; I < s.ndet; I += 32) {
+    int iu = s.ciu[I], id = s.cid[I];
+    double t = s.ccoef[I] * wd[iu] * wd[nd0 + id];
+    chi += t;
+    atomicAdd(&wg[iu], t);
+    atomicAdd(&wg[nd0 + id], t);
+  }
+  chi = warp_sum(chi);
+  __syncwarp();
+  double ichi = 1.0 / chi;
+  for (int sp = 0; sp < 2; sp++) {
+    const int n = sp ? s.ndn : s.nup, nv = s.nvirt[sp];
+    if (n == 0) continue;
+    double *Y = v.ymd + (sp ? s.nup * s.nvirt[0] : 0);
+    const double *A = v.ainv + (sp ? s.nup * s.nup : 0);
+    const double *Tv = v.tv + (sp ? s.nup * s.nvirt[0] : 0);
+    double *G = v.gam + (sp ? s.nocc[0] * s.nup : 0);
+    for (int i = lane; i < nv * n; i += 32) Y[i] = 0.0;
+    __syncwarp();
+    for (int I = lane; I < s.ndu[sp]; I += 32) {
+      double a[16], inv[16];
+      int k = load_alpha(s, v, sp, I, a);
+      double wI = wg[(sp ? nd0 : 0) + I] * ichi;
+      if (k == 0 || wI == 0.0) continue;
+      small_det_inv(a, k, inv);
+      for (int ia = 0; ia < k; ia++)
+        for (int ib = 0; ib < k; ib++)
+          atomicAdd(&Y[s.dpart[sp][4 * I + ib] * n + s.dh[sp][4 * I + ia]], wI * inv[ib * k + ia]);
+    }
+    __syncwarp();
+    for (int i = lane; i < nv * n; i += 32) {
+      int p = i / n, e = i - p * n;
+      double acc = 0;
+      for (int k = 0; k < n; k++) acc += Y[p * n + k] * A[k * n + e];
+      G[(n + p) * n + e] = acc;
+    }
+    __syncwarp();
+    for (int i = lane; i < n * n; i += 32) {
+      int k = i / n, e = i - k * n;
+      double acc = A[i];
+      for (int p = 0; p < nv; p++) acc -= Tv[k * nv + p] * G[(n + p) * n + e];
+      G[k * n + e] = acc;
+    }
+    __syncwarp();
+  }
+  lnchi = log(fabs(chi));
+  sgnchi = chi < 0 ? -1.0 : 1.0;
+}
+
+// ---------------------------------------------------------------------------------------
+// hpsi for one walker (qmc/vmc/hpsi.f90:2-381), warp-cooperative.
+// ---------------------------------------------------------------------------------------
+struct EvalRes {
+  double lnpsi, sign, psij, d2lnpsi, pe, pe_ee, pe_nl, eloc;
+  bool singular;
+};
+
+template <class T, int NORD, bool MD>
+__device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, const State<T> &st, int w,
+                          const View<T> &v, const double *R, int lane, bool outputs, EvalRes &res) {
+  const int N = s.N, C = s.C, nomax = s.nomax;
+  const double *xs = v.xs;
+  T *fso = v.fso;
+  const T sk = J.scalek;
+  // --- electron-nucleus distance table (distances.f90:16-27)
+  for (int i = lane; i < N * C; i += 32) {
+    int e = i / C, c = i - e * C;
+    T r, d;
+    cen_dist(s, sk, xs + 3 * e, c, r, d);
+    v.ren[2 * i] = r;
+    v.ren[2 * i + 1] = d;
+  }
+  for (int i = lane; i < 3 * N; i += 32) v.vacc[i] = 0;
+  for (int i = lane; i < N; i += 32) v.divj[i] = 0;
+  __syncwarp();
+  // --- Jastrow (jastrow4.f90) and e-e Coulomb (distances.f90:131-158)
+  double fsum = 0, d2j = 0, pe_ee = 0, pe_en = 0;
+  const int npair = N * (N - 1) / 2;
+  for (int p = lane; p < npair; p += 32) {
+    int i = (int)((1.0 + sqrt(1.0 + 8.0 * (double)p)) * 0.5);
+    while (i * (i - 1) / 2 > p) i--;
+    while ((i + 1) * i / 2 <= p) i++;
+    int j = p - i * (i - 1) / 2;
+    const double *xi = xs + 3 * i, *xj = xs + 3 * j;
+    int isb, ipar;
+    T ss;
+    pair_class(J, s.nup, i, j, isb, ss, ipar);
+    double dx = xi[0] - xj[0], dy = xi[1] - xj[1], dz = xi[2] - xj[2];
+    double rijd = sqrt(dx * dx + dy * dy + dz * dz);
+    pe_ee += 1.0 / rijd;
+    T rv[3] = {T(dx), T(dy), T(dz)};
+    T rij = tsqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
+    T du = T(1) / (T(1) + sk * rij);
+    T fu, fuu;
+    T f = jas_ee<T, true>(J, isb, ss, ipar, rij, du, fu, fuu);
+    T gi[3], gj[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) { gi[k] = fu * rv[k]; gj[k] = -fu * rv[k]; }
+    T d2 = 2 * (fuu + 2 * fu);
+    if (NORD > 1) {
+      const T *ri_ = v.ren + 2 * C * i, *rj_ = v.ren + 2 * C * j;
+      for (int c = 0; c < C; c++) {
+        const double *cc = s.cent + 3 * c;
+        T ri = ri_[2 * c], rj = rj_[2 * c];
+        Een<T> o;
+        jas_een<T, NORD, 2>(J, s.ctype[c], rij, du, ri, ri_[2 * c + 1], rj, rj_[2 * c + 1], o);
+        f += o.fc;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          gi[k] += o.fi * T(xi[k] - cc[k]) + o.fu * rv[k];
+          gj[k] += o.fj * T(xj[k] - cc[k]) - o.fu * rv[k];
+        }
+        T sp = ri + rj, tm = ri - rj;
+        d2 += 2 * (2 * o.fu + o.fi + o.fj) + 2 * o.fuu + o.fii + o.fjj + o.fui * (rij * rij + sp * tm) / (ri * rij) +
+              o.fuj * (rij * rij - sp * tm) / (rj * rij);
+      }
+    }
+    fsum += (double)f;
+    d2j += (double)d2;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      atomicAdd(&v.vacc[3 * i + k], (double)gi[k]);
+      atomicAdd(&v.vacc[3 * j + k], (double)gj[k]);
+    }
+    atomicAdd(&v.divj[i], 0.5 * (double)d2);
+    atomicAdd(&v.divj[j], 0.5 * (double)d2);
+    fso[i * N + j] = f;
+    fso[j * N + i] = f;
+  }
+  __syncwarp();
+  for (int i = lane; i < N; i += 32) {
+    const double *xi = xs + 3 * i;
+    T f = 0, d2 = 0, g[3] = {0, 0, 0};
+    for (int c = 0; c < C; c++) {
+      const double *cc = s.cent + 3 * c;
+      T r = v.ren[2 * (i * C + c)], dn = v.ren[2 * (i * C + c) + 1];
+      T fi, fii;
+      f += jas_en<T, true>(J, s.ctype[c], r, dn, fi, fii);
+#pragma unroll
+      for (int k = 0; k < 3; k++) g[k] += fi * T(xi[k] - cc[k]);
+      d2 += fii + 2 * fi;
+      if (s.nloc == 0) {
+        double rd = sqrt((xi[0] - cc[0]) * (xi[0] - cc[0]) + (xi[1] - cc[1]) * (xi[1] - cc[1]) +
+                         (xi[2] - cc[2]) * (xi[2] - cc[2]));
+        pe_en -= s.zc[c] / rd;
+      }
+    }
+    fsum += (double)f;
+    d2j += (double)d2;
+#pragma unroll
+    for (int k = 0; k < 3; k++) v.vacc[3 * i + k] += (double)g[k];
+    v.divj[i] += (double)d2;
+    fso[i * N + i] = f;
+  }
+  fsum = warp_sum(fsum);
+  d2j = warp_sum(d2j);
+  pe_ee = warp_sum(pe_ee);
+  pe_en = warp_sum(pe_en);
+  __syncwarp();
+
+  // --- orbitals of every electron, Slater matrices (determinant.f90:36-42, t_bld)
+  double *ainv = v.ainv;
+  T *orb5 = v.orb5;
+  for (int e = 0; e < N; e++) {
+    int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
+    double *A = ainv + (sp ? s.nup * s.nup : 0);
+    warp_basis<T, 5>(s, xs + 3 * e, v.phi, lane);
+    T *oe = orb5 + (size_t)e * 5 * nomax;
+    warp_orbitals<T, 5>(v.phi, s.cocc[sp], s.nbasis, s.nocc[sp], oe, nomax, lane);
+    for (int k = lane; k < n; k += 32) A[eo * n + k] = (double)oe[k];
+  }
+  __syncwarp();
+  double lnd = 0, sgn = 1;
+  bool ok = true;
+  for (int sp = 0; sp < 2; sp++) {
+    int n = sp ? s.ndn : s.nup;
+    if (n == 0) continue;
+    double l1, s1;
+    bool o1 = warp_gj(ainv + (sp ? s.nup * s.nup : 0), n, v.perm, l1, s1, lane);
+    ok = ok && o1;
+    lnd += l1;
+    sgn *= s1;
+  }
+  if (MD && ok) {
+    // T = Ainv Atilde on the virtual columns (t_bld, deriv_fast_mod.f90:367-398)
+    for (int sp = 0; sp < 2; sp++) {
+      const int n = sp ? s.ndn : s.nup, nv = s.nvirt[sp], e0 = sp ? s.nup : 0;
+      const double *A = ainv + (sp ? s.nup * s.nup : 0);
+      double *Tv = v.tv + (sp ? s.nup * s.nvirt[0] : 0);
+      for (int i = lane; i < n * nv; i += 32) {
+        int k = i / nv, p = i - k * nv;
+        double acc = 0;
+        for (int e = 0; e < n; e++) acc += A[k * n + e] * (double)orb5[(size_t)(e0 + e) * 5 * nomax + n + p];
+        Tv[i] = acc;
+      }
+    }
+    __syncwarp();
+    double lc, sc;
+    build_gamma(s, v, lane, lc, sc);
+    lnd += lc;
+    sgn *= sc;
+  }
+  // --- grad ln D, lap D / D per electron (determinant.f90:96-150)
+  double d2lnd = 0, v2 = 0;
+  for (int e = 0; e < N; e++) {
+    int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
+    const double *G = gam_ptr<T, MD>(s, v, sp);
+    const T *oe = orb5 + (size_t)e * 5 * nomax;
+    double g0 = 0, g1 = 0, g2 = 0, lp = 0;
+    for (int k = lane; k < s.nocc[sp]; k += 32) {
+      double a = G[k * n + eo];
+      g0 += a * (double)oe[nomax + k];
+      g1 += a * (double)oe[2 * nomax + k];
+      g2 += a * (double)oe[3 * nomax + k];
+      lp += a * (double)oe[4 * nomax + k];
+    }
+    g0 = warp_sum(g0); g1 = warp_sum(g1); g2 = warp_sum(g2); lp = warp_sum(lp);
+    double dvd = lp - (g0 * g0 + g1 * g1 + g2 * g2);
+    d2lnd += dvd;
+    double vx = v.vacc[3 * e] + g0, vy = v.vacc[3 * e + 1] + g1, vz = v.vacc[3 * e + 2] + g2;
+    v2 += vx * vx + vy * vy + vz * vz;
+    if (outputs && lane == 0) {
+      double *ov = st.o_vel + ((size_t)w * N + e) * 3;
+      ov[0] = vx; ov[1] = vy; ov[2] = vz;
+      st.o_divv[(size_t)w * N + e] = v.divj[e] + dvd;
+    }
+  }
+
+  // --- pseudopotential (nonloc_pot.f90, nonloc.f90), quadrature rotated by R
+  double vloc = 0, vnl = 0;
+  if (s.nloc > 0 && ok) {
+    const int B = s.nbasis;
+    T *gp = v.gproj;
+    // G projected onto the basis: g_e[b] = sum_k coef[b][k] Ainv[k][e] (psp_nonloc_pot_bld)
+    for (int e = 0; e < N; e++) {
+      int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
+      const double *G = gam_ptr<T, MD>(s, v, sp);
+      const T *cr = s.cocc[sp];
+      const int no = s.nocc[sp];
+      for (int b = lane; b < B; b += 32) {
+        double acc = 0;
+        for (int k = 0; k < no; k++) acc += (double)cr[b * no + k] * G[k * n + eo];
+        gp[(size_t)e * B + b] = (T)acc;
+      }
+    }
+    double *tl = v.nlt;
+    int ntask = 0;
+    for (int base = 0; base < N * C; base += 32) {
+      int idx = base + lane;
+      bool nl = false;
+      double vps[MAXLCH], r = 0;
+      int c = 0;
+      if (idx < N * C) {
+        int e = idx / C;
+        c = idx - e * C;
+        const double *cc = s.cent + 3 * c, *xe = xs + 3 * e;
+        r = sqrt((xe[0] - cc[0]) * (xe[0] - cc[0]) + (xe[1] - cc[1]) * (xe[1] - cc[1]) +
+                 (xe[2] - cc[2]) * (xe[2] - cc[2]));
+        int it = s.ctype[c];
+        ecp_vps(E, it, r, vps);
+        vloc += vps[E.lpotp1[it] - 1];
+        for (int l = 0; l < E.npotd[it]; l++)
+          if (l + 1 != E.lpotp1[it] && fabs(vps[l]) > 1e-4) nl = true;
+      }
+      unsigned m = __ballot_sync(0xffffffffu, nl);
+      if (nl) {
+        int pos = ntask + __popc(m & ((1u << lane) - 1u));
+        double *rec = tl + (size_t)pos * NLT;
+        rec[0] = (double)idx;
+        rec[1] = r;
+        for (int l = 0; l < MAXLCH; l++) rec[2 + l] = (l < E.npotd[s.ctype[c]]) ? vps[l] : 0.0;
+      }
+      ntask += __popc(m);
+    }
+    vloc = warp_sum(vloc);
+    __syncwarp();
+    const int nq = E.nquad;
+    for (int t = lane; t < ntask * nq; t += 32) {
+      int task = t / nq, q = t - task * nq;
+      const double *rec = tl + (size_t)task * NLT;
+      int idx = (int)rec[0], e = idx / C, c = idx - (idx / C) * C;
+      double r = rec[1];
+      const double *cc = s.cent + 3 * c, *xe = xs + 3 * e;
+      double qv[3];
+#pragma unroll
+      for (int k = 0; k < 3; k++) qv[k] = R[3 * k] * E.q0[q][0] + R[3 * k + 1] * E.q0[q][1] + R[3 * k + 2] * E.q0[q][2];
+      double costh = ((xe[0] - cc[0]) * qv[0] + (xe[1] - cc[1]) * qv[1] + (xe[2] - cc[2]) * qv[2]) / r;
+      double xn[3] = {cc[0] + r * qv[0], cc[1] + r * qv[1], cc[2] + r * qv[2]};
+      // determinant ratio: orbitals at the point contracted with G
+      const T *ge = gp + (size_t)e * B;
+      T dr = 0;
+      for (int ish = 0; ish < s.nshell; ish++) dr += shell_dot<T>(s, ish, xn, ge);
+      // Jastrow ratio (nonlocj, nonloc.f90:432-522)
+      double dj = 0;
+      for (int j = 0; j < N; j++) {
+        if (j == e) continue;
+        int isb, ipar;
+        T ss;
+        pair_class(J, s.nup, e, j, isb, ss, ipar);
+        const double *xj = xs + 3 * j;
+        T a0 = T(xn[0] - xj[0]), a1 = T(xn[1] - xj[1]), a2 = T(xn[2] - xj[2]);
+        T rij = tsqrt(a0 * a0 + a1 * a1 + a2 * a2);
+        T du = T(1) / (T(1) + sk * rij);
+        T fu, fuu;
+        T f = jas_ee<T, false>(J, isb, ss, ipar, rij, du, fu, fuu);
+        if (NORD > 1) {
+          const T *rj_ = v.ren + 2 * C * j;
+          for (int c2 = 0; c2 < C; c2++) {
+            T ri, di;
+            cen_dist(s, sk, xn, c2, ri, di);
+            Een<T> o;
+            jas_een<T, NORD, 0>(J, s.ctype[c2], rij, du, ri, di, rj_[2 * c2], rj_[2 * c2 + 1], o);
+            f += o.fc;
+          }
+        }
+        dj += (double)f - (double)fso[e * N + j];
+      }
+      {
+        T f = 0;
+        for (int c2 = 0; c2 < C; c2++) {
+          T ri, di, fi, fii;
+          cen_dist(s, sk, xn, c2, ri, di);
+          f += jas_en<T, false>(J, s.ctype[c2], ri, di, fi, fii);
+        }
+        dj += (double)f - (double)fso[e * N + e];
+      }
+      int it = s.ctype[c];
+      double vp = 0;
+      for (int l = 0; l < E.npotd[it]; l++)
+        if (l + 1 != E.lpotp1[it]) vp += rec[2 + l] * yl0(l, costh);
+      vnl += E.wq[q] * exp(dj) * vp * (double)dr;
+    }
+    vnl = warp_sum(vnl);
+  }
+  double pe = s.pecent + pe_ee + (s.nloc > 0 ? vloc + vnl : pe_en);
+  double d2lnpsi = d2lnd + d2j;
+  double eloc = pe - HB * (d2lnpsi + v2);
+  if (!ok) eloc = nan("");
+  res.lnpsi = lnd + fsum;
+  res.sign = ok ? sgn : 0.0;
+  res.psij = fsum;
+  res.d2lnpsi = d2lnpsi;
+  res.pe = pe;
+  res.pe_ee = pe_ee;
+  res.pe_nl = vnl;
+  res.eloc = eloc;
+  res.singular = !ok;
+  if (lane == 0) {
+    st.fsum[w] = fsum;
+    st.lnd[w] = ok ? lnd : -INFINITY;
+    st.sgn[w] = ok ? sgn : 0.0;
+    uint32_t flag = 0;
+    if (!ok) flag |= CHAMP_WS_SINGULAR;
+    if (!isfinite(eloc) || !isfinite(lnd + fsum)) flag |= CHAMP_WS_NONFINITE;
+    st.status[w] = flag;
+    if (outputs) {
+      st.o_lnpsi[w] = res.lnpsi;
+      st.o_sign[w] = res.sign;
+      st.o_psij[w] = fsum;
+      st.o_d2[w] = d2lnpsi;
+      st.o_pe[w] = pe;
+      st.o_peee[w] = pe_ee;
+      st.o_penl[w] = vnl;
+      st.o_eloc[w] = eloc;
+    }
+  }
+  __syncwarp();
+}
+
+// ---------------------------------------------------------------------------------------
+// single-electron proposal (hpsie, qmc/vmc/hpsie.f90) and acceptance (jassav/detsav)
+// ---------------------------------------------------------------------------------------
+template <class T, int NORD, bool MD, bool GRAD>
+__device__ void propose(const Sys<T> &s, const JasPar<T> &J, const State<T> &st, int w, const View<T> &v, int e,
+                        const double *xn, int lane, double &rho, double &dj, double *grad) {
+  const int N = s.N, C = s.C, nomax = s.nomax;
+  int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
+  const double *A = gam_ptr<T, MD>(s, v, sp);
+  const int no = s.nocc[sp];
+  constexpr int NCH = GRAD ? 5 : 1;
+  for (int c = lane; c < C; c += 32) {
+    T r, d;
+    cen_dist(s, J.scalek, xn, c, r, d);
+    v.rnew[2 * c] = r;
+    v.rnew[2 * c + 1] = d;
+  }
+  warp_basis<T, NCH>(s, xn, v.phi, lane);
+  warp_orbitals<T, NCH>(v.phi, s.cocc[sp], s.nbasis, no, v.arow, nomax, lane);
+  // the wave function is linear in the moved electron's orbital row: ratio = sum_m G[m][e] phi_m
+  double r0 = 0, g0 = 0, g1 = 0, g2 = 0;
+  for (int k = lane; k < no; k += 32) {
+    double a = A[k * n + eo];
+    r0 += a * (double)v.arow[k];
+    if (GRAD) {
+      g0 += a * (double)v.arow[nomax + k];
+      g1 += a * (double)v.arow[2 * nomax + k];
+      g2 += a * (double)v.arow[3 * nomax + k];
+    }
+  }
+  rho = warp_sum(r0);
+  const T *fso = v.fso;
+  T *pf = v.pf;
+  double d = 0, gj0 = 0, gj1 = 0, gj2 = 0;
+  for (int j = lane; j < N; j += 32) {
+    if (j == e) continue;
+    T g[3];
+    T f = pair_value<T, NORD, GRAD>(s, J, e, j, xn, v.rnew, v.xs + 3 * j, v.ren + 2 * C * j, g);
+    d += (double)f - (double)fso[e * N + j];
+    pf[j] = f;
+    if (GRAD) { gj0 += g[0]; gj1 += g[1]; gj2 += g[2]; }
+  }
+  T fen = 0;
+  for (int c = lane; c < C; c += 32) {
+    T fi = 0, fii = 0;
+    fen += jas_en<T, GRAD>(J, s.ctype[c], v.rnew[2 * c], v.rnew[2 * c + 1], fi, fii);
+    if (GRAD) {
+      const double *cc = s.cent + 3 * c;
+      gj0 += fi * T(xn[0] - cc[0]);
+      gj1 += fi * T(xn[1] - cc[1]);
+      gj2 += fi * T(xn[2] - cc[2]);
+    }
+  }
+  double fent = warp_sum((double)fen);
+  if (lane == 0) {
+    pf[e] = (T)fent;
+    d += fent - (double)fso[e * N + e];
+  }
+  dj = warp_sum(d);
+  if (GRAD) {
+    g0 = warp_sum(g0); g1 = warp_sum(g1); g2 = warp_sum(g2);
+    gj0 = warp_sum(gj0); gj1 = warp_sum(gj1); gj2 = warp_sum(gj2);
+    grad[0] = gj0 + g0 / rho;
+    grad[1] = gj1 + g1 / rho;
+    grad[2] = gj2 + g2 / rho;
+  }
+  __syncwarp();
+}
+
+// Sherman-Morrison update of the inverse and Jastrow tables after accepting electron e
+// at xn (dete_update/detsav, qmc/dete_mod.f90:165-190; jassav.f90).  The proposed orbital
+// row is v.arow (channel 0), the proposed pair values v.pf, distances v.rnew.
+template <class T, bool MD>
+__device__ void accept_move(const Sys<T> &s, const State<T> &st, int w, const View<T> &v, int e, const double *xn,
+                            double dj, double rho, int lane) {
+  const int N = s.N, C = s.C;
+  int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
+  double *A = v.ainv + (sp ? s.nup * s.nup : 0);
+  for (int k = lane; k < n; k += 32) v.colb[k] = A[k * n + eo];
+  for (int j = lane; j < n; j += 32) {
+    double a = 0;
+    for (int k = 0; k < n; k++) a += (double)v.arow[k] * A[k * n + j];
+    v.vb[j] = a - (j == eo ? 1.0 : 0.0);
+  }
+  __syncwarp();
+  double rinv = 1.0 / (v.vb[eo] + 1.0);
+  if (MD) {
+    // T update: T += Ainv[:,e] (atilde'_virt - a'^T T) / rho_ref (dete_update, dete_mod.f90:186-190)
+    const int nv = s.nvirt[sp];
+    double *Tv = v.tv + (sp ? s.nup * s.nvirt[0] : 0);
+    double *wb = v.ymd;  // scratch
+    for (int p = lane; p < nv; p += 32) {
+      double a = (double)v.arow[n + p];
+      for (int k = 0; k < n; k++) a -= (double)v.arow[k] * Tv[k * nv + p];
+      wb[p] = a;
+    }
+    __syncwarp();
+    for (int i = lane; i < n * nv; i += 32) {
+      int k = i / nv, p = i - k * nv;
+      Tv[i] += v.colb[k] * wb[p] * rinv;
+    }
+    __syncwarp();
+  }
+  for (int idx = lane; idx < n * n; idx += 32) {
+    int k = idx / n, j = idx - k * n;
+    A[idx] -= v.colb[k] * v.vb[j] * rinv;
+  }
+  if (MD) {
+    __syncwarp();
+    double lc, sc;
+    build_gamma(s, v, lane, lc, sc);
+  }
+  T *fso = v.fso;
+  for (int j = lane; j < N; j += 32) {
+    T f = v.pf[j];
+    fso[e * N + j] = f;
+    fso[j * N + e] = f;
+  }
+  for (int i = lane; i < 2 * C; i += 32) v.ren[2 * C * e + i] = v.rnew[i];
+  if (lane < 3) v.xs[3 * e + lane] = xn[lane];
+  if (lane == 0) {
+    st.fsum[w] += dj;
+    st.lnd[w] += log(fabs(rho));
+    if (rho < 0) st.sgn[w] = -st.sgn[w];
+  }
+  __syncwarp();
+}
+
+// ---------------------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------------------
+template <class T>
+__device__ inline void load_params(const Sys<T> &s, JasPar<T> &J, EcpPar &E) {
+  const int *src = (const int *)s.jas;
+  int *dst = (int *)&J;
+  for (int i = threadIdx.x; i < (int)(sizeof(JasPar<T>) / 4); i += blockDim.x) dst[i] = src[i];
+  src = (const int *)s.ecp;
+  dst = (int *)&E;
+  for (int i = threadIdx.x; i < (int)(sizeof(EcpPar) / 4); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+}
+
+template <class T, int NORD, bool MD>
+__global__ void __launch_bounds__(128, 4) k_eval(Sys<T> s, State<T> st, Layout L, double r0, double r1, double r2,
+                                                 double r3, double r4, double r5, double r6, double r7, double r8,
+                                                 int outputs) {
+  __shared__ JasPar<T> J;
+  __shared__ EcpPar E;
+  extern __shared__ __align__(16) char dsm[];
+  load_params(s, J, E);
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  const double R[9] = {r0, r1, r2, r3, r4, r5, r6, r7, r8};
+  for (int w = blockIdx.x * wpb + wib; w < st.W; w += gridDim.x * wpb) {
+    View<T> v = make_view<T>(dsm + L.bytes * wib, L, st, w, s.N, s.C, s.nbasis, s.nomax, L.resident != 0);
+    for (int i = lane; i < 3 * s.N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * s.N + i];
+    __syncwarp();
+    EvalRes res;
+    full_eval<T, NORD, MD>(s, J, E, st, w, v, R, lane, outputs != 0, res);
+    if (L.resident) view_store(v, st, w, s.N, s.C, lane);
+  }
+}
+
+// The per-call proposal/accept kernels always work on the HBM copy of the state.
+template <class T, int NORD, bool MD>
+__global__ void __launch_bounds__(128, 4) k_propose(Sys<T> s, State<T> st, Layout L, int e, const double *xnew,
+                                                    double *ratio, double *grad) {
+  __shared__ JasPar<T> J;
+  __shared__ EcpPar E;
+  extern __shared__ __align__(16) char dsm[];
+  load_params(s, J, E);
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  const int nomax = s.nomax;
+  for (int w = blockIdx.x * wpb + wib; w < st.W; w += gridDim.x * wpb) {
+    View<T> v = make_view<T>(dsm + L.bytes * wib, L, st, w, s.N, s.C, s.nbasis, s.nomax, false);
+    for (int i = lane; i < 3 * s.N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * s.N + i];
+    __syncwarp();
+    double xn[3] = {xnew[3 * w], xnew[3 * w + 1], xnew[3 * w + 2]};
+    double rho, dj, g[3];
+    if (grad)
+      propose<T, NORD, MD, true>(s, J, st, w, v, e, xn, lane, rho, dj, g);
+    else
+      propose<T, NORD, MD, false>(s, J, st, w, v, e, xn, lane, rho, dj, g);
+    int sp = e < s.nup ? 0 : 1;
+    for (int k = lane; k < s.nocc[sp]; k += 32) st.pa[(size_t)w * nomax + k] = (double)v.arow[k];
+    if (lane == 0) {
+      st.pdj[w] = dj;
+      st.prho[w] = rho;
+      st.piel[w] = e;
+      st.pxn[3 * w] = xn[0]; st.pxn[3 * w + 1] = xn[1]; st.pxn[3 * w + 2] = xn[2];
+      ratio[w] = rho * exp(dj);
+      if (grad) { grad[3 * w] = g[0]; grad[3 * w + 1] = g[1]; grad[3 * w + 2] = g[2]; }
+    }
+    __syncwarp();
+  }
+}
+
+template <class T, bool MD>
+__global__ void __launch_bounds__(128, 4) k_accept(Sys<T> s, State<T> st, Layout L, int e, const uint8_t *mask) {
+  extern __shared__ __align__(16) char dsm[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  const int nomax = s.nomax, C = s.C;
+  for (int w = blockIdx.x * wpb + wib; w < st.W; w += gridDim.x * wpb) {
+    if (!mask[w] || st.piel[w] != e) continue;
+    View<T> v = make_view<T>(dsm + L.bytes * wib, L, st, w, s.N, s.C, s.nbasis, s.nomax, false);
+    int sp = e < s.nup ? 0 : 1;
+    for (int k = lane; k < s.nocc[sp]; k += 32) v.arow[k] = (T)st.pa[(size_t)w * nomax + k];
+    for (int i = lane; i < 3 * s.N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * s.N + i];
+    double xn[3] = {st.pxn[3 * w], st.pxn[3 * w + 1], st.pxn[3 * w + 2]};
+    for (int c = lane; c < C; c += 32) {
+      T r, d;
+      const double *cc = s.cent + 3 * c;
+      T a = T(xn[0] - cc[0]), b = T(xn[1] - cc[1]), z = T(xn[2] - cc[2]);
+      r = tsqrt(a * a + b * b + z * z);
+      d = T(1) / (T(1) + (T)s.scalek * r);
+      v.rnew[2 * c] = r;
+      v.rnew[2 * c + 1] = d;
+    }
+    __syncwarp();
+    accept_move<T, MD>(s, st, w, v, e, xn, st.pdj[w], st.prho[w], lane);
+    if (lane < 3) st.x[(size_t)w * 3 * s.N + 3 * e + lane] = xn[lane];
+    if (lane == 0) st.piel[w] = -1;
+    __syncwarp();
+  }
+}
+
+// Fused VMC: nsweep sweeps of single-electron Metropolis moves plus E_L after each sweep.
+template <class T, int NORD, bool MD>
+__global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L, int nsweep, uint64_t seed,
+                                                uint64_t sweep0, double step) {
+  __shared__ JasPar<T> J;
+  __shared__ EcpPar E;
+  extern __shared__ __align__(16) char dsm[];
+  load_params(s, J, E);
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  const int N = s.N;
+  for (int w = blockIdx.x * wpb + wib; w < st.W; w += gridDim.x * wpb) {
+    View<T> v = make_view<T>(dsm + L.bytes * wib, L, st, w, s.N, s.C, s.nbasis, s.nomax, L.resident != 0);
+    if (L.resident) {
+      view_load(v, st, w, N, s.C, lane);
+    } else {
+      for (int i = lane; i < 3 * N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * N + i];
+      __syncwarp();
+    }
+    double es = 0, e2 = 0, acc = 0, el = 0;
+    for (int isw = 0; isw < nsweep; isw++) {
+      uint64_t sweep = sweep0 + (uint64_t)isw;
+      for (int e = 0; e < N; e++) {
+        double g[3], ua;
+        move_randoms(seed, (uint32_t)w, sweep, (uint32_t)e, g, &ua);
+        double xn[3] = {v.xs[3 * e] + step * g[0], v.xs[3 * e + 1] + step * g[1], v.xs[3 * e + 2] + step * g[2]};
+        double rho, dj, gr[3];
+        propose<T, NORD, MD, false>(s, J, st, w, v, e, xn, lane, rho, dj, gr);
+        double p = rho * rho * exp(2.0 * dj);
+        if (ua < p) {
+          accept_move<T, MD>(s, st, w, v, e, xn, dj, rho, lane);
+          acc += 1;
+        }
+      }
+      double R[9];
+      random_rotation(seed, (uint32_t)w, sweep, R);
+      EvalRes res;
+      full_eval<T, NORD, MD>(s, J, E, st, w, v, R, lane, false, res);
+      el = res.eloc;
+      es += el;
+      e2 += el * el;
+    }
+    if (L.resident) {
+      view_store(v, st, w, N, s.C, lane);
+    } else {
+      for (int i = lane; i < 3 * N; i += 32) st.x[(size_t)w * 3 * N + i] = v.xs[i];
+    }
+    if (lane == 0) {
+      st.s_esum[w] = es;
+      st.s_e2sum[w] = e2;
+      st.s_acc[w] = acc;
+      st.s_elast[w] = el;
+    }
+    __syncwarp();
+  }
+}
+

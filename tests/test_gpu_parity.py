@@ -33,14 +33,18 @@ def oracle_eval_all(o, x, rot=None):
     return [o.eval(xi) for xi in x]
 
 
-SYSTEMS = [(1, 64), (2, 64), (5, 4)]
+def get(k):
+    return S.be_example() if k == "be" else S.get_system(k)
+
+
+SYSTEMS = [(1, 64), (2, 64), (3, 32), ("be", 64), (5, 4)]
 
 
 @pytest.mark.parametrize("k,nw", SYSTEMS)
 def test_eval_full_fp64_matches_oracle(oracle_mod, k, nw):
-    s = S.get_system(k)
+    s = get(k)
     o = oracle_mod.Oracle(s)
-    x = S.initial_walkers(s, nw, seed=100 + k)
+    x = S.initial_walkers(s, nw, seed=100 + (4 if k == "be" else k))
     rot = oracle_mod.random_rotation(7, 0, 3)
     eng = make_engine(s, nw, "fp64")
     eng.set_walkers(x)
@@ -60,11 +64,11 @@ def test_eval_full_fp64_matches_oracle(oracle_mod, k, nw):
         assert abs(g["energy"][w] - r["energy"]) <= 1e-8 * sc
 
 
-@pytest.mark.parametrize("k,nw", [(1, 64), (2, 64)])
+@pytest.mark.parametrize("k,nw", [(1, 64), (2, 64), (3, 32), ("be", 64)])
 def test_eval_full_mixed_matches_oracle(oracle_mod, k, nw):
-    s = S.get_system(k)
+    s = get(k)
     o = oracle_mod.Oracle(s)
-    x = S.initial_walkers(s, nw, seed=200 + k)
+    x = S.initial_walkers(s, nw, seed=200 + (4 if k == "be" else k))
     eng = make_engine(s, nw, "mixed")
     eng.set_walkers(x)
     g = eng.eval_full()
@@ -75,13 +79,13 @@ def test_eval_full_mixed_matches_oracle(oracle_mod, k, nw):
         assert abs(g["energy"][w] - r["energy"]) <= 2e-3 * max(1.0, abs(r["d2lnpsi"]))
 
 
-@pytest.mark.parametrize("k,prec", [(1, "fp64"), (2, "fp64"), (2, "mixed")])
+@pytest.mark.parametrize("k,prec", [(1, "fp64"), (2, "fp64"), (2, "mixed"), (3, "fp64"), ("be", "fp64"), ("be", "mixed")])
 def test_propose_accept_sequence_matches_oracle(oracle_mod, k, prec):
-    """hpsie ratios and gradients, then jassav/detsav updates, for a sequence of moves."""
-    s = S.get_system(k)
+    """hpsie ratios and gradients, then jassav/detsav/dete_save updates, for a sequence of moves."""
+    s = get(k)
     o = oracle_mod.Oracle(s)
     nw = 32
-    x = S.initial_walkers(s, nw, seed=300 + k)
+    x = S.initial_walkers(s, nw, seed=300 + (4 if k == "be" else k))
     eng = make_engine(s, nw, prec)
     eng.set_walkers(x)
     rng = np.random.default_rng(5)
@@ -143,3 +147,26 @@ def test_walker_status_clean(oracle_mod):
     eng = make_engine(s, 16, "fp64")
     eng.set_walkers(S.initial_walkers(s, 16, seed=1))
     assert not eng.walker_status().any()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_vmc_be_example_matches_reference_transcript(prec):
+    """Statistical pin of the GPU path: VMC of the reference's Be example (4 determinants,
+    examples/be_vb1_jcas24_vmc_j_opt_lin.out: E = -14.6463051 +- 0.0075680, sigma = 0.579)."""
+    import json
+    import os
+    fx = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "be_vb1.json")))
+    ref = fx["reference"]
+    s = S.be_example()
+    nw = 4096
+    eng = make_engine(s, nw, prec)
+    eng.set_walkers(S.initial_walkers(s, nw, seed=17))
+    eng.vmc_sweeps(100, seed=99, sweep0=0, step=0.5, stats=False)
+    ns = 200
+    st = eng.vmc_sweeps(ns, seed=99, sweep0=100, step=0.5)
+    e_w = st["esum"] / ns
+    e, err = e_w.mean(), e_w.std(ddof=1) / np.sqrt(nw)
+    sigma = np.sqrt(st["e2sum"].sum() / (nw * ns) - (st["esum"].sum() / (nw * ns)) ** 2)
+    assert abs(e - ref["energy"]) < 3.5 * np.hypot(err, ref["energy_err"]), (e, err)
+    # the all-electron E_L has heavy tails near the nucleus; sigma's sampling error is large
+    assert abs(sigma - ref["sigma"]) < 0.05, sigma
