@@ -42,7 +42,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
     with ThreadPoolExecutor(len(UNITS)) as ex:
         objs = list(ex.map(compile_unit, UNITS))
-    subprocess.check_call([NVCC] + ARCH + ["-shared", "-o", LIB] + objs)
+    subprocess.check_call([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcublas"])
     return LIB
 
 

@@ -50,6 +50,17 @@ struct champ_ctx {
   double *d_in = nullptr, *d_out = nullptr;
   uint8_t *d_mask = nullptr;
   int nparm_jas = 0;
+  // parameter derivatives and O/H accumulation
+  int np_raw = 0;          // raw Jastrow parameters on the device (a, b, all c terms)
+  int ncfree = 0;          // free e-e-n coefficients per centre type
+  std::vector<double> cproj;
+  int nfree = 0;           // free parameters reported
+  size_t smem_pg = 0;      // dynamic shared memory of the derivative kernel
+  int wpb_pg = 4;
+  double *pg_dl = nullptr, *pg_de = nullptr, *pg_el = nullptr, *pg_wt = nullptr;
+  double *oh_oa = nullptr, *oh_ow = nullptr, *oh_mb = nullptr, *oh_s = nullptr, *oh_h = nullptr;
+  bool have_pgrad = false;
+  void *cublas = nullptr;
 };
 
 template <class T>
@@ -67,7 +78,7 @@ inline State<float> &stof<float>(champ_ctx *c) { return c->stf; }
 
 inline int nblocks(champ_ctx *c) { return (c->W + c->wpb - 1) / c->wpb; }
 
-enum class Op { Eval, EvalOut, Propose, ProposeGrad, Accept, Vmc };
+enum class Op { Eval, EvalOut, Propose, ProposeGrad, Accept, Vmc, PGrad };
 struct OpArgs {
   int e = 0;
   const double *xnew = nullptr;
@@ -76,6 +87,7 @@ struct OpArgs {
   int nsweep = 0;
   uint64_t seed = 0, sweep0 = 0;
   double step = 0;
+  PGOut pgout;
 };
 
 

@@ -67,6 +67,10 @@ struct Sys {
   const double *dsg[2];   // [ndu_s] sign of det(T[:, L]) / det(alpha)
   const int *ciu, *cid;   // [ndet] unique up / down determinant of each determinant
   const double *ccoef;    // [ndet] determinant coefficient (csf coefficients folded in)
+  // free e-e-n coefficients: d c_ll / d c_free (cusp dependences, checkdepend4 in
+  // qmc/fit/cuspinit4.f90) as a [nterms][ncfree] matrix
+  int ncfree;
+  const double *cproj;
   const JasPar<T> *jas;
   const EcpPar *ecp;
 };

@@ -18,6 +18,8 @@
 #include <vector>
 
 #include "../../include/champ_b200.h"
+#include <cublas_v2.h>
+
 #include "ctx.h"
 
 using namespace champ;
@@ -159,7 +161,7 @@ static double host_anorm(int kind, int n, int l, double z) {
 }
 
 // cuspinit4 + cuspexact4 (qmc/fit/cuspinit4.f90:1-60, qmc/fit/cuspexact4.f90:14-40)
-static void host_een_cusp(int nordc, int nct, int nt, std::vector<double> &c) {
+static void host_een_cusp(int nordc, int nct, int nt, std::vector<double> &c, std::vector<int> *dependents = nullptr) {
   if (nordc <= 1) return;
   int neq = 2 * (nordc - 1);
   std::vector<double> d((size_t)neq * nt, 0.0);
@@ -180,6 +182,10 @@ static void host_een_cusp(int nordc, int nct, int nt, std::vector<double> &c) {
         if (m > 0) { iord = nordc - 1 + k + l + m; d[(size_t)(iord - 1) * nt + i - 1] -= m; }
       }
     }
+  if (dependents) {
+    dependents->clear();
+    for (int e = 0; e < neq; e++) dependents->push_back(iwc[e] - 1);
+  }
   std::vector<int> order;
   for (int e = 1; e <= nordc - 1; e++) order.push_back(e);
   for (int e = nordc + 1; e <= neq; e++) order.push_back(e);
@@ -284,6 +290,13 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
     CK(cudaMemcpy(cid, md.cid.data(), sizeof(int) * md.ndet, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(cc, md.ccoef.data(), sizeof(double) * md.ndet, cudaMemcpyHostToDevice));
     s.ciu = ciu; s.cid = cid; s.ccoef = cc;
+  }
+  {
+    s.ncfree = c->ncfree;
+    double *cp = dalloc<double>(c, std::max<size_t>(1, c->cproj.size()));
+    if (!cp) return fail(CHAMP_ENOMEM, "device allocation failed");
+    if (!c->cproj.empty()) CK(cudaMemcpy(cp, c->cproj.data(), sizeof(double) * c->cproj.size(), cudaMemcpyHostToDevice));
+    s.cproj = cp;
   }
   JasPar<T> J;
   memset(&J, 0, sizeof J);
@@ -433,6 +446,30 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
   std::vector<double> cfull((size_t)d->nctype * std::max(nt, 1), 0.0);
   if (nt) memcpy(cfull.data(), d->c, sizeof(double) * d->nctype * nt);
   if (d->een_cusp) host_een_cusp(d->nordc, d->nctype, nt, cfull);
+  // free e-e-n coefficients and d c / d c_free (the cusp map is linear, so unit vectors give
+  // its columns exactly)
+  {
+    std::vector<int> dep;
+    if (d->een_cusp && nt > 0) {
+      std::vector<double> z(nt, 0.0);
+      host_een_cusp(d->nordc, 1, nt, z, &dep);
+    }
+    std::vector<int> fr;
+    for (int ll = 0; ll < nt; ll++)
+      if (std::find(dep.begin(), dep.end(), ll) == dep.end()) fr.push_back(ll);
+    c->ncfree = (d->nordc > 1) ? (int)fr.size() : 0;
+    c->cproj.assign((size_t)std::max(nt, 1) * std::max(c->ncfree, 1), 0.0);
+    for (int f = 0; f < c->ncfree; f++) {
+      std::vector<double> u(nt, 0.0);
+      u[fr[f]] = 1.0;
+      if (d->een_cusp) host_een_cusp(d->nordc, 1, nt, u);
+      for (int ll = 0; ll < nt; ll++) c->cproj[(size_t)ll * c->ncfree + f] = u[ll];
+    }
+    int na = d->nctype * std::max(0, d->norda - 1), nb = d->nspin2b * d->nordb;
+    c->np_raw = na + nb + (d->nordc > 1 ? d->nctype * nt : 0);
+    c->nfree = na + nb + d->nctype * c->ncfree;
+    c->nparm_jas = c->nfree;
+  }
   if (nt == 0) cfull.assign(d->nctype, 0.0);
   // asymptotic values for isc=4 (set_scale_dist, scale_dist.f90:147-225)
   double ar = 1.0 / d->scalek, asa[MAXCT] = {0}, asb[2] = {0, 0};
@@ -514,12 +551,37 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
   while (c->wpb > 1 && c->smem * c->wpb > 96 * 1024) c->wpb >>= 1;
   if (c->smem * c->wpb > 200 * 1024) { champ_destroy(c); return fail(CHAMP_EINVAL, "system too large for the per-warp shared memory"); }
   c->smem *= c->wpb;
+  {
+    // the derivative kernel adds its accumulators to the always-shared part of the layout
+    size_t pgb = c->lay.base + align16(sizeof(double) * (4 * (size_t)c->N + 3 * (size_t)c->np_raw +
+                                                         (size_t)c->N * c->np_raw));
+    c->wpb_pg = 4;
+    while (c->wpb_pg > 1 && pgb * c->wpb_pg > 160 * 1024) c->wpb_pg >>= 1;
+    c->smem_pg = pgb * c->wpb_pg;
+    if (c->smem_pg > 220 * 1024) c->smem_pg = 0;  // parameter derivatives unavailable for this size
+  }
   rc = c->prec == CHAMP_PREC_FP64 ? attrs_f64(c) : attrs_f32(c);
   if (rc) { champ_destroy(c); return rc; }
   c->d_in = dalloc<double>(c, (size_t)w_max * 3 * c->N);
   c->d_out = dalloc<double>(c, (size_t)w_max * 4 * c->N);
   c->d_mask = dalloc<uint8_t>(c, w_max);
   if (!c->d_in || !c->d_out || !c->d_mask) { champ_destroy(c); return fail(CHAMP_ENOMEM, "staging allocation failed"); }
+  {
+    size_t W = w_max, P = c->nfree, P1 = P + 1;
+    c->pg_dl = dalloc<double>(c, W * std::max<size_t>(P, 1));
+    c->pg_de = dalloc<double>(c, W * std::max<size_t>(P, 1));
+    c->pg_el = dalloc<double>(c, W);
+    c->pg_wt = dalloc<double>(c, W);
+    c->oh_oa = dalloc<double>(c, W * P1);
+    c->oh_ow = dalloc<double>(c, W * P1);
+    c->oh_mb = dalloc<double>(c, W * P1);
+    c->oh_s = dalloc<double>(c, P1 * P1);
+    c->oh_h = dalloc<double>(c, P1 * P1);
+    if (!c->pg_dl || !c->pg_de || !c->pg_el || !c->pg_wt || !c->oh_oa || !c->oh_ow || !c->oh_mb || !c->oh_s || !c->oh_h) {
+      champ_destroy(c);
+      return fail(CHAMP_ENOMEM, "allocation of the parameter-derivative buffers failed");
+    }
+  }
   *out = c;
   return CHAMP_OK;
 }
@@ -529,7 +591,56 @@ int champ_destroy(champ_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   else cudaDeviceSynchronize();
   for (void *p : c->allocs) cudaFree(p);
+  if (c->cublas) cublasDestroy((cublasHandle_t)c->cublas);
   delete c;
+  return CHAMP_OK;
+}
+
+int champ_param_grad(champ_ctx *c, double *dlnpsi, double *deloc, double *eloc) {
+  if (!c) return fail(CHAMP_EINVAL, "null context");
+  if (!c->have_walkers) return fail(CHAMP_ESTATE, "no walkers set");
+  if (c->smem_pg == 0) return fail(CHAMP_EINVAL, "parameter derivatives: system too large for the kernel's shared memory");
+  OpArgs a;
+  a.pgout.dlnpsi = c->pg_dl;
+  a.pgout.deloc = c->pg_de;
+  a.pgout.eloc = c->pg_el;
+  a.pgout.nfree = c->nfree;
+  int rc = launch(c, Op::PGrad, a);
+  if (rc) return rc;
+  size_t W = c->W, P = c->nfree;
+  if (dlnpsi) CK(cudaMemcpyAsync(dlnpsi, c->pg_dl, sizeof(double) * W * P, cudaMemcpyDeviceToHost, c->stream));
+  if (deloc) CK(cudaMemcpyAsync(deloc, c->pg_de, sizeof(double) * W * P, cudaMemcpyDeviceToHost, c->stream));
+  if (eloc) CK(cudaMemcpyAsync(eloc, c->pg_el, sizeof(double) * W, cudaMemcpyDeviceToHost, c->stream));
+  if (dlnpsi || deloc || eloc) CK(cudaStreamSynchronize(c->stream));
+  c->have_pgrad = true;
+  return CHAMP_OK;
+}
+
+int champ_accumulate_oh(champ_ctx *c, const double *weights, double *S, double *H) {
+  if (!c) return fail(CHAMP_EINVAL, "null context");
+  if (!c->have_pgrad) return fail(CHAMP_ESTATE, "call champ_param_grad first");
+  const int W = c->W, P = c->nfree, P1 = P + 1;
+  if (!c->cublas) {
+    cublasHandle_t h;
+    if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) return fail(CHAMP_ECUDA, "cublasCreate failed");
+    c->cublas = h;
+  }
+  cublasHandle_t h = (cublasHandle_t)c->cublas;
+  if (cublasSetStream(h, c->stream) != CUBLAS_STATUS_SUCCESS) return fail(CHAMP_ECUDA, "cublasSetStream failed");
+  if (weights) CK(cudaMemcpyAsync(c->pg_wt, weights, sizeof(double) * W, cudaMemcpyHostToDevice, c->stream));
+  k_pack_oh<<<592, 256, 0, c->stream>>>(W, P, c->pg_dl, c->pg_de, c->pg_el, weights ? c->pg_wt : nullptr, c->oh_oa,
+                                        c->oh_ow, c->oh_mb);
+  CK(cudaGetLastError());
+  // S[a][b] = sum_w wt (1,O)_a (1,O)_b ;  H[a][b] = sum_w wt (1,O)_a (E_L, E_L O + dE)_b  (row-major)
+  const double one = 1.0, zero = 0.0;
+  if (cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, P1, P1, W, &one, c->oh_ow, P1, c->oh_oa, P1, &zero, c->oh_s, P1) !=
+          CUBLAS_STATUS_SUCCESS ||
+      cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, P1, P1, W, &one, c->oh_mb, P1, c->oh_oa, P1, &zero, c->oh_h, P1) !=
+          CUBLAS_STATUS_SUCCESS)
+    return fail(CHAMP_ECUDA, "cublasDgemm failed");
+  if (S) CK(cudaMemcpyAsync(S, c->oh_s, sizeof(double) * P1 * P1, cudaMemcpyDeviceToHost, c->stream));
+  if (H) CK(cudaMemcpyAsync(H, c->oh_h, sizeof(double) * P1 * P1, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return CHAMP_OK;
 }
 

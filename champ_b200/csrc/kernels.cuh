@@ -60,7 +60,7 @@ constexpr int NLT = 2 + MAXLCH;  // task record: (e*C+c), r, vps[0..MAXLCH-1]
 struct Layout {
   size_t phi, arow, xs, vacc, divj, colb, vb, perm, rnew;  // always in shared memory
   size_t ainv, fso, ren, pf, orb5, gproj, nlt, tv, gam, ymd, wdet;  // resident mode only
-  size_t bytes;
+  size_t bytes, base;  // total bytes per warp; bytes of the always-shared part
   int resident;
 };
 
@@ -105,6 +105,7 @@ static Layout make_layout(int N, int C, int nbasis, int nmax, int nomax, int ast
   L.gam = take(sizeof(double) * gstride);
   L.ymd = take(sizeof(double) * tvstride);
   L.wdet = take(sizeof(double) * wstride);
+  L.base = base;
   L.resident = (o <= resident_limit) ? 1 : 0;
   L.bytes = L.resident ? o : base;
   return L;
@@ -434,9 +435,27 @@ struct EvalRes {
   bool singular;
 };
 
-template <class T, int NORD, bool MD>
+// Shared-memory accumulators of the Jastrow parameter derivatives of one walker.
+// Raw parameters: a_k (k = 3..norda+1) per centre type, b_k (k = 2..nordb+1) per b set,
+// all e-e-n c terms per centre type.
+struct PGBuf {
+  double *vt;    // [N*3] grad ln psi
+  double *csum;  // [N] sum over the electron's quadrature points of w e^dJ v_l(r) P_l D-ratio
+  double *dvn;   // [P] sum over points of that coefficient times the parameter's basis function
+  double *G;     // [P] d ln psi / dp
+  double *K;     // [P] sum_e (lap_e g_p + 2 v_e . grad_e g_p)
+  double *old;   // [N][P] basis function of p summed over the terms involving electron e
+  int P, na, nb;
+};
+
+template <class T, int NORD>
+__device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const View<T> &v, int e, const double *xn,
+                                   double coeff, const PGBuf &pg);
+
+template <class T, int NORD, bool MD, bool PG = false>
 __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, const State<T> &st, int w,
-                          const View<T> &v, const double *R, int lane, bool outputs, EvalRes &res) {
+                          const View<T> &v, const double *R, int lane, bool outputs, EvalRes &res,
+                          const PGBuf *pg = nullptr) {
   const int N = s.N, C = s.C, nomax = s.nomax;
   const double *xs = v.xs;
   T *fso = v.fso;
@@ -598,6 +617,9 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
     d2lnd += dvd;
     double vx = v.vacc[3 * e] + g0, vy = v.vacc[3 * e + 1] + g1, vz = v.vacc[3 * e + 2] + g2;
     v2 += vx * vx + vy * vy + vz * vz;
+    if (PG && lane == 0) {
+      pg->vt[3 * e] = vx; pg->vt[3 * e + 1] = vy; pg->vt[3 * e + 2] = vz;
+    }
     if (outputs && lane == 0) {
       double *ov = st.o_vel + ((size_t)w * N + e) * 3;
       ov[0] = vx; ov[1] = vy; ov[2] = vz;
@@ -708,6 +730,11 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
       for (int l = 0; l < E.npotd[it]; l++)
         if (l + 1 != E.lpotp1[it]) vp += rec[2 + l] * yl0(l, costh);
       vnl += E.wq[q] * exp(dj) * vp * (double)dr;
+      if (PG) {
+        double coeff = E.wq[q] * exp(dj) * vp * (double)dr;
+        atomicAdd(&pg->csum[e], coeff);
+        point_param_values<T, NORD>(s, J, v, e, xn, coeff, *pg);
+      }
     }
     vnl = warp_sum(vnl);
   }
@@ -1027,3 +1054,4 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
   }
 }
 
+#include "pgrad.cuh"

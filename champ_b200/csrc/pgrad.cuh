@@ -1,0 +1,302 @@
+// pgrad.cuh -- Jastrow parameter derivatives of ln psi and E_L for every walker.
+//
+// For each Jastrow parameter p the log-derivative g_p = d ln psi / dp is the parameter's
+// basis function summed over all e-e, e-n and e-e-n terms (gvalue of
+// qmc/vmc/deriv_jastrow4.f90), and
+//   dE_L/dp = -1/2 sum_e (lap_e g_p + 2 grad_e ln psi . grad_e g_p) + dV_NL/dp
+// (denergy, qmc/vmc/hpsi.f90:357-376), where dV_NL/dp is the nonlocal quadrature weighted
+// by the change of g_p when the electron moves to each quadrature point
+// (qmc/fit/deriv_nonloc.f90).  The asymptotic constants subtracted from the e-e and e-n
+// terms depend on the parameters too, and their derivatives are included.
+#pragma once
+
+// basis functions of the e-e parameters b2..b_{nordb+1} for one pair: value t, and with
+// DERIV the chain-ruled pieces T1 = t'(r)/r and T2 = t''(r)
+template <class T>
+__device__ __forceinline__ void ee_param_terms(const JasPar<T> &J, int isb, T ss, T rij, T deni, int k, T &t, T &T1,
+                                               T &T2, bool deriv) {
+  const T sk = J.scalek, ar = T(1) / sk;
+  T u = rij * deni;
+  T tu, tuu;
+  if (k == 1) {
+    T b1 = J.b[isb][0], b2 = J.b[isb][1];
+    T bu = T(1) + b2 * u, ba = T(1) + b2 * ar;
+    t = -ss * b1 * (u * u / (bu * bu) - ar * ar / (ba * ba));
+    tu = -ss * b1 * 2 * u / (bu * bu * bu);
+    tuu = -ss * b1 * 2 * (T(1) - 2 * b2 * u) / (bu * bu * bu * bu);
+  } else {
+    T up = ipow(u, k - 2);
+    t = up * u * u - ipow(ar, k);
+    tu = T(k) * up * u;
+    tuu = T(k * (k - 1)) * up;
+  }
+  if (deriv) {
+    T dd1 = deni * deni, dd2 = -2 * sk * deni * dd1;
+    T1 = tu * dd1 / rij;
+    T2 = tuu * dd1 * dd1 + tu * dd2;
+  }
+}
+
+// basis function of the e-n parameter a_{k+1} (k = 2..norda): rr^k - ar^k
+template <class T>
+__device__ __forceinline__ void en_param_terms(const JasPar<T> &J, T r, T deni, int k, T &t, T &T1, T &T2, bool deriv) {
+  const T sk = J.scalek, ar = T(1) / sk;
+  T rr = r * deni;
+  T p = ipow(rr, k - 2);
+  t = p * rr * rr - ipow(ar, k);
+  if (deriv) {
+    T tr = T(k) * p * rr, trr = T(k * (k - 1)) * p;
+    T dd7 = deni * deni, dd9 = -2 * sk * deni * dd7;
+    T1 = tr * dd7 / r;
+    T2 = trr * dd7 * dd7 + tr * dd9;
+  }
+}
+
+// Parameter basis functions with electron e at the quadrature point xn, weighted by coeff
+// and added to pg.dvn.
+template <class T, int NORD>
+__device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const View<T> &v, int e, const double *xn,
+                                   double coeff, const PGBuf &pg) {
+  const int N = s.N, C = s.C;
+  const T sk = J.scalek;
+  constexpr Terms tl = make_terms(NORD);
+  for (int j = 0; j < N; j++) {
+    if (j == e) continue;
+    int isb, ipar;
+    T ss;
+    pair_class(J, s.nup, e, j, isb, ss, ipar);
+    const double *xj = v.xs + 3 * j;
+    T a0 = T(xn[0] - xj[0]), a1 = T(xn[1] - xj[1]), a2 = T(xn[2] - xj[2]);
+    T rij = tsqrt(a0 * a0 + a1 * a1 + a2 * a2);
+    T du = T(1) / (T(1) + sk * rij);
+    for (int k = 1; k <= J.nordb; k++) {
+      T t, t1, t2;
+      ee_param_terms(J, isb, ss, rij, du, k, t, t1, t2, false);
+      atomicAdd(&pg.dvn[pg.na + isb * J.nordb + (k - 1)], coeff * (double)t);
+    }
+    if (NORD > 1) {
+      const T *rj_ = v.ren + 2 * C * j;
+      for (int c = 0; c < C; c++) {
+        T ri, di;
+        cen_dist(s, sk, xn, c, ri, di);
+        T rj1 = rj_[2 * c + 1];
+        T uu[NORD + 1], pi[NORD + 1], pj[NORD + 1];
+        uu[0] = pi[0] = pj[0] = T(1);
+#pragma unroll
+        for (int q = 1; q <= NORD; q++) { uu[q] = uu[q - 1] * du; pi[q] = pi[q - 1] * di; pj[q] = pj[q - 1] * rj1; }
+        double *dst = pg.dvn + pg.na + pg.nb + s.ctype[c] * tl.n;
+#pragma unroll
+        for (int ll = 0; ll < tl.n; ll++) {
+          const int k = tl.k[ll], l = tl.l[ll], m = tl.m[ll];
+          T sl = (l == 0) ? T(2) : pi[l] + pj[l];
+          atomicAdd(&dst[ll], coeff * (double)(uu[k] * sl * pi[m] * pj[m]));
+        }
+      }
+    }
+  }
+  for (int c = 0; c < C; c++) {
+    T r, d;
+    cen_dist(s, sk, xn, c, r, d);
+    int it = s.ctype[c];
+    for (int k = 2; k <= J.norda; k++) {
+      T t, t1, t2;
+      en_param_terms(J, r, d, k, t, t1, t2, false);
+      atomicAdd(&pg.dvn[it * (J.norda - 1) + (k - 2)], coeff * (double)t);
+    }
+  }
+}
+
+// g_p, K_p = sum_e (lap_e g_p + 2 v_e . grad_e g_p) and old[e][p] for all Jastrow
+// parameters (deriv_jastrow4.f90), warp-cooperative; v = pg.vt.
+template <class T, int NORD>
+__device__ void jastrow_param_pass(const Sys<T> &s, const JasPar<T> &J, const View<T> &v, const PGBuf &pg, int lane) {
+  const int N = s.N, C = s.C, P = pg.P;
+  const T sk = J.scalek;
+  constexpr Terms tl = make_terms(NORD);
+  const int npair = N * (N - 1) / 2;
+  for (int p = lane; p < npair; p += 32) {
+    int i = (int)((1.0 + sqrt(1.0 + 8.0 * (double)p)) * 0.5);
+    while (i * (i - 1) / 2 > p) i--;
+    while ((i + 1) * i / 2 <= p) i++;
+    int j = p - i * (i - 1) / 2;
+    const double *xi = v.xs + 3 * i, *xj = v.xs + 3 * j;
+    const double *vi = pg.vt + 3 * i, *vj = pg.vt + 3 * j;
+    int isb, ipar;
+    T ss;
+    pair_class(J, s.nup, i, j, isb, ss, ipar);
+    double rvd[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
+    T rij = tsqrt(T(rvd[0] * rvd[0] + rvd[1] * rvd[1] + rvd[2] * rvd[2]));
+    T du = T(1) / (T(1) + sk * rij);
+    double dv_rv = (vi[0] - vj[0]) * rvd[0] + (vi[1] - vj[1]) * rvd[1] + (vi[2] - vj[2]) * rvd[2];
+    for (int k = 1; k <= J.nordb; k++) {
+      T t, t1, t2;
+      ee_param_terms(J, isb, ss, rij, du, k, t, t1, t2, true);
+      int ip = pg.na + isb * J.nordb + (k - 1);
+      double lap = 2.0 * ((double)t2 + 2.0 * (double)t1);
+      atomicAdd(&pg.G[ip], (double)t);
+      atomicAdd(&pg.K[ip], lap + 2.0 * (double)t1 * dv_rv);
+      atomicAdd(&pg.old[i * P + ip], (double)t);
+      atomicAdd(&pg.old[j * P + ip], (double)t);
+    }
+    if (NORD > 1) {
+      const T *ri_ = v.ren + 2 * C * i, *rj_ = v.ren + 2 * C * j;
+      for (int c = 0; c < C; c++) {
+        const double *cc = s.cent + 3 * c;
+        T ri = ri_[2 * c], di = ri_[2 * c + 1], rj = rj_[2 * c], dj = rj_[2 * c + 1];
+        double vi_ri = vi[0] * (xi[0] - cc[0]) + vi[1] * (xi[1] - cc[1]) + vi[2] * (xi[2] - cc[2]);
+        double vi_rv = vi[0] * rvd[0] + vi[1] * rvd[1] + vi[2] * rvd[2];
+        double vj_rj = vj[0] * (xj[0] - cc[0]) + vj[1] * (xj[1] - cc[1]) + vj[2] * (xj[2] - cc[2]);
+        double vj_rv = vj[0] * rvd[0] + vj[1] * rvd[1] + vj[2] * rvd[2];
+        // power tables with two zero entries below 0, as in jas_een
+        T uu[NORD + 3], rri[NORD + 3], rrj[NORD + 3];
+        uu[0] = uu[1] = rri[0] = rri[1] = rrj[0] = rrj[1] = T(0);
+        uu[2] = rri[2] = rrj[2] = T(1);
+#pragma unroll
+        for (int q = 1; q <= NORD; q++) {
+          uu[q + 2] = uu[q + 1] * du;
+          rri[q + 2] = rri[q + 1] * di;
+          rrj[q + 2] = rrj[q + 1] * dj;
+        }
+        T dd1 = -sk * du * du, dd7 = -sk * di * di, dd8 = -sk * dj * dj;
+        T dd2 = 2 * sk * sk * du * du * du, dd9 = 2 * sk * sk * di * di * di, dd10 = 2 * sk * sk * dj * dj * dj;
+        T sp = ri + rj, tm = ri - rj;
+        T cpst = (rij * rij + sp * tm) / (ri * rij), cmst = (rij * rij - sp * tm) / (rj * rij);
+        const int base = pg.na + pg.nb + s.ctype[c] * tl.n;
+#pragma unroll
+        for (int ll = 0; ll < tl.n; ll++) {
+          const int k = tl.k[ll], l = tl.l[ll], m = tl.m[ll];
+          T ssl = (l == 0) ? T(2) : rri[l + 2] + rrj[l + 2];
+          T st = ssl * rri[m + 2] * rrj[m + 2];
+          T pi_ = T(l + m) * rri[l + m + 1] * rrj[m + 2] + T(m) * rri[m + 1] * rrj[l + m + 2];
+          T pj_ = T(l + m) * rrj[l + m + 1] * rri[m + 2] + T(m) * rrj[m + 1] * rri[l + m + 2];
+          T pii = T((l + m) * (l + m - 1)) * rri[l + m] * rrj[m + 2] + T(m * (m - 1)) * rri[m] * rrj[l + m + 2];
+          T pjj = T((l + m) * (l + m - 1)) * rrj[l + m] * rri[m + 2] + T(m * (m - 1)) * rrj[m] * rri[l + m + 2];
+          T fc = uu[k + 2] * st;
+          T fu = T(k) * uu[k + 1] * st, fuu = T(k * (k - 1)) * uu[k] * st;
+          T fi = uu[k + 2] * pi_, fj = uu[k + 2] * pj_, fii = uu[k + 2] * pii, fjj = uu[k + 2] * pjj;
+          T fui = T(k) * uu[k + 1] * pi_, fuj = T(k) * uu[k + 1] * pj_;
+          fuu = fuu * dd1 * dd1 + fu * dd2;
+          fui = fui * dd1 * dd7;
+          fuj = fuj * dd1 * dd8;
+          fii = fii * dd7 * dd7 + fi * dd9;
+          fjj = fjj * dd8 * dd8 + fj * dd10;
+          fu = fu * dd1 / rij;
+          fi = fi * dd7 / ri;
+          fj = fj * dd8 / rj;
+          double lap = (double)(2 * (2 * fu + fi + fj) + 2 * fuu + fii + fjj + fui * cpst + fuj * cmst);
+          double kk = lap + 2.0 * ((double)fi * vi_ri + (double)fu * vi_rv + (double)fj * vj_rj - (double)fu * vj_rv);
+          atomicAdd(&pg.G[base + ll], (double)fc);
+          atomicAdd(&pg.K[base + ll], kk);
+          atomicAdd(&pg.old[i * P + base + ll], (double)fc);
+          atomicAdd(&pg.old[j * P + base + ll], (double)fc);
+        }
+      }
+    }
+  }
+  for (int idx = lane; idx < N * C; idx += 32) {
+    int i = idx / C, c = idx - i * C;
+    const double *xi = v.xs + 3 * i, *cc = s.cent + 3 * c, *vi = pg.vt + 3 * i;
+    T r = v.ren[2 * idx], d = v.ren[2 * idx + 1];
+    double v_r = vi[0] * (xi[0] - cc[0]) + vi[1] * (xi[1] - cc[1]) + vi[2] * (xi[2] - cc[2]);
+    int it = s.ctype[c];
+    for (int k = 2; k <= J.norda; k++) {
+      T t, t1, t2;
+      en_param_terms(J, r, d, k, t, t1, t2, true);
+      int ip = it * (J.norda - 1) + (k - 2);
+      atomicAdd(&pg.G[ip], (double)t);
+      atomicAdd(&pg.K[ip], (double)(t2 + 2 * t1) + 2.0 * (double)t1 * v_r);
+      atomicAdd(&pg.old[i * P + ip], (double)t);
+    }
+  }
+  __syncwarp();
+}
+
+// Per-walker derivative output: free Jastrow parameters (a, b, then c with the cusp
+// dependences folded in), written as d ln psi / dp and dE_L / dp.
+struct PGOut {
+  double *dlnpsi;  // [W][nfree]
+  double *deloc;   // [W][nfree]
+  double *eloc;    // [W]
+  int nfree;
+};
+
+template <class T, int NORD, bool MD>
+__global__ void __launch_bounds__(128, 4) k_pgrad(Sys<T> s, State<T> st, Layout L, PGOut out, double r0, double r1,
+                                                  double r2, double r3, double r4, double r5, double r6, double r7,
+                                                  double r8) {
+  __shared__ JasPar<T> J;
+  __shared__ EcpPar E;
+  extern __shared__ __align__(16) char dsm[];
+  load_params(s, J, E);
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  const int N = s.N;
+  const int na = J.nct * (J.norda - 1 > 0 ? J.norda - 1 : 0), nb = J.nspin2b * J.nordb;
+  const int nt = make_terms(NORD).n, P = na + nb + (NORD > 1 ? J.nct * nt : 0);
+  const size_t pgbytes = sizeof(double) * (3 * N + N + 3 * P + N * P);
+  const size_t wb = L.base + align16(pgbytes);
+  const double R[9] = {r0, r1, r2, r3, r4, r5, r6, r7, r8};
+  for (int w = blockIdx.x * wpb + wib; w < st.W; w += gridDim.x * wpb) {
+    char *base = dsm + wb * wib;
+    View<T> v = make_view<T>(base, L, st, w, s.N, s.C, s.nbasis, s.nomax, false);
+    PGBuf pg;
+    double *q = (double *)(base + L.base);
+    pg.vt = q; q += 3 * N;
+    pg.csum = q; q += N;
+    pg.dvn = q; q += P;
+    pg.G = q; q += P;
+    pg.K = q; q += P;
+    pg.old = q;
+    pg.P = P; pg.na = na; pg.nb = nb;
+    for (int i = lane; i < (int)(pgbytes / sizeof(double)); i += 32) pg.vt[i] = 0.0;
+    for (int i = lane; i < 3 * N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * N + i];
+    __syncwarp();
+    EvalRes res;
+    full_eval<T, NORD, MD, true>(s, J, E, st, w, v, R, lane, false, res, &pg);
+    __syncwarp();
+    jastrow_param_pass<T, NORD>(s, J, v, pg, lane);
+    // dE_L/dp for the raw parameters, into pg.K; d ln psi / dp stays in pg.G
+    for (int p = lane; p < P; p += 32) {
+      double dv = pg.dvn[p];
+      for (int e = 0; e < N; e++) dv -= pg.csum[e] * pg.old[e * P + p];
+      pg.K[p] = -HB * pg.K[p] + dv;
+    }
+    __syncwarp();
+    // free parameters: a, b as they are; c through the cusp projection (cdep, checkdepend4)
+    double *ol = out.dlnpsi + (size_t)w * out.nfree, *oe = out.deloc + (size_t)w * out.nfree;
+    for (int f = lane; f < out.nfree; f += 32) {
+      double g, d;
+      if (f < na + nb) {
+        g = pg.G[f];
+        d = pg.K[f];
+      } else {
+        int fc = f - na - nb, it = fc / s.ncfree, jf = fc - it * s.ncfree;
+        g = 0;
+        d = 0;
+        for (int ll = 0; ll < nt; ll++) {
+          double pm = s.cproj[ll * s.ncfree + jf];
+          g += pm * pg.G[na + nb + it * nt + ll];
+          d += pm * pg.K[na + nb + it * nt + ll];
+        }
+      }
+      ol[f] = g;
+      oe[f] = d;
+    }
+    if (lane == 0) out.eloc[w] = res.eloc;
+    __syncwarp();
+  }
+}
+
+// O/H packing: Oa[w] = wt (1, O_w), Mb[w] = (E_L, E_L O_w + dE_w)
+static __global__ void k_pack_oh(int W, int P, const double *dl, const double *de, const double *el, const double *wt,
+                          double *Oa, double *Ow, double *Mb) {
+  const int P1 = P + 1;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)W * P1; i += (size_t)gridDim.x * blockDim.x) {
+    int w = (int)(i / P1), p = (int)(i - (size_t)w * P1);
+    double o = p ? dl[(size_t)w * P + p - 1] : 1.0;
+    double m = p ? el[w] * o + de[(size_t)w * P + p - 1] : el[w];
+    double ww = wt ? wt[w] : 1.0;
+    Oa[i] = o;
+    Ow[i] = ww * o;
+    Mb[i] = ww * m;
+  }
+}

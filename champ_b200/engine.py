@@ -21,7 +21,7 @@ EXPORTED_SYMBOLS = [
     "champ_last_error", "champ_version", "champ_create", "champ_destroy", "champ_nparam",
     "champ_set_walkers", "champ_get_walkers", "champ_set_quadrature_rotation", "champ_eval_full",
     "champ_propose_1e", "champ_accept_1e", "champ_grad_1e", "champ_vmc_sweeps", "champ_vmc_run_host",
-    "champ_walker_status", "champ_synchronize",
+    "champ_walker_status", "champ_synchronize", "champ_param_grad", "champ_accumulate_oh",
 ]
 
 PREC = {"fp64": 0, "mixed": 1}
@@ -67,6 +67,8 @@ def load_library(path: str = LIB_PATH):
     L.champ_vmc_run_host.argtypes = [vp, i32, dp, i32, u64, u64, C.c_double, dp]
     L.champ_walker_status.argtypes = [vp, C.POINTER(C.c_uint32)]
     L.champ_synchronize.argtypes = [vp]
+    L.champ_param_grad.argtypes = [vp, dp, dp, dp]
+    L.champ_accumulate_oh.argtypes = [vp, dp, dp, dp]
     for n in EXPORTED_SYMBOLS:
         if n not in ("champ_last_error", "champ_version"):
             getattr(L, n).restype = C.c_int
@@ -169,6 +171,28 @@ class Engine:
         self._check(self.lib.champ_vmc_run_host(self.h, nw, _p(x), nsweep, seed, sweep0, step, _p(el)))
         self.nw = nw
         return x, el
+
+    def nparam(self):
+        a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
+        self._check(self.lib.champ_nparam(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def param_grad(self, host=True):
+        """d ln psi/dp, dE_L/dp (walkers x P) and E_L at the current positions."""
+        P = sum(self.nparam())
+        if not host:
+            self._check(self.lib.champ_param_grad(self.h, None, None, None))
+            return None
+        dl, de, el = np.zeros((self.nw, P)), np.zeros((self.nw, P)), np.zeros(self.nw)
+        self._check(self.lib.champ_param_grad(self.h, _p(dl), _p(de), _p(el)))
+        return dl, de, el
+
+    def accumulate_oh(self, weights=None):
+        P1 = sum(self.nparam()) + 1
+        S, H = np.zeros((P1, P1)), np.zeros((P1, P1))
+        w = None if weights is None else np.ascontiguousarray(weights, np.float64)
+        self._check(self.lib.champ_accumulate_oh(self.h, _p(w) if w is not None else None, _p(S), _p(H)))
+        return S, H
 
     def walker_status(self):
         f = np.zeros(self.nw, np.uint32)

@@ -187,6 +187,21 @@ int champ_vmc_run_host(champ_ctx *ctx, int32_t nw, double *x /* host [nw][nelec]
                        int32_t nsweep, uint64_t seed, uint64_t sweep0, double step,
                        double *eloc /* host [nw] */);
 
+/* Parameter derivatives for the linear method (dpsi_bld / deloc_bld, qmc/deriv_mod.f90:248,437;
+   Jastrow parts: deriv_jastrow4, qmc/vmc/deriv_jastrow4.f90, and deriv_nonloc_pot,
+   qmc/fit/deriv_nonloc_pot.f90), for every walker at its current position: d ln psi / dp and
+   dE_L / dp for the P = champ_nparam() free parameters, ordered as the reference orders them
+   (Jastrow: a_3..a_{norda+1} per centre type, b_2..b_{nordb+1} per b set, then the free e-e-n
+   coefficients per centre type, i.e. those the cusp conditions do not fix).  Host outputs may
+   be NULL; the results stay on the device for champ_accumulate_oh. */
+int champ_param_grad(champ_ctx *ctx, double *dlnpsi /* [nw][P] */, double *deloc /* [nw][P] */,
+                     double *eloc /* [nw] */);
+/* O/H accumulation of the linear method (dpsi_dpsi / dpsi_deloc / dpsi_dpsi_eloc averages,
+   qmc/deriv_mod.f90:683,898,1375; opt_lin_mod.f90:249,404) over the walkers of the last
+   champ_param_grad, with optional weights: with Oa = (1, dlnpsi) and Mb = (E_L, E_L dlnpsi + deloc),
+   S[a][b] = sum_w wt_w Oa_a Oa_b and H[a][b] = sum_w wt_w Oa_a Mb_b, row-major (P+1)x(P+1), in FP64. */
+int champ_accumulate_oh(champ_ctx *ctx, const double *weights /* [nw] or NULL */, double *S, double *H);
+
 int champ_walker_status(champ_ctx *ctx, uint32_t *flags /* [nw] */);
 int champ_synchronize(champ_ctx *ctx);
 

@@ -1,0 +1,113 @@
+"""Parameter derivatives on the GPU (C ABI champ_param_grad / champ_accumulate_oh) against
+central finite differences (h = 1e-5) of the FP64 oracle's ln|psi| and E_L in each free
+Jastrow parameter, on the same walkers (checks of the kind deriv_jastrow4 / deriv_nonloc_pot
+feed into the linear method).
+
+Tolerance: |GPU - FD| <= 2e-5 * max(1, |FD|) for d ln psi/dp, and <= 2e-4 * max(1, |E_L|)
+for dE_L/dp (FD truncation and cancellation bound the comparison, not the GPU result).
+"""
+import copy
+
+import numpy as np
+import pytest
+
+from champ_b200 import system as S
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def oracle_mod():
+    from oracle import oracle
+    oracle.build()
+    return oracle
+
+
+def cusp_dependents(nordc):
+    """Indices fixed by the e-e-n cusp conditions (iwc4 of qmc/fit/cuspinit4.f90)."""
+    if nordc <= 1:
+        return []
+    iwc = [0] * (2 * (nordc - 1))
+    i = 0
+    for n in range(2, nordc + 1):
+        for k in range(n - 1, -1, -1):
+            l_hi = n - k - 2 if k == 0 else n - k
+            for l in range(l_hi, -1, -1):
+                m = (n - k - l) // 2
+                if 2 * m != n - k - l:
+                    continue
+                i += 1
+                if k == 1 and iwc[n - 2] == 0:
+                    iwc[n - 2] = i
+                if k == 0 and iwc[n + nordc - 3] == 0:
+                    iwc[n + nordc - 3] = i
+    return [v - 1 for v in iwc]
+
+
+def jastrow_params(s):
+    """Free Jastrow parameters in the engine's order: (array name, index)."""
+    out = []
+    for it in range(s.nctype):
+        for k in range(2, s.norda + 1):
+            out.append(("a4", (it, k)))
+    for isb in range(s.nspin2b):
+        for k in range(1, s.nordb + 1):
+            out.append(("b", (isb, k)))
+    if s.nordc > 1:
+        dep = cusp_dependents(s.nordc) if s.een_cusp else []
+        nt = S.nterms4(s.nordc)
+        for it in range(s.nctype):
+            for ll in range(nt):
+                if ll not in dep:
+                    out.append(("c", (it, ll)))
+    return out
+
+
+def perturbed(s, name, idx, h):
+    s2 = copy.deepcopy(s)
+    arr = getattr(s2, name).copy()
+    arr[idx] += h
+    setattr(s2, name, arr)
+    return s2
+
+
+@pytest.mark.parametrize("k", [1, 2, 3])
+def test_param_derivatives_match_finite_differences(oracle_mod, k):
+    from champ_b200.engine import Engine
+    s = S.get_system(k)
+    nw = 4
+    x = S.initial_walkers(s, nw, seed=60 + k)
+    eng = Engine(s, nw, "fp64")
+    eng.set_walkers(x)
+    nj, ncsf, norb = eng.nparam()
+    params = jastrow_params(s)
+    assert nj == len(params)
+    dl, de, el = eng.param_grad()
+    o0 = oracle_mod.Oracle(s)
+    for w in range(nw):
+        assert abs(el[w] - o0.eval(x[w])["energy"]) <= 1e-8 * max(1, abs(el[w]))
+    h = 1e-5
+    for ip, (name, idx) in enumerate(params):
+        op = oracle_mod.Oracle(perturbed(s, name, idx, h))
+        om = oracle_mod.Oracle(perturbed(s, name, idx, -h))
+        for w in range(nw):
+            rp, rm = op.eval(x[w]), om.eval(x[w])
+            g_fd = (rp["lnpsi"] - rm["lnpsi"]) / (2 * h)
+            e_fd = (rp["energy"] - rm["energy"]) / (2 * h)
+            assert abs(dl[w, ip] - g_fd) <= 2e-5 * max(1, abs(g_fd)), (name, idx, w, dl[w, ip], g_fd)
+            assert abs(de[w, ip] - e_fd) <= 2e-4 * max(1, abs(el[w])), (name, idx, w, de[w, ip], e_fd)
+
+
+def test_oh_accumulation_matches_numpy():
+    from champ_b200.engine import Engine
+    s = S.c2_dimer()
+    nw = 256
+    eng = Engine(s, nw, "fp64")
+    eng.set_walkers(S.initial_walkers(s, nw, seed=3))
+    dl, de, el = eng.param_grad()
+    wt = np.random.default_rng(1).uniform(0.5, 1.5, nw)
+    Sm, Hm = eng.accumulate_oh(wt)
+    Oa = np.hstack([np.ones((nw, 1)), dl])
+    Mb = np.hstack([el[:, None], el[:, None] * dl + de])
+    assert np.allclose(Sm, (Oa * wt[:, None]).T @ Oa, rtol=1e-12, atol=1e-9)
+    assert np.allclose(Hm, (Oa * wt[:, None]).T @ Mb, rtol=1e-12, atol=1e-7)
