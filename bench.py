@@ -191,6 +191,12 @@ def config_of(system, nw, prec):
             "l2": "flushed between timed steps (256 MB write)"}
 
 
+def lib_accumulate(eng):
+    """champ_accumulate_oh with the results left on the device (no host copies)."""
+    import ctypes as C
+    return eng.lib.champ_accumulate_oh(eng.h, None, None, None)
+
+
 def time_engine(eng, system, args, nsteps, nwarm, flush, torch, sweep_base):
     st = step_size(system)
     for i in range(nwarm):
@@ -274,6 +280,35 @@ def main():
         fp64 = {"value": v64, "unit": UNIT, "ms_per_step": ms64 / max(3, args.steps // 4),
                 "mixed_over_fp64": value / v64}
         eng64.close()
+    # parameter-gradient samples: d ln psi/dp and dE_L/dp for every walker, folded into the
+    # FP64 O/H accumulators (one champ_param_grad + champ_accumulate_oh per step); the walkers
+    # move by one VMC sweep between steps, outside the timed events
+    pg = None
+    try:
+        nj, ncsf, norb = eng.nparam()
+        npg = max(3, args.steps // 20)
+        tpg = 0.0
+        for k in range(npg + 2):
+            eng.vmc_sweeps(1, SEED, sweep0=30000 + k, step=step_size(system), stats=False)
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            eng.param_grad(host=False)
+            eng._check(lib_accumulate(eng))
+            e1.record()
+            torch.cuda.synchronize()
+            if k >= 2:
+                tpg += e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([tpg], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            tpg = float(t.item())
+        pg = {"value": nw * world * npg / (tpg * 1e-3), "unit": "param-grad samples/s", "n_params": nj + ncsf + norb,
+              "params": {"jastrow": nj, "csf": ncsf, "orbital": norb}, "ms_per_step": tpg / npg,
+              "step": "d ln psi/dp and dE_L/dp for all walkers + FP64 O/H accumulation (cuBLAS DGEMM)"}
+    except Exception as ex:  # report, do not hide
+        pg = {"error": str(ex)}
     # end to end through the host-facing call: walkers in from pinned host memory, one sweep,
     # E_L and walkers back to host memory, every step
     xh = torch.empty((nw, system.nelec, 3), dtype=torch.float64, pin_memory=True)
@@ -307,8 +342,8 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32+f64" if prec == "mixed" else "f64", "data": "synthetic",
-                "config": config_of(system, nw, prec), "clocks": clocks, "gpu_launches": args.steps,
-                "roofline": roof, "fp64_arm": fp64, "e2e": e2e, "cpu_baseline": cpu,
+                "config": config_of(system, nw, prec), "clocks": clocks, "gpu_launches": args.steps,  # one fused sweep kernel per step
+                "roofline": roof, "fp64_arm": fp64, "param_grad": pg, "e2e": e2e, "cpu_baseline": cpu,
                 "wall_s_timed_region": t_wall}
         print(json.dumps(line), flush=True)
     eng.close()

@@ -53,6 +53,10 @@ struct champ_ctx {
   // parameter derivatives and O/H accumulation
   int np_raw = 0;          // raw Jastrow parameters on the device (a, b, all c terms)
   int ncfree = 0;          // free e-e-n coefficients per centre type
+  int ncsfp = 0, norbp = 0;  // CSF and orbital-rotation parameters
+  std::vector<int2> orbp;
+  double *pg_scr = nullptr;
+  size_t scr_stride = 0;
   std::vector<double> cproj;
   int nfree = 0;           // free parameters reported
   size_t smem_pg = 0;      // dynamic shared memory of the derivative kernel

@@ -71,6 +71,15 @@ struct Sys {
   // qmc/fit/cuspinit4.f90) as a [nterms][ncfree] matrix
   int ncfree;
   const double *cproj;
+  // CSF and orbital-rotation parameters
+  int norb, ncsf, norbp;
+  const T *call;           // [nbasis][norb] all orbitals (internal basis order)
+  const int *csf_off;      // [ncsf+1]
+  const int *csf_det;      // determinant of each CSF entry
+  const double *csf_cd;    // coefficient of each CSF entry
+  const int2 *orbp;        // [norbp] (i, j): orbital i rotated towards orbital j
+  const int *refpos[2];    // [norb] column of orbital in the spin's reference determinant, or -1
+  const int *occo[2];      // [nocc_s] orbital index of each occupied column
   const JasPar<T> *jas;
   const EcpPar *ecp;
 };
@@ -319,6 +328,26 @@ __device__ __forceinline__ T shell_dot(const Sys<T> &s, int ish, const double *p
   return acc * ipow(T(1) / r, l) * R[0];
 }
 
+// Adds c times every basis function of one shell at pt into acc[b] (atomically).
+template <class T>
+__device__ __forceinline__ void shell_accum(const Sys<T> &s, int ish, const double *pt, double c, double *acc) {
+  int4 sh = s.shell[ish];
+  int cn = sh.x, l = sh.z;
+  T d0 = T(pt[0] - s.cent[3 * cn]), d1 = T(pt[1] - s.cent[3 * cn + 1]), d2 = T(pt[2] - s.cent[3 * cn + 2]);
+  T r = tsqrt(d0 * d0 + d1 * d1 + d2 * d2);
+  if (r == T(0)) { r = T(1e-30); d0 = r; }
+  T R[3];
+  shell_radial<T, false>(s, ish, r, R);
+  T S[9], G[9][3];
+  solid_all<T, false>(l, d0, d1, d2, S, G);
+  int b0 = s.shb0[ish];
+  const int nm = 2 * l + 1;
+  double f = c * (double)(ipow(T(1) / r, l) * R[0]);
+#pragma unroll
+  for (int sl = 0; sl < 9; sl++)
+    if (sl < nm) atomicAdd(&acc[b0 + sl], f * (double)S[sl]);
+}
+
 // Warp: all basis functions at pt into phi (shared memory).
 template <class T, int NCH>
 __device__ __forceinline__ void warp_basis(const Sys<T> &s, const double *pt, T *phi, int lane) {
@@ -329,8 +358,8 @@ __device__ __forceinline__ void warp_basis(const Sys<T> &s, const double *pt, T 
 // Warp: orbitals o_m = sum_b coef[b][m] phi[b] for m < n (orbitals_loc_ana.f90:50-64).
 // Lanes are split into LM lanes along m and 32/LM along b, reduced by shuffles.
 // out[ch*ostride + m].
-template <class T, int NCH>
-__device__ __forceinline__ void warp_orbitals(const T *phi, const T *coef, int nbasis, int n, T *out, int ostride,
+template <class T, int NCH, class O>
+__device__ __forceinline__ void warp_orbitals(const T *phi, const T *coef, int nbasis, int n, O *out, int ostride,
                                               int lane) {
   int LM = 1;
   while (LM < n && LM < 32) LM <<= 1;
@@ -353,7 +382,7 @@ __device__ __forceinline__ void warp_orbitals(const T *phi, const T *coef, int n
       for (int ch = 0; ch < NCH; ch++) acc[ch] += __shfl_xor_sync(0xffffffffu, acc[ch], o);
     if (lb == 0 && m < n)
 #pragma unroll
-      for (int ch = 0; ch < NCH; ch++) out[ch * ostride + m] = acc[ch];
+      for (int ch = 0; ch < NCH; ch++) out[ch * ostride + m] = (O)acc[ch];
   }
   __syncwarp();
 }

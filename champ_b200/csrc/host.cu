@@ -293,6 +293,46 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
   }
   {
     s.ncfree = c->ncfree;
+    // CSF and orbital-rotation parameter tables
+    s.norb = d->norb;
+    s.ncsf = d->ncsf;
+    s.norbp = c->norbp;
+    {
+      T *ca = dalloc<T>(c, (size_t)c->nbasis * d->norb);
+      std::vector<T> cav((size_t)c->nbasis * d->norb);
+      for (int m = 0; m < d->norb; m++)
+        for (int b = 0; b < c->nbasis; b++) cav[(size_t)b * d->norb + m] = (T)d->coef[(size_t)m * c->nbasis + perm_b[b]];
+      std::vector<int> off(d->ncsf + 1, 0), cdet;
+      std::vector<double> cd;
+      for (int q = 0, t = 0; q < d->ncsf; q++) {
+        for (int i = 0; i < d->csf_ndet[q]; i++, t++) { cdet.push_back(d->csf_det[t]); cd.push_back(d->csf_det_coef[t]); }
+        off[q + 1] = (int)cdet.size();
+      }
+      int *co = dalloc<int>(c, off.size()), *cdt = dalloc<int>(c, std::max<size_t>(1, cdet.size()));
+      double *cdd = dalloc<double>(c, std::max<size_t>(1, cd.size()));
+      int2 *op = dalloc<int2>(c, std::max(1, c->norbp));
+      int *rp0 = dalloc<int>(c, d->norb), *rp1 = dalloc<int>(c, d->norb);
+      int *oo0 = dalloc<int>(c, std::max(1, md.nocc[0])), *oo1 = dalloc<int>(c, std::max(1, md.nocc[1]));
+      if (!ca || !co || !cdt || !cdd || !op || !rp0 || !rp1 || !oo0 || !oo1) return fail(CHAMP_ENOMEM, "device allocation failed");
+      CK(cudaMemcpy(ca, cav.data(), sizeof(T) * cav.size(), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(co, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
+      if (!cdet.empty()) {
+        CK(cudaMemcpy(cdt, cdet.data(), sizeof(int) * cdet.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(cdd, cd.data(), sizeof(double) * cd.size(), cudaMemcpyHostToDevice));
+      }
+      if (c->norbp) CK(cudaMemcpy(op, c->orbp.data(), sizeof(int2) * c->norbp, cudaMemcpyHostToDevice));
+      int *rp[2] = {rp0, rp1}, *oo[2] = {oo0, oo1};
+      for (int sp = 0; sp < 2; sp++) {
+        std::vector<int> rpv(d->norb, -1);
+        int n = sp ? c->ndn : c->nup;
+        for (int k = 0; k < n; k++) rpv[md.occ[sp][k]] = k;
+        CK(cudaMemcpy(rp[sp], rpv.data(), sizeof(int) * d->norb, cudaMemcpyHostToDevice));
+        if (md.nocc[sp]) CK(cudaMemcpy(oo[sp], md.occ[sp].data(), sizeof(int) * md.nocc[sp], cudaMemcpyHostToDevice));
+        s.refpos[sp] = rp[sp];
+        s.occo[sp] = oo[sp];
+      }
+      s.call = ca; s.csf_off = co; s.csf_det = cdt; s.csf_cd = cdd; s.orbp = op;
+    }
     double *cp = dalloc<double>(c, std::max<size_t>(1, c->cproj.size()));
     if (!cp) return fail(CHAMP_ENOMEM, "device allocation failed");
     if (!c->cproj.empty()) CK(cudaMemcpy(cp, c->cproj.data(), sizeof(double) * c->cproj.size(), cudaMemcpyHostToDevice));
@@ -429,6 +469,21 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
     int rc0 = build_multidet(d, c->md);
     if (rc0) { delete c; return rc0; }
     c->nomax = std::max(1, std::max(c->md.nocc[0], c->md.nocc[1]));
+    // orbital rotations (single determinant): every reference orbital towards every orbital no
+    // reference determinant occupies (orb_opt_lab, orbitals_mod.f90:1829-2140)
+    c->orbp.clear();
+    if (!c->md.multidet) {
+      std::vector<int> occ;
+      for (int sp = 0; sp < 2; sp++)
+        for (int k = 0; k < (sp ? c->ndn : c->nup); k++)
+          if (std::find(occ.begin(), occ.end(), c->md.occ[sp][k]) == occ.end()) occ.push_back(c->md.occ[sp][k]);
+      std::sort(occ.begin(), occ.end());
+      for (int i : occ)
+        for (int j = 0; j < d->norb; j++)
+          if (std::find(occ.begin(), occ.end(), j) == occ.end()) c->orbp.push_back(make_int2(i, j));
+    }
+    c->norbp = (int)c->orbp.size();
+    c->ncsfp = c->md.multidet && d->ncsf > 1 ? d->ncsf - 1 : 0;
     if (c->nomax > 256) { delete c; return fail(CHAMP_EINVAL, "more than 256 occupied orbitals of one spin"); }
   }
   // normalised primitive weights (basis_norm)
@@ -467,8 +522,7 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
     }
     int na = d->nctype * std::max(0, d->norda - 1), nb = d->nspin2b * d->nordb;
     c->np_raw = na + nb + (d->nordc > 1 ? d->nctype * nt : 0);
-    c->nfree = na + nb + d->nctype * c->ncfree;
-    c->nparm_jas = c->nfree;
+    c->nparm_jas = na + nb + d->nctype * c->ncfree;
   }
   if (nt == 0) cfull.assign(d->nctype, 0.0);
   // asymptotic values for isc=4 (set_scale_dist, scale_dist.f90:147-225)
@@ -546,6 +600,7 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
     c->smem = c->lay.bytes;
   }
   if (rc) { champ_destroy(c); return rc; }
+  c->nfree = c->ncsfp + c->norbp + c->nparm_jas;
   // warps per block: up to 8, keeping the block's dynamic shared memory under 96 KB
   c->wpb = 4;  // 128-thread blocks (the kernels' launch bounds)
   while (c->wpb > 1 && c->smem * c->wpb > 96 * 1024) c->wpb >>= 1;
@@ -577,6 +632,12 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
     c->oh_mb = dalloc<double>(c, W * P1);
     c->oh_s = dalloc<double>(c, P1 * P1);
     c->oh_h = dalloc<double>(c, P1 * P1);
+    if (c->ncsfp + c->norbp > 0) {
+      size_t N = c->N, B = c->nbasis, M = d->norb, nm = c->nmax;
+      c->scr_stride = N * B + N * 5 * M + N * M + 4 * nm * M + nm * nm + (size_t)(c->md.ndu[0] + c->md.ndu[1]) + 1;
+      c->pg_scr = dalloc<double>(c, W * c->scr_stride);
+      if (!c->pg_scr) { champ_destroy(c); return fail(CHAMP_ENOMEM, "allocation of the derivative scratch failed"); }
+    }
     if (!c->pg_dl || !c->pg_de || !c->pg_el || !c->pg_wt || !c->oh_oa || !c->oh_ow || !c->oh_mb || !c->oh_s || !c->oh_h) {
       champ_destroy(c);
       return fail(CHAMP_ENOMEM, "allocation of the parameter-derivative buffers failed");
@@ -605,6 +666,8 @@ int champ_param_grad(champ_ctx *c, double *dlnpsi, double *deloc, double *eloc) 
   a.pgout.deloc = c->pg_de;
   a.pgout.eloc = c->pg_el;
   a.pgout.nfree = c->nfree;
+  a.pgout.scr = c->pg_scr;
+  a.pgout.scr_stride = c->scr_stride;
   int rc = launch(c, Op::PGrad, a);
   if (rc) return rc;
   size_t W = c->W, P = c->nfree;
@@ -647,8 +710,8 @@ int champ_accumulate_oh(champ_ctx *c, const double *weights, double *S, double *
 int champ_nparam(const champ_ctx *c, int32_t *nj, int32_t *ncsf, int32_t *norb) {
   if (!c) return fail(CHAMP_EINVAL, "null context");
   if (nj) *nj = c->nparm_jas;
-  if (ncsf) *ncsf = 0;
-  if (norb) *norb = 0;
+  if (ncsf) *ncsf = c->ncsfp;
+  if (norb) *norb = c->norbp;
   return CHAMP_OK;
 }
 

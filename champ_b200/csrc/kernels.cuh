@@ -431,7 +431,7 @@ __device__ void build_gamma(const Sys<T> &s, const View<T> &v, int lane, double 
 // hpsi for one walker (qmc/vmc/hpsi.f90:2-381), warp-cooperative.
 // ---------------------------------------------------------------------------------------
 struct EvalRes {
-  double lnpsi, sign, psij, d2lnpsi, pe, pe_ee, pe_nl, eloc;
+  double lnpsi, sign, psij, d2lnpsi, pe, pe_ee, pe_nl, eloc, d2j, vj2;
   bool singular;
 };
 
@@ -446,6 +446,8 @@ struct PGBuf {
   double *K;     // [P] sum_e (lap_e g_p + 2 v_e . grad_e g_p)
   double *old;   // [N][P] basis function of p summed over the terms involving electron e
   int P, na, nb;
+  double *phis;  // [N][nbasis] or null: sum over the electron's quadrature points of
+                 // w e^dJ v_l(r) P_l times each basis function (nonlocal part of B in basis space)
 };
 
 template <class T, int NORD>
@@ -734,6 +736,11 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
         double coeff = E.wq[q] * exp(dj) * vp * (double)dr;
         atomicAdd(&pg->csum[e], coeff);
         point_param_values<T, NORD>(s, J, v, e, xn, coeff, *pg);
+        if (pg->phis) {
+          double c2 = E.wq[q] * exp(dj) * vp;
+          double *ph = pg->phis + (size_t)e * s.nbasis;
+          for (int ish = 0; ish < s.nshell; ish++) shell_accum<T>(s, ish, xn, c2, ph);
+        }
       }
     }
     vnl = warp_sum(vnl);
@@ -750,6 +757,12 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
   res.pe_ee = pe_ee;
   res.pe_nl = vnl;
   res.eloc = eloc;
+  res.d2j = d2j;
+  {
+    double vj2 = 0;
+    for (int i = lane; i < 3 * N; i += 32) vj2 += v.vacc[i] * v.vacc[i];
+    res.vj2 = warp_sum(vj2);
+  }
   res.singular = !ok;
   if (lane == 0) {
     st.fsum[w] = fsum;

@@ -218,7 +218,129 @@ struct PGOut {
   double *deloc;   // [W][nfree]
   double *eloc;    // [W]
   int nfree;
+  double *scr;     // per-walker scratch of the CSF/orbital part (null when there is none)
+  size_t scr_stride;
 };
+
+// CSF and orbital-rotation derivatives from the orbital-resolved local energy
+// B[e][m] = -1/2 (lap phi_m + 2 v_J . grad phi_m + ddjas phi_m) + V_loc/N phi_m + V_NL,m
+// (elocal_orb_bld, deriv_fast_mod.f90:174-209).  Per spin: T = Ainv Atilde and
+// dT = Ainv B - (Ainv B)_ref T over all orbitals (dt_bld, :400), E_ref = tr (Ainv B)_ref.
+// CSF: dlnpsi = sum_K c_K D_K/psi_D, dE_L = sum_K c_K (D_K/psi_D)(E_K - E_L) with
+// E_K = E_ref + tr(alpha_K^-1 dalpha_K) per spin (alpha_deloc_bld :468, csf_derivs_bld :781).
+// Orbital rotation i -> j (single determinant): dlnpsi = sum_spin T[i][j], dE_L = sum_spin dT[i][j]
+// (dpsi_orb_bld / deloc_orb_bld, deriv_orb_mod.f90:1486,1557).
+template <class T, bool MD>
+__device__ void orbital_csf_derivs(const Sys<T> &s, const View<T> &v, const PGBuf &pg, const EvalRes &res, int lane,
+                                   double *scr, double *ol, double *oe) {
+  const int N = s.N, B = s.nbasis, M = s.norb, nmax = s.nmax;
+  double *orbA = scr + (size_t)N * B;
+  double *Bm = orbA + (size_t)N * 5 * M;
+  double *Ta = Bm + (size_t)N * M;
+  double *dTa = Ta + (size_t)2 * nmax * M;
+  double *Qr = dTa + (size_t)2 * nmax * M;
+  double *delo = Qr + (size_t)nmax * nmax;
+  for (int e = 0; e < N; e++) {
+    warp_basis<T, 5>(s, v.xs + 3 * e, v.phi, lane);
+    warp_orbitals<T, 5>(v.phi, s.call, B, M, orbA + (size_t)e * 5 * M, M, lane);
+  }
+  const double ddjas = (res.d2j + res.vj2) / N, vloc = (res.pe - res.pe_nl) / N;
+  for (int i = lane; i < N * M; i += 32) {
+    int e = i / M, m = i - e * M;
+    const double *o = orbA + (size_t)e * 5 * M + m;
+    const double *vj = v.vacc + 3 * e;
+    double b = -HB * (o[4 * M] + 2 * (vj[0] * o[M] + vj[1] * o[2 * M] + vj[2] * o[3 * M]) + ddjas * o[0]) + vloc * o[0];
+    const double *ph = scr + (size_t)e * B;
+    for (int k = 0; k < B; k++) b += ph[k] * (double)s.call[(size_t)k * M + m];
+    Bm[i] = b;
+  }
+  __syncwarp();
+  double eref = 0;
+  for (int sp = 0; sp < 2; sp++) {
+    const int n = sp ? s.ndn : s.nup, e0 = sp ? s.nup : 0;
+    if (n == 0) continue;
+    const double *A = v.ainv + (sp ? s.nup * s.nup : 0);
+    double *Ts = Ta + (size_t)sp * nmax * M, *dTs = dTa + (size_t)sp * nmax * M;
+    for (int i = lane; i < n * M; i += 32) {
+      int k = i / M, m = i - k * M;
+      double t = 0, q = 0;
+      for (int e = 0; e < n; e++) {
+        double a = A[k * n + e];
+        t += a * orbA[(size_t)(e0 + e) * 5 * M + m];
+        q += a * Bm[(size_t)(e0 + e) * M + m];
+      }
+      Ts[i] = t;
+      dTs[i] = q;
+    }
+    __syncwarp();
+    const int *ro = s.occo[sp];
+    double er = 0;
+    for (int i = lane; i < n * n; i += 32) {
+      int k = i / n, k2 = i - k * n;
+      Qr[i] = dTs[k * M + ro[k2]];
+      if (k == k2) er += Qr[i];
+    }
+    eref += warp_sum(er);
+    __syncwarp();
+    for (int i = lane; i < n * M; i += 32) {
+      int k = i / M, m = i - k * M;
+      double d = dTs[i];
+      for (int k2 = 0; k2 < n; k2++) d -= Qr[k * n + k2] * Ts[k2 * M + m];
+      dTs[i] = d;
+    }
+    __syncwarp();
+  }
+  if (MD && s.ncsf > 1) {
+    const int nd0 = s.ndu[0];
+    const double *wd = v.wdet;
+    for (int sp = 0; sp < 2; sp++) {
+      const int n = sp ? s.ndn : s.nup;
+      const double *dTs = dTa + (size_t)sp * nmax * M;
+      for (int I = lane; I < s.ndu[sp]; I += 32) {
+        double a[16], inv[16];
+        int k = load_alpha(s, v, sp, I, a);
+        double dl = 0;
+        if (k) {
+          small_det_inv(a, k, inv);
+          for (int ia = 0; ia < k; ia++)
+            for (int ib = 0; ib < k; ib++)
+              dl += inv[ib * k + ia] * dTs[s.dh[sp][4 * I + ia] * M + s.occo[sp][n + s.dpart[sp][4 * I + ib]]];
+        }
+        delo[(sp ? nd0 : 0) + I] = dl;
+      }
+    }
+    __syncwarp();
+    double chi = 0;
+    for (int K = lane; K < s.ndet; K += 32) chi += s.ccoef[K] * wd[s.ciu[K]] * wd[nd0 + s.cid[K]];
+    chi = warp_sum(chi);
+    for (int q = 1 + lane; q < s.ncsf; q += 32) {
+      double dl = 0, de = 0;
+      for (int t = s.csf_off[q]; t < s.csf_off[q + 1]; t++) {
+        int K = s.csf_det[t], iu = s.ciu[K], id = s.cid[K];
+        double r = wd[iu] * wd[nd0 + id] / chi;
+        double eK = eref + delo[iu] + delo[nd0 + id];
+        dl += s.csf_cd[t] * r;
+        de += s.csf_cd[t] * r * (eK - res.eloc);
+      }
+      ol[q - 1] = dl;
+      oe[q - 1] = de;
+    }
+  }
+  const int off = MD ? (s.ncsf > 1 ? s.ncsf - 1 : 0) : 0;
+  for (int p = lane; p < s.norbp; p += 32) {
+    int2 ij = s.orbp[p];
+    double g = 0, h = 0;
+    for (int sp = 0; sp < 2; sp++) {
+      int k = s.refpos[sp][ij.x];
+      if (k < 0) continue;
+      g += Ta[(size_t)sp * nmax * M + (size_t)k * M + ij.y];
+      h += dTa[(size_t)sp * nmax * M + (size_t)k * M + ij.y];
+    }
+    ol[off + p] = g;
+    oe[off + p] = h;
+  }
+  __syncwarp();
+}
 
 template <class T, int NORD, bool MD>
 __global__ void __launch_bounds__(128, 4) k_pgrad(Sys<T> s, State<T> st, Layout L, PGOut out, double r0, double r1,
@@ -247,7 +369,11 @@ __global__ void __launch_bounds__(128, 4) k_pgrad(Sys<T> s, State<T> st, Layout 
     pg.K = q; q += P;
     pg.old = q;
     pg.P = P; pg.na = na; pg.nb = nb;
+    double *scr = out.scr ? out.scr + (size_t)w * out.scr_stride : nullptr;
+    pg.phis = scr;
     for (int i = lane; i < (int)(pgbytes / sizeof(double)); i += 32) pg.vt[i] = 0.0;
+    if (scr)
+      for (int i = lane; i < N * s.nbasis; i += 32) scr[i] = 0.0;
     for (int i = lane; i < 3 * N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * N + i];
     __syncwarp();
     EvalRes res;
@@ -261,9 +387,14 @@ __global__ void __launch_bounds__(128, 4) k_pgrad(Sys<T> s, State<T> st, Layout 
       pg.K[p] = -HB * pg.K[p] + dv;
     }
     __syncwarp();
-    // free parameters: a, b as they are; c through the cusp projection (cdep, checkdepend4)
+    // output order: CSF, orbital rotations, Jastrow (as deriv_mod.f90:120-247 concatenates them)
     double *ol = out.dlnpsi + (size_t)w * out.nfree, *oe = out.deloc + (size_t)w * out.nfree;
-    for (int f = lane; f < out.nfree; f += 32) {
+    if (scr) orbital_csf_derivs<T, MD>(s, v, pg, res, lane, scr, ol, oe);
+    const int jo = (MD && s.ncsf > 1 ? s.ncsf - 1 : 0) + s.norbp;
+    ol += jo;
+    oe += jo;
+    // free Jastrow parameters: a, b as they are; c through the cusp projection (cdep, checkdepend4)
+    for (int f = lane; f < out.nfree - jo; f += 32) {
       double g, d;
       if (f < na + nb) {
         g = pg.G[f];

@@ -1,7 +1,7 @@
 """Parameter derivatives on the GPU (C ABI champ_param_grad / champ_accumulate_oh) against
 central finite differences (h = 1e-5) of the FP64 oracle's ln|psi| and E_L in each free
-Jastrow parameter, on the same walkers (checks of the kind deriv_jastrow4 / deriv_nonloc_pot
-feed into the linear method).
+parameter -- CSF coefficients, orbital rotations (coefficients of orbital i += h times those of
+orbital j) and Jastrow coefficients -- on the same walkers.
 
 Tolerance: |GPU - FD| <= 2e-5 * max(1, |FD|) for d ln psi/dp, and <= 2e-4 * max(1, |E_L|)
 for dE_L/dp (FD truncation and cancellation bound the comparison, not the GPU result).
@@ -63,10 +63,33 @@ def jastrow_params(s):
     return out
 
 
+def orbital_params(s):
+    """Orbital rotations i -> j of a single determinant: i a reference orbital, j an orbital no
+    reference column uses."""
+    if s.ndet > 1:
+        return []
+    occ = sorted(set(int(o) for o in s.det_orb[0]))
+    return [(i, j) for i in occ for j in range(s.norb) if j not in occ]
+
+
+def all_params(s):
+    """(kind, name, idx) in the engine's order: CSF, orbital rotations, Jastrow."""
+    out = []
+    if s.ndet > 1:
+        out += [("csf", "csf_coef", (q,)) for q in range(1, len(s.csf_coef))]
+    out += [("orb", "coef", ij) for ij in orbital_params(s)]
+    out += [("jas", name, idx) for name, idx in jastrow_params(s)]
+    return out
+
+
 def perturbed(s, name, idx, h):
     s2 = copy.deepcopy(s)
     arr = getattr(s2, name).copy()
-    arr[idx] += h
+    if name == "coef":  # rotate orbital i towards orbital j
+        i, j = idx
+        arr[i] = arr[i] + h * arr[j]
+    else:
+        arr[idx] += h
     setattr(s2, name, arr)
     return s2
 
@@ -80,14 +103,15 @@ def test_param_derivatives_match_finite_differences(oracle_mod, k):
     eng = Engine(s, nw, "fp64")
     eng.set_walkers(x)
     nj, ncsf, norb = eng.nparam()
-    params = jastrow_params(s)
-    assert nj == len(params)
+    params = all_params(s)
+    assert nj == len(jastrow_params(s)) and norb == len(orbital_params(s))
+    assert nj + ncsf + norb == len(params)
     dl, de, el = eng.param_grad()
     o0 = oracle_mod.Oracle(s)
     for w in range(nw):
         assert abs(el[w] - o0.eval(x[w])["energy"]) <= 1e-8 * max(1, abs(el[w]))
     h = 1e-5
-    for ip, (name, idx) in enumerate(params):
+    for ip, (kind, name, idx) in enumerate(params):
         op = oracle_mod.Oracle(perturbed(s, name, idx, h))
         om = oracle_mod.Oracle(perturbed(s, name, idx, -h))
         for w in range(nw):
