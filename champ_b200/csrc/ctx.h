@@ -65,6 +65,15 @@ struct champ_ctx {
   double *oh_oa = nullptr, *oh_ow = nullptr, *oh_mb = nullptr, *oh_s = nullptr, *oh_h = nullptr;
   bool have_pgrad = false;
   void *cublas = nullptr;
+  // DMC: second state buffer for branching, per-walker weights/energies, device scalars
+  bool dmc_ready = false;
+  DmcPar dpar;
+  DmcData dA, dB;
+  State<double> std2;
+  State<float> stf2;
+  void *scan_tmp = nullptr;
+  size_t scan_bytes = 0;
+  int dmc_step = 0;
 };
 
 template <class T>
@@ -80,9 +89,16 @@ inline State<double> &stof<double>(champ_ctx *c) { return c->std_; }
 template <>
 inline State<float> &stof<float>(champ_ctx *c) { return c->stf; }
 
+template <class T>
+inline State<T> &st2of(champ_ctx *c);
+template <>
+inline State<double> &st2of<double>(champ_ctx *c) { return c->std2; }
+template <>
+inline State<float> &st2of<float>(champ_ctx *c) { return c->stf2; }
+
 inline int nblocks(champ_ctx *c) { return (c->W + c->wpb - 1) / c->wpb; }
 
-enum class Op { Eval, EvalOut, Propose, ProposeGrad, Accept, Vmc, PGrad };
+enum class Op { Eval, EvalOut, Propose, ProposeGrad, Accept, Vmc, PGrad, DmcMove, DmcCopy };
 struct OpArgs {
   int e = 0;
   const double *xnew = nullptr;
@@ -92,6 +108,7 @@ struct OpArgs {
   uint64_t seed = 0, sweep0 = 0;
   double step = 0;
   PGOut pgout;
+  int istep = 0;
 };
 
 

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/champ_b200.h"
+#include <cub/cub.cuh>
 #include <cublas_v2.h>
 
 #include "ctx.h"
@@ -436,6 +437,27 @@ static int copy_stats(champ_ctx *c, const champ_vmc_stats *s) {
   return CHAMP_OK;
 }
 
+// ---- DMC
+template <class T>
+static int alloc_state_copy(champ_ctx *c, const State<T> &a, State<T> &b) {
+  b = a;  // strides, scratch and output buffers are shared
+  size_t W = c->wmax, N = c->N;
+  b.x = dalloc<double>(c, W * N * 3);
+  b.ainv = dalloc<double>(c, W * a.astride);
+  b.fso = dalloc<T>(c, W * N * N);
+  b.ren = dalloc<T>(c, W * N * c->C * 2);
+  b.tv = dalloc<double>(c, W * a.tvstride);
+  b.gam = dalloc<double>(c, W * a.gstride);
+  b.fsum = dalloc<double>(c, W);
+  b.lnd = dalloc<double>(c, W);
+  b.sgn = dalloc<double>(c, W);
+  if (!b.x || !b.ainv || !b.fso || !b.ren || !b.tv || !b.gam || !b.fsum || !b.lnd || !b.sgn)
+    return fail(CHAMP_ENOMEM, "allocation of the DMC state buffer failed");
+  return CHAMP_OK;
+}
+
+static const int DMC_STAT_CAP = 1 << 16;
+
 extern "C" {
 
 const char *champ_last_error(void) { return g_err.c_str(); }
@@ -707,6 +729,100 @@ int champ_accumulate_oh(champ_ctx *c, const double *weights, double *S, double *
   return CHAMP_OK;
 }
 
+
+int champ_dmc_init(champ_ctx *c, int32_t w_target, double tau, double gpop) {
+  if (!c) return fail(CHAMP_EINVAL, "null context");
+  if (!c->have_walkers) return fail(CHAMP_ESTATE, "set the initial walkers first");
+  if (w_target < 1 || tau <= 0 || gpop <= 0) return fail(CHAMP_EINVAL, "bad DMC parameters");
+  if (!c->dmc_ready) {
+    int rc = c->prec == CHAMP_PREC_FP64 ? alloc_state_copy<double>(c, c->std_, c->std2)
+                                        : alloc_state_copy<float>(c, c->stf, c->stf2);
+    if (rc) return rc;
+    size_t W = c->wmax;
+    int *nw = dalloc<int>(c, 1);
+    double *sc = dalloc<double>(c, 4);
+    int *nc = dalloc<int>(c, W), *off = dalloc<int>(c, W);
+    double *stat = dalloc<double>(c, 4 * (size_t)DMC_STAT_CAP);
+    double *w0 = dalloc<double>(c, W), *w1 = dalloc<double>(c, W), *e0 = dalloc<double>(c, W), *e1 = dalloc<double>(c, W);
+    if (!nw || !sc || !nc || !off || !stat || !w0 || !w1 || !e0 || !e1) return fail(CHAMP_ENOMEM, "DMC allocation failed");
+    c->dA.nw = c->dB.nw = nw;
+    c->dA.et = c->dB.et = sc;
+    c->dA.eest = c->dB.eest = sc + 1;
+    c->dA.red = c->dB.red = sc + 2;
+    c->dA.ncopy = c->dB.ncopy = nc;
+    c->dA.off = c->dB.off = off;
+    c->dA.stat = c->dB.stat = stat;
+    c->dA.wt = w0; c->dB.wt = w1;
+    c->dA.el = e0; c->dB.el = e1;
+    c->scan_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, c->scan_bytes, nc, off, (int)W, c->stream);
+    c->scan_tmp = dalloc<char>(c, c->scan_bytes);
+    if (!c->scan_tmp) return fail(CHAMP_ENOMEM, "DMC scan allocation failed");
+    c->dmc_ready = true;
+  }
+  c->dpar.tau = tau;
+  c->dpar.adrift = 0.5;  // adrift_default (control_mod.f90:16)
+  c->dpar.gpop = gpop;
+  c->dpar.ecut = 10.0 / std::sqrt(tau);
+  c->dpar.wtarget = w_target;
+  c->dpar.wmax = c->wmax;
+  // initial population: the current walkers, weight 1, with their local energies
+  int rc = launch(c, Op::EvalOut);
+  if (rc) return rc;
+  double *el = c->prec == CHAMP_PREC_FP64 ? c->std_.o_eloc : c->stf.o_eloc;
+  std::vector<double> elh(c->W), one(c->W, 1.0);
+  CK(cudaMemcpyAsync(elh.data(), el, sizeof(double) * c->W, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double em = 0;
+  int nf = 0;
+  for (double e : elh)
+    if (std::isfinite(e)) { em += e; nf++; }
+  em = nf ? em / nf : 0.0;
+  double sc[4] = {em, em, 0.0, 0.0};
+  int nw = c->W;
+  CK(cudaMemcpyAsync(c->dA.el, elh.data(), sizeof(double) * c->W, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->dA.wt, one.data(), sizeof(double) * c->W, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->dA.et, sc, sizeof(double) * 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->dA.nw, &nw, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->dmc_step = 0;
+  return CHAMP_OK;
+}
+
+int champ_dmc_steps(champ_ctx *c, int32_t nstep, uint64_t seed, double *stats) {
+  if (!c) return fail(CHAMP_EINVAL, "null context");
+  if (!c->dmc_ready) return fail(CHAMP_ESTATE, "call champ_dmc_init first");
+  if (nstep < 0 || nstep > DMC_STAT_CAP) return fail(CHAMP_EINVAL, "nstep out of range");
+  c->dpar.seed = seed;
+  for (int i = 0; i < nstep; i++) {
+    OpArgs a;
+    a.istep = c->dmc_step;
+    int rc = launch(c, Op::DmcMove, a);
+    if (rc) return rc;
+    k_dmc_sums<<<148, 256, 0, c->stream>>>(c->dA, c->dpar.wmax);
+    k_dmc_count<<<(c->dpar.wmax + 255) / 256, 256, 0, c->stream>>>(c->dA, c->dpar, c->dmc_step);
+    if (cub::DeviceScan::ExclusiveSum(c->scan_tmp, c->scan_bytes, c->dA.ncopy, c->dA.off, c->dpar.wmax, c->stream) !=
+        cudaSuccess)
+      return fail(CHAMP_ECUDA, "DMC scan failed");
+    rc = launch(c, Op::DmcCopy, a);
+    if (rc) return rc;
+    k_dmc_finish<<<1, 32, 0, c->stream>>>(c->dA, c->dB, c->dpar, i);
+    CK(cudaGetLastError());
+    std::swap(c->std_, c->std2);
+    std::swap(c->stf, c->stf2);
+    std::swap(c->dA.wt, c->dB.wt);
+    std::swap(c->dA.el, c->dB.el);
+    c->dmc_step++;
+  }
+  int nw = 0;
+  CK(cudaMemcpyAsync(&nw, c->dA.nw, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  if (stats && nstep)
+    CK(cudaMemcpyAsync(stats, c->dA.stat, sizeof(double) * 4 * nstep, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->W = nw;
+  return CHAMP_OK;
+}
+
 int champ_nparam(const champ_ctx *c, int32_t *nj, int32_t *ncsf, int32_t *norb) {
   if (!c) return fail(CHAMP_EINVAL, "null context");
   if (nj) *nj = c->nparm_jas;
@@ -851,6 +967,12 @@ int champ_walker_status(champ_ctx *c, uint32_t *flags) {
   uint32_t *s = c->prec == CHAMP_PREC_FP64 ? c->std_.status : c->stf.status;
   CK(cudaMemcpyAsync(flags, s, sizeof(uint32_t) * c->W, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return CHAMP_OK;
+}
+
+int champ_num_walkers(const champ_ctx *c, int32_t *nw) {
+  if (!c || !nw) return fail(CHAMP_EINVAL, "null argument");
+  *nw = c->W;
   return CHAMP_OK;
 }
 

@@ -1068,3 +1068,4 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
 }
 
 #include "pgrad.cuh"
+#include "dmc.cuh"

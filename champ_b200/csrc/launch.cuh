@@ -16,6 +16,7 @@ static int set_smem_attrs(champ_ctx *c) {
   if (!rc) rc = set_attrs(c, k_propose<T, NORD, MD>);
   if (!rc) rc = set_attrs(c, k_accept<T, MD>);
   if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD>);
+  if (!rc) rc = set_attrs(c, k_dmc_move<T, NORD, MD>);
   if (!rc) {
     CK(cudaFuncSetAttribute(k_pgrad<T, NORD, MD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_pg));
     CK(cudaFuncSetAttribute(k_pgrad<T, NORD, MD>, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -48,6 +49,14 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
     k_pgrad<T, NORD, MD><<<dim3((c->W + c->wpb_pg - 1) / c->wpb_pg), dim3(32 * c->wpb_pg), c->smem_pg, c->stream>>>(s, st, c->lay, a.pgout, R[0], R[1], R[2], R[3], R[4],
                                                                  R[5], R[6], R[7], R[8]);
     break;
+  case Op::DmcMove:
+    k_dmc_move<T, NORD, MD><<<dim3((c->dpar.wmax + c->wpb - 1) / c->wpb), block, c->smem, c->stream>>>(
+        s, st, c->lay, c->dpar, c->dA, a.istep);
+    break;
+  case Op::DmcCopy: {
+    k_dmc_copy<T><<<592, 128, 0, c->stream>>>(st, st2of<T>(c), c->dA, c->dB, c->N, c->C, c->dpar.wmax);
+    break;
+  }
   case Op::Vmc:
     k_vmc<T, NORD, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, a.nsweep, a.seed, a.sweep0, a.step);
     break;

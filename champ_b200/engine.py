@@ -22,6 +22,7 @@ EXPORTED_SYMBOLS = [
     "champ_set_walkers", "champ_get_walkers", "champ_set_quadrature_rotation", "champ_eval_full",
     "champ_propose_1e", "champ_accept_1e", "champ_grad_1e", "champ_vmc_sweeps", "champ_vmc_run_host",
     "champ_walker_status", "champ_synchronize", "champ_param_grad", "champ_accumulate_oh",
+    "champ_dmc_init", "champ_dmc_steps", "champ_num_walkers",
 ]
 
 PREC = {"fp64": 0, "mixed": 1}
@@ -69,6 +70,9 @@ def load_library(path: str = LIB_PATH):
     L.champ_synchronize.argtypes = [vp]
     L.champ_param_grad.argtypes = [vp, dp, dp, dp]
     L.champ_accumulate_oh.argtypes = [vp, dp, dp, dp]
+    L.champ_dmc_init.argtypes = [vp, i32, C.c_double, C.c_double]
+    L.champ_dmc_steps.argtypes = [vp, i32, u64, dp]
+    L.champ_num_walkers.argtypes = [vp, C.POINTER(i32)]
     for n in EXPORTED_SYMBOLS:
         if n not in ("champ_last_error", "champ_version"):
             getattr(L, n).restype = C.c_int
@@ -193,6 +197,21 @@ class Engine:
         w = None if weights is None else np.ascontiguousarray(weights, np.float64)
         self._check(self.lib.champ_accumulate_oh(self.h, _p(w) if w is not None else None, _p(S), _p(H)))
         return S, H
+
+    def dmc_init(self, w_target, tau, gpop=10.0):
+        self._check(self.lib.champ_dmc_init(self.h, w_target, tau, gpop))
+
+    def dmc_steps(self, nstep, seed):
+        """Runs nstep DMC steps; returns per-step [population, sum w, sum w E_L, E_T]."""
+        st = np.zeros((nstep, 4))
+        self._check(self.lib.champ_dmc_steps(self.h, nstep, seed, _p(st)))
+        nw = C.c_int32()
+        self._check(self.lib.champ_num_walkers(self.h, C.byref(nw)))
+        self.nw = nw.value
+        return st
+
+    def population(self):
+        return self.nw
 
     def walker_status(self):
         f = np.zeros(self.nw, np.uint32)

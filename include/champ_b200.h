@@ -13,7 +13,8 @@
  *   champ_set_walkers <->  psi_at for every walker (qmc/psi_utils_mod.f90:13)
  *   champ_vmc_sweeps  <->  the metrop_mov1 sweep loop + hpsi per sweep
  *                          (qmc/vmc/metrop_mov1.f90:64-296, qmc/vmc/vmc.f90:250-331)
- *   champ_dmc_steps   <->  rundmc walker/electron loops (qmc/rundmc_mod.f90:123-365)
+ *   champ_dmc_init/champ_dmc_steps <-> rundmc walker/electron loops, split_join
+ *                          (qmc/rundmc_mod.f90:123-365)
  *   champ_param_grad  <->  dpsi_bld / deloc_bld (qmc/deriv_mod.f90:248,437)
  *   champ_accumulate_oh <-> dpsi_dpsi / dpsi_deloc / dpsi_dpsi_eloc averages
  *                          (qmc/deriv_mod.f90:683,1375,898)
@@ -202,7 +203,19 @@ int champ_param_grad(champ_ctx *ctx, double *dlnpsi /* [nw][P] */, double *deloc
    S[a][b] = sum_w wt_w Oa_a Oa_b and H[a][b] = sum_w wt_w Oa_a Mb_b, row-major (P+1)x(P+1), in FP64. */
 int champ_accumulate_oh(champ_ctx *ctx, const double *weights /* [nw] or NULL */, double *S, double *H);
 
+/* Diffusion Monte Carlo (rundmc, qmc/rundmc_mod.f90:17-422).  champ_dmc_init starts from the
+   current walkers (weight 1); w_target is the target population and the trial energy follows
+   E_T = E_est - ln(W / w_target) / (gpop * tau).  The population may range up to w_max.
+   champ_dmc_steps runs nstep steps (drift-diffusion moves with the Green's-function acceptance
+   of green_functions_mod.f90, E_L, reweighting, branching) without host synchronisation and
+   returns per step {population, sum w, sum w E_L, E_T} in stats (host [nstep][4] or NULL).
+   Afterwards the context's walker count is the new population. */
+int champ_dmc_init(champ_ctx *ctx, int32_t w_target, double tau, double gpop);
+int champ_dmc_steps(champ_ctx *ctx, int32_t nstep, uint64_t seed, double *stats);
+
 int champ_walker_status(champ_ctx *ctx, uint32_t *flags /* [nw] */);
+/* Current number of walkers (changes with DMC branching). */
+int champ_num_walkers(const champ_ctx *ctx, int32_t *nw);
 int champ_synchronize(champ_ctx *ctx);
 
 #ifdef __cplusplus

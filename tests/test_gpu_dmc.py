@@ -1,0 +1,50 @@
+"""Diffusion Monte Carlo on the GPU (champ_dmc_init / champ_dmc_steps).
+
+The Be example wave function of the reference (4 determinants) has a VMC energy of
+-14.6463 +- 0.0076 Ha in the reference transcript; its fixed-node DMC energy must lie below
+that and above the exact non-relativistic Be energy (-14.66736 Ha) within error bars.  The
+population is controlled around its target; FP64 and mixed precision agree statistically.
+"""
+import numpy as np
+import pytest
+
+from champ_b200 import system as S
+
+pytestmark = pytest.mark.gpu
+
+E_EXACT_BE = -14.66736
+
+
+def run_dmc(system, prec, target, tau, neq, nacc, seed=5, wmax=None):
+    from champ_b200.engine import Engine
+    eng = Engine(system, wmax or 2 * target, prec)
+    eng.set_walkers(S.initial_walkers(system, target, seed=seed))
+    eng.vmc_sweeps(50, seed=seed, sweep0=0, step=0.4, stats=False)
+    eng.dmc_init(target, tau)
+    eng.dmc_steps(neq, seed=seed + 1)
+    st = eng.dmc_steps(nacc, seed=seed + 2)
+    return eng, st
+
+
+def block_energy(st, nblock=20):
+    e = np.array([b[:, 2].sum() / b[:, 1].sum() for b in np.array_split(st, nblock)])
+    return e.mean(), e.std(ddof=1) / np.sqrt(len(e))
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_dmc_be_example_energy(prec):
+    eng, st = run_dmc(S.be_example(), prec, target=4096, tau=0.01, neq=300, nacc=1000)
+    e, err = block_energy(st)
+    print(f"DMC Be example ({prec}): E = {e:.5f} +- {err:.5f} Ha, population {st[:, 0].min():.0f}..{st[:, 0].max():.0f}")
+    pop = st[:, 0]
+    assert pop.min() > 0.5 * 4096 and pop.max() < 2 * 4096, (pop.min(), pop.max())
+    assert e < -14.6463 - 0.005, (e, err)
+    assert e > E_EXACT_BE - 4 * err - 0.002, (e, err)
+    assert not eng.walker_status().any()
+
+
+def test_dmc_c2_population_and_energies_finite():
+    eng, st = run_dmc(S.c2_dmc(), "mixed", target=8192, tau=0.01, neq=20, nacc=40, wmax=24576)
+    assert np.all(np.isfinite(st))
+    assert st[:, 0].min() > 0.3 * 8192 and st[:, 0].max() <= 24576
+    assert eng.population() == eng.get_walkers().shape[0]

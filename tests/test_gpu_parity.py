@@ -167,6 +167,8 @@ def test_vmc_be_example_matches_reference_transcript(prec):
     e_w = st["esum"] / ns
     e, err = e_w.mean(), e_w.std(ddof=1) / np.sqrt(nw)
     sigma = np.sqrt(st["e2sum"].sum() / (nw * ns) - (st["esum"].sum() / (nw * ns)) ** 2)
+    print(f"VMC Be example ({prec}): E = {e:.5f} +- {err:.5f} Ha, sigma {sigma:.4f}; reference "
+          f"{ref['energy']} +- {ref['energy_err']}")
     assert abs(e - ref["energy"]) < 3.5 * np.hypot(err, ref["energy_err"]), (e, err)
     # the all-electron E_L has heavy tails near the nucleus; sigma's sampling error is large
     assert abs(sigma - ref["sigma"]) < 0.05, sigma
