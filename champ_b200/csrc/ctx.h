@@ -109,6 +109,8 @@ struct OpArgs {
   double step = 0;
   PGOut pgout;
   int istep = 0;
+  const void *st_override = nullptr;  // State<T> to use instead of the context's (and its walker count)
+  int nw_override = 0;
 };
 
 

@@ -458,6 +458,108 @@ static int alloc_state_copy(champ_ctx *c, const State<T> &a, State<T> &b) {
 
 static const int DMC_STAT_CAP = 1 << 16;
 
+// ---------------------------------------------------------------------------------------
+// Evaluation without allocation.  Some callers cannot call cudaMalloc: host codes whose
+// device memory is entirely owned by their own pool allocator, or that must not pay for an
+// allocation (and its implicit synchronisation) inside a time-critical loop.  For them
+// champ_eval_energy_noalloc takes the walkers and the output as device buffers the caller
+// owns, and keeps every per-walker intermediate in the fixed array below.  The array is a
+// file-scope device variable: every GPU that loads this library holds it until the process
+// exits, and every call shares it.
+// ---------------------------------------------------------------------------------------
+static constexpr size_t NOALLOC_BYTES = (size_t)16 << 20;  // 16 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
+
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_ptr[256];  // device address of g_noalloc_scratch, per device ordinal
+
+// Device address of the scratch array for the current device, looked up once per device.
+static int noalloc_scratch(void **out) {
+  int dev = -1;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) return fail(CHAMP_ECUDA, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(CHAMP_ECUDA, std::string("cudaGetSymbolAddress of the scratch array: ") + cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return CHAMP_OK;
+}
+
+// Carves a State<T> for nw walkers out of the scratch array (256-byte aligned pieces).
+// Returns the bytes used, or 0 if they do not fit.
+template <class T>
+static size_t noalloc_carve(const champ_ctx *c, const State<T> &ref, int nw, char *base, double *eloc, State<T> &st) {
+  size_t o = 0;
+  auto take = [&](size_t bytes) -> char * {
+    char *p = base + o;
+    o += (bytes + 255) & ~(size_t)255;
+    return p;
+  };
+  const size_t W = nw, N = c->N, C = c->C, B = c->nbasis, nm = c->nomax;
+  st = ref;
+  st.x = (double *)take(sizeof(double) * W * N * 3);
+  st.ainv = (double *)take(sizeof(double) * W * ref.astride);
+  st.fso = (T *)take(sizeof(T) * W * N * N);
+  st.ren = (T *)take(sizeof(T) * W * N * C * 2);
+  st.fsum = (double *)take(sizeof(double) * W);
+  st.lnd = (double *)take(sizeof(double) * W);
+  st.sgn = (double *)take(sizeof(double) * W);
+  st.status = (uint32_t *)take(sizeof(uint32_t) * W);
+  st.pf = (T *)take(sizeof(T) * W * N);
+  st.pa = (double *)take(sizeof(double) * W * nm);
+  st.pdj = (double *)take(sizeof(double) * W);
+  st.prho = (double *)take(sizeof(double) * W);
+  st.pxn = (double *)take(sizeof(double) * W * 3);
+  st.piel = (int *)take(sizeof(int) * W);
+  st.orb5 = (T *)take(sizeof(T) * W * N * 5 * nm);
+  st.gproj = c->nloc > 0 ? (T *)take(sizeof(T) * W * N * B) : nullptr;
+  st.nlt = c->nloc > 0 ? (double *)take(sizeof(double) * W * N * C * NLT) : nullptr;
+  st.tv = (double *)take(sizeof(double) * W * ref.tvstride);
+  st.gam = (double *)take(sizeof(double) * W * ref.gstride);
+  st.ymd = (double *)take(sizeof(double) * W * ref.tvstride);
+  st.wdet = (double *)take(sizeof(double) * W * ref.wstride);
+  st.o_lnpsi = (double *)take(sizeof(double) * W);
+  st.o_sign = (double *)take(sizeof(double) * W);
+  st.o_psij = (double *)take(sizeof(double) * W);
+  st.o_vel = (double *)take(sizeof(double) * W * N * 3);
+  st.o_divv = (double *)take(sizeof(double) * W * N);
+  st.o_d2 = (double *)take(sizeof(double) * W);
+  st.o_pe = (double *)take(sizeof(double) * W);
+  st.o_peee = (double *)take(sizeof(double) * W);
+  st.o_penl = (double *)take(sizeof(double) * W);
+  st.o_eloc = eloc;  // written straight into the caller's buffer
+  return o <= NOALLOC_BYTES ? o : 0;
+}
+
+template <class T>
+static int eval_noalloc_t(champ_ctx *c, const State<T> &ref, int32_t nw, const double *x, double *eloc) {
+  void *scr = nullptr;
+  int rc = noalloc_scratch(&scr);
+  if (rc) return rc;
+  State<T> st;
+  if (!noalloc_carve<T>(c, ref, nw, (char *)scr, eloc, st)) {
+    State<T> one;
+    size_t per = noalloc_carve<T>(c, ref, 1, (char *)scr, eloc, one);
+    return fail(CHAMP_EINVAL, "champ_eval_energy_noalloc: " + std::to_string(nw) + " walkers need more than the " +
+                                  std::to_string(NOALLOC_BYTES >> 20) + " MiB scratch array (at most " +
+                                  std::to_string(per ? NOALLOC_BYTES / per : 0) + " walkers of this system)");
+  }
+  // the kernel writes the walkers back after its shared-memory pass, so it works on a copy
+  CK(cudaMemcpyAsync(st.x, x, sizeof(double) * (size_t)nw * c->N * 3, cudaMemcpyDeviceToDevice, c->stream));
+  OpArgs a;
+  a.st_override = &st;
+  a.nw_override = nw;
+  rc = launch(c, Op::EvalOut, a);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  return CHAMP_OK;
+}
+
 extern "C" {
 
 const char *champ_last_error(void) { return g_err.c_str(); }
@@ -968,6 +1070,13 @@ int champ_walker_status(champ_ctx *c, uint32_t *flags) {
   CK(cudaMemcpyAsync(flags, s, sizeof(uint32_t) * c->W, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return CHAMP_OK;
+}
+
+int champ_eval_energy_noalloc(champ_ctx *c, int32_t nw, const double *x, double *eloc) {
+  if (!c || !x || !eloc) return fail(CHAMP_EINVAL, "null argument");
+  if (nw < 1) return fail(CHAMP_EINVAL, "nw < 1");
+  return c->prec == CHAMP_PREC_FP64 ? eval_noalloc_t<double>(c, c->std_, nw, x, eloc)
+                                    : eval_noalloc_t<float>(c, c->stf, nw, x, eloc);
 }
 
 int champ_num_walkers(const champ_ctx *c, int32_t *nw) {

@@ -28,9 +28,9 @@ static int set_smem_attrs(champ_ctx *c) {
 template <class T, int NORD, bool MD>
 static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
   Sys<T> &s = sysof<T>(c);
-  State<T> st = stof<T>(c);
-  st.W = c->W;
-  dim3 grid(nblocks(c)), block(32 * c->wpb);
+  State<T> st = a.st_override ? *(const State<T> *)a.st_override : stof<T>(c);
+  st.W = a.st_override ? a.nw_override : c->W;
+  dim3 grid((st.W + c->wpb - 1) / c->wpb), block(32 * c->wpb);
   const double *R = c->rot;
   switch (op) {
   case Op::Eval:

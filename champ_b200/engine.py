@@ -22,7 +22,7 @@ EXPORTED_SYMBOLS = [
     "champ_set_walkers", "champ_get_walkers", "champ_set_quadrature_rotation", "champ_eval_full",
     "champ_propose_1e", "champ_accept_1e", "champ_grad_1e", "champ_vmc_sweeps", "champ_vmc_run_host",
     "champ_walker_status", "champ_synchronize", "champ_param_grad", "champ_accumulate_oh",
-    "champ_dmc_init", "champ_dmc_steps", "champ_num_walkers",
+    "champ_dmc_init", "champ_dmc_steps", "champ_num_walkers", "champ_eval_energy_noalloc",
 ]
 
 PREC = {"fp64": 0, "mixed": 1}
@@ -73,6 +73,7 @@ def load_library(path: str = LIB_PATH):
     L.champ_dmc_init.argtypes = [vp, i32, C.c_double, C.c_double]
     L.champ_dmc_steps.argtypes = [vp, i32, u64, dp]
     L.champ_num_walkers.argtypes = [vp, C.POINTER(i32)]
+    L.champ_eval_energy_noalloc.argtypes = [vp, i32, vp, vp]
     for n in EXPORTED_SYMBOLS:
         if n not in ("champ_last_error", "champ_version"):
             getattr(L, n).restype = C.c_int

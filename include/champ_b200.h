@@ -216,6 +216,18 @@ int champ_dmc_steps(champ_ctx *ctx, int32_t nstep, uint64_t seed, double *stats)
 int champ_walker_status(champ_ctx *ctx, uint32_t *flags /* [nw] */);
 /* Current number of walkers (changes with DMC branching). */
 int champ_num_walkers(const champ_ctx *ctx, int32_t *nw);
+
+/* Local energy without allocation (no counterpart in the reference: an addition for callers
+   that cannot allocate device memory, such as host codes whose GPU memory is wholly owned by
+   their own pool allocator or that must not allocate inside a time-critical loop).
+   x and eloc are DEVICE pointers the caller owns (x[nw][nelec][3], eloc[nw]); E_L is
+   evaluated as champ_eval_full does, on the context's stream, with the quadrature rotation
+   of champ_set_quadrature_rotation.  Intermediates live in one fixed 16 MiB device array
+   compiled into the library: nw beyond what fits returns CHAMP_EINVAL with the limit in
+   champ_last_error().  The first call on a device looks the array's address up.  The call
+   makes no device allocation; it leaves the context's walkers untouched.  All calls share the
+   array, so calls that overlap on the GPU (other streams, other contexts on the device) race. */
+int champ_eval_energy_noalloc(champ_ctx *ctx, int32_t nw, const double *x, double *eloc);
 int champ_synchronize(champ_ctx *ctx);
 
 #ifdef __cplusplus
