@@ -326,7 +326,7 @@ def c2_dmc(seed=1004) -> System:
     return s
 
 
-def cluster128(seed=1005, ncent=32, box=14.0, dmin=2.5, norb=80) -> System:
+def cluster128(seed=1005, ncent=32, box=14.0, dmin=2.5, norb=96) -> System:
     """System 5: 32 pseudo-atoms (Z_eff=4) uniform in a 14-bohr cube with minimum separation
     2.5 bohr, 64+64 electrons, 13 contracted Gaussians per centre (2s 2p 1d)."""
     rng = np.random.default_rng(seed)
