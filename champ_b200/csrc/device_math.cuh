@@ -409,6 +409,98 @@ __host__ __device__ constexpr Terms make_terms(int nord) {
   return t;
 }
 
+// The e-e-n value sum over centres, for one pair (i, j), rewritten as
+//   sum_c sum_klm c_klm u^k (a_c^l + r_c^l)(a_c r_c)^m = sum_klm c_klm u^k [X(l+m, m) + X(m, l+m)],
+//   X(p, q) = sum_c a_c^p r_c^q,  a_c = 1/(1+k r_ic), r_c = 1/(1+k r_jc)  (switched distances),
+// with X(p, 0) depending only on electron i and X(0, q) only on electron j: per centre only the
+// products with p, q >= 1 remain.  Valid when all centres share one type (one c set).
+struct MixedPQ {
+  int n;
+  int p[40], q[40];
+};
+__host__ __device__ constexpr MixedPQ make_mixed(int nord) {
+  MixedPQ x{};
+  Terms t = make_terms(nord);
+  for (int ll = 0; ll < t.n; ll++) {
+    int l = t.l[ll], m = t.m[ll];
+    int pp[2] = {l + m, m}, qq[2] = {m, l + m};
+    for (int s2 = 0; s2 < 2; s2++) {
+      if (pp[s2] == 0 || qq[s2] == 0) continue;
+      bool seen = false;
+      for (int i = 0; i < x.n; i++)
+        if (x.p[i] == pp[s2] && x.q[i] == qq[s2]) seen = true;
+      if (!seen) { x.p[x.n] = pp[s2]; x.q[x.n] = qq[s2]; x.n++; }
+    }
+  }
+  return x;
+}
+__host__ __device__ constexpr int mixed_index(const MixedPQ &x, int p, int q) {
+  for (int i = 0; i < x.n; i++)
+    if (x.p[i] == p && x.q[i] == q) return i;
+  return -1;
+}
+
+// X sums of one pair: a[2c+1] = a_c (stride 2), r[2c+1] = r_c; mixed products only.
+template <class T, int NORD>
+__device__ __forceinline__ void een_xsums(int C, const T *a, const T *r, T *X) {
+  constexpr MixedPQ mx = make_mixed(NORD);
+#pragma unroll
+  for (int i = 0; i < mx.n; i++) X[i] = T(0);
+  for (int c = 0; c < C; c++) {
+    T ac = a[2 * c + 1], rc = r[2 * c + 1];
+    T ap[NORD + 1], rp[NORD + 1];
+    ap[0] = rp[0] = T(1);
+#pragma unroll
+    for (int q = 1; q <= NORD; q++) { ap[q] = ap[q - 1] * ac; rp[q] = rp[q - 1] * rc; }
+#pragma unroll
+    for (int i = 0; i < mx.n; i++) X[i] += ap[mx.p[i]] * rp[mx.q[i]];
+  }
+}
+
+// Per term, where its two X factors come from: code < 100 -> mixed sum X[code],
+// 100 + p -> ai[p] (sum over centres of a_c^p), 200 + q -> rj[q] (sum of r_c^q).
+struct XIdx {
+  int a1[64], a2[64];
+};
+__host__ __device__ constexpr XIdx make_xidx(int nord) {
+  XIdx x{};
+  Terms t = make_terms(nord);
+  MixedPQ mx = make_mixed(nord);
+  for (int ll = 0; ll < t.n; ll++) {
+    int l = t.l[ll], m = t.m[ll];
+    int pp[2] = {l + m, m}, qq[2] = {m, l + m};
+    for (int s2 = 0; s2 < 2; s2++) {
+      int code = 0;
+      if (qq[s2] == 0) code = 100 + pp[s2];
+      else if (pp[s2] == 0) code = 200 + qq[s2];
+      else code = mixed_index(mx, pp[s2], qq[s2]);
+      if (s2 == 0) x.a1[ll] = code; else x.a2[ll] = code;
+    }
+  }
+  return x;
+}
+
+template <class T>
+__device__ __forceinline__ T xsel(int code, const T *ai, const T *rj, const T *X) {
+  return code >= 200 ? rj[code - 200] : (code >= 100 ? ai[code - 100] : X[code]);
+}
+
+// e-e-n value of one pair from its X sums (jastrow4.f90:211-257 summed over centres)
+template <class T, int NORD>
+__device__ __forceinline__ T een_from_x(const T *c, T du, const T *ai, const T *rj, const T *X) {
+  constexpr Terms tl = make_terms(NORD);
+  constexpr XIdx xi = make_xidx(NORD);
+  T uu[NORD + 1];
+  uu[0] = T(1);
+#pragma unroll
+  for (int q = 1; q <= NORD; q++) uu[q] = uu[q - 1] * du;
+  T f = 0;
+#pragma unroll
+  for (int ll = 0; ll < tl.n; ll++)
+    f += c[ll] * uu[tl.k[ll]] * (xsel(xi.a1[ll], ai, rj, X) + xsel(xi.a2[ll], ai, rj, X));
+  return f;
+}
+
 // spin class of pair (i,j): parallel spins use b set 2 (nspin2b=2) or 1/2 on b1.
 template <class T>
 __device__ __forceinline__ void pair_class(const JasPar<T> &J, int nup, int i, int j, int &isb, T &ss, int &ipar) {

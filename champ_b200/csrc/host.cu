@@ -382,6 +382,7 @@ static int build_state(champ_ctx *c, State<T> &st) {
   st.ainv = dalloc<double>(c, W * st.astride);
   st.fso = dalloc<T>(c, W * N * N);
   st.ren = dalloc<T>(c, W * N * c->C * 2);
+  st.zq = dalloc<T>(c, W * N * ZQ);
   st.fsum = dalloc<double>(c, W); st.lnd = dalloc<double>(c, W); st.sgn = dalloc<double>(c, W);
   st.status = dalloc<uint32_t>(c, W);
   st.pf = dalloc<T>(c, W * N);
@@ -402,7 +403,7 @@ static int build_state(champ_ctx *c, State<T> &st) {
   st.o_eloc = dalloc<double>(c, W);
   st.s_esum = dalloc<double>(c, W); st.s_e2sum = dalloc<double>(c, W); st.s_acc = dalloc<double>(c, W);
   st.s_elast = dalloc<double>(c, W);
-  if (!st.x || !st.ainv || !st.fso || !st.ren || !st.orb5 || !st.s_elast || (c->nloc > 0 && (!st.gproj || !st.nlt)))
+  if (!st.x || !st.ainv || !st.fso || !st.ren || !st.zq || !st.orb5 || !st.s_elast || (c->nloc > 0 && (!st.gproj || !st.nlt)))
     return fail(CHAMP_ENOMEM, "device allocation of the walker state failed");
   return CHAMP_OK;
 }
@@ -446,12 +447,13 @@ static int alloc_state_copy(champ_ctx *c, const State<T> &a, State<T> &b) {
   b.ainv = dalloc<double>(c, W * a.astride);
   b.fso = dalloc<T>(c, W * N * N);
   b.ren = dalloc<T>(c, W * N * c->C * 2);
+  b.zq = dalloc<T>(c, W * N * ZQ);
   b.tv = dalloc<double>(c, W * a.tvstride);
   b.gam = dalloc<double>(c, W * a.gstride);
   b.fsum = dalloc<double>(c, W);
   b.lnd = dalloc<double>(c, W);
   b.sgn = dalloc<double>(c, W);
-  if (!b.x || !b.ainv || !b.fso || !b.ren || !b.tv || !b.gam || !b.fsum || !b.lnd || !b.sgn)
+  if (!b.x || !b.ainv || !b.fso || !b.ren || !b.zq || !b.tv || !b.gam || !b.fsum || !b.lnd || !b.sgn)
     return fail(CHAMP_ENOMEM, "allocation of the DMC state buffer failed");
   return CHAMP_OK;
 }
@@ -506,6 +508,7 @@ static size_t noalloc_carve(const champ_ctx *c, const State<T> &ref, int nw, cha
   st.ainv = (double *)take(sizeof(double) * W * ref.astride);
   st.fso = (T *)take(sizeof(T) * W * N * N);
   st.ren = (T *)take(sizeof(T) * W * N * C * 2);
+  st.zq = (T *)take(sizeof(T) * W * N * ZQ);
   st.fsum = (double *)take(sizeof(double) * W);
   st.lnd = (double *)take(sizeof(double) * W);
   st.sgn = (double *)take(sizeof(double) * W);

@@ -33,6 +33,7 @@ struct State {
   double *ainv;    // [W][astride]; spin-up block at 0 (nup x nup), spin-down at nup*nup
   T *fso;          // [W][N][N]
   T *ren;          // [W][N][C][2]: r_en and 1/(1 + scalek r_en)
+  T *zq;           // [W][N][ZQ]: sum_c (1/(1 + scalek r_en))^q, q = 0..7
   double *fsum, *lnd, *sgn;
   uint32_t *status;
   T *pf;           // [W][N] proposed pair values
@@ -53,13 +54,15 @@ struct State {
   double *s_esum, *s_e2sum, *s_acc, *s_elast;
 };
 constexpr int NLT = 2 + MAXLCH;  // task record: (e*C+c), r, vps[0..MAXLCH-1]
+constexpr int ZQ = 8;            // stride of the per-electron power sums zq
+constexpr int MAXC_NL = 64;      // centres for the value-only e-e-n fast path
 
 // Per-warp shared-memory layout, computed on the host.  When `resident` is set the
 // walker's whole state and scratch live in shared memory for the life of a kernel
 // (small systems); otherwise they stay in HBM.
 struct Layout {
-  size_t phi, arow, xs, vacc, divj, colb, vb, perm, rnew;  // always in shared memory
-  size_t ainv, fso, ren, pf, orb5, gproj, nlt, tv, gam, ymd, wdet;  // resident mode only
+  size_t phi, arow, xs, vacc, divj, colb, vb, perm, rnew, asum;  // always in shared memory
+  size_t ainv, fso, ren, zq, pf, orb5, gproj, nlt, tv, gam, ymd, wdet;  // resident mode only
   size_t bytes, base;  // total bytes per warp; bytes of the always-shared part
   int resident;
 };
@@ -71,8 +74,9 @@ struct View {
   double *xs, *vacc, *divj, *colb, *vb;
   int *perm;
   T *rnew;         // [C][2] proposed electron's distances to the centres
+  T *asum;         // [ZQ] power sums of the proposed electron
   double *ainv;
-  T *fso, *ren, *pf, *orb5, *gproj;
+  T *fso, *ren, *zq, *pf, *orb5, *gproj;
   double *nlt, *tv, *gam, *ymd, *wdet;
 };
 
@@ -93,10 +97,12 @@ static Layout make_layout(int N, int C, int nbasis, int nmax, int nomax, int ast
   L.vb = take(sizeof(double) * nmax);
   L.perm = take(sizeof(int) * nmax);
   L.rnew = take(sizeof(T) * C * 2);
+  L.asum = take(sizeof(T) * ZQ);
   size_t base = o;
   L.ainv = take(sizeof(double) * astride);
   L.fso = take(sizeof(T) * N * N);
   L.ren = take(sizeof(T) * N * C * 2);
+  L.zq = take(sizeof(T) * N * ZQ);
   L.pf = take(sizeof(T) * N);
   L.orb5 = take(sizeof(T) * N * 5 * nomax);
   L.gproj = nl ? take(sizeof(T) * N * nbasis) : 0;
@@ -124,10 +130,12 @@ __device__ inline View<T> make_view(char *base, const Layout &L, const State<T> 
   v.vb = (double *)(base + L.vb);
   v.perm = (int *)(base + L.perm);
   v.rnew = (T *)(base + L.rnew);
+  v.asum = (T *)(base + L.asum);
   if (resident) {
     v.ainv = (double *)(base + L.ainv);
     v.fso = (T *)(base + L.fso);
     v.ren = (T *)(base + L.ren);
+    v.zq = (T *)(base + L.zq);
     v.pf = (T *)(base + L.pf);
     v.orb5 = (T *)(base + L.orb5);
     v.gproj = (T *)(base + L.gproj);
@@ -140,6 +148,7 @@ __device__ inline View<T> make_view(char *base, const Layout &L, const State<T> 
     v.ainv = st.ainv + (size_t)w * st.astride;
     v.fso = st.fso + (size_t)w * N * N;
     v.ren = st.ren + (size_t)w * N * C * 2;
+    v.zq = st.zq + (size_t)w * N * ZQ;
     v.pf = st.pf + (size_t)w * N;
     v.orb5 = st.orb5 + (size_t)w * N * 5 * nomax;
     v.gproj = st.gproj ? st.gproj + (size_t)w * N * nbasis : nullptr;
@@ -159,6 +168,7 @@ __device__ inline void view_load(const View<T> &v, const State<T> &st, int w, in
   for (int i = lane; i < st.astride; i += 32) v.ainv[i] = st.ainv[(size_t)w * st.astride + i];
   for (int i = lane; i < N * N; i += 32) v.fso[i] = st.fso[(size_t)w * N * N + i];
   for (int i = lane; i < N * C * 2; i += 32) v.ren[i] = st.ren[(size_t)w * N * C * 2 + i];
+  for (int i = lane; i < N * ZQ; i += 32) v.zq[i] = st.zq[(size_t)w * N * ZQ + i];
   for (int i = lane; i < st.tvstride; i += 32) v.tv[i] = st.tv[(size_t)w * st.tvstride + i];
   for (int i = lane; i < st.gstride; i += 32) v.gam[i] = st.gam[(size_t)w * st.gstride + i];
   __syncwarp();
@@ -170,6 +180,7 @@ __device__ inline void view_store(const View<T> &v, const State<T> &st, int w, i
   for (int i = lane; i < st.astride; i += 32) st.ainv[(size_t)w * st.astride + i] = v.ainv[i];
   for (int i = lane; i < N * N; i += 32) st.fso[(size_t)w * N * N + i] = v.fso[i];
   for (int i = lane; i < N * C * 2; i += 32) st.ren[(size_t)w * N * C * 2 + i] = v.ren[i];
+  for (int i = lane; i < N * ZQ; i += 32) st.zq[(size_t)w * N * ZQ + i] = v.zq[i];
   for (int i = lane; i < st.tvstride; i += 32) st.tv[(size_t)w * st.tvstride + i] = v.tv[i];
   for (int i = lane; i < st.gstride; i += 32) st.gam[(size_t)w * st.gstride + i] = v.gam[i];
   __syncwarp();
@@ -278,7 +289,8 @@ __device__ __forceinline__ void cen_dist(const Sys<T> &s, T sk, const double *p,
 // electron j at xj (distances rj[c][2]); gradient wrt xe if GRAD.
 template <class T, int NORD, bool GRAD>
 __device__ __forceinline__ T pair_value(const Sys<T> &s, const JasPar<T> &J, int e, int j, const double *xe,
-                                        const T *re, const double *xj, const T *rj, T *g) {
+                                        const T *re, const double *xj, const T *rj, T *g, const T *ae = nullptr,
+                                        const T *zj = nullptr) {
   int isb, ipar;
   T ss;
   pair_class(J, s.nup, e, j, isb, ss, ipar);
@@ -288,7 +300,12 @@ __device__ __forceinline__ T pair_value(const Sys<T> &s, const JasPar<T> &J, int
   T fu = 0, fuu = 0;
   T f = jas_ee<T, GRAD>(J, isb, ss, ipar, rij, du, fu, fuu);
   if (GRAD) { g[0] = fu * rv[0]; g[1] = fu * rv[1]; g[2] = fu * rv[2]; }
-  if (NORD > 1) {
+  if (NORD > 1 && !GRAD && J.nct == 1 && s.C <= MAXC_NL) {
+    // value only, one centre type: X sums (see een_xsums)
+    T X[make_mixed(NORD).n > 0 ? make_mixed(NORD).n : 1];
+    een_xsums<T, NORD>(s.C, re, rj, X);
+    f += een_from_x<T, NORD>(J.c[0], du, ae, zj, X);
+  } else if (NORD > 1) {
     for (int c = 0; c < s.C; c++) {
       Een<T> o;
       jas_een<T, NORD, GRAD ? 1 : 0>(J, s.ctype[c], rij, du, re[2 * c], re[2 * c + 1], rj[2 * c], rj[2 * c + 1], o);
@@ -469,6 +486,17 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
     cen_dist(s, sk, xs + 3 * e, c, r, d);
     v.ren[2 * i] = r;
     v.ren[2 * i + 1] = d;
+  }
+  __syncwarp();
+  for (int e = lane; e < N; e += 32) {
+    T z[ZQ];
+    z[0] = T(C);
+    for (int q = 1; q < ZQ; q++) z[q] = T(0);
+    for (int c = 0; c < C; c++) {
+      T d = v.ren[2 * (e * C + c) + 1], p = d;
+      for (int q = 1; q < ZQ; q++) { z[q] += p; p *= d; }
+    }
+    for (int q = 0; q < ZQ; q++) v.zq[e * ZQ + q] = z[q];
   }
   for (int i = lane; i < 3 * N; i += 32) v.vacc[i] = 0;
   for (int i = lane; i < N; i += 32) v.divj[i] = 0;
@@ -693,8 +721,26 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
       const T *ge = gp + (size_t)e * B;
       T dr = 0;
       for (int ish = 0; ish < s.nshell; ish++) dr += shell_dot<T>(s, ish, xn, ge);
-      // Jastrow ratio (nonlocj, nonloc.f90:432-522)
+      // Jastrow ratio (nonlocj, nonloc.f90:432-522): point-centre distances once per point
       double dj = 0;
+      const bool fast = (NORD > 1) && J.nct == 1 && C <= MAXC_NL;
+      T pr[2 * MAXC_NL], asum[ZQ];
+      {
+        T f = 0;
+        for (int q2 = 0; q2 < ZQ; q2++) asum[q2] = (q2 == 0) ? T(C) : T(0);
+        for (int c2 = 0; c2 < C; c2++) {
+          T ri, di, fi, fii;
+          cen_dist(s, sk, xn, c2, ri, di);
+          f += jas_en<T, false>(J, s.ctype[c2], ri, di, fi, fii);
+          if (fast) {
+            pr[2 * c2] = ri;
+            pr[2 * c2 + 1] = di;
+            T p = di;
+            for (int q2 = 1; q2 < ZQ; q2++) { asum[q2] += p; p *= di; }
+          }
+        }
+        dj += (double)f - (double)fso[e * N + e];
+      }
       for (int j = 0; j < N; j++) {
         if (j == e) continue;
         int isb, ipar;
@@ -706,7 +752,11 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
         T du = T(1) / (T(1) + sk * rij);
         T fu, fuu;
         T f = jas_ee<T, false>(J, isb, ss, ipar, rij, du, fu, fuu);
-        if (NORD > 1) {
+        if (fast) {
+          T X[make_mixed(NORD).n > 0 ? make_mixed(NORD).n : 1];
+          een_xsums<T, NORD>(C, pr, v.ren + 2 * C * j, X);
+          f += een_from_x<T, NORD>(J.c[0], du, asum, v.zq + ZQ * j, X);
+        } else if (NORD > 1) {
           const T *rj_ = v.ren + 2 * C * j;
           for (int c2 = 0; c2 < C; c2++) {
             T ri, di;
@@ -717,15 +767,6 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
           }
         }
         dj += (double)f - (double)fso[e * N + j];
-      }
-      {
-        T f = 0;
-        for (int c2 = 0; c2 < C; c2++) {
-          T ri, di, fi, fii;
-          cen_dist(s, sk, xn, c2, ri, di);
-          f += jas_en<T, false>(J, s.ctype[c2], ri, di, fi, fii);
-        }
-        dj += (double)f - (double)fso[e * N + e];
       }
       int it = s.ctype[c];
       double vp = 0;
@@ -803,6 +844,13 @@ __device__ void propose(const Sys<T> &s, const JasPar<T> &J, const State<T> &st,
     v.rnew[2 * c] = r;
     v.rnew[2 * c + 1] = d;
   }
+  __syncwarp();
+  if (lane < ZQ) {
+    T z = (lane == 0) ? T(C) : T(0);
+    if (lane > 0)
+      for (int c = 0; c < C; c++) z += ipow(v.rnew[2 * c + 1], lane);
+    v.asum[lane] = z;
+  }
   warp_basis<T, NCH>(s, xn, v.phi, lane);
   warp_orbitals<T, NCH>(v.phi, s.cocc[sp], s.nbasis, no, v.arow, nomax, lane);
   // the wave function is linear in the moved electron's orbital row: ratio = sum_m G[m][e] phi_m
@@ -823,7 +871,8 @@ __device__ void propose(const Sys<T> &s, const JasPar<T> &J, const State<T> &st,
   for (int j = lane; j < N; j += 32) {
     if (j == e) continue;
     T g[3];
-    T f = pair_value<T, NORD, GRAD>(s, J, e, j, xn, v.rnew, v.xs + 3 * j, v.ren + 2 * C * j, g);
+    T f = pair_value<T, NORD, GRAD>(s, J, e, j, xn, v.rnew, v.xs + 3 * j, v.ren + 2 * C * j, g, v.asum,
+                                    v.zq + ZQ * j);
     d += (double)f - (double)fso[e * N + j];
     pf[j] = f;
     if (GRAD) { gj0 += g[0]; gj1 += g[1]; gj2 += g[2]; }
@@ -905,6 +954,7 @@ __device__ void accept_move(const Sys<T> &s, const State<T> &st, int w, const Vi
     fso[j * N + e] = f;
   }
   for (int i = lane; i < 2 * C; i += 32) v.ren[2 * C * e + i] = v.rnew[i];
+  for (int q = lane; q < ZQ; q += 32) v.zq[ZQ * e + q] = v.asum[q];
   if (lane < 3) v.xs[3 * e + lane] = xn[lane];
   if (lane == 0) {
     st.fsum[w] += dj;
@@ -1002,6 +1052,13 @@ __global__ void __launch_bounds__(128, 4) k_accept(Sys<T> s, State<T> st, Layout
       d = T(1) / (T(1) + (T)s.scalek * r);
       v.rnew[2 * c] = r;
       v.rnew[2 * c + 1] = d;
+    }
+    __syncwarp();
+    if (lane < ZQ) {
+      T z = (lane == 0) ? T(C) : T(0);
+      if (lane > 0)
+        for (int c = 0; c < C; c++) z += ipow(v.rnew[2 * c + 1], lane);
+      v.asum[lane] = z;
     }
     __syncwarp();
     accept_move<T, MD>(s, st, w, v, e, xn, st.pdj[w], st.prho[w], lane);

@@ -60,6 +60,28 @@ __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const Vi
   const int N = s.N, C = s.C;
   const T sk = J.scalek;
   constexpr Terms tl = make_terms(NORD);
+  const bool fast = (NORD > 1) && J.nct == 1 && C <= MAXC_NL;
+  T pr[2 * MAXC_NL], asum[ZQ];
+  for (int q = 0; q < ZQ; q++) asum[q] = (q == 0) ? T(C) : T(0);
+  for (int c = 0; c < C; c++) {
+    T r, d;
+    cen_dist(s, sk, xn, c, r, d);
+    int it = s.ctype[c];
+    for (int k = 2; k <= J.norda; k++) {
+      T t, t1, t2;
+      en_param_terms(J, r, d, k, t, t1, t2, false);
+      atomicAdd(&pg.dvn[it * (J.norda - 1) + (k - 2)], coeff * (double)t);
+    }
+    if (fast) {
+      pr[2 * c] = r;
+      pr[2 * c + 1] = d;
+      T p = d;
+      for (int q = 1; q < ZQ; q++) { asum[q] += p; p *= d; }
+    }
+  }
+  T tsum[tl.n > 0 ? tl.n : 1];
+#pragma unroll
+  for (int ll = 0; ll < tl.n; ll++) tsum[ll] = T(0);
   for (int j = 0; j < N; j++) {
     if (j == e) continue;
     int isb, ipar;
@@ -74,7 +96,19 @@ __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const Vi
       ee_param_terms(J, isb, ss, rij, du, k, t, t1, t2, false);
       atomicAdd(&pg.dvn[pg.na + isb * J.nordb + (k - 1)], coeff * (double)t);
     }
-    if (NORD > 1) {
+    if (fast) {
+      T X[make_mixed(NORD).n > 0 ? make_mixed(NORD).n : 1];
+      een_xsums<T, NORD>(C, pr, v.ren + 2 * C * j, X);
+      const T *zj = v.zq + ZQ * j;
+      constexpr XIdx xi = make_xidx(NORD);
+      T uu[NORD + 1];
+      uu[0] = T(1);
+#pragma unroll
+      for (int q = 1; q <= NORD; q++) uu[q] = uu[q - 1] * du;
+#pragma unroll
+      for (int ll = 0; ll < tl.n; ll++)
+        tsum[ll] += uu[tl.k[ll]] * (xsel(xi.a1[ll], asum, zj, X) + xsel(xi.a2[ll], asum, zj, X));
+    } else if (NORD > 1) {
       const T *rj_ = v.ren + 2 * C * j;
       for (int c = 0; c < C; c++) {
         T ri, di;
@@ -94,15 +128,10 @@ __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const Vi
       }
     }
   }
-  for (int c = 0; c < C; c++) {
-    T r, d;
-    cen_dist(s, sk, xn, c, r, d);
-    int it = s.ctype[c];
-    for (int k = 2; k <= J.norda; k++) {
-      T t, t1, t2;
-      en_param_terms(J, r, d, k, t, t1, t2, false);
-      atomicAdd(&pg.dvn[it * (J.norda - 1) + (k - 2)], coeff * (double)t);
-    }
+  if (fast) {
+    double *dst = pg.dvn + pg.na + pg.nb;
+#pragma unroll
+    for (int ll = 0; ll < tl.n; ll++) atomicAdd(&dst[ll], coeff * (double)tsum[ll]);
   }
 }
 
