@@ -58,6 +58,7 @@ struct Sys {
   int nocc[2], nvirt[2], nomax, nvmax;
   const T *cocc[2];     // [nbasis][nocc_s] orbital coefficients; rows in the internal basis
                         // order (each shell's functions in harmonic-slot order m = 0, 1, -1, ...)
+  const T *coccT[2];    // the same coefficients transposed, [nocc_s][nbasis]
   // multi-determinant tables (deriv_fast_mod.f90:261 excit_bld): unique determinants per
   // spin as excitations of the reference, and the (up, down, coefficient) combinations
   int multidet, ndet, ndu[2];

@@ -220,9 +220,11 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
   const MultiDet &md = c->md;
   T *cr0 = dalloc<T>(c, (size_t)c->nbasis * std::max(1, md.nocc[0]));
   T *cr1 = dalloc<T>(c, (size_t)c->nbasis * std::max(1, md.nocc[1]));
+  T *ct0 = dalloc<T>(c, (size_t)c->nbasis * std::max(1, md.nocc[0]));
+  T *ct1 = dalloc<T>(c, (size_t)c->nbasis * std::max(1, md.nocc[1]));
   JasPar<T> *jp = dalloc<JasPar<T>>(c, 1);
   EcpPar *ep = dalloc<EcpPar>(c, 1);
-  if (!cent || !ctype || !zc || !sh || !shp || !shb0 || !pz || !pc || !cr0 || !cr1 || !jp || !ep)
+  if (!cent || !ctype || !zc || !sh || !shp || !shb0 || !pz || !pc || !cr0 || !cr1 || !ct0 || !ct1 || !jp || !ep)
     return fail(CHAMP_ENOMEM, "device allocation of the system data failed");
   std::vector<double> zcv(c->C);
   for (int i = 0; i < c->C; i++) zcv[i] = d->znuc[d->iwctype[i]];
@@ -260,6 +262,10 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
       int o = md.occ[sp][k];
       for (int b = 0; b < c->nbasis; b++) crv[sp][(size_t)b * no + k] = (T)d->coef[(size_t)o * c->nbasis + perm_b[b]];
     }
+  }
+  if constexpr (std::is_same<T, float>::value) {
+    c->tc_coef[0] = crv[0];
+    c->tc_coef[1] = crv[1];
   }
   // determinant tables
   s.multidet = md.multidet;
@@ -362,10 +368,17 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
   CK(cudaMemcpy(pc, pcv.data(), sizeof(T) * nprim, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(cr0, crv[0].data(), sizeof(T) * crv[0].size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(cr1, crv[1].data(), sizeof(T) * crv[1].size(), cudaMemcpyHostToDevice));
+  for (int sp = 0; sp < 2; sp++) {
+    int no = std::max(1, md.nocc[sp]);
+    std::vector<T> tv((size_t)c->nbasis * no);
+    for (int b = 0; b < c->nbasis; b++)
+      for (int k = 0; k < no; k++) tv[(size_t)k * c->nbasis + b] = crv[sp][(size_t)b * no + k];
+    CK(cudaMemcpy(sp ? ct1 : ct0, tv.data(), sizeof(T) * tv.size(), cudaMemcpyHostToDevice));
+  }
   CK(cudaMemcpy(jp, &J, sizeof J, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(ep, &ecp, sizeof ecp, cudaMemcpyHostToDevice));
   s.cent = cent; s.ctype = ctype; s.zc = zc; s.shell = sh; s.shprim = shp; s.shb0 = shb0;
-  s.pz = pz; s.pc = pc; s.cocc[0] = cr0; s.cocc[1] = cr1; s.jas = jp; s.ecp = ep;
+  s.pz = pz; s.pc = pc; s.cocc[0] = cr0; s.cocc[1] = cr1; s.coccT[0] = ct0; s.coccT[1] = ct1; s.jas = jp; s.ecp = ep;
   return CHAMP_OK;
 }
 
@@ -563,6 +576,59 @@ static int eval_noalloc_t(champ_ctx *c, const State<T> &ref, int32_t nw, const d
   return CHAMP_OK;
 }
 
+// Tensor-core orbital contraction (orbtc.cuh): padded sizes, split coefficients, basis-row
+// buffer.  Left off (CUDA-core contraction) where unsupported or the buffer does not fit.
+static int tc_setup(champ_ctx *c) {
+  c->tc_on = c->tc_ok = 0;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev));
+  if (c->prec != CHAMP_PREC_MIXED || c->lay.resident) return CHAMP_OK;
+  if (std::max(c->md.nocc[0], c->md.nocc[1]) < 16) return CHAMP_OK;
+  const int B = c->nbasis, Kp = (B + orbtc::BK - 1) / orbtc::BK * orbtc::BK;
+  c->tc_Kp = Kp;
+  for (int sp = 0; sp < 2; sp++) {
+    const int no = c->md.nocc[sp];
+    if (no == 0 || (sp ? c->ndn : c->nup) == 0) continue;
+    const int Np = (std::max(no, 16) + 15) / 16 * 16;
+    int nc = 32;
+    while (nc < Np) nc <<= 1;
+    c->tc_Np[sp] = Np;
+    c->tc_ncols[sp] = nc;
+    int by_smem = (int)((227 * 1024) / (orbtc::smem_bytes(Np) + 1024)), by_tmem = 512 / nc;
+    c->tc_ctas_per_sm[sp] = std::max(1, std::min(std::min(by_smem, by_tmem), 4));
+    std::vector<float> hi((size_t)Np * Kp, 0.f), lo((size_t)Np * Kp, 0.f);
+    for (int m = 0; m < no; m++)
+      for (int b = 0; b < B; b++) {
+        float v = c->tc_coef[sp][(size_t)b * no + m], h = orbtc::tf32_hi(v);
+        hi[(size_t)m * Kp + b] = h;
+        lo[(size_t)m * Kp + b] = v - h;
+      }
+    c->tc_b[sp][0] = dalloc<float>(c, hi.size());
+    c->tc_b[sp][1] = dalloc<float>(c, lo.size());
+    if (!c->tc_b[sp][0] || !c->tc_b[sp][1]) return fail(CHAMP_ENOMEM, "device allocation failed");
+    CK(cudaMemcpy(c->tc_b[sp][0], hi.data(), sizeof(float) * hi.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->tc_b[sp][1], lo.data(), sizeof(float) * lo.size(), cudaMemcpyHostToDevice));
+  }
+  c->tc_err = dalloc<int>(c, 1);
+  c->tc_phi = dalloc<float>(c, (size_t)c->wmax * c->N * 5 * Kp);
+  if (!c->tc_err || !c->tc_phi) {
+    cudaGetLastError();
+    return CHAMP_OK;  // no room for the basis rows: the CUDA-core contraction stays in use
+  }
+  c->tc_ok = c->tc_on = 1;
+  return CHAMP_OK;
+}
+
+static int tc_check(champ_ctx *c) {
+  if (!c->tc_err) return CHAMP_OK;
+  int h = 0;
+  CK(cudaMemcpyAsync(&h, c->tc_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (h) return fail(CHAMP_ECUDA, "tensor-core orbital contraction gave up waiting for its MMA groups");
+  return CHAMP_OK;
+}
+
 extern "C" {
 
 const char *champ_last_error(void) { return g_err.c_str(); }
@@ -743,6 +809,7 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
     if (c->smem_pg > 220 * 1024) c->smem_pg = 0;  // parameter derivatives unavailable for this size
   }
   rc = c->prec == CHAMP_PREC_FP64 ? attrs_f64(c) : attrs_f32(c);
+  if (!rc) rc = tc_setup(c);
   if (rc) { champ_destroy(c); return rc; }
   c->d_in = dalloc<double>(c, (size_t)w_max * 3 * c->N);
   c->d_out = dalloc<double>(c, (size_t)w_max * 4 * c->N);
@@ -1072,7 +1139,19 @@ int champ_walker_status(champ_ctx *c, uint32_t *flags) {
   uint32_t *s = c->prec == CHAMP_PREC_FP64 ? c->std_.status : c->stf.status;
   CK(cudaMemcpyAsync(flags, s, sizeof(uint32_t) * c->W, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  return CHAMP_OK;
+  return tc_check(c);
+}
+
+int champ_set_option(champ_ctx *c, const char *name, int64_t value) {
+  if (!c || !name) return fail(CHAMP_EINVAL, "null argument");
+  if (!strcmp(name, "orbital_tc")) {
+    if (value && !c->tc_ok)
+      return fail(CHAMP_EINVAL, "orbital_tc: needs mixed precision, walker state in HBM, >= 16 orbitals of a spin "
+                                "and room for the basis rows");
+    c->tc_on = value ? 1 : 0;
+    return CHAMP_OK;
+  }
+  return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);
 }
 
 int champ_eval_energy_noalloc(champ_ctx *c, int32_t nw, const double *x, double *eloc) {
@@ -1091,7 +1170,7 @@ int champ_num_walkers(const champ_ctx *c, int32_t *nw) {
 int champ_synchronize(champ_ctx *c) {
   if (!c) return fail(CHAMP_EINVAL, "null context");
   CK(cudaStreamSynchronize(c->stream));
-  return CHAMP_OK;
+  return tc_check(c);
 }
 
 }  // extern "C"

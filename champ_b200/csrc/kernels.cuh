@@ -474,7 +474,7 @@ __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const Vi
 template <class T, int NORD, bool MD, bool PG = false>
 __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, const State<T> &st, int w,
                           const View<T> &v, const double *R, int lane, bool outputs, EvalRes &res,
-                          const PGBuf *pg = nullptr) {
+                          const PGBuf *pg = nullptr, bool orbs_ready = false) {
   const int N = s.N, C = s.C, nomax = s.nomax;
   const double *xs = v.xs;
   T *fso = v.fso;
@@ -586,15 +586,18 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
   pe_en = warp_sum(pe_en);
   __syncwarp();
 
-  // --- orbitals of every electron, Slater matrices (determinant.f90:36-42, t_bld)
+  // --- orbitals of every electron, Slater matrices (determinant.f90:36-42, t_bld); with
+  // orbs_ready they were computed for all walkers by the tensor-core contraction
   double *ainv = v.ainv;
   T *orb5 = v.orb5;
   for (int e = 0; e < N; e++) {
     int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
     double *A = ainv + (sp ? s.nup * s.nup : 0);
-    warp_basis<T, 5>(s, xs + 3 * e, v.phi, lane);
     T *oe = orb5 + (size_t)e * 5 * nomax;
-    warp_orbitals<T, 5>(v.phi, s.cocc[sp], s.nbasis, s.nocc[sp], oe, nomax, lane);
+    if (!orbs_ready) {
+      warp_basis<T, 5>(s, xs + 3 * e, v.phi, lane);
+      warp_orbitals<T, 5>(v.phi, s.cocc[sp], s.nbasis, s.nocc[sp], oe, nomax, lane);
+    }
     for (int k = lane; k < n; k += 32) A[eo * n + k] = (double)oe[k];
   }
   __syncwarp();
@@ -662,16 +665,41 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
   if (s.nloc > 0 && ok) {
     const int B = s.nbasis;
     T *gp = v.gproj;
-    // G projected onto the basis: g_e[b] = sum_k coef[b][k] Ainv[k][e] (psp_nonloc_pot_bld)
-    for (int e = 0; e < N; e++) {
-      int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
+    // G projected onto the basis: g_e[b] = sum_k coef[b][k] G[k][e] (psp_nonloc_pot_bld), one
+    // [nbasis x nocc] x [nocc x n] product per spin in compute precision: lanes along b over
+    // rows of the transposed coefficients (coalesced), 4 electrons x 4 basis functions per lane.
+    for (int sp = 0; sp < 2; sp++) {
+      const int n = sp ? s.ndn : s.nup, e0 = sp ? s.nup : 0, no = s.nocc[sp];
       const double *G = gam_ptr<T, MD>(s, v, sp);
-      const T *cr = s.cocc[sp];
-      const int no = s.nocc[sp];
-      for (int b = lane; b < B; b += 32) {
-        double acc = 0;
-        for (int k = 0; k < no; k++) acc += (double)cr[b * no + k] * G[k * n + eo];
-        gp[(size_t)e * B + b] = (T)acc;
+      const T *ct = s.coccT[sp];
+      for (int eo0 = 0; eo0 < n; eo0 += 4) {
+        const int ne = min(4, n - eo0);
+        for (int b0 = 0; b0 < B; b0 += 128) {
+          T acc[4][4];
+#pragma unroll
+          for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[i][j] = T(0);
+          for (int k = 0; k < no; k++) {
+            T g[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) g[i] = (i < ne) ? (T)G[k * n + eo0 + i] : T(0);
+            const T *row = ct + (size_t)k * B + b0 + lane;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+              T cf = (b0 + lane + 32 * j < B) ? row[32 * j] : T(0);
+#pragma unroll
+              for (int i = 0; i < 4; i++) acc[i][j] += cf * g[i];
+            }
+          }
+#pragma unroll
+          for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+              int b = b0 + lane + 32 * j;
+              if (i < ne && b < B) gp[(size_t)(e0 + eo0 + i) * B + b] = acc[i][j];
+            }
+        }
       }
     }
     double *tl = v.nlt;
@@ -981,7 +1009,7 @@ __device__ inline void load_params(const Sys<T> &s, JasPar<T> &J, EcpPar &E) {
 template <class T, int NORD, bool MD>
 __global__ void __launch_bounds__(128, 4) k_eval(Sys<T> s, State<T> st, Layout L, double r0, double r1, double r2,
                                                  double r3, double r4, double r5, double r6, double r7, double r8,
-                                                 int outputs) {
+                                                 int outputs, int orbs_ready) {
   __shared__ JasPar<T> J;
   __shared__ EcpPar E;
   extern __shared__ __align__(16) char dsm[];
@@ -993,7 +1021,7 @@ __global__ void __launch_bounds__(128, 4) k_eval(Sys<T> s, State<T> st, Layout L
     for (int i = lane; i < 3 * s.N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * s.N + i];
     __syncwarp();
     EvalRes res;
-    full_eval<T, NORD, MD>(s, J, E, st, w, v, R, lane, outputs != 0, res);
+    full_eval<T, NORD, MD>(s, J, E, st, w, v, R, lane, outputs != 0, res, nullptr, orbs_ready != 0);
     if (L.resident) view_store(v, st, w, s.N, s.C, lane);
   }
 }
@@ -1068,10 +1096,12 @@ __global__ void __launch_bounds__(128, 4) k_accept(Sys<T> s, State<T> st, Layout
   }
 }
 
-// Fused VMC: nsweep sweeps of single-electron Metropolis moves plus E_L after each sweep.
+// Fused VMC: nsweep sweeps of single-electron Metropolis moves plus E_L after each sweep
+// (phase 0).  Phase 1 runs only the moves and phase 2 only the E_L, from orbitals computed in
+// between for all walkers (tensor-core contraction).  Statistics are added to st.s_*.
 template <class T, int NORD, bool MD>
 __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L, int nsweep, uint64_t seed,
-                                                uint64_t sweep0, double step) {
+                                                uint64_t sweep0, double step, int phase) {
   __shared__ JasPar<T> J;
   __shared__ EcpPar E;
   extern __shared__ __align__(16) char dsm[];
@@ -1089,7 +1119,7 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
     double es = 0, e2 = 0, acc = 0, el = 0;
     for (int isw = 0; isw < nsweep; isw++) {
       uint64_t sweep = sweep0 + (uint64_t)isw;
-      for (int e = 0; e < N; e++) {
+      for (int e = 0; e < N && phase != 2; e++) {
         double g[3], ua;
         move_randoms(seed, (uint32_t)w, sweep, (uint32_t)e, g, &ua);
         double xn[3] = {v.xs[3 * e] + step * g[0], v.xs[3 * e + 1] + step * g[1], v.xs[3 * e + 2] + step * g[2]};
@@ -1101,10 +1131,11 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
           acc += 1;
         }
       }
+      if (phase == 1) continue;
       double R[9];
       random_rotation(seed, (uint32_t)w, sweep, R);
       EvalRes res;
-      full_eval<T, NORD, MD>(s, J, E, st, w, v, R, lane, false, res);
+      full_eval<T, NORD, MD>(s, J, E, st, w, v, R, lane, false, res, nullptr, phase == 2);
       el = res.eloc;
       es += el;
       e2 += el * el;
@@ -1115,10 +1146,10 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
       for (int i = lane; i < 3 * N; i += 32) st.x[(size_t)w * 3 * N + i] = v.xs[i];
     }
     if (lane == 0) {
-      st.s_esum[w] = es;
-      st.s_e2sum[w] = e2;
-      st.s_acc[w] = acc;
-      st.s_elast[w] = el;
+      st.s_esum[w] += es;
+      st.s_e2sum[w] += e2;
+      st.s_acc[w] += acc;
+      if (phase != 1) st.s_elast[w] = el;
     }
     __syncwarp();
   }
@@ -1126,3 +1157,4 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
 
 #include "pgrad.cuh"
 #include "dmc.cuh"
+#include "orbtc.cuh"

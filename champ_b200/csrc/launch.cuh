@@ -1,5 +1,8 @@
 // launch.cuh -- kernel dispatch over (precision, e-e-n order, multi-determinant).
 #pragma once
+#include <algorithm>
+#include <type_traits>
+
 #include "ctx.h"
 
 #define fail champ_fail
@@ -17,12 +20,58 @@ static int set_smem_attrs(champ_ctx *c) {
   if (!rc) rc = set_attrs(c, k_accept<T, MD>);
   if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD>);
   if (!rc) rc = set_attrs(c, k_dmc_move<T, NORD, MD>);
+  if (!rc && std::is_same<T, float>::value) {
+    CK(cudaFuncSetAttribute(orbtc::k_orb_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)orbtc::smem_bytes(256)));
+    CK(cudaFuncSetAttribute(k_basis_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)std::min<size_t>(4 * (size_t)c->nbasis * 5 * sizeof(float), 227 * 1024)));
+  }
   if (!rc) {
     CK(cudaFuncSetAttribute(k_pgrad<T, NORD, MD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_pg));
     CK(cudaFuncSetAttribute(k_pgrad<T, NORD, MD>, cudaFuncAttributePreferredSharedMemoryCarveout,
                             (int)cudaSharedmemCarveoutMaxShared));
   }
   return rc;
+}
+
+// Orbitals (5 channels) of every electron of every walker in st.orb5 by the tensor cores:
+// basis rows to HBM, then one tcgen05 contraction per spin.
+template <class T>
+static int run_orb_tc(champ_ctx *c, const State<T> &st) {
+  if constexpr (!std::is_same<T, float>::value) {
+    return fail(CHAMP_EINVAL, "tensor-core orbitals are a mixed-precision path");
+  } else {
+    const long long items = (long long)st.W * c->N;
+    const int sm = c->num_sms > 0 ? c->num_sms : 148;
+    long long gb = std::min<long long>((items + 3) / 4, (long long)sm * 8);
+    k_basis_rows<<<(unsigned)std::max<long long>(gb, 1), 128, 4 * (size_t)c->nbasis * 5 * sizeof(float), c->stream>>>(
+        c->sf, st.x, items, c->tc_Kp, c->tc_phi);
+    CK(cudaGetLastError());
+    for (int sp = 0; sp < 2; sp++) {
+      const int n = sp ? c->ndn : c->nup;
+      if (n == 0) continue;
+      orbtc::Args g;
+      g.phi = c->tc_phi;
+      g.bhi = c->tc_b[sp][0];
+      g.blo = c->tc_b[sp][1];
+      g.orb = st.orb5;
+      g.M = (long long)st.W * n * 5;
+      g.Kp = c->tc_Kp;
+      g.Np = c->tc_Np[sp];
+      g.ncols = c->tc_ncols[sp];
+      g.n = n;
+      g.N = c->N;
+      g.e0 = sp ? c->nup : 0;
+      g.nomax = c->nomax;
+      g.nocc = c->md.nocc[sp];
+      g.err = c->tc_err;
+      long long tiles = (g.M + orbtc::BM - 1) / orbtc::BM;
+      unsigned grid = (unsigned)std::min<long long>(tiles, (long long)sm * c->tc_ctas_per_sm[sp]);
+      orbtc::k_orb_tc<<<grid, orbtc::NTHR, orbtc::smem_bytes(g.Np), c->stream>>>(g);
+      CK(cudaGetLastError());
+    }
+    return CHAMP_OK;
+  }
 }
 
 template <class T, int NORD, bool MD>
@@ -34,10 +83,16 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
   const double *R = c->rot;
   switch (op) {
   case Op::Eval:
-  case Op::EvalOut:
+  case Op::EvalOut: {
+    const bool tc = c->tc_on && !a.st_override;  // only mixed-precision contexts turn it on
+    if (tc) {
+      int rc = run_orb_tc<T>(c, st);
+      if (rc) return rc;
+    }
     k_eval<T, NORD, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, R[0], R[1], R[2], R[3], R[4], R[5], R[6], R[7], R[8],
-                                                       op == Op::EvalOut ? 1 : 0);
+                                                       op == Op::EvalOut ? 1 : 0, tc ? 1 : 0);
     break;
+  }
   case Op::Propose:
   case Op::ProposeGrad:
     k_propose<T, NORD, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, a.e, a.xnew, a.ratio, op == Op::ProposeGrad ? a.grad : nullptr);
@@ -57,9 +112,26 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
     k_dmc_copy<T><<<592, 128, 0, c->stream>>>(st, st2of<T>(c), c->dA, c->dB, c->N, c->C, c->dpar.wmax);
     break;
   }
-  case Op::Vmc:
-    k_vmc<T, NORD, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, a.nsweep, a.seed, a.sweep0, a.step);
+  case Op::Vmc: {
+    CK(cudaMemsetAsync(st.s_esum, 0, sizeof(double) * st.W, c->stream));
+    CK(cudaMemsetAsync(st.s_e2sum, 0, sizeof(double) * st.W, c->stream));
+    CK(cudaMemsetAsync(st.s_acc, 0, sizeof(double) * st.W, c->stream));
+    const bool tc = c->tc_on && !a.st_override;  // only mixed-precision contexts turn it on
+    if (!tc) {
+      k_vmc<T, NORD, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, a.nsweep, a.seed, a.sweep0, a.step, 0);
+      break;
+    }
+    // per sweep: moves, orbitals of all walkers on the tensor cores, E_L
+    for (int isw = 0; isw < a.nsweep; isw++) {
+      k_vmc<T, NORD, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, 1, a.seed, a.sweep0 + isw, a.step, 1);
+      CK(cudaGetLastError());
+      int rc = run_orb_tc<T>(c, st);
+      if (rc) return rc;
+      k_vmc<T, NORD, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, 1, a.seed, a.sweep0 + isw, a.step, 2);
+      CK(cudaGetLastError());
+    }
     break;
+  }
   }
   CK(cudaGetLastError());
   return CHAMP_OK;

@@ -1,0 +1,244 @@
+// orbtc.cuh -- the basis-to-orbital contraction of the full evaluation on the tensor cores.
+//
+// orbitals_loc_ana (orbitals_loc_ana.f90:50-64) for every electron of every walker is one GEMM
+// per spin: rows (walker, electron, channel) x K = basis functions x N = orbitals of that spin,
+//   orb[w][e][ch][m] = sum_b phi[w][e][ch][b] coef[b][m],   ch = value, d/dx, d/dy, d/dz, lap.
+// k_basis_rows writes phi (FP32, K-major rows padded to Kp) to HBM; k_orb_tc runs the product
+// with tcgen05.mma kind::tf32 into a TMEM accumulator.  TF32 keeps 10 mantissa bits, so each
+// operand is split as x = hi + lo (hi = x with the low 13 mantissa bits cleared, lo = x - hi,
+// exact in FP32) and the product is hi*hi + hi*lo + lo*hi: about FP32 accuracy (relative error
+// ~2^-21 per product, FP32 accumulation), three tensor-core passes.  Used by the mixed-precision
+// engine only; the FP64 engine keeps the CUDA-core contraction.
+#pragma once
+#include <cstdint>
+
+namespace orbtc {
+
+constexpr int BM = 128;        // rows per tile (TMEM lanes)
+constexpr int BK = 32;         // K (fp32 elements) per stage: 128 bytes per row
+constexpr int NTHR = 128;      // 4 warps: all load, thread 0 issues, all drain TMEM
+constexpr uint32_t WAIT_LIMIT = 1u << 24;  // bounded mbarrier polls before giving up
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor, K-major without swizzle: the operand is stored as core
+// matrices of 8 rows x 16 bytes (128 contiguous bytes); lbo = bytes between core matrices
+// adjacent along K, sbo = bytes between adjacent 8-row groups.  Bit 46 = descriptor version 1.
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+// Instruction descriptor: D f32 (bits 4-5 = 1), A and B tf32 (bits 7-9, 10-12 = 2), both
+// K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t dt, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dt),
+      "l"(a), "l"(b), "r"(id), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}\n"
+      : "=r"(ok)
+      : "r"(mbar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for completion `parity` of the barrier; false after WAIT_LIMIT polls.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (uint32_t i = 0; i < WAIT_LIMIT; i++)
+    if (mbar_try(mbar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+      "[%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__host__ __device__ inline float tf32_hi(float x) {
+#ifdef __CUDA_ARCH__
+  return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
+#else
+  uint32_t u;
+  memcpy(&u, &x, 4);
+  u &= 0xFFFFE000u;
+  float h;
+  memcpy(&h, &u, 4);
+  return h;
+#endif
+}
+
+struct Args {
+  const float *phi;          // [rows of all walkers][Kp]; row = (w*N + e)*5 + ch
+  const float *bhi, *blo;    // [Np][Kp] coefficients of this spin, transposed, split, zero padded
+  float *orb;                // [rows][nomax]
+  long long M;               // rows of this spin: W * n * 5
+  int Kp, Np, ncols;         // padded K (multiple of BK), padded N (multiple of 16), TMEM columns
+  int n, N, e0, nomax, nocc; // electrons of the spin, all electrons, first electron, row stride, orbitals
+  int *err;
+};
+
+__host__ __device__ inline size_t smem_bytes(int Np) { return 2 * (size_t)(2 * BM * BK * 4 + 2 * Np * BK * 4) + 128; }
+
+// Byte offset of element (row r, k) of a [rows][BK] tile in the core-matrix layout.
+__device__ __forceinline__ uint32_t tile_off(int r, int chunk) { return (uint32_t)((((r >> 3) * (BK / 4) + chunk) << 7) + ((r & 7) << 4)); }
+
+static __global__ void __launch_bounds__(NTHR) k_orb_tc(Args a) {
+  extern __shared__ __align__(128) unsigned char sm[];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t tslot;
+  __shared__ int bail;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  unsigned char *base = (unsigned char *)(((uintptr_t)sm + 127) & ~(uintptr_t)127);
+  const uint32_t sA = BM * BK * 4, sB = (uint32_t)a.Np * BK * 4, stage = 2 * sA + 2 * sB;
+  if (tid == 0) {
+    mbar_init(smem_u32(&mbar[0]), 1);
+    mbar_init(smem_u32(&mbar[1]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    bail = 0;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tslot)), "r"(a.ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tbase = tslot;
+  const uint32_t idesc = idesc_tf32(BM, a.Np);
+  const int nkb = a.Kp / BK;
+  const long long ntile = (a.M + BM - 1) / BM;
+  const int nw_rows = a.n * 5;  // rows per walker of this spin
+  uint32_t it = 0;              // stage uses so far (commit count)
+  bool ok = true;
+  for (long long tile = blockIdx.x; tile < ntile && ok; tile += gridDim.x) {
+    const long long row0 = tile * BM;
+    for (int kb = 0; kb < nkb; kb++, it++) {
+      const int s = it & 1;
+      // the stage is free once the group committed two uses ago has completed; every thread
+      // polls, and the block agrees on the outcome before going on
+      const bool got = it < 2 || mbar_wait(smem_u32(&mbar[s]), ((it - 2) >> 1) & 1);
+      unsigned char *st = base + s * stage;
+      unsigned char *ahi = st, *alo = st + sA, *bhi = st + 2 * sA, *blo = st + 2 * sA + sB;
+      const int k0 = kb * BK;
+      for (int i = tid; i < BM * (BK / 4); i += NTHR) {
+        int r = i >> 3, ch = i & 7;
+        long long gr = row0 + r;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (gr < a.M) {
+          long long w = gr / nw_rows, rem = gr - w * nw_rows;
+          long long orow = (w * a.N + a.e0) * 5 + rem;
+          v = *(const float4 *)(a.phi + orow * a.Kp + k0 + 4 * ch);
+        }
+        float4 h = make_float4(tf32_hi(v.x), tf32_hi(v.y), tf32_hi(v.z), tf32_hi(v.w));
+        float4 l = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+        uint32_t off = tile_off(r, ch);
+        *(float4 *)(ahi + off) = h;
+        *(float4 *)(alo + off) = l;
+      }
+      for (int i = tid; i < a.Np * (BK / 4); i += NTHR) {
+        int r = i >> 3, ch = i & 7;
+        uint32_t off = tile_off(r, ch);
+        *(float4 *)(bhi + off) = *(const float4 *)(a.bhi + (size_t)r * a.Kp + k0 + 4 * ch);
+        *(float4 *)(blo + off) = *(const float4 *)(a.blo + (size_t)r * a.Kp + k0 + 4 * ch);
+      }
+      fence_async_smem();
+      if (!__syncthreads_and(got)) { ok = false; break; }
+      if (tid == 0) {
+        fence_after();
+        const uint32_t uah = smem_u32(ahi), ual = smem_u32(alo), ubh = smem_u32(bhi), ubl = smem_u32(blo);
+#pragma unroll
+        for (int ks = 0; ks < BK / 8; ks++) {
+          // one instruction covers K = 8 (two core matrices along K)
+          const uint32_t ko = ks * 256;
+          uint64_t dah = sdesc(uah + ko, 128, (BK / 4) * 128), dal = sdesc(ual + ko, 128, (BK / 4) * 128);
+          uint64_t dbh = sdesc(ubh + ko, 128, (BK / 4) * 128), dbl = sdesc(ubl + ko, 128, (BK / 4) * 128);
+          uint32_t acc0 = (kb > 0 || ks > 0) ? 1u : 0u;
+          mma_tf32(tbase, dal, dbh, idesc, acc0);
+          mma_tf32(tbase, dah, dbl, idesc, 1u);
+          mma_tf32(tbase, dah, dbh, idesc, 1u);
+        }
+        mma_commit(smem_u32(&mbar[s]));
+      }
+    }
+    if (!ok) break;
+    // epilogue: wait for the tile's last commit, drain TMEM (warp q owns lanes 32q..32q+31)
+    if (!__syncthreads_and(mbar_wait(smem_u32(&mbar[(it - 1) & 1]), ((it - 1) >> 1) & 1))) { ok = false; break; }
+    fence_after();
+    const int r = warp * 32 + lane;
+    const long long gr = row0 + r;
+    float *dst = nullptr;
+    if (gr < a.M) {
+      long long w = gr / nw_rows, rem = gr - w * nw_rows;
+      dst = a.orb + ((w * a.N + a.e0) * 5 + rem) * a.nomax;
+    }
+    for (int c0 = 0; c0 < a.Np; c0 += 16) {
+      float v[16];
+      tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+      if (dst)
+#pragma unroll
+        for (int i = 0; i < 16; i++)
+          if (c0 + i < a.nocc) dst[c0 + i] = v[i];
+    }
+    fence_before();
+    __syncthreads();
+  }
+  if (!ok) {
+    bail = 1;
+    if (a.err) atomicExch(a.err, 1);
+  }
+  __syncthreads();
+  // a CTA that gave up still lets every committed group finish before freeing TMEM
+  if (bail && it > 0) {
+    if (tid == 0) {
+      for (uint32_t u = (it >= 2 ? it - 2 : 0); u < it; u++) mbar_wait(smem_u32(&mbar[u & 1]), (u >> 1) & 1);
+    }
+    __syncthreads();
+  }
+  fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(a.ncols));
+}
+
+}  // namespace orbtc
+
+// Basis values (5 channels) of every electron of every walker as K-major FP32 rows:
+// phi[((w*N + e)*5 + ch)*Kp + b], zero for nbasis <= b < Kp.  One warp per electron.
+static __global__ void __launch_bounds__(128) k_basis_rows(Sys<float> s, const double *x, long long items, int Kp,
+                                                    float *phi) {
+  extern __shared__ __align__(16) float sphi[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  float *ph = sphi + (size_t)wib * s.nbasis * 5;
+  for (long long it = (long long)blockIdx.x * 4 + wib; it < items; it += (long long)gridDim.x * 4) {
+    warp_basis<float, 5>(s, x + 3 * it, ph, lane);
+    for (int ch = 0; ch < 5; ch++) {
+      float *row = phi + (it * 5 + ch) * Kp;
+      for (int b = lane; b < Kp; b += 32) row[b] = b < s.nbasis ? ph[b * 5 + ch] : 0.f;
+    }
+    __syncwarp();
+  }
+}

@@ -22,7 +22,7 @@ EXPORTED_SYMBOLS = [
     "champ_set_walkers", "champ_get_walkers", "champ_set_quadrature_rotation", "champ_eval_full",
     "champ_propose_1e", "champ_accept_1e", "champ_grad_1e", "champ_vmc_sweeps", "champ_vmc_run_host",
     "champ_walker_status", "champ_synchronize", "champ_param_grad", "champ_accumulate_oh",
-    "champ_dmc_init", "champ_dmc_steps", "champ_num_walkers", "champ_eval_energy_noalloc",
+    "champ_dmc_init", "champ_dmc_steps", "champ_num_walkers", "champ_eval_energy_noalloc", "champ_set_option",
 ]
 
 PREC = {"fp64": 0, "mixed": 1}
@@ -74,6 +74,7 @@ def load_library(path: str = LIB_PATH):
     L.champ_dmc_steps.argtypes = [vp, i32, u64, dp]
     L.champ_num_walkers.argtypes = [vp, C.POINTER(i32)]
     L.champ_eval_energy_noalloc.argtypes = [vp, i32, vp, vp]
+    L.champ_set_option.argtypes = [vp, C.c_char_p, C.c_int64]
     for n in EXPORTED_SYMBOLS:
         if n not in ("champ_last_error", "champ_version"):
             getattr(L, n).restype = C.c_int
@@ -218,6 +219,9 @@ class Engine:
         f = np.zeros(self.nw, np.uint32)
         self._check(self.lib.champ_walker_status(self.h, f.ctypes.data_as(C.POINTER(C.c_uint32))))
         return f
+
+    def set_option(self, name: str, value: int):
+        self._check(self.lib.champ_set_option(self.h, name.encode(), int(value)))
 
     def synchronize(self):
         self._check(self.lib.champ_synchronize(self.h))

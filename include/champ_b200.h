@@ -228,7 +228,16 @@ int champ_num_walkers(const champ_ctx *ctx, int32_t *nw);
    makes no device allocation; it leaves the context's walkers untouched.  All calls share the
    array, so calls that overlap on the GPU (other streams, other contexts on the device) race. */
 int champ_eval_energy_noalloc(champ_ctx *ctx, int32_t nw, const double *x, double *eloc);
+/* Waits for the context's stream; also reports a tensor-core contraction that gave up. */
 int champ_synchronize(champ_ctx *ctx);
+
+/* Engine options (no counterpart in the reference, which has one code path).
+   "orbital_tc": 1 computes the orbitals of the full evaluation (value, gradient, Laplacian of
+   every electron of every walker) as one tcgen05 tensor-core contraction per spin with a
+   3-term TF32 split (about FP32 accuracy); 0 uses the CUDA-core contraction.  Available for
+   mixed precision when the walker state lives in HBM and a spin has >= 16 orbitals, and on by
+   default there; CHAMP_EINVAL otherwise. */
+int champ_set_option(champ_ctx *ctx, const char *name, int64_t value);
 
 #ifdef __cplusplus
 }
