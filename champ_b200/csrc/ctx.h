@@ -77,7 +77,7 @@ struct champ_ctx {
   // tensor-core orbital contraction of the full evaluation (mixed precision, state in HBM)
   int num_sms = 0;
   int tc_on = 0, tc_ok = 0;       // in use; supported for this system and precision
-  int tc_Kp = 0, tc_Np[2] = {0, 0}, tc_ncols[2] = {32, 32}, tc_ctas_per_sm[2] = {1, 1};
+  int tc_Kp = 0, tc_Np[2] = {0, 0}, tc_ncols[2] = {32, 32};
   float *tc_phi = nullptr;        // [wmax*N*5][Kp] basis rows
   float *tc_b[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [spin][hi, lo]: [Np][Kp]
   int *tc_err = nullptr;          // set by a contraction that gave up waiting

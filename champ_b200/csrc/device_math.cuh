@@ -362,6 +362,52 @@ __device__ __forceinline__ void warp_basis(const Sys<T> &s, const double *pt, T 
 template <class T, int NCH, class O>
 __device__ __forceinline__ void warp_orbitals(const T *phi, const T *coef, int nbasis, int n, O *out, int ostride,
                                               int lane) {
+  if (n > 16) {
+    // lanes along m, two orbitals per lane per pass (64 per pass); the coefficient rows of U
+    // basis functions are loaded together so that the L2 latency of the coefficient stream is
+    // paid once per U functions.  Each orbital is summed over b in order, as on the path below.
+    constexpr int U = NCH == 1 ? 8 : 4;
+    for (int m0 = 0; m0 < n; m0 += 64) {
+      const int ma = m0 + lane, mb = m0 + 32 + lane;
+      const bool ha = ma < n, hb = mb < n;
+      T aa[NCH], ab[NCH];
+#pragma unroll
+      for (int ch = 0; ch < NCH; ch++) aa[ch] = ab[ch] = T(0);
+      int b = 0;
+      for (; b + U <= nbasis; b += U) {
+        T ca[U], cb[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          ca[u] = ha ? coef[(size_t)(b + u) * n + ma] : T(0);
+          cb[u] = hb ? coef[(size_t)(b + u) * n + mb] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+#pragma unroll
+          for (int ch = 0; ch < NCH; ch++) {
+            T p = phi[(b + u) * NCH + ch];
+            aa[ch] += ca[u] * p;
+            ab[ch] += cb[u] * p;
+          }
+      }
+      for (; b < nbasis; b++) {
+        T ca = ha ? coef[(size_t)b * n + ma] : T(0), cb = hb ? coef[(size_t)b * n + mb] : T(0);
+#pragma unroll
+        for (int ch = 0; ch < NCH; ch++) {
+          T p = phi[b * NCH + ch];
+          aa[ch] += ca * p;
+          ab[ch] += cb * p;
+        }
+      }
+#pragma unroll
+      for (int ch = 0; ch < NCH; ch++) {
+        if (ha) out[ch * ostride + ma] = (O)aa[ch];
+        if (hb) out[ch * ostride + mb] = (O)ab[ch];
+      }
+    }
+    __syncwarp();
+    return;
+  }
   int LM = 1;
   while (LM < n && LM < 32) LM <<= 1;
   int LB = 32 / LM;

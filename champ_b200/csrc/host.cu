@@ -595,8 +595,6 @@ static int tc_setup(champ_ctx *c) {
     while (nc < Np) nc <<= 1;
     c->tc_Np[sp] = Np;
     c->tc_ncols[sp] = nc;
-    int by_smem = (int)((227 * 1024) / (orbtc::smem_bytes(Np) + 1024)), by_tmem = 512 / nc;
-    c->tc_ctas_per_sm[sp] = std::max(1, std::min(std::min(by_smem, by_tmem), 4));
     std::vector<float> hi((size_t)Np * Kp, 0.f), lo((size_t)Np * Kp, 0.f);
     for (int m = 0; m < no; m++)
       for (int b = 0; b < B; b++) {

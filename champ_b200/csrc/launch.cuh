@@ -21,8 +21,10 @@ static int set_smem_attrs(champ_ctx *c) {
   if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD>);
   if (!rc) rc = set_attrs(c, k_dmc_move<T, NORD, MD>);
   if (!rc && std::is_same<T, float>::value) {
-    CK(cudaFuncSetAttribute(orbtc::k_orb_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)orbtc::smem_bytes(256)));
+    CK(cudaFuncSetAttribute(orbtc::k_orb_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024 + 128));
+    CK(cudaFuncSetAttribute(orbtc::k_orb_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024 + 128));
+    CK(cudaFuncSetAttribute(orbtc::k_orb_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)orbtc::smem_bytes(256, 2)));
     CK(cudaFuncSetAttribute(k_basis_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)std::min<size_t>(4 * (size_t)c->nbasis * 5 * sizeof(float), 227 * 1024)));
   }
@@ -55,7 +57,7 @@ static int run_orb_tc(champ_ctx *c, const State<T> &st) {
       g.bhi = c->tc_b[sp][0];
       g.blo = c->tc_b[sp][1];
       g.orb = st.orb5;
-      g.M = (long long)st.W * n * 5;
+      g.M = st.W * n * 5;
       g.Kp = c->tc_Kp;
       g.Np = c->tc_Np[sp];
       g.ncols = c->tc_ncols[sp];
@@ -65,9 +67,12 @@ static int run_orb_tc(champ_ctx *c, const State<T> &st) {
       g.nomax = c->nomax;
       g.nocc = c->md.nocc[sp];
       g.err = c->tc_err;
-      long long tiles = (g.M + orbtc::BM - 1) / orbtc::BM;
-      unsigned grid = (unsigned)std::min<long long>(tiles, (long long)sm * c->tc_ctas_per_sm[sp]);
-      orbtc::k_orb_tc<<<grid, orbtc::NTHR, orbtc::smem_bytes(g.Np), c->stream>>>(g);
+      const int tiles = (g.M + orbtc::BM - 1) / orbtc::BM, ns = orbtc::stages_for(g.Np);
+      const unsigned grid = (unsigned)std::min(tiles, sm);
+      const size_t smb = orbtc::smem_bytes(g.Np, ns);
+      if (ns == 4) orbtc::k_orb_tc<4><<<grid, orbtc::NTHR, smb, c->stream>>>(g);
+      else if (ns == 3) orbtc::k_orb_tc<3><<<grid, orbtc::NTHR, smb, c->stream>>>(g);
+      else orbtc::k_orb_tc<2><<<grid, orbtc::NTHR, smb, c->stream>>>(g);
       CK(cudaGetLastError());
     }
     return CHAMP_OK;

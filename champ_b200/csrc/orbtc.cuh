@@ -97,30 +97,45 @@ struct Args {
   const float *phi;          // [rows of all walkers][Kp]; row = (w*N + e)*5 + ch
   const float *bhi, *blo;    // [Np][Kp] coefficients of this spin, transposed, split, zero padded
   float *orb;                // [rows][nomax]
-  long long M;               // rows of this spin: W * n * 5
+  int M;                     // rows of this spin: W * n * 5
   int Kp, Np, ncols;         // padded K (multiple of BK), padded N (multiple of 16), TMEM columns
   int n, N, e0, nomax, nocc; // electrons of the spin, all electrons, first electron, row stride, orbitals
   int *err;
 };
 
-__host__ __device__ inline size_t smem_bytes(int Np) { return 2 * (size_t)(2 * BM * BK * 4 + 2 * Np * BK * 4) + 128; }
+// Bytes of one pipeline stage: A hi, A lo (BM x BK), B hi, B lo (Np x BK), core-matrix layout.
+__host__ __device__ inline size_t stage_bytes(int Np) { return 2 * (size_t)BM * BK * 4 + 2 * (size_t)Np * BK * 4; }
+__host__ __device__ inline size_t smem_bytes(int Np, int ns) { return ns * stage_bytes(Np) + 128; }
+// Deepest pipeline (2..4 stages) that fits 200 KB of shared memory.
+__host__ inline int stages_for(int Np) {
+  int ns = 4;
+  while (ns > 2 && smem_bytes(Np, ns) > 200 * 1024) ns--;
+  return ns;
+}
 
-// Byte offset of element (row r, k) of a [rows][BK] tile in the core-matrix layout.
-__device__ __forceinline__ uint32_t tile_off(int r, int chunk) { return (uint32_t)((((r >> 3) * (BK / 4) + chunk) << 7) + ((r & 7) << 4)); }
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32_t bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-static __global__ void __launch_bounds__(NTHR) k_orb_tc(Args a) {
+// One CTA streams tiles of BM rows through an NS-stage ring: cp.async brings the FP32 basis
+// rows and the split coefficients of K-block i+NS-1 while the tensor cores work on block i.
+// Each 16-byte piece q of a [rows][BK] tile lands at byte 16q, which is the core-matrix layout:
+// q = (group*8 + k chunk)*8 + row in group.
+template <int NS>
+__global__ void __launch_bounds__(NTHR, 1) k_orb_tc(Args a) {
   extern __shared__ __align__(128) unsigned char sm[];
-  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ __align__(8) uint64_t mbar[NS];
   __shared__ uint32_t tslot;
-  __shared__ int bail;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   unsigned char *base = (unsigned char *)(((uintptr_t)sm + 127) & ~(uintptr_t)127);
   const uint32_t sA = BM * BK * 4, sB = (uint32_t)a.Np * BK * 4, stage = 2 * sA + 2 * sB;
   if (tid == 0) {
-    mbar_init(smem_u32(&mbar[0]), 1);
-    mbar_init(smem_u32(&mbar[1]), 1);
+    for (int i = 0; i < NS; i++) mbar_init(smem_u32(&mbar[i]), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    bail = 0;
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tslot)), "r"(a.ncols));
@@ -132,94 +147,107 @@ static __global__ void __launch_bounds__(NTHR) k_orb_tc(Args a) {
   const uint32_t tbase = tslot;
   const uint32_t idesc = idesc_tf32(BM, a.Np);
   const int nkb = a.Kp / BK;
-  const long long ntile = (a.M + BM - 1) / BM;
-  const int nw_rows = a.n * 5;  // rows per walker of this spin
-  uint32_t it = 0;              // stage uses so far (commit count)
-  bool ok = true;
-  for (long long tile = blockIdx.x; tile < ntile && ok; tile += gridDim.x) {
-    const long long row0 = tile * BM;
-    for (int kb = 0; kb < nkb; kb++, it++) {
-      const int s = it & 1;
-      // the stage is free once the group committed two uses ago has completed; every thread
-      // polls, and the block agrees on the outcome before going on
-      const bool got = it < 2 || mbar_wait(smem_u32(&mbar[s]), ((it - 2) >> 1) & 1);
-      unsigned char *st = base + s * stage;
-      unsigned char *ahi = st, *alo = st + sA, *bhi = st + 2 * sA, *blo = st + 2 * sA + sB;
-      const int k0 = kb * BK;
-      for (int i = tid; i < BM * (BK / 4); i += NTHR) {
-        int r = i >> 3, ch = i & 7;
-        long long gr = row0 + r;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+  const int ntile = (a.M + BM - 1) / BM;
+  const int my_tiles = blockIdx.x < ntile ? (ntile - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const int T = my_tiles * nkb;  // K-blocks this CTA runs
+  const int nw_rows = a.n * 5;   // rows per walker of this spin
+
+  // issue the copies of K-block i into its stage (an empty group past the end)
+  auto issue = [&](int i) {
+    if (i < T) {
+      const int tile = (int)blockIdx.x + (i / nkb) * (int)gridDim.x, kb = i % nkb, k0 = kb * BK;
+      const uint32_t st = smem_u32(base + (size_t)(i % NS) * stage);
+      for (int q = tid; q < BM * (BK / 4); q += NTHR) {
+        const int cm = q >> 3, r = ((cm >> 3) << 3) + (q & 7), ch = cm & 7, gr = tile * BM + r;
+        const float *src = a.phi;
+        uint32_t bytes = 0;
         if (gr < a.M) {
-          long long w = gr / nw_rows, rem = gr - w * nw_rows;
-          long long orow = (w * a.N + a.e0) * 5 + rem;
-          v = *(const float4 *)(a.phi + orow * a.Kp + k0 + 4 * ch);
+          const int w = gr / nw_rows, rem = gr - w * nw_rows;
+          src = a.phi + ((long long)(w * a.N + a.e0) * 5 + rem) * a.Kp + k0 + 4 * ch;
+          bytes = 16;
         }
-        float4 h = make_float4(tf32_hi(v.x), tf32_hi(v.y), tf32_hi(v.z), tf32_hi(v.w));
-        float4 l = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
-        uint32_t off = tile_off(r, ch);
-        *(float4 *)(ahi + off) = h;
-        *(float4 *)(alo + off) = l;
+        cp_async16(st + 16 * q, src, bytes);
       }
-      for (int i = tid; i < a.Np * (BK / 4); i += NTHR) {
-        int r = i >> 3, ch = i & 7;
-        uint32_t off = tile_off(r, ch);
-        *(float4 *)(bhi + off) = *(const float4 *)(a.bhi + (size_t)r * a.Kp + k0 + 4 * ch);
-        *(float4 *)(blo + off) = *(const float4 *)(a.blo + (size_t)r * a.Kp + k0 + 4 * ch);
-      }
-      fence_async_smem();
-      if (!__syncthreads_and(got)) { ok = false; break; }
-      if (tid == 0) {
-        fence_after();
-        const uint32_t uah = smem_u32(ahi), ual = smem_u32(alo), ubh = smem_u32(bhi), ubl = smem_u32(blo);
-#pragma unroll
-        for (int ks = 0; ks < BK / 8; ks++) {
-          // one instruction covers K = 8 (two core matrices along K)
-          const uint32_t ko = ks * 256;
-          uint64_t dah = sdesc(uah + ko, 128, (BK / 4) * 128), dal = sdesc(ual + ko, 128, (BK / 4) * 128);
-          uint64_t dbh = sdesc(ubh + ko, 128, (BK / 4) * 128), dbl = sdesc(ubl + ko, 128, (BK / 4) * 128);
-          uint32_t acc0 = (kb > 0 || ks > 0) ? 1u : 0u;
-          mma_tf32(tbase, dal, dbh, idesc, acc0);
-          mma_tf32(tbase, dah, dbl, idesc, 1u);
-          mma_tf32(tbase, dah, dbh, idesc, 1u);
-        }
-        mma_commit(smem_u32(&mbar[s]));
+      for (int q = tid; q < a.Np * (BK / 4); q += NTHR) {
+        const int cm = q >> 3, r = ((cm >> 3) << 3) + (q & 7), ch = cm & 7;
+        const size_t o = (size_t)r * a.Kp + k0 + 4 * ch;
+        cp_async16(st + 2 * sA + 16 * q, a.bhi + o, 16);
+        cp_async16(st + 2 * sA + sB + 16 * q, a.blo + o, 16);
       }
     }
-    if (!ok) break;
-    // epilogue: wait for the tile's last commit, drain TMEM (warp q owns lanes 32q..32q+31)
-    if (!__syncthreads_and(mbar_wait(smem_u32(&mbar[(it - 1) & 1]), ((it - 1) >> 1) & 1))) { ok = false; break; }
-    fence_after();
-    const int r = warp * 32 + lane;
-    const long long gr = row0 + r;
-    float *dst = nullptr;
-    if (gr < a.M) {
-      long long w = gr / nw_rows, rem = gr - w * nw_rows;
-      dst = a.orb + ((w * a.N + a.e0) * 5 + rem) * a.nomax;
-    }
-    for (int c0 = 0; c0 < a.Np; c0 += 16) {
-      float v[16];
-      tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-      if (dst)
-#pragma unroll
-        for (int i = 0; i < 16; i++)
-          if (c0 + i < a.nocc) dst[c0 + i] = v[i];
-    }
-    fence_before();
+    cp_commit();
+  };
+
+  for (int i = 0; i < NS - 1; i++) issue(i);
+  bool ok = true;
+  int done = 0;  // K-blocks whose MMA group was committed
+  for (int i = 0; i < T; i++) {
+    const int s = i % NS, kb = i % nkb;
+    unsigned char *st = base + (size_t)s * stage;
+    cp_wait<NS - 2>();  // this thread's copies of block i have landed
     __syncthreads();
+    // split A in place: hi = x with the low 13 mantissa bits cleared, lo = x - hi
+    for (int q = tid; q < BM * (BK / 4); q += NTHR) {
+      float4 v = *(float4 *)(st + 16 * q);
+      float4 h = make_float4(tf32_hi(v.x), tf32_hi(v.y), tf32_hi(v.z), tf32_hi(v.w));
+      *(float4 *)(st + 16 * q) = h;
+      *(float4 *)(st + sA + 16 * q) = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+    }
+    fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      fence_after();
+      const uint32_t uah = smem_u32(st), ual = uah + sA, ubh = uah + 2 * sA, ubl = ubh + sB;
+#pragma unroll
+      for (int ks = 0; ks < BK / 8; ks++) {
+        // one instruction covers K = 8 (two core matrices along K)
+        const uint32_t ko = ks * 256;
+        uint64_t dah = sdesc(uah + ko, 128, (BK / 4) * 128), dal = sdesc(ual + ko, 128, (BK / 4) * 128);
+        uint64_t dbh = sdesc(ubh + ko, 128, (BK / 4) * 128), dbl = sdesc(ubl + ko, 128, (BK / 4) * 128);
+        mma_tf32(tbase, dal, dbh, idesc, (kb > 0 || ks > 0) ? 1u : 0u);
+        mma_tf32(tbase, dah, dbl, idesc, 1u);
+        mma_tf32(tbase, dah, dbh, idesc, 1u);
+      }
+      mma_commit(smem_u32(&mbar[s]));
+    }
+    done = i + 1;
+    // the stage of block i-1 is refilled with block i+NS-1 once block i-1's MMAs completed;
+    // every thread polls, and the block agrees on the outcome
+    bool got = true;
+    if (i >= 1) got = mbar_wait(smem_u32(&mbar[(i - 1) % NS]), ((i - 1) / NS) & 1);
+    if (!__syncthreads_and(got)) { ok = false; break; }
+    issue(i + NS - 1);
+    if (kb == nkb - 1) {
+      // epilogue: drain the accumulator (warp q owns TMEM lanes 32q..32q+31)
+      if (!__syncthreads_and(mbar_wait(smem_u32(&mbar[s]), (i / NS) & 1))) { ok = false; break; }
+      fence_after();
+      const int tile = (int)blockIdx.x + (i / nkb) * (int)gridDim.x;
+      const int gr = tile * BM + warp * 32 + lane;
+      float *dst = nullptr;
+      if (gr < a.M) {
+        const int w = gr / nw_rows, rem = gr - w * nw_rows;
+        dst = a.orb + ((long long)(w * a.N + a.e0) * 5 + rem) * a.nomax;
+      }
+      for (int c0 = 0; c0 < a.Np; c0 += 16) {
+        float v[16];
+        tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+        if (dst)
+#pragma unroll
+          for (int k = 0; k < 16; k++)
+            if (c0 + k < a.nocc) dst[c0 + k] = v[k];
+      }
+      fence_before();
+      __syncthreads();
+    }
   }
+  cp_wait_all();
   if (!ok) {
-    bail = 1;
     if (a.err) atomicExch(a.err, 1);
+    // let the committed MMA groups finish (bounded) before the accumulator is freed
+    if (tid == 0)
+      for (int u = done > NS ? done - NS : 0; u < done; u++) mbar_wait(smem_u32(&mbar[u % NS]), (u / NS) & 1);
   }
   __syncthreads();
-  // a CTA that gave up still lets every committed group finish before freeing TMEM
-  if (bail && it > 0) {
-    if (tid == 0) {
-      for (uint32_t u = (it >= 2 ? it - 2 : 0); u < it; u++) mbar_wait(smem_u32(&mbar[u & 1]), (u >> 1) & 1);
-    }
-    __syncthreads();
-  }
   fence_after();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(a.ncols));
 }
