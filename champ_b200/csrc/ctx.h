@@ -54,7 +54,7 @@ struct champ_ctx {
   int np_raw = 0;          // raw Jastrow parameters on the device (a, b, all c terms)
   int ncfree = 0;          // free e-e-n coefficients per centre type
   int ncsfp = 0, norbp = 0;  // CSF and orbital-rotation parameters
-  std::vector<int2> orbp;
+  std::vector<int4> orbp;  // (i, j, antisymmetric, 0)
   double *pg_scr = nullptr;
   size_t scr_stride = 0;
   std::vector<double> cproj;

@@ -78,8 +78,10 @@ struct Sys {
   const int *csf_off;      // [ncsf+1]
   const int *csf_det;      // determinant of each CSF entry
   const double *csf_cd;    // coefficient of each CSF entry
-  const int2 *orbp;        // [norbp] (i, j): orbital i rotated towards orbital j
-  const int *refpos[2];    // [norb] column of orbital in the spin's reference determinant, or -1
+  const int4 *orbp;        // [norbp] (i, j, rev, 0): orbital i rotated towards orbital j (and j
+                           // away from i when rev: both active, single_ex_wf_bld)
+  const int *refpos[2];    // [norb] position of the orbital in the spin's orbital set (reference
+                           // columns, then virtuals), or -1
   const int *occo[2];      // [nocc_s] orbital index of each occupied column
   const JasPar<T> *jas;
   const EcpPar *ecp;

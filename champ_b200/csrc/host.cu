@@ -317,7 +317,7 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
       }
       int *co = dalloc<int>(c, off.size()), *cdt = dalloc<int>(c, std::max<size_t>(1, cdet.size()));
       double *cdd = dalloc<double>(c, std::max<size_t>(1, cd.size()));
-      int2 *op = dalloc<int2>(c, std::max(1, c->norbp));
+      int4 *op = dalloc<int4>(c, std::max(1, c->norbp));
       int *rp0 = dalloc<int>(c, d->norb), *rp1 = dalloc<int>(c, d->norb);
       int *oo0 = dalloc<int>(c, std::max(1, md.nocc[0])), *oo1 = dalloc<int>(c, std::max(1, md.nocc[1]));
       if (!ca || !co || !cdt || !cdd || !op || !rp0 || !rp1 || !oo0 || !oo1) return fail(CHAMP_ENOMEM, "device allocation failed");
@@ -327,12 +327,11 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
         CK(cudaMemcpy(cdt, cdet.data(), sizeof(int) * cdet.size(), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(cdd, cd.data(), sizeof(double) * cd.size(), cudaMemcpyHostToDevice));
       }
-      if (c->norbp) CK(cudaMemcpy(op, c->orbp.data(), sizeof(int2) * c->norbp, cudaMemcpyHostToDevice));
+      if (c->norbp) CK(cudaMemcpy(op, c->orbp.data(), sizeof(int4) * c->norbp, cudaMemcpyHostToDevice));
       int *rp[2] = {rp0, rp1}, *oo[2] = {oo0, oo1};
       for (int sp = 0; sp < 2; sp++) {
         std::vector<int> rpv(d->norb, -1);
-        int n = sp ? c->ndn : c->nup;
-        for (int k = 0; k < n; k++) rpv[md.occ[sp][k]] = k;
+        for (int k = 0; k < md.nocc[sp]; k++) rpv[md.occ[sp][k]] = k;
         CK(cudaMemcpy(rp[sp], rpv.data(), sizeof(int) * d->norb, cudaMemcpyHostToDevice));
         if (md.nocc[sp]) CK(cudaMemcpy(oo[sp], md.occ[sp].data(), sizeof(int) * md.nocc[sp], cudaMemcpyHostToDevice));
         s.refpos[sp] = rp[sp];
@@ -660,18 +659,37 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
     int rc0 = build_multidet(d, c->md);
     if (rc0) { delete c; return rc0; }
     c->nomax = std::max(1, std::max(c->md.nocc[0], c->md.nocc[1]));
-    // orbital rotations (single determinant): every reference orbital towards every orbital no
-    // reference determinant occupies (orb_opt_lab, orbitals_mod.f90:1829-2140)
+    // orbital rotations by orbital class (single_ex_wf_bld, deriv_orb_mod.f90:130-417).  One
+    // determinant: closed (both spins) -> open (one spin), closed -> virtual, open -> virtual.
+    // Several: closed (both spins in every determinant) -> active, closed -> virtual,
+    // active i -> active j (i < j, antisymmetric), active -> virtual.
     c->orbp.clear();
-    if (!c->md.multidet) {
-      std::vector<int> occ;
-      for (int sp = 0; sp < 2; sp++)
-        for (int k = 0; k < (sp ? c->ndn : c->nup); k++)
-          if (std::find(occ.begin(), occ.end(), c->md.occ[sp][k]) == occ.end()) occ.push_back(c->md.occ[sp][k]);
-      std::sort(occ.begin(), occ.end());
-      for (int i : occ)
-        for (int j = 0; j < d->norb; j++)
-          if (std::find(occ.begin(), occ.end(), j) == occ.end()) c->orbp.push_back(make_int2(i, j));
+    {
+      const int no = d->norb, ne = d->nelec, nu = d->nup;
+      std::vector<int> cnt_all(no, 0), any(no, 0);
+      for (int K = 0; K < d->ndet; K++) {
+        std::vector<int> inu(no, 0), ind(no, 0);
+        for (int e = 0; e < ne; e++) (e < nu ? inu : ind)[d->det_orb[(size_t)K * ne + e]] = 1;
+        for (int m = 0; m < no; m++) {
+          if (inu[m] && ind[m]) cnt_all[m]++;
+          if (inu[m] || ind[m]) any[m] = 1;
+        }
+      }
+      std::vector<int> cls, mid, vir;  // closed, open/active, virtual
+      for (int m = 0; m < no; m++) {
+        if (cnt_all[m] == d->ndet) cls.push_back(m);
+        else if (any[m]) mid.push_back(m);
+        else vir.push_back(m);
+      }
+      for (int i : cls)
+        for (int j : mid) c->orbp.push_back(make_int4(i, j, 0, 0));
+      for (int i : cls)
+        for (int j : vir) c->orbp.push_back(make_int4(i, j, 0, 0));
+      if (c->md.multidet)
+        for (size_t a = 0; a < mid.size(); a++)
+          for (size_t b = a + 1; b < mid.size(); b++) c->orbp.push_back(make_int4(mid[a], mid[b], 1, 0));
+      for (int i : mid)
+        for (int j : vir) c->orbp.push_back(make_int4(i, j, 0, 0));
     }
     c->norbp = (int)c->orbp.size();
     c->ncsfp = c->md.multidet && d->ncsf > 1 ? d->ncsf - 1 : 0;
@@ -827,6 +845,10 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
     if (c->ncsfp + c->norbp > 0) {
       size_t N = c->N, B = c->nbasis, M = d->norb, nm = c->nmax;
       c->scr_stride = N * B + N * 5 * M + N * M + 4 * nm * M + nm * nm + (size_t)(c->md.ndu[0] + c->md.ndu[1]) + 1;
+      if (c->md.multidet) {
+        size_t no = c->nomax;
+        c->scr_stride += 4 * no * M + 5 * no * nm + (size_t)(c->md.ndu[0] + c->md.ndu[1]);
+      }
       c->pg_scr = dalloc<double>(c, W * c->scr_stride);
       if (!c->pg_scr) { champ_destroy(c); return fail(CHAMP_ENOMEM, "allocation of the derivative scratch failed"); }
     }

@@ -259,6 +259,126 @@ struct PGOut {
 // E_K = E_ref + tr(alpha_K^-1 dalpha_K) per spin (alpha_deloc_bld :468, csf_derivs_bld :781).
 // Orbital rotation i -> j (single determinant): dlnpsi = sum_spin T[i][j], dE_L = sum_spin dT[i][j]
 // (dpsi_orb_bld / deloc_orb_bld, deriv_orb_mod.f90:1486,1557).
+// Scratch of the multi-determinant orbital tables after the single-determinant part
+// [N*B phis][N*5*M orbitals][N*M B][2*nmax*M T][2*nmax*M dT][nmax^2][ndu delo]: per spin
+// G At and G B + dG At over the spin's orbital set (2 x [nomax][M] each), dY, dG (2 x [nomax][nmax]
+// each), one [nomax][nmax] work matrix and the local-energy-weighted determinant sums ([ndu]).
+template <class T>
+__device__ __forceinline__ size_t md_ga_offset(const Sys<T> &s) {
+  const size_t N = s.N, B = s.nbasis, M = s.norb, nm = s.nmax;
+  return N * B + N * 5 * M + N * M + 4 * nm * M + nm * nm + (size_t)(s.ndu[0] + s.ndu[1]);
+}
+
+// dY, dG and the orbital tables of a multi-determinant wave function (dy_bld, dg_bld,
+// deriv_fast_mod.f90:648-779).  With c_I = sum over determinants K containing unique
+// determinant I of c_K w_K (w = product of the spin determinants' signed alpha determinants) and
+// cE_I the same sum weighted by the determinant's local-energy delta (delo_up + delo_dn):
+//   dY[p][h] = (1/chi) sum_I (cE_I inv_I - c_I inv_I dalpha_I inv_I)[p][h] - esum Y[p][h],
+//   esum = sum_spin sum Y[p][k] dT[k][p],
+//   dG = (dY - G B_ref - [ref rows] (T_v dY + dT_v Y)) Ainv.
+template <class T>
+__device__ void md_orbital_tables(const Sys<T> &s, const View<T> &v, int lane, double *scr, double chi, double eref) {
+  const int N = s.N, M = s.norb, nmax = s.nmax, nomax = s.nomax, nd0 = s.ndu[0], nd1 = s.ndu[1];
+  const double *orbA = scr + (size_t)N * s.nbasis, *Bm = orbA + (size_t)N * 5 * M;
+  const double *dTa = Bm + (size_t)N * M + (size_t)2 * nmax * M;
+  const double *delo = dTa + (size_t)2 * nmax * M + (size_t)nmax * nmax;
+  double *GA = scr + md_ga_offset(s), *GH = GA + (size_t)2 * nomax * M;
+  double *dY = GH + (size_t)2 * nomax * M, *dG = dY + (size_t)2 * nomax * nmax, *aux = dG + (size_t)2 * nomax * nmax;
+  double *cE = aux + (size_t)nomax * nmax;
+  const double *wd = v.wdet, *wg = v.wdet + nd0 + nd1;
+  (void)eref;
+  // cE per unique determinant of each spin
+  for (int i = lane; i < nd0 + nd1; i += 32) cE[i] = 0.0;
+  for (int i = lane; i < 2 * nomax * nmax; i += 32) dY[i] = 0.0;
+  __syncwarp();
+  for (int K = lane; K < s.ndet; K += 32) {
+    int iu = s.ciu[K], id = s.cid[K];
+    double t = s.ccoef[K] * wd[iu] * wd[nd0 + id] * (delo[iu] + delo[nd0 + id]);
+    atomicAdd(&cE[iu], t);
+    atomicAdd(&cE[nd0 + id], t);
+  }
+  __syncwarp();
+  const double ichi = 1.0 / chi;
+  double esum = 0;
+  for (int sp = 0; sp < 2; sp++) {
+    const int n = sp ? s.ndn : s.nup, nv = s.nvirt[sp];
+    const double *Y = v.ymd + (sp ? s.nup * s.nvirt[0] : 0), *dTs = dTa + (size_t)sp * nmax * M;
+    for (int i = lane; i < nv * n; i += 32) {
+      int p = i / n, k = i - p * n;
+      esum += Y[i] * dTs[(size_t)k * M + s.occo[sp][n + p]];
+    }
+  }
+  esum = warp_sum(esum);
+  for (int sp = 0; sp < 2; sp++) {
+    const int n = sp ? s.ndn : s.nup, nv = s.nvirt[sp], no = s.nocc[sp];
+    if (n == 0) continue;
+    const double *dTs = dTa + (size_t)sp * nmax * M;
+    double *dYs = dY + (size_t)sp * nomax * nmax;  // [nv][n] (virtual rows)
+    for (int I = lane; I < s.ndu[sp]; I += 32) {
+      double a[16], inv[16], da[16], t1[16];
+      int k = load_alpha(s, v, sp, I, a);
+      if (k == 0) continue;
+      small_det_inv(a, k, inv);
+      const double cI = wg[(sp ? nd0 : 0) + I], cEI = cE[(sp ? nd0 : 0) + I];
+      for (int ia = 0; ia < k; ia++)
+        for (int ib = 0; ib < k; ib++) da[ia * k + ib] = dTs[(size_t)s.dh[sp][4 * I + ia] * M + s.occo[sp][n + s.dpart[sp][4 * I + ib]]];
+      // t1 = inv da inv (inv rows: particles, columns: holes; da rows: holes, columns: particles)
+      for (int ib = 0; ib < k; ib++)
+        for (int ia = 0; ia < k; ia++) {
+          double acc = 0;
+          for (int x = 0; x < k; x++)
+            for (int y = 0; y < k; y++) acc += inv[ib * k + x] * da[x * k + y] * inv[y * k + ia];
+          t1[ib * k + ia] = acc;
+        }
+      for (int ib = 0; ib < k; ib++)
+        for (int ia = 0; ia < k; ia++)
+          atomicAdd(&dYs[s.dpart[sp][4 * I + ib] * n + s.dh[sp][4 * I + ia]],
+                    (cEI * inv[ib * k + ia] - cI * t1[ib * k + ia]) * ichi);
+    }
+    __syncwarp();
+    const double *Y = v.ymd + (sp ? s.nup * s.nvirt[0] : 0);
+    for (int i = lane; i < nv * n; i += 32) dYs[i] -= esum * Y[i];
+    __syncwarp();
+    // aux = dY - G B_ref - [ref rows] (T_v dY + dT_v Y), then dG = aux Ainv
+    const double *G = v.gam + (sp ? s.nocc[0] * s.nup : 0), *A = v.ainv + (sp ? s.nup * s.nup : 0);
+    const double *Tv = v.tv + (sp ? s.nup * s.nvirt[0] : 0);
+    const int e0 = sp ? s.nup : 0;
+    double *dGs = dG + (size_t)sp * nomax * nmax;
+    for (int i = lane; i < no * n; i += 32) {
+      int o = i / n, kk = i - o * n;
+      double acc = o >= n ? dYs[(o - n) * n + kk] : 0.0;
+      const int rk = s.occo[sp][kk];
+      for (int e = 0; e < n; e++) acc -= G[o * n + e] * Bm[(size_t)(e0 + e) * M + rk];
+      if (o < n) {
+        for (int p = 0; p < nv; p++)
+          acc -= Tv[o * nv + p] * dYs[p * n + kk] + dTs[(size_t)o * M + s.occo[sp][n + p]] * Y[p * n + kk];
+      }
+      aux[i] = acc;
+    }
+    __syncwarp();
+    for (int i = lane; i < no * n; i += 32) {
+      int o = i / n, e = i - o * n;
+      double acc = 0;
+      for (int kk = 0; kk < n; kk++) acc += aux[o * n + kk] * A[kk * n + e];
+      dGs[i] = acc;
+    }
+    __syncwarp();
+    double *GAs = GA + (size_t)sp * nomax * M, *GHs = GH + (size_t)sp * nomax * M;
+    for (int i = lane; i < no * M; i += 32) {
+      int o = i / M, m = i - o * M;
+      double ga = 0, gh = 0;
+      for (int e = 0; e < n; e++) {
+        double at = orbA[(size_t)(e0 + e) * 5 * M + m];
+        ga += G[o * n + e] * at;
+        gh += G[o * n + e] * Bm[(size_t)(e0 + e) * M + m] + dGs[o * n + e] * at;
+      }
+      GAs[i] = ga;
+      GHs[i] = gh;
+    }
+    __syncwarp();
+  }
+}
+
 template <class T, bool MD>
 __device__ void orbital_csf_derivs(const Sys<T> &s, const View<T> &v, const PGBuf &pg, const EvalRes &res, int lane,
                                    double *scr, double *ol, double *oe) {
@@ -319,7 +439,7 @@ __device__ void orbital_csf_derivs(const Sys<T> &s, const View<T> &v, const PGBu
     }
     __syncwarp();
   }
-  if (MD && s.ncsf > 1) {
+  if (MD) {
     const int nd0 = s.ndu[0];
     const double *wd = v.wdet;
     for (int sp = 0; sp < 2; sp++) {
@@ -342,6 +462,7 @@ __device__ void orbital_csf_derivs(const Sys<T> &s, const View<T> &v, const PGBu
     double chi = 0;
     for (int K = lane; K < s.ndet; K += 32) chi += s.ccoef[K] * wd[s.ciu[K]] * wd[nd0 + s.cid[K]];
     chi = warp_sum(chi);
+    if (s.norbp > 0) md_orbital_tables(s, v, lane, scr, chi, eref);
     for (int q = 1 + lane; q < s.ncsf; q += 32) {
       double dl = 0, de = 0;
       for (int t = s.csf_off[q]; t < s.csf_off[q + 1]; t++) {
@@ -356,14 +477,26 @@ __device__ void orbital_csf_derivs(const Sys<T> &s, const View<T> &v, const PGBu
     }
   }
   const int off = MD ? (s.ncsf > 1 ? s.ncsf - 1 : 0) : 0;
+  // orbital rotation (i -> j, minus j -> i where both are active): dpsi_orb_bld and
+  // deloc_orb_bld (deriv_orb_mod.f90:1486-1629): g = sum_spin (G At)[i][j], h = sum_spin
+  // (G B + dG At)[i][j] with G, dG over the spin's orbital set.  One determinant: G = Ainv, so
+  // G At = T and G B + dG At = dT.
+  const double *GA = MD ? scr + md_ga_offset(s) : Ta, *GH = MD ? GA + (size_t)2 * s.nomax * M : dTa;
+  const size_t sps = MD ? (size_t)s.nomax * M : (size_t)nmax * M;
   for (int p = lane; p < s.norbp; p += 32) {
-    int2 ij = s.orbp[p];
+    int4 ij = s.orbp[p];
     double g = 0, h = 0;
     for (int sp = 0; sp < 2; sp++) {
-      int k = s.refpos[sp][ij.x];
-      if (k < 0) continue;
-      g += Ta[(size_t)sp * nmax * M + (size_t)k * M + ij.y];
-      h += dTa[(size_t)sp * nmax * M + (size_t)k * M + ij.y];
+      int oi = s.refpos[sp][ij.x];
+      if (oi >= 0) {
+        g += GA[sp * sps + (size_t)oi * M + ij.y];
+        h += GH[sp * sps + (size_t)oi * M + ij.y];
+      }
+      int oj = ij.z ? s.refpos[sp][ij.y] : -1;
+      if (oj >= 0) {
+        g -= GA[sp * sps + (size_t)oj * M + ij.x];
+        h -= GH[sp * sps + (size_t)oj * M + ij.x];
+      }
     }
     ol[off + p] = g;
     oe[off + p] = h;

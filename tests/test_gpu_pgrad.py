@@ -64,12 +64,27 @@ def jastrow_params(s):
 
 
 def orbital_params(s):
-    """Orbital rotations i -> j of a single determinant: i a reference orbital, j an orbital no
-    reference column uses."""
+    """Orbital rotations (i, j, antisymmetric) by orbital class, in the order of
+    single_ex_wf_bld (qmc/deriv_orb_mod.f90:130-417).  Closed: occupied in both spins of every
+    determinant; open/active: occupied somewhere else; virtual: nowhere.  One determinant:
+    closed->open, closed->virtual, open->virtual.  Several: closed->active, closed->virtual,
+    active i->active j (i < j, antisymmetric), active->virtual."""
+    ne, nu = s.nelec, s.nup
+    both_all = np.ones(s.norb, bool)
+    anyocc = np.zeros(s.norb, bool)
+    for det in s.det_orb:
+        up, dn = set(int(o) for o in det[:nu]), set(int(o) for o in det[nu:ne])
+        for m in range(s.norb):
+            both_all[m] &= (m in up) and (m in dn)
+            anyocc[m] |= (m in up) or (m in dn)
+    cls = [m for m in range(s.norb) if both_all[m]]
+    mid = [m for m in range(s.norb) if anyocc[m] and not both_all[m]]
+    vir = [m for m in range(s.norb) if not anyocc[m]]
+    out = [(i, j, 0) for i in cls for j in mid] + [(i, j, 0) for i in cls for j in vir]
     if s.ndet > 1:
-        return []
-    occ = sorted(set(int(o) for o in s.det_orb[0]))
-    return [(i, j) for i in occ for j in range(s.norb) if j not in occ]
+        out += [(mid[a], mid[b], 1) for a in range(len(mid)) for b in range(a + 1, len(mid))]
+    out += [(i, j, 0) for i in mid for j in vir]
+    return out
 
 
 def all_params(s):
@@ -85,9 +100,12 @@ def all_params(s):
 def perturbed(s, name, idx, h):
     s2 = copy.deepcopy(s)
     arr = getattr(s2, name).copy()
-    if name == "coef":  # rotate orbital i towards orbital j
-        i, j = idx
-        arr[i] = arr[i] + h * arr[j]
+    if name == "coef":  # rotate orbital i towards orbital j (and j away from i)
+        i, j, rev = idx
+        ai, aj = arr[i].copy(), arr[j].copy()
+        arr[i] = ai + h * aj
+        if rev:
+            arr[j] = aj - h * ai
     else:
         arr[idx] += h
     setattr(s2, name, arr)
