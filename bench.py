@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--step-size", type=float, default=0.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-arm", action="store_true")
+    ap.add_argument("--no-cluster", action="store_true", help="skip the 128-electron cluster measurement")
     return ap.parse_args()
 
 
@@ -221,6 +222,90 @@ def time_engine(eng, system, args, nsteps, nwarm, flush, torch, sweep_base):
     return sum(a.elapsed_time(b) for a, b in evs)  # ms
 
 
+def allmax(x, world, torch, dist):
+    """Max over ranks of a per-rank number (every rank calls this in the same order)."""
+    if world == 1:
+        return x
+    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def time_param_grad(eng, system, nsteps, flush, torch):
+    """d ln psi/dp and dE_L/dp for every walker, folded into the FP64 O/H accumulators (one
+    champ_param_grad + champ_accumulate_oh per step); the walkers move by one VMC sweep between
+    steps, outside the timed events.  Returns ms for nsteps."""
+    tpg = 0.0
+    for k in range(nsteps + 2):
+        eng.vmc_sweeps(1, SEED, sweep0=30000 + k, step=step_size(system), stats=False)
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        eng.param_grad(host=False)
+        eng._check(lib_accumulate(eng))
+        e1.record()
+        torch.cuda.synchronize()
+        if k >= 2:
+            tpg += e0.elapsed_time(e1)
+    return tpg
+
+
+def measure(system, nw, prec, steps, warmup, pg_steps, rank, world, flush, torch, dist, fp64_arm=True):
+    """e-moves/s of the fused VMC sweep (mixed or FP64), the FP64 arm of the same workload,
+    param-grad samples/s in both precisions and the mixed-precision E_L error on the same walkers."""
+    from champ_b200.engine import Engine
+    eng = Engine(system, nw, prec)
+    eng.set_walkers(system_walkers(system, nw, seed=1000 + rank))
+    eng.vmc_sweeps(10, SEED + rank, sweep0=0, step=step_size(system), stats=False)  # equilibration
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clk.start()
+    time.sleep(0.5)  # let the sampler start before the timed region
+    t_wall = time.perf_counter()
+    ms = time_engine(eng, system, None, steps, warmup, flush, torch, 100)
+    t_wall = time.perf_counter() - t_wall
+    clocks = clk.stop()
+    ms = allmax(ms, world, torch, dist)
+    out = {"value": nw * world * system.nelec * steps / (ms * 1e-3), "ms_per_step": ms / steps,
+           "clocks": clocks, "wall_s_timed_region": t_wall,
+           "launches_per_step": eng.get_option("launches_per_sweep")}
+    nj, ncsf, norb = eng.nparam()
+    npar = {"jastrow": nj, "csf": ncsf, "orbital": norb}
+    tpg = allmax(time_param_grad(eng, system, pg_steps, flush, torch), world, torch, dist)
+    out["param_grad"] = {"value": nw * world * pg_steps / (tpg * 1e-3), "unit": "param-grad samples/s",
+                         "n_params": nj + ncsf + norb, "params": npar, "ms_per_step": tpg / pg_steps,
+                         "step": "d ln psi/dp and dE_L/dp for all walkers + FP64 O/H accumulation (cuBLAS DGEMM)"}
+    if prec == "mixed" and fp64_arm:
+        eng64 = Engine(system, nw, "fp64")
+        xw = eng.get_walkers()
+        eng64.set_walkers(xw)
+        n64 = max(3, steps // 4)
+        ms64 = allmax(time_engine(eng64, system, None, n64, 2, flush, torch, 10000), world, torch, dist)
+        v64 = nw * world * system.nelec * n64 / (ms64 * 1e-3)
+        pg64 = max(2, pg_steps // 2)
+        tpg64 = allmax(time_param_grad(eng64, system, pg64, flush, torch), world, torch, dist)
+        vpg64 = nw * world * pg64 / (tpg64 * 1e-3)
+        # mixed-precision error of E_L on identical walkers (same quadrature rotation)
+        eng.set_walkers(xw)
+        eng64.set_walkers(xw)
+        em, e64 = eng.eval_full(), eng64.eval_full()
+        d = np.abs(em["energy"] - e64["energy"])
+        sc = np.maximum(1.0, np.maximum(np.abs(e64["energy"]), np.abs(e64["d2lnpsi"])))
+        out["fp64_arm"] = {"value": v64, "unit": UNIT, "ms_per_step": ms64 / n64, "mixed_over_fp64": out["value"] / v64,
+                           "param_grad": {"value": vpg64, "unit": "param-grad samples/s", "ms_per_step": tpg64 / pg64,
+                                          "mixed_over_fp64": out["param_grad"]["value"] / vpg64}}
+        out["mixed_error"] = {"max_abs_dEL_Ha": float(d.max()), "median_abs_dEL_Ha": float(np.median(d)),
+                              "frac_samples_within_1e-6_Ha": float(np.mean(d <= 1e-6)),
+                              "max_rel_to_max(1,|E_L|,|lap ln psi|)": float(np.max(d / sc)),
+                              "walkers": nw}
+        eng64.close()
+    out["_eng"] = eng
+    return out
+
+
 def main():
     global ARGS
     args = ARGS = parse()
@@ -236,33 +321,13 @@ def main():
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
-    from champ_b200.engine import Engine
     nw = args.walkers or system.walkers
     prec = args.precision
-    eng = Engine(system, nw, prec)
-    x0 = system_walkers(system, nw, seed=1000 + rank)
-    eng.set_walkers(x0)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    # equilibration (untimed)
-    eng.vmc_sweeps(10, SEED + rank, sweep0=0, step=step_size(system), stats=False)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    clk = ClockSampler(local)
-    clk.start()
-    time.sleep(0.5)  # let the sampler start before the timed region
-    t_wall = time.perf_counter()
-    ms = time_engine(eng, system, args, args.steps, args.warmup, flush, torch, 100)
-    t_wall = time.perf_counter() - t_wall
-    clocks = clk.stop()
-    if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.barrier()
-        ms = float(t.item())
-    total_moves = nw * world * system.nelec * args.steps
-    value = total_moves / (ms * 1e-3)
-    ms_step = ms / args.steps
+    m = measure(system, nw, prec, args.steps, args.warmup, max(3, args.steps // 20), rank, world, flush, torch, dist,
+                fp64_arm=not args.no_fp64_arm)
+    eng = m.pop("_eng")
+    value, ms_step = m["value"], m["ms_per_step"]
     # roofline of the dominant kernel (the fused sweep kernel, one launch per step)
     peaks, peak_kind = measured_peaks()
     alg_bytes = state_bytes(system, prec) * nw
@@ -275,49 +340,6 @@ def main():
             "kernel": "k_vmc (fused sweep)",
             "note": "algorithmic bytes = persistent walker state read+written once per sweep; the kernel is "
                     "CUDA-core bound (see profiles/), so this fraction is small by construction"}
-    # FP64 arm of the same workload (the metric compares mixed with FP64)
-    fp64 = None
-    if prec == "mixed" and not args.no_fp64_arm:
-        eng64 = Engine(system, nw, "fp64")
-        eng64.set_walkers(eng.get_walkers())
-        ms64 = time_engine(eng64, system, args, max(3, args.steps // 4), 2, flush, torch, 10000)
-        if world > 1:
-            t = torch.tensor([ms64], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms64 = float(t.item())
-        v64 = nw * world * system.nelec * max(3, args.steps // 4) / (ms64 * 1e-3)
-        fp64 = {"value": v64, "unit": UNIT, "ms_per_step": ms64 / max(3, args.steps // 4),
-                "mixed_over_fp64": value / v64}
-        eng64.close()
-    # parameter-gradient samples: d ln psi/dp and dE_L/dp for every walker, folded into the
-    # FP64 O/H accumulators (one champ_param_grad + champ_accumulate_oh per step); the walkers
-    # move by one VMC sweep between steps, outside the timed events
-    pg = None
-    try:
-        nj, ncsf, norb = eng.nparam()
-        npg = max(3, args.steps // 20)
-        tpg = 0.0
-        for k in range(npg + 2):
-            eng.vmc_sweeps(1, SEED, sweep0=30000 + k, step=step_size(system), stats=False)
-            flush.zero_()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record()
-            eng.param_grad(host=False)
-            eng._check(lib_accumulate(eng))
-            e1.record()
-            torch.cuda.synchronize()
-            if k >= 2:
-                tpg += e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([tpg], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            tpg = float(t.item())
-        pg = {"value": nw * world * npg / (tpg * 1e-3), "unit": "param-grad samples/s", "n_params": nj + ncsf + norb,
-              "params": {"jastrow": nj, "csf": ncsf, "orbital": norb}, "ms_per_step": tpg / npg,
-              "step": "d ln psi/dp and dE_L/dp for all walkers + FP64 O/H accumulation (cuBLAS DGEMM)"}
-    except Exception as ex:  # report, do not hide
-        pg = {"error": str(ex)}
     # end to end through the host-facing call: walkers in from pinned host memory, one sweep,
     # E_L and walkers back to host memory, every step
     xh = torch.empty((nw, system.nelec, 3), dtype=torch.float64, pin_memory=True)
@@ -336,14 +358,20 @@ def main():
     t0 = time.perf_counter()
     for k in range(ne2e):
         eng._check(lib.champ_vmc_run_host(eng.h, nw, px, 1, SEED, 20010 + k, step_size(system), pel))
-    te2e = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([te2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        te2e = float(t.item())
+    te2e = allmax(time.perf_counter() - t0, world, torch, dist)
     e2e = {"value": nw * world * system.nelec * ne2e / te2e, "unit": UNIT,
            "h2d_bytes_per_step": nw * system.nelec * 3 * 8, "d2h_bytes_per_step": nw * system.nelec * 3 * 8 + nw * 8,
            "call": "champ_vmc_run_host (walkers host->device, state rebuild, 1 sweep, E_L and walkers device->host)"}
+    eng.close()
+    # the 128-electron cluster, where the mixed-vs-FP64 target is set (4096 walkers)
+    big = None
+    if args.system != 5 and not args.no_cluster:
+        s5 = S.get_system(5)
+        b = measure(s5, s5.walkers, "mixed", max(6, args.steps // 100), 2, 2, rank, world, flush, torch, dist)
+        b.pop("_eng").close()
+        big = {"workload": config_of(s5, s5.walkers, "mixed")["workload"], "walkers_per_gpu": s5.walkers, **b}
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            big["cpu_baseline"] = cpu_baseline_sample(s5, seconds=8.0)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(system)
@@ -351,11 +379,12 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32+f64" if prec == "mixed" else "f64", "data": "synthetic",
-                "config": config_of(system, nw, prec), "clocks": clocks, "gpu_launches": args.steps,  # one fused sweep kernel per step
-                "roofline": roof, "fp64_arm": fp64, "param_grad": pg, "e2e": e2e, "cpu_baseline": cpu,
-                "wall_s_timed_region": t_wall}
+                "config": config_of(system, nw, prec), "clocks": m["clocks"],
+                "gpu_launches": args.steps * m["launches_per_step"],
+                "roofline": roof, "fp64_arm": m.get("fp64_arm"), "param_grad": m["param_grad"],
+                "mixed_error": m.get("mixed_error"), "e2e": e2e, "cpu_baseline": cpu,
+                "wall_s_timed_region": m["wall_s_timed_region"], "cluster128": big}
         print(json.dumps(line), flush=True)
-    eng.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -54,6 +54,8 @@ struct champ_ctx {
   int np_raw = 0;          // raw Jastrow parameters on the device (a, b, all c terms)
   int ncfree = 0;          // free e-e-n coefficients per centre type
   int ncsfp = 0, norbp = 0;  // CSF and orbital-rotation parameters
+  int norb = 0;
+  double *call_d = nullptr;  // [nbasis][norb] coefficients of all orbitals in FP64 (B-matrix GEMM)
   std::vector<int4> orbp;  // (i, j, antisymmetric, 0)
   double *pg_scr = nullptr;
   size_t scr_stride = 0;

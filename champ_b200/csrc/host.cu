@@ -322,6 +322,12 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
       int *oo0 = dalloc<int>(c, std::max(1, md.nocc[0])), *oo1 = dalloc<int>(c, std::max(1, md.nocc[1]));
       if (!ca || !co || !cdt || !cdd || !op || !rp0 || !rp1 || !oo0 || !oo1) return fail(CHAMP_ENOMEM, "device allocation failed");
       CK(cudaMemcpy(ca, cav.data(), sizeof(T) * cav.size(), cudaMemcpyHostToDevice));
+      {
+        std::vector<double> cdv(cav.begin(), cav.end());
+        c->call_d = dalloc<double>(c, cdv.size());
+        if (!c->call_d) return fail(CHAMP_ENOMEM, "device allocation failed");
+        CK(cudaMemcpy(c->call_d, cdv.data(), sizeof(double) * cdv.size(), cudaMemcpyHostToDevice));
+      }
       CK(cudaMemcpy(co, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
       if (!cdet.empty()) {
         CK(cudaMemcpy(cdt, cdet.data(), sizeof(int) * cdet.size(), cudaMemcpyHostToDevice));
@@ -617,6 +623,17 @@ static int tc_setup(champ_ctx *c) {
   return CHAMP_OK;
 }
 
+static int cublas_handle(champ_ctx *c) {
+  if (!c->cublas) {
+    cublasHandle_t h;
+    if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) return fail(CHAMP_ECUDA, "cublasCreate failed");
+    c->cublas = h;
+  }
+  if (cublasSetStream((cublasHandle_t)c->cublas, c->stream) != CUBLAS_STATUS_SUCCESS)
+    return fail(CHAMP_ECUDA, "cublasSetStream failed");
+  return CHAMP_OK;
+}
+
 static int tc_check(champ_ctx *c) {
   if (!c->tc_err) return CHAMP_OK;
   int h = 0;
@@ -692,6 +709,7 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
         for (int j : vir) c->orbp.push_back(make_int4(i, j, 0, 0));
     }
     c->norbp = (int)c->orbp.size();
+    c->norb = d->norb;
     c->ncsfp = c->md.multidet && d->ncsf > 1 ? d->ncsf - 1 : 0;
     if (c->nomax > 256) { delete c; return fail(CHAMP_EINVAL, "more than 256 occupied orbitals of one spin"); }
   }
@@ -882,8 +900,25 @@ int champ_param_grad(champ_ctx *c, double *dlnpsi, double *deloc, double *eloc) 
   a.pgout.nfree = c->nfree;
   a.pgout.scr = c->pg_scr;
   a.pgout.scr_stride = c->scr_stride;
+  a.pgout.part = 1;
   int rc = launch(c, Op::PGrad, a);
   if (rc) return rc;
+  if (c->pg_scr) {
+    // nonlocal part of B for all walkers at once: Bm[w] += phis[w] (N x B) coef (B x M), row-major,
+    // as the column-major product Bm^T (M x N) += coef^T (M x B) phis^T (B x N)
+    rc = cublas_handle(c);
+    if (rc) return rc;
+    const int N = c->N, B = c->nbasis, M = c->norb;
+    const double one = 1.0;
+    if (cublasDgemmStridedBatched((cublasHandle_t)c->cublas, CUBLAS_OP_N, CUBLAS_OP_N, M, N, B, &one, c->call_d, M, 0,
+                                  c->pg_scr, B, (long long)c->scr_stride, &one,
+                                  c->pg_scr + (size_t)N * B + (size_t)N * 5 * M, M, (long long)c->scr_stride,
+                                  c->W) != CUBLAS_STATUS_SUCCESS)
+      return fail(CHAMP_ECUDA, "cublasDgemmStridedBatched failed");
+    a.pgout.part = 2;
+    rc = launch(c, Op::PGrad, a);
+    if (rc) return rc;
+  }
   size_t W = c->W, P = c->nfree;
   if (dlnpsi) CK(cudaMemcpyAsync(dlnpsi, c->pg_dl, sizeof(double) * W * P, cudaMemcpyDeviceToHost, c->stream));
   if (deloc) CK(cudaMemcpyAsync(deloc, c->pg_de, sizeof(double) * W * P, cudaMemcpyDeviceToHost, c->stream));
@@ -897,13 +932,9 @@ int champ_accumulate_oh(champ_ctx *c, const double *weights, double *S, double *
   if (!c) return fail(CHAMP_EINVAL, "null context");
   if (!c->have_pgrad) return fail(CHAMP_ESTATE, "call champ_param_grad first");
   const int W = c->W, P = c->nfree, P1 = P + 1;
-  if (!c->cublas) {
-    cublasHandle_t h;
-    if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) return fail(CHAMP_ECUDA, "cublasCreate failed");
-    c->cublas = h;
-  }
+  int rc = cublas_handle(c);
+  if (rc) return rc;
   cublasHandle_t h = (cublasHandle_t)c->cublas;
-  if (cublasSetStream(h, c->stream) != CUBLAS_STATUS_SUCCESS) return fail(CHAMP_ECUDA, "cublasSetStream failed");
   if (weights) CK(cudaMemcpyAsync(c->pg_wt, weights, sizeof(double) * W, cudaMemcpyHostToDevice, c->stream));
   k_pack_oh<<<592, 256, 0, c->stream>>>(W, P, c->pg_dl, c->pg_de, c->pg_el, weights ? c->pg_wt : nullptr, c->oh_oa,
                                         c->oh_ow, c->oh_mb);
@@ -1171,6 +1202,13 @@ int champ_set_option(champ_ctx *c, const char *name, int64_t value) {
     c->tc_on = value ? 1 : 0;
     return CHAMP_OK;
   }
+  return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);
+}
+
+int champ_get_option(const champ_ctx *c, const char *name, int64_t *value) {
+  if (!c || !name || !value) return fail(CHAMP_EINVAL, "null argument");
+  if (!strcmp(name, "orbital_tc")) { *value = c->tc_on; return CHAMP_OK; }
+  if (!strcmp(name, "launches_per_sweep")) { *value = c->tc_on ? 5 : 1; return CHAMP_OK; }
   return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);
 }
 

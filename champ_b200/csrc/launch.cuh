@@ -107,7 +107,7 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
     break;
   case Op::PGrad:
     k_pgrad<T, NORD, MD><<<dim3((c->W + c->wpb_pg - 1) / c->wpb_pg), dim3(32 * c->wpb_pg), c->smem_pg, c->stream>>>(s, st, c->lay, a.pgout, R[0], R[1], R[2], R[3], R[4],
-                                                                 R[5], R[6], R[7], R[8]);
+                                                                 R[5], R[6], R[7], R[8], a.pgout.part);
     break;
   case Op::DmcMove:
     k_dmc_move<T, NORD, MD><<<dim3((c->dpar.wmax + c->wpb - 1) / c->wpb), block, c->smem, c->stream>>>(

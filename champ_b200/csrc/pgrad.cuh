@@ -137,105 +137,187 @@ __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const Vi
 
 // g_p, K_p = sum_e (lap_e g_p + 2 v_e . grad_e g_p) and old[e][p] for all Jastrow
 // parameters (deriv_jastrow4.f90), warp-cooperative; v = pg.vt.
+// Pairs are visited as (i, (i + d) mod N), d = 1..N/2 (at d = N/2 for even N only i < N/2),
+// lanes along (d, i) with i fastest: when 32 divides N the lanes of one warp instruction have
+// distinct i and distinct j, so the per-electron sums old[i][p], old[j][p] take uncontended
+// shared-memory atomics (a few lanes share an electron for small N); the K sums
+// accumulate in registers and are reduced over the warp once, and G = (1/2) sum_e old[e][p]
+// for pair parameters (sum_e old[e][p] for e-n parameters).  With several centre types the
+// e-e-n sums are flushed per centre.
 template <class T, int NORD>
 __device__ void jastrow_param_pass(const Sys<T> &s, const JasPar<T> &J, const View<T> &v, const PGBuf &pg, int lane) {
-  const int N = s.N, C = s.C, P = pg.P;
+  const int N = s.N, C = s.C, P = pg.P, half = N / 2;
   const T sk = J.scalek;
   constexpr Terms tl = make_terms(NORD);
-  const int npair = N * (N - 1) / 2;
-  for (int p = lane; p < npair; p += 32) {
-    int i = (int)((1.0 + sqrt(1.0 + 8.0 * (double)p)) * 0.5);
-    while (i * (i - 1) / 2 > p) i--;
-    while ((i + 1) * i / 2 <= p) i++;
-    int j = p - i * (i - 1) / 2;
-    const double *xi = v.xs + 3 * i, *xj = v.xs + 3 * j;
-    const double *vi = pg.vt + 3 * i, *vj = pg.vt + 3 * j;
-    int isb, ipar;
-    T ss;
-    pair_class(J, s.nup, i, j, isb, ss, ipar);
-    double rvd[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
-    T rij = tsqrt(T(rvd[0] * rvd[0] + rvd[1] * rvd[1] + rvd[2] * rvd[2]));
-    T du = T(1) / (T(1) + sk * rij);
-    double dv_rv = (vi[0] - vj[0]) * rvd[0] + (vi[1] - vj[1]) * rvd[1] + (vi[2] - vj[2]) * rvd[2];
-    for (int k = 1; k <= J.nordb; k++) {
-      T t, t1, t2;
-      ee_param_terms(J, isb, ss, rij, du, k, t, t1, t2, true);
-      int ip = pg.na + isb * J.nordb + (k - 1);
-      double lap = 2.0 * ((double)t2 + 2.0 * (double)t1);
-      atomicAdd(&pg.G[ip], (double)t);
-      atomicAdd(&pg.K[ip], lap + 2.0 * (double)t1 * dv_rv);
-      atomicAdd(&pg.old[i * P + ip], (double)t);
-      atomicAdd(&pg.old[j * P + ip], (double)t);
+  // e-e parameters b_{k+1}, k = 1..nordb, per b set
+  {
+    double kb0[MAXORD], kb1[MAXORD];
+#pragma unroll
+    for (int k = 0; k < MAXORD; k++) kb0[k] = kb1[k] = 0.0;
+    for (int t = lane; t < half * N; t += 32) {
+        const int d = t / N + 1, i = t - (d - 1) * N;
+        if (2 * d == N && i >= half) continue;
+        const int j = i + d < N ? i + d : i + d - N;
+        const double *xi = v.xs + 3 * i, *xj = v.xs + 3 * j;
+        const double *vi = pg.vt + 3 * i, *vj = pg.vt + 3 * j;
+        int isb, ipar;
+        T ss;
+        pair_class(J, s.nup, i, j, isb, ss, ipar);
+        double rvd[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
+        T rij = tsqrt(T(rvd[0] * rvd[0] + rvd[1] * rvd[1] + rvd[2] * rvd[2]));
+        T du = T(1) / (T(1) + sk * rij);
+        double dv_rv = (vi[0] - vj[0]) * rvd[0] + (vi[1] - vj[1]) * rvd[1] + (vi[2] - vj[2]) * rvd[2];
+#pragma unroll
+        for (int k = 1; k < MAXORD; k++) {
+          if (k > J.nordb) break;
+          T t, t1, t2;
+          ee_param_terms(J, isb, ss, rij, du, k, t, t1, t2, true);
+          const int ip = pg.na + isb * J.nordb + (k - 1);
+          const double kk = 2.0 * ((double)t2 + 2.0 * (double)t1) + 2.0 * (double)t1 * dv_rv;
+          if (isb) kb1[k - 1] += kk; else kb0[k - 1] += kk;
+          atomicAdd(&pg.old[i * P + ip], (double)t);
+          atomicAdd(&pg.old[j * P + ip], (double)t);
+        }
+      }
+#pragma unroll
+    for (int k = 1; k < MAXORD; k++) {
+      double a0 = warp_sum(kb0[k - 1]), a1 = warp_sum(kb1[k - 1]);
+      if (lane == 0 && k <= J.nordb) {
+        pg.K[pg.na + (k - 1)] += a0;
+        if (J.nspin2b > 1) pg.K[pg.na + J.nordb + (k - 1)] += a1;
+      }
     }
-    if (NORD > 1) {
-      const T *ri_ = v.ren + 2 * C * i, *rj_ = v.ren + 2 * C * j;
+  }
+  if (NORD > 1) {
+    double kc[tl.n > 0 ? tl.n : 1];
+#pragma unroll
+    for (int ll = 0; ll < tl.n; ll++) kc[ll] = 0.0;
+    for (int t = lane; t < half * N; t += 32) {
+        const int d = t / N + 1, i = t - (d - 1) * N;
+        if (2 * d == N && i >= half) continue;
+        const int j = i + d < N ? i + d : i + d - N;
+        const double *xi = v.xs + 3 * i, *xj = v.xs + 3 * j;
+        const double *vi = pg.vt + 3 * i, *vj = pg.vt + 3 * j;
+        double rvd[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
+        T rij = tsqrt(T(rvd[0] * rvd[0] + rvd[1] * rvd[1] + rvd[2] * rvd[2]));
+        T du = T(1) / (T(1) + sk * rij);
+        const T *ri_ = v.ren + 2 * C * i, *rj_ = v.ren + 2 * C * j;
+        double oc[tl.n > 0 ? tl.n : 1];
+#pragma unroll
+        for (int ll = 0; ll < tl.n; ll++) oc[ll] = 0.0;
+        for (int c = 0; c < C; c++) {
+          const double *cc = s.cent + 3 * c;
+          T ri = ri_[2 * c], di = ri_[2 * c + 1], rj = rj_[2 * c], dj = rj_[2 * c + 1];
+          double vi_ri = vi[0] * (xi[0] - cc[0]) + vi[1] * (xi[1] - cc[1]) + vi[2] * (xi[2] - cc[2]);
+          double vi_rv = vi[0] * rvd[0] + vi[1] * rvd[1] + vi[2] * rvd[2];
+          double vj_rj = vj[0] * (xj[0] - cc[0]) + vj[1] * (xj[1] - cc[1]) + vj[2] * (xj[2] - cc[2]);
+          double vj_rv = vj[0] * rvd[0] + vj[1] * rvd[1] + vj[2] * rvd[2];
+          // power tables with two zero entries below 0, as in jas_een
+          T uu[NORD + 3], rri[NORD + 3], rrj[NORD + 3];
+          uu[0] = uu[1] = rri[0] = rri[1] = rrj[0] = rrj[1] = T(0);
+          uu[2] = rri[2] = rrj[2] = T(1);
+#pragma unroll
+          for (int q = 1; q <= NORD; q++) {
+            uu[q + 2] = uu[q + 1] * du;
+            rri[q + 2] = rri[q + 1] * di;
+            rrj[q + 2] = rrj[q + 1] * dj;
+          }
+          T dd1 = -sk * du * du, dd7 = -sk * di * di, dd8 = -sk * dj * dj;
+          T dd2 = 2 * sk * sk * du * du * du, dd9 = 2 * sk * sk * di * di * di, dd10 = 2 * sk * sk * dj * dj * dj;
+          T sp = ri + rj, tm = ri - rj;
+          T cpst = (rij * rij + sp * tm) / (ri * rij), cmst = (rij * rij - sp * tm) / (rj * rij);
+#pragma unroll
+          for (int ll = 0; ll < tl.n; ll++) {
+            const int k = tl.k[ll], l = tl.l[ll], m = tl.m[ll];
+            T ssl = (l == 0) ? T(2) : rri[l + 2] + rrj[l + 2];
+            T st = ssl * rri[m + 2] * rrj[m + 2];
+            T pi_ = T(l + m) * rri[l + m + 1] * rrj[m + 2] + T(m) * rri[m + 1] * rrj[l + m + 2];
+            T pj_ = T(l + m) * rrj[l + m + 1] * rri[m + 2] + T(m) * rrj[m + 1] * rri[l + m + 2];
+            T pii = T((l + m) * (l + m - 1)) * rri[l + m] * rrj[m + 2] + T(m * (m - 1)) * rri[m] * rrj[l + m + 2];
+            T pjj = T((l + m) * (l + m - 1)) * rrj[l + m] * rri[m + 2] + T(m * (m - 1)) * rrj[m] * rri[l + m + 2];
+            T fc = uu[k + 2] * st;
+            T fu = T(k) * uu[k + 1] * st, fuu = T(k * (k - 1)) * uu[k] * st;
+            T fi = uu[k + 2] * pi_, fj = uu[k + 2] * pj_, fii = uu[k + 2] * pii, fjj = uu[k + 2] * pjj;
+            T fui = T(k) * uu[k + 1] * pi_, fuj = T(k) * uu[k + 1] * pj_;
+            fuu = fuu * dd1 * dd1 + fu * dd2;
+            fui = fui * dd1 * dd7;
+            fuj = fuj * dd1 * dd8;
+            fii = fii * dd7 * dd7 + fi * dd9;
+            fjj = fjj * dd8 * dd8 + fj * dd10;
+            fu = fu * dd1 / rij;
+            fi = fi * dd7 / ri;
+            fj = fj * dd8 / rj;
+            double lap = (double)(2 * (2 * fu + fi + fj) + 2 * fuu + fii + fjj + fui * cpst + fuj * cmst);
+            kc[ll] += lap + 2.0 * ((double)fi * vi_ri + (double)fu * vi_rv + (double)fj * vj_rj - (double)fu * vj_rv);
+            oc[ll] += (double)fc;
+          }
+          if (J.nct > 1) {  // each centre type has its own c set
+            const int base = pg.na + pg.nb + s.ctype[c] * tl.n;
+#pragma unroll
+            for (int ll = 0; ll < tl.n; ll++) {
+              atomicAdd(&pg.K[base + ll], kc[ll]);
+              atomicAdd(&pg.old[i * P + base + ll], oc[ll]);
+              atomicAdd(&pg.old[j * P + base + ll], oc[ll]);
+              kc[ll] = oc[ll] = 0.0;
+            }
+          }
+        }
+        if (J.nct == 1) {
+          const int base = pg.na + pg.nb;
+#pragma unroll
+          for (int ll = 0; ll < tl.n; ll++) {
+            atomicAdd(&pg.old[i * P + base + ll], oc[ll]);
+            atomicAdd(&pg.old[j * P + base + ll], oc[ll]);
+          }
+        }
+      }
+    if (J.nct == 1) {
+#pragma unroll
+      for (int ll = 0; ll < tl.n; ll++) {
+        double a = warp_sum(kc[ll]);
+        if (lane == 0) pg.K[pg.na + pg.nb + ll] += a;
+      }
+    }
+  }
+  // e-n parameters: lanes along electrons, centres in registers
+  {
+    double ot[MAXORD], kt[MAXORD];
+    for (int i = lane; i < N; i += 32) {
+#pragma unroll
+      for (int k = 0; k < MAXORD; k++) ot[k] = kt[k] = 0.0;
+      const double *xi = v.xs + 3 * i, *vi = pg.vt + 3 * i;
       for (int c = 0; c < C; c++) {
         const double *cc = s.cent + 3 * c;
-        T ri = ri_[2 * c], di = ri_[2 * c + 1], rj = rj_[2 * c], dj = rj_[2 * c + 1];
-        double vi_ri = vi[0] * (xi[0] - cc[0]) + vi[1] * (xi[1] - cc[1]) + vi[2] * (xi[2] - cc[2]);
-        double vi_rv = vi[0] * rvd[0] + vi[1] * rvd[1] + vi[2] * rvd[2];
-        double vj_rj = vj[0] * (xj[0] - cc[0]) + vj[1] * (xj[1] - cc[1]) + vj[2] * (xj[2] - cc[2]);
-        double vj_rv = vj[0] * rvd[0] + vj[1] * rvd[1] + vj[2] * rvd[2];
-        // power tables with two zero entries below 0, as in jas_een
-        T uu[NORD + 3], rri[NORD + 3], rrj[NORD + 3];
-        uu[0] = uu[1] = rri[0] = rri[1] = rrj[0] = rrj[1] = T(0);
-        uu[2] = rri[2] = rrj[2] = T(1);
+        T r = v.ren[2 * (i * C + c)], d = v.ren[2 * (i * C + c) + 1];
+        double v_r = vi[0] * (xi[0] - cc[0]) + vi[1] * (xi[1] - cc[1]) + vi[2] * (xi[2] - cc[2]);
 #pragma unroll
-        for (int q = 1; q <= NORD; q++) {
-          uu[q + 2] = uu[q + 1] * du;
-          rri[q + 2] = rri[q + 1] * di;
-          rrj[q + 2] = rrj[q + 1] * dj;
+        for (int k = 2; k < MAXORD; k++) {
+          if (k > J.norda) break;
+          T t, t1, t2;
+          en_param_terms(J, r, d, k, t, t1, t2, true);
+          ot[k - 2] += (double)t;
+          kt[k - 2] += (double)(t2 + 2 * t1) + 2.0 * (double)t1 * v_r;
         }
-        T dd1 = -sk * du * du, dd7 = -sk * di * di, dd8 = -sk * dj * dj;
-        T dd2 = 2 * sk * sk * du * du * du, dd9 = 2 * sk * sk * di * di * di, dd10 = 2 * sk * sk * dj * dj * dj;
-        T sp = ri + rj, tm = ri - rj;
-        T cpst = (rij * rij + sp * tm) / (ri * rij), cmst = (rij * rij - sp * tm) / (rj * rij);
-        const int base = pg.na + pg.nb + s.ctype[c] * tl.n;
+        if (J.nct > 1 || c == C - 1) {  // flush: per centre with several types, else once
+          const int it = s.ctype[c];
 #pragma unroll
-        for (int ll = 0; ll < tl.n; ll++) {
-          const int k = tl.k[ll], l = tl.l[ll], m = tl.m[ll];
-          T ssl = (l == 0) ? T(2) : rri[l + 2] + rrj[l + 2];
-          T st = ssl * rri[m + 2] * rrj[m + 2];
-          T pi_ = T(l + m) * rri[l + m + 1] * rrj[m + 2] + T(m) * rri[m + 1] * rrj[l + m + 2];
-          T pj_ = T(l + m) * rrj[l + m + 1] * rri[m + 2] + T(m) * rrj[m + 1] * rri[l + m + 2];
-          T pii = T((l + m) * (l + m - 1)) * rri[l + m] * rrj[m + 2] + T(m * (m - 1)) * rri[m] * rrj[l + m + 2];
-          T pjj = T((l + m) * (l + m - 1)) * rrj[l + m] * rri[m + 2] + T(m * (m - 1)) * rrj[m] * rri[l + m + 2];
-          T fc = uu[k + 2] * st;
-          T fu = T(k) * uu[k + 1] * st, fuu = T(k * (k - 1)) * uu[k] * st;
-          T fi = uu[k + 2] * pi_, fj = uu[k + 2] * pj_, fii = uu[k + 2] * pii, fjj = uu[k + 2] * pjj;
-          T fui = T(k) * uu[k + 1] * pi_, fuj = T(k) * uu[k + 1] * pj_;
-          fuu = fuu * dd1 * dd1 + fu * dd2;
-          fui = fui * dd1 * dd7;
-          fuj = fuj * dd1 * dd8;
-          fii = fii * dd7 * dd7 + fi * dd9;
-          fjj = fjj * dd8 * dd8 + fj * dd10;
-          fu = fu * dd1 / rij;
-          fi = fi * dd7 / ri;
-          fj = fj * dd8 / rj;
-          double lap = (double)(2 * (2 * fu + fi + fj) + 2 * fuu + fii + fjj + fui * cpst + fuj * cmst);
-          double kk = lap + 2.0 * ((double)fi * vi_ri + (double)fu * vi_rv + (double)fj * vj_rj - (double)fu * vj_rv);
-          atomicAdd(&pg.G[base + ll], (double)fc);
-          atomicAdd(&pg.K[base + ll], kk);
-          atomicAdd(&pg.old[i * P + base + ll], (double)fc);
-          atomicAdd(&pg.old[j * P + base + ll], (double)fc);
+          for (int k = 2; k < MAXORD; k++) {
+            if (k > J.norda) break;
+            const int ip = it * (J.norda - 1) + (k - 2);
+            pg.old[i * P + ip] += ot[k - 2];
+            atomicAdd(&pg.K[ip], kt[k - 2]);
+            ot[k - 2] = kt[k - 2] = 0.0;
+          }
         }
       }
     }
   }
-  for (int idx = lane; idx < N * C; idx += 32) {
-    int i = idx / C, c = idx - i * C;
-    const double *xi = v.xs + 3 * i, *cc = s.cent + 3 * c, *vi = pg.vt + 3 * i;
-    T r = v.ren[2 * idx], d = v.ren[2 * idx + 1];
-    double v_r = vi[0] * (xi[0] - cc[0]) + vi[1] * (xi[1] - cc[1]) + vi[2] * (xi[2] - cc[2]);
-    int it = s.ctype[c];
-    for (int k = 2; k <= J.norda; k++) {
-      T t, t1, t2;
-      en_param_terms(J, r, d, k, t, t1, t2, true);
-      int ip = it * (J.norda - 1) + (k - 2);
-      atomicAdd(&pg.G[ip], (double)t);
-      atomicAdd(&pg.K[ip], (double)(t2 + 2 * t1) + 2.0 * (double)t1 * v_r);
-      atomicAdd(&pg.old[i * P + ip], (double)t);
-    }
+  __syncwarp();
+  // G from the per-electron sums: pair parameters are counted on both electrons of the pair
+  for (int p = lane; p < P; p += 32) {
+    double g = 0;
+    for (int e = 0; e < N; e++) g += pg.old[e * P + p];
+    pg.G[p] = p < pg.na ? g : 0.5 * g;
   }
   __syncwarp();
 }
@@ -249,6 +331,7 @@ struct PGOut {
   int nfree;
   double *scr;     // per-walker scratch of the CSF/orbital part (null when there is none)
   size_t scr_stride;
+  int part;        // 1: E_L, Jastrow derivatives, local B; 2: CSF and orbital derivatives
 };
 
 // CSF and orbital-rotation derivatives from the orbital-resolved local energy
@@ -379,16 +462,15 @@ __device__ void md_orbital_tables(const Sys<T> &s, const View<T> &v, int lane, d
   }
 }
 
-template <class T, bool MD>
-__device__ void orbital_csf_derivs(const Sys<T> &s, const View<T> &v, const PGBuf &pg, const EvalRes &res, int lane,
-                                   double *scr, double *ol, double *oe) {
-  const int N = s.N, B = s.nbasis, M = s.norb, nmax = s.nmax;
+// Orbital-resolved local energy (elocal_orb_bld, deriv_fast_mod.f90:174-210), local part:
+// orbitals of all M orbitals with gradient and Laplacian, and
+// B[e][m] = -hb (lap phi_m + 2 v_J . grad phi_m + ddjas phi_m) + vloc phi_m.  The nonlocal part
+// sum_b phis[e][b] coef[b][m] is added afterwards by one batched GEMM over all walkers.
+template <class T>
+__device__ void orbital_local_energy(const Sys<T> &s, const View<T> &v, const EvalRes &res, int lane, double *scr) {
+  const int N = s.N, B = s.nbasis, M = s.norb;
   double *orbA = scr + (size_t)N * B;
   double *Bm = orbA + (size_t)N * 5 * M;
-  double *Ta = Bm + (size_t)N * M;
-  double *dTa = Ta + (size_t)2 * nmax * M;
-  double *Qr = dTa + (size_t)2 * nmax * M;
-  double *delo = Qr + (size_t)nmax * nmax;
   for (int e = 0; e < N; e++) {
     warp_basis<T, 5>(s, v.xs + 3 * e, v.phi, lane);
     warp_orbitals<T, 5>(v.phi, s.call, B, M, orbA + (size_t)e * 5 * M, M, lane);
@@ -398,12 +480,22 @@ __device__ void orbital_csf_derivs(const Sys<T> &s, const View<T> &v, const PGBu
     int e = i / M, m = i - e * M;
     const double *o = orbA + (size_t)e * 5 * M + m;
     const double *vj = v.vacc + 3 * e;
-    double b = -HB * (o[4 * M] + 2 * (vj[0] * o[M] + vj[1] * o[2 * M] + vj[2] * o[3 * M]) + ddjas * o[0]) + vloc * o[0];
-    const double *ph = scr + (size_t)e * B;
-    for (int k = 0; k < B; k++) b += ph[k] * (double)s.call[(size_t)k * M + m];
-    Bm[i] = b;
+    Bm[i] = -HB * (o[4 * M] + 2 * (vj[0] * o[M] + vj[1] * o[2 * M] + vj[2] * o[3 * M]) + ddjas * o[0]) + vloc * o[0];
   }
   __syncwarp();
+}
+
+// CSF and orbital-rotation derivatives from the orbitals and the complete B matrix.
+template <class T, bool MD>
+__device__ void orbital_csf_derivs(const Sys<T> &s, const View<T> &v, double eloc, int lane, double *scr, double *ol,
+                                   double *oe) {
+  const int N = s.N, B = s.nbasis, M = s.norb, nmax = s.nmax;
+  double *orbA = scr + (size_t)N * B;
+  double *Bm = orbA + (size_t)N * 5 * M;
+  double *Ta = Bm + (size_t)N * M;
+  double *dTa = Ta + (size_t)2 * nmax * M;
+  double *Qr = dTa + (size_t)2 * nmax * M;
+  double *delo = Qr + (size_t)nmax * nmax;
   double eref = 0;
   for (int sp = 0; sp < 2; sp++) {
     const int n = sp ? s.ndn : s.nup, e0 = sp ? s.nup : 0;
@@ -470,7 +562,7 @@ __device__ void orbital_csf_derivs(const Sys<T> &s, const View<T> &v, const PGBu
         double r = wd[iu] * wd[nd0 + id] / chi;
         double eK = eref + delo[iu] + delo[nd0 + id];
         dl += s.csf_cd[t] * r;
-        de += s.csf_cd[t] * r * (eK - res.eloc);
+        de += s.csf_cd[t] * r * (eK - eloc);
       }
       ol[q - 1] = dl;
       oe[q - 1] = de;
@@ -505,9 +597,11 @@ __device__ void orbital_csf_derivs(const Sys<T> &s, const View<T> &v, const PGBu
 }
 
 template <class T, int NORD, bool MD>
+// part 1: E_L with the Jastrow parameter derivatives and the local part of B; part 2 (after the
+// nonlocal part of B was added for all walkers): CSF and orbital-rotation derivatives.
 __global__ void __launch_bounds__(128, 4) k_pgrad(Sys<T> s, State<T> st, Layout L, PGOut out, double r0, double r1,
                                                   double r2, double r3, double r4, double r5, double r6, double r7,
-                                                  double r8) {
+                                                  double r8, int part) {
   __shared__ JasPar<T> J;
   __shared__ EcpPar E;
   extern __shared__ __align__(16) char dsm[];
@@ -533,6 +627,11 @@ __global__ void __launch_bounds__(128, 4) k_pgrad(Sys<T> s, State<T> st, Layout 
     pg.P = P; pg.na = na; pg.nb = nb;
     double *scr = out.scr ? out.scr + (size_t)w * out.scr_stride : nullptr;
     pg.phis = scr;
+    if (part == 2) {
+      orbital_csf_derivs<T, MD>(s, v, out.eloc[w], lane, scr, out.dlnpsi + (size_t)w * out.nfree,
+                                out.deloc + (size_t)w * out.nfree);
+      continue;
+    }
     for (int i = lane; i < (int)(pgbytes / sizeof(double)); i += 32) pg.vt[i] = 0.0;
     if (scr)
       for (int i = lane; i < N * s.nbasis; i += 32) scr[i] = 0.0;
@@ -551,7 +650,7 @@ __global__ void __launch_bounds__(128, 4) k_pgrad(Sys<T> s, State<T> st, Layout 
     __syncwarp();
     // output order: CSF, orbital rotations, Jastrow (as deriv_mod.f90:120-247 concatenates them)
     double *ol = out.dlnpsi + (size_t)w * out.nfree, *oe = out.deloc + (size_t)w * out.nfree;
-    if (scr) orbital_csf_derivs<T, MD>(s, v, pg, res, lane, scr, ol, oe);
+    if (scr) orbital_local_energy<T>(s, v, res, lane, scr);
     const int jo = (MD && s.ncsf > 1 ? s.ncsf - 1 : 0) + s.norbp;
     ol += jo;
     oe += jo;

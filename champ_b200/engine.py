@@ -23,6 +23,7 @@ EXPORTED_SYMBOLS = [
     "champ_propose_1e", "champ_accept_1e", "champ_grad_1e", "champ_vmc_sweeps", "champ_vmc_run_host",
     "champ_walker_status", "champ_synchronize", "champ_param_grad", "champ_accumulate_oh",
     "champ_dmc_init", "champ_dmc_steps", "champ_num_walkers", "champ_eval_energy_noalloc", "champ_set_option",
+    "champ_get_option",
 ]
 
 PREC = {"fp64": 0, "mixed": 1}
@@ -75,6 +76,7 @@ def load_library(path: str = LIB_PATH):
     L.champ_num_walkers.argtypes = [vp, C.POINTER(i32)]
     L.champ_eval_energy_noalloc.argtypes = [vp, i32, vp, vp]
     L.champ_set_option.argtypes = [vp, C.c_char_p, C.c_int64]
+    L.champ_get_option.argtypes = [vp, C.c_char_p, C.POINTER(C.c_int64)]
     for n in EXPORTED_SYMBOLS:
         if n not in ("champ_last_error", "champ_version"):
             getattr(L, n).restype = C.c_int
@@ -222,6 +224,11 @@ class Engine:
 
     def set_option(self, name: str, value: int):
         self._check(self.lib.champ_set_option(self.h, name.encode(), int(value)))
+
+    def get_option(self, name: str) -> int:
+        v = C.c_int64()
+        self._check(self.lib.champ_get_option(self.h, name.encode(), C.byref(v)))
+        return v.value
 
     def synchronize(self):
         self._check(self.lib.champ_synchronize(self.h))

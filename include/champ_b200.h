@@ -238,6 +238,9 @@ int champ_synchronize(champ_ctx *ctx);
    mixed precision when the walker state lives in HBM and a spin has >= 16 orbitals, and on by
    default there; CHAMP_EINVAL otherwise. */
 int champ_set_option(champ_ctx *ctx, const char *name, int64_t value);
+/* Current value of an option ("orbital_tc"); kernel launches per champ_vmc_sweeps sweep
+   ("launches_per_sweep": 1 for the fused sweep kernel, 5 with the tensor-core orbitals). */
+int champ_get_option(const champ_ctx *ctx, const char *name, int64_t *value);
 
 #ifdef __cplusplus
 }
