@@ -306,6 +306,26 @@ def measure(system, nw, prec, steps, warmup, pg_steps, rank, world, flush, torch
     return out
 
 
+def mixed_error_of(system, nw, seed=5):
+    """|E_L(mixed) - E_L(FP64)| on identical walkers of one system (eval_full of both engines)."""
+    from champ_b200.engine import Engine
+    x = system_walkers(system, nw, seed=seed)
+    em, e64 = Engine(system, nw, "mixed"), Engine(system, nw, "fp64")
+    em.set_walkers(x)
+    e64.set_walkers(x)
+    em.vmc_sweeps(20, SEED, sweep0=0, step=step_size(system), stats=False)  # equilibrate the mixed walkers
+    xw = em.get_walkers()
+    em.set_walkers(xw)
+    e64.set_walkers(xw)
+    a, b = em.eval_full(), e64.eval_full()
+    d = np.abs(a["energy"] - b["energy"])
+    out = {"system": system.name, "walkers": nw, "max_abs_dEL_Ha": float(d.max()), "median_abs_dEL_Ha": float(np.median(d)),
+           "frac_samples_within_1e-6_Ha": float(np.mean(d <= 1e-6))}
+    em.close()
+    e64.close()
+    return out
+
+
 def main():
     global ARGS
     args = ARGS = parse()
@@ -372,6 +392,9 @@ def main():
         big = {"workload": config_of(s5, s5.walkers, "mixed")["workload"], "walkers_per_gpu": s5.walkers, **b}
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             big["cpu_baseline"] = cpu_baseline_sample(s5, seconds=8.0)
+    # the same error on a physical wave function (the reference's Be example: 4 determinants,
+    # Slater basis, optimised Jastrow), where E_L varies little between samples
+    phys = mixed_error_of(S.be_example(), 4096) if prec == "mixed" else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(system)
@@ -382,7 +405,7 @@ def main():
                 "config": config_of(system, nw, prec), "clocks": m["clocks"],
                 "gpu_launches": args.steps * m["launches_per_step"],
                 "roofline": roof, "fp64_arm": m.get("fp64_arm"), "param_grad": m["param_grad"],
-                "mixed_error": m.get("mixed_error"), "e2e": e2e, "cpu_baseline": cpu,
+                "mixed_error": m.get("mixed_error"), "mixed_error_physical": phys, "e2e": e2e, "cpu_baseline": cpu,
                 "wall_s_timed_region": m["wall_s_timed_region"], "cluster128": big}
         print(json.dumps(line), flush=True)
     if world > 1:
