@@ -102,8 +102,8 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-# DRAM bytes per walker of one k_vmc launch, from the ncu capture summarised in
-# profiles/k_vmc_c2_dimer_sweep.md (2048 walkers, mixed precision: 6.26 MB read + 0.10 MB
+# DRAM bytes per walker of one k_vmc launch, from a full ncu capture of one launch
+# (2048 walkers, mixed precision: 6.26 MB read + 0.10 MB
 # written); the traffic grows with the walker count, so a full launch is scaled by walkers.
 KVMC_DRAM_BYTES_PER_WALKER = {(2, "mixed"): (6.263552e6 + 0.099072e6) / 2048}
 
@@ -355,7 +355,7 @@ def main():
     tpw = KVMC_DRAM_BYTES_PER_WALKER.get((args.system, prec))
     roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / peaks["hbm_gbs"], "traffic": (tpw * nw) if tpw else None,
-            "traffic_source": "ncu dram__bytes_read+write per walker x walkers (profiles/k_vmc_c2_dimer_sweep.md)"
+            "traffic_source": "ncu dram__bytes_read+write of one 2048-walker launch, per walker x walkers"
             if tpw else None, "algorithmic_bytes": alg_bytes, "peak_source": peak_kind,
             "kernel": "k_vmc (fused sweep)",
             "note": "algorithmic bytes = persistent walker state read+written once per sweep; the kernel is "

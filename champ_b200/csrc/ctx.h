@@ -78,6 +78,7 @@ struct champ_ctx {
   int dmc_step = 0;
   // tensor-core orbital contraction of the full evaluation (mixed precision, state in HBM)
   int num_sms = 0;
+  int reinv_every = 1;            // VMC sweeps between FP64 re-inversions of the Slater matrices
   int tc_on = 0, tc_ok = 0;       // in use; supported for this system and precision
   int tc_Kp = 0, tc_Np[2] = {0, 0}, tc_ncols[2] = {32, 32};
   float *tc_phi = nullptr;        // [wmax*N*5][Kp] basis rows

@@ -844,6 +844,7 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
   }
   rc = c->prec == CHAMP_PREC_FP64 ? attrs_f64(c) : attrs_f32(c);
   if (!rc) rc = tc_setup(c);
+  c->reinv_every = std::max(1, (100 + c->N - 1) / c->N);  // about every 100 single-electron moves
   if (rc) { champ_destroy(c); return rc; }
   c->d_in = dalloc<double>(c, (size_t)w_max * 3 * c->N);
   c->d_out = dalloc<double>(c, (size_t)w_max * 4 * c->N);
@@ -1202,6 +1203,11 @@ int champ_set_option(champ_ctx *c, const char *name, int64_t value) {
     c->tc_on = value ? 1 : 0;
     return CHAMP_OK;
   }
+  if (!strcmp(name, "reinvert_every")) {
+    if (value < 1 || value > (1 << 30)) return fail(CHAMP_EINVAL, "reinvert_every must be >= 1");
+    c->reinv_every = (int)value;
+    return CHAMP_OK;
+  }
   return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);
 }
 
@@ -1209,6 +1215,7 @@ int champ_get_option(const champ_ctx *c, const char *name, int64_t *value) {
   if (!c || !name || !value) return fail(CHAMP_EINVAL, "null argument");
   if (!strcmp(name, "orbital_tc")) { *value = c->tc_on; return CHAMP_OK; }
   if (!strcmp(name, "launches_per_sweep")) { *value = c->tc_on ? 5 : 1; return CHAMP_OK; }
+  if (!strcmp(name, "reinvert_every")) { *value = c->reinv_every; return CHAMP_OK; }
   return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);
 }
 

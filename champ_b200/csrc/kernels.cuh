@@ -474,7 +474,7 @@ __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const Vi
 template <class T, int NORD, bool MD, bool PG = false>
 __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, const State<T> &st, int w,
                           const View<T> &v, const double *R, int lane, bool outputs, EvalRes &res,
-                          const PGBuf *pg = nullptr, bool orbs_ready = false) {
+                          const PGBuf *pg = nullptr, bool orbs_ready = false, bool reinvert = true) {
   const int N = s.N, C = s.C, nomax = s.nomax;
   const double *xs = v.xs;
   T *fso = v.fso;
@@ -598,12 +598,19 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
       warp_basis<T, 5>(s, xs + 3 * e, v.phi, lane);
       warp_orbitals<T, 5>(v.phi, s.cocc[sp], s.nbasis, s.nocc[sp], oe, nomax, lane);
     }
-    for (int k = lane; k < n; k += 32) A[eo * n + k] = (double)oe[k];
+    if (reinvert)
+      for (int k = lane; k < n; k += 32) A[eo * n + k] = (double)oe[k];
   }
   __syncwarp();
   double lnd = 0, sgn = 1;
   bool ok = true;
-  for (int sp = 0; sp < 2; sp++) {
+  if (!reinvert) {
+    // inverses, T and G as kept current by the accepted moves' updates; ln|psi_D| likewise
+    lnd = st.lnd[w];
+    sgn = st.sgn[w];
+    ok = isfinite(lnd) && sgn != 0.0;
+  }
+  for (int sp = 0; sp < 2 && reinvert; sp++) {
     int n = sp ? s.ndn : s.nup;
     if (n == 0) continue;
     double l1, s1;
@@ -612,7 +619,7 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
     lnd += l1;
     sgn *= s1;
   }
-  if (MD && ok) {
+  if (MD && ok && reinvert) {
     // T = Ainv Atilde on the virtual columns (t_bld, deriv_fast_mod.f90:367-398)
     for (int sp = 0; sp < 2; sp++) {
       const int n = sp ? s.ndn : s.nup, nv = s.nvirt[sp], e0 = sp ? s.nup : 0;
@@ -1097,11 +1104,11 @@ __global__ void __launch_bounds__(128, 4) k_accept(Sys<T> s, State<T> st, Layout
 }
 
 // Fused VMC: nsweep sweeps of single-electron Metropolis moves plus E_L after each sweep
-// (phase 0).  Phase 1 runs only the moves and phase 2 only the E_L, from orbitals computed in
+// (phase 0); the E_L re-inverts the Slater matrices every reinv_every sweeps.  Phase 1 runs only the moves and phase 2 only the E_L, from orbitals computed in
 // between for all walkers (tensor-core contraction).  Statistics are added to st.s_*.
 template <class T, int NORD, bool MD>
 __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L, int nsweep, uint64_t seed,
-                                                uint64_t sweep0, double step, int phase) {
+                                                uint64_t sweep0, double step, int phase, int reinv_every) {
   __shared__ JasPar<T> J;
   __shared__ EcpPar E;
   extern __shared__ __align__(16) char dsm[];
@@ -1135,7 +1142,9 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
       double R[9];
       random_rotation(seed, (uint32_t)w, sweep, R);
       EvalRes res;
-      full_eval<T, NORD, MD>(s, J, E, st, w, v, R, lane, false, res, nullptr, phase == 2);
+      // periodic FP64 re-inversion: every reinv_every sweeps, in between the updated inverses
+      const bool reinv = reinv_every <= 1 || sweep % (uint64_t)reinv_every == 0;
+      full_eval<T, NORD, MD>(s, J, E, st, w, v, R, lane, false, res, nullptr, phase == 2, reinv);
       el = res.eloc;
       es += el;
       e2 += el * el;

@@ -123,16 +123,19 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
     CK(cudaMemsetAsync(st.s_acc, 0, sizeof(double) * st.W, c->stream));
     const bool tc = c->tc_on && !a.st_override;  // only mixed-precision contexts turn it on
     if (!tc) {
-      k_vmc<T, NORD, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, a.nsweep, a.seed, a.sweep0, a.step, 0);
+      k_vmc<T, NORD, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, a.nsweep, a.seed, a.sweep0, a.step, 0,
+                                                               c->reinv_every);
       break;
     }
     // per sweep: moves, orbitals of all walkers on the tensor cores, E_L
     for (int isw = 0; isw < a.nsweep; isw++) {
-      k_vmc<T, NORD, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, 1, a.seed, a.sweep0 + isw, a.step, 1);
+      k_vmc<T, NORD, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, 1, a.seed, a.sweep0 + isw, a.step, 1,
+                                                               c->reinv_every);
       CK(cudaGetLastError());
       int rc = run_orb_tc<T>(c, st);
       if (rc) return rc;
-      k_vmc<T, NORD, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, 1, a.seed, a.sweep0 + isw, a.step, 2);
+      k_vmc<T, NORD, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, 1, a.seed, a.sweep0 + isw, a.step, 2,
+                                                               c->reinv_every);
       CK(cudaGetLastError());
     }
     break;

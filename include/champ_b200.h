@@ -236,9 +236,13 @@ int champ_synchronize(champ_ctx *ctx);
    every electron of every walker) as one tcgen05 tensor-core contraction per spin with a
    3-term TF32 split (about FP32 accuracy); 0 uses the CUDA-core contraction.  Available for
    mixed precision when the walker state lives in HBM and a spin has >= 16 orbitals, and on by
-   default there; CHAMP_EINVAL otherwise. */
+   default there; CHAMP_EINVAL otherwise.
+   "reinvert_every": the full evaluation after a VMC sweep re-inverts the Slater matrices in
+   FP64 every this many sweeps (sweep index divisible by it) and otherwise uses the inverses
+   kept current by the Sherman-Morrison updates of the accepted moves; default
+   ceil(100 / nelec), i.e. a re-inversion about every 100 single-electron moves. */
 int champ_set_option(champ_ctx *ctx, const char *name, int64_t value);
-/* Current value of an option ("orbital_tc"); kernel launches per champ_vmc_sweeps sweep
+/* Current value of an option ("orbital_tc", "reinvert_every"); kernel launches per champ_vmc_sweeps sweep
    ("launches_per_sweep": 1 for the fused sweep kernel, 5 with the tensor-core orbitals). */
 int champ_get_option(const champ_ctx *ctx, const char *name, int64_t *value);
 

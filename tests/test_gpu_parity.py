@@ -142,6 +142,30 @@ def test_vmc_sweeps_follow_the_oracle_trajectory(oracle_mod):
     assert np.allclose(st["esum"][m], ref["esum"][m], rtol=1e-8, atol=1e-7)
 
 
+@pytest.mark.parametrize("k", [2, 3])
+def test_vmc_periodic_reinversion_matches_every_sweep(k):
+    """The E_L after a sweep with the Sherman-Morrison-updated inverses (re-inversion every
+    reinvert_every sweeps, by default about every 100 moves) equals the one with a fresh FP64
+    re-inversion after every sweep: same walk, local energies to 1e-9 relative."""
+    s = get(k)
+    nw = 64
+    x = S.initial_walkers(s, nw, seed=18)
+    res = {}
+    for every in (1, 13):
+        eng = make_engine(s, nw, "fp64")
+        eng.set_option("reinvert_every", every)
+        assert eng.get_option("reinvert_every") == every
+        eng.set_walkers(x)
+        st = eng.vmc_sweeps(12, seed=77, sweep0=1, step=0.4)
+        res[every] = (eng.get_walkers(), st)
+    # both inverses agree to rounding, so a Metropolis decision at the last bit may split a walker
+    same = np.all(res[1][0] == res[13][0], axis=(1, 2))
+    assert same.sum() >= nw - 1
+    for key in ("esum", "e2sum", "elast"):
+        a, b = res[1][1][key][same], res[13][1][key][same]
+        assert np.allclose(a, b, rtol=1e-9, atol=1e-9 * np.abs(a).max()), key
+
+
 def test_walker_status_clean(oracle_mod):
     s = S.c2_dimer()
     eng = make_engine(s, 16, "fp64")
