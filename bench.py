@@ -103,9 +103,9 @@ class ClockSampler:
 
 
 # DRAM bytes per walker of one k_vmc launch, from a full ncu capture of one launch
-# (2048 walkers, mixed precision: 6.26 MB read + 0.10 MB
+# (2048 walkers, mixed precision: 6.88 MB read + 0.17 MB
 # written); the traffic grows with the walker count, so a full launch is scaled by walkers.
-KVMC_DRAM_BYTES_PER_WALKER = {(2, "mixed"): (6.263552e6 + 0.099072e6) / 2048}
+KVMC_DRAM_BYTES_PER_WALKER = {(2, "mixed"): (6.883072e6 + 0.165888e6) / 2048}
 
 
 def measured_peaks():
