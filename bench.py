@@ -224,17 +224,17 @@ def time_engine(eng, system, args, nsteps, nwarm, flush, torch, sweep_base):
 
 def allmax(x, world, torch, dist):
     """Max over ranks of a per-rank number (every rank calls this in the same order)."""
-    if world == 1:
-        return x
-    t = torch.tensor([x], device="cuda", dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from champ_b200.dist import max_over_ranks
+    return max_over_ranks(x)
 
 
 def time_param_grad(eng, system, nsteps, flush, torch):
     """d ln psi/dp and dE_L/dp for every walker, folded into the FP64 O/H accumulators (one
-    champ_param_grad + champ_accumulate_oh per step); the walkers move by one VMC sweep between
-    steps, outside the timed events.  Returns ms for nsteps."""
+    champ_param_grad + champ_accumulate_oh per step, and with several ranks the all-reduce of
+    the accumulators, the one exchange step of the path); the walkers move by one VMC sweep
+    between steps, outside the timed events.  Returns ms for nsteps."""
+    from champ_b200.dist import reduce_oh, rank_world
+    multi = rank_world()[1] > 1
     tpg = 0.0
     for k in range(nsteps + 2):
         eng.vmc_sweeps(1, SEED, sweep0=30000 + k, step=step_size(system), stats=False)
@@ -244,6 +244,8 @@ def time_param_grad(eng, system, nsteps, flush, torch):
         e0.record()
         eng.param_grad(host=False)
         eng._check(lib_accumulate(eng))
+        if multi:
+            reduce_oh(eng)
         e1.record()
         torch.cuda.synchronize()
         if k >= 2:

@@ -929,6 +929,13 @@ int champ_param_grad(champ_ctx *c, double *dlnpsi, double *deloc, double *eloc) 
   return CHAMP_OK;
 }
 
+int champ_oh_buffers(const champ_ctx *c, const double **S, const double **H) {
+  if (!c || !S || !H) return fail(CHAMP_EINVAL, "null argument");
+  *S = c->oh_s;
+  *H = c->oh_h;
+  return CHAMP_OK;
+}
+
 int champ_accumulate_oh(champ_ctx *c, const double *weights, double *S, double *H) {
   if (!c) return fail(CHAMP_EINVAL, "null context");
   if (!c->have_pgrad) return fail(CHAMP_ESTATE, "call champ_param_grad first");

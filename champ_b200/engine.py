@@ -23,7 +23,7 @@ EXPORTED_SYMBOLS = [
     "champ_propose_1e", "champ_accept_1e", "champ_grad_1e", "champ_vmc_sweeps", "champ_vmc_run_host",
     "champ_walker_status", "champ_synchronize", "champ_param_grad", "champ_accumulate_oh",
     "champ_dmc_init", "champ_dmc_steps", "champ_num_walkers", "champ_eval_energy_noalloc", "champ_set_option",
-    "champ_get_option",
+    "champ_get_option", "champ_oh_buffers",
 ]
 
 PREC = {"fp64": 0, "mixed": 1}
@@ -77,6 +77,7 @@ def load_library(path: str = LIB_PATH):
     L.champ_eval_energy_noalloc.argtypes = [vp, i32, vp, vp]
     L.champ_set_option.argtypes = [vp, C.c_char_p, C.c_int64]
     L.champ_get_option.argtypes = [vp, C.c_char_p, C.POINTER(C.c_int64)]
+    L.champ_oh_buffers.argtypes = [vp, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
     for n in EXPORTED_SYMBOLS:
         if n not in ("champ_last_error", "champ_version"):
             getattr(L, n).restype = C.c_int
@@ -201,6 +202,12 @@ class Engine:
         w = None if weights is None else np.ascontiguousarray(weights, np.float64)
         self._check(self.lib.champ_accumulate_oh(self.h, _p(w) if w is not None else None, _p(S), _p(H)))
         return S, H
+
+    def oh_buffers(self):
+        """Device addresses of the S and H accumulators ((P+1)^2 FP64 each, row-major)."""
+        S, H = C.c_void_p(), C.c_void_p()
+        self._check(self.lib.champ_oh_buffers(self.h, C.byref(S), C.byref(H)))
+        return S.value, H.value
 
     def dmc_init(self, w_target, tau, gpop=10.0):
         self._check(self.lib.champ_dmc_init(self.h, w_target, tau, gpop))

@@ -202,6 +202,11 @@ int champ_param_grad(champ_ctx *ctx, double *dlnpsi /* [nw][P] */, double *deloc
    champ_param_grad, with optional weights: with Oa = (1, dlnpsi) and Mb = (E_L, E_L dlnpsi + deloc),
    S[a][b] = sum_w wt_w Oa_a Oa_b and H[a][b] = sum_w wt_w Oa_a Mb_b, row-major (P+1)x(P+1), in FP64. */
 int champ_accumulate_oh(champ_ctx *ctx, const double *weights /* [nw] or NULL */, double *S, double *H);
+/* Device addresses of the O/H accumulators that champ_accumulate_oh fills (row-major
+   (P+1)x(P+1) FP64, owned by the context, valid until champ_destroy), for a caller that reduces
+   them across ranks on the device (the MPI reduction of the averages in the reference,
+   deriv_mod.f90:683,898,1375) without copying them to the host. */
+int champ_oh_buffers(const champ_ctx *ctx, const double **S, const double **H);
 
 /* Diffusion Monte Carlo (rundmc, qmc/rundmc_mod.f90:17-422).  champ_dmc_init starts from the
    current walkers (weight 1); w_target is the target population and the trial energy follows

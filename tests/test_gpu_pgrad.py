@@ -153,3 +153,22 @@ def test_oh_accumulation_matches_numpy():
     Mb = np.hstack([el[:, None], el[:, None] * dl + de])
     assert np.allclose(Sm, (Oa * wt[:, None]).T @ Oa, rtol=1e-12, atol=1e-9)
     assert np.allclose(Hm, (Oa * wt[:, None]).T @ Mb, rtol=1e-12, atol=1e-7)
+
+
+def test_oh_device_buffers_match_host_copy():
+    """champ_oh_buffers exposes the same accumulators champ_accumulate_oh copies to the host (the
+    device tensors the multi-rank all-reduce sums in place)."""
+    import torch
+    from champ_b200.engine import Engine
+    from champ_b200.dist import oh_tensors, reduce_oh
+    s = S.c2_dimer()
+    nw = 128
+    eng = Engine(s, nw, "fp64")
+    eng.set_walkers(S.initial_walkers(s, nw, seed=4))
+    eng.param_grad()
+    Sh, Hh = eng.accumulate_oh()
+    Sd, Hd = oh_tensors(eng)
+    torch.cuda.synchronize()
+    assert np.array_equal(Sd.cpu().numpy(), Sh) and np.array_equal(Hd.cpu().numpy(), Hh)
+    Sr, Hr = reduce_oh(eng)  # one rank: unchanged
+    assert np.array_equal(Sr.cpu().numpy(), Sh)
