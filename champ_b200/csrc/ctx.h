@@ -76,6 +76,11 @@ struct champ_ctx {
   void *scan_tmp = nullptr;
   size_t scan_bytes = 0;
   int dmc_step = 0;
+  // CUDA graph of two DMC steps (A->B->A buffers), captured on a private stream, replayed per pair
+  int dmc_graph_on = 1;
+  void *dmc_graph = nullptr, *dmc_exec = nullptr;  // cudaGraph_t, cudaGraphExec_t
+  uint64_t dmc_graph_seed = 0;
+  cudaStream_t cap_stream = nullptr;
   // tensor-core orbital contraction of the full evaluation (mixed precision, state in HBM)
   int num_sms = 0;
   int reinv_every = 1;            // VMC sweeps between FP64 re-inversions of the Slater matrices

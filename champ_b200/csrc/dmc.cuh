@@ -26,6 +26,7 @@ struct DmcData {
   int *ncopy, *off;       // [wmax]
   double *stat;           // [nstep][4]: population, sum w, sum w E_L, E_T
   double *red;            // [2] sum w, sum w E_L of the step
+  long long *ctr;         // [2] (device) step counter (random-number key), statistics record index
 };
 
 // averaged drift (averaged_1e_velocity with n_drift_param = 2)
@@ -37,7 +38,7 @@ __device__ __forceinline__ void avg_drift(const double *g, double tau, double a,
 }
 
 template <class T, int NORD, bool MD>
-__global__ void __launch_bounds__(128, 4) k_dmc_move(Sys<T> s, State<T> st, Layout L, DmcPar P, DmcData D, int step) {
+__global__ void __launch_bounds__(128, 4) k_dmc_move(Sys<T> s, State<T> st, Layout L, DmcPar P, DmcData D) {
   __shared__ JasPar<T> J;
   __shared__ EcpPar E;
   extern __shared__ __align__(16) char dsm[];
@@ -45,6 +46,7 @@ __global__ void __launch_bounds__(128, 4) k_dmc_move(Sys<T> s, State<T> st, Layo
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   const int N = s.N, W = *D.nw;
   const double et = *D.et, sqt = sqrt(P.tau);
+  const uint64_t step = (uint64_t)D.ctr[0];
   for (int w = blockIdx.x * wpb + wib; w < W; w += gridDim.x * wpb) {
     View<T> v = make_view<T>(dsm + L.bytes * wib, L, st, w, s.N, s.C, s.nbasis, s.nomax, L.resident != 0);
     if (L.resident) {
@@ -60,7 +62,7 @@ __global__ void __launch_bounds__(128, 4) k_dmc_move(Sys<T> s, State<T> st, Layo
       propose<T, NORD, MD, true>(s, J, st, w, v, e, xo, lane, r0, d0, go);  // grad at the current position
       avg_drift(go, P.tau, P.adrift, vo);
       double g[3], ua;
-      move_randoms(P.seed, (uint32_t)w, (uint64_t)step, (uint32_t)e, g, &ua);
+      move_randoms(P.seed, (uint32_t)w, step, (uint32_t)e, g, &ua);
       double xn[3];
       for (int k = 0; k < 3; k++) xn[k] = xo[k] + P.tau * vo[k] + sqt * g[k];
       double rho, dj;
@@ -76,7 +78,7 @@ __global__ void __launch_bounds__(128, 4) k_dmc_move(Sys<T> s, State<T> st, Layo
       }
     }
     double R[9];
-    random_rotation(P.seed, (uint32_t)w, (uint64_t)step, R);
+    random_rotation(P.seed, (uint32_t)w, step, R);
     EvalRes res;
     full_eval<T, NORD, MD>(s, J, E, st, w, v, R, lane, false, res);
     if (L.resident) view_store(v, st, w, N, s.C, lane);
@@ -98,13 +100,14 @@ __global__ void __launch_bounds__(128, 4) k_dmc_move(Sys<T> s, State<T> st, Layo
 }
 
 // weights -> copy counts (stochastic rounding); zero beyond the population
-static __global__ void k_dmc_count(DmcData D, DmcPar P, int step) {
+static __global__ void k_dmc_count(DmcData D, DmcPar P) {
   const int W = *D.nw;
+  const uint64_t step = (uint64_t)D.ctr[0];
   for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < P.wmax; w += gridDim.x * blockDim.x) {
     int nc = 0;
     if (w < W) {
       uint32_t o[4];
-      philox(P.seed, (uint32_t)w, (uint32_t)step, (uint32_t)((uint64_t)step >> 32), 0xFFFFFFFEu, o);
+      philox(P.seed, (uint32_t)w, (uint32_t)step, (uint32_t)(step >> 32), 0xFFFFFFFEu, o);
       double u = u53(o[0], o[1]);
       double c = floor(D.wt[w] + u);
       nc = c > 8 ? 8 : (int)c;
@@ -158,9 +161,11 @@ __global__ void k_dmc_copy(State<T> a, State<T> b, DmcData Da, DmcData Db, int N
   }
 }
 
-// new population, statistics record and trial-energy update (single thread)
-static __global__ void k_dmc_finish(DmcData Da, DmcData Db, DmcPar P, int istat) {
+// new population, statistics record and trial-energy update (single thread); advances the
+// device step counters, so a captured sequence of steps replays with fresh random numbers
+static __global__ void k_dmc_finish(DmcData Da, DmcData Db, DmcPar P) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const long long istat = Da.ctr[1];
   int W = *Da.nw;
   int tot = (W > 0) ? Da.off[P.wmax - 1] + Da.ncopy[P.wmax - 1] : 0;
   if (tot > P.wmax) tot = P.wmax;
@@ -183,4 +188,6 @@ static __global__ void k_dmc_finish(DmcData Da, DmcData Db, DmcPar P, int istat)
   Da.red[1] = 0;
   Db.red[0] = 0;
   Db.red[1] = 0;
+  Da.ctr[0] += 1;
+  Da.ctr[1] += 1;
 }

@@ -623,6 +623,66 @@ static int tc_setup(champ_ctx *c) {
   return CHAMP_OK;
 }
 
+// One DMC step (rundmc_mod.f90:17-422): drift-diffusion moves and E_L, weight sums, copy counts,
+// their prefix sum, the branching copy into the other state buffer, population and E_T update;
+// then the buffers swap roles.  Reads its step number from the device counter.
+static int dmc_one_step(champ_ctx *c) {
+  int rc = launch(c, Op::DmcMove);
+  if (rc) return rc;
+  k_dmc_sums<<<148, 256, 0, c->stream>>>(c->dA, c->dpar.wmax);
+  k_dmc_count<<<(c->dpar.wmax + 255) / 256, 256, 0, c->stream>>>(c->dA, c->dpar);
+  if (cub::DeviceScan::ExclusiveSum(c->scan_tmp, c->scan_bytes, c->dA.ncopy, c->dA.off, c->dpar.wmax, c->stream) !=
+      cudaSuccess)
+    return fail(CHAMP_ECUDA, "DMC scan failed");
+  rc = launch(c, Op::DmcCopy);
+  if (rc) return rc;
+  k_dmc_finish<<<1, 32, 0, c->stream>>>(c->dA, c->dB, c->dpar);
+  CK(cudaGetLastError());
+  std::swap(c->std_, c->std2);
+  std::swap(c->stf, c->stf2);
+  std::swap(c->dA.wt, c->dB.wt);
+  std::swap(c->dA.el, c->dB.el);
+  return CHAMP_OK;
+}
+
+static void dmc_graph_release(champ_ctx *c) {
+  if (c->dmc_exec) cudaGraphExecDestroy((cudaGraphExec_t)c->dmc_exec);
+  if (c->dmc_graph) cudaGraphDestroy((cudaGraph_t)c->dmc_graph);
+  c->dmc_exec = c->dmc_graph = nullptr;
+}
+
+// Captures two consecutive DMC steps (buffers A -> B -> A, so the host-side roles are unchanged
+// afterwards) into a CUDA graph on a private stream; re-captured when the seed changes (the seed
+// is a kernel parameter, the step number is read on the device).
+static int dmc_graph_prepare(champ_ctx *c, uint64_t seed) {
+  if (c->dmc_exec && c->dmc_graph_seed == seed) return CHAMP_OK;
+  dmc_graph_release(c);
+  if (!c->cap_stream) CK(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+  cudaStream_t saved = c->stream;
+  c->stream = c->cap_stream;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = dmc_one_step(c);
+  if (!rc) rc = dmc_one_step(c);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  c->stream = saved;
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return fail(CHAMP_ECUDA, std::string("DMC step capture: ") + cudaGetErrorString(e));
+  cudaGraphExec_t x = nullptr;
+  e = cudaGraphInstantiate(&x, g, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return fail(CHAMP_ECUDA, std::string("DMC graph instantiation: ") + cudaGetErrorString(e));
+  }
+  c->dmc_graph = g;
+  c->dmc_exec = x;
+  c->dmc_graph_seed = seed;
+  return CHAMP_OK;
+}
+
 static int cublas_handle(champ_ctx *c) {
   if (!c->cublas) {
     cublasHandle_t h;
@@ -884,6 +944,8 @@ int champ_destroy(champ_ctx *c) {
   if (!c) return CHAMP_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
   else cudaDeviceSynchronize();
+  dmc_graph_release(c);
+  if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   for (void *p : c->allocs) cudaFree(p);
   if (c->cublas) cublasDestroy((cublasHandle_t)c->cublas);
   delete c;
@@ -975,7 +1037,10 @@ int champ_dmc_init(champ_ctx *c, int32_t w_target, double tau, double gpop) {
     int *nc = dalloc<int>(c, W), *off = dalloc<int>(c, W);
     double *stat = dalloc<double>(c, 4 * (size_t)DMC_STAT_CAP);
     double *w0 = dalloc<double>(c, W), *w1 = dalloc<double>(c, W), *e0 = dalloc<double>(c, W), *e1 = dalloc<double>(c, W);
-    if (!nw || !sc || !nc || !off || !stat || !w0 || !w1 || !e0 || !e1) return fail(CHAMP_ENOMEM, "DMC allocation failed");
+    long long *ctr = dalloc<long long>(c, 2);
+    if (!nw || !sc || !nc || !off || !stat || !w0 || !w1 || !e0 || !e1 || !ctr)
+      return fail(CHAMP_ENOMEM, "DMC allocation failed");
+    c->dA.ctr = c->dB.ctr = ctr;
     c->dA.nw = c->dB.nw = nw;
     c->dA.et = c->dB.et = sc;
     c->dA.eest = c->dB.eest = sc + 1;
@@ -1017,6 +1082,7 @@ int champ_dmc_init(champ_ctx *c, int32_t w_target, double tau, double gpop) {
   CK(cudaMemcpyAsync(c->dA.nw, &nw, sizeof(int), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->dmc_step = 0;
+  dmc_graph_release(c);
   return CHAMP_OK;
 }
 
@@ -1025,26 +1091,21 @@ int champ_dmc_steps(champ_ctx *c, int32_t nstep, uint64_t seed, double *stats) {
   if (!c->dmc_ready) return fail(CHAMP_ESTATE, "call champ_dmc_init first");
   if (nstep < 0 || nstep > DMC_STAT_CAP) return fail(CHAMP_EINVAL, "nstep out of range");
   c->dpar.seed = seed;
-  for (int i = 0; i < nstep; i++) {
-    OpArgs a;
-    a.istep = c->dmc_step;
-    int rc = launch(c, Op::DmcMove, a);
+  // step counter (random-number key) and statistics index live on the device
+  const long long ctr[2] = {(long long)c->dmc_step, 0};
+  CK(cudaMemcpyAsync(c->dA.ctr, ctr, sizeof(ctr), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  int done = 0;
+  if (c->dmc_graph_on && nstep >= 2) {
+    int rc = dmc_graph_prepare(c, seed);
     if (rc) return rc;
-    k_dmc_sums<<<148, 256, 0, c->stream>>>(c->dA, c->dpar.wmax);
-    k_dmc_count<<<(c->dpar.wmax + 255) / 256, 256, 0, c->stream>>>(c->dA, c->dpar, c->dmc_step);
-    if (cub::DeviceScan::ExclusiveSum(c->scan_tmp, c->scan_bytes, c->dA.ncopy, c->dA.off, c->dpar.wmax, c->stream) !=
-        cudaSuccess)
-      return fail(CHAMP_ECUDA, "DMC scan failed");
-    rc = launch(c, Op::DmcCopy, a);
-    if (rc) return rc;
-    k_dmc_finish<<<1, 32, 0, c->stream>>>(c->dA, c->dB, c->dpar, i);
-    CK(cudaGetLastError());
-    std::swap(c->std_, c->std2);
-    std::swap(c->stf, c->stf2);
-    std::swap(c->dA.wt, c->dB.wt);
-    std::swap(c->dA.el, c->dB.el);
-    c->dmc_step++;
+    for (; done + 2 <= nstep; done += 2) CK(cudaGraphLaunch((cudaGraphExec_t)c->dmc_exec, c->stream));
   }
+  for (; done < nstep; done++) {
+    int rc = dmc_one_step(c);
+    if (rc) return rc;
+  }
+  c->dmc_step += nstep;
   int nw = 0;
   CK(cudaMemcpyAsync(&nw, c->dA.nw, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   if (stats && nstep)
@@ -1210,6 +1271,10 @@ int champ_set_option(champ_ctx *c, const char *name, int64_t value) {
     c->tc_on = value ? 1 : 0;
     return CHAMP_OK;
   }
+  if (!strcmp(name, "dmc_graph")) {
+    c->dmc_graph_on = value ? 1 : 0;
+    return CHAMP_OK;
+  }
   if (!strcmp(name, "reinvert_every")) {
     if (value < 1 || value > (1 << 30)) return fail(CHAMP_EINVAL, "reinvert_every must be >= 1");
     c->reinv_every = (int)value;
@@ -1223,6 +1288,7 @@ int champ_get_option(const champ_ctx *c, const char *name, int64_t *value) {
   if (!strcmp(name, "orbital_tc")) { *value = c->tc_on; return CHAMP_OK; }
   if (!strcmp(name, "launches_per_sweep")) { *value = c->tc_on ? 5 : 1; return CHAMP_OK; }
   if (!strcmp(name, "reinvert_every")) { *value = c->reinv_every; return CHAMP_OK; }
+  if (!strcmp(name, "dmc_graph")) { *value = c->dmc_graph_on; return CHAMP_OK; }
   return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);
 }
 

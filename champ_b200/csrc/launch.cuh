@@ -111,7 +111,7 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
     break;
   case Op::DmcMove:
     k_dmc_move<T, NORD, MD><<<dim3((c->dpar.wmax + c->wpb - 1) / c->wpb), block, c->smem, c->stream>>>(
-        s, st, c->lay, c->dpar, c->dA, a.istep);
+        s, st, c->lay, c->dpar, c->dA);
     break;
   case Op::DmcCopy: {
     k_dmc_copy<T><<<592, 128, 0, c->stream>>>(st, st2of<T>(c), c->dA, c->dB, c->N, c->C, c->dpar.wmax);

@@ -214,7 +214,9 @@ int champ_oh_buffers(const champ_ctx *ctx, const double **S, const double **H);
    champ_dmc_steps runs nstep steps (drift-diffusion moves with the Green's-function acceptance
    of green_functions_mod.f90, E_L, reweighting, branching) without host synchronisation and
    returns per step {population, sum w, sum w E_L, E_T} in stats (host [nstep][4] or NULL).
-   Afterwards the context's walker count is the new population. */
+   Afterwards the context's walker count is the new population.  Pairs of steps run as one
+   CUDA graph (captured on first use and whenever the seed changes; option "dmc_graph" 0 launches
+   step by step); the step number that keys the random numbers is kept on the device. */
 int champ_dmc_init(champ_ctx *ctx, int32_t w_target, double tau, double gpop);
 int champ_dmc_steps(champ_ctx *ctx, int32_t nstep, uint64_t seed, double *stats);
 
@@ -245,9 +247,11 @@ int champ_synchronize(champ_ctx *ctx);
    "reinvert_every": the full evaluation after a VMC sweep re-inverts the Slater matrices in
    FP64 every this many sweeps (sweep index divisible by it) and otherwise uses the inverses
    kept current by the Sherman-Morrison updates of the accepted moves; default
-   ceil(100 / nelec), i.e. a re-inversion about every 100 single-electron moves. */
+   ceil(100 / nelec), i.e. a re-inversion about every 100 single-electron moves.
+   "dmc_graph": 1 (default) replays pairs of DMC steps as a captured CUDA graph, 0 launches the
+   kernels of every step from the host. */
 int champ_set_option(champ_ctx *ctx, const char *name, int64_t value);
-/* Current value of an option ("orbital_tc", "reinvert_every"); kernel launches per champ_vmc_sweeps sweep
+/* Current value of an option ("orbital_tc", "reinvert_every", "dmc_graph"); kernel launches per champ_vmc_sweeps sweep
    ("launches_per_sweep": 1 for the fused sweep kernel, 5 with the tensor-core orbitals). */
 int champ_get_option(const champ_ctx *ctx, const char *name, int64_t *value);
 

@@ -48,3 +48,26 @@ def test_dmc_c2_population_and_energies_finite():
     assert np.all(np.isfinite(st))
     assert st[:, 0].min() > 0.3 * 8192 and st[:, 0].max() <= 24576
     assert eng.population() == eng.get_walkers().shape[0]
+
+
+def test_dmc_graph_replay_matches_step_by_step_launches():
+    """The DMC steps replayed as a captured CUDA graph (two steps per replay) follow the same
+    trajectory as step-by-step launches: same population per step and the same weights and
+    energies (FP64, to summation-order rounding), including an odd step count and a seed change."""
+    from champ_b200.engine import Engine
+    s = S.c2_dmc()
+    out = {}
+    for graph in (0, 1):
+        eng = Engine(s, 4096, "fp64")
+        eng.set_option("dmc_graph", graph)
+        assert eng.get_option("dmc_graph") == graph
+        eng.set_walkers(S.initial_walkers(s, 2048, seed=9))
+        eng.vmc_sweeps(10, seed=9, sweep0=0, step=0.4, stats=False)
+        eng.dmc_init(2048, 0.01)
+        a = eng.dmc_steps(7, seed=31)
+        b = eng.dmc_steps(6, seed=32)
+        out[graph] = (np.vstack([a, b]), eng.get_walkers())
+    st0, st1 = out[0][0], out[1][0]
+    assert np.array_equal(st0[:, 0], st1[:, 0])
+    assert np.allclose(st0[:, 1:], st1[:, 1:], rtol=1e-10, atol=1e-10)
+    assert np.allclose(out[0][1], out[1][1], rtol=0, atol=1e-12)
