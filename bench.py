@@ -308,6 +308,33 @@ def measure(system, nw, prec, steps, warmup, pg_steps, rank, world, flush, torch
     return out
 
 
+def measure_dmc(system, target, nstep, torch):
+    """DMC throughput of the DMC workload: drift-diffusion moves (two gradient evaluations per
+    proposal), E_L, reweighting and branching for the whole population per step, steps replayed
+    as CUDA graphs; e-moves/s = sum over steps of population x electrons / device time."""
+    from champ_b200.engine import Engine
+    eng = Engine(system, int(1.6 * target), "mixed")
+    eng.set_walkers(system_walkers(system, target, seed=11))
+    eng.vmc_sweeps(20, SEED, sweep0=0, step=step_size(system), stats=False)
+    eng.dmc_init(target, 0.01)
+    eng.dmc_steps(20, seed=SEED)  # equilibration, graph capture
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    st = eng.dmc_steps(nstep, seed=SEED)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    moves = float(st[:, 0].sum()) * system.nelec
+    eng.close()
+    return {"workload": f"{system.name}: DMC, target population {target}, tau 0.01", "value": moves / (ms * 1e-3),
+            "unit": UNIT, "ms_per_step": ms / nstep, "steps": nstep,
+            "population": [float(st[:, 0].min()), float(st[:, 0].max())],
+            "step": "per walker: N drift-diffusion proposals (gradient before and after), Green's-function "
+                    "acceptance, updates; E_L with NLPP; reweighting; branching; one CUDA graph per two steps",
+            "note": "the timed call includes one device-to-host copy of the step statistics and population"}
+
+
 def mixed_error_of(system, nw, seed=5):
     """|E_L(mixed) - E_L(FP64)| on identical walkers of one system (eval_full of both engines)."""
     from champ_b200.engine import Engine
@@ -394,6 +421,10 @@ def main():
         big = {"workload": config_of(s5, s5.walkers, "mixed")["workload"], "walkers_per_gpu": s5.walkers, **b}
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             big["cpu_baseline"] = cpu_baseline_sample(s5, seconds=8.0)
+    dmc = None
+    if args.system != 4 and not args.no_cluster and world == 1:
+        s4 = S.get_system(4)
+        dmc = measure_dmc(s4, s4.walkers, max(10, args.steps // 20), torch)
     # the same error on a physical wave function (the reference's Be example: 4 determinants,
     # Slater basis, optimised Jastrow), where E_L varies little between samples
     phys = mixed_error_of(S.be_example(), 4096) if prec == "mixed" else None
@@ -408,7 +439,7 @@ def main():
                 "gpu_launches": args.steps * m["launches_per_step"],
                 "roofline": roof, "fp64_arm": m.get("fp64_arm"), "param_grad": m["param_grad"],
                 "mixed_error": m.get("mixed_error"), "mixed_error_physical": phys, "e2e": e2e, "cpu_baseline": cpu,
-                "wall_s_timed_region": m["wall_s_timed_region"], "cluster128": big}
+                "wall_s_timed_region": m["wall_s_timed_region"], "cluster128": big, "dmc": dmc}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
