@@ -52,6 +52,8 @@ struct Sys {
   const int4 *shell;    // [nshell]: centre, n, l, kind
   const int2 *shprim;   // [nshell]: first primitive, count
   const int *shb0;      // [nshell] first basis function
+  const int *cshell0;   // [C+1] first shell of each centre (shells grouped by centre)
+  int nshc;             // most shells on one centre; 0 when shells are not grouped by centre
   const T *pz, *pc;     // primitive exponent, normalised weight
   // occupied orbitals of each spin: det-0 (reference) orbitals in column order, then the
   // other orbitals any determinant of that spin uses ("virtuals"), ascending
@@ -320,6 +322,29 @@ __device__ __forceinline__ T shell_dot(const Sys<T> &s, int ish, const double *p
   if (r == T(0)) { r = T(1e-30); d0 = r; }
   T R[3];
   shell_radial<T, false>(s, ish, r, R);
+  T S[9], G[9][3];
+  solid_all<T, false>(l, d0, d1, d2, S, G);
+  int b0 = s.shb0[ish];
+  const int nm = 2 * l + 1;
+  T acc = 0;
+#pragma unroll
+  for (int sl = 0; sl < 9; sl++)
+    if (sl < nm) acc += S[sl] * g[b0 + sl];
+  return acc * ipow(T(1) / r, l) * R[0];
+}
+
+// shell_dot with the radial value taken from *R0 when R0 is not null (the point's distance from
+// the shell's centre known in advance).
+template <class T>
+__device__ __forceinline__ T shell_dot_r(const Sys<T> &s, int ish, const double *pt, const T *g, const T *R0) {
+  int4 sh = s.shell[ish];
+  int c = sh.x, l = sh.z;
+  T d0 = T(pt[0] - s.cent[3 * c]), d1 = T(pt[1] - s.cent[3 * c + 1]), d2 = T(pt[2] - s.cent[3 * c + 2]);
+  T r = tsqrt(d0 * d0 + d1 * d1 + d2 * d2);
+  if (r == T(0)) { r = T(1e-30); d0 = r; }
+  T R[3];
+  if (R0) R[0] = *R0;
+  else shell_radial<T, false>(s, ish, r, R);
   T S[9], G[9][3];
   solid_all<T, false>(l, d0, d1, d2, S, G);
   int b0 = s.shb0[ish];

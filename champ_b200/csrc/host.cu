@@ -369,6 +369,27 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
   CK(cudaMemcpy(sh, shv.data(), sizeof(int4) * c->nshell, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(shp, shpv.data(), sizeof(int2) * c->nshell, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(shb0, shb0v.data(), sizeof(int) * c->nshell, cudaMemcpyHostToDevice));
+  {
+    // shells grouped by centre: first shell of each centre and the largest group
+    std::vector<int> cs0(c->C + 1, 0);
+    bool grouped = true;
+    for (int i = 1; i < c->nshell; i++)
+      if (d->shell_cent[i] < d->shell_cent[i - 1]) grouped = false;
+    int nshc = 0;
+    if (grouped) {
+      for (int cc = 0, i = 0; cc <= c->C; cc++) {
+        while (i < c->nshell && d->shell_cent[i] < cc) i++;
+        cs0[cc] = i;
+      }
+      cs0[c->C] = c->nshell;
+      for (int cc = 0; cc < c->C; cc++) nshc = std::max(nshc, cs0[cc + 1] - cs0[cc]);
+    }
+    int *cs = dalloc<int>(c, c->C + 1);
+    if (!cs) return fail(CHAMP_ENOMEM, "device allocation failed");
+    CK(cudaMemcpy(cs, cs0.data(), sizeof(int) * (c->C + 1), cudaMemcpyHostToDevice));
+    s.cshell0 = cs;
+    s.nshc = grouped ? nshc : 0;
+  }
   CK(cudaMemcpy(pz, pzv.data(), sizeof(T) * nprim, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(pc, pcv.data(), sizeof(T) * nprim, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(cr0, crv[0].data(), sizeof(T) * crv[0].size(), cudaMemcpyHostToDevice));

@@ -711,14 +711,18 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
     }
     double *tl = v.nlt;
     int ntask = 0;
+    // tasks in centre-major order, so that the points of one round of 32 lanes mostly share
+    // their centre (and with it the shells whose radial parts are precomputed per task)
     for (int base = 0; base < N * C; base += 32) {
-      int idx = base + lane;
+      const int j = base + lane;
+      int idx = j;
       bool nl = false;
       double vps[MAXLCH], r = 0;
       int c = 0;
-      if (idx < N * C) {
-        int e = idx / C;
-        c = idx - e * C;
+      if (j < N * C) {
+        c = j / N;
+        const int e = j - c * N;
+        idx = e * C + c;
         const double *cc = s.cent + 3 * c, *xe = xs + 3 * e;
         r = sqrt((xe[0] - cc[0]) * (xe[0] - cc[0]) + (xe[1] - cc[1]) * (xe[1] - cc[1]) +
                  (xe[2] - cc[2]) * (xe[2] - cc[2]));
@@ -741,6 +745,24 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
     vloc = warp_sum(vloc);
     __syncwarp();
     const int nq = E.nquad;
+    // The points of an (electron, centre) task lie at the task's distance r from that centre, so
+    // the radial parts of the centre's own shells are evaluated once per task (into the per-warp
+    // basis scratch, unused in this phase) when the table fits there.
+    const int nshc = (s.nshc > 0 && ntask * s.nshc <= B * 5) ? s.nshc : 0;
+    T *rown = v.phi;  // [ntask][nshc]
+    if (nshc > 0) {
+      for (int i = lane; i < ntask * nshc; i += 32) {
+        const int tk = i / nshc, k = i - tk * nshc;
+        const double *rc = tl + (size_t)tk * NLT;
+        const int ci = (int)rc[0] % C, ish = s.cshell0[ci] + k;
+        if (ish < s.cshell0[ci + 1]) {
+          T R3[3];
+          shell_radial<T, false>(s, ish, (T)rc[1], R3);
+          rown[i] = R3[0];
+        }
+      }
+      __syncwarp();
+    }
     for (int t = lane; t < ntask * nq; t += 32) {
       int task = t / nq, q = t - task * nq;
       const double *rec = tl + (size_t)task * NLT;
@@ -755,7 +777,12 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
       // determinant ratio: orbitals at the point contracted with G
       const T *ge = gp + (size_t)e * B;
       T dr = 0;
-      for (int ish = 0; ish < s.nshell; ish++) dr += shell_dot<T>(s, ish, xn, ge);
+      {
+        const int c0 = nshc > 0 ? s.cshell0[c] : 0, c1 = nshc > 0 ? s.cshell0[c + 1] : 0;
+        const T *ro = rown + task * nshc - c0;
+        for (int ish = 0; ish < s.nshell; ish++)
+          dr += shell_dot_r<T>(s, ish, xn, ge, (ish >= c0 && ish < c1) ? ro + ish : nullptr);
+      }
       // Jastrow ratio (nonlocj, nonloc.f90:432-522): point-centre distances once per point
       double dj = 0;
       const bool fast = (NORD > 1) && J.nct == 1 && C <= MAXC_NL;
