@@ -90,6 +90,12 @@ struct champ_ctx {
   float *tc_b[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [spin][hi, lo]: [Np][Kp]
   int *tc_err = nullptr;          // set by a contraction that gave up waiting
   std::vector<float> tc_coef[2];  // host copy of the occupied coefficients [nbasis][nocc]
+  std::vector<int> tc_shl;        // host copy of the shells' l (internal basis order)
+  // fused basis + contraction (orbfused.cuh): padded K layout and split coefficients
+  int tc_fused_ok = 0, tc_mode = 0;  // fused kernel supported; mode in use: 1 fused, 2 basis rows + product
+  int tc_kq = 0, tc_nkb = 0, tc_fcols[2] = {32, 32};
+  int *tc_blk_sh = nullptr, *tc_kpos = nullptr;
+  float *tc_bf[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [spin][hi, lo]: [Np][Kq]
 };
 
 template <class T>

@@ -276,10 +276,11 @@ __device__ __forceinline__ void shell_radial(const Sys<T> &s, int ish, T r, T *R
   }
 }
 
-// All basis functions of one shell at point pt; NCH=1 values, NCH=5 value, grad, laplacian.
-// out[b*NCH + ch] for the shell's basis functions b.
-template <class T, int NCH>
-__device__ __forceinline__ void shell_eval(const Sys<T> &s, int ish, const double *pt, T *out) {
+// All basis functions of one shell at point pt, handed to put(slot, channel, value) as they are
+// formed: NCH=1 values, NCH=5 value, gradient, Laplacian; slots in harmonic order
+// m = 0, 1, -1, ... (the shell's basis functions are stored as b = b0 + slot).
+template <class T, int NCH, class Put>
+__device__ __forceinline__ void shell_eval_put(const Sys<T> &s, int ish, const double *pt, Put put) {
   int4 sh = s.shell[ish];
   int c = sh.x, l = sh.z;
   T d0 = T(pt[0] - s.cent[3 * c]), d1 = T(pt[1] - s.cent[3 * c + 1]), d2 = T(pt[2] - s.cent[3 * c + 2]);
@@ -292,24 +293,29 @@ __device__ __forceinline__ void shell_eval(const Sys<T> &s, int ish, const doubl
   T ril = ipow(ri, l);
   T S[9], G[9][3];
   solid_all<T, NCH == 5>(l, d0, d1, d2, S, G);
-  // the shell's basis functions are stored in harmonic-slot order: b = b0 + slot
-  int b0 = s.shb0[ish];
   const int nm = 2 * l + 1;
 #pragma unroll
   for (int sl = 0; sl < 9; sl++) {
     if (sl < nm) {
-      int b = b0 + sl;
       T Y = S[sl] * ril;
-      out[b * NCH] = Y * R[0];
+      put(sl, 0, Y * R[0]);
       if (NCH == 5) {
         T lr = T(l) * S[sl] * ril * ri * ri;
-        out[b * NCH + 1] = Y * d0 * ri * R[1] + (G[sl][0] * ril - lr * d0) * R[0];
-        out[b * NCH + 2] = Y * d1 * ri * R[1] + (G[sl][1] * ril - lr * d1) * R[0];
-        out[b * NCH + 3] = Y * d2 * ri * R[1] + (G[sl][2] * ril - lr * d2) * R[0];
-        out[b * NCH + 4] = Y * (R[2] + 2 * ri * R[1] - T(l * (l + 1)) * ri * ri * R[0]);
+        put(sl, 1, Y * d0 * ri * R[1] + (G[sl][0] * ril - lr * d0) * R[0]);
+        put(sl, 2, Y * d1 * ri * R[1] + (G[sl][1] * ril - lr * d1) * R[0]);
+        put(sl, 3, Y * d2 * ri * R[1] + (G[sl][2] * ril - lr * d2) * R[0]);
+        put(sl, 4, Y * (R[2] + 2 * ri * R[1] - T(l * (l + 1)) * ri * ri * R[0]));
       }
     }
   }
+}
+
+// All basis functions of one shell at point pt; NCH=1 values, NCH=5 value, grad, laplacian.
+// out[b*NCH + ch] for the shell's basis functions b.
+template <class T, int NCH>
+__device__ __forceinline__ void shell_eval(const Sys<T> &s, int ish, const double *pt, T *out) {
+  T *o = out + s.shb0[ish] * NCH;
+  shell_eval_put<T, NCH>(s, ish, pt, [o](int sl, int ch, T v) { o[sl * NCH + ch] = v; });
 }
 
 // Values of all basis functions of one shell at pt contracted with g: sum_b phi_b(pt) g_b.

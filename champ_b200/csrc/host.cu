@@ -266,6 +266,7 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
   if constexpr (std::is_same<T, float>::value) {
     c->tc_coef[0] = crv[0];
     c->tc_coef[1] = crv[1];
+    c->tc_shl.assign(d->shell_l, d->shell_l + c->nshell);
   }
   // determinant tables
   s.multidet = md.multidet;
@@ -602,10 +603,23 @@ static int eval_noalloc_t(champ_ctx *c, const State<T> &ref, int32_t nw, const d
   return CHAMP_OK;
 }
 
-// Tensor-core orbital contraction (orbtc.cuh): padded sizes, split coefficients, basis-row
-// buffer.  Left off (CUDA-core contraction) where unsupported or the buffer does not fit.
+// Tensor-core orbital contraction: padded sizes and split coefficients.  Fused (orbfused.cuh):
+// basis functions formed in shared memory, K in a padded order in which no shell straddles a
+// 16-function block; usable when 5 channels x the padded orbital count fit the 512 TMEM columns.
+// Otherwise basis rows in HBM (k_basis_rows) and the streamed product (k_orb_tc), when the rows
+// fit in memory.  Left off (CUDA-core contraction) where neither applies.
+static int tc_alloc_rows(champ_ctx *c) {
+  if (c->tc_phi) return CHAMP_OK;
+  c->tc_phi = dalloc<float>(c, (size_t)c->wmax * c->N * 5 * c->tc_Kp);
+  if (!c->tc_phi) {
+    cudaGetLastError();
+    return fail(CHAMP_ENOMEM, "no room for the basis rows of the unfused tensor-core contraction");
+  }
+  return CHAMP_OK;
+}
+
 static int tc_setup(champ_ctx *c) {
-  c->tc_on = c->tc_ok = 0;
+  c->tc_on = c->tc_ok = c->tc_fused_ok = c->tc_mode = 0;
   int dev = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev));
@@ -613,6 +627,25 @@ static int tc_setup(champ_ctx *c) {
   if (std::max(c->md.nocc[0], c->md.nocc[1]) < 16) return CHAMP_OK;
   const int B = c->nbasis, Kp = (B + orbtc::BK - 1) / orbtc::BK * orbtc::BK;
   c->tc_Kp = Kp;
+  // padded order for the fused kernel: kpos[shell], blocks of BKF functions holding whole shells
+  const int BKF = orbf::BKF;
+  std::vector<int> kpos(c->nshell), b0(c->nshell);
+  int pos = 0, bb = 0;
+  for (int i = 0; i < c->nshell; i++) {
+    const int nf = 2 * c->tc_shl[i] + 1;
+    if (pos % BKF + nf > BKF) pos = (pos + BKF - 1) / BKF * BKF;
+    kpos[i] = pos;
+    b0[i] = bb;
+    pos += nf;
+    bb += nf;
+  }
+  const int Kq = (pos + BKF - 1) / BKF * BKF, nkb = Kq / BKF;
+  std::vector<int> blk(nkb + 1, c->nshell);
+  for (int kb = 0, i = 0; kb <= nkb; kb++) {
+    while (i < c->nshell && kpos[i] < kb * BKF) i++;
+    blk[kb] = i;
+  }
+  bool fused = true;
   for (int sp = 0; sp < 2; sp++) {
     const int no = c->md.nocc[sp];
     if (no == 0 || (sp ? c->ndn : c->nup) == 0) continue;
@@ -621,26 +654,53 @@ static int tc_setup(champ_ctx *c) {
     while (nc < Np) nc <<= 1;
     c->tc_Np[sp] = Np;
     c->tc_ncols[sp] = nc;
+    int fc = 32;
+    while (fc < 5 * Np) fc <<= 1;
+    c->tc_fcols[sp] = fc;
+    if (5 * Np > 512) fused = false;
     std::vector<float> hi((size_t)Np * Kp, 0.f), lo((size_t)Np * Kp, 0.f);
-    for (int m = 0; m < no; m++)
+    std::vector<float> fhi((size_t)Np * Kq, 0.f), flo((size_t)Np * Kq, 0.f);
+    for (int m = 0; m < no; m++) {
       for (int b = 0; b < B; b++) {
         float v = c->tc_coef[sp][(size_t)b * no + m], h = orbtc::tf32_hi(v);
         hi[(size_t)m * Kp + b] = h;
         lo[(size_t)m * Kp + b] = v - h;
       }
+      for (int i = 0; i < c->nshell; i++)
+        for (int sl = 0; sl < 2 * c->tc_shl[i] + 1; sl++) {
+          float v = c->tc_coef[sp][(size_t)(b0[i] + sl) * no + m], h = orbtc::tf32_hi(v);
+          fhi[(size_t)m * Kq + kpos[i] + sl] = h;
+          flo[(size_t)m * Kq + kpos[i] + sl] = v - h;
+        }
+    }
     c->tc_b[sp][0] = dalloc<float>(c, hi.size());
     c->tc_b[sp][1] = dalloc<float>(c, lo.size());
-    if (!c->tc_b[sp][0] || !c->tc_b[sp][1]) return fail(CHAMP_ENOMEM, "device allocation failed");
+    c->tc_bf[sp][0] = dalloc<float>(c, fhi.size());
+    c->tc_bf[sp][1] = dalloc<float>(c, flo.size());
+    if (!c->tc_b[sp][0] || !c->tc_b[sp][1] || !c->tc_bf[sp][0] || !c->tc_bf[sp][1])
+      return fail(CHAMP_ENOMEM, "device allocation failed");
     CK(cudaMemcpy(c->tc_b[sp][0], hi.data(), sizeof(float) * hi.size(), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c->tc_b[sp][1], lo.data(), sizeof(float) * lo.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->tc_bf[sp][0], fhi.data(), sizeof(float) * fhi.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->tc_bf[sp][1], flo.data(), sizeof(float) * flo.size(), cudaMemcpyHostToDevice));
   }
+  c->tc_kq = Kq;
+  c->tc_nkb = nkb;
+  c->tc_blk_sh = dalloc<int>(c, nkb + 1);
+  c->tc_kpos = dalloc<int>(c, c->nshell);
   c->tc_err = dalloc<int>(c, 1);
-  c->tc_phi = dalloc<float>(c, (size_t)c->wmax * c->N * 5 * Kp);
-  if (!c->tc_err || !c->tc_phi) {
-    cudaGetLastError();
-    return CHAMP_OK;  // no room for the basis rows: the CUDA-core contraction stays in use
+  if (!c->tc_blk_sh || !c->tc_kpos || !c->tc_err) return fail(CHAMP_ENOMEM, "device allocation failed");
+  CK(cudaMemcpy(c->tc_blk_sh, blk.data(), sizeof(int) * (nkb + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->tc_kpos, kpos.data(), sizeof(int) * c->nshell, cudaMemcpyHostToDevice));
+  c->tc_fused_ok = fused ? 1 : 0;
+  if (fused) {
+    c->tc_ok = c->tc_on = 1;
+    c->tc_mode = 1;
+    return CHAMP_OK;
   }
+  if (tc_alloc_rows(c) != CHAMP_OK) return CHAMP_OK;  // the CUDA-core contraction stays in use
   c->tc_ok = c->tc_on = 1;
+  c->tc_mode = 2;
   return CHAMP_OK;
 }
 
@@ -1286,9 +1346,16 @@ int champ_walker_status(champ_ctx *c, uint32_t *flags) {
 int champ_set_option(champ_ctx *c, const char *name, int64_t value) {
   if (!c || !name) return fail(CHAMP_EINVAL, "null argument");
   if (!strcmp(name, "orbital_tc")) {
+    if (value < 0 || value > 2) return fail(CHAMP_EINVAL, "orbital_tc: 0, 1 or 2");
     if (value && !c->tc_ok)
       return fail(CHAMP_EINVAL, "orbital_tc: needs mixed precision, walker state in HBM, >= 16 orbitals of a spin "
                                 "and room for the basis rows");
+    if (value == 1) c->tc_mode = c->tc_fused_ok ? 1 : 2;
+    if (value == 2) {
+      int rc = tc_alloc_rows(c);
+      if (rc) return rc;
+      c->tc_mode = 2;
+    }
     c->tc_on = value ? 1 : 0;
     return CHAMP_OK;
   }
@@ -1306,8 +1373,12 @@ int champ_set_option(champ_ctx *c, const char *name, int64_t value) {
 
 int champ_get_option(const champ_ctx *c, const char *name, int64_t *value) {
   if (!c || !name || !value) return fail(CHAMP_EINVAL, "null argument");
-  if (!strcmp(name, "orbital_tc")) { *value = c->tc_on; return CHAMP_OK; }
-  if (!strcmp(name, "launches_per_sweep")) { *value = c->tc_on ? 5 : 1; return CHAMP_OK; }
+  if (!strcmp(name, "orbital_tc")) { *value = c->tc_on ? c->tc_mode : 0; return CHAMP_OK; }
+  if (!strcmp(name, "launches_per_sweep")) {
+    int spins = (c->nup > 0) + (c->ndn > 0);
+    *value = c->tc_on ? 2 + spins + (c->tc_mode == 2 ? 1 : 0) : 1;
+    return CHAMP_OK;
+  }
   if (!strcmp(name, "reinvert_every")) { *value = c->reinv_every; return CHAMP_OK; }
   if (!strcmp(name, "dmc_graph")) { *value = c->dmc_graph_on; return CHAMP_OK; }
   return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);

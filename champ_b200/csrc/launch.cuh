@@ -25,6 +25,8 @@ static int set_smem_attrs(champ_ctx *c) {
     CK(cudaFuncSetAttribute(orbtc::k_orb_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024 + 128));
     CK(cudaFuncSetAttribute(orbtc::k_orb_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)orbtc::smem_bytes(256, 2)));
+    CK(cudaFuncSetAttribute(orbf::k_orb_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)orbf::fsmem_bytes(96)));
     CK(cudaFuncSetAttribute(k_basis_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)std::min<size_t>(4 * (size_t)c->nbasis * 5 * sizeof(float), 227 * 1024)));
   }
@@ -43,8 +45,36 @@ static int run_orb_tc(champ_ctx *c, const State<T> &st) {
   if constexpr (!std::is_same<T, float>::value) {
     return fail(CHAMP_EINVAL, "tensor-core orbitals are a mixed-precision path");
   } else {
-    const long long items = (long long)st.W * c->N;
     const int sm = c->num_sms > 0 ? c->num_sms : 148;
+    if (c->tc_mode == 1) {
+      for (int sp = 0; sp < 2; sp++) {
+        const int n = sp ? c->ndn : c->nup;
+        if (n == 0) continue;
+        orbf::FArgs f;
+        f.x = st.x;
+        f.bhi = c->tc_bf[sp][0];
+        f.blo = c->tc_bf[sp][1];
+        f.blk_sh = c->tc_blk_sh;
+        f.kpos = c->tc_kpos;
+        f.orb = st.orb5;
+        f.M = st.W * n;
+        f.Kq = c->tc_kq;
+        f.nkb = c->tc_nkb;
+        f.Np = c->tc_Np[sp];
+        f.ncols = c->tc_fcols[sp];
+        f.n = n;
+        f.N = c->N;
+        f.e0 = sp ? c->nup : 0;
+        f.nomax = c->nomax;
+        f.nocc = c->md.nocc[sp];
+        f.err = c->tc_err;
+        const int tiles = (f.M + orbtc::BM - 1) / orbtc::BM;
+        orbf::k_orb_fused<<<(unsigned)std::min(tiles, sm), orbf::NTF, orbf::fsmem_bytes(f.Np), c->stream>>>(c->sf, f);
+        CK(cudaGetLastError());
+      }
+      return CHAMP_OK;
+    }
+    const long long items = (long long)st.W * c->N;
     long long gb = std::min<long long>((items + 3) / 4, (long long)sm * 8);
     k_basis_rows<<<(unsigned)std::max<long long>(gb, 1), 128, 4 * (size_t)c->nbasis * 5 * sizeof(float), c->stream>>>(
         c->sf, st.x, items, c->tc_Kp, c->tc_phi);

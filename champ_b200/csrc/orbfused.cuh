@@ -1,0 +1,171 @@
+// orbfused.cuh -- basis functions and the basis-to-orbital contraction of the full evaluation in
+// one tensor-core kernel: the basis rows are formed in shared memory and never reach HBM.
+//
+// Per spin, rows = electrons of that spin of all walkers, K = basis functions in a padded order
+// in which no shell straddles a K-block of 16, N = orbitals of the spin.  Five products share the
+// coefficients: one per channel (value, d/dx, d/dy, d/dz, Laplacian), accumulated in five TMEM
+// column ranges.  Warps 0-3 evaluate the basis functions of one K-block for 128 electrons (one
+// thread per electron, all lanes walk the same shells), split each value into TF32 hi + FP32
+// remainder and store both into the channel's A tile; warps 4-7 bring the split coefficients of
+// the block with cp.async; one thread issues 5 x 2 x 3 tcgen05.mma (kind::tf32, hi.hi + hi.lo +
+// lo.hi) per block and commits to the stage's mbarrier, so the evaluation of the next block
+// overlaps the tensor cores.  All waits are bounded.
+#pragma once
+
+namespace orbf {
+
+using namespace orbtc;
+
+constexpr int BKF = 16;   // basis functions per K-block (two MMA k-steps of 8)
+constexpr int NTF = 256;  // threads: 0-127 one electron row each, 128-255 coefficient loads
+
+struct FArgs {
+  const double *x;          // walker positions [W][N][3]
+  const float *bhi, *blo;   // [Np][Kq] split coefficients in the padded order (zero at pads)
+  const int *blk_sh;        // [nkb+1] first shell of each K-block
+  const int *kpos;          // [nshell] padded position of each shell's first function
+  float *orb;               // orbital rows [(w*N + e)*5 + ch][nomax]
+  int M;                    // rows: W * n
+  int Kq, nkb, Np, ncols;   // padded K, K-blocks, padded N (multiple of 16, 5*Np <= 512), TMEM columns
+  int n, N, e0, nomax, nocc;
+  int *err;
+};
+
+// One stage: 5 channels x (hi, lo) A tiles [128][16] and (hi, lo) B tiles [Np][16].
+__host__ __device__ inline size_t fstage_bytes(int Np) {
+  return 10 * (size_t)BM * BKF * 4 + 2 * (size_t)Np * BKF * 4;
+}
+__host__ __device__ inline size_t fsmem_bytes(int Np) { return 2 * fstage_bytes(Np) + 128; }
+
+// byte offset of element (row r, k) of a [rows][BKF] tile in the no-swizzle K-major core-matrix
+// layout: core matrices of 8 rows x 4 elements (128 B), BKF/4 of them along K per 8-row group
+__device__ __forceinline__ uint32_t foff(int r, int k) {
+  return (uint32_t)((((r >> 3) * (BKF / 4) + (k >> 2)) << 7) + ((r & 7) << 4) + ((k & 3) << 2));
+}
+
+static __global__ void __launch_bounds__(NTF, 1) k_orb_fused(Sys<float> s, FArgs a) {
+  extern __shared__ __align__(128) unsigned char sm[];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t tslot;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  unsigned char *base = (unsigned char *)(((uintptr_t)sm + 127) & ~(uintptr_t)127);
+  const uint32_t sA = BM * BKF * 4, sB = (uint32_t)a.Np * BKF * 4, stage = 10 * sA + 2 * sB;
+  // both stages start at zero: a block's pad positions are never written and must stay finite
+  for (uint32_t i = 16 * tid; i < 2 * stage; i += 16 * NTF) *(float4 *)(base + i) = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (tid == 0) {
+    mbar_init(smem_u32(&mbar[0]), 1);
+    mbar_init(smem_u32(&mbar[1]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tslot)), "r"(a.ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tbase = tslot;
+  const uint32_t idesc = idesc_tf32(BM, a.Np);
+  const int ntile = (a.M + BM - 1) / BM;
+  uint32_t it = 0;  // K-blocks issued so far (commit count)
+  bool ok = true;
+  for (int tile = blockIdx.x; tile < ntile && ok; tile += gridDim.x) {
+    double pt[3] = {0, 0, 0};
+    bool live = false;
+    if (tid < BM) {
+      const int r = tile * BM + tid;
+      if (r < a.M) {
+        const int w = r / a.n, eo = r - w * a.n;
+        const double *p = a.x + ((size_t)w * a.N + a.e0 + eo) * 3;
+        pt[0] = p[0]; pt[1] = p[1]; pt[2] = p[2];
+        live = true;
+      }
+    }
+    for (int kb = 0; kb < a.nkb; kb++, it++) {
+      const int sg = it & 1;
+      unsigned char *st = base + (size_t)sg * stage;
+      // the stage is free once the MMAs committed two blocks ago have completed
+      const bool got = it < 2 || mbar_wait(smem_u32(&mbar[sg]), ((it - 2) >> 1) & 1);
+      if (tid < BM) {
+        if (live) {
+          const int k0 = kb * BKF;
+          for (int ish = a.blk_sh[kb]; ish < a.blk_sh[kb + 1]; ish++) {
+            const int kk = a.kpos[ish] - k0;
+            shell_eval_put<float, 5>(s, ish, pt, [&](int sl, int ch, float v) {
+              const float h = tf32_hi(v);
+              const uint32_t o = foff(tid, kk + sl);
+              *(float *)(st + (2 * ch) * sA + o) = h;
+              *(float *)(st + (2 * ch + 1) * sA + o) = v - h;
+            });
+          }
+        }  // rows past the end keep finite stale values; their outputs are not stored
+      } else {
+        // coefficients of the block: 16-byte piece q lands at byte 16q (core-matrix order)
+        const uint32_t ub = smem_u32(st + 10 * sA);
+        for (int q = tid - BM; q < a.Np * (BKF / 4); q += NTF - BM) {
+          const int cm = q >> 3, row = (cm / (BKF / 4)) * 8 + (q & 7), ck = cm % (BKF / 4);
+          const size_t o = (size_t)row * a.Kq + (size_t)kb * BKF + 4 * ck;
+          cp_async16(ub + 16 * q, a.bhi + o, 16);
+          cp_async16(ub + sB + 16 * q, a.blo + o, 16);
+        }
+        cp_commit();
+        cp_wait_all();
+      }
+      fence_async_smem();
+      if (!__syncthreads_and(got)) { ok = false; break; }
+      if (tid == BM) {
+        fence_after();
+        const uint32_t ua = smem_u32(st), ub = ua + 10 * sA;
+#pragma unroll
+        for (int ch = 0; ch < 5; ch++)
+#pragma unroll
+          for (int ks = 0; ks < BKF / 8; ks++) {
+            const uint32_t ko = ks * 256;
+            const uint64_t dah = sdesc(ua + 2 * ch * sA + ko, 128, (BKF / 4) * 128);
+            const uint64_t dal = sdesc(ua + (2 * ch + 1) * sA + ko, 128, (BKF / 4) * 128);
+            const uint64_t dbh = sdesc(ub + ko, 128, (BKF / 4) * 128), dbl = sdesc(ub + sB + ko, 128, (BKF / 4) * 128);
+            const uint32_t d = tbase + (uint32_t)(ch * a.Np);
+            mma_tf32(d, dal, dbh, idesc, (kb > 0 || ks > 0) ? 1u : 0u);
+            mma_tf32(d, dah, dbl, idesc, 1u);
+            mma_tf32(d, dah, dbh, idesc, 1u);
+          }
+        mma_commit(smem_u32(&mbar[sg]));
+      }
+    }
+    if (!ok) break;
+    // epilogue: warp q reads TMEM lanes 32(q mod 4)..+31; warps q and q+4 take alternate groups
+    // of 16 columns of the 5 channel ranges (Np is a multiple of 16: a group is in one channel)
+    if (!__syncthreads_and(mbar_wait(smem_u32(&mbar[(it - 1) & 1]), ((it - 1) >> 1) & 1))) { ok = false; break; }
+    fence_after();
+    const int quad = warp & 3, half = warp >> 2;
+    const int r = tile * BM + quad * 32 + lane;
+    float *dst = nullptr;
+    if (r < a.M) {
+      const int w = r / a.n, eo = r - w * a.n;
+      dst = a.orb + ((size_t)w * a.N + a.e0 + eo) * 5 * a.nomax;
+    }
+    for (int c0 = 16 * half; c0 < 5 * a.Np; c0 += 32) {
+      float v[16];
+      tmem_ld16(tbase + ((uint32_t)(quad * 32) << 16) + (uint32_t)c0, v);
+      const int ch = c0 / a.Np, m0 = c0 - ch * a.Np;
+      if (dst)
+#pragma unroll
+        for (int k = 0; k < 16; k++)
+          if (m0 + k < a.nocc) dst[ch * a.nomax + m0 + k] = v[k];
+    }
+    fence_before();
+    __syncthreads();
+  }
+  cp_wait_all();
+  if (!ok) {
+    if (a.err) atomicExch(a.err, 1);
+    // let the committed MMA groups finish (bounded) before the accumulator is freed
+    if (tid == 0)
+      for (uint32_t u = it > 2 ? it - 2 : 0; u < it; u++) mbar_wait(smem_u32(&mbar[u & 1]), (u >> 1) & 1);
+  }
+  __syncthreads();
+  fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(a.ncols));
+}
+
+}  // namespace orbf

@@ -16,7 +16,7 @@ namespace orbtc {
 
 constexpr int BM = 128;        // rows per tile (TMEM lanes)
 constexpr int BK = 32;         // K (fp32 elements) per stage: 128 bytes per row
-constexpr int NTHR = 128;      // 4 warps: all load, thread 0 issues, all drain TMEM
+constexpr int NTHR = 256;      // 8 warps: all load and split, thread 0 issues, all drain TMEM
 constexpr uint32_t WAIT_LIMIT = 1u << 24;  // bounded mbarrier polls before giving up
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -218,19 +218,21 @@ __global__ void __launch_bounds__(NTHR, 1) k_orb_tc(Args a) {
     if (!__syncthreads_and(got)) { ok = false; break; }
     issue(i + NS - 1);
     if (kb == nkb - 1) {
-      // epilogue: drain the accumulator (warp q owns TMEM lanes 32q..32q+31)
+      // epilogue: drain the accumulator; warp q reads TMEM lanes 32(q mod 4)..+31 (the lanes a
+      // warp may access), warps q and q+4 take alternate groups of 16 columns
       if (!__syncthreads_and(mbar_wait(smem_u32(&mbar[s]), (i / NS) & 1))) { ok = false; break; }
       fence_after();
       const int tile = (int)blockIdx.x + (i / nkb) * (int)gridDim.x;
-      const int gr = tile * BM + warp * 32 + lane;
+      const int quad = warp & 3, half = warp >> 2;
+      const int gr = tile * BM + quad * 32 + lane;
       float *dst = nullptr;
       if (gr < a.M) {
         const int w = gr / nw_rows, rem = gr - w * nw_rows;
         dst = a.orb + ((long long)(w * a.N + a.e0) * 5 + rem) * a.nomax;
       }
-      for (int c0 = 0; c0 < a.Np; c0 += 16) {
+      for (int c0 = 16 * half; c0 < a.Np; c0 += 32) {
         float v[16];
-        tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+        tmem_ld16(tbase + ((uint32_t)(quad * 32) << 16) + (uint32_t)c0, v);
         if (dst)
 #pragma unroll
           for (int k = 0; k < 16; k++)
@@ -270,3 +272,5 @@ static __global__ void __launch_bounds__(128) k_basis_rows(Sys<float> s, const d
     __syncwarp();
   }
 }
+
+#include "orbfused.cuh"

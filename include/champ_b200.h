@@ -241,7 +241,9 @@ int champ_synchronize(champ_ctx *ctx);
 /* Engine options (no counterpart in the reference, which has one code path).
    "orbital_tc": 1 computes the orbitals of the full evaluation (value, gradient, Laplacian of
    every electron of every walker) as one tcgen05 tensor-core contraction per spin with a
-   3-term TF32 split (about FP32 accuracy); 0 uses the CUDA-core contraction.  Available for
+   3-term TF32 split (about FP32 accuracy), with the basis functions formed in shared memory
+   (fused; up to 96 orbitals of a spin, else as 2); 2 the same contraction from basis rows
+   written to HBM first; 0 uses the CUDA-core contraction.  Available for
    mixed precision when the walker state lives in HBM and a spin has >= 16 orbitals, and on by
    default there; CHAMP_EINVAL otherwise.
    "reinvert_every": the full evaluation after a VMC sweep re-inverts the Slater matrices in

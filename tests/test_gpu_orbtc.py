@@ -1,10 +1,12 @@
 """Tensor-core orbital contraction (tcgen05, 3-term TF32 split) against the CUDA-core paths.
 
 The full evaluation of a mixed-precision engine whose walker state lives in HBM computes the
-orbitals of all electrons of all walkers as one tensor-core product per spin.  These tests
-switch it on and off through champ_set_option("orbital_tc") and compare with the CUDA-core
-contraction of the same engine and with the FP64 engine: the tensor-core E_L error relative to
-max(1, |E_L|, |lap ln psi|) must stay within 3x that of the CUDA-core FP32 contraction (or 1e-6).
+orbitals of all electrons of all walkers as one tensor-core product per spin, either fused with
+the basis evaluation in shared memory (orbital_tc 1) or from basis rows in HBM (orbital_tc 2).
+These tests switch the modes through champ_set_option("orbital_tc") and compare with the
+CUDA-core contraction of the same engine (0) and with the FP64 engine: the tensor-core E_L error
+relative to max(1, |E_L|, |lap ln psi|) must stay within 3x that of the CUDA-core FP32
+contraction (or 1e-6).
 """
 import numpy as np
 import pytest
@@ -36,20 +38,23 @@ def test_eval_full_tensor_core_orbitals(ncent):
     x, e64, em = _engines(s, nw, 21)
     ref = e64.eval_full()
     out = {}
-    for tc in (0, 1):
+    for tc in (0, 1, 2):
         em.set_option("orbital_tc", tc)
+        assert em.get_option("orbital_tc") == tc
         em.set_walkers(x)
         out[tc] = em.eval_full()
     sc = _scale(ref)
     err = {}
-    for tc in (0, 1):
+    for tc in (0, 1, 2):
         err[tc] = float(np.max(np.abs(out[tc]["energy"] - ref["energy"]) / sc))
         assert err[tc] <= 2e-3  # the mixed-precision parity tolerance of the other tests
         lerr = np.abs(out[tc]["lnpsi"] - ref["lnpsi"]) / np.maximum(1.0, np.abs(ref["lnpsi"]))
         assert np.all(lerr <= 1e-5), (tc, float(lerr.max()))
-    print(f"cluster ncent={ncent}: max |dE_L|/scale vs FP64: CUDA-core {err[0]:.2e}, tensor-core {err[1]:.2e}")
-    # the tensor-core contraction is as accurate as the CUDA-core FP32 one
+    print(f"cluster ncent={ncent}: max |dE_L|/scale vs FP64: CUDA-core {err[0]:.2e}, "
+          f"tensor-core fused {err[1]:.2e}, from basis rows {err[2]:.2e}")
+    # the tensor-core contractions are as accurate as the CUDA-core FP32 one
     assert err[1] <= max(3 * err[0], TOL), err
+    assert err[2] <= max(3 * err[0], TOL), err
 
 
 def test_vmc_split_sweep_matches_fused_sweep():
@@ -60,7 +65,7 @@ def test_vmc_split_sweep_matches_fused_sweep():
     nw = 256
     x = S.initial_walkers(s, nw, seed=5)
     res = {}
-    for tc in (0, 1):
+    for tc in (0, 1, 2):
         e = Engine(s, nw, "mixed")
         e.set_option("orbital_tc", tc)
         e.set_walkers(x)
@@ -68,12 +73,13 @@ def test_vmc_split_sweep_matches_fused_sweep():
         res[tc] = (e.get_walkers(), st, _scale(e.eval_full()))
     # the starting inverses differ at FP32 rounding level, so a Metropolis decision within that
     # distance of its threshold may differ: compare the walkers whose trajectories coincide
-    same = np.all(res[0][0] == res[1][0], axis=(1, 2))
-    assert same.mean() >= 0.98
-    assert np.array_equal(res[0][1]["accept"][same], res[1][1]["accept"][same])
-    el0, el1 = res[0][1]["elast"][same], res[1][1]["elast"][same]
-    sc = res[0][2][same]
-    assert np.all(np.abs(el0 - el1) <= 1e-5 * sc), float(np.max(np.abs(el0 - el1) / sc))
+    for tc in (1, 2):
+        same = np.all(res[0][0] == res[tc][0], axis=(1, 2))
+        assert same.mean() >= 0.98
+        assert np.array_equal(res[0][1]["accept"][same], res[tc][1]["accept"][same])
+        el0, el1 = res[0][1]["elast"][same], res[tc][1]["elast"][same]
+        sc = res[0][2][same]
+        assert np.all(np.abs(el0 - el1) <= 1e-5 * sc), (tc, float(np.max(np.abs(el0 - el1) / sc)))
 
 
 def test_orbital_tc_option_rejected_where_unsupported():
