@@ -63,6 +63,7 @@ struct champ_ctx {
   int nfree = 0;           // free parameters reported
   size_t smem_pg = 0;      // dynamic shared memory of the derivative kernel
   int wpb_pg = 4;
+  int pg_lanesum = 0;      // per-lane slots for the NLPP parameter sums in the derivative kernel
   double *pg_dl = nullptr, *pg_de = nullptr, *pg_el = nullptr, *pg_wt = nullptr;
   double *oh_oa = nullptr, *oh_ow = nullptr, *oh_mb = nullptr, *oh_s = nullptr, *oh_h = nullptr;
   bool have_pgrad = false;

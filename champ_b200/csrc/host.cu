@@ -978,6 +978,9 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
     // the derivative kernel adds its accumulators to the always-shared part of the layout
     size_t pgb = c->lay.base + align16(sizeof(double) * (4 * (size_t)c->N + 3 * (size_t)c->np_raw +
                                                          (size_t)c->N * c->np_raw));
+    // per-lane NLPP parameter slots: always in FP32; in FP64 while the warp's share stays small
+    c->pg_lanesum = (c->prec == CHAMP_PREC_MIXED || pgb <= 24 * 1024) ? 1 : 0;
+    if (c->pg_lanesum) pgb += align16(sizeof(double) * 32 * (size_t)c->np_raw);
     c->wpb_pg = 4;
     while (c->wpb_pg > 1 && pgb * c->wpb_pg > 160 * 1024) c->wpb_pg >>= 1;
     c->smem_pg = pgb * c->wpb_pg;
@@ -1045,6 +1048,7 @@ int champ_param_grad(champ_ctx *c, double *dlnpsi, double *deloc, double *eloc) 
   a.pgout.scr = c->pg_scr;
   a.pgout.scr_stride = c->scr_stride;
   a.pgout.part = 1;
+  a.pgout.lanesum = c->pg_lanesum;
   int rc = launch(c, Op::PGrad, a);
   if (rc) return rc;
   if (c->pg_scr) {

@@ -8,6 +8,7 @@
 // shared memory; larger per-walker scratch (orbitals of all electrons, projected
 // coefficients, pseudopotential task lists) in HBM.
 #pragma once
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -462,12 +463,13 @@ struct PGBuf {
   double *G;     // [P] d ln psi / dp
   double *K;     // [P] sum_e (lap_e g_p + 2 v_e . grad_e g_p)
   double *old;   // [N][P] basis function of p summed over the terms involving electron e
+  double *dvl;   // [P][32] each lane's part of dvn (summed into dvn after the quadrature loop)
   int P, na, nb;
   double *phis;  // [N][nbasis] or null: sum over the electron's quadrature points of
                  // w e^dJ v_l(r) P_l times each basis function (nonlocal part of B in basis space)
 };
 
-template <class T, int NORD>
+template <class T, int NORD, bool SLOTS>
 __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const View<T> &v, int e, const double *xn,
                                    double coeff, const PGBuf &pg);
 
@@ -838,7 +840,8 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
       if (PG) {
         double coeff = E.wq[q] * exp(dj) * vp * (double)dr;
         atomicAdd(&pg->csum[e], coeff);
-        point_param_values<T, NORD>(s, J, v, e, xn, coeff, *pg);
+        if (std::is_same<T, float>::value || pg->dvl) point_param_values<T, NORD, true>(s, J, v, e, xn, coeff, *pg);
+        else point_param_values<T, NORD, false>(s, J, v, e, xn, coeff, *pg);
         if (pg->phis) {
           double c2 = E.wq[q] * exp(dj) * vp;
           double *ph = pg->phis + (size_t)e * s.nbasis;
@@ -847,6 +850,15 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
       }
     }
     vnl = warp_sum(vnl);
+    if (PG && pg->dvl) {
+      __syncwarp();
+      for (int p = lane; p < pg->P; p += 32) {
+        double a = 0;
+        for (int l = 0; l < 32; l++) a += pg->dvl[p * 32 + l];
+        pg->dvn[p] += a;
+      }
+      __syncwarp();
+    }
   }
   double pe = s.pecent + pe_ee + (s.nloc > 0 ? vloc + vnl : pe_en);
   double d2lnpsi = d2lnd + d2j;

@@ -52,13 +52,27 @@ __device__ __forceinline__ void en_param_terms(const JasPar<T> &J, T r, T deni, 
   }
 }
 
+// Adds one point's contribution to the NLPP parameter sum dvn[idx]: into this lane's slot of
+// pg.dvl when the context gave the warp those slots (every lane of the warp adds to the same
+// parameters, so atomics serialise 32-fold; the slots are summed into dvn after the quadrature
+// loop), else a shared-memory atomic (large FP64 systems, where the slots' shared memory would
+// cost more L1 for the kernel's register spills than the atomics cost).
+// (The choice is a template parameter, which lets the compiler keep a slot in a register across
+// the loop that adds to it.)
+template <bool SLOTS>
+__device__ __forceinline__ void padd(double *slot, double *dvn, int idx, double v) {
+  if (SLOTS) slot[32 * idx] += v;
+  else atomicAdd(&dvn[idx], v);
+}
+
 // Parameter basis functions with electron e at the quadrature point xn, weighted by coeff
-// and added to pg.dvn.
-template <class T, int NORD>
+// and added to pg.dvn (through padd).
+template <class T, int NORD, bool SLOTS>
 __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const View<T> &v, int e, const double *xn,
                                    double coeff, const PGBuf &pg) {
   const int N = s.N, C = s.C;
   const T sk = J.scalek;
+  double *const slot = pg.dvl ? pg.dvl + (threadIdx.x & 31) : nullptr, *const dvn = pg.dvn;
   constexpr Terms tl = make_terms(NORD);
   const bool fast = (NORD > 1) && J.nct == 1 && C <= MAXC_NL;
   T pr[2 * MAXC_NL], asum[ZQ];
@@ -70,7 +84,7 @@ __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const Vi
     for (int k = 2; k <= J.norda; k++) {
       T t, t1, t2;
       en_param_terms(J, r, d, k, t, t1, t2, false);
-      atomicAdd(&pg.dvn[it * (J.norda - 1) + (k - 2)], coeff * (double)t);
+      padd<SLOTS>(slot, dvn, it * (J.norda - 1) + (k - 2), coeff * (double)t);
     }
     if (fast) {
       pr[2 * c] = r;
@@ -94,7 +108,7 @@ __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const Vi
     for (int k = 1; k <= J.nordb; k++) {
       T t, t1, t2;
       ee_param_terms(J, isb, ss, rij, du, k, t, t1, t2, false);
-      atomicAdd(&pg.dvn[pg.na + isb * J.nordb + (k - 1)], coeff * (double)t);
+      padd<SLOTS>(slot, dvn, pg.na + isb * J.nordb + (k - 1), coeff * (double)t);
     }
     if (fast) {
       T X[make_mixed(NORD).n > 0 ? make_mixed(NORD).n : 1];
@@ -118,20 +132,19 @@ __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const Vi
         uu[0] = pi[0] = pj[0] = T(1);
 #pragma unroll
         for (int q = 1; q <= NORD; q++) { uu[q] = uu[q - 1] * du; pi[q] = pi[q - 1] * di; pj[q] = pj[q - 1] * rj1; }
-        double *dst = pg.dvn + pg.na + pg.nb + s.ctype[c] * tl.n;
+        const int dst = pg.na + pg.nb + s.ctype[c] * tl.n;
 #pragma unroll
         for (int ll = 0; ll < tl.n; ll++) {
           const int k = tl.k[ll], l = tl.l[ll], m = tl.m[ll];
           T sl = (l == 0) ? T(2) : pi[l] + pj[l];
-          atomicAdd(&dst[ll], coeff * (double)(uu[k] * sl * pi[m] * pj[m]));
+          padd<SLOTS>(slot, dvn, dst + ll, coeff * (double)(uu[k] * sl * pi[m] * pj[m]));
         }
       }
     }
   }
   if (fast) {
-    double *dst = pg.dvn + pg.na + pg.nb;
 #pragma unroll
-    for (int ll = 0; ll < tl.n; ll++) atomicAdd(&dst[ll], coeff * (double)tsum[ll]);
+    for (int ll = 0; ll < tl.n; ll++) padd<SLOTS>(slot, dvn, pg.na + pg.nb + ll, coeff * (double)tsum[ll]);
   }
 }
 
@@ -332,6 +345,7 @@ struct PGOut {
   double *scr;     // per-walker scratch of the CSF/orbital part (null when there is none)
   size_t scr_stride;
   int part;        // 1: E_L, Jastrow derivatives, local B; 2: CSF and orbital derivatives
+  int lanesum;     // per-lane slots for the NLPP parameter sums (see padd)
 };
 
 // CSF and orbital-rotation derivatives from the orbital-resolved local energy
@@ -610,7 +624,7 @@ __global__ void __launch_bounds__(128, 4) k_pgrad(Sys<T> s, State<T> st, Layout 
   const int N = s.N;
   const int na = J.nct * (J.norda - 1 > 0 ? J.norda - 1 : 0), nb = J.nspin2b * J.nordb;
   const int nt = make_terms(NORD).n, P = na + nb + (NORD > 1 ? J.nct * nt : 0);
-  const size_t pgbytes = sizeof(double) * (3 * N + N + 3 * P + N * P);
+  const size_t pgbytes = sizeof(double) * (3 * N + N + 3 * P + N * P + (out.lanesum ? 32 * P : 0));
   const size_t wb = L.base + align16(pgbytes);
   const double R[9] = {r0, r1, r2, r3, r4, r5, r6, r7, r8};
   for (int w = blockIdx.x * wpb + wib; w < st.W; w += gridDim.x * wpb) {
@@ -623,7 +637,8 @@ __global__ void __launch_bounds__(128, 4) k_pgrad(Sys<T> s, State<T> st, Layout 
     pg.dvn = q; q += P;
     pg.G = q; q += P;
     pg.K = q; q += P;
-    pg.old = q;
+    pg.old = q; q += N * P;
+    pg.dvl = out.lanesum ? q : nullptr;
     pg.P = P; pg.na = na; pg.nb = nb;
     double *scr = out.scr ? out.scr + (size_t)w * out.scr_stride : nullptr;
     pg.phis = scr;
