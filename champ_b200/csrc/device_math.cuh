@@ -362,24 +362,33 @@ __device__ __forceinline__ T shell_dot_r(const Sys<T> &s, int ish, const double 
   return acc * ipow(T(1) / r, l) * R[0];
 }
 
-// Adds c times every basis function of one shell at pt into acc[b] (atomically).
+// shell_dot_r that also adds c times every basis function of the shell into acc[b] (atomically),
+// from the same values.
 template <class T>
-__device__ __forceinline__ void shell_accum(const Sys<T> &s, int ish, const double *pt, double c, double *acc) {
+__device__ __forceinline__ T shell_dot_acc(const Sys<T> &s, int ish, const double *pt, const T *g, const T *R0,
+                                           double cf, double *acc) {
   int4 sh = s.shell[ish];
-  int cn = sh.x, l = sh.z;
-  T d0 = T(pt[0] - s.cent[3 * cn]), d1 = T(pt[1] - s.cent[3 * cn + 1]), d2 = T(pt[2] - s.cent[3 * cn + 2]);
+  int c = sh.x, l = sh.z;
+  T d0 = T(pt[0] - s.cent[3 * c]), d1 = T(pt[1] - s.cent[3 * c + 1]), d2 = T(pt[2] - s.cent[3 * c + 2]);
   T r = tsqrt(d0 * d0 + d1 * d1 + d2 * d2);
   if (r == T(0)) { r = T(1e-30); d0 = r; }
   T R[3];
-  shell_radial<T, false>(s, ish, r, R);
+  if (R0) R[0] = *R0;
+  else shell_radial<T, false>(s, ish, r, R);
   T S[9], G[9][3];
   solid_all<T, false>(l, d0, d1, d2, S, G);
   int b0 = s.shb0[ish];
   const int nm = 2 * l + 1;
-  double f = c * (double)(ipow(T(1) / r, l) * R[0]);
+  const T rad = ipow(T(1) / r, l) * R[0];
+  const double f = cf * (double)rad;
+  T dot = 0;
 #pragma unroll
   for (int sl = 0; sl < 9; sl++)
-    if (sl < nm) atomicAdd(&acc[b0 + sl], f * (double)S[sl]);
+    if (sl < nm) {
+      dot += S[sl] * g[b0 + sl];
+      atomicAdd(&acc[b0 + sl], f * (double)S[sl]);
+    }
+  return dot * rad;
 }
 
 // Warp: all basis functions at pt into phi (shared memory).

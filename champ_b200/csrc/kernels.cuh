@@ -779,12 +779,14 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
       // determinant ratio: orbitals at the point contracted with G
       const T *ge = gp + (size_t)e * B;
       T dr = 0;
-      {
-        const int c0 = nshc > 0 ? s.cshell0[c] : 0, c1 = nshc > 0 ? s.cshell0[c + 1] : 0;
-        const T *ro = rown + task * nshc - c0;
+      const int c0 = nshc > 0 ? s.cshell0[c] : 0, c1 = nshc > 0 ? s.cshell0[c + 1] : 0;
+      const T *ro = rown + task * nshc - c0;
+      // with the nonlocal B-matrix sums wanted, the basis values at the point are formed once,
+      // after the Jastrow ratio, for both the ratio and those sums
+      const bool merged = PG && pg->phis != nullptr;
+      if (!merged)
         for (int ish = 0; ish < s.nshell; ish++)
           dr += shell_dot_r<T>(s, ish, xn, ge, (ish >= c0 && ish < c1) ? ro + ish : nullptr);
-      }
       // Jastrow ratio (nonlocj, nonloc.f90:432-522): point-centre distances once per point
       double dj = 0;
       const bool fast = (NORD > 1) && J.nct == 1 && C <= MAXC_NL;
@@ -836,17 +838,18 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
       double vp = 0;
       for (int l = 0; l < E.npotd[it]; l++)
         if (l + 1 != E.lpotp1[it]) vp += rec[2 + l] * yl0(l, costh);
+      if (merged) {
+        const double c2 = E.wq[q] * exp(dj) * vp;
+        double *ph = pg->phis + (size_t)e * s.nbasis;
+        for (int ish = 0; ish < s.nshell; ish++)
+          dr += shell_dot_acc<T>(s, ish, xn, ge, (ish >= c0 && ish < c1) ? ro + ish : nullptr, c2, ph);
+      }
       vnl += E.wq[q] * exp(dj) * vp * (double)dr;
       if (PG) {
         double coeff = E.wq[q] * exp(dj) * vp * (double)dr;
         atomicAdd(&pg->csum[e], coeff);
         if (std::is_same<T, float>::value || pg->dvl) point_param_values<T, NORD, true>(s, J, v, e, xn, coeff, *pg);
         else point_param_values<T, NORD, false>(s, J, v, e, xn, coeff, *pg);
-        if (pg->phis) {
-          double c2 = E.wq[q] * exp(dj) * vp;
-          double *ph = pg->phis + (size_t)e * s.nbasis;
-          for (int ish = 0; ish < s.nshell; ish++) shell_accum<T>(s, ish, xn, c2, ph);
-        }
       }
     }
     vnl = warp_sum(vnl);
