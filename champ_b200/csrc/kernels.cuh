@@ -471,7 +471,7 @@ struct PGBuf {
 
 template <class T, int NORD, bool SLOTS>
 __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const View<T> &v, int e, const double *xn,
-                                   double coeff, const PGBuf &pg);
+                                   double coeff, const PGBuf &pg, const T *tsum_pre);
 
 template <class T, int NORD, bool MD, bool PG = false>
 __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, const State<T> &st, int w,
@@ -807,6 +807,15 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
         }
         dj += (double)f - (double)fso[e * N + e];
       }
+      // FP32 derivative run: the e-e-n parameter basis functions at the point, summed over the
+      // other electrons from the same X sums as the value (handed to point_param_values).  The
+      // FP64 run forms them there instead: 13 more FP64 registers here cost it more in spills.
+      constexpr bool SHARE = PG && std::is_same<T, float>::value;
+      constexpr int NT = make_terms(NORD).n > 0 ? make_terms(NORD).n : 1;
+      T tsum[SHARE ? NT : 1];
+      if (SHARE)
+#pragma unroll
+        for (int ll = 0; ll < NT; ll++) tsum[ll] = T(0);
       for (int j = 0; j < N; j++) {
         if (j == e) continue;
         int isb, ipar;
@@ -821,7 +830,23 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
         if (fast) {
           T X[make_mixed(NORD).n > 0 ? make_mixed(NORD).n : 1];
           een_xsums<T, NORD>(C, pr, v.ren + 2 * C * j, X);
-          f += een_from_x<T, NORD>(J.c[0], du, asum, v.zq + ZQ * j, X);
+          if (SHARE) {
+            constexpr Terms tl = make_terms(NORD);
+            constexpr XIdx xi = make_xidx(NORD);
+            const T *zj = v.zq + ZQ * j;
+            T uu[NORD + 1];
+            uu[0] = T(1);
+#pragma unroll
+            for (int q2 = 1; q2 <= NORD; q2++) uu[q2] = uu[q2 - 1] * du;
+#pragma unroll
+            for (int ll = 0; ll < tl.n; ll++) {
+              const T t = uu[tl.k[ll]] * (xsel(xi.a1[ll], asum, zj, X) + xsel(xi.a2[ll], asum, zj, X));
+              f += J.c[0][ll] * t;
+              tsum[ll] += t;
+            }
+          } else {
+            f += een_from_x<T, NORD>(J.c[0], du, asum, v.zq + ZQ * j, X);
+          }
         } else if (NORD > 1) {
           const T *rj_ = v.ren + 2 * C * j;
           for (int c2 = 0; c2 < C; c2++) {
@@ -848,8 +873,9 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
       if (PG) {
         double coeff = E.wq[q] * exp(dj) * vp * (double)dr;
         atomicAdd(&pg->csum[e], coeff);
-        if (std::is_same<T, float>::value || pg->dvl) point_param_values<T, NORD, true>(s, J, v, e, xn, coeff, *pg);
-        else point_param_values<T, NORD, false>(s, J, v, e, xn, coeff, *pg);
+        const T *ts = (SHARE && fast) ? tsum : nullptr;
+        if (std::is_same<T, float>::value || pg->dvl) point_param_values<T, NORD, true>(s, J, v, e, xn, coeff, *pg, ts);
+        else point_param_values<T, NORD, false>(s, J, v, e, xn, coeff, *pg, ts);
       }
     }
     vnl = warp_sum(vnl);

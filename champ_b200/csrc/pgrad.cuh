@@ -69,12 +69,13 @@ __device__ __forceinline__ void padd(double *slot, double *dvn, int idx, double 
 // and added to pg.dvn (through padd).
 template <class T, int NORD, bool SLOTS>
 __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const View<T> &v, int e, const double *xn,
-                                   double coeff, const PGBuf &pg) {
+                                   double coeff, const PGBuf &pg, const T *tsum_pre) {
   const int N = s.N, C = s.C;
   const T sk = J.scalek;
   double *const slot = pg.dvl ? pg.dvl + (threadIdx.x & 31) : nullptr, *const dvn = pg.dvn;
   constexpr Terms tl = make_terms(NORD);
   const bool fast = (NORD > 1) && J.nct == 1 && C <= MAXC_NL;
+  const bool xsums = fast && tsum_pre == nullptr;  // e-e-n sums still to form here
   T pr[2 * MAXC_NL], asum[ZQ];
   for (int q = 0; q < ZQ; q++) asum[q] = (q == 0) ? T(C) : T(0);
   for (int c = 0; c < C; c++) {
@@ -86,7 +87,7 @@ __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const Vi
       en_param_terms(J, r, d, k, t, t1, t2, false);
       padd<SLOTS>(slot, dvn, it * (J.norda - 1) + (k - 2), coeff * (double)t);
     }
-    if (fast) {
+    if (xsums) {
       pr[2 * c] = r;
       pr[2 * c + 1] = d;
       T p = d;
@@ -110,7 +111,7 @@ __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const Vi
       ee_param_terms(J, isb, ss, rij, du, k, t, t1, t2, false);
       padd<SLOTS>(slot, dvn, pg.na + isb * J.nordb + (k - 1), coeff * (double)t);
     }
-    if (fast) {
+    if (xsums) {
       T X[make_mixed(NORD).n > 0 ? make_mixed(NORD).n : 1];
       een_xsums<T, NORD>(C, pr, v.ren + 2 * C * j, X);
       const T *zj = v.zq + ZQ * j;
@@ -122,7 +123,7 @@ __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const Vi
 #pragma unroll
       for (int ll = 0; ll < tl.n; ll++)
         tsum[ll] += uu[tl.k[ll]] * (xsel(xi.a1[ll], asum, zj, X) + xsel(xi.a2[ll], asum, zj, X));
-    } else if (NORD > 1) {
+    } else if (!fast && NORD > 1) {
       const T *rj_ = v.ren + 2 * C * j;
       for (int c = 0; c < C; c++) {
         T ri, di;
@@ -144,7 +145,8 @@ __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const Vi
   }
   if (fast) {
 #pragma unroll
-    for (int ll = 0; ll < tl.n; ll++) padd<SLOTS>(slot, dvn, pg.na + pg.nb + ll, coeff * (double)tsum[ll]);
+    for (int ll = 0; ll < tl.n; ll++)
+      padd<SLOTS>(slot, dvn, pg.na + pg.nb + ll, coeff * (double)(tsum_pre ? tsum_pre[ll] : tsum[ll]));
   }
 }
 
