@@ -217,16 +217,23 @@ __device__ void jastrow_param_pass(const Sys<T> &s, const JasPar<T> &J, const Vi
         T rij = tsqrt(T(rvd[0] * rvd[0] + rvd[1] * rvd[1] + rvd[2] * rvd[2]));
         T du = T(1) / (T(1) + sk * rij);
         const T *ri_ = v.ren + 2 * C * i, *rj_ = v.ren + 2 * C * j;
-        double oc[tl.n > 0 ? tl.n : 1];
+        // sums over the centres of this pair in the compute precision (FP32 in the mixed
+        // engine: no FP64 work per term), added to the FP64 totals once per pair
+        constexpr bool PP = std::is_same<T, float>::value;
+        T ocp[tl.n > 0 ? tl.n : 1], kcp[PP && tl.n > 0 ? tl.n : 1];
 #pragma unroll
-        for (int ll = 0; ll < tl.n; ll++) oc[ll] = 0.0;
+        for (int ll = 0; ll < tl.n; ll++) ocp[ll] = T(0);
+        if (PP)
+#pragma unroll
+          for (int ll = 0; ll < tl.n; ll++) kcp[ll] = T(0);
+        const T vi0 = T(vi[0]), vi1 = T(vi[1]), vi2 = T(vi[2]), vj0 = T(vj[0]), vj1 = T(vj[1]), vj2 = T(vj[2]);
+        const T vi_rv = vi0 * T(rvd[0]) + vi1 * T(rvd[1]) + vi2 * T(rvd[2]);
+        const T vj_rv = vj0 * T(rvd[0]) + vj1 * T(rvd[1]) + vj2 * T(rvd[2]);
         for (int c = 0; c < C; c++) {
           const double *cc = s.cent + 3 * c;
           T ri = ri_[2 * c], di = ri_[2 * c + 1], rj = rj_[2 * c], dj = rj_[2 * c + 1];
-          double vi_ri = vi[0] * (xi[0] - cc[0]) + vi[1] * (xi[1] - cc[1]) + vi[2] * (xi[2] - cc[2]);
-          double vi_rv = vi[0] * rvd[0] + vi[1] * rvd[1] + vi[2] * rvd[2];
-          double vj_rj = vj[0] * (xj[0] - cc[0]) + vj[1] * (xj[1] - cc[1]) + vj[2] * (xj[2] - cc[2]);
-          double vj_rv = vj[0] * rvd[0] + vj[1] * rvd[1] + vj[2] * rvd[2];
+          const T vi_ri = vi0 * T(xi[0] - cc[0]) + vi1 * T(xi[1] - cc[1]) + vi2 * T(xi[2] - cc[2]);
+          const T vj_rj = vj0 * T(xj[0] - cc[0]) + vj1 * T(xj[1] - cc[1]) + vj2 * T(xj[2] - cc[2]);
           // power tables with two zero entries below 0, as in jas_een
           T uu[NORD + 3], rri[NORD + 3], rrj[NORD + 3];
           uu[0] = uu[1] = rri[0] = rri[1] = rrj[0] = rrj[1] = T(0);
@@ -262,18 +269,22 @@ __device__ void jastrow_param_pass(const Sys<T> &s, const JasPar<T> &J, const Vi
             fu = fu * dd1 / rij;
             fi = fi * dd7 / ri;
             fj = fj * dd8 / rj;
-            double lap = (double)(2 * (2 * fu + fi + fj) + 2 * fuu + fii + fjj + fui * cpst + fuj * cmst);
-            kc[ll] += lap + 2.0 * ((double)fi * vi_ri + (double)fu * vi_rv + (double)fj * vj_rj - (double)fu * vj_rv);
-            oc[ll] += (double)fc;
+            const T kk = 2 * (2 * fu + fi + fj) + 2 * fuu + fii + fjj + fui * cpst + fuj * cmst +
+                         2 * (fi * vi_ri + fu * vi_rv + fj * vj_rj - fu * vj_rv);
+            if (PP) kcp[ll] += kk;
+            else kc[ll] += (double)kk;
+            ocp[ll] += fc;
           }
           if (J.nct > 1) {  // each centre type has its own c set
             const int base = pg.na + pg.nb + s.ctype[c] * tl.n;
 #pragma unroll
             for (int ll = 0; ll < tl.n; ll++) {
-              atomicAdd(&pg.K[base + ll], kc[ll]);
-              atomicAdd(&pg.old[i * P + base + ll], oc[ll]);
-              atomicAdd(&pg.old[j * P + base + ll], oc[ll]);
-              kc[ll] = oc[ll] = 0.0;
+              atomicAdd(&pg.K[base + ll], kc[ll] + (PP ? (double)kcp[ll] : 0.0));
+              atomicAdd(&pg.old[i * P + base + ll], (double)ocp[ll]);
+              atomicAdd(&pg.old[j * P + base + ll], (double)ocp[ll]);
+              kc[ll] = 0.0;
+              ocp[ll] = T(0);
+              if (PP) kcp[ll] = T(0);
             }
           }
         }
@@ -281,8 +292,9 @@ __device__ void jastrow_param_pass(const Sys<T> &s, const JasPar<T> &J, const Vi
           const int base = pg.na + pg.nb;
 #pragma unroll
           for (int ll = 0; ll < tl.n; ll++) {
-            atomicAdd(&pg.old[i * P + base + ll], oc[ll]);
-            atomicAdd(&pg.old[j * P + base + ll], oc[ll]);
+            if (PP) kc[ll] += (double)kcp[ll];
+            atomicAdd(&pg.old[i * P + base + ll], (double)ocp[ll]);
+            atomicAdd(&pg.old[j * P + base + ll], (double)ocp[ll]);
           }
         }
       }
