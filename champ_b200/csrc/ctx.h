@@ -94,6 +94,7 @@ struct champ_ctx {
   std::vector<int> tc_shl;        // host copy of the shells' l (internal basis order)
   // fused basis + contraction (orbfused.cuh): padded K layout and split coefficients
   int tc_fused_ok = 0, tc_mode = 0;  // fused kernel supported; mode in use: 1 fused, 2 basis rows + product
+  int tc_kchunk = 4;                 // fused kernel: K-blocks per TMEM accumulation chunk (0: all)
   int tc_kq = 0, tc_nkb = 0, tc_fcols[2] = {32, 32};
   int *tc_blk_sh = nullptr, *tc_kpos = nullptr;
   float *tc_bf[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [spin][hi, lo]: [Np][Kq]

@@ -664,13 +664,13 @@ static int tc_setup(champ_ctx *c) {
       for (int b = 0; b < B; b++) {
         float v = c->tc_coef[sp][(size_t)b * no + m], h = orbtc::tf32_hi(v);
         hi[(size_t)m * Kp + b] = h;
-        lo[(size_t)m * Kp + b] = v - h;
+        lo[(size_t)m * Kp + b] = orbtc::tf32_lo(v, h);
       }
       for (int i = 0; i < c->nshell; i++)
         for (int sl = 0; sl < 2 * c->tc_shl[i] + 1; sl++) {
           float v = c->tc_coef[sp][(size_t)(b0[i] + sl) * no + m], h = orbtc::tf32_hi(v);
           fhi[(size_t)m * Kq + kpos[i] + sl] = h;
-          flo[(size_t)m * Kq + kpos[i] + sl] = v - h;
+          flo[(size_t)m * Kq + kpos[i] + sl] = orbtc::tf32_lo(v, h);
         }
     }
     c->tc_b[sp][0] = dalloc<float>(c, hi.size());
@@ -1372,6 +1372,11 @@ int champ_set_option(champ_ctx *c, const char *name, int64_t value) {
     c->reinv_every = (int)value;
     return CHAMP_OK;
   }
+  if (!strcmp(name, "orbital_tc_chunk")) {
+    if (value < 0 || value > (1 << 20)) return fail(CHAMP_EINVAL, "orbital_tc_chunk must be >= 0");
+    c->tc_kchunk = (int)value;
+    return CHAMP_OK;
+  }
   return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);
 }
 
@@ -1385,6 +1390,7 @@ int champ_get_option(const champ_ctx *c, const char *name, int64_t *value) {
   }
   if (!strcmp(name, "reinvert_every")) { *value = c->reinv_every; return CHAMP_OK; }
   if (!strcmp(name, "dmc_graph")) { *value = c->dmc_graph_on; return CHAMP_OK; }
+  if (!strcmp(name, "orbital_tc_chunk")) { *value = c->tc_kchunk; return CHAMP_OK; }
   return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);
 }
 

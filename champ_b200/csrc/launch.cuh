@@ -67,6 +67,7 @@ static int run_orb_tc(champ_ctx *c, const State<T> &st) {
         f.e0 = sp ? c->nup : 0;
         f.nomax = c->nomax;
         f.nocc = c->md.nocc[sp];
+        f.kchunk = c->tc_kchunk > 0 ? c->tc_kchunk : f.nkb;
         f.err = c->tc_err;
         const int tiles = (f.M + orbtc::BM - 1) / orbtc::BM;
         orbf::k_orb_fused<<<(unsigned)std::min(tiles, sm), orbf::NTF, orbf::fsmem_bytes(f.Np), c->stream>>>(c->sf, f);

@@ -5,11 +5,18 @@
 // in which no shell straddles a K-block of 16, N = orbitals of the spin.  Five products share the
 // coefficients: one per channel (value, d/dx, d/dy, d/dz, Laplacian), accumulated in five TMEM
 // column ranges.  Warps 0-3 evaluate the basis functions of one K-block for 128 electrons (one
-// thread per electron, all lanes walk the same shells), split each value into TF32 hi + FP32
-// remainder and store both into the channel's A tile; warps 4-7 bring the split coefficients of
+// thread per electron, all lanes walk the same shells), split each value into its TF32 parts
+// hi + lo (both rounded to nearest) and store both into the channel's A tile; warps 4-7 bring the split coefficients of
 // the block with cp.async; one thread issues 5 x 2 x 3 tcgen05.mma (kind::tf32, hi.hi + hi.lo +
 // lo.hi) per block and commits to the stage's mbarrier, so the evaluation of the next block
 // overlaps the tensor cores.  All waits are bounded.
+//
+// Accumulation in chunks: the tensor core sums each MMA's products into the FP32 accumulator
+// with truncation, so a long chain of MMAs into one accumulator shrinks it systematically
+// (about half an ulp per MMA; over the 150 MMAs of a 416-function basis the E_L of a
+// 128-electron walker moves by ~1e-6 relative).  The K-blocks are therefore taken in chunks of
+// `kchunk`: after each chunk the accumulator is drained and added to the orbital rows in HBM
+// with round-to-nearest FP32 adds (the first chunk stores), and the next chunk starts from zero.
 #pragma once
 
 namespace orbf {
@@ -28,6 +35,7 @@ struct FArgs {
   int M;                    // rows: W * n
   int Kq, nkb, Np, ncols;   // padded K, K-blocks, padded N (multiple of 16, 5*Np <= 512), TMEM columns
   int n, N, e0, nomax, nocc;
+  int kchunk;               // K-blocks per accumulation chunk (>= 1)
   int *err;
 };
 
@@ -67,6 +75,9 @@ static __global__ void __launch_bounds__(NTF, 1) k_orb_fused(Sys<float> s, FArgs
   const uint32_t tbase = tslot;
   const uint32_t idesc = idesc_tf32(BM, a.Np);
   const int ntile = (a.M + BM - 1) / BM;
+  const int cb = a.kchunk > 0 ? a.kchunk : a.nkb;
+  const int quad = warp & 3, half = warp >> 2;
+  const bool vec = (a.nomax & 3) == 0 && ((uintptr_t)a.orb & 15) == 0;  // rows and groups 16-byte aligned
   uint32_t it = 0;  // K-blocks issued so far (commit count)
   bool ok = true;
   for (int tile = blockIdx.x; tile < ntile && ok; tile += gridDim.x) {
@@ -79,6 +90,14 @@ static __global__ void __launch_bounds__(NTF, 1) k_orb_fused(Sys<float> s, FArgs
         const double *p = a.x + ((size_t)w * a.N + a.e0 + eo) * 3;
         pt[0] = p[0]; pt[1] = p[1]; pt[2] = p[2];
         live = true;
+      }
+    }
+    float *dst = nullptr;  // this thread's epilogue row
+    {
+      const int r = tile * BM + quad * 32 + lane;
+      if (r < a.M) {
+        const int w = r / a.n, eo = r - w * a.n;
+        dst = a.orb + ((size_t)w * a.N + a.e0 + eo) * 5 * a.nomax;
       }
     }
     for (int kb = 0; kb < a.nkb; kb++, it++) {
@@ -95,7 +114,7 @@ static __global__ void __launch_bounds__(NTF, 1) k_orb_fused(Sys<float> s, FArgs
               const float h = tf32_hi(v);
               const uint32_t o = foff(tid, kk + sl);
               *(float *)(st + (2 * ch) * sA + o) = h;
-              *(float *)(st + (2 * ch + 1) * sA + o) = v - h;
+              *(float *)(st + (2 * ch + 1) * sA + o) = tf32_lo(v, h);
             });
           }
         }  // rows past the end keep finite stale values; their outputs are not stored
@@ -125,36 +144,49 @@ static __global__ void __launch_bounds__(NTF, 1) k_orb_fused(Sys<float> s, FArgs
             const uint64_t dal = sdesc(ua + (2 * ch + 1) * sA + ko, 128, (BKF / 4) * 128);
             const uint64_t dbh = sdesc(ub + ko, 128, (BKF / 4) * 128), dbl = sdesc(ub + sB + ko, 128, (BKF / 4) * 128);
             const uint32_t d = tbase + (uint32_t)(ch * a.Np);
-            mma_tf32(d, dal, dbh, idesc, (kb > 0 || ks > 0) ? 1u : 0u);
+            mma_tf32(d, dal, dbh, idesc, (kb % cb > 0 || ks > 0) ? 1u : 0u);
             mma_tf32(d, dah, dbl, idesc, 1u);
             mma_tf32(d, dah, dbh, idesc, 1u);
           }
         mma_commit(smem_u32(&mbar[sg]));
       }
+      if ((kb + 1) % cb != 0 && kb + 1 != a.nkb) continue;
+      // end of a chunk: drain.  Warp q reads TMEM lanes 32(q mod 4)..+31; warps q and q+4 take
+      // alternate groups of 16 columns of the 5 channel ranges (Np is a multiple of 16: a group
+      // is in one channel).  Each thread adds into the row elements it stored itself.
+      if (!__syncthreads_and(mbar_wait(smem_u32(&mbar[sg]), (it >> 1) & 1))) { ok = false; break; }
+      fence_after();
+      const bool first = kb < cb;
+      for (int c0 = 16 * half; c0 < 5 * a.Np; c0 += 32) {
+        float v[16];
+        tmem_ld16(tbase + ((uint32_t)(quad * 32) << 16) + (uint32_t)c0, v);
+        const int ch = c0 / a.Np, m0 = c0 - ch * a.Np;
+        if (dst) {
+          float *o = dst + ch * a.nomax + m0;
+          if (vec && m0 + 16 <= a.nocc) {  // 16-byte aligned: four float4 per group
+            float4 *o4 = (float4 *)o;
+            if (first) {
+#pragma unroll
+              for (int k = 0; k < 4; k++) o4[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+            } else {
+              float4 p[4];
+#pragma unroll
+              for (int k = 0; k < 4; k++) p[k] = o4[k];
+#pragma unroll
+              for (int k = 0; k < 4; k++)
+                o4[k] = make_float4(p[k].x + v[4 * k], p[k].y + v[4 * k + 1], p[k].z + v[4 * k + 2], p[k].w + v[4 * k + 3]);
+            }
+          } else {
+#pragma unroll
+            for (int k = 0; k < 16; k++)
+              if (m0 + k < a.nocc) o[k] = first ? v[k] : o[k] + v[k];
+          }
+        }
+      }
+      fence_before();
+      __syncthreads();
     }
     if (!ok) break;
-    // epilogue: warp q reads TMEM lanes 32(q mod 4)..+31; warps q and q+4 take alternate groups
-    // of 16 columns of the 5 channel ranges (Np is a multiple of 16: a group is in one channel)
-    if (!__syncthreads_and(mbar_wait(smem_u32(&mbar[(it - 1) & 1]), ((it - 1) >> 1) & 1))) { ok = false; break; }
-    fence_after();
-    const int quad = warp & 3, half = warp >> 2;
-    const int r = tile * BM + quad * 32 + lane;
-    float *dst = nullptr;
-    if (r < a.M) {
-      const int w = r / a.n, eo = r - w * a.n;
-      dst = a.orb + ((size_t)w * a.N + a.e0 + eo) * 5 * a.nomax;
-    }
-    for (int c0 = 16 * half; c0 < 5 * a.Np; c0 += 32) {
-      float v[16];
-      tmem_ld16(tbase + ((uint32_t)(quad * 32) << 16) + (uint32_t)c0, v);
-      const int ch = c0 / a.Np, m0 = c0 - ch * a.Np;
-      if (dst)
-#pragma unroll
-        for (int k = 0; k < 16; k++)
-          if (m0 + k < a.nocc) dst[ch * a.nomax + m0 + k] = v[k];
-    }
-    fence_before();
-    __syncthreads();
   }
   cp_wait_all();
   if (!ok) {

@@ -5,10 +5,13 @@
 //   orb[w][e][ch][m] = sum_b phi[w][e][ch][b] coef[b][m],   ch = value, d/dx, d/dy, d/dz, lap.
 // k_basis_rows writes phi (FP32, K-major rows padded to Kp) to HBM; k_orb_tc runs the product
 // with tcgen05.mma kind::tf32 into a TMEM accumulator.  TF32 keeps 10 mantissa bits, so each
-// operand is split as x = hi + lo (hi = x with the low 13 mantissa bits cleared, lo = x - hi,
-// exact in FP32) and the product is hi*hi + hi*lo + lo*hi: about FP32 accuracy (relative error
-// ~2^-21 per product, FP32 accumulation), three tensor-core passes.  Used by the mixed-precision
-// engine only; the FP64 engine keeps the CUDA-core contraction.
+// operand is split as x = hi + lo + r with hi = x rounded to nearest TF32 and lo = (x - hi)
+// rounded to nearest TF32 (both exact TF32 values, so the tensor core drops no bits of them),
+// and the product is hi*hi + hi*lo + lo*hi: about FP32 accuracy (|r| <= 2^-22 |x|, lo*lo below
+// 2^-22, FP32 accumulation), three tensor-core passes.  Rounding to nearest keeps the dropped
+// parts of either sign; a truncating split would drop them all towards zero and shrink every
+// product by ~1e-6 on average, a bias that accumulates in ln|D| over many rows.  Used by the
+// mixed-precision engine only; the FP64 engine keeps the CUDA-core contraction.
 #pragma once
 #include <cstdint>
 
@@ -80,18 +83,26 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
-__host__ __device__ inline float tf32_hi(float x) {
+// x rounded to the nearest TF32 value (ties away from zero), returned as an FP32 bit pattern
+// with the low 13 mantissa bits zero
+__host__ __device__ inline float tf32_rn(float x) {
 #ifdef __CUDA_ARCH__
-  return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
 #else
   uint32_t u;
   memcpy(&u, &x, 4);
+  if ((u & 0x7F800000u) != 0x7F800000u) u += 0x1000u;  // half an ulp of TF32, carry into the exponent
   u &= 0xFFFFE000u;
   float h;
   memcpy(&h, &u, 4);
   return h;
 #endif
 }
+// the two TF32 parts of x: hi = rn(x), lo = rn(x - hi)
+__host__ __device__ inline float tf32_hi(float x) { return tf32_rn(x); }
+__host__ __device__ inline float tf32_lo(float x, float hi) { return tf32_rn(x - hi); }
 
 struct Args {
   const float *phi;          // [rows of all walkers][Kp]; row = (w*N + e)*5 + ch
@@ -186,12 +197,13 @@ __global__ void __launch_bounds__(NTHR, 1) k_orb_tc(Args a) {
     unsigned char *st = base + (size_t)s * stage;
     cp_wait<NS - 2>();  // this thread's copies of block i have landed
     __syncthreads();
-    // split A in place: hi = x with the low 13 mantissa bits cleared, lo = x - hi
+    // split A in place into its TF32 parts hi and lo
     for (int q = tid; q < BM * (BK / 4); q += NTHR) {
       float4 v = *(float4 *)(st + 16 * q);
       float4 h = make_float4(tf32_hi(v.x), tf32_hi(v.y), tf32_hi(v.z), tf32_hi(v.w));
       *(float4 *)(st + 16 * q) = h;
-      *(float4 *)(st + sA + 16 * q) = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+      *(float4 *)(st + sA + 16 * q) =
+          make_float4(tf32_lo(v.x, h.x), tf32_lo(v.y, h.y), tf32_lo(v.z, h.z), tf32_lo(v.w, h.w));
     }
     fence_async_smem();
     __syncthreads();

@@ -246,6 +246,11 @@ int champ_synchronize(champ_ctx *ctx);
    written to HBM first; 0 uses the CUDA-core contraction.  Available for
    mixed precision when the walker state lives in HBM and a spin has >= 16 orbitals, and on by
    default there; CHAMP_EINVAL otherwise.
+   "orbital_tc_chunk": K-blocks of 16 basis functions that the fused contraction sums into one
+   TMEM accumulator before adding it to the orbital rows in FP32 (default 4; 0 = all of K).  The
+   tensor core truncates while it accumulates, so shorter chunks shrink the resulting bias
+   towards zero of the orbitals (and with it of ln|D| and E_L) at the cost of a read-modify-write
+   of the rows per chunk.
    "reinvert_every": the full evaluation after a VMC sweep re-inverts the Slater matrices in
    FP64 every this many sweeps (sweep index divisible by it) and otherwise uses the inverses
    kept current by the Sherman-Morrison updates of the accepted moves; default
@@ -253,7 +258,7 @@ int champ_synchronize(champ_ctx *ctx);
    "dmc_graph": 1 (default) replays pairs of DMC steps as a captured CUDA graph, 0 launches the
    kernels of every step from the host. */
 int champ_set_option(champ_ctx *ctx, const char *name, int64_t value);
-/* Current value of an option ("orbital_tc", "reinvert_every", "dmc_graph"); kernel launches per champ_vmc_sweeps sweep
+/* Current value of an option ("orbital_tc", "orbital_tc_chunk", "reinvert_every", "dmc_graph"); kernel launches per champ_vmc_sweeps sweep
    ("launches_per_sweep": 1 for the fused sweep kernel, 5 with the tensor-core orbitals). */
 int champ_get_option(const champ_ctx *ctx, const char *name, int64_t *value);
 
