@@ -97,6 +97,8 @@ static int run_orb_tc(champ_ctx *c, const State<T> &st) {
       g.e0 = sp ? c->nup : 0;
       g.nomax = c->nomax;
       g.nocc = c->md.nocc[sp];
+      // the same MMA chain length as the fused kernel's chunks (its K-blocks are half as long)
+      g.kchunk = c->tc_kchunk > 0 ? std::max(1, c->tc_kchunk * orbf::BKF / orbtc::BK) : g.Kp / orbtc::BK;
       g.err = c->tc_err;
       const int tiles = (g.M + orbtc::BM - 1) / orbtc::BM, ns = orbtc::stages_for(g.Np);
       const unsigned grid = (unsigned)std::min(tiles, sm);

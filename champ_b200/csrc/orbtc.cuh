@@ -111,6 +111,7 @@ struct Args {
   int M;                     // rows of this spin: W * n * 5
   int Kp, Np, ncols;         // padded K (multiple of BK), padded N (multiple of 16), TMEM columns
   int n, N, e0, nomax, nocc; // electrons of the spin, all electrons, first electron, row stride, orbitals
+  int kchunk;                // K-blocks per TMEM accumulation chunk (>= 1), drained into orb
   int *err;
 };
 
@@ -162,6 +163,8 @@ __global__ void __launch_bounds__(NTHR, 1) k_orb_tc(Args a) {
   const int my_tiles = blockIdx.x < ntile ? (ntile - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   const int T = my_tiles * nkb;  // K-blocks this CTA runs
   const int nw_rows = a.n * 5;   // rows per walker of this spin
+  const int cb = a.kchunk > 0 ? a.kchunk : nkb;
+  const bool vec = (a.nomax & 3) == 0 && ((uintptr_t)a.orb & 15) == 0;
 
   // issue the copies of K-block i into its stage (an empty group past the end)
   auto issue = [&](int i) {
@@ -216,7 +219,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_orb_tc(Args a) {
         const uint32_t ko = ks * 256;
         uint64_t dah = sdesc(uah + ko, 128, (BK / 4) * 128), dal = sdesc(ual + ko, 128, (BK / 4) * 128);
         uint64_t dbh = sdesc(ubh + ko, 128, (BK / 4) * 128), dbl = sdesc(ubl + ko, 128, (BK / 4) * 128);
-        mma_tf32(tbase, dal, dbh, idesc, (kb > 0 || ks > 0) ? 1u : 0u);
+        mma_tf32(tbase, dal, dbh, idesc, (kb % cb > 0 || ks > 0) ? 1u : 0u);
         mma_tf32(tbase, dah, dbl, idesc, 1u);
         mma_tf32(tbase, dah, dbh, idesc, 1u);
       }
@@ -229,10 +232,13 @@ __global__ void __launch_bounds__(NTHR, 1) k_orb_tc(Args a) {
     if (i >= 1) got = mbar_wait(smem_u32(&mbar[(i - 1) % NS]), ((i - 1) / NS) & 1);
     if (!__syncthreads_and(got)) { ok = false; break; }
     issue(i + NS - 1);
-    if (kb == nkb - 1) {
-      // epilogue: drain the accumulator; warp q reads TMEM lanes 32(q mod 4)..+31 (the lanes a
+    if ((kb + 1) % cb == 0 || kb == nkb - 1) {
+      // end of an accumulation chunk: drain the accumulator and store it (first chunk of the
+      // tile) or add it to the rows (round-to-nearest FP32; the tensor core's own accumulation
+      // truncates, so chains stay short); warp q reads TMEM lanes 32(q mod 4)..+31 (the lanes a
       // warp may access), warps q and q+4 take alternate groups of 16 columns
       if (!__syncthreads_and(mbar_wait(smem_u32(&mbar[s]), (i / NS) & 1))) { ok = false; break; }
+      const bool first = kb < cb;
       fence_after();
       const int tile = (int)blockIdx.x + (i / nkb) * (int)gridDim.x;
       const int quad = warp & 3, half = warp >> 2;
@@ -245,10 +251,24 @@ __global__ void __launch_bounds__(NTHR, 1) k_orb_tc(Args a) {
       for (int c0 = 16 * half; c0 < a.Np; c0 += 32) {
         float v[16];
         tmem_ld16(tbase + ((uint32_t)(quad * 32) << 16) + (uint32_t)c0, v);
-        if (dst)
+        if (!dst) continue;
+        float *o = dst + c0;
+        if (vec && c0 + 16 <= a.nocc) {  // 16-byte aligned: four float4 per group
+          float4 *o4 = (float4 *)o;
+          float4 p[4];
+          if (!first)
+#pragma unroll
+            for (int k = 0; k < 4; k++) p[k] = o4[k];
+#pragma unroll
+          for (int k = 0; k < 4; k++)
+            o4[k] = first ? make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3])
+                          : make_float4(p[k].x + v[4 * k], p[k].y + v[4 * k + 1], p[k].z + v[4 * k + 2],
+                                        p[k].w + v[4 * k + 3]);
+        } else {
 #pragma unroll
           for (int k = 0; k < 16; k++)
-            if (c0 + k < a.nocc) dst[c0 + k] = v[k];
+            if (c0 + k < a.nocc) o[k] = first ? v[k] : o[k] + v[k];
+        }
       }
       fence_before();
       __syncthreads();
