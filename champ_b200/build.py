@@ -13,7 +13,7 @@ from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-UNITS = ["host.cu", "inst_f32.cu", "inst_f64.cu"]
+UNITS = ["host.cu"] + [f"inst_{t}_n{n}.cu" for t in ("f32", "f64") for n in (0, 4, 5)]
 DEPS = [os.path.join(HERE, "..", "include", "champ_b200.h")] + glob.glob(os.path.join(CSRC, "*"))
 LIB = os.path.join(HERE, "libchamp_b200.so")
 OBJDIR = os.path.join(HERE, "_build")

@@ -29,6 +29,14 @@ struct MultiDet {
 // shared memory inside the fused kernels (keeps >= 16 warps per SM).
 constexpr size_t RESIDENT_LIMIT = 12 * 1024;
 
+// Launch configuration of the kernels of one compute type: per-warp shared-memory layout,
+// dynamic shared memory per block and warps (walkers) per block.
+struct KCfg {
+  Layout lay{};
+  size_t smem = 0;
+  int wpb = 4;
+};
+
 struct champ_ctx {
   int prec = 0;
   cudaStream_t stream = nullptr;
@@ -36,6 +44,12 @@ struct champ_ctx {
   int N = 0, nup = 0, ndn = 0, C = 0, nct = 0, nshell = 0, nbasis = 0, nmax = 0, nordc = 0, nloc = 0;
   int nomax = 1;
   MultiDet md;
+  // numerical radial tables (kind-2 shells), prepared at create: per table (grid, points, first
+  // value index, 0), 10 parameters (r0, h, log h, c0..c4, a0, ak), values and spline second
+  // derivatives of all tables one after another; shell -> table
+  std::vector<int4> rad_tab;
+  std::vector<double> rad_par, rad_y, rad_y2;
+  std::vector<int> rad_shell;
   std::vector<void *> allocs;
   Sys<double> sd;
   Sys<float> sf;
@@ -43,9 +57,7 @@ struct champ_ctx {
   State<float> stf;
   double rot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
   bool have_walkers = false;
-  int wpb = 4;
-  size_t smem = 0;
-  Layout lay;
+  KCfg kf, kd;  // FP32 and FP64 kernels (a mixed-precision context uses both)
   // device staging for per-call host arrays
   double *d_in = nullptr, *d_out = nullptr;
   uint8_t *d_mask = nullptr;
@@ -120,7 +132,12 @@ inline State<double> &st2of<double>(champ_ctx *c) { return c->std2; }
 template <>
 inline State<float> &st2of<float>(champ_ctx *c) { return c->stf2; }
 
-inline int nblocks(champ_ctx *c) { return (c->W + c->wpb - 1) / c->wpb; }
+template <class T>
+inline KCfg &kcfg(champ_ctx *c);
+template <>
+inline KCfg &kcfg<double>(champ_ctx *c) { return c->kd; }
+template <>
+inline KCfg &kcfg<float>(champ_ctx *c) { return c->kf; }
 
 enum class Op { Eval, EvalOut, Propose, ProposeGrad, Accept, Vmc, PGrad, DmcMove, DmcCopy };
 struct OpArgs {
@@ -135,11 +152,48 @@ struct OpArgs {
   int istep = 0;
   const void *st_override = nullptr;  // State<T> to use instead of the context's (and its walker count)
   int nw_override = 0;
+  int phase = -1;  // Vmc: one k_vmc launch of this phase (no statistics reset); DmcMove: k_dmc_move phase
 };
 
 
-// per-precision kernel launchers (inst_f32.cu, inst_f64.cu)
-int launch_f32(champ_ctx *c, Op op, const OpArgs &a);
-int launch_f64(champ_ctx *c, Op op, const OpArgs &a);
-int attrs_f32(champ_ctx *c);
-int attrs_f64(champ_ctx *c);
+// kernel launchers per (compute type, e-e-n order), one translation unit each (inst_*.cu)
+#define CHAMP_DECL(TAG, NORD)                                    \
+  int launch_##TAG##_n##NORD(champ_ctx *c, Op op, const OpArgs &a); \
+  int attrs_##TAG##_n##NORD(champ_ctx *c);
+CHAMP_DECL(f32, 0) CHAMP_DECL(f32, 4) CHAMP_DECL(f32, 5)
+CHAMP_DECL(f64, 0) CHAMP_DECL(f64, 4) CHAMP_DECL(f64, 5)
+#undef CHAMP_DECL
+
+int champ_fail(int code, const std::string &msg);
+inline int launch_f32(champ_ctx *c, Op op, const OpArgs &a) {
+  switch (c->nordc) {
+  case 0: case 1: return launch_f32_n0(c, op, a);
+  case 4: return launch_f32_n4(c, op, a);
+  case 5: return launch_f32_n5(c, op, a);
+  default: return champ_fail(CHAMP_EINVAL, "nordc must be 0, 1, 4 or 5");
+  }
+}
+inline int launch_f64(champ_ctx *c, Op op, const OpArgs &a) {
+  switch (c->nordc) {
+  case 0: case 1: return launch_f64_n0(c, op, a);
+  case 4: return launch_f64_n4(c, op, a);
+  case 5: return launch_f64_n5(c, op, a);
+  default: return champ_fail(CHAMP_EINVAL, "nordc must be 0, 1, 4 or 5");
+  }
+}
+inline int attrs_f32(champ_ctx *c) {
+  switch (c->nordc) {
+  case 0: case 1: return attrs_f32_n0(c);
+  case 4: return attrs_f32_n4(c);
+  case 5: return attrs_f32_n5(c);
+  default: return champ_fail(CHAMP_EINVAL, "nordc must be 0, 1, 4 or 5");
+  }
+}
+inline int attrs_f64(champ_ctx *c) {
+  switch (c->nordc) {
+  case 0: case 1: return attrs_f64_n0(c);
+  case 4: return attrs_f64_n4(c);
+  case 5: return attrs_f64_n5(c);
+  default: return champ_fail(CHAMP_EINVAL, "nordc must be 0, 1, 4 or 5");
+  }
+}

@@ -15,7 +15,7 @@ constexpr int MAXORD = 8;    // norda, nordb <= 7
 constexpr int MAXT = 24;     // e-e-n terms (nordc <= 5)
 constexpr int MG = 4;        // Gaussian terms per pseudopotential channel
 constexpr int MAXLCH = 5;    // pseudopotential channels
-constexpr int MAXQ = 12;     // quadrature points
+constexpr int MAXQ = 86;     // quadrature points (rules of 4 ... 86 points)
 constexpr double HB = 0.5;   // hbar^2 / 2m
 
 // ---------------------------------------------------------------------------------------
@@ -55,6 +55,13 @@ struct Sys {
   const int *cshell0;   // [C+1] first shell of each centre (shells grouped by centre)
   int nshc;             // most shells on one centre; 0 when shells are not grouped by centre
   const T *pz, *pc;     // primitive exponent, normalised weight
+  // numerical radial tables (shell kind 2): per table (grid type, points, first value, 0) and
+  // (r0, h, log h, small-r polynomial c0..c4, large-r a0, ak); per point the value and its
+  // spline second derivative
+  const int *shrad;     // [nshell] table of a kind-2 shell
+  const int4 *rtab;     // [nrad]
+  const double *rpar;   // [nrad][10]
+  const T *ry, *ry2;    // [sum nr]
   // occupied orbitals of each spin: det-0 (reference) orbitals in column order, then the
   // other orbitals any determinant of that spin uses ("virtuals"), ascending
   int nocc[2], nvirt[2], nomax, nvmax;
@@ -245,11 +252,75 @@ __device__ __forceinline__ void solid_all(int l, T x, T y, T z, T *S, T (*G)[3])
   }
 }
 
+// Numerical radial function f, f', f'' of table t at r (splfit_bas, qmc/vmc/splfit.f90): the
+// grid interval from the grid's closed form, cubic-spline interpolation inside the grid, the
+// small-r polynomial below its first point and the exponential beyond its last.
+template <class T, bool DERIV>
+__device__ __forceinline__ void table_radial(const Sys<T> &s, int t, T r, T *R) {
+  const int4 tb = s.rtab[t];
+  const double *p = s.rpar + 10 * t;
+  const T r0 = (T)p[0], h = (T)p[1], lh = (T)p[2];
+  int jx;
+  T ref0, ref1;
+  if (tb.x == 1) {
+    jx = (int)((r - r0) / h + T(1));
+    ref0 = r0 + h * T(jx - 1);
+    ref1 = ref0 + h;
+  } else if (tb.x == 2) {
+    const T xr = log(r / r0) / lh + T(1);
+    jx = xr < T(1) ? 0 : (int)xr;
+    ref0 = r0 * pow(h, T(jx - 1));
+    ref1 = ref0 * h;
+  } else {
+    jx = (int)(log((r + r0) / r0) / lh + T(1));
+    ref0 = r0 * pow(h, T(jx - 1)) - r0;
+    ref1 = (ref0 + r0) * h - r0;
+  }
+  if (jx < 1) {
+    R[0] = (T)p[3];
+    T rp = T(1);
+    for (int i = 1; i < 5; i++) { rp *= r; R[0] += (T)p[3 + i] * rp; }
+    if (DERIV) {
+      R[1] = R[2] = T(0);
+      T pm2 = T(0), pm1 = T(1);  // r^(i-2), r^(i-1)
+      for (int i = 1; i < 5; i++) {
+        R[1] += T(i) * (T)p[3 + i] * pm1;
+        R[2] += T(i * (i - 1)) * (T)p[3 + i] * pm2;
+        pm2 = pm1;
+        pm1 *= r;
+      }
+    }
+  } else if (jx >= tb.y) {
+    const T ak = (T)p[9];
+    R[0] = (T)p[8] * exp(-ak * r);
+    if (DERIV) {
+      R[1] = -ak * R[0];
+      R[2] = -ak * R[1];
+    }
+  } else {
+    const T *y = s.ry + tb.z + (jx - 1), *y2 = s.ry2 + tb.z + (jx - 1);
+    const T delh = ref1 - ref0, bb = (r - ref0) / delh, aa = (ref1 - r) / delh;
+    const T cc = aa * (aa * aa - T(1)) * delh * delh / T(6), dd = bb * (bb * bb - T(1)) * delh * delh / T(6);
+    R[0] = aa * y[0] + bb * y[1] + cc * y2[0] + dd * y2[1];
+    if (DERIV) {
+      R[1] = (y[1] - y[0]) / delh + (-(T(3) * aa * aa - T(1)) * y2[0] + (T(3) * bb * bb - T(1)) * y2[1]) * delh / T(6);
+      R[2] = aa * y2[0] + bb * y2[1];
+    }
+  }
+}
+
 // Radial function R, R', R'' of one shell at distance r (wfv(1..3), basis_fns.f90:118-157).
 template <class T, bool DERIV>
 __device__ __forceinline__ void shell_radial(const Sys<T> &s, int ish, T r, T *R) {
   int4 sh = s.shell[ish];
   int2 pr = s.shprim[ish];
+  if (sh.w == 2) {
+    table_radial<T, DERIV>(s, s.shrad[ish], r, R);
+    const T w = s.pc[pr.x];
+    R[0] *= w;
+    if (DERIV) { R[1] *= w; R[2] *= w; }
+    return;
+  }
   int n = sh.y;
   T rn = T(n);
   T rm1 = ipow(r, n - 1);

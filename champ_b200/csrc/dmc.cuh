@@ -37,8 +37,11 @@ __device__ __forceinline__ void avg_drift(const double *g, double tau, double a,
   vb[0] = f * g[0]; vb[1] = f * g[1]; vb[2] = f * g[2];
 }
 
+// phase 0: moves, E_L and reweighting in one pass; 1: the moves only; 2: E_L (from the positions,
+// re-inverting, refreshing the FP32 move tables when the state has them) and reweighting only --
+// the FP32 and FP64 halves of a mixed-precision step.
 template <class T, int NORD, bool MD>
-__global__ void __launch_bounds__(128, 4) k_dmc_move(Sys<T> s, State<T> st, Layout L, DmcPar P, DmcData D) {
+__global__ void __launch_bounds__(128, 4) k_dmc_move(Sys<T> s, State<T> st, Layout L, DmcPar P, DmcData D, int phase) {
   __shared__ JasPar<T> J;
   __shared__ EcpPar E;
   extern __shared__ __align__(16) char dsm[];
@@ -49,14 +52,14 @@ __global__ void __launch_bounds__(128, 4) k_dmc_move(Sys<T> s, State<T> st, Layo
   const uint64_t step = (uint64_t)D.ctr[0];
   for (int w = blockIdx.x * wpb + wib; w < W; w += gridDim.x * wpb) {
     View<T> v = make_view<T>(dsm + L.bytes * wib, L, st, w, s.N, s.C, s.nbasis, s.nomax, L.resident != 0);
-    if (L.resident) {
+    if (L.resident && phase != 2) {
       view_load(v, st, w, N, s.C, lane);
     } else {
       for (int i = lane; i < 3 * N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * N + i];
       __syncwarp();
     }
     int acc = 0;
-    for (int e = 0; e < N; e++) {
+    for (int e = 0; e < N && phase != 2; e++) {
       double xo[3] = {v.xs[3 * e], v.xs[3 * e + 1], v.xs[3 * e + 2]};
       double r0, d0, go[3], gn[3], vo[3], vn[3];
       propose<T, NORD, MD, true>(s, J, st, w, v, e, xo, lane, r0, d0, go);  // grad at the current position
@@ -77,11 +80,22 @@ __global__ void __launch_bounds__(128, 4) k_dmc_move(Sys<T> s, State<T> st, Layo
         acc++;
       }
     }
+    if (phase == 1) {
+      if (L.resident) view_store(v, st, w, N, s.C, lane);
+      else {
+        for (int i = lane; i < 3 * N; i += 32) st.x[(size_t)w * 3 * N + i] = v.xs[i];
+        __syncwarp();
+      }
+      continue;
+    }
     double R[9];
     random_rotation(P.seed, (uint32_t)w, step, R);
     EvalRes res;
     full_eval<T, NORD, MD>(s, J, E, st, w, v, R, lane, false, res);
-    if (L.resident) view_store(v, st, w, N, s.C, lane);
+    if (phase == 2) {
+      if (L.resident) eval_store(v, st, w, N, s.C, lane);
+      else mirror_store(v, st, w, N, s.C, lane);
+    } else if (L.resident) view_store(v, st, w, N, s.C, lane);
     else {
       for (int i = lane; i < 3 * N; i += 32) st.x[(size_t)w * 3 * N + i] = v.xs[i];
       __syncwarp();

@@ -161,6 +161,216 @@ static double host_anorm(int kind, int n, int l, double z) {
   return std::sqrt(2 * std::pow(2 * z, n + 0.5) * (2 * l + 1) / (g * 4 * pi));
 }
 
+// Numerical radial tables (read_bas_num.f90:213-378, spline2.f90): per table the grid
+// parameters as splfit_bas uses them, a 5-point polynomial through the first grid points (its
+// slope at the first point is the spline's left end condition), an exponential a0 exp(-ak r)
+// matched at the last points (its slope is the right end condition), and the spline's second
+// derivatives.  Grid 3 reads the last point as r0 and derives r0 = r_last / (h^(nr-1) - 1).
+static int build_radial_tables(const champ_system *d, champ_ctx *c) {
+  c->rad_tab.clear(); c->rad_par.clear(); c->rad_y.clear(); c->rad_y2.clear();
+  c->rad_shell.assign(d->nshell, -1);
+  bool any = false;
+  for (int i = 0; i < d->nshell; i++)
+    if (d->shell_kind[i] == 2) {
+      if (d->nrad < 1 || !d->shell_rad || d->shell_rad[i] < 0 || d->shell_rad[i] >= d->nrad)
+        return fail(CHAMP_EINVAL, "numerical shell without a valid radial table");
+      if (d->shell_nprim[i] != 1) return fail(CHAMP_EINVAL, "a numerical shell has exactly one primitive");
+      c->rad_shell[i] = d->shell_rad[i];
+      any = true;
+    }
+  if (!any) return CHAMP_OK;
+  if (!d->rad_igrid || !d->rad_nr || !d->rad_h || !d->rad_r0 || !d->rad_x || !d->rad_val)
+    return fail(CHAMP_EINVAL, "numerical radial tables: null array");
+  size_t off = 0;
+  for (int t = 0; t < d->nrad; t++) {
+    const int g = d->rad_igrid[t], nr = d->rad_nr[t];
+    if (g < 1 || g > 3) return fail(CHAMP_EINVAL, "radial grid type must be 1, 2 or 3");
+    if (nr < 6) return fail(CHAMP_EINVAL, "a radial table needs at least 6 points");
+    const double *x = d->rad_x + off, *y = d->rad_val + off;
+    double h = d->rad_h[t], r0 = d->rad_r0[t];
+    if (g == 2 && h <= 1.0) h = x[1] / x[0];
+    if (g == 3) r0 = r0 / (std::pow(h, nr - 1) - 1.0);
+    if (g == 2 && (r0 <= 0.0 || h <= 0.0)) { r0 = x[0]; h = x[1] / x[0]; }
+    // small r: y = c0 + c1 r + ... + c4 r^4 through the first 5 points (Gauss-Jordan, pivoting)
+    double A[5][6];
+    for (int i = 0; i < 5; i++) {
+      double pw = 1.0;
+      for (int j = 0; j < 5; j++) { A[i][j] = pw; pw *= x[i]; }
+      A[i][5] = y[i];
+    }
+    for (int col = 0; col < 5; col++) {
+      int pv = col;
+      for (int i = col + 1; i < 5; i++)
+        if (std::fabs(A[i][col]) > std::fabs(A[pv][col])) pv = i;
+      if (A[pv][col] == 0.0) return fail(CHAMP_EINVAL, "radial table: singular small-r fit");
+      for (int j = 0; j < 6; j++) std::swap(A[col][j], A[pv][j]);
+      for (int i = 0; i < 5; i++) {
+        if (i == col) continue;
+        const double f = A[i][col] / A[col][col];
+        for (int j = col; j < 6; j++) A[i][j] -= f * A[col][j];
+      }
+    }
+    double ce[5];
+    for (int i = 0; i < 5; i++) ce[i] = A[i][5] / A[i][i];
+    double dwf1 = 0;
+    for (int i = 1; i < 5; i++) dwf1 += i * ce[i] * std::pow(x[0], i - 1);
+    // large r: a0 exp(-ak r) with ak from the last two points
+    double ae1 = 0, ae2 = 0, dwfn = 0;
+    const double wfm = 0.5 * (y[nr - 1] + y[nr - 2]), dwfm = (y[nr - 1] - y[nr - 2]) / (x[nr - 1] - x[nr - 2]);
+    if (std::fabs(wfm) > 1e-99) {
+      ae2 = (dwfm / wfm < 0) ? -dwfm / wfm : 0.1;
+      ae1 = y[nr - 1] * std::exp(ae2 * x[nr - 1]);
+      dwfn = -ae2 * y[nr - 1];
+    }
+    // cubic spline with those end slopes (tridiagonal solve)
+    std::vector<double> y2(nr), u(nr);
+    y2[0] = -0.5;
+    u[0] = (3.0 / (x[1] - x[0])) * ((y[1] - y[0]) / (x[1] - x[0]) - dwf1);
+    for (int i = 1; i < nr - 1; i++) {
+      const double sig = (x[i] - x[i - 1]) / (x[i + 1] - x[i - 1]), pp = sig * y2[i - 1] + 2.0;
+      y2[i] = (sig - 1.0) / pp;
+      u[i] = (6.0 * ((y[i + 1] - y[i]) / (x[i + 1] - x[i]) - (y[i] - y[i - 1]) / (x[i] - x[i - 1])) / (x[i + 1] - x[i - 1]) -
+              sig * u[i - 1]) / pp;
+    }
+    const double qn = 0.5, un = (3.0 / (x[nr - 1] - x[nr - 2])) * (dwfn - (y[nr - 1] - y[nr - 2]) / (x[nr - 1] - x[nr - 2]));
+    y2[nr - 1] = (un - qn * u[nr - 2]) / (qn * y2[nr - 2] + 1.0);
+    for (int k = nr - 2; k >= 0; k--) y2[k] = y2[k] * y2[k + 1] + u[k];
+    c->rad_tab.push_back(make_int4(g, nr, (int)c->rad_y.size(), 0));
+    const double par[10] = {r0, h, std::log(h), ce[0], ce[1], ce[2], ce[3], ce[4], ae1, ae2};
+    c->rad_par.insert(c->rad_par.end(), par, par + 10);
+    c->rad_y.insert(c->rad_y.end(), y, y + nr);
+    c->rad_y2.insert(c->rad_y2.end(), y2.begin(), y2.end());
+    off += nr;
+  }
+  return CHAMP_OK;
+}
+
+// Angular quadrature of the nonlocal integration (gesqua, qmc/vmc/rotqua.f90:1-618): the rule
+// with the number of points closest to nq among 4, 6, 12, 18, 26, 32, 50, 24, 20, 86 (ties go to
+// the first listed), points on the unit sphere and weights summing to one.  Returns the points.
+static int quadrature_rule(int nq_in, double (*q)[3], double *w) {
+  static const int iq[10] = {4, 6, 12, 18, 26, 32, 50, 24, 20, 86};
+  int icase = 0;
+  for (int i = 1; i < 10; i++)
+    if (std::abs(nq_in - iq[i]) < std::abs(nq_in - iq[icase])) icase = i;
+  const int nq = iq[icase];
+  for (int j = 0; j < MAXQ; j++) q[j][0] = q[j][1] = q[j][2] = w[j] = 0.0;
+  // weights per point type (rows: rule; columns: point type), then the types' point counts
+  double ww[10][6] = {{0}};
+  ww[0][0] = 1.0 / 4; ww[1][0] = 1.0 / 6; ww[2][0] = 1.0 / 12; ww[3][0] = 1.0 / 30; ww[4][0] = 1.0 / 21;
+  ww[5][0] = 5.0 / 168; ww[6][0] = 4.0 / 315; ww[2][1] = 1.0 / 12; ww[3][1] = 1.0 / 15; ww[4][1] = 4.0 / 105;
+  ww[5][1] = 5.0 / 168; ww[6][1] = 64.0 / 2835; ww[4][2] = 27.0 / 840; ww[5][2] = 27.0 / 840;
+  ww[6][2] = 27.0 / 1280; ww[6][3] = 14641.0 / 725760; ww[7][0] = 1.0 / 24; ww[8][0] = 1.0 / 20;
+  ww[9][0] = .0115440115441; ww[9][2] = .0119439090859; ww[9][3] = .0111105557106; ww[9][4] = .0118765012945;
+  ww[9][5] = .0118123037469;
+  static const int octa[6] = {6, 12, 8, 24, 0, 0}, icosa[6] = {2, 10, 20, 0, 0, 0}, tetr[6] = {4, 0, 0, 0, 0, 0},
+                   n24[6] = {24, 0, 0, 0, 0, 0}, n20[6] = {20, 0, 0, 0, 0, 0}, n86[6] = {6, 0, 8, 24, 24, 24};
+  const int *cnt = nq == 4 ? tetr : (nq == 12 || nq == 32) ? icosa : nq == 20 ? n20 : nq == 24 ? n24 : nq == 86 ? n86 : octa;
+  for (int k = 0, jj = 0; k < (nq == 86 ? 6 : 4); k++)
+    for (int j = 0; j < cnt[k]; j++, jj++)
+      if (jj < nq) w[jj] = ww[icase][k];
+  const double p = 1.0 / std::sqrt(2.0), qq = 1.0 / std::sqrt(3.0), r = 1.0 / std::sqrt(11.0), sv = 3.0 / std::sqrt(11.0);
+  const double pi = 3.14159265359;
+  if (nq == 4) {  // tetrahedron
+    for (int j = 0; j < 4; j++) {
+      q[j][0] = j < 2 ? qq : -qq;
+      q[j][1] = (j == 1 || j == 3) ? -qq : qq;
+      q[j][2] = (j == 1 || j == 2) ? -qq : qq;
+    }
+  } else if (nq == 6 || nq == 18 || nq == 26 || nq == 50) {  // octahedral symmetry
+    int ip = 0, lp = 0;
+    for (int ii = 0; ii < 2; ii++) {
+      const double si = ii == 0 ? 1.0 : -1.0;
+      q[ii][0] = si; q[2 + ii][1] = si; q[4 + ii][2] = si;
+      if (nq <= 6) continue;
+      for (int jj = 0; jj < 2; jj++) {
+        const double sj = jj == 0 ? 1.0 : -1.0;
+        q[6 + ip][0] = si * p; q[6 + ip][1] = sj * p;
+        q[10 + ip][1] = si * p; q[10 + ip][2] = sj * p;
+        q[14 + ip][2] = si * p; q[14 + ip][0] = sj * p;
+        ip++;
+        if (nq <= 18) continue;
+        for (int kk = 0; kk < 2; kk++) {
+          const double sk = kk == 0 ? 1.0 : -1.0;
+          q[18 + lp][0] = si * qq; q[18 + lp][1] = sj * qq; q[18 + lp][2] = sk * qq;
+          if (nq > 26) {
+            q[26 + lp][0] = si * r; q[26 + lp][1] = sj * r; q[26 + lp][2] = sk * sv;
+            q[34 + lp][0] = si * r; q[34 + lp][1] = sj * sv; q[34 + lp][2] = sk * r;
+            q[42 + lp][0] = si * sv; q[42 + lp][1] = sj * r; q[42 + lp][2] = sk * r;
+          }
+          lp++;
+        }
+      }
+    }
+  } else if (nq == 12 || nq == 20 || nq == 32) {  // icosahedral symmetry
+    q[0][2] = 1.0;
+    q[1][2] = -1.0;
+    const double fi0 = pi / 5.0, s5 = std::sqrt(5.0), cstha = 1.0 / s5, sntha = 2.0 / s5;
+    const double den = std::sqrt(15.0 + 6.0 * s5), csth1 = (2.0 + s5) / den, snth1 = std::sqrt(1.0 - csth1 * csth1);
+    const double csth2 = 1.0 / den, snth2 = std::sqrt(1.0 - csth2 * csth2);
+    for (int j = 1; j <= 5; j++) {
+      const double rk2 = 2.0 * (j - 1), rk21 = rk2 + 1.0;
+      const double c2 = std::cos(rk2 * fi0), s2 = std::sin(rk2 * fi0), c21 = std::cos(rk21 * fi0), s21 = std::sin(rk21 * fi0);
+      if (nq != 20) {
+        q[j + 1][0] = sntha * c2; q[j + 1][1] = sntha * s2; q[j + 1][2] = cstha;
+        q[j + 6][0] = sntha * c21; q[j + 6][1] = sntha * s21; q[j + 6][2] = -cstha;
+      }
+      if (nq > 12) {
+        const int k0 = nq == 20 ? 0 : 12;
+        const int k1 = j + k0 - 1, k2 = j + k0 + 4, k3 = j + k0 + 9, k4 = j + k0 + 14;
+        q[k1][0] = snth1 * c21; q[k1][1] = snth1 * s21; q[k1][2] = csth1;
+        q[k2][0] = snth2 * c21; q[k2][1] = snth2 * s21; q[k2][2] = csth2;
+        q[k3][0] = snth1 * c2; q[k3][1] = snth1 * s2; q[k3][2] = -csth1;
+        q[k4][0] = snth2 * c2; q[k4][1] = snth2 * s2; q[k4][2] = -csth2;
+      }
+    }
+  } else if (nq == 24) {
+    int lq = 0;
+    double x = .8662468181078, y = .4225186537611, z = .2666354015167;
+    for (int l = 0; l < 3; l++) {
+      if (l == 1) { const double hold = y; y = x; x = z; z = hold; }
+      if (l == 2) { const double hold = z; z = y; y = x; x = hold; }
+      const double cp = std::cos(-pi / 2.0), sp = std::sin(-pi / 2.0);
+      const double u = cp * x - sp * z, v = y, ww2 = sp * x + cp * z;
+      for (int m = 0; m < 4; m++) {
+        const double fi = pi * m / 2.0, cf = std::cos(fi), sf = std::sin(fi);
+        q[lq][0] = x * cf - y * sf; q[lq][1] = x * sf + y * cf; q[lq][2] = z; lq++;
+        q[lq][0] = u * cf - v * sf; q[lq][1] = u * sf + v * cf; q[lq][2] = ww2; lq++;
+      }
+    }
+  } else {  // 86 points
+    const double pp = .927330657151, q2 = .374243039090, rl1 = .369602846454, sm1 = .852518311701,
+                 rl2 = .694354006603, sm2 = .189063552885;
+    int ip = 0, lp = 0;
+    for (int ii = 0; ii < 2; ii++) {
+      const double si = ii == 0 ? 1.0 : -1.0;
+      q[ii][0] = si; q[2 + ii][1] = si; q[4 + ii][2] = si;
+      for (int jj = 0; jj < 2; jj++) {
+        const double sj = jj == 0 ? 1.0 : -1.0;
+        q[62 + ip][0] = si * pp; q[62 + ip][1] = sj * q2;
+        q[66 + ip][0] = si * pp; q[66 + ip][2] = sj * q2;
+        q[70 + ip][1] = si * pp; q[70 + ip][2] = sj * q2;
+        q[74 + ip][0] = si * q2; q[74 + ip][1] = sj * pp;
+        q[78 + ip][0] = si * q2; q[78 + ip][2] = sj * pp;
+        q[82 + ip][1] = si * q2; q[82 + ip][2] = sj * pp;
+        ip++;
+        for (int kk = 0; kk < 2; kk++) {
+          const double sk = kk == 0 ? 1.0 : -1.0;
+          q[6 + lp][0] = si * qq; q[6 + lp][1] = sj * qq; q[6 + lp][2] = sk * qq;
+          q[14 + lp][0] = si * rl1; q[14 + lp][1] = sj * rl1; q[14 + lp][2] = sk * sm1;
+          q[22 + lp][0] = si * rl1; q[22 + lp][1] = sj * sm1; q[22 + lp][2] = sk * rl1;
+          q[30 + lp][0] = si * sm1; q[30 + lp][1] = sj * rl1; q[30 + lp][2] = sk * rl1;
+          q[38 + lp][0] = si * rl2; q[38 + lp][1] = sj * rl2; q[38 + lp][2] = sk * sm2;
+          q[46 + lp][0] = si * rl2; q[46 + lp][1] = sj * sm2; q[46 + lp][2] = sk * rl2;
+          q[54 + lp][0] = si * sm2; q[54 + lp][1] = sj * rl2; q[54 + lp][2] = sk * rl2;
+          lp++;
+        }
+      }
+    }
+  }
+  return nq;
+}
+
 // cuspinit4 + cuspexact4 (qmc/fit/cuspinit4.f90:1-60, qmc/fit/cuspexact4.f90:14-40)
 static void host_een_cusp(int nordc, int nct, int nt, std::vector<double> &c, std::vector<int> *dependents = nullptr) {
   if (nordc <= 1) return;
@@ -406,6 +616,24 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
   CK(cudaMemcpy(ep, &ecp, sizeof ecp, cudaMemcpyHostToDevice));
   s.cent = cent; s.ctype = ctype; s.zc = zc; s.shell = sh; s.shprim = shp; s.shb0 = shb0;
   s.pz = pz; s.pc = pc; s.cocc[0] = cr0; s.cocc[1] = cr1; s.coccT[0] = ct0; s.coccT[1] = ct1; s.jas = jp; s.ecp = ep;
+  {
+    // numerical radial tables (kind-2 shells)
+    const size_t nt = c->rad_tab.size(), ny = c->rad_y.size();
+    int *shr = dalloc<int>(c, c->nshell);
+    int4 *rt = dalloc<int4>(c, std::max<size_t>(nt, 1));
+    double *rp = dalloc<double>(c, std::max<size_t>(10 * nt, 1));
+    T *ry = dalloc<T>(c, std::max<size_t>(ny, 1)), *ry2 = dalloc<T>(c, std::max<size_t>(ny, 1));
+    if (!shr || !rt || !rp || !ry || !ry2) return fail(CHAMP_ENOMEM, "device allocation of the radial tables failed");
+    CK(cudaMemcpy(shr, c->rad_shell.data(), sizeof(int) * c->nshell, cudaMemcpyHostToDevice));
+    if (nt) {
+      std::vector<T> yv(c->rad_y.begin(), c->rad_y.end()), y2v(c->rad_y2.begin(), c->rad_y2.end());
+      CK(cudaMemcpy(rt, c->rad_tab.data(), sizeof(int4) * nt, cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(rp, c->rad_par.data(), sizeof(double) * 10 * nt, cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(ry, yv.data(), sizeof(T) * ny, cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(ry2, y2v.data(), sizeof(T) * ny, cudaMemcpyHostToDevice));
+    }
+    s.shrad = shr; s.rtab = rt; s.rpar = rp; s.ry = ry; s.ry2 = ry2;
+  }
   return CHAMP_OK;
 }
 
@@ -448,8 +676,81 @@ static int build_state(champ_ctx *c, State<T> &st) {
   return CHAMP_OK;
 }
 
+// Mixed precision: the FP32 state of the single-electron moves shares every FP64 buffer with the
+// FP64 state (positions, inverses, log-det, determinant tables, outputs, statistics) and owns
+// only the FP32 Jastrow pair table, distances and power sums, which every FP64 full evaluation
+// refreshes (State::m_fso, m_ren, m_zq).
+static void link_move_state(State<double> &d, State<float> &f) {
+  float *fso = f.fso, *ren = f.ren, *zq = f.zq, *pf = f.pf;
+  f.W = d.W;
+  f.x = d.x; f.ainv = d.ainv; f.fsum = d.fsum; f.lnd = d.lnd; f.sgn = d.sgn; f.status = d.status;
+  f.pa = d.pa; f.pdj = d.pdj; f.prho = d.prho; f.pxn = d.pxn; f.piel = d.piel;
+  f.orb5 = nullptr; f.gproj = nullptr; f.nlt = nullptr;
+  f.tv = d.tv; f.gam = d.gam; f.ymd = d.ymd; f.wdet = d.wdet;
+  f.astride = d.astride; f.tvstride = d.tvstride; f.gstride = d.gstride; f.wstride = d.wstride;
+  f.o_lnpsi = d.o_lnpsi; f.o_sign = d.o_sign; f.o_psij = d.o_psij; f.o_vel = d.o_vel; f.o_divv = d.o_divv;
+  f.o_d2 = d.o_d2; f.o_pe = d.o_pe; f.o_peee = d.o_peee; f.o_penl = d.o_penl; f.o_eloc = d.o_eloc;
+  f.s_esum = d.s_esum; f.s_e2sum = d.s_e2sum; f.s_acc = d.s_acc; f.s_elast = d.s_elast;
+  f.fso = fso; f.ren = ren; f.zq = zq; f.pf = pf;
+  f.m_fso = f.m_ren = f.m_zq = nullptr;
+  d.m_fso = fso; d.m_ren = ren; d.m_zq = zq;
+}
+
+static int build_move_state(champ_ctx *c, State<double> &d, State<float> &f) {
+  size_t W = c->wmax, N = c->N;
+  memset(&f, 0, sizeof f);
+  f.fso = dalloc<float>(c, W * N * N);
+  f.ren = dalloc<float>(c, W * N * c->C * 2);
+  f.zq = dalloc<float>(c, W * N * ZQ);
+  f.pf = dalloc<float>(c, W * N);
+  if (!f.fso || !f.ren || !f.zq || !f.pf) return fail(CHAMP_ENOMEM, "device allocation of the FP32 move tables failed");
+  link_move_state(d, f);
+  return CHAMP_OK;
+}
+
 static int launch(champ_ctx *c, Op op, const OpArgs &a = OpArgs()) {
-  return c->prec == CHAMP_PREC_FP64 ? launch_f64(c, op, a) : launch_f32(c, op, a);
+  if (c->prec == CHAMP_PREC_FP64) return launch_f64(c, op, a);
+  if (c->prec == CHAMP_PREC_FP32) return launch_f32(c, op, a);
+  // mixed precision: moves on the FP32 instantiation, full evaluations on the FP64 one
+  switch (op) {
+  case Op::Eval:
+  case Op::EvalOut:
+  case Op::PGrad:
+    return launch_f64(c, op, a);
+  case Op::Propose:
+  case Op::ProposeGrad:
+  case Op::Accept:
+  case Op::DmcCopy:
+    return launch_f32(c, op, a);
+  case Op::DmcMove: {
+    OpArgs b = a;
+    b.phase = 1;
+    int rc = launch_f32(c, op, b);
+    if (rc) return rc;
+    b.phase = 2;
+    return launch_f64(c, op, b);
+  }
+  case Op::Vmc: {
+    if (a.phase >= 0) return fail(CHAMP_EINVAL, "internal: explicit VMC phase on a mixed context");
+    const State<double> &st = c->std_;
+    CK(cudaMemsetAsync(st.s_esum, 0, sizeof(double) * c->W, c->stream));
+    CK(cudaMemsetAsync(st.s_e2sum, 0, sizeof(double) * c->W, c->stream));
+    CK(cudaMemsetAsync(st.s_acc, 0, sizeof(double) * c->W, c->stream));
+    OpArgs b = a;
+    b.nsweep = 1;
+    for (int isw = 0; isw < a.nsweep; isw++) {
+      b.sweep0 = a.sweep0 + (uint64_t)isw;
+      b.phase = 1;  // the sweep's moves, FP32
+      int rc = launch_f32(c, op, b);
+      if (rc) return rc;
+      b.phase = 3;  // its E_L, FP64 from the positions
+      rc = launch_f64(c, op, b);
+      if (rc) return rc;
+    }
+    return CHAMP_OK;
+  }
+  }
+  return fail(CHAMP_EINVAL, "internal: unknown operation");
 }
 // ---------------------------------------------------------------------------------------
 // C ABI
@@ -576,6 +877,7 @@ static size_t noalloc_carve(const champ_ctx *c, const State<T> &ref, int nw, cha
   st.o_peee = (double *)take(sizeof(double) * W);
   st.o_penl = (double *)take(sizeof(double) * W);
   st.o_eloc = eloc;  // written straight into the caller's buffer
+  st.m_fso = st.m_ren = st.m_zq = nullptr;  // the context's own move tables stay untouched
   return o <= NOALLOC_BYTES ? o : 0;
 }
 
@@ -623,7 +925,7 @@ static int tc_setup(champ_ctx *c) {
   int dev = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev));
-  if (c->prec != CHAMP_PREC_MIXED || c->lay.resident) return CHAMP_OK;
+  if (c->prec != CHAMP_PREC_FP32 || c->kf.lay.resident) return CHAMP_OK;
   if (std::max(c->md.nocc[0], c->md.nocc[1]) < 16) return CHAMP_OK;
   const int B = c->nbasis, Kp = (B + orbtc::BK - 1) / orbtc::BK * orbtc::BK;
   c->tc_Kp = Kp;
@@ -775,12 +1077,19 @@ static int cublas_handle(champ_ctx *c) {
   return CHAMP_OK;
 }
 
+// Reports (once) a tensor-core orbital contraction that gave up waiting for its MMA groups since
+// the last check, and clears the flag.  Synchronises the stream when the contraction is in use.
 static int tc_check(champ_ctx *c) {
-  if (!c->tc_err) return CHAMP_OK;
+  if (!c->tc_err || !c->tc_on) return CHAMP_OK;
   int h = 0;
   CK(cudaMemcpyAsync(&h, c->tc_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  if (h) return fail(CHAMP_ECUDA, "tensor-core orbital contraction gave up waiting for its MMA groups");
+  if (h) {
+    CK(cudaMemsetAsync(c->tc_err, 0, sizeof(int), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return fail(CHAMP_ECUDA, "tensor-core orbital contraction gave up waiting for its MMA groups; the orbitals, "
+                             "and the energies of the call that reported it, are not valid");
+  }
   return CHAMP_OK;
 }
 
@@ -801,11 +1110,14 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
   if (d->norda > MAXORD - 1 || d->nordb > MAXORD - 1) return fail(CHAMP_EINVAL, "norda/nordb > 7");
   if (!(d->nordc == 0 || d->nordc == 1 || d->nordc == 4 || d->nordc == 5)) return fail(CHAMP_EINVAL, "nordc must be 0, 1, 4 or 5");
   if (d->nloc != 0 && d->nloc != 6) return fail(CHAMP_EINVAL, "nloc must be 0 or 6");
-  if (d->nloc == 6 && d->nquad != 12) return fail(CHAMP_EINVAL, "nquad must be 12");
+  if (d->nloc == 6 && (d->nquad < 1 || d->nquad > 1000)) return fail(CHAMP_EINVAL, "nquad out of range");
   if (d->nloc == 6 && d->mgauss > MG) return fail(CHAMP_EINVAL, "more than 4 Gaussian terms per channel");
-  if (precision != CHAMP_PREC_FP64 && precision != CHAMP_PREC_MIXED) return fail(CHAMP_EINVAL, "bad precision");
-  for (int i = 0; i < d->nshell; i++)
+  if (precision != CHAMP_PREC_FP64 && precision != CHAMP_PREC_MIXED && precision != CHAMP_PREC_FP32)
+    return fail(CHAMP_EINVAL, "bad precision");
+  for (int i = 0; i < d->nshell; i++) {
     if (d->shell_l[i] < 0 || d->shell_l[i] > CHAMP_MAX_L || d->shell_n[i] < 1) return fail(CHAMP_EINVAL, "shell with bad n or l");
+    if (d->shell_kind[i] < 0 || d->shell_kind[i] > 2) return fail(CHAMP_EINVAL, "shell kind must be 0, 1 or 2");
+  }
   champ_ctx *c = new champ_ctx();
   c->prec = precision;
   c->stream = (cudaStream_t)stream;
@@ -854,11 +1166,18 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
     c->ncsfp = c->md.multidet && d->ncsf > 1 ? d->ncsf - 1 : 0;
     if (c->nomax > 256) { delete c; return fail(CHAMP_EINVAL, "more than 256 occupied orbitals of one spin"); }
   }
-  // normalised primitive weights (basis_norm)
+  // normalised primitive weights (basis_norm; numerical radial functions take the angular factor
+  // sqrt((2l+1)/4pi) only, basis_norm.f90:57-58)
   std::vector<double> pcn;
   for (int i = 0, p = 0; i < d->nshell; i++)
     for (int q = 0; q < d->shell_nprim[i]; q++, p++)
-      pcn.push_back(d->prim_coef[p] * host_anorm(d->shell_kind[i], d->shell_n[i], d->shell_l[i], d->prim_zeta[p]));
+      pcn.push_back(d->prim_coef[p] * (d->shell_kind[i] == 2
+                                           ? std::sqrt((2 * d->shell_l[i] + 1) / (4 * 3.141592653589793))
+                                           : host_anorm(d->shell_kind[i], d->shell_n[i], d->shell_l[i], d->prim_zeta[p])));
+  {
+    int rc0 = build_radial_tables(d, c);
+    if (rc0) { delete c; return rc0; }
+  }
   // e-e-n coefficients with the cusp conditions applied
   int nt = 0;
   for (int n = 2; n <= d->nordc; n++)
@@ -912,7 +1231,6 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
   // pseudopotential and quadrature (rotqua.f90 icosahedral rule)
   EcpPar ecp;
   memset(&ecp, 0, sizeof ecp);
-  ecp.nquad = 12;
   for (int it = 0; it < d->nctype; it++) ecp.znuc[it] = d->znuc[it];
   if (d->nloc == 6) {
     for (int it = 0; it < d->nctype; it++) {
@@ -935,17 +1253,7 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
       }
     }
   }
-  {
-    const double pi = 3.141592653589793, zr = 1.0 / std::sqrt(5.0), rr = 2.0 / std::sqrt(5.0);
-    ecp.q0[0][0] = 0; ecp.q0[0][1] = 0; ecp.q0[0][2] = 1;
-    ecp.q0[1][0] = 0; ecp.q0[1][1] = 0; ecp.q0[1][2] = -1;
-    for (int k = 0; k < 5; k++) {
-      double a = 2 * pi * k / 5.0, b = a + pi / 5.0;
-      ecp.q0[2 + k][0] = rr * std::cos(a); ecp.q0[2 + k][1] = rr * std::sin(a); ecp.q0[2 + k][2] = zr;
-      ecp.q0[7 + k][0] = rr * std::cos(b); ecp.q0[7 + k][1] = rr * std::sin(b); ecp.q0[7 + k][2] = -zr;
-    }
-    for (int k = 0; k < 12; k++) ecp.wq[k] = 1.0 / 12.0;
-  }
+  ecp.nquad = quadrature_rule(d->nloc == 6 ? d->nquad : 12, ecp.q0, ecp.wq);
   double pecent = 0;
   for (int i = 0; i < d->ncent; i++)
     for (int j = 0; j < i; j++) {
@@ -953,40 +1261,51 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
              dz = d->cent[3 * i + 2] - d->cent[3 * j + 2];
       pecent += d->znuc[d->iwctype[i]] * d->znuc[d->iwctype[j]] / std::sqrt(dx * dx + dy * dy + dz * dz);
     }
-  int rc;
-  if (precision == CHAMP_PREC_FP64) {
+  int rc = CHAMP_OK;
+  const bool use64 = precision != CHAMP_PREC_FP32, use32 = precision != CHAMP_PREC_FP64;
+  // warps per block: up to 4, keeping the block's dynamic shared memory under 96 KB
+  auto finish_cfg = [&](KCfg &k) -> int {
+    k.smem = k.lay.bytes;
+    k.wpb = 4;  // 128-thread blocks (the kernels' launch bounds)
+    while (k.wpb > 1 && k.smem * k.wpb > 96 * 1024) k.wpb >>= 1;
+    if (k.smem * k.wpb > 200 * 1024) return fail(CHAMP_EINVAL, "system too large for the per-warp shared memory");
+    k.smem *= k.wpb;
+    return CHAMP_OK;
+  };
+  if (use64) {
     rc = build_sys<double>(c, d, pcn, cfull, asa, asb, ecp, pecent, c->sd);
     if (!rc) rc = build_state<double>(c, c->std_);
-    c->lay = make_layout<double>(c->N, c->C, c->nbasis, c->nmax, c->nomax, c->std_.astride, c->std_.tvstride,
-                                 c->std_.gstride, c->std_.wstride, c->nloc > 0, RESIDENT_LIMIT);
-    c->smem = c->lay.bytes;
-  } else {
+    c->kd.lay = make_layout<double>(c->N, c->C, c->nbasis, c->nmax, c->nomax, c->std_.astride, c->std_.tvstride,
+                                    c->std_.gstride, c->std_.wstride, c->nloc > 0, RESIDENT_LIMIT);
+    if (!rc) rc = finish_cfg(c->kd);
+  }
+  if (use32 && !rc) {
     rc = build_sys<float>(c, d, pcn, cfull, asa, asb, ecp, pecent, c->sf);
-    if (!rc) rc = build_state<float>(c, c->stf);
-    c->lay = make_layout<float>(c->N, c->C, c->nbasis, c->nmax, c->nomax, c->stf.astride, c->stf.tvstride,
-                                c->stf.gstride, c->stf.wstride, c->nloc > 0, RESIDENT_LIMIT);
-    c->smem = c->lay.bytes;
+    if (!rc) rc = precision == CHAMP_PREC_MIXED ? build_move_state(c, c->std_, c->stf) : build_state<float>(c, c->stf);
+    // the mixed move kernels need no orbital, projection or quadrature scratch
+    c->kf.lay = make_layout<float>(c->N, c->C, c->nbasis, c->nmax, c->nomax, c->stf.astride, c->stf.tvstride,
+                                   c->stf.gstride, c->stf.wstride, c->nloc > 0 && precision == CHAMP_PREC_FP32,
+                                   RESIDENT_LIMIT);
+    if (!rc) rc = finish_cfg(c->kf);
   }
   if (rc) { champ_destroy(c); return rc; }
   c->nfree = c->ncsfp + c->norbp + c->nparm_jas;
-  // warps per block: up to 8, keeping the block's dynamic shared memory under 96 KB
-  c->wpb = 4;  // 128-thread blocks (the kernels' launch bounds)
-  while (c->wpb > 1 && c->smem * c->wpb > 96 * 1024) c->wpb >>= 1;
-  if (c->smem * c->wpb > 200 * 1024) { champ_destroy(c); return fail(CHAMP_EINVAL, "system too large for the per-warp shared memory"); }
-  c->smem *= c->wpb;
   {
-    // the derivative kernel adds its accumulators to the always-shared part of the layout
-    size_t pgb = c->lay.base + align16(sizeof(double) * (4 * (size_t)c->N + 3 * (size_t)c->np_raw +
-                                                         (size_t)c->N * c->np_raw));
+    // the derivative kernel (FP64 for FP64 and mixed contexts) adds its accumulators to the
+    // always-shared part of the layout
+    const Layout &lp = use64 ? c->kd.lay : c->kf.lay;
+    size_t pgb = lp.base + align16(sizeof(double) * (4 * (size_t)c->N + 3 * (size_t)c->np_raw +
+                                                     (size_t)c->N * c->np_raw));
     // per-lane NLPP parameter slots: always in FP32; in FP64 while the warp's share stays small
-    c->pg_lanesum = (c->prec == CHAMP_PREC_MIXED || pgb <= 24 * 1024) ? 1 : 0;
+    c->pg_lanesum = (c->prec == CHAMP_PREC_FP32 || pgb <= 24 * 1024) ? 1 : 0;
     if (c->pg_lanesum) pgb += align16(sizeof(double) * 32 * (size_t)c->np_raw);
     c->wpb_pg = 4;
     while (c->wpb_pg > 1 && pgb * c->wpb_pg > 160 * 1024) c->wpb_pg >>= 1;
     c->smem_pg = pgb * c->wpb_pg;
     if (c->smem_pg > 220 * 1024) c->smem_pg = 0;  // parameter derivatives unavailable for this size
   }
-  rc = c->prec == CHAMP_PREC_FP64 ? attrs_f64(c) : attrs_f32(c);
+  if (use64) rc = attrs_f64(c);
+  if (use32 && !rc) rc = attrs_f32(c);
   if (!rc) rc = tc_setup(c);
   c->reinv_every = std::max(1, (100 + c->N - 1) / c->N);  // about every 100 single-electron moves
   if (rc) { champ_destroy(c); return rc; }
@@ -1113,8 +1432,21 @@ int champ_dmc_init(champ_ctx *c, int32_t w_target, double tau, double gpop) {
   if (!c->have_walkers) return fail(CHAMP_ESTATE, "set the initial walkers first");
   if (w_target < 1 || tau <= 0 || gpop <= 0) return fail(CHAMP_EINVAL, "bad DMC parameters");
   if (!c->dmc_ready) {
-    int rc = c->prec == CHAMP_PREC_FP64 ? alloc_state_copy<double>(c, c->std_, c->std2)
-                                        : alloc_state_copy<float>(c, c->stf, c->stf2);
+    int rc;
+    if (c->prec == CHAMP_PREC_FP64) rc = alloc_state_copy<double>(c, c->std_, c->std2);
+    else if (c->prec == CHAMP_PREC_FP32) rc = alloc_state_copy<float>(c, c->stf, c->stf2);
+    else {
+      // the second buffer holds the FP32 move state; its FP64 twin shares the FP64 scratch
+      rc = alloc_state_copy<float>(c, c->stf, c->stf2);
+      if (!rc) {
+        c->std2 = c->std_;
+        State<double> &d2 = c->std2;
+        const State<float> &f2 = c->stf2;
+        d2.x = f2.x; d2.ainv = f2.ainv; d2.tv = f2.tv; d2.gam = f2.gam;
+        d2.fsum = f2.fsum; d2.lnd = f2.lnd; d2.sgn = f2.sgn;
+        d2.m_fso = f2.fso; d2.m_ren = f2.ren; d2.m_zq = f2.zq;
+      }
+    }
     if (rc) return rc;
     size_t W = c->wmax;
     int *nw = dalloc<int>(c, 1);
@@ -1150,7 +1482,7 @@ int champ_dmc_init(champ_ctx *c, int32_t w_target, double tau, double gpop) {
   // initial population: the current walkers, weight 1, with their local energies
   int rc = launch(c, Op::EvalOut);
   if (rc) return rc;
-  double *el = c->prec == CHAMP_PREC_FP64 ? c->std_.o_eloc : c->stf.o_eloc;
+  double *el = c->prec == CHAMP_PREC_FP32 ? c->stf.o_eloc : c->std_.o_eloc;
   std::vector<double> elh(c->W), one(c->W, 1.0);
   CK(cudaMemcpyAsync(elh.data(), el, sizeof(double) * c->W, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -1208,20 +1540,22 @@ int champ_nparam(const champ_ctx *c, int32_t *nj, int32_t *ncsf, int32_t *norb) 
   return CHAMP_OK;
 }
 
-static double *state_x(champ_ctx *c) { return c->prec == CHAMP_PREC_FP64 ? c->std_.x : c->stf.x; }
+// buffers that an FP64 or mixed context keeps in its FP64 state and an FP32 context in its FP32 one
+static State<double> *st64(champ_ctx *c) { return c->prec == CHAMP_PREC_FP32 ? nullptr : &c->std_; }
+static double *state_x(champ_ctx *c) { return st64(c) ? c->std_.x : c->stf.x; }
 
 int champ_set_walkers(champ_ctx *c, int32_t nw, const double *x) {
   if (!c || !x) return fail(CHAMP_EINVAL, "null argument");
   if (nw < 1 || nw > c->wmax) return fail(CHAMP_EINVAL, "nw out of range");
   c->W = nw;
   CK(cudaMemcpyAsync(state_x(c), x, sizeof(double) * nw * 3 * c->N, cudaMemcpyHostToDevice, c->stream));
-  int *piel = c->prec == CHAMP_PREC_FP64 ? c->std_.piel : c->stf.piel;
+  int *piel = st64(c) ? c->std_.piel : c->stf.piel;
   CK(cudaMemsetAsync(piel, 0xFF, sizeof(int) * nw, c->stream));
   int rc = launch(c, Op::Eval);
   if (rc) return rc;
   c->have_walkers = true;
   CK(cudaStreamSynchronize(c->stream));
-  return CHAMP_OK;
+  return tc_check(c);
 }
 
 int champ_get_walkers(champ_ctx *c, double *x) {
@@ -1246,11 +1580,11 @@ int champ_eval_full(champ_ctx *c, const champ_eval_out *o) {
   int rc = launch(c, Op::EvalOut);
   if (rc) return rc;
   if (o) {
-    rc = c->prec == CHAMP_PREC_FP64 ? copy_eval_out<double>(c, o) : copy_eval_out<float>(c, o);
+    rc = st64(c) ? copy_eval_out<double>(c, o) : copy_eval_out<float>(c, o);
     if (rc) return rc;
   }
   CK(cudaStreamSynchronize(c->stream));
-  return CHAMP_OK;
+  return tc_check(c);
 }
 
 int champ_propose_1e(champ_ctx *c, int32_t iel, const double *xnew, double *ratio, double *grad_new) {
@@ -1313,11 +1647,11 @@ int champ_vmc_sweeps(champ_ctx *c, int32_t nsweep, uint64_t seed, uint64_t sweep
   int rc = launch(c, Op::Vmc, a);
   if (rc) return rc;
   if (stats) {
-    rc = c->prec == CHAMP_PREC_FP64 ? copy_stats<double>(c, stats) : copy_stats<float>(c, stats);
+    rc = st64(c) ? copy_stats<double>(c, stats) : copy_stats<float>(c, stats);
     if (rc) return rc;
     CK(cudaStreamSynchronize(c->stream));
   }
-  return CHAMP_OK;
+  return tc_check(c);
 }
 
 int champ_vmc_run_host(champ_ctx *c, int32_t nw, double *x, int32_t nsweep, uint64_t seed, uint64_t sweep0,
@@ -1329,10 +1663,10 @@ int champ_vmc_run_host(champ_ctx *c, int32_t nw, double *x, int32_t nsweep, uint
   int rc = launch(c, Op::Eval);
   if (rc) return rc;
   c->have_walkers = true;
-  champ_vmc_stats st = {nullptr, nullptr, nullptr, nullptr};
+  champ_vmc_stats st = {nullptr, nullptr, nullptr, nullptr};  // champ_vmc_sweeps reports a tensor-core give-up
   rc = champ_vmc_sweeps(c, nsweep, seed, sweep0, step, &st);
   if (rc) return rc;
-  double *el = c->prec == CHAMP_PREC_FP64 ? c->std_.s_elast : c->stf.s_elast;
+  double *el = st64(c) ? c->std_.s_elast : c->stf.s_elast;
   CK(cudaMemcpyAsync(eloc, el, sizeof(double) * nw, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(x, state_x(c), sizeof(double) * nw * 3 * c->N, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -1341,7 +1675,7 @@ int champ_vmc_run_host(champ_ctx *c, int32_t nw, double *x, int32_t nsweep, uint
 
 int champ_walker_status(champ_ctx *c, uint32_t *flags) {
   if (!c || !flags) return fail(CHAMP_EINVAL, "null argument");
-  uint32_t *s = c->prec == CHAMP_PREC_FP64 ? c->std_.status : c->stf.status;
+  uint32_t *s = st64(c) ? c->std_.status : c->stf.status;
   CK(cudaMemcpyAsync(flags, s, sizeof(uint32_t) * c->W, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return tc_check(c);
@@ -1352,7 +1686,7 @@ int champ_set_option(champ_ctx *c, const char *name, int64_t value) {
   if (!strcmp(name, "orbital_tc")) {
     if (value < 0 || value > 2) return fail(CHAMP_EINVAL, "orbital_tc: 0, 1 or 2");
     if (value && !c->tc_ok)
-      return fail(CHAMP_EINVAL, "orbital_tc: needs mixed precision, walker state in HBM, >= 16 orbitals of a spin "
+      return fail(CHAMP_EINVAL, "orbital_tc: needs FP32 precision, walker state in HBM, >= 16 orbitals of a spin "
                                 "and room for the basis rows");
     if (value == 1) c->tc_mode = c->tc_fused_ok ? 1 : 2;
     if (value == 2) {
@@ -1385,7 +1719,7 @@ int champ_get_option(const champ_ctx *c, const char *name, int64_t *value) {
   if (!strcmp(name, "orbital_tc")) { *value = c->tc_on ? c->tc_mode : 0; return CHAMP_OK; }
   if (!strcmp(name, "launches_per_sweep")) {
     int spins = (c->nup > 0) + (c->ndn > 0);
-    *value = c->tc_on ? 2 + spins + (c->tc_mode == 2 ? 1 : 0) : 1;
+    *value = c->tc_on ? 2 + spins + (c->tc_mode == 2 ? 1 : 0) : (c->prec == CHAMP_PREC_MIXED ? 2 : 1);
     return CHAMP_OK;
   }
   if (!strcmp(name, "reinvert_every")) { *value = c->reinv_every; return CHAMP_OK; }
@@ -1397,8 +1731,7 @@ int champ_get_option(const champ_ctx *c, const char *name, int64_t *value) {
 int champ_eval_energy_noalloc(champ_ctx *c, int32_t nw, const double *x, double *eloc) {
   if (!c || !x || !eloc) return fail(CHAMP_EINVAL, "null argument");
   if (nw < 1) return fail(CHAMP_EINVAL, "nw < 1");
-  return c->prec == CHAMP_PREC_FP64 ? eval_noalloc_t<double>(c, c->std_, nw, x, eloc)
-                                    : eval_noalloc_t<float>(c, c->stf, nw, x, eloc);
+  return st64(c) ? eval_noalloc_t<double>(c, c->std_, nw, x, eloc) : eval_noalloc_t<float>(c, c->stf, nw, x, eloc);
 }
 
 int champ_num_walkers(const champ_ctx *c, int32_t *nw) {

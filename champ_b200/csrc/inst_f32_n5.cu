@@ -1,0 +1,5 @@
+// inst_f32_n5.cu -- instantiates every kernel for compute type float and e-e-n order 5
+// (order 0 also serves nordc = 1, which has no e-e-n terms).
+#include "launch.cuh"
+
+CHAMP_INST(f32, float, 5)

@@ -53,6 +53,9 @@ struct State {
   double *o_lnpsi, *o_sign, *o_psij, *o_vel, *o_divv, *o_d2, *o_pe, *o_peee, *o_penl, *o_eloc;
   // VMC accumulators
   double *s_esum, *s_e2sum, *s_acc, *s_elast;
+  // mixed precision: the FP32 tables of the single-electron moves ([W][N][N], [W][N][C][2],
+  // [W][N][ZQ]), refreshed from the FP64 tables by every full evaluation; null otherwise
+  float *m_fso, *m_ren, *m_zq;
 };
 constexpr int NLT = 2 + MAXLCH;  // task record: (e*C+c), r, vps[0..MAXLCH-1]
 constexpr int ZQ = 8;            // stride of the per-electron power sums zq
@@ -173,6 +176,34 @@ __device__ inline void view_load(const View<T> &v, const State<T> &st, int w, in
   for (int i = lane; i < st.tvstride; i += 32) v.tv[i] = st.tv[(size_t)w * st.tvstride + i];
   for (int i = lane; i < st.gstride; i += 32) v.gam[i] = st.gam[(size_t)w * st.gstride + i];
   __syncwarp();
+}
+// Mixed precision: after an FP64 full evaluation, the FP32 copies of the Jastrow pair table,
+// the e-n distances and the power sums that the single-electron moves read.
+template <class T>
+__device__ inline void mirror_store(const View<T> &v, const State<T> &st, int w, int N, int C, int lane) {
+  if (!st.m_fso) return;
+  __syncwarp();
+  for (int i = lane; i < N * N; i += 32) st.m_fso[(size_t)w * N * N + i] = (float)v.fso[i];
+  for (int i = lane; i < N * C * 2; i += 32) st.m_ren[(size_t)w * N * C * 2 + i] = (float)v.ren[i];
+  for (int i = lane; i < N * ZQ; i += 32) st.m_zq[(size_t)w * N * ZQ + i] = (float)v.zq[i];
+  __syncwarp();
+}
+// The persistent state a full evaluation produces, from a resident view back to HBM: the FP64
+// tables, or only their FP32 mirrors when the state has them.
+template <class T>
+__device__ inline void eval_store(const View<T> &v, const State<T> &st, int w, int N, int C, int lane) {
+  __syncwarp();
+  for (int i = lane; i < 3 * N; i += 32) st.x[(size_t)w * 3 * N + i] = v.xs[i];
+  for (int i = lane; i < st.astride; i += 32) st.ainv[(size_t)w * st.astride + i] = v.ainv[i];
+  if (!st.m_fso) {
+    for (int i = lane; i < N * N; i += 32) st.fso[(size_t)w * N * N + i] = v.fso[i];
+    for (int i = lane; i < N * C * 2; i += 32) st.ren[(size_t)w * N * C * 2 + i] = v.ren[i];
+    for (int i = lane; i < N * ZQ; i += 32) st.zq[(size_t)w * N * ZQ + i] = v.zq[i];
+  }
+  for (int i = lane; i < st.tvstride; i += 32) st.tv[(size_t)w * st.tvstride + i] = v.tv[i];
+  for (int i = lane; i < st.gstride; i += 32) st.gam[(size_t)w * st.gstride + i] = v.gam[i];
+  __syncwarp();
+  mirror_store(v, st, w, N, C, lane);
 }
 template <class T>
 __device__ inline void view_store(const View<T> &v, const State<T> &st, int w, int N, int C, int lane) {
@@ -1097,7 +1128,8 @@ __global__ void __launch_bounds__(128, 4) k_eval(Sys<T> s, State<T> st, Layout L
     __syncwarp();
     EvalRes res;
     full_eval<T, NORD, MD>(s, J, E, st, w, v, R, lane, outputs != 0, res, nullptr, orbs_ready != 0);
-    if (L.resident) view_store(v, st, w, s.N, s.C, lane);
+    if (L.resident) eval_store(v, st, w, s.N, s.C, lane);
+    else mirror_store(v, st, w, s.N, s.C, lane);
   }
 }
 
@@ -1172,8 +1204,11 @@ __global__ void __launch_bounds__(128, 4) k_accept(Sys<T> s, State<T> st, Layout
 }
 
 // Fused VMC: nsweep sweeps of single-electron Metropolis moves plus E_L after each sweep
-// (phase 0); the E_L re-inverts the Slater matrices every reinv_every sweeps.  Phase 1 runs only the moves and phase 2 only the E_L, from orbitals computed in
-// between for all walkers (tensor-core contraction).  Statistics are added to st.s_*.
+// (phase 0); the E_L re-inverts the Slater matrices every reinv_every sweeps.  Phase 1 runs only
+// the moves and phase 2 only the E_L, from orbitals computed in between for all walkers
+// (tensor-core contraction).  Phase 3 runs only the E_L, from the positions alone (re-inverting,
+// and refreshing the FP32 move tables when the state has them): the FP64 half of a mixed-precision
+// sweep whose moves ran in FP32.  Statistics are added to st.s_*.
 template <class T, int NORD, bool MD>
 __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L, int nsweep, uint64_t seed,
                                                 uint64_t sweep0, double step, int phase, int reinv_every) {
@@ -1185,6 +1220,29 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
   const int N = s.N;
   for (int w = blockIdx.x * wpb + wib; w < st.W; w += gridDim.x * wpb) {
     View<T> v = make_view<T>(dsm + L.bytes * wib, L, st, w, s.N, s.C, s.nbasis, s.nomax, L.resident != 0);
+    if (phase == 3) {
+      for (int i = lane; i < 3 * N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * N + i];
+      __syncwarp();
+      double es = 0, e2 = 0, el = 0;
+      for (int isw = 0; isw < nsweep; isw++) {
+        double R[9];
+        random_rotation(seed, (uint32_t)w, sweep0 + (uint64_t)isw, R);
+        EvalRes res;
+        full_eval<T, NORD, MD>(s, J, E, st, w, v, R, lane, false, res, nullptr, false, true);
+        el = res.eloc;
+        es += el;
+        e2 += el * el;
+      }
+      if (L.resident) eval_store(v, st, w, N, s.C, lane);
+      else mirror_store(v, st, w, N, s.C, lane);
+      if (lane == 0) {
+        st.s_esum[w] += es;
+        st.s_e2sum[w] += e2;
+        st.s_elast[w] = el;
+      }
+      __syncwarp();
+      continue;
+    }
     if (L.resident) {
       view_load(v, st, w, N, s.C, lane);
     } else {

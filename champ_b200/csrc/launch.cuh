@@ -8,19 +8,20 @@
 #define fail champ_fail
 // ---- kernel dispatch over (precision, e-e-n order)
 template <class K>
-static int set_attrs(champ_ctx *c, K kern) {
-  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem));
+static int set_attrs(champ_ctx *c, K kern, size_t smem) {
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   CK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
   return CHAMP_OK;
 }
 template <class T, int NORD, bool MD>
 static int set_smem_attrs(champ_ctx *c) {
-  int rc = set_attrs(c, k_eval<T, NORD, MD>);
-  if (!rc) rc = set_attrs(c, k_propose<T, NORD, MD>);
-  if (!rc) rc = set_attrs(c, k_accept<T, MD>);
-  if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD>);
-  if (!rc) rc = set_attrs(c, k_dmc_move<T, NORD, MD>);
-  if (!rc && std::is_same<T, float>::value) {
+  const size_t sm = kcfg<T>(c).smem;
+  int rc = set_attrs(c, k_eval<T, NORD, MD>, sm);
+  if (!rc) rc = set_attrs(c, k_propose<T, NORD, MD>, sm);
+  if (!rc) rc = set_attrs(c, k_accept<T, MD>, sm);
+  if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD>, sm);
+  if (!rc) rc = set_attrs(c, k_dmc_move<T, NORD, MD>, sm);
+  if (!rc && std::is_same<T, float>::value && c->prec == CHAMP_PREC_FP32) {
     CK(cudaFuncSetAttribute(orbtc::k_orb_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024 + 128));
     CK(cudaFuncSetAttribute(orbtc::k_orb_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024 + 128));
     CK(cudaFuncSetAttribute(orbtc::k_orb_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -30,7 +31,7 @@ static int set_smem_attrs(champ_ctx *c) {
     CK(cudaFuncSetAttribute(k_basis_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)std::min<size_t>(4 * (size_t)c->nbasis * 5 * sizeof(float), 227 * 1024)));
   }
-  if (!rc) {
+  if (!rc && c->smem_pg > 0 && (std::is_same<T, double>::value || c->prec == CHAMP_PREC_FP32)) {
     CK(cudaFuncSetAttribute(k_pgrad<T, NORD, MD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_pg));
     CK(cudaFuncSetAttribute(k_pgrad<T, NORD, MD>, cudaFuncAttributePreferredSharedMemoryCarveout,
                             (int)cudaSharedmemCarveoutMaxShared));
@@ -117,57 +118,63 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
   Sys<T> &s = sysof<T>(c);
   State<T> st = a.st_override ? *(const State<T> *)a.st_override : stof<T>(c);
   st.W = a.st_override ? a.nw_override : c->W;
-  dim3 grid((st.W + c->wpb - 1) / c->wpb), block(32 * c->wpb);
+  const KCfg &K = kcfg<T>(c);
+  dim3 grid((st.W + K.wpb - 1) / K.wpb), block(32 * K.wpb);
   const double *R = c->rot;
   switch (op) {
   case Op::Eval:
   case Op::EvalOut: {
-    const bool tc = c->tc_on && !a.st_override;  // only mixed-precision contexts turn it on
+    const bool tc = c->tc_on && !a.st_override;  // only FP32 contexts turn it on
     if (tc) {
       int rc = run_orb_tc<T>(c, st);
       if (rc) return rc;
     }
-    k_eval<T, NORD, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, R[0], R[1], R[2], R[3], R[4], R[5], R[6], R[7], R[8],
+    k_eval<T, NORD, MD><<<grid, block, K.smem, c->stream>>>(s, st, K.lay, R[0], R[1], R[2], R[3], R[4], R[5], R[6], R[7], R[8],
                                                        op == Op::EvalOut ? 1 : 0, tc ? 1 : 0);
     break;
   }
   case Op::Propose:
   case Op::ProposeGrad:
-    k_propose<T, NORD, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, a.e, a.xnew, a.ratio, op == Op::ProposeGrad ? a.grad : nullptr);
+    k_propose<T, NORD, MD><<<grid, block, K.smem, c->stream>>>(s, st, K.lay, a.e, a.xnew, a.ratio, op == Op::ProposeGrad ? a.grad : nullptr);
     break;
   case Op::Accept:
-    k_accept<T, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, a.e, a.mask);
+    k_accept<T, MD><<<grid, block, K.smem, c->stream>>>(s, st, K.lay, a.e, a.mask);
     break;
   case Op::PGrad:
-    k_pgrad<T, NORD, MD><<<dim3((c->W + c->wpb_pg - 1) / c->wpb_pg), dim3(32 * c->wpb_pg), c->smem_pg, c->stream>>>(s, st, c->lay, a.pgout, R[0], R[1], R[2], R[3], R[4],
+    k_pgrad<T, NORD, MD><<<dim3((c->W + c->wpb_pg - 1) / c->wpb_pg), dim3(32 * c->wpb_pg), c->smem_pg, c->stream>>>(s, st, K.lay, a.pgout, R[0], R[1], R[2], R[3], R[4],
                                                                  R[5], R[6], R[7], R[8], a.pgout.part);
     break;
   case Op::DmcMove:
-    k_dmc_move<T, NORD, MD><<<dim3((c->dpar.wmax + c->wpb - 1) / c->wpb), block, c->smem, c->stream>>>(
-        s, st, c->lay, c->dpar, c->dA);
+    k_dmc_move<T, NORD, MD><<<dim3((c->dpar.wmax + K.wpb - 1) / K.wpb), block, K.smem, c->stream>>>(
+        s, st, K.lay, c->dpar, c->dA, a.phase < 0 ? 0 : a.phase);
     break;
   case Op::DmcCopy: {
     k_dmc_copy<T><<<592, 128, 0, c->stream>>>(st, st2of<T>(c), c->dA, c->dB, c->N, c->C, c->dpar.wmax);
     break;
   }
   case Op::Vmc: {
+    if (a.phase >= 0) {
+      k_vmc<T, NORD, MD><<<grid, block, K.smem, c->stream>>>(s, st, K.lay, a.nsweep, a.seed, a.sweep0, a.step, a.phase,
+                                                              c->reinv_every);
+      break;
+    }
     CK(cudaMemsetAsync(st.s_esum, 0, sizeof(double) * st.W, c->stream));
     CK(cudaMemsetAsync(st.s_e2sum, 0, sizeof(double) * st.W, c->stream));
     CK(cudaMemsetAsync(st.s_acc, 0, sizeof(double) * st.W, c->stream));
-    const bool tc = c->tc_on && !a.st_override;  // only mixed-precision contexts turn it on
+    const bool tc = c->tc_on && !a.st_override;  // only FP32 contexts turn it on
     if (!tc) {
-      k_vmc<T, NORD, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, a.nsweep, a.seed, a.sweep0, a.step, 0,
+      k_vmc<T, NORD, MD><<<grid, block, K.smem, c->stream>>>(s, st, K.lay, a.nsweep, a.seed, a.sweep0, a.step, 0,
                                                                c->reinv_every);
       break;
     }
     // per sweep: moves, orbitals of all walkers on the tensor cores, E_L
     for (int isw = 0; isw < a.nsweep; isw++) {
-      k_vmc<T, NORD, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, 1, a.seed, a.sweep0 + isw, a.step, 1,
+      k_vmc<T, NORD, MD><<<grid, block, K.smem, c->stream>>>(s, st, K.lay, 1, a.seed, a.sweep0 + isw, a.step, 1,
                                                                c->reinv_every);
       CK(cudaGetLastError());
       int rc = run_orb_tc<T>(c, st);
       if (rc) return rc;
-      k_vmc<T, NORD, MD><<<grid, block, c->smem, c->stream>>>(s, st, c->lay, 1, a.seed, a.sweep0 + isw, a.step, 2,
+      k_vmc<T, NORD, MD><<<grid, block, K.smem, c->stream>>>(s, st, K.lay, 1, a.seed, a.sweep0 + isw, a.step, 2,
                                                                c->reinv_every);
       CK(cudaGetLastError());
     }
@@ -178,32 +185,15 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
   return CHAMP_OK;
 }
 
-template <class T, bool MD>
-static int launch_m(champ_ctx *c, Op op, const OpArgs &a) {
-  switch (c->nordc) {
-  case 0: case 1: return launch_t<T, 0, MD>(c, op, a);
-  case 4: return launch_t<T, 4, MD>(c, op, a);
-  case 5: return launch_t<T, 5, MD>(c, op, a);
-  default: return fail(CHAMP_EINVAL, "nordc must be 0, 1, 4 or 5");
+// One translation unit per (compute type, e-e-n order) instantiates its kernels through this macro
+// (CHAMP_INST(f32, float, 4) defines launch_f32_n4 and attrs_f32_n4); launch_f32 / launch_f64
+// dispatch on the context's e-e-n order.
+#define CHAMP_INST(TAG, T, NORD)                                                                  \
+  int launch_##TAG##_n##NORD(champ_ctx *c, Op op, const OpArgs &a) {                              \
+    return c->md.multidet ? launch_t<T, NORD, true>(c, op, a) : launch_t<T, NORD, false>(c, op, a); \
+  }                                                                                               \
+  int attrs_##TAG##_n##NORD(champ_ctx *c) {                                                       \
+    return c->md.multidet ? set_smem_attrs<T, NORD, true>(c) : set_smem_attrs<T, NORD, false>(c); \
   }
-}
-template <class T>
-static int launch_p(champ_ctx *c, Op op, const OpArgs &a) {
-  return c->md.multidet ? launch_m<T, true>(c, op, a) : launch_m<T, false>(c, op, a);
-}
-
-template <class T, bool MD>
-static int attrs_m(champ_ctx *c) {
-  switch (c->nordc) {
-  case 0: case 1: return set_smem_attrs<T, 0, MD>(c);
-  case 4: return set_smem_attrs<T, 4, MD>(c);
-  case 5: return set_smem_attrs<T, 5, MD>(c);
-  default: return fail(CHAMP_EINVAL, "nordc must be 0, 1, 4 or 5");
-  }
-}
-template <class T>
-static int attrs_p(champ_ctx *c) {
-  return c->md.multidet ? attrs_m<T, true>(c) : attrs_m<T, false>(c);
-}
 
 #undef fail

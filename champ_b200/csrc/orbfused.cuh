@@ -78,7 +78,8 @@ static __global__ void __launch_bounds__(NTF, 1) k_orb_fused(Sys<float> s, FArgs
   const int cb = a.kchunk > 0 ? a.kchunk : a.nkb;
   const int quad = warp & 3, half = warp >> 2;
   const bool vec = (a.nomax & 3) == 0 && ((uintptr_t)a.orb & 15) == 0;  // rows and groups 16-byte aligned
-  uint32_t it = 0;  // K-blocks issued so far (commit count)
+  uint32_t it = 0;       // K-blocks started so far
+  uint32_t ncommit = 0;  // K-blocks whose MMA group was committed (the same on every thread)
   bool ok = true;
   for (int tile = blockIdx.x; tile < ntile && ok; tile += gridDim.x) {
     double pt[3] = {0, 0, 0};
@@ -150,6 +151,7 @@ static __global__ void __launch_bounds__(NTF, 1) k_orb_fused(Sys<float> s, FArgs
           }
         mma_commit(smem_u32(&mbar[sg]));
       }
+      ncommit = it + 1;
       if ((kb + 1) % cb != 0 && kb + 1 != a.nkb) continue;
       // end of a chunk: drain.  Warp q reads TMEM lanes 32(q mod 4)..+31; warps q and q+4 take
       // alternate groups of 16 columns of the 5 channel ranges (Np is a multiple of 16: a group
@@ -193,7 +195,7 @@ static __global__ void __launch_bounds__(NTF, 1) k_orb_fused(Sys<float> s, FArgs
     if (a.err) atomicExch(a.err, 1);
     // let the committed MMA groups finish (bounded) before the accumulator is freed
     if (tid == 0)
-      for (uint32_t u = it > 2 ? it - 2 : 0; u < it; u++) mbar_wait(smem_u32(&mbar[u & 1]), (u >> 1) & 1);
+      for (uint32_t u = ncommit > 2 ? ncommit - 2 : 0; u < ncommit; u++) mbar_wait(smem_u32(&mbar[u & 1]), (u >> 1) & 1);
   }
   __syncthreads();
   fence_after();

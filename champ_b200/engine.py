@@ -26,7 +26,7 @@ EXPORTED_SYMBOLS = [
     "champ_get_option", "champ_oh_buffers",
 ]
 
-PREC = {"fp64": 0, "mixed": 1}
+PREC = {"fp64": 0, "mixed": 1, "fp32": 2}
 
 _lib = None
 

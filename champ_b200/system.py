@@ -42,6 +42,9 @@ class ChampSystem(C.Structure):
         ("npotd", C.POINTER(C.c_int32)), ("lpotp1", C.POINTER(C.c_int32)),
         ("necp_term", C.POINTER(C.c_int32)), ("necp_power", C.POINTER(C.c_int32)),
         ("ecp_coef", C.POINTER(C.c_double)), ("ecp_exponent", C.POINTER(C.c_double)),
+        ("nrad", C.c_int32), ("rad_igrid", C.POINTER(C.c_int32)), ("rad_nr", C.POINTER(C.c_int32)),
+        ("rad_h", C.POINTER(C.c_double)), ("rad_r0", C.POINTER(C.c_double)), ("rad_x", C.POINTER(C.c_double)),
+        ("rad_val", C.POINTER(C.c_double)), ("shell_rad", C.POINTER(C.c_int32)),
     ]
 
 
@@ -98,6 +101,15 @@ class System:
     necp_power: np.ndarray = field(default_factory=lambda: np.zeros((1, MAX_LCHAN, 1), np.int32))
     ecp_coef: np.ndarray = field(default_factory=lambda: np.zeros((1, MAX_LCHAN, 1)))
     ecp_exponent: np.ndarray = field(default_factory=lambda: np.zeros((1, MAX_LCHAN, 1)))
+    # numerical radial tables (shell kind 2): grid type, points, step or ratio, r0 as read,
+    # grid points and values of every table one after another, and each shell's table
+    rad_igrid: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    rad_nr: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    rad_h: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    rad_r0: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    rad_x: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    rad_val: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    shell_rad: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
     walkers: int = 256          # walker count of the benchmark definition
     step: float = 0.5           # Metropolis step (bohr)
 
@@ -152,6 +164,11 @@ class System:
             npotd=P(self.npotd, i4), lpotp1=P(self.lpotp1, i4),
             necp_term=P(self.necp_term, i4), necp_power=P(self.necp_power, i4),
             ecp_coef=P(self.ecp_coef, f8), ecp_exponent=P(self.ecp_exponent, f8),
+            nrad=len(self.rad_igrid), rad_igrid=P(np.append(self.rad_igrid, 0), i4),
+            rad_nr=P(np.append(self.rad_nr, 0), i4), rad_h=P(np.append(self.rad_h, 0.0), f8),
+            rad_r0=P(np.append(self.rad_r0, 0.0), f8), rad_x=P(np.append(self.rad_x, 0.0), f8),
+            rad_val=P(np.append(self.rad_val, 0.0), f8),
+            shell_rad=P(self.shell_rad if len(self.shell_rad) else np.full(len(self.shell_cent), -1), i4),
         )
         return s, keep
 
@@ -419,6 +436,81 @@ def be_example() -> System:
     here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     with open(os.path.join(here, "tests", "golden", "be_vb1.json")) as f:
         return from_slater_example(json.load(f))
+
+
+_LABEL_LM = {"S": (0, 0), "PX": (1, 1), "PY": (1, -1), "PZ": (1, 0)}
+for _l, _c in ((2, "D"), (3, "F"), (4, "G")):
+    _LABEL_LM[f"{_c}0"] = (_l, 0)
+    for _m in range(1, _l + 1):
+        _LABEL_LM[f"{_c}+{_m}"] = (_l, _m)
+        _LABEL_LM[f"{_c}-{_m}"] = (_l, -_m)
+
+
+def c2_bfd_fixture():
+    """The parsed reference example (tests/golden/c2_bfd.npz, made by make_c2_bfd_fixture.py)."""
+    import json
+    import os
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    d = np.load(os.path.join(here, "tests", "golden", "c2_bfd.npz"))
+    return json.loads(str(d["meta"])), d["coef"], d["grid_x"], d["grid_val"]
+
+
+def c2_bfd_example(run: int = 0) -> System:
+    """The reference's C2 pseudopotential example (examples/c2_bfd_vtz_rhf_vmc_new.inp): two
+    carbon pseudo-atoms (Z_eff 4), 68 basis functions on 9 numerical radial functions
+    (examples/basis.1, splined as splfit_bas does), BFD pseudopotential with an s nonlocal
+    channel (examples/pseudopot1), 6-point quadrature, one determinant, Jastrow ijas=4 isc=4
+    with the parameters of VMC run `run` of the transcript (0: the input's)."""
+    meta, coef, gx, gv = c2_bfd_fixture()
+    par = meta["runs"][run]["params"]
+    shells, bshell, bm, srad, key = [], [], [], [], {}
+    ncent = len(meta["cent"])
+    for ic in range(ncent):
+        for lab, irad in meta["labels"]:
+            l, m = _LABEL_LM[lab.upper()]
+            k = (ic, l, irad)
+            if k not in key:
+                key[k] = len(shells)
+                shells.append((ic, l + 1, l, 2, [0.0], [1.0]))
+                srad.append(irad - 1)
+            bshell.append(key[k])
+            bm.append(m)
+    bas = _basis_from_shells(shells)
+    bas["basis_shell"] = np.array(bshell, np.int32)
+    bas["basis_m"] = np.array(bm, np.int32)
+    g = meta["grid"]
+    nrb = g["nrbas"]
+    ps = meta["pseudopot"]
+    nct = len(meta["znuc"])
+    necp = np.zeros((nct, MAX_LCHAN), np.int32)
+    mg = max(len(t) for t in ps["components"])
+    ecoef, eexp = np.zeros((nct, MAX_LCHAN, mg)), np.zeros((nct, MAX_LCHAN, mg))
+    epow = np.zeros((nct, MAX_LCHAN, mg), np.int32)
+    lpotp1 = meta["lpotp1"]
+    for it in range(nct):
+        for k, terms in enumerate(ps["components"]):
+            ch = lpotp1[it] - 1 if k == 0 else k - 1  # local component first in the file
+            necp[it, ch] = len(terms)
+            for i, (cf, pw, ex) in enumerate(terms):
+                ecoef[it, ch, i], epow[it, ch, i], eexp[it, ch, i] = cf, pw, ex
+    a = np.array(par["a"], float)[None, :]
+    b = np.array(par["b"], float)[None, :]
+    c = np.array(par["c"], float)[None, :]
+    nordc = 0
+    while nterms4(nordc + 1) <= c.shape[1] and nordc < 7:
+        nordc += 1
+    ne, nup = meta["nelec"], meta["nup"]
+    det = np.array(meta["iworbd"], np.int32)[None, :] - 1
+    return System(name="c2_bfd_example", nelec=ne, nup=nup, cent=np.array(meta["cent"], float),
+                  iwctype=np.array(meta["iwctype"], np.int32), znuc=np.array(meta["znuc"], float), **bas,
+                  coef=np.ascontiguousarray(coef), det_orb=det, **_one_csf(), scalek=meta["scalek"],
+                  norda=a.shape[1] - 1, nordb=b.shape[1] - 1, nordc=nordc, nspin2b=1, een_cusp=1 if nordc > 1 else 0,
+                  a4=a, b=b, c=c, nloc=meta["nloc"], nquad=meta["nquad"], npotd=np.full(nct, ps["npotd"], np.int32),
+                  lpotp1=np.array(lpotp1, np.int32), necp_term=necp, necp_power=epow, ecp_coef=ecoef,
+                  ecp_exponent=eexp, rad_igrid=np.full(nrb, g["igrid"], np.int32), rad_nr=np.full(nrb, g["nr"], np.int32),
+                  rad_h=np.full(nrb, g["exph"]), rad_r0=np.full(nrb, g["r0"]), rad_x=np.tile(gx, nrb),
+                  rad_val=np.ascontiguousarray(gv).ravel(), shell_rad=np.array(srad, np.int32), walkers=8192,
+                  step=0.45)
 
 
 def hydrogenic(z=2.0) -> System:

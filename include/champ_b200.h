@@ -43,8 +43,19 @@ extern "C" {
 #define CHAMP_ESINGULAR 5   /* a walker hit a singular Slater matrix (see champ_walker_status) */
 
 #define CHAMP_PREC_FP64 0   /* every step in FP64 */
-#define CHAMP_PREC_MIXED 1  /* orbitals, Jastrow, NLPP quadrature in FP32; inverse, log-det,
-                               accepted Sherman-Morrison update and E_L sums in FP64 */
+#define CHAMP_PREC_MIXED 1  /* single-electron moves (basis and orbitals at the proposed position,
+                               Jastrow pair values, ratio and drift) in FP32 with FP32 Jastrow and
+                               distance tables; the accepted Sherman-Morrison update, the inverse
+                               and log-det in FP64; every full evaluation (E_L, velocities, the
+                               nonlocal quadrature, parameter derivatives) in FP64 from the
+                               positions, re-inverting the Slater matrices and refreshing the FP32
+                               tables.  E_L therefore equals the FP64 engine's on the same
+                               configuration; FP32 only steers the Metropolis acceptance. */
+#define CHAMP_PREC_FP32 2   /* as MIXED, but the full evaluation also in FP32 (orbitals optionally
+                               on the tensor cores, option "orbital_tc"): inverse, log-det, the
+                               Sherman-Morrison update and the E_L sums stay FP64.  E_L carries
+                               FP32-level relative errors (1e-7 of |lap ln psi|), which exceed
+                               1e-6 Ha on systems with large kinetic energies. */
 
 /* Per-walker status bits (champ_walker_status). */
 #define CHAMP_WS_SINGULAR 1u   /* Slater matrix singular at the last full evaluation */
@@ -57,6 +68,7 @@ extern "C" {
 #define CHAMP_MAX_CTYPE 8
 #define CHAMP_MAX_NORD 7
 #define CHAMP_MAX_LCHAN 5      /* pseudopotential l channels (npotd) */
+#define CHAMP_MAX_QUAD 86      /* nonlocal quadrature points */
 
 /*
  * System descriptor: everything the reference reads from its input menus
@@ -73,13 +85,15 @@ typedef struct champ_system {
   /* Basis (qmc/vmc/basis_fns.f90:38-474): a shell is one radial function on one centre,
      R(r) = sum_p coef_p * N(n,l,zeta_p) * r^(n-1) * exp(-zeta_p r)     (Slater, kind 0)
                                           * exp(-zeta_p r^2)   (Gaussian, kind 1)
+     R(r) = coef_0 * sqrt((2l+1)/4pi) * f(r)    (numerical, kind 2: f is radial table
+                                                 shell_rad[ish], one primitive)
      N is the reference normalisation (qmc/vmc/basis_norm.f90), including sqrt((2l+1)/4pi).
      Basis function b = R_shell(b)(r) * C_{l,m}(rhat), C the real harmonics of basis_fns. */
   int32_t nshell;
   const int32_t *shell_cent;   /* [nshell] */
   const int32_t *shell_n;      /* [nshell] */
   const int32_t *shell_l;      /* [nshell] 0..4 */
-  const int32_t *shell_kind;   /* [nshell] 0 Slater, 1 Gaussian */
+  const int32_t *shell_kind;   /* [nshell] 0 Slater, 1 Gaussian, 2 numerical radial table */
   const int32_t *shell_nprim;  /* [nshell] */
   const double *prim_zeta;     /* [sum nprim] */
   const double *prim_coef;     /* [sum nprim] contraction weights */
@@ -112,7 +126,9 @@ typedef struct champ_system {
 
   /* Pseudopotential (nloc=6: Gaussian ECP, qmc/vmc/readps_gauss.f90:126-165). */
   int32_t nloc;                /* 0 all-electron, 6 Gaussian ECP */
-  int32_t nquad;               /* 12 (icosahedral rule of qmc/vmc/rotqua.f90) */
+  int32_t nquad;               /* quadrature points of the nonlocal integration: the rule of
+                                  qmc/vmc/rotqua.f90 (gesqua) with the number of points closest
+                                  to nquad among 4, 6, 12, 18, 20, 24, 26, 32, 50, 86 */
   int32_t mgauss;              /* max terms per channel */
   const int32_t *npotd;        /* [nctype] number of l channels */
   const int32_t *lpotp1;       /* [nctype] 1-based local channel */
@@ -120,6 +136,20 @@ typedef struct champ_system {
   const int32_t *necp_power;   /* [nctype][CHAMP_MAX_LCHAN][mgauss] */
   const double *ecp_coef;      /* [nctype][CHAMP_MAX_LCHAN][mgauss] */
   const double *ecp_exponent;  /* [nctype][CHAMP_MAX_LCHAN][mgauss] */
+
+  /* Numerical radial functions (numr=1: the basis.<centre type> grids of read_bas_num.f90,
+     interpolated as splfit_bas does, qmc/vmc/splfit.f90): a cubic spline through the grid values
+     with end slopes from a 5-point polynomial fit at small r and an exponential a0 exp(-ak r)
+     matched at the last point, which also continues the function beyond the grid. */
+  int32_t nrad;                /* radial tables (0: none) */
+  const int32_t *rad_igrid;    /* [nrad] grid: 1 linear r(i) = r0 + (i-1) h; 2 exponential
+                                  r(i) = r0 h^(i-1); 3 shifted exponential r(i) = r0 (h^(i-1) - 1) */
+  const int32_t *rad_nr;       /* [nrad] grid points (>= 6) */
+  const double *rad_h;         /* [nrad] exp_h_bas: the step (grid 1) or the ratio (grids 2, 3) */
+  const double *rad_r0;        /* [nrad] r0_bas as read: first point (grids 1, 2) or last point (3) */
+  const double *rad_x;         /* [sum rad_nr] grid points, tables one after another */
+  const double *rad_val;       /* [sum rad_nr] function values at the grid points */
+  const int32_t *shell_rad;    /* [nshell] radial table of each kind-2 shell (others ignored) */
 } champ_system;
 
 /* Outputs of a full evaluation (hpsi).  Host pointers; any may be NULL. */
@@ -232,7 +262,9 @@ int champ_num_walkers(const champ_ctx *ctx, int32_t *nw);
    of champ_set_quadrature_rotation.  Intermediates live in one fixed 16 MiB device array
    compiled into the library: nw beyond what fits returns CHAMP_EINVAL with the limit in
    champ_last_error().  The first call on a device looks the array's address up.  The call
-   makes no device allocation; it leaves the context's walkers untouched.  All calls share the
+   makes no device allocation; it leaves the context's walkers untouched.  In FP32 precision it
+   computes the orbitals on the CUDA cores (the tensor-core contraction of option "orbital_tc" is
+   not used here); mixed precision evaluates in FP64 as champ_eval_full does.  All calls share the
    array, so calls that overlap on the GPU (other streams, other contexts on the device) race. */
 int champ_eval_energy_noalloc(champ_ctx *ctx, int32_t nw, const double *x, double *eloc);
 /* Waits for the context's stream; also reports a tensor-core contraction that gave up. */
@@ -244,8 +276,10 @@ int champ_synchronize(champ_ctx *ctx);
    3-term TF32 split (about FP32 accuracy), with the basis functions formed in shared memory
    (fused; up to 96 orbitals of a spin, else as 2); 2 the same contraction from basis rows
    written to HBM first; 0 uses the CUDA-core contraction.  Available for
-   mixed precision when the walker state lives in HBM and a spin has >= 16 orbitals, and on by
-   default there; CHAMP_EINVAL otherwise.
+   FP32 precision when the walker state lives in HBM and a spin has >= 16 orbitals, and on by
+   default there; CHAMP_EINVAL otherwise.  The calls that run it (champ_set_walkers,
+   champ_eval_full, champ_vmc_sweeps, champ_vmc_run_host) synchronise and return CHAMP_ECUDA if
+   a contraction gave up waiting for its MMA groups (bounded waits), then clear that flag.
    "orbital_tc_chunk": K-blocks of 16 basis functions that the fused contraction sums into one
    TMEM accumulator before adding it to the orbital rows in FP32 (default 4; 0 = all of K).  The
    tensor core truncates while it accumulates, so shorter chunks shrink the resulting bias

@@ -102,7 +102,13 @@ struct orc_sys {
   int npotd[CHAMP_MAX_CTYPE], lpotp1[CHAMP_MAX_CTYPE];
   int *necp_term, *necp_power;
   double *ecp_coef, *ecp_exp;
-  double q0[32][3], wq[32], q[32][3];
+  double q0[86][3], wq[86], q[86][3];
+  /* numerical radial tables (kind-2 shells): grid type, points, derived r0, h, the small-r
+     polynomial, the large-r exponential, values and spline second derivatives */
+  int nrad, *rad_of_shell;
+  int *rt_grid, *rt_nr;
+  double *rt_r0, *rt_h, (*rt_ce)[5], (*rt_ae)[2];
+  double **rt_y, **rt_y2;
 };
 
 int orc_nterms4(int nord) {
@@ -178,27 +184,259 @@ static void apply_een_cusp(orc_sys *s) {
   }
 }
 
-/* Icosahedral 12-point rule (qmc/vmc/rotqua.f90:1-30, weights 1/12): the two poles and
-   two rings of five points at z = +-1/sqrt(5), the lower ring turned by 36 degrees. */
-static void quad12(double q[][3], double *w) {
-  const double pi = 3.141592653589793;
-  double zr = 1.0 / sqrt(5.0), rr = 2.0 / sqrt(5.0);
-  q[0][0] = 0; q[0][1] = 0; q[0][2] = 1;
-  q[1][0] = 0; q[1][1] = 0; q[1][2] = -1;
-  for (int k = 0; k < 5; k++) {
-    double a = 2 * pi * k / 5.0, b = a + pi / 5.0;
-    q[2 + k][0] = rr * cos(a); q[2 + k][1] = rr * sin(a); q[2 + k][2] = zr;
-    q[7 + k][0] = rr * cos(b); q[7 + k][1] = rr * sin(b); q[7 + k][2] = -zr;
-  }
-  for (int k = 0; k < 12; k++) w[k] = 1.0 / 12.0;
-}
-
 static void *dupmem(const void *p, size_t n) {
   if (!p || n == 0) return calloc(1, n ? n : 1);
   void *q = malloc(n);
   memcpy(q, p, n);
   return q;
 }
+
+/* gesqua (qmc/vmc/rotqua.f90:1-618): of the rules with 4, 6, 12, 18, 26, 32, 50, 24, 20 and 86
+   points the one closest to nq (first on ties).  Points are generated by symmetry type as the
+   reference does; weights by point type.  Returns the number of points. */
+static int gesqua(int nq_in, double q[][3], double *w) {
+  static const int iq[10] = {4, 6, 12, 18, 26, 32, 50, 24, 20, 86};
+  int best = 0;
+  for (int i = 1; i < 10; i++)
+    if (abs(nq_in - iq[i]) < abs(nq_in - iq[best])) best = i;
+  int nq = iq[best];
+  memset(q, 0, sizeof(double) * 3 * 86);
+  memset(w, 0, sizeof(double) * 86);
+  /* weight of each point type per rule (ww of the reference) and the types' sizes */
+  double wt[10][6];
+  memset(wt, 0, sizeof wt);
+  wt[0][0] = 1.0 / 4.0;  wt[1][0] = 1.0 / 6.0;  wt[2][0] = 1.0 / 12.0; wt[2][1] = 1.0 / 12.0;
+  wt[3][0] = 1.0 / 30.0; wt[3][1] = 1.0 / 15.0;
+  wt[4][0] = 1.0 / 21.0; wt[4][1] = 4.0 / 105.0; wt[4][2] = 27.0 / 840.0;
+  wt[5][0] = 5.0 / 168.0; wt[5][1] = 5.0 / 168.0; wt[5][2] = 27.0 / 840.0;
+  wt[6][0] = 4.0 / 315.0; wt[6][1] = 64.0 / 2835.0; wt[6][2] = 27.0 / 1280.0; wt[6][3] = 14641.0 / 725760.0;
+  wt[7][0] = 1.0 / 24.0; wt[8][0] = 1.0 / 20.0;
+  wt[9][0] = .0115440115441; wt[9][2] = .0119439090859; wt[9][3] = .0111105557106;
+  wt[9][4] = .0118765012945; wt[9][5] = .0118123037469;
+  int sizes[6] = {6, 12, 8, 24, 0, 0}, ntyp = 4;
+  if (nq == 4) { sizes[0] = 4; sizes[1] = sizes[2] = sizes[3] = 0; }
+  if (nq == 12 || nq == 32) { sizes[0] = 2; sizes[1] = 10; sizes[2] = 20; sizes[3] = 0; }
+  if (nq == 20) { sizes[0] = 20; sizes[1] = sizes[2] = sizes[3] = 0; }
+  if (nq == 24) { sizes[0] = 24; sizes[1] = sizes[2] = sizes[3] = 0; }
+  if (nq == 86) { int s86[6] = {6, 0, 8, 24, 24, 24}; memcpy(sizes, s86, sizeof s86); ntyp = 6; }
+  for (int k = 0, j = 0; k < ntyp; k++)
+    for (int i = 0; i < sizes[k]; i++, j++)
+      if (j < nq) w[j] = wt[best][k];
+  const double pi = 3.14159265359, a = 1.0 / sqrt(2.0), b = 1.0 / sqrt(3.0), c11 = 1.0 / sqrt(11.0),
+               d11 = 3.0 / sqrt(11.0);
+  if (nq == 4) {
+    /* tetrahedron: (+,+,+) (+,-,-) (-,+,-) (-,-,+) scaled by 1/sqrt(3) */
+    static const int sg[4][3] = {{1, 1, 1}, {1, -1, -1}, {-1, 1, -1}, {-1, -1, 1}};
+    for (int j = 0; j < 4; j++)
+      for (int k = 0; k < 3; k++) q[j][k] = sg[j][k] * b;
+  } else if (nq == 6 || nq == 18 || nq == 26 || nq == 50) {
+    /* octahedral families: the 6 axis points; 12 edge midpoints; 8 cube corners; 24 (r,r,s) */
+    int m = 6, n8 = 0;
+    for (int k = 0; k < 3; k++) { q[2 * k][k] = 1; q[2 * k + 1][k] = -1; }
+    if (nq > 6) {
+      /* pairs in (x,y), (y,z), (z,x) planes, the reference's order: for each sign of the first
+         coordinate and of the second */
+      for (int s1 = 0; s1 < 2; s1++)
+        for (int s2 = 0; s2 < 2; s2++) {
+          double u = s1 ? -a : a, v = s2 ? -a : a;
+          int i = 2 * s1 + s2;
+          q[6 + i][0] = u;  q[6 + i][1] = v;
+          q[10 + i][1] = u; q[10 + i][2] = v;
+          q[14 + i][2] = u; q[14 + i][0] = v;
+        }
+      m = 18;
+    }
+    if (nq > 18) {
+      for (int s1 = 0; s1 < 2; s1++)
+        for (int s2 = 0; s2 < 2; s2++)
+          for (int s3 = 0; s3 < 2; s3++, n8++) {
+            double sx = s1 ? -1 : 1, sy = s2 ? -1 : 1, sz = s3 ? -1 : 1;
+            q[18 + n8][0] = sx * b; q[18 + n8][1] = sy * b; q[18 + n8][2] = sz * b;
+            if (nq > 26) {
+              q[26 + n8][0] = sx * c11; q[26 + n8][1] = sy * c11; q[26 + n8][2] = sz * d11;
+              q[34 + n8][0] = sx * c11; q[34 + n8][1] = sy * d11; q[34 + n8][2] = sz * c11;
+              q[42 + n8][0] = sx * d11; q[42 + n8][1] = sy * c11; q[42 + n8][2] = sz * c11;
+            }
+          }
+    }
+    (void)m;
+  } else if (nq == 12 || nq == 20 || nq == 32) {
+    /* icosahedral families: poles + two rings of 5 at z = +-1/sqrt(5) (12); the 20 dodecahedron
+       vertices (20, overwriting the poles); both (32) */
+    double s5 = sqrt(5.0), den = sqrt(15.0 + 6.0 * s5);
+    double ct = 1.0 / s5, st = 2.0 / s5, c1 = (2.0 + s5) / den, s1 = sqrt(1.0 - c1 * c1), c2 = 1.0 / den,
+           s2 = sqrt(1.0 - c2 * c2);
+    q[0][2] = 1.0; q[1][2] = -1.0;
+    for (int j = 0; j < 5; j++) {
+      double ph0 = 2.0 * j * pi / 5.0, ph1 = (2.0 * j + 1.0) * pi / 5.0;
+      if (nq != 20) {
+        q[2 + j][0] = st * cos(ph0); q[2 + j][1] = st * sin(ph0); q[2 + j][2] = ct;
+        q[7 + j][0] = st * cos(ph1); q[7 + j][1] = st * sin(ph1); q[7 + j][2] = -ct;
+      }
+      if (nq > 12) {
+        int k0 = nq == 20 ? 0 : 12;
+        q[k0 + j][0] = s1 * cos(ph1);      q[k0 + j][1] = s1 * sin(ph1);      q[k0 + j][2] = c1;
+        q[k0 + 5 + j][0] = s2 * cos(ph1);  q[k0 + 5 + j][1] = s2 * sin(ph1);  q[k0 + 5 + j][2] = c2;
+        q[k0 + 10 + j][0] = s1 * cos(ph0); q[k0 + 10 + j][1] = s1 * sin(ph0); q[k0 + 10 + j][2] = -c1;
+        q[k0 + 15 + j][0] = s2 * cos(ph0); q[k0 + 15 + j][1] = s2 * sin(ph0); q[k0 + 15 + j][2] = -c2;
+      }
+    }
+  } else if (nq == 24) {
+    /* one point, its images under the three cyclic coordinate shifts, each also turned by -90
+       degrees about y, then all rotated about z in steps of 90 degrees */
+    double p3[3] = {.8662468181078, .4225186537611, .2666354015167};
+    int n = 0;
+    for (int l = 0; l < 3; l++) {
+      double x, y, z;
+      if (l == 0) { x = p3[0]; y = p3[1]; z = p3[2]; }
+      else if (l == 1) { x = p3[2]; y = p3[0]; z = p3[1]; }
+      else { x = p3[1]; y = p3[2]; z = p3[0]; }
+      double u = -z * sin(-pi / 2.0) + x * cos(-pi / 2.0), v = y, t = x * sin(-pi / 2.0) + z * cos(-pi / 2.0);
+      for (int m = 0; m < 4; m++) {
+        double f = pi * m / 2.0, cf = cos(f), sf = sin(f);
+        q[n][0] = x * cf - y * sf; q[n][1] = x * sf + y * cf; q[n][2] = z; n++;
+        q[n][0] = u * cf - v * sf; q[n][1] = u * sf + v * cf; q[n][2] = t; n++;
+      }
+    }
+  } else {
+    /* 86 points: axes; cube corners; three families of 24 (r,r,s); 24 (p,q,0) */
+    double pp = .927330657151, qq = .374243039090, r1 = .369602846454, m1 = .852518311701,
+           r2 = .694354006603, m2 = .189063552885;
+    for (int k = 0; k < 3; k++) { q[2 * k][k] = 1; q[2 * k + 1][k] = -1; }
+    for (int s1 = 0; s1 < 2; s1++)
+      for (int s2 = 0; s2 < 2; s2++) {
+        double u = s1 ? -1 : 1, v = s2 ? -1 : 1;
+        int i = 2 * s1 + s2;
+        q[62 + i][0] = u * pp; q[62 + i][1] = v * qq;
+        q[66 + i][0] = u * pp; q[66 + i][2] = v * qq;
+        q[70 + i][1] = u * pp; q[70 + i][2] = v * qq;
+        q[74 + i][0] = u * qq; q[74 + i][1] = v * pp;
+        q[78 + i][0] = u * qq; q[78 + i][2] = v * pp;
+        q[82 + i][1] = u * qq; q[82 + i][2] = v * pp;
+        for (int s3 = 0; s3 < 2; s3++) {
+          double t = s3 ? -1 : 1;
+          int k = 4 * s1 + 2 * s2 + s3;
+          q[6 + k][0] = u * b;   q[6 + k][1] = v * b;   q[6 + k][2] = t * b;
+          q[14 + k][0] = u * r1; q[14 + k][1] = v * r1; q[14 + k][2] = t * m1;
+          q[22 + k][0] = u * r1; q[22 + k][1] = v * m1; q[22 + k][2] = t * r1;
+          q[30 + k][0] = u * m1; q[30 + k][1] = v * r1; q[30 + k][2] = t * r1;
+          q[38 + k][0] = u * r2; q[38 + k][1] = v * r2; q[38 + k][2] = t * m2;
+          q[46 + k][0] = u * r2; q[46 + k][1] = v * m2; q[46 + k][2] = t * r2;
+          q[54 + k][0] = u * m2; q[54 + k][1] = v * r2; q[54 + k][2] = t * r2;
+        }
+      }
+  }
+  return nq;
+}
+
+/* Numerical radial function tables (qmc/vmc/read_bas_num.f90:213-378): grid parameters as
+   splfit_bas uses them; c_k of the polynomial through the first five grid points (ncoef = 5,
+   the fit used with pseudopotentials); a0 exp(-ak r) from the last two points; the clamped
+   cubic spline of spline2 (Numerical Recipes p. 88) with the polynomial's slope at the first
+   point and the exponential's at the last. */
+static void build_tables(orc_sys *s, const champ_system *d) {
+  s->nrad = d->nrad;
+  s->rad_of_shell = (int *)calloc(s->nshell, sizeof(int));
+  for (int i = 0; i < s->nshell; i++) s->rad_of_shell[i] = (s->sh_kind[i] == 2 && d->shell_rad) ? d->shell_rad[i] : -1;
+  if (s->nrad <= 0) return;
+  int nt = s->nrad;
+  s->rt_grid = (int *)calloc(nt, sizeof(int)); s->rt_nr = (int *)calloc(nt, sizeof(int));
+  s->rt_r0 = (double *)calloc(nt, sizeof(double)); s->rt_h = (double *)calloc(nt, sizeof(double));
+  s->rt_ce = (double(*)[5])calloc(nt, sizeof(double[5])); s->rt_ae = (double(*)[2])calloc(nt, sizeof(double[2]));
+  s->rt_y = (double **)calloc(nt, sizeof(double *)); s->rt_y2 = (double **)calloc(nt, sizeof(double *));
+  size_t off = 0;
+  for (int t = 0; t < nt; t++) {
+    int g = d->rad_igrid[t], n = d->rad_nr[t];
+    const double *x = d->rad_x + off, *y = d->rad_val + off;
+    double h = d->rad_h[t], r0 = d->rad_r0[t];
+    if (g == 2 && h <= 1.0) h = x[1] / x[0];
+    if (g == 3) r0 = r0 / (pow(h, n - 1) - 1.0);
+    if (g == 2 && (r0 <= 0 || h <= 0)) { r0 = x[0]; h = x[1] / x[0]; }
+    s->rt_grid[t] = g; s->rt_nr[t] = n; s->rt_r0[t] = r0; s->rt_h[t] = h;
+    /* Vandermonde system of the first five points, Gaussian elimination with partial pivoting */
+    double m[5][6];
+    for (int i = 0; i < 5; i++) {
+      for (int j = 0; j < 5; j++) m[i][j] = pow(x[i], j);
+      m[i][5] = y[i];
+    }
+    for (int k = 0; k < 5; k++) {
+      int pv = k;
+      for (int i = k + 1; i < 5; i++) if (fabs(m[i][k]) > fabs(m[pv][k])) pv = i;
+      for (int j = 0; j < 6; j++) { double tmp = m[k][j]; m[k][j] = m[pv][j]; m[pv][j] = tmp; }
+      for (int i = k + 1; i < 5; i++) {
+        double f = m[i][k] / m[k][k];
+        for (int j = k; j < 6; j++) m[i][j] -= f * m[k][j];
+      }
+    }
+    for (int i = 4; i >= 0; i--) {
+      double acc = m[i][5];
+      for (int j = i + 1; j < 5; j++) acc -= m[i][j] * s->rt_ce[t][j];
+      s->rt_ce[t][i] = acc / m[i][i];
+    }
+    double yp1 = 0;
+    for (int i = 1; i < 5; i++) yp1 += i * s->rt_ce[t][i] * pow(x[0], i - 1);
+    double wfm = 0.5 * (y[n - 1] + y[n - 2]), dwfm = (y[n - 1] - y[n - 2]) / (x[n - 1] - x[n - 2]), ypn = 0;
+    if (fabs(wfm) > 1e-99) {
+      s->rt_ae[t][1] = dwfm / wfm < 0 ? -dwfm / wfm : 0.1;
+      s->rt_ae[t][0] = y[n - 1] * exp(s->rt_ae[t][1] * x[n - 1]);
+      ypn = -s->rt_ae[t][1] * y[n - 1];
+    }
+    double *y2 = (double *)calloc(n, sizeof(double)), *wk = (double *)calloc(n, sizeof(double));
+    y2[0] = -0.5;
+    wk[0] = (3.0 / (x[1] - x[0])) * ((y[1] - y[0]) / (x[1] - x[0]) - yp1);
+    for (int i = 1; i < n - 1; i++) {
+      double sig = (x[i] - x[i - 1]) / (x[i + 1] - x[i - 1]), p = sig * y2[i - 1] + 2.0;
+      y2[i] = (sig - 1.0) / p;
+      wk[i] = (6.0 * ((y[i + 1] - y[i]) / (x[i + 1] - x[i]) - (y[i] - y[i - 1]) / (x[i] - x[i - 1])) /
+                   (x[i + 1] - x[i - 1]) - sig * wk[i - 1]) / p;
+    }
+    double un = (3.0 / (x[n - 1] - x[n - 2])) * (ypn - (y[n - 1] - y[n - 2]) / (x[n - 1] - x[n - 2]));
+    y2[n - 1] = (un - 0.5 * wk[n - 2]) / (0.5 * y2[n - 2] + 1.0);
+    for (int k = n - 2; k >= 0; k--) y2[k] = y2[k] * y2[k + 1] + wk[k];
+    free(wk);
+    s->rt_y2[t] = y2;
+    s->rt_y[t] = (double *)dupmem(y, sizeof(double) * n);
+    off += n;
+  }
+}
+
+/* splfit_bas (qmc/vmc/splfit.f90): f, f', f'' of table t at r. */
+static void table_fit(const orc_sys *s, int t, double r, double *f) {
+  int g = s->rt_grid[t], n = s->rt_nr[t], jx;
+  double r0 = s->rt_r0[t], h = s->rt_h[t], ref0, ref1;
+  if (g == 1) {
+    jx = (int)((r - r0) / h + 1);
+    ref0 = r0 + h * (jx - 1); ref1 = ref0 + h;
+  } else if (g == 2) {
+    double xr = log(r / r0) / log(h) + 1;
+    jx = xr < 1 ? 0 : (int)xr;
+    ref0 = r0 * pow(h, jx - 1); ref1 = ref0 * h;
+  } else {
+    jx = (int)(log((r + r0) / r0) / log(h) + 1.0);
+    ref0 = r0 * pow(h, jx - 1) - r0; ref1 = (ref0 + r0) * h - r0;
+  }
+  const double *ce = s->rt_ce[t];
+  if (jx < 1) {
+    f[0] = ce[0]; f[1] = 0; f[2] = 0;
+    for (int i = 1; i < 5; i++) {
+      f[0] += ce[i] * pow(r, i);
+      f[1] += i * ce[i] * pow(r, i - 1);
+      if (i >= 2) f[2] += i * (i - 1) * ce[i] * pow(r, i - 2);
+    }
+  } else if (jx >= n) {
+    f[0] = s->rt_ae[t][0] * exp(-s->rt_ae[t][1] * r);
+    f[1] = -s->rt_ae[t][1] * f[0];
+    f[2] = -s->rt_ae[t][1] * f[1];
+  } else {
+    const double *y = s->rt_y[t] + jx - 1, *y2 = s->rt_y2[t] + jx - 1;
+    double dh = ref1 - ref0, bb = (r - ref0) / dh, aa = (ref1 - r) / dh;
+    double cc = aa * (aa * aa - 1) * dh * dh / 6, dd = bb * (bb * bb - 1) * dh * dh / 6;
+    f[0] = aa * y[0] + bb * y[1] + cc * y2[0] + dd * y2[1];
+    f[1] = (y[1] - y[0]) / dh + (-(3 * aa * aa - 1) * y2[0] + (3 * bb * bb - 1) * y2[1]) * dh / 6;
+    f[2] = aa * y2[0] + bb * y2[1];
+  }
+}
+
 
 orc_sys *orc_create(const champ_system *d) {
   orc_sys *s = (orc_sys *)calloc(1, sizeof(orc_sys));
@@ -228,7 +466,9 @@ orc_sys *orc_create(const champ_system *d) {
   s->pc = (double *)dupmem(d->prim_coef, sizeof(double) * s->nprim);
   for (int i = 0; i < s->nshell; i++)
     for (int p = s->sh_p0[i]; p < s->sh_p0[i + 1]; p++)
-      s->pc[p] *= basis_anorm(s->sh_kind[i], s->sh_n[i], s->sh_l[i], s->pz[p]);
+      s->pc[p] *= s->sh_kind[i] == 2 ? sqrt((2 * s->sh_l[i] + 1) / (4 * 3.141592653589793))
+                                     : basis_anorm(s->sh_kind[i], s->sh_n[i], s->sh_l[i], s->pz[p]);
+  build_tables(s, d);
   s->nbasis = d->nbasis;
   s->b_shell = (int *)dupmem(d->basis_shell, sizeof(int) * s->nbasis);
   s->b_m = (int *)dupmem(d->basis_m, sizeof(int) * s->nbasis);
@@ -310,7 +550,7 @@ orc_sys *orc_create(const champ_system *d) {
     s->ecp_coef = (double *)dupmem(d->ecp_coef, sizeof(double) * nt * s->mgauss);
     s->ecp_exp = (double *)dupmem(d->ecp_exponent, sizeof(double) * nt * s->mgauss);
   }
-  quad12(s->q0, s->wq);
+  s->nquad = gesqua(s->nloc > 0 ? s->nquad : 12, s->q0, s->wq);
   orc_set_rotation(s, NULL);
   return s;
 }
@@ -322,6 +562,9 @@ void orc_destroy(orc_sys *s) {
   free(s->pz); free(s->pc); free(s->b_shell); free(s->b_m); free(s->coef);
   free(s->det_orb); free(s->cdet); free(s->c);
   free(s->necp_term); free(s->necp_power); free(s->ecp_coef); free(s->ecp_exp);
+  for (int t = 0; t < s->nrad && s->rt_y; t++) { free(s->rt_y[t]); free(s->rt_y2[t]); }
+  free(s->rt_y); free(s->rt_y2); free(s->rt_grid); free(s->rt_nr); free(s->rt_r0); free(s->rt_h);
+  free(s->rt_ce); free(s->rt_ae); free(s->rad_of_shell);
   free(s);
 }
 
@@ -414,6 +657,12 @@ static void solid_harm(int l, int m, double x, double y, double z, double *S, do
 /* Radial function and its first two derivatives for one shell (wfv(1..3) of
    basis_fns.f90:118-157, summed over the contraction). */
 static void radial(const orc_sys *s, int ish, double r, double *R) {
+  if (s->sh_kind[ish] == 2) {
+    table_fit(s, s->rad_of_shell[ish], r, R);
+    double w = s->pc[s->sh_p0[ish]];
+    R[0] *= w; R[1] *= w; R[2] *= w;
+    return;
+  }
   int n = s->sh_n[ish];
   double rn = n;
   R[0] = R[1] = R[2] = 0;

@@ -1,6 +1,6 @@
 """Tensor-core orbital contraction (tcgen05, 3-term TF32 split) against the CUDA-core paths.
 
-The full evaluation of a mixed-precision engine whose walker state lives in HBM computes the
+The full evaluation of an FP32-precision engine whose walker state lives in HBM computes the
 orbitals of all electrons of all walkers as one tensor-core product per spin, either fused with
 the basis evaluation in shared memory (orbital_tc 1) or from basis rows in HBM (orbital_tc 2).
 These tests switch the modes through champ_set_option("orbital_tc") and compare with the
@@ -27,7 +27,7 @@ def _engines(s, nw, seed):
     x = S.initial_walkers(s, nw, seed=seed)
     e64 = Engine(s, nw, "fp64")
     e64.set_walkers(x)
-    em = Engine(s, nw, "mixed")
+    em = Engine(s, nw, "fp32")
     return x, e64, em
 
 
@@ -47,7 +47,7 @@ def test_eval_full_tensor_core_orbitals(ncent):
     err = {}
     for tc in (0, 1, 2):
         err[tc] = float(np.max(np.abs(out[tc]["energy"] - ref["energy"]) / sc))
-        assert err[tc] <= 2e-3  # the mixed-precision parity tolerance of the other tests
+        assert err[tc] <= 2e-3  # the FP32 parity tolerance of the other tests
         lerr = np.abs(out[tc]["lnpsi"] - ref["lnpsi"]) / np.maximum(1.0, np.abs(ref["lnpsi"]))
         assert np.all(lerr <= 1e-5), (tc, float(lerr.max()))
     print(f"cluster ncent={ncent}: max |dE_L|/scale vs FP64: CUDA-core {err[0]:.2e}, "
@@ -64,6 +64,29 @@ def test_eval_full_tensor_core_orbitals(ncent):
     assert abs(shift[1]) <= 5e-5 and abs(shift[2]) <= 5e-5, shift
 
 
+def test_fused_contraction_with_more_tiles_than_sms():
+    """1024 walkers x 64 electrons of a spin = 512 tiles of 128 rows per spin, more than the
+    148 CTAs of the grid: each CTA carries its stage and barrier-parity counters across several
+    tiles.  Both tensor-core paths against the CUDA-core contraction of the same engine."""
+    s = S.cluster128(ncent=8)
+    nw = 1024
+    x, e64, em = _engines(s, nw, 29)
+    ref = e64.eval_full()
+    sc = _scale(ref)
+    out = {}
+    for tc in (0, 1, 2):
+        em.set_option("orbital_tc", tc)
+        em.set_walkers(x)
+        out[tc] = em.eval_full()
+    e0 = float(np.max(np.abs(out[0]["energy"] - ref["energy"]) / sc))
+    for tc in (1, 2):
+        err = float(np.max(np.abs(out[tc]["energy"] - ref["energy"]) / sc))
+        assert err <= max(3 * e0, TOL), (tc, err, e0)
+        shift = float(np.mean(out[tc]["lnpsi"] - out[0]["lnpsi"]))
+        assert abs(shift) <= 5e-5, (tc, shift)
+        assert np.all(np.isfinite(out[tc]["energy"]))
+
+
 def test_fused_accumulation_chunks_remove_the_truncation_bias():
     """orbital_tc_chunk 0 (one accumulator over all of K) against the default chunking and
     chunks of one K-block: the walker-mean ln|psi| offset from the CUDA-core contraction of the
@@ -72,7 +95,7 @@ def test_fused_accumulation_chunks_remove_the_truncation_bias():
     s = S.cluster128(ncent=32)
     nw = 256
     x = S.initial_walkers(s, nw, seed=23)
-    em = Engine(s, nw, "mixed")
+    em = Engine(s, nw, "fp32")
     em.set_option("orbital_tc", 0)
     em.set_walkers(x)
     base = em.eval_full()["lnpsi"]
@@ -89,14 +112,14 @@ def test_fused_accumulation_chunks_remove_the_truncation_bias():
 
 def test_vmc_split_sweep_matches_fused_sweep():
     """A VMC sweep run as moves / tensor-core orbitals / E_L gives the walkers of the fused sweep
-    (moves do not depend on the E_L) and the same local energies at mixed tolerance."""
+    (moves do not depend on the E_L) and the same local energies at FP32 tolerance."""
     from champ_b200.engine import Engine
     s = S.cluster128(ncent=8)
     nw = 256
     x = S.initial_walkers(s, nw, seed=5)
     res = {}
     for tc in (0, 1, 2):
-        e = Engine(s, nw, "mixed")
+        e = Engine(s, nw, "fp32")
         e.set_option("orbital_tc", tc)
         e.set_walkers(x)
         st = e.vmc_sweeps(1, 99, 0, 0.3)
@@ -115,7 +138,7 @@ def test_vmc_split_sweep_matches_fused_sweep():
 def test_orbital_tc_option_rejected_where_unsupported():
     from champ_b200.engine import Engine, ChampError
     s = S.c2_dimer()
-    e = Engine(s, 8, "mixed")
+    e = Engine(s, 8, "fp32")
     with pytest.raises(ChampError):
         e.set_option("orbital_tc", 1)
     e.set_option("orbital_tc", 0)

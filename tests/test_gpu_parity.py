@@ -4,9 +4,12 @@ same seeded walkers.
 Tolerances
   FP64 engine: relative 1e-9 on ln|psi|, drift velocities, sum of Laplacians and E_L
                (absolute floor 1e-8 Ha times max(1, |E_L|)).
-  mixed engine (FP32 orbitals/Jastrow/quadrature, FP64 inverse and sums): the measured
-               error is reported by tests/test_gpu_precision.py; here the bound is
-               |d ln psi| <= 2e-4 |ln psi| + 1e-3 and |dE_L| <= 2e-3 max(1, |d2lnpsi|).
+  mixed engine (FP32 single-electron moves, FP64 full evaluation): the full evaluation is held
+               to the FP64 tolerances and to the precision contract |dE_L| <= 1e-6 Ha per
+               sample; proposal ratios and gradients (FP32) to 2e-3 relative.
+  FP32 engine (FP32 full evaluation as well): |d ln psi| <= 2e-4 |ln psi| + 1e-3 and
+               |dE_L| <= 2e-3 max(1, |d2lnpsi|); this mode does not meet the 1e-6 Ha contract
+               (bench.py reports its measured error).
 """
 import numpy as np
 import pytest
@@ -64,12 +67,38 @@ def test_eval_full_fp64_matches_oracle(oracle_mod, k, nw):
         assert abs(g["energy"][w] - r["energy"]) <= 1e-8 * sc
 
 
-@pytest.mark.parametrize("k,nw", [(1, 64), (2, 64), (3, 32), ("be", 64)])
-def test_eval_full_mixed_matches_oracle(oracle_mod, k, nw):
+@pytest.mark.parametrize("k,nw", [(1, 64), (2, 64), (3, 32), ("be", 64), (5, 4)])
+def test_eval_full_mixed_meets_the_precision_contract(oracle_mod, k, nw):
+    """Mixed precision: |E_L(mixed) - E_L(FP64 oracle)| <= 1e-6 Ha on every sample, after FP32
+    moves have changed the walkers (the full evaluation re-inverts and rebuilds every table in
+    FP64 from the positions)."""
     s = get(k)
     o = oracle_mod.Oracle(s)
     x = S.initial_walkers(s, nw, seed=200 + (4 if k == "be" else k))
     eng = make_engine(s, nw, "mixed")
+    eng.set_walkers(x)
+    eng.vmc_sweeps(2, seed=5, sweep0=0, step=0.3, stats=False)  # FP32 moves, SM updates
+    x = eng.get_walkers()
+    rot = oracle_mod.random_rotation(3, 1, 4)
+    eng.set_rotation(rot)
+    g = eng.eval_full()
+    ref = oracle_eval_all(o, x, rot)
+    for w in range(nw):
+        r = ref[w]
+        sc = max(1.0, abs(r["energy"]), abs(r["d2lnpsi"]))
+        assert abs(g["energy"][w] - r["energy"]) <= 1e-6, (w, g["energy"][w], r["energy"])
+        assert abs(g["energy"][w] - r["energy"]) <= 1e-8 * sc
+        assert abs(g["lnpsi"][w] - r["lnpsi"]) <= 1e-9 * max(1, abs(r["lnpsi"]))
+        assert np.allclose(g["velocity"][w], r["vel"], rtol=1e-9, atol=1e-9 * sc)
+        assert abs(g["pe_nonloc"][w] - r["pe_nonloc"]) <= 1e-9 * max(1, abs(r["pe_nonloc"]))
+
+
+@pytest.mark.parametrize("k,nw", [(1, 64), (2, 64), (3, 32), ("be", 64)])
+def test_eval_full_fp32_matches_oracle(oracle_mod, k, nw):
+    s = get(k)
+    o = oracle_mod.Oracle(s)
+    x = S.initial_walkers(s, nw, seed=200 + (4 if k == "be" else k))
+    eng = make_engine(s, nw, "fp32")
     eng.set_walkers(x)
     g = eng.eval_full()
     ref = oracle_eval_all(o, x)
@@ -79,7 +108,8 @@ def test_eval_full_mixed_matches_oracle(oracle_mod, k, nw):
         assert abs(g["energy"][w] - r["energy"]) <= 2e-3 * max(1.0, abs(r["d2lnpsi"]))
 
 
-@pytest.mark.parametrize("k,prec", [(1, "fp64"), (2, "fp64"), (2, "mixed"), (3, "fp64"), ("be", "fp64"), ("be", "mixed")])
+@pytest.mark.parametrize("k,prec", [(1, "fp64"), (2, "fp64"), (2, "mixed"), (2, "fp32"), (3, "fp64"), (3, "mixed"),
+                                    ("be", "fp64"), ("be", "mixed")])
 def test_propose_accept_sequence_matches_oracle(oracle_mod, k, prec):
     """hpsie ratios and gradients, then jassav/detsav/dete_save updates, for a sequence of moves."""
     s = get(k)
@@ -89,7 +119,9 @@ def test_propose_accept_sequence_matches_oracle(oracle_mod, k, prec):
     eng = make_engine(s, nw, prec)
     eng.set_walkers(x)
     rng = np.random.default_rng(5)
-    tol = 1e-9 if prec == "fp64" else 2e-3
+    # mixed and FP32 propose in FP32 (orbitals at the new position, Jastrow pair values); the
+    # multi-determinant ratio contracts them with G, whose entries grow near a node
+    tol = {"fp64": 1e-9, "mixed": 2e-3, "fp32": 2e-3}[prec]
     for step in range(2 * s.nelec):
         iel = step % s.nelec
         xn = x[:, iel, :] + 0.3 * rng.standard_normal((nw, 3))
@@ -173,7 +205,35 @@ def test_walker_status_clean(oracle_mod):
     assert not eng.walker_status().any()
 
 
-@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_vmc_mixed_energy_within_one_sigma_of_fp64():
+    """VMC energy of the mixed engine within 1 sigma of the FP64 engine's (C2-like dimer, same
+    seeds: the FP32 ratios change only a few Metropolis decisions), and every sample's E_L of the
+    final configurations within 1e-6 Ha of the FP64 engine on the same walkers."""
+    s = S.c2_dimer()
+    nw, ns = 4096, 60
+    x = S.initial_walkers(s, nw, seed=33)
+    res = {}
+    for prec in ("fp64", "mixed"):
+        eng = make_engine(s, nw, prec)
+        eng.set_walkers(x)
+        eng.vmc_sweeps(30, seed=71, sweep0=0, step=0.5, stats=False)
+        st = eng.vmc_sweeps(ns, seed=71, sweep0=30, step=0.5)
+        e_w = st["esum"] / ns
+        res[prec] = (e_w.mean(), e_w.std(ddof=1) / np.sqrt(nw), eng.get_walkers(), st)
+    e64, err64, xw, _ = res["fp64"]
+    em, errm, _, stm = res["mixed"]
+    print(f"VMC c2_dimer: FP64 {e64:.6f} +- {err64:.6f}, mixed {em:.6f} +- {errm:.6f} Ha")
+    assert abs(em - e64) <= err64
+    assert np.all(np.isfinite(stm["esum"]))
+    # per sample, on identical configurations
+    a, b = make_engine(s, nw, "mixed"), make_engine(s, nw, "fp64")
+    a.set_walkers(xw)
+    b.set_walkers(xw)
+    d = np.abs(a.eval_full()["energy"] - b.eval_full()["energy"])
+    assert d.max() <= 1e-6, d.max()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed", "fp32"])
 def test_vmc_be_example_matches_reference_transcript(prec):
     """Statistical pin of the GPU path: VMC of the reference's Be example (4 determinants,
     examples/be_vb1_jcas24_vmc_j_opt_lin.out: E = -14.6463051 +- 0.0075680, sigma = 0.579)."""

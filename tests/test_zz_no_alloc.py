@@ -18,13 +18,20 @@ from champ_b200 import system as S
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("mixed", 1e-6)])
-def test_noalloc_energy_matches_eval_full_on_two_calls(prec, tol):
+@pytest.mark.parametrize("sysname,nw,prec,tol", [("c2_dimer", 512, "fp64", 1e-9), ("c2_dimer", 512, "mixed", 1e-9),
+                                                  ("c2_dimer", 512, "fp32", 1e-6), ("cluster128", 8, "fp64", 1e-9),
+                                                  ("cluster128", 8, "mixed", 1e-9), ("cluster128", 8, "fp32", 1e-6)])
+def test_noalloc_energy_matches_eval_full_on_two_calls(sysname, nw, prec, tol):
+    """c2_dimer keeps each walker's state in shared memory during the evaluation; cluster128
+    (128 electrons) keeps it in HBM, here inside the fixed array.  In FP32 precision this entry
+    point computes the orbitals on the CUDA cores, so the reference is the same context with the
+    tensor-core contraction switched off."""
     import torch
     from champ_b200.engine import Engine
-    s = S.c2_dimer()
-    nw = 512
+    s = S.c2_dimer() if sysname == "c2_dimer" else S.cluster128()
     eng = Engine(s, nw, prec)
+    if prec == "fp32" and sysname == "cluster128":
+        eng.set_option("orbital_tc", 0)
     for seed in (11, 12):
         x = S.initial_walkers(s, nw, seed=seed)
         eng.set_walkers(x)
