@@ -50,6 +50,11 @@ struct champ_ctx {
   std::vector<int4> rad_tab;
   std::vector<double> rad_par, rad_y, rad_y2;
   std::vector<int> rad_shell;
+  // opt-in device timing of the VMC sweep kernels (option "phase_timing"): event pairs per
+  // launch, summed per phase by champ_phase_times
+  int ptime = 0;
+  std::vector<void *> ev_pool;             // cudaEvent_t, reused
+  std::vector<std::pair<int, int>> ev_use; // (phase, index of the start event; stop = index + 1)
   std::vector<void *> allocs;
   Sys<double> sd;
   Sys<float> sf;
@@ -77,6 +82,12 @@ struct champ_ctx {
   int wpb_pg = 4;
   int pg_lanesum = 0;      // per-lane slots for the NLPP parameter sums in the derivative kernel
   double *pg_dl = nullptr, *pg_de = nullptr, *pg_el = nullptr, *pg_wt = nullptr;
+  // tape of the parameter-gradient forward pass (see PGOut)
+  double *pg_tv = nullptr, *pg_tc = nullptr;
+  int *pg_tn = nullptr;
+  bool have_tape = false;
+  int pg_mode = 0;  // 0: forward pass + reverse sweep; 1: one fused pass
+  int nquad = 12;   // points of the nonlocal quadrature rule in use
   double *oh_oa = nullptr, *oh_ow = nullptr, *oh_mb = nullptr, *oh_s = nullptr, *oh_h = nullptr;
   bool have_pgrad = false;
   void *cublas = nullptr;
@@ -139,7 +150,7 @@ inline KCfg &kcfg<double>(champ_ctx *c) { return c->kd; }
 template <>
 inline KCfg &kcfg<float>(champ_ctx *c) { return c->kf; }
 
-enum class Op { Eval, EvalOut, Propose, ProposeGrad, Accept, Vmc, PGrad, DmcMove, DmcCopy };
+enum class Op { Eval, EvalOut, Propose, ProposeGrad, Accept, Vmc, PGrad, PGradBwd, DmcMove, DmcCopy };
 struct OpArgs {
   int e = 0;
   const double *xnew = nullptr;

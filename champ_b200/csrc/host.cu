@@ -35,6 +35,7 @@ int champ_fail(int code, const std::string &msg) {
 }
 
 static int fail(int code, const std::string &msg) { return champ_fail(code, msg); }
+static int quad_points(const champ_ctx *c) { return c->nquad > 0 ? c->nquad : 12; }
 
 
 static double host_det(std::vector<double> a, int n) {
@@ -708,7 +709,34 @@ static int build_move_state(champ_ctx *c, State<double> &d, State<float> &f) {
   return CHAMP_OK;
 }
 
+// Phase timing: events recorded on the context's stream around a launch when "phase_timing" is on.
+enum { PH_SWEEP = 0, PH_MOVES = 1, PH_EVAL = 2, PH_TC = 3, PH_N = 4 };
+static int ev_mark(champ_ctx *c, int phase, bool start) {
+  if (!c->ptime) return CHAMP_OK;
+  size_t i;
+  if (start) {
+    i = c->ev_use.empty() ? 0 : (size_t)c->ev_use.back().second + 2;
+    while (c->ev_pool.size() < i + 2) {
+      cudaEvent_t e;
+      CK(cudaEventCreate(&e));
+      c->ev_pool.push_back((void *)e);
+    }
+    c->ev_use.push_back({phase, (int)i});
+  } else {
+    i = (size_t)c->ev_use.back().second + 1;
+  }
+  CK(cudaEventRecord((cudaEvent_t)c->ev_pool[i], c->stream));
+  return CHAMP_OK;
+}
+
 static int launch(champ_ctx *c, Op op, const OpArgs &a = OpArgs()) {
+  if (op == Op::Vmc && a.phase < 0 && c->prec != CHAMP_PREC_MIXED && !c->tc_on) {
+    // the fused sweep kernel: moves and E_L in one launch
+    int rc = ev_mark(c, PH_SWEEP, true);
+    if (!rc) rc = c->prec == CHAMP_PREC_FP64 ? launch_f64(c, op, a) : launch_f32(c, op, a);
+    if (!rc) rc = ev_mark(c, PH_SWEEP, false);
+    return rc;
+  }
   if (c->prec == CHAMP_PREC_FP64) return launch_f64(c, op, a);
   if (c->prec == CHAMP_PREC_FP32) return launch_f32(c, op, a);
   // mixed precision: moves on the FP32 instantiation, full evaluations on the FP64 one
@@ -721,6 +749,7 @@ static int launch(champ_ctx *c, Op op, const OpArgs &a = OpArgs()) {
   case Op::ProposeGrad:
   case Op::Accept:
   case Op::DmcCopy:
+  case Op::PGradBwd:  // the parameter derivatives' reverse sweep in FP32 (E_L stays FP64)
     return launch_f32(c, op, a);
   case Op::DmcMove: {
     OpArgs b = a;
@@ -741,10 +770,14 @@ static int launch(champ_ctx *c, Op op, const OpArgs &a = OpArgs()) {
     for (int isw = 0; isw < a.nsweep; isw++) {
       b.sweep0 = a.sweep0 + (uint64_t)isw;
       b.phase = 1;  // the sweep's moves, FP32
-      int rc = launch_f32(c, op, b);
+      int rc = ev_mark(c, PH_MOVES, true);
+      if (!rc) rc = launch_f32(c, op, b);
+      if (!rc) rc = ev_mark(c, PH_MOVES, false);
       if (rc) return rc;
       b.phase = 3;  // its E_L, FP64 from the positions
-      rc = launch_f64(c, op, b);
+      rc = ev_mark(c, PH_EVAL, true);
+      if (!rc) rc = launch_f64(c, op, b);
+      if (!rc) rc = ev_mark(c, PH_EVAL, false);
       if (rc) return rc;
     }
     return CHAMP_OK;
@@ -1254,6 +1287,7 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
     }
   }
   ecp.nquad = quadrature_rule(d->nloc == 6 ? d->nquad : 12, ecp.q0, ecp.wq);
+  c->nquad = ecp.nquad;
   double pecent = 0;
   for (int i = 0; i < d->ncent; i++)
     for (int j = 0; j < i; j++) {
@@ -1334,6 +1368,13 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
       c->pg_scr = dalloc<double>(c, W * c->scr_stride);
       if (!c->pg_scr) { champ_destroy(c); return fail(CHAMP_ENOMEM, "allocation of the derivative scratch failed"); }
     }
+    c->pg_tv = dalloc<double>(c, W * 4 * (size_t)c->N);
+    c->pg_tn = dalloc<int>(c, W);
+    c->pg_tc = c->nloc > 0 ? dalloc<double>(c, W * (size_t)c->N * c->C * quad_points(c)) : nullptr;
+    if (!c->pg_tv || !c->pg_tn || (c->nloc > 0 && !c->pg_tc)) {
+      champ_destroy(c);
+      return fail(CHAMP_ENOMEM, "allocation of the parameter-gradient tape failed");
+    }
     if (!c->pg_dl || !c->pg_de || !c->pg_el || !c->pg_wt || !c->oh_oa || !c->oh_ow || !c->oh_mb || !c->oh_s || !c->oh_h) {
       champ_destroy(c);
       return fail(CHAMP_ENOMEM, "allocation of the parameter-derivative buffers failed");
@@ -1348,6 +1389,7 @@ int champ_destroy(champ_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   else cudaDeviceSynchronize();
   dmc_graph_release(c);
+  for (void *e : c->ev_pool) cudaEventDestroy((cudaEvent_t)e);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   for (void *p : c->allocs) cudaFree(p);
   if (c->cublas) cublasDestroy((cublasHandle_t)c->cublas);
@@ -1355,10 +1397,7 @@ int champ_destroy(champ_ctx *c) {
   return CHAMP_OK;
 }
 
-int champ_param_grad(champ_ctx *c, double *dlnpsi, double *deloc, double *eloc) {
-  if (!c) return fail(CHAMP_EINVAL, "null context");
-  if (!c->have_walkers) return fail(CHAMP_ESTATE, "no walkers set");
-  if (c->smem_pg == 0) return fail(CHAMP_EINVAL, "parameter derivatives: system too large for the kernel's shared memory");
+static OpArgs pg_args(champ_ctx *c, int part) {
   OpArgs a;
   a.pgout.dlnpsi = c->pg_dl;
   a.pgout.deloc = c->pg_de;
@@ -1366,26 +1405,87 @@ int champ_param_grad(champ_ctx *c, double *dlnpsi, double *deloc, double *eloc) 
   a.pgout.nfree = c->nfree;
   a.pgout.scr = c->pg_scr;
   a.pgout.scr_stride = c->scr_stride;
-  a.pgout.part = 1;
+  a.pgout.part = part;
   a.pgout.lanesum = c->pg_lanesum;
+  a.pgout.tape_v = c->pg_tv;
+  a.pgout.tape_n = c->pg_tn;
+  a.pgout.tape_nlt = c->prec == CHAMP_PREC_FP32 ? c->stf.nlt : c->std_.nlt;
+  a.pgout.tape_c = c->pg_tc;
+  return a;
+}
+
+// The nonlocal part of the orbital-resolved local energy for all walkers, then the CSF and
+// orbital-rotation derivatives (part 2 of the derivative kernel).
+static int pg_orbital_part(champ_ctx *c) {
+  if (!c->pg_scr) return CHAMP_OK;
+  // nonlocal part of B for all walkers at once: Bm[w] += phis[w] (N x B) coef (B x M), row-major,
+  // as the column-major product Bm^T (M x N) += coef^T (M x B) phis^T (B x N)
+  int rc = cublas_handle(c);
+  if (rc) return rc;
+  const int N = c->N, B = c->nbasis, M = c->norb;
+  const double one = 1.0;
+  if (cublasDgemmStridedBatched((cublasHandle_t)c->cublas, CUBLAS_OP_N, CUBLAS_OP_N, M, N, B, &one, c->call_d, M, 0,
+                                c->pg_scr, B, (long long)c->scr_stride, &one,
+                                c->pg_scr + (size_t)N * B + (size_t)N * 5 * M, M, (long long)c->scr_stride,
+                                c->W) != CUBLAS_STATUS_SUCCESS)
+    return fail(CHAMP_ECUDA, "cublasDgemmStridedBatched failed");
+  OpArgs a = pg_args(c, 2);
+  return launch(c, Op::PGrad, a);
+}
+
+int champ_param_grad_fwd(champ_ctx *c, double *eloc) {
+  if (!c) return fail(CHAMP_EINVAL, "null context");
+  if (!c->have_walkers) return fail(CHAMP_ESTATE, "no walkers set");
+  if (c->smem_pg == 0) return fail(CHAMP_EINVAL, "parameter derivatives: system too large for the kernel's shared memory");
+  OpArgs a = pg_args(c, 3);
   int rc = launch(c, Op::PGrad, a);
   if (rc) return rc;
-  if (c->pg_scr) {
-    // nonlocal part of B for all walkers at once: Bm[w] += phis[w] (N x B) coef (B x M), row-major,
-    // as the column-major product Bm^T (M x N) += coef^T (M x B) phis^T (B x N)
-    rc = cublas_handle(c);
-    if (rc) return rc;
-    const int N = c->N, B = c->nbasis, M = c->norb;
-    const double one = 1.0;
-    if (cublasDgemmStridedBatched((cublasHandle_t)c->cublas, CUBLAS_OP_N, CUBLAS_OP_N, M, N, B, &one, c->call_d, M, 0,
-                                  c->pg_scr, B, (long long)c->scr_stride, &one,
-                                  c->pg_scr + (size_t)N * B + (size_t)N * 5 * M, M, (long long)c->scr_stride,
-                                  c->W) != CUBLAS_STATUS_SUCCESS)
-      return fail(CHAMP_ECUDA, "cublasDgemmStridedBatched failed");
-    a.pgout.part = 2;
-    rc = launch(c, Op::PGrad, a);
-    if (rc) return rc;
+  c->have_tape = true;
+  c->have_pgrad = false;
+  if (eloc) {
+    CK(cudaMemcpyAsync(eloc, c->pg_el, sizeof(double) * c->W, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
   }
+  return CHAMP_OK;
+}
+
+int champ_param_grad_bwd(champ_ctx *c, double *dlnpsi, double *deloc) {
+  if (!c) return fail(CHAMP_EINVAL, "null context");
+  if (!c->have_tape) return fail(CHAMP_ESTATE, "call champ_param_grad_fwd first");
+  OpArgs a = pg_args(c, 4);
+  int rc = launch(c, Op::PGradBwd, a);
+  if (!rc) rc = pg_orbital_part(c);
+  if (rc) return rc;
+  c->have_tape = false;
+  size_t W = c->W, P = c->nfree;
+  if (dlnpsi) CK(cudaMemcpyAsync(dlnpsi, c->pg_dl, sizeof(double) * W * P, cudaMemcpyDeviceToHost, c->stream));
+  if (deloc) CK(cudaMemcpyAsync(deloc, c->pg_de, sizeof(double) * W * P, cudaMemcpyDeviceToHost, c->stream));
+  if (dlnpsi || deloc) CK(cudaStreamSynchronize(c->stream));
+  c->have_pgrad = true;
+  return CHAMP_OK;
+}
+
+int champ_param_grad(champ_ctx *c, double *dlnpsi, double *deloc, double *eloc) {
+  if (!c) return fail(CHAMP_EINVAL, "null context");
+  if (!c->have_walkers) return fail(CHAMP_ESTATE, "no walkers set");
+  if (c->smem_pg == 0) return fail(CHAMP_EINVAL, "parameter derivatives: system too large for the kernel's shared memory");
+  if (c->pg_mode == 0) {
+    int rc = champ_param_grad_fwd(c, nullptr);
+    if (!rc) rc = champ_param_grad_bwd(c, nullptr, nullptr);
+    if (rc) return rc;
+    size_t W = c->W, P = c->nfree;
+    if (dlnpsi) CK(cudaMemcpyAsync(dlnpsi, c->pg_dl, sizeof(double) * W * P, cudaMemcpyDeviceToHost, c->stream));
+    if (deloc) CK(cudaMemcpyAsync(deloc, c->pg_de, sizeof(double) * W * P, cudaMemcpyDeviceToHost, c->stream));
+    if (eloc) CK(cudaMemcpyAsync(eloc, c->pg_el, sizeof(double) * W, cudaMemcpyDeviceToHost, c->stream));
+    if (dlnpsi || deloc || eloc) CK(cudaStreamSynchronize(c->stream));
+    return CHAMP_OK;
+  }
+  // one pass: E_L and the Jastrow derivatives together (option "param_grad_mode" 1)
+  OpArgs a = pg_args(c, 1);
+  int rc = launch(c, Op::PGrad, a);
+  if (rc) return rc;
+  rc = pg_orbital_part(c);
+  if (rc) return rc;
   size_t W = c->W, P = c->nfree;
   if (dlnpsi) CK(cudaMemcpyAsync(dlnpsi, c->pg_dl, sizeof(double) * W * P, cudaMemcpyDeviceToHost, c->stream));
   if (deloc) CK(cudaMemcpyAsync(deloc, c->pg_de, sizeof(double) * W * P, cudaMemcpyDeviceToHost, c->stream));
@@ -1711,7 +1811,34 @@ int champ_set_option(champ_ctx *c, const char *name, int64_t value) {
     c->tc_kchunk = (int)value;
     return CHAMP_OK;
   }
+  if (!strcmp(name, "phase_timing")) {
+    c->ptime = value ? 1 : 0;
+    c->ev_use.clear();
+    return CHAMP_OK;
+  }
+  if (!strcmp(name, "param_grad_mode")) {
+    if (value < 0 || value > 1) return fail(CHAMP_EINVAL, "param_grad_mode: 0 or 1");
+    c->pg_mode = (int)value;
+    return CHAMP_OK;
+  }
   return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);
+}
+
+int champ_phase_times(champ_ctx *c, double *ms, int32_t *launches) {
+  if (!c || !ms) return fail(CHAMP_EINVAL, "null argument");
+  CK(cudaStreamSynchronize(c->stream));
+  for (int p = 0; p < PH_N; p++) {
+    ms[p] = 0;
+    if (launches) launches[p] = 0;
+  }
+  for (const auto &u : c->ev_use) {
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, (cudaEvent_t)c->ev_pool[u.second], (cudaEvent_t)c->ev_pool[u.second + 1]));
+    ms[u.first] += t;
+    if (launches) launches[u.first]++;
+  }
+  c->ev_use.clear();
+  return CHAMP_OK;
 }
 
 int champ_get_option(const champ_ctx *c, const char *name, int64_t *value) {
@@ -1725,6 +1852,8 @@ int champ_get_option(const champ_ctx *c, const char *name, int64_t *value) {
   if (!strcmp(name, "reinvert_every")) { *value = c->reinv_every; return CHAMP_OK; }
   if (!strcmp(name, "dmc_graph")) { *value = c->dmc_graph_on; return CHAMP_OK; }
   if (!strcmp(name, "orbital_tc_chunk")) { *value = c->tc_kchunk; return CHAMP_OK; }
+  if (!strcmp(name, "phase_timing")) { *value = c->ptime; return CHAMP_OK; }
+  if (!strcmp(name, "param_grad_mode")) { *value = c->pg_mode; return CHAMP_OK; }
   return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);
 }
 

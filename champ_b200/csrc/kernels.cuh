@@ -482,6 +482,7 @@ __device__ void build_gamma(const Sys<T> &s, const View<T> &v, int lane, double 
 struct EvalRes {
   double lnpsi, sign, psij, d2lnpsi, pe, pe_ee, pe_nl, eloc, d2j, vj2;
   bool singular;
+  int ntask;  // (electron, centre) pairs inside the nonlocal range (task records in the view's nlt)
 };
 
 // Shared-memory accumulators of the Jastrow parameter derivatives of one walker.
@@ -498,6 +499,8 @@ struct PGBuf {
   int P, na, nb;
   double *phis;  // [N][nbasis] or null: sum over the electron's quadrature points of
                  // w e^dJ v_l(r) P_l times each basis function (nonlocal part of B in basis space)
+  double *tape;  // [N*C][nquad] or null: the forward pass of the parameter gradient stores each
+                 // point's coefficient here (per task and point) instead of adding its parameter sums
 };
 
 template <class T, int NORD, bool SLOTS>
@@ -702,6 +705,7 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
 
   // --- pseudopotential (nonloc_pot.f90, nonloc.f90), quadrature rotated by R
   double vloc = 0, vnl = 0;
+  int ntask_all = 0;
   if (s.nloc > 0 && ok) {
     const int B = s.nbasis;
     T *gp = v.gproj;
@@ -776,6 +780,7 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
       ntask += __popc(m);
     }
     vloc = warp_sum(vloc);
+    ntask_all = ntask;
     __syncwarp();
     const int nq = E.nquad;
     // The points of an (electron, centre) task lie at the task's distance r from that centre, so
@@ -904,9 +909,13 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
       if (PG) {
         double coeff = E.wq[q] * exp(dj) * vp * (double)dr;
         atomicAdd(&pg->csum[e], coeff);
-        const T *ts = (SHARE && fast) ? tsum : nullptr;
-        if (std::is_same<T, float>::value || pg->dvl) point_param_values<T, NORD, true>(s, J, v, e, xn, coeff, *pg, ts);
-        else point_param_values<T, NORD, false>(s, J, v, e, xn, coeff, *pg, ts);
+        if (pg->tape) {
+          pg->tape[t] = coeff;  // the backward pass forms the parameter sums at this point
+        } else {
+          const T *ts = (SHARE && fast) ? tsum : nullptr;
+          if (pg->dvl) point_param_values<T, NORD, true>(s, J, v, e, xn, coeff, *pg, ts);
+          else point_param_values<T, NORD, false>(s, J, v, e, xn, coeff, *pg, ts);
+        }
       }
     }
     vnl = warp_sum(vnl);
@@ -939,6 +948,7 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
     res.vj2 = warp_sum(vj2);
   }
   res.singular = !ok;
+  res.ntask = ntask_all;
   if (lane == 0) {
     st.fsum[w] = fsum;
     st.lnd[w] = ok ? lnd : -INFINITY;
@@ -1209,41 +1219,21 @@ __global__ void __launch_bounds__(128, 4) k_accept(Sys<T> s, State<T> st, Layout
 // (tensor-core contraction).  Phase 3 runs only the E_L, from the positions alone (re-inverting,
 // and refreshing the FP32 move tables when the state has them): the FP64 half of a mixed-precision
 // sweep whose moves ran in FP32.  Statistics are added to st.s_*.
-template <class T, int NORD, bool MD>
+// (One kernel per phase, PH, so that each holds only the code it runs.)
+template <class T, int NORD, bool MD, int PH>
 __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L, int nsweep, uint64_t seed,
-                                                uint64_t sweep0, double step, int phase, int reinv_every) {
+                                                uint64_t sweep0, double step, int reinv_every) {
   __shared__ JasPar<T> J;
   __shared__ EcpPar E;
   extern __shared__ __align__(16) char dsm[];
   load_params(s, J, E);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   const int N = s.N;
+  constexpr int phase = PH;
+  constexpr bool moves = phase == 0 || phase == 1, eval = phase != 1;
   for (int w = blockIdx.x * wpb + wib; w < st.W; w += gridDim.x * wpb) {
     View<T> v = make_view<T>(dsm + L.bytes * wib, L, st, w, s.N, s.C, s.nbasis, s.nomax, L.resident != 0);
-    if (phase == 3) {
-      for (int i = lane; i < 3 * N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * N + i];
-      __syncwarp();
-      double es = 0, e2 = 0, el = 0;
-      for (int isw = 0; isw < nsweep; isw++) {
-        double R[9];
-        random_rotation(seed, (uint32_t)w, sweep0 + (uint64_t)isw, R);
-        EvalRes res;
-        full_eval<T, NORD, MD>(s, J, E, st, w, v, R, lane, false, res, nullptr, false, true);
-        el = res.eloc;
-        es += el;
-        e2 += el * el;
-      }
-      if (L.resident) eval_store(v, st, w, N, s.C, lane);
-      else mirror_store(v, st, w, N, s.C, lane);
-      if (lane == 0) {
-        st.s_esum[w] += es;
-        st.s_e2sum[w] += e2;
-        st.s_elast[w] = el;
-      }
-      __syncwarp();
-      continue;
-    }
-    if (L.resident) {
+    if (L.resident && phase != 3) {
       view_load(v, st, w, N, s.C, lane);
     } else {
       for (int i = lane; i < 3 * N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * N + i];
@@ -1252,7 +1242,7 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
     double es = 0, e2 = 0, acc = 0, el = 0;
     for (int isw = 0; isw < nsweep; isw++) {
       uint64_t sweep = sweep0 + (uint64_t)isw;
-      for (int e = 0; e < N && phase != 2; e++) {
+      for (int e = 0; moves && e < N; e++) {
         double g[3], ua;
         move_randoms(seed, (uint32_t)w, sweep, (uint32_t)e, g, &ua);
         double xn[3] = {v.xs[3 * e] + step * g[0], v.xs[3 * e + 1] + step * g[1], v.xs[3 * e + 2] + step * g[2]};
@@ -1264,18 +1254,22 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
           acc += 1;
         }
       }
-      if (phase == 1) continue;
+      if constexpr (!eval) continue;
       double R[9];
       random_rotation(seed, (uint32_t)w, sweep, R);
       EvalRes res;
-      // periodic FP64 re-inversion: every reinv_every sweeps, in between the updated inverses
-      const bool reinv = reinv_every <= 1 || sweep % (uint64_t)reinv_every == 0;
+      // periodic FP64 re-inversion: every reinv_every sweeps, in between the updated inverses;
+      // phase 3 evaluates from the positions alone and always re-inverts
+      const bool reinv = phase == 3 || reinv_every <= 1 || sweep % (uint64_t)reinv_every == 0;
       full_eval<T, NORD, MD>(s, J, E, st, w, v, R, lane, false, res, nullptr, phase == 2, reinv);
       el = res.eloc;
       es += el;
       e2 += el * el;
     }
-    if (L.resident) {
+    if (phase == 3) {
+      if (L.resident) eval_store(v, st, w, N, s.C, lane);
+      else mirror_store(v, st, w, N, s.C, lane);
+    } else if (L.resident) {
       view_store(v, st, w, N, s.C, lane);
     } else {
       for (int i = lane; i < 3 * N; i += 32) st.x[(size_t)w * 3 * N + i] = v.xs[i];
@@ -1284,7 +1278,7 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
       st.s_esum[w] += es;
       st.s_e2sum[w] += e2;
       st.s_acc[w] += acc;
-      if (phase != 1) st.s_elast[w] = el;
+      if (eval) st.s_elast[w] = el;
     }
     __syncwarp();
   }

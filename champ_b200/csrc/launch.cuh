@@ -19,7 +19,10 @@ static int set_smem_attrs(champ_ctx *c) {
   int rc = set_attrs(c, k_eval<T, NORD, MD>, sm);
   if (!rc) rc = set_attrs(c, k_propose<T, NORD, MD>, sm);
   if (!rc) rc = set_attrs(c, k_accept<T, MD>, sm);
-  if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD>, sm);
+  if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD, 0>, sm);
+  if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD, 1>, sm);
+  if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD, 2>, sm);
+  if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD, 3>, sm);
   if (!rc) rc = set_attrs(c, k_dmc_move<T, NORD, MD>, sm);
   if (!rc && std::is_same<T, float>::value && c->prec == CHAMP_PREC_FP32) {
     CK(cudaFuncSetAttribute(orbtc::k_orb_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024 + 128));
@@ -31,10 +34,11 @@ static int set_smem_attrs(champ_ctx *c) {
     CK(cudaFuncSetAttribute(k_basis_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)std::min<size_t>(4 * (size_t)c->nbasis * 5 * sizeof(float), 227 * 1024)));
   }
-  if (!rc && c->smem_pg > 0 && (std::is_same<T, double>::value || c->prec == CHAMP_PREC_FP32)) {
-    CK(cudaFuncSetAttribute(k_pgrad<T, NORD, MD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_pg));
-    CK(cudaFuncSetAttribute(k_pgrad<T, NORD, MD>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                            (int)cudaSharedmemCarveoutMaxShared));
+  if (!rc && c->smem_pg > 0) {
+    for (auto kern : {k_pgrad<T, NORD, MD, 1>, k_pgrad<T, NORD, MD, 2>, k_pgrad<T, NORD, MD, 3>, k_pgrad<T, NORD, MD, 4>}) {
+      CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_pg));
+      CK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
+    }
   }
   return rc;
 }
@@ -141,9 +145,14 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
     k_accept<T, MD><<<grid, block, K.smem, c->stream>>>(s, st, K.lay, a.e, a.mask);
     break;
   case Op::PGrad:
-    k_pgrad<T, NORD, MD><<<dim3((c->W + c->wpb_pg - 1) / c->wpb_pg), dim3(32 * c->wpb_pg), c->smem_pg, c->stream>>>(s, st, K.lay, a.pgout, R[0], R[1], R[2], R[3], R[4],
-                                                                 R[5], R[6], R[7], R[8], a.pgout.part);
+  case Op::PGradBwd: {
+    const dim3 pgrid((c->W + c->wpb_pg - 1) / c->wpb_pg), pblock(32 * c->wpb_pg);
+    auto kern = a.pgout.part == 1 ? k_pgrad<T, NORD, MD, 1>
+              : a.pgout.part == 2 ? k_pgrad<T, NORD, MD, 2>
+              : a.pgout.part == 3 ? k_pgrad<T, NORD, MD, 3> : k_pgrad<T, NORD, MD, 4>;
+    kern<<<pgrid, pblock, c->smem_pg, c->stream>>>(s, st, K.lay, a.pgout, R[0], R[1], R[2], R[3], R[4], R[5], R[6], R[7], R[8]);
     break;
+  }
   case Op::DmcMove:
     k_dmc_move<T, NORD, MD><<<dim3((c->dpar.wmax + K.wpb - 1) / K.wpb), block, K.smem, c->stream>>>(
         s, st, K.lay, c->dpar, c->dA, a.phase < 0 ? 0 : a.phase);
@@ -154,8 +163,9 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
   }
   case Op::Vmc: {
     if (a.phase >= 0) {
-      k_vmc<T, NORD, MD><<<grid, block, K.smem, c->stream>>>(s, st, K.lay, a.nsweep, a.seed, a.sweep0, a.step, a.phase,
-                                                              c->reinv_every);
+      auto kern = a.phase == 1 ? k_vmc<T, NORD, MD, 1> : a.phase == 2 ? k_vmc<T, NORD, MD, 2>
+                : a.phase == 3 ? k_vmc<T, NORD, MD, 3> : k_vmc<T, NORD, MD, 0>;
+      kern<<<grid, block, K.smem, c->stream>>>(s, st, K.lay, a.nsweep, a.seed, a.sweep0, a.step, c->reinv_every);
       break;
     }
     CK(cudaMemsetAsync(st.s_esum, 0, sizeof(double) * st.W, c->stream));
@@ -163,19 +173,19 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
     CK(cudaMemsetAsync(st.s_acc, 0, sizeof(double) * st.W, c->stream));
     const bool tc = c->tc_on && !a.st_override;  // only FP32 contexts turn it on
     if (!tc) {
-      k_vmc<T, NORD, MD><<<grid, block, K.smem, c->stream>>>(s, st, K.lay, a.nsweep, a.seed, a.sweep0, a.step, 0,
-                                                               c->reinv_every);
+      k_vmc<T, NORD, MD, 0><<<grid, block, K.smem, c->stream>>>(s, st, K.lay, a.nsweep, a.seed, a.sweep0, a.step,
+                                                                  c->reinv_every);
       break;
     }
     // per sweep: moves, orbitals of all walkers on the tensor cores, E_L
     for (int isw = 0; isw < a.nsweep; isw++) {
-      k_vmc<T, NORD, MD><<<grid, block, K.smem, c->stream>>>(s, st, K.lay, 1, a.seed, a.sweep0 + isw, a.step, 1,
-                                                               c->reinv_every);
+      k_vmc<T, NORD, MD, 1><<<grid, block, K.smem, c->stream>>>(s, st, K.lay, 1, a.seed, a.sweep0 + isw, a.step,
+                                                                  c->reinv_every);
       CK(cudaGetLastError());
       int rc = run_orb_tc<T>(c, st);
       if (rc) return rc;
-      k_vmc<T, NORD, MD><<<grid, block, K.smem, c->stream>>>(s, st, K.lay, 1, a.seed, a.sweep0 + isw, a.step, 2,
-                                                               c->reinv_every);
+      k_vmc<T, NORD, MD, 2><<<grid, block, K.smem, c->stream>>>(s, st, K.lay, 1, a.seed, a.sweep0 + isw, a.step,
+                                                                  c->reinv_every);
       CK(cudaGetLastError());
     }
     break;

@@ -358,9 +358,55 @@ struct PGOut {
   int nfree;
   double *scr;     // per-walker scratch of the CSF/orbital part (null when there is none)
   size_t scr_stride;
-  int part;        // 1: E_L, Jastrow derivatives, local B; 2: CSF and orbital derivatives
+  int part;        // 1: E_L, Jastrow derivatives, local B; 2: CSF and orbital derivatives;
+                   // 3: forward pass (E_L, local B, tape); 4: backward pass (Jastrow derivatives)
   int lanesum;     // per-lane slots for the NLPP parameter sums (see padd)
+  // tape of the forward pass: per walker the velocities and per-electron point-coefficient sums
+  // ([W][4N]), the number of nonlocal tasks ([W]), the task records ([W][N*C][NLT], the
+  // evaluation's own) and each point's coefficient ([W][N*C][nquad])
+  double *tape_v;
+  int *tape_n;
+  const double *tape_nlt;
+  double *tape_c;
 };
+
+// dE_L/dp from the accumulated sums (K -> -1/2 K + the nonlocal part) and the outputs of the
+// free Jastrow parameters: a, b as they are, c through the cusp projection (checkdepend4).
+template <class T, int NORD>
+__device__ void pg_finish(const Sys<T> &s, const JasPar<T> &J, const PGBuf &pg, const PGOut &out, int w, int lane,
+                          bool MDcsf) {
+  const int N = s.N, P = pg.P, na = pg.na, nb = pg.nb, nt = make_terms(NORD).n;
+  for (int p = lane; p < P; p += 32) {
+    double dv = pg.dvn[p];
+    for (int e = 0; e < N; e++) dv -= pg.csum[e] * pg.old[e * P + p];
+    pg.K[p] = -HB * pg.K[p] + dv;
+  }
+  __syncwarp();
+  // output order: CSF, orbital rotations, Jastrow (as deriv_mod.f90:120-247 concatenates them)
+  double *ol = out.dlnpsi + (size_t)w * out.nfree, *oe = out.deloc + (size_t)w * out.nfree;
+  const int jo = (MDcsf && s.ncsf > 1 ? s.ncsf - 1 : 0) + s.norbp;
+  ol += jo;
+  oe += jo;
+  for (int f = lane; f < out.nfree - jo; f += 32) {
+    double g, d;
+    if (f < na + nb) {
+      g = pg.G[f];
+      d = pg.K[f];
+    } else {
+      int fc = f - na - nb, it = fc / s.ncfree, jf = fc - it * s.ncfree;
+      g = 0;
+      d = 0;
+      for (int ll = 0; ll < nt; ll++) {
+        double pm = s.cproj[ll * s.ncfree + jf];
+        g += pm * pg.G[na + nb + it * nt + ll];
+        d += pm * pg.K[na + nb + it * nt + ll];
+      }
+    }
+    ol[f] = g;
+    oe[f] = d;
+  }
+  __syncwarp();
+}
 
 // CSF and orbital-rotation derivatives from the orbital-resolved local energy
 // B[e][m] = -1/2 (lap phi_m + 2 v_J . grad phi_m + ddjas phi_m) + V_loc/N phi_m + V_NL,m
@@ -624,12 +670,14 @@ __device__ void orbital_csf_derivs(const Sys<T> &s, const View<T> &v, double elo
   __syncwarp();
 }
 
-template <class T, int NORD, bool MD>
 // part 1: E_L with the Jastrow parameter derivatives and the local part of B; part 2 (after the
-// nonlocal part of B was added for all walkers): CSF and orbital-rotation derivatives.
+// nonlocal part of B was added for all walkers): CSF and orbital-rotation derivatives; part 3: the
+// forward pass (E_L, local part of B, tape); part 4: the reverse sweep of the Jastrow parameters.
+// One kernel per part, so that each holds only its own code.
+template <class T, int NORD, bool MD, int PART>
 __global__ void __launch_bounds__(128, 4) k_pgrad(Sys<T> s, State<T> st, Layout L, PGOut out, double r0, double r1,
                                                   double r2, double r3, double r4, double r5, double r6, double r7,
-                                                  double r8, int part) {
+                                                  double r8) {
   __shared__ JasPar<T> J;
   __shared__ EcpPar E;
   extern __shared__ __align__(16) char dsm[];
@@ -654,56 +702,77 @@ __global__ void __launch_bounds__(128, 4) k_pgrad(Sys<T> s, State<T> st, Layout 
     pg.old = q; q += N * P;
     pg.dvl = out.lanesum ? q : nullptr;
     pg.P = P; pg.na = na; pg.nb = nb;
+    pg.tape = nullptr;
     double *scr = out.scr ? out.scr + (size_t)w * out.scr_stride : nullptr;
     pg.phis = scr;
-    if (part == 2) {
+    if constexpr (PART == 2) {
       orbital_csf_derivs<T, MD>(s, v, out.eloc[w], lane, scr, out.dlnpsi + (size_t)w * out.nfree,
                                 out.deloc + (size_t)w * out.nfree);
-      continue;
-    }
+    } else if constexpr (PART == 4) {
+      const int NC = N * s.C, nq = E.nquad;
+      // backward pass: one reverse sweep from the tape.  Seeds: -1/2 on every electron's
+      // Laplacian of J, -v_e on its gradient, and each nonlocal point's coefficient on the change
+      // of J when its electron moves there; the parameter basis functions (every pair, e-n term
+      // and point) are recomputed from the positions, in this pass's precision.
+      for (int i = lane; i < (int)(pgbytes / sizeof(double)); i += 32) pg.vt[i] = 0.0;
+      __syncwarp();
+      for (int i = lane; i < 4 * N; i += 32) pg.vt[i] = out.tape_v[(size_t)w * 4 * N + i];  // vt, then csum
+      for (int i = lane; i < 3 * N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * N + i];
+      __syncwarp();
+      if (s.nloc > 0) {
+        const int ntask = out.tape_n[w];
+        const double *tl = out.tape_nlt + (size_t)w * NC * NLT;
+        const double *tc = out.tape_c + (size_t)w * NC * nq;
+        for (int t = lane; t < ntask * nq; t += 32) {
+          const double coeff = tc[t];
+          if (coeff == 0.0) continue;
+          const int task = t / nq, q = t - task * nq;
+          const double *rec = tl + (size_t)task * NLT;
+          const int idx = (int)rec[0], e = idx / s.C, c = idx - e * s.C;
+          const double r = rec[1], *cc = s.cent + 3 * c;
+          double xn[3];
+#pragma unroll
+          for (int k = 0; k < 3; k++)
+            xn[k] = cc[k] + r * (R[3 * k] * E.q0[q][0] + R[3 * k + 1] * E.q0[q][1] + R[3 * k + 2] * E.q0[q][2]);
+          if (pg.dvl) point_param_values<T, NORD, true>(s, J, v, e, xn, coeff, pg, nullptr);
+          else point_param_values<T, NORD, false>(s, J, v, e, xn, coeff, pg, nullptr);
+        }
+        if (pg.dvl) {
+          __syncwarp();
+          for (int p = lane; p < P; p += 32) {
+            double a = 0;
+            for (int l = 0; l < 32; l++) a += pg.dvl[p * 32 + l];
+            pg.dvn[p] += a;
+          }
+        }
+      }
+      __syncwarp();
+      jastrow_param_pass<T, NORD>(s, J, v, pg, lane);
+      pg_finish<T, NORD>(s, J, pg, out, w, lane, MD);
+    } else {
+    const int NC = N * s.C, nq = E.nquad;
     for (int i = lane; i < (int)(pgbytes / sizeof(double)); i += 32) pg.vt[i] = 0.0;
     if (scr)
       for (int i = lane; i < N * s.nbasis; i += 32) scr[i] = 0.0;
     for (int i = lane; i < 3 * N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * N + i];
+    if (PART == 3 && s.nloc > 0) pg.tape = out.tape_c + (size_t)w * NC * nq;
     __syncwarp();
     EvalRes res;
     full_eval<T, NORD, MD, true>(s, J, E, st, w, v, R, lane, false, res, &pg);
     __syncwarp();
-    jastrow_param_pass<T, NORD>(s, J, v, pg, lane);
-    // dE_L/dp for the raw parameters, into pg.K; d ln psi / dp stays in pg.G
-    for (int p = lane; p < P; p += 32) {
-      double dv = pg.dvn[p];
-      for (int e = 0; e < N; e++) dv -= pg.csum[e] * pg.old[e * P + p];
-      pg.K[p] = -HB * pg.K[p] + dv;
-    }
-    __syncwarp();
-    // output order: CSF, orbital rotations, Jastrow (as deriv_mod.f90:120-247 concatenates them)
-    double *ol = out.dlnpsi + (size_t)w * out.nfree, *oe = out.deloc + (size_t)w * out.nfree;
     if (scr) orbital_local_energy<T>(s, v, res, lane, scr);
-    const int jo = (MD && s.ncsf > 1 ? s.ncsf - 1 : 0) + s.norbp;
-    ol += jo;
-    oe += jo;
-    // free Jastrow parameters: a, b as they are; c through the cusp projection (cdep, checkdepend4)
-    for (int f = lane; f < out.nfree - jo; f += 32) {
-      double g, d;
-      if (f < na + nb) {
-        g = pg.G[f];
-        d = pg.K[f];
-      } else {
-        int fc = f - na - nb, it = fc / s.ncfree, jf = fc - it * s.ncfree;
-        g = 0;
-        d = 0;
-        for (int ll = 0; ll < nt; ll++) {
-          double pm = s.cproj[ll * s.ncfree + jf];
-          g += pm * pg.G[na + nb + it * nt + ll];
-          d += pm * pg.K[na + nb + it * nt + ll];
-        }
-      }
-      ol[f] = g;
-      oe[f] = d;
-    }
     if (lane == 0) out.eloc[w] = res.eloc;
-    __syncwarp();
+    if constexpr (PART == 3) {
+      // forward pass: the tape for the backward pass
+      for (int i = lane; i < 4 * N; i += 32) out.tape_v[(size_t)w * 4 * N + i] = pg.vt[i];
+      if (lane == 0) out.tape_n[w] = res.ntask;
+      mirror_store(v, st, w, N, s.C, lane);
+      __syncwarp();
+    } else {
+      jastrow_param_pass<T, NORD>(s, J, v, pg, lane);
+      pg_finish<T, NORD>(s, J, pg, out, w, lane, MD);
+    }
+    }
   }
 }
 

@@ -23,7 +23,7 @@ EXPORTED_SYMBOLS = [
     "champ_propose_1e", "champ_accept_1e", "champ_grad_1e", "champ_vmc_sweeps", "champ_vmc_run_host",
     "champ_walker_status", "champ_synchronize", "champ_param_grad", "champ_accumulate_oh",
     "champ_dmc_init", "champ_dmc_steps", "champ_num_walkers", "champ_eval_energy_noalloc", "champ_set_option",
-    "champ_get_option", "champ_oh_buffers",
+    "champ_get_option", "champ_oh_buffers", "champ_phase_times", "champ_param_grad_fwd", "champ_param_grad_bwd",
 ]
 
 PREC = {"fp64": 0, "mixed": 1, "fp32": 2}
@@ -78,6 +78,9 @@ def load_library(path: str = LIB_PATH):
     L.champ_set_option.argtypes = [vp, C.c_char_p, C.c_int64]
     L.champ_get_option.argtypes = [vp, C.c_char_p, C.POINTER(C.c_int64)]
     L.champ_oh_buffers.argtypes = [vp, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
+    L.champ_phase_times.argtypes = [vp, dp, C.POINTER(i32)]
+    L.champ_param_grad_fwd.argtypes = [vp, dp]
+    L.champ_param_grad_bwd.argtypes = [vp, dp, dp]
     for n in EXPORTED_SYMBOLS:
         if n not in ("champ_last_error", "champ_version"):
             getattr(L, n).restype = C.c_int
@@ -196,6 +199,22 @@ class Engine:
         self._check(self.lib.champ_param_grad(self.h, _p(dl), _p(de), _p(el)))
         return dl, de, el
 
+    def param_grad_fwd(self, host=True):
+        """Forward pass: E_L at the current positions and the tape for param_grad_bwd."""
+        el = np.zeros(self.nw) if host else None
+        self._check(self.lib.champ_param_grad_fwd(self.h, _p(el) if host else None))
+        return el
+
+    def param_grad_bwd(self, host=True):
+        """Reverse sweep from the tape: d ln psi/dp and dE_L/dp (walkers x P)."""
+        if not host:
+            self._check(self.lib.champ_param_grad_bwd(self.h, None, None))
+            return None
+        P = sum(self.nparam())
+        dl, de = np.zeros((self.nw, P)), np.zeros((self.nw, P))
+        self._check(self.lib.champ_param_grad_bwd(self.h, _p(dl), _p(de)))
+        return dl, de
+
     def accumulate_oh(self, weights=None):
         P1 = sum(self.nparam()) + 1
         S, H = np.zeros((P1, P1)), np.zeros((P1, P1))
@@ -239,3 +258,11 @@ class Engine:
 
     def synchronize(self):
         self._check(self.lib.champ_synchronize(self.h))
+
+    def phase_times(self):
+        """Device ms and launch counts of the VMC sweep kernels since the last call (option
+        "phase_timing" on): {"sweep", "moves", "eval"} -> (ms, launches)."""
+        ms = np.zeros(4)
+        n = (C.c_int32 * 4)()
+        self._check(self.lib.champ_phase_times(self.h, _p(ms), n))
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(("sweep", "moves", "eval"))}

@@ -273,24 +273,27 @@ def be_atom(seed=1001) -> System:
                   **_jastrow(r_jas, 1, 5, 5, 0), walkers=256, step=0.5)
 
 
-def c2_dimer(seed=1002, nordc=4) -> System:
-    """System 2: C2-like pseudopotential dimer, 60 contracted Gaussians, 1 determinant."""
+def c2_dimer(seed=1002, nordc=4, norb=16) -> System:
+    """System 2: C2-like pseudopotential dimer, 60 contracted Gaussians, 1 determinant; norb
+    orthonormal orbitals (the determinants use the first 16)."""
     rng = np.random.default_rng(seed)
     r_bas, r_orb, r_jas, r_ecp = [np.random.default_rng(s) for s in rng.integers(0, 2**63, 4)]
     per_centre = [(1, 0)] * 6 + [(2, 1)] * 3 + [(3, 2)] * 3
     bas = _basis_from_shells(_contracted_gaussian_shells(r_bas, 2, per_centre))
     nb = len(bas["basis_shell"])
-    coef = _orthonormal_rows(r_orb, 16, nb)
+    coef = _orthonormal_rows(r_orb, norb, nb)
     cent = np.array([[0.0, 0.0, 1.175], [0.0, 0.0, -1.175]])
     return System(name="c2_dimer", nelec=8, nup=4, cent=cent, iwctype=np.zeros(2, np.int32),
                   znuc=np.array([4.0]), **bas, coef=coef, det_orb=_single_det(8, 4), **_one_csf(),
                   **_jastrow(r_jas, 1, 5, 5, nordc), **_gaussian_ecp(r_ecp, 1), walkers=8192, step=0.5)
 
 
-def c2_multidet(seed=1003, ndet=200, ncsf=60, norb_act=16) -> System:
+def c2_multidet(seed=1003, ndet=200, ncsf=60, norb_act=16, norb=36) -> System:
     """System 3: system 2 with ndet seeded single/double excitations in 16 orbitals, grouped
-    into ncsf CSFs whose coefficients decay as 0.5**(excitation rank)."""
-    base = c2_dimer()
+    into ncsf CSFs whose coefficients decay as 0.5**(excitation rank); 36 orbitals, so that the
+    optimisable parameters (59 CSF, 440 orbital rotations: 120 among the 16 active orbitals and
+    16 x 20 active -> virtual, 16 Jastrow) number 515."""
+    base = c2_dimer(norb=norb)
     rng = np.random.default_rng(seed)
     nup = ndn = 4
     ref = tuple(range(nup)), tuple(range(ndn))

@@ -227,6 +227,21 @@ int champ_vmc_run_host(champ_ctx *ctx, int32_t nw, double *x /* host [nw][nelec]
    be NULL; the results stay on the device for champ_accumulate_oh. */
 int champ_param_grad(champ_ctx *ctx, double *dlnpsi /* [nw][P] */, double *deloc /* [nw][P] */,
                      double *eloc /* [nw] */);
+/* The same derivatives as a forward / backward pair (the reference's forward derivative chains,
+   qmc/vmc/deriv_jastrow4.f90, qmc/fit/deriv_nonloc.f90, qmc/deriv_orb_mod.f90:1486,1557, and
+   qmc/deriv_csf_mod.f90, replaced by one reverse sweep).  champ_param_grad_fwd evaluates E_L
+   (FP64 in FP64 and mixed precision) and keeps on the device a tape: each walker's velocities,
+   the coefficients of its nonlocal quadrature points and the orbital-resolved local energy.
+   champ_param_grad_bwd sweeps once in reverse: with the adjoint seeds -1/2 on every electron's
+   Laplacian of ln J, -grad ln psi on its gradient and each quadrature point's coefficient on
+   the change of ln J when its electron moves there, it accumulates d ln psi/dp and dE_L/dp for
+   all Jastrow parameters from the pair, e-n and point terms recomputed from the positions
+   (in FP32 for mixed precision, FP64 otherwise), then contracts the orbital-resolved local
+   energy for the CSF and orbital-rotation parameters (FP64).  champ_param_grad runs both (or,
+   with option "param_grad_mode" 1, one fused FP64/FP32 pass).  Outputs as champ_param_grad;
+   the bwd call consumes the tape (CHAMP_ESTATE without a preceding fwd). */
+int champ_param_grad_fwd(champ_ctx *ctx, double *eloc /* [nw] or NULL */);
+int champ_param_grad_bwd(champ_ctx *ctx, double *dlnpsi /* [nw][P] or NULL */, double *deloc /* [nw][P] or NULL */);
 /* O/H accumulation of the linear method (dpsi_dpsi / dpsi_deloc / dpsi_dpsi_eloc averages,
    qmc/deriv_mod.f90:683,898,1375; opt_lin_mod.f90:249,404) over the walkers of the last
    champ_param_grad, with optional weights: with Oa = (1, dlnpsi) and Mb = (E_L, E_L dlnpsi + deloc),
@@ -290,8 +305,16 @@ int champ_synchronize(champ_ctx *ctx);
    kept current by the Sherman-Morrison updates of the accepted moves; default
    ceil(100 / nelec), i.e. a re-inversion about every 100 single-electron moves.
    "dmc_graph": 1 (default) replays pairs of DMC steps as a captured CUDA graph, 0 launches the
-   kernels of every step from the host. */
+   kernels of every step from the host.
+   "phase_timing": 1 records CUDA events around the VMC sweep kernels (champ_phase_times). */
 int champ_set_option(champ_ctx *ctx, const char *name, int64_t value);
+/* Device time of the VMC sweep kernels launched since option "phase_timing" was set to 1 or
+   since the previous call (no counterpart in the reference: instrumentation for benchmarks),
+   from CUDA events on the context's stream: ms[0] the fused sweep kernel (moves and E_L in one
+   launch: FP64, and FP32 without the tensor-core orbitals), ms[1] the FP32 move kernel and ms[2]
+   the FP64 full-evaluation kernel of a mixed-precision sweep, ms[3] unused; launches[] (may be
+   NULL) the launch counts.  Synchronises the stream and resets the sums. */
+int champ_phase_times(champ_ctx *ctx, double *ms /* [4] */, int32_t *launches /* [4] or NULL */);
 /* Current value of an option ("orbital_tc", "orbital_tc_chunk", "reinvert_every", "dmc_graph"); kernel launches per champ_vmc_sweeps sweep
    ("launches_per_sweep": 1 for the fused sweep kernel, 5 with the tensor-core orbitals). */
 int champ_get_option(const champ_ctx *ctx, const char *name, int64_t *value);

@@ -112,13 +112,17 @@ def perturbed(s, name, idx, h):
     return s2
 
 
-@pytest.mark.parametrize("k", [1, 2, 3])
-def test_param_derivatives_match_finite_differences(oracle_mod, k):
+@pytest.mark.parametrize("k,prec", [(1, "fp64"), (2, "fp64"), (3, "fp64"), (1, "mixed"), (2, "mixed"), (3, "mixed"),
+                                    (5, "fp64"), (5, "mixed"), ("c2bfd", "mixed")])
+def test_param_derivatives_match_finite_differences(oracle_mod, k, prec):
+    """Systems 1-3: every parameter; the 128-electron cluster (2064 parameters) and the
+    reference's C2 example (24 Jastrow, 256 orbital-rotation parameters): a seeded subset of 24.
+    Mixed precision evaluates the derivatives in FP64 like the FP64 engine."""
     from champ_b200.engine import Engine
-    s = S.get_system(k)
-    nw = 4
-    x = S.initial_walkers(s, nw, seed=60 + k)
-    eng = Engine(s, nw, "fp64")
+    s = S.c2_bfd_example(10) if k == "c2bfd" else S.get_system(k)
+    nw = 2 if k in (5, "c2bfd") else 4
+    x = S.initial_walkers(s, nw, seed=60 + (9 if k == "c2bfd" else k))
+    eng = Engine(s, nw, prec)
     eng.set_walkers(x)
     nj, ncsf, norb = eng.nparam()
     params = all_params(s)
@@ -129,7 +133,14 @@ def test_param_derivatives_match_finite_differences(oracle_mod, k):
     for w in range(nw):
         assert abs(el[w] - o0.eval(x[w])["energy"]) <= 1e-8 * max(1, abs(el[w]))
     h = 1e-5
-    for ip, (kind, name, idx) in enumerate(params):
+    sel = range(len(params))
+    if k in (5, "c2bfd"):
+        rng = np.random.default_rng(17)
+        jas0 = len(params) - nj
+        sel = sorted(set(rng.choice(jas0, 12, replace=False).tolist()) |
+                     set((jas0 + rng.choice(nj, min(12, nj), replace=False)).tolist()))
+    for ip in sel:
+        kind, name, idx = params[ip]
         op = oracle_mod.Oracle(perturbed(s, name, idx, h))
         om = oracle_mod.Oracle(perturbed(s, name, idx, -h))
         for w in range(nw):
@@ -138,6 +149,38 @@ def test_param_derivatives_match_finite_differences(oracle_mod, k):
             e_fd = (rp["energy"] - rm["energy"]) / (2 * h)
             assert abs(dl[w, ip] - g_fd) <= 2e-5 * max(1, abs(g_fd)), (name, idx, w, dl[w, ip], g_fd)
             assert abs(de[w, ip] - e_fd) <= 2e-4 * max(1, abs(el[w])), (name, idx, w, de[w, ip], e_fd)
+
+
+@pytest.mark.parametrize("k,nw", [(2, 64), (3, 32), (5, 8), ("c2bfd", 64)])
+def test_forward_backward_pair_matches_fused_pass(k, nw):
+    """champ_param_grad_fwd + champ_param_grad_bwd (the reverse sweep over the tape) against the
+    one-pass evaluation (option param_grad_mode 1) on the same walkers: FP64 to 1e-9 relative;
+    the mixed engine's FP32 reverse sweep to 1e-5 of max(1, |value|) for d ln psi/dp and 1e-5 of
+    max(1, |E_L|) for dE_L/dp, with E_L itself identical to the FP64 engine's."""
+    from champ_b200.engine import Engine
+    s = S.c2_bfd_example(10) if k == "c2bfd" else S.get_system(k)
+    x = S.initial_walkers(s, nw, seed=90)
+    e64 = Engine(s, nw, "fp64")
+    e64.set_walkers(x)
+    e64.set_option("param_grad_mode", 1)
+    dl1, de1, el1 = e64.param_grad()
+    e64.set_option("param_grad_mode", 0)
+    el0 = e64.param_grad_fwd()
+    dl0, de0 = e64.param_grad_bwd()
+    assert np.allclose(el0, el1, rtol=1e-12, atol=1e-12)
+    sc = np.maximum(1.0, np.abs(el1))[:, None]
+    assert np.all(np.abs(dl0 - dl1) <= 1e-9 * np.maximum(1.0, np.abs(dl1)))
+    assert np.all(np.abs(de0 - de1) <= 1e-9 * sc)
+    with pytest.raises(Exception):
+        e64.param_grad_bwd()  # the tape was consumed
+    em = Engine(s, nw, "mixed")
+    em.set_walkers(x)
+    dlm, dem, elm = em.param_grad()
+    assert np.all(np.abs(elm - el1) <= 1e-6)
+    ed = float(np.max(np.abs(dlm - dl1) / np.maximum(1.0, np.abs(dl1))))
+    ee = float(np.max(np.abs(dem - de1) / sc))
+    print(f"system {k}: mixed reverse sweep vs FP64: d ln psi/dp {ed:.2e}, dE_L/dp {ee:.2e} (relative)")
+    assert ed <= 1e-5 and ee <= 1e-5, (ed, ee)
 
 
 def test_oh_accumulation_matches_numpy():
