@@ -1,7 +1,8 @@
 """Builds the engine's shared library in-tree with nvcc for sm_100a.
 
-The kernels are instantiated in two translation units (FP32 and FP64 compute types)
-compiled in parallel with the C-ABI unit, then linked into libchamp_b200.so.
+The kernels are instantiated in one translation unit per (compute type, e-e-n order), compiled
+in parallel with the C-ABI unit and the host-side linear-method unit, then linked into
+libchamp_b200.so.
 """
 from __future__ import annotations
 
@@ -13,7 +14,7 @@ from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-UNITS = ["host.cu"] + [f"inst_{t}_n{n}.cu" for t in ("f32", "f64") for n in (0, 4, 5)]
+UNITS = ["host.cu", "linear.cu"] + [f"inst_{t}_n{n}.cu" for t in ("f32", "f64") for n in (0, 4, 5)]
 DEPS = [os.path.join(HERE, "..", "include", "champ_b200.h")] + glob.glob(os.path.join(CSRC, "*"))
 LIB = os.path.join(HERE, "libchamp_b200.so")
 OBJDIR = os.path.join(HERE, "_build")

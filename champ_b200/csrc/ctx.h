@@ -88,6 +88,7 @@ struct champ_ctx {
   bool have_tape = false;
   int pg_mode = 0;  // 0: forward pass + reverse sweep; 1: one fused pass
   int nquad = 12;   // points of the nonlocal quadrature rule in use
+  QuadRule quad{};  // its points and weights (host copy)
   double *oh_oa = nullptr, *oh_ow = nullptr, *oh_mb = nullptr, *oh_s = nullptr, *oh_h = nullptr;
   bool have_pgrad = false;
   void *cublas = nullptr;

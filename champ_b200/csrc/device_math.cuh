@@ -37,8 +37,13 @@ struct EcpPar {
   double coef[MAXCT][MAXLCH][MG], expo[MAXCT][MAXLCH][MG];
   int pw[MAXCT][MAXLCH][MG];
   double znuc[MAXCT];
-  double q0[MAXQ][3], wq[MAXQ];
   int nquad;
+};
+
+// The quadrature rule (points and weights, [nquad][4]) lives in global memory, not in the
+// per-block shared copy of EcpPar: the 86-point rule would cost every block 2.7 KB of shared memory.
+struct QuadRule {
+  double q0[MAXQ][3], wq[MAXQ];
 };
 
 // System data in device memory (pointers into one allocation).
@@ -94,6 +99,7 @@ struct Sys {
   const int *occo[2];      // [nocc_s] orbital index of each occupied column
   const JasPar<T> *jas;
   const EcpPar *ecp;
+  const QuadRule *quad;
 };
 
 // ---------------------------------------------------------------------------------------

@@ -435,6 +435,10 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
   T *ct1 = dalloc<T>(c, (size_t)c->nbasis * std::max(1, md.nocc[1]));
   JasPar<T> *jp = dalloc<JasPar<T>>(c, 1);
   EcpPar *ep = dalloc<EcpPar>(c, 1);
+  QuadRule *qr = dalloc<QuadRule>(c, 1);
+  if (!qr) return fail(CHAMP_ENOMEM, "device allocation of the quadrature rule failed");
+  CK(cudaMemcpy(qr, &c->quad, sizeof(QuadRule), cudaMemcpyHostToDevice));
+  s.quad = qr;
   if (!cent || !ctype || !zc || !sh || !shp || !shb0 || !pz || !pc || !cr0 || !cr1 || !ct0 || !ct1 || !jp || !ep)
     return fail(CHAMP_ENOMEM, "device allocation of the system data failed");
   std::vector<double> zcv(c->C);
@@ -1286,7 +1290,7 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
       }
     }
   }
-  ecp.nquad = quadrature_rule(d->nloc == 6 ? d->nquad : 12, ecp.q0, ecp.wq);
+  ecp.nquad = quadrature_rule(d->nloc == 6 ? d->nquad : 12, c->quad.q0, c->quad.wq);
   c->nquad = ecp.nquad;
   double pecent = 0;
   for (int i = 0; i < d->ncent; i++)

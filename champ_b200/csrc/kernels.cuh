@@ -809,7 +809,7 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
       const double *cc = s.cent + 3 * c, *xe = xs + 3 * e;
       double qv[3];
 #pragma unroll
-      for (int k = 0; k < 3; k++) qv[k] = R[3 * k] * E.q0[q][0] + R[3 * k + 1] * E.q0[q][1] + R[3 * k + 2] * E.q0[q][2];
+      for (int k = 0; k < 3; k++) qv[k] = R[3 * k] * s.quad->q0[q][0] + R[3 * k + 1] * s.quad->q0[q][1] + R[3 * k + 2] * s.quad->q0[q][2];
       double costh = ((xe[0] - cc[0]) * qv[0] + (xe[1] - cc[1]) * qv[1] + (xe[2] - cc[2]) * qv[2]) / r;
       double xn[3] = {cc[0] + r * qv[0], cc[1] + r * qv[1], cc[2] + r * qv[2]};
       // determinant ratio: orbitals at the point contracted with G
@@ -900,14 +900,14 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
       for (int l = 0; l < E.npotd[it]; l++)
         if (l + 1 != E.lpotp1[it]) vp += rec[2 + l] * yl0(l, costh);
       if (merged) {
-        const double c2 = E.wq[q] * exp(dj) * vp;
+        const double c2 = s.quad->wq[q] * exp(dj) * vp;
         double *ph = pg->phis + (size_t)e * s.nbasis;
         for (int ish = 0; ish < s.nshell; ish++)
           dr += shell_dot_acc<T>(s, ish, xn, ge, (ish >= c0 && ish < c1) ? ro + ish : nullptr, c2, ph);
       }
-      vnl += E.wq[q] * exp(dj) * vp * (double)dr;
+      vnl += s.quad->wq[q] * exp(dj) * vp * (double)dr;
       if (PG) {
-        double coeff = E.wq[q] * exp(dj) * vp * (double)dr;
+        double coeff = s.quad->wq[q] * exp(dj) * vp * (double)dr;
         atomicAdd(&pg->csum[e], coeff);
         if (pg->tape) {
           pg->tape[t] = coeff;  // the backward pass forms the parameter sums at this point

@@ -217,9 +217,10 @@ __device__ void jastrow_param_pass(const Sys<T> &s, const JasPar<T> &J, const Vi
         T rij = tsqrt(T(rvd[0] * rvd[0] + rvd[1] * rvd[1] + rvd[2] * rvd[2]));
         T du = T(1) / (T(1) + sk * rij);
         const T *ri_ = v.ren + 2 * C * i, *rj_ = v.ren + 2 * C * j;
-        // sums over the centres of this pair in the compute precision (FP32 in the mixed
-        // engine: no FP64 work per term), added to the FP64 totals once per pair
-        constexpr bool PP = std::is_same<T, float>::value;
+        // the values' sums over the centres in the compute precision, added to the FP64 totals
+        // once per pair; the K terms (Laplacian and velocity products, which cancel between
+        // centres) are accumulated in FP64 term by term
+        constexpr bool PP = false;
         T ocp[tl.n > 0 ? tl.n : 1], kcp[PP && tl.n > 0 ? tl.n : 1];
 #pragma unroll
         for (int ll = 0; ll < tl.n; ll++) ocp[ll] = T(0);
@@ -733,7 +734,7 @@ __global__ void __launch_bounds__(128, 4) k_pgrad(Sys<T> s, State<T> st, Layout 
           double xn[3];
 #pragma unroll
           for (int k = 0; k < 3; k++)
-            xn[k] = cc[k] + r * (R[3 * k] * E.q0[q][0] + R[3 * k + 1] * E.q0[q][1] + R[3 * k + 2] * E.q0[q][2]);
+            xn[k] = cc[k] + r * (R[3 * k] * s.quad->q0[q][0] + R[3 * k + 1] * s.quad->q0[q][1] + R[3 * k + 2] * s.quad->q0[q][2]);
           if (pg.dvl) point_param_values<T, NORD, true>(s, J, v, e, xn, coeff, pg, nullptr);
           else point_param_values<T, NORD, false>(s, J, v, e, xn, coeff, pg, nullptr);
         }

@@ -24,6 +24,7 @@ EXPORTED_SYMBOLS = [
     "champ_walker_status", "champ_synchronize", "champ_param_grad", "champ_accumulate_oh",
     "champ_dmc_init", "champ_dmc_steps", "champ_num_walkers", "champ_eval_energy_noalloc", "champ_set_option",
     "champ_get_option", "champ_oh_buffers", "champ_phase_times", "champ_param_grad_fwd", "champ_param_grad_bwd",
+    "champ_linear_update",
 ]
 
 PREC = {"fp64": 0, "mixed": 1, "fp32": 2}
@@ -81,6 +82,7 @@ def load_library(path: str = LIB_PATH):
     L.champ_phase_times.argtypes = [vp, dp, C.POINTER(i32)]
     L.champ_param_grad_fwd.argtypes = [vp, dp]
     L.champ_param_grad_bwd.argtypes = [vp, dp, dp]
+    L.champ_linear_update.argtypes = [i32, i32, dp, dp, C.c_double, C.c_double, i32, dp, dp]
     for n in EXPORTED_SYMBOLS:
         if n not in ("champ_last_error", "champ_version"):
             getattr(L, n).restype = C.c_int
@@ -90,6 +92,19 @@ def load_library(path: str = LIB_PATH):
 
 def _p(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def linear_update(S, H, ncsf=0, sigma=0.0, diag_stab=0.0, select=0):
+    """champ_linear_update: parameter variations of the linear method from the O/H sums."""
+    L = load_library()
+    S = np.ascontiguousarray(S, np.float64)
+    H = np.ascontiguousarray(H, np.float64)
+    P = S.shape[0] - 1
+    dp, info = np.zeros(P), np.zeros(4)
+    rc = L.champ_linear_update(P, ncsf, _p(S), _p(H), sigma, diag_stab, select, _p(dp), _p(info))
+    if rc != 0:
+        raise ChampError(f"champ error {rc}: {L.champ_last_error().decode()}")
+    return dp, info
 
 
 class Engine:

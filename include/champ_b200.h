@@ -253,6 +253,23 @@ int champ_accumulate_oh(champ_ctx *ctx, const double *weights /* [nw] or NULL */
    deriv_mod.f90:683,898,1375) without copying them to the host. */
 int champ_oh_buffers(const champ_ctx *ctx, const double **S, const double **H);
 
+/* Linear-method update (ovlp_lin_bld, ham_lin_energy_bld, ham_lin_renorm_stab_bld and
+   delta_lin_bld, qmc/opt_lin_mod.f90:249-1265; host code, no context or GPU needed).  S and H are
+   the (nparm+1)^2 sums of champ_accumulate_oh (possibly summed over ranks); the first ncsf
+   parameters are CSF coefficients (the engine's parameter order puts them first).  Builds the
+   overlap and Hamiltonian of the wave function and its derivatives, renormalises them by the
+   overlap's diagonal, adds diag_stab to the Hamiltonian's diagonal (stabilization 'identity'),
+   solves H c = E S c, and selects the eigenvector as the reference does by default: the lowest
+   eigenvalue inside (E - sigma, E + 0.01) (E = the current energy, sigma its standard deviation;
+   sigma <= 0: no lower bound) unless its wave-function variation exceeds 100 times the smallest
+   one, else the one with the smallest variation (select 0; 1: lowest in the window, 2: largest
+   first component, 3: smallest variation).  dp[nparm] receives the parameter variations with the
+   semi-orthogonal normalisation (update_nonlinear 'semiorthogonal', xi = 1); parameters with no
+   variance get 0.  info (may be NULL): [selected eigenvalue, lowest eigenvalue, wave-function
+   variation of the selection, parameters kept]. */
+int champ_linear_update(int32_t nparm, int32_t ncsf, const double *S, const double *H, double sigma,
+                        double diag_stab, int32_t select, double *dp, double *info /* [4] or NULL */);
+
 /* Diffusion Monte Carlo (rundmc, qmc/rundmc_mod.f90:17-422).  champ_dmc_init starts from the
    current walkers (weight 1); w_target is the target population and the trial energy follows
    E_T = E_est - ln(W / w_target) / (gpop * tau).  The population may range up to w_max.
