@@ -25,6 +25,18 @@ struct MultiDet {
   std::vector<double> ccoef;
 };
 
+// The optimisable parameters in the caller's layouts (champ_system), kept for champ_set_params /
+// champ_apply_param_step, and the structure needed to re-derive what the kernels use.
+struct Params {
+  std::vector<double> a4, b, c, csf, coef;  // [nct][norda+1], [nspin2b][nordb+1], [nct][nterms] as given,
+                                            // [ncsf], [norb][nbasis] (input basis order)
+  std::vector<int> csf_ndet, csf_det;
+  std::vector<double> csf_det_coef;
+  int norda = 0, nordb = 0, nordc = 0, nspin2b = 1, een_cusp = 0, nterms = 0;
+  double scalek = 1;
+  std::vector<int> cfree;  // free e-e-n coefficients of a centre type (term indices)
+};
+
 // Largest per-warp shared-memory footprint for which a walker's state stays resident in
 // shared memory inside the fused kernels (keeps >= 16 warps per SM).
 constexpr size_t RESIDENT_LIMIT = 12 * 1024;
@@ -44,6 +56,8 @@ struct champ_ctx {
   int N = 0, nup = 0, ndn = 0, C = 0, nct = 0, nshell = 0, nbasis = 0, nmax = 0, nordc = 0, nloc = 0;
   int nomax = 1;
   MultiDet md;
+  Params par;
+  std::vector<int> perm_b;  // internal basis index -> caller's basis index
   // numerical radial tables (kind-2 shells), prepared at create: per table (grid, points, first
   // value index, 0), 10 parameters (r0, h, log h, c0..c4, a0, ak), values and spline second
   // derivatives of all tables one after another; shell -> table
@@ -120,6 +134,7 @@ struct champ_ctx {
   int tc_fused_ok = 0, tc_mode = 0;  // fused kernel supported; mode in use: 1 fused, 2 basis rows + product
   int tc_kchunk = 4;                 // fused kernel: K-blocks per TMEM accumulation chunk (0: all)
   int tc_kq = 0, tc_nkb = 0, tc_fcols[2] = {32, 32};
+  std::vector<int> tc_kpos_h, tc_b0_h;  // host copies: padded position and first basis function per shell
   int *tc_blk_sh = nullptr, *tc_kpos = nullptr;
   float *tc_bf[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [spin][hi, lo]: [Np][Kq]
 };

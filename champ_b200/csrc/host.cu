@@ -373,7 +373,7 @@ static int quadrature_rule(int nq_in, double (*q)[3], double *w) {
 }
 
 // cuspinit4 + cuspexact4 (qmc/fit/cuspinit4.f90:1-60, qmc/fit/cuspexact4.f90:14-40)
-static void host_een_cusp(int nordc, int nct, int nt, std::vector<double> &c, std::vector<int> *dependents = nullptr) {
+static void host_een_cusp(int nordc, int nct, int nt, std::vector<double> &c, std::vector<int> *dependents) {
   if (nordc <= 1) return;
   int neq = 2 * (nordc - 1);
   std::vector<double> d((size_t)neq * nt, 0.0);
@@ -411,6 +411,52 @@ static void host_een_cusp(int nordc, int nct, int nt, std::vector<double> &c, st
         if (j != jd) sum += d[(size_t)(e - 1) * nt + j - 1] * cc[j - 1];
       cc[jd - 1] = -sum / d[(size_t)(e - 1) * nt + jd - 1];
     }
+  }
+}
+
+// Jastrow parameters of the kernels from the context's parameters, e-e-n coefficients with the cusp
+// conditions applied (cfull) and the asymptotic values.
+template <class T>
+static void fill_jaspar(const champ_ctx *c, const std::vector<double> &cfull, const double *asymp_a,
+                        const double *asymp_b, JasPar<T> &J) {
+  const Params &q = c->par;
+  memset(&J, 0, sizeof J);
+  J.scalek = (T)q.scalek; J.norda = q.norda; J.nordb = q.nordb; J.nspin2b = q.nspin2b; J.nct = c->nct;
+  const int nt = (int)(cfull.size() / std::max(1, c->nct));
+  for (int it = 0; it < c->nct; it++) {
+    for (int k = 0; k <= q.norda; k++) J.a4[it][k] = (T)q.a4[it * (q.norda + 1) + k];
+    for (int k = 0; k < nt; k++) J.c[it][k] = (T)cfull[(size_t)it * nt + k];
+    J.asymp_a[it] = (T)asymp_a[it];
+  }
+  for (int is = 0; is < q.nspin2b; is++)
+    for (int k = 0; k <= q.nordb; k++) J.b[is][k] = (T)q.b[is * (q.nordb + 1) + k];
+  J.asymp_b[0] = (T)asymp_b[0]; J.asymp_b[1] = (T)asymp_b[1];
+}
+
+// e-e-n coefficients with the cusp conditions applied, and the isc=4 asymptotic values
+// (set_scale_dist, scale_dist.f90:147-225), from the context's parameters.
+static void derive_jastrow(const champ_ctx *c, std::vector<double> &cfull, double *asa, double *asb) {
+  const Params &q = c->par;
+  const int nt = q.nterms;
+  cfull.assign((size_t)c->nct * std::max(nt, 1), 0.0);
+  if (nt) std::copy(q.c.begin(), q.c.end(), cfull.begin());
+  if (q.een_cusp && nt) host_een_cusp(q.nordc, c->nct, nt, cfull, nullptr);
+  if (nt == 0) cfull.assign(c->nct, 0.0);
+  const double ar = 1.0 / q.scalek;
+  for (int it = 0; it < MAXCT; it++) asa[it] = 0;
+  for (int it = 0; it < c->nct; it++) {
+    const double *a = q.a4.data() + it * (q.norda + 1);
+    double v = a[0] * ar / (1 + a[1] * ar);
+    for (int k = 2; k <= q.norda; k++) v += a[k] * std::pow(ar, k);
+    asa[it] = v;
+  }
+  for (int i = 0; i < 2; i++) {
+    double ss = (i == 1 && q.nspin2b == 1) ? 0.5 : 1.0;
+    int isp = (i == 1) ? q.nspin2b - 1 : 0;
+    const double *b = q.b.data() + isp * (q.nordb + 1);
+    double v = ss * b[0] * ar / (1 + b[1] * ar);
+    for (int k = 2; k <= q.nordb; k++) v += b[k] * std::pow(ar, k);
+    asb[i] = v;
   }
 }
 
@@ -460,6 +506,7 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
       if (perm_b[ib] >= 0) return fail(CHAMP_EINVAL, "two basis functions with the same shell and m");
       perm_b[ib] = b;  // internal index ib holds input basis function b
     }
+    c->perm_b = perm_b;
   }
   int p0 = 0;
   for (int i = 0; i < c->nshell; i++) {
@@ -567,17 +614,7 @@ static int build_sys(champ_ctx *c, const champ_system *d, const std::vector<doub
     s.cproj = cp;
   }
   JasPar<T> J;
-  memset(&J, 0, sizeof J);
-  J.scalek = (T)d->scalek; J.norda = d->norda; J.nordb = d->nordb; J.nspin2b = d->nspin2b; J.nct = c->nct;
-  int nt = (int)(cfull.size() / std::max(1, c->nct));
-  for (int it = 0; it < c->nct; it++) {
-    for (int k = 0; k <= d->norda; k++) J.a4[it][k] = (T)d->a4[it * (d->norda + 1) + k];
-    for (int k = 0; k < nt; k++) J.c[it][k] = (T)cfull[(size_t)it * nt + k];
-    J.asymp_a[it] = (T)asymp_a[it];
-  }
-  for (int is = 0; is < d->nspin2b; is++)
-    for (int k = 0; k <= d->nordb; k++) J.b[is][k] = (T)d->b[is * (d->nordb + 1) + k];
-  J.asymp_b[0] = (T)asymp_b[0]; J.asymp_b[1] = (T)asymp_b[1];
+  fill_jaspar<T>(c, cfull, asymp_a, asymp_b, J);
   std::vector<int> ctv(d->iwctype, d->iwctype + c->C);
   CK(cudaMemcpy(cent, d->cent, sizeof(double) * 3 * c->C, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(ctype, ctv.data(), sizeof(int) * c->C, cudaMemcpyHostToDevice));
@@ -957,6 +994,37 @@ static int tc_alloc_rows(champ_ctx *c) {
   return CHAMP_OK;
 }
 
+// The occupied orbitals' coefficients split for the 3-term TF32 products: x = hi + lo with hi and
+// lo rounded to TF32, in the layouts of the two tensor-core contractions (K padded to BK; and the
+// fused kernel's blocks of whole shells).
+static int tc_upload_split(champ_ctx *c) {
+  const int B = c->nbasis, Kp = c->tc_Kp, Kq = c->tc_kq;
+  for (int sp = 0; sp < 2; sp++) {
+    const int no = c->md.nocc[sp], Np = c->tc_Np[sp];
+    if (no == 0 || (sp ? c->ndn : c->nup) == 0 || !c->tc_b[sp][0]) continue;
+    std::vector<float> hi((size_t)Np * Kp, 0.f), lo((size_t)Np * Kp, 0.f);
+    std::vector<float> fhi((size_t)Np * Kq, 0.f), flo((size_t)Np * Kq, 0.f);
+    for (int m = 0; m < no; m++) {
+      for (int b = 0; b < B; b++) {
+        float v = c->tc_coef[sp][(size_t)b * no + m], h = orbtc::tf32_hi(v);
+        hi[(size_t)m * Kp + b] = h;
+        lo[(size_t)m * Kp + b] = orbtc::tf32_lo(v, h);
+      }
+      for (int i = 0; i < c->nshell; i++)
+        for (int sl = 0; sl < 2 * c->tc_shl[i] + 1; sl++) {
+          float v = c->tc_coef[sp][(size_t)(c->tc_b0_h[i] + sl) * no + m], h = orbtc::tf32_hi(v);
+          fhi[(size_t)m * Kq + c->tc_kpos_h[i] + sl] = h;
+          flo[(size_t)m * Kq + c->tc_kpos_h[i] + sl] = orbtc::tf32_lo(v, h);
+        }
+    }
+    CK(cudaMemcpy(c->tc_b[sp][0], hi.data(), sizeof(float) * hi.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->tc_b[sp][1], lo.data(), sizeof(float) * lo.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->tc_bf[sp][0], fhi.data(), sizeof(float) * fhi.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->tc_bf[sp][1], flo.data(), sizeof(float) * flo.size(), cudaMemcpyHostToDevice));
+  }
+  return CHAMP_OK;
+}
+
 static int tc_setup(champ_ctx *c) {
   c->tc_on = c->tc_ok = c->tc_fused_ok = c->tc_mode = 0;
   int dev = 0;
@@ -997,33 +1065,20 @@ static int tc_setup(champ_ctx *c) {
     while (fc < 5 * Np) fc <<= 1;
     c->tc_fcols[sp] = fc;
     if (5 * Np > 512) fused = false;
-    std::vector<float> hi((size_t)Np * Kp, 0.f), lo((size_t)Np * Kp, 0.f);
-    std::vector<float> fhi((size_t)Np * Kq, 0.f), flo((size_t)Np * Kq, 0.f);
-    for (int m = 0; m < no; m++) {
-      for (int b = 0; b < B; b++) {
-        float v = c->tc_coef[sp][(size_t)b * no + m], h = orbtc::tf32_hi(v);
-        hi[(size_t)m * Kp + b] = h;
-        lo[(size_t)m * Kp + b] = orbtc::tf32_lo(v, h);
-      }
-      for (int i = 0; i < c->nshell; i++)
-        for (int sl = 0; sl < 2 * c->tc_shl[i] + 1; sl++) {
-          float v = c->tc_coef[sp][(size_t)(b0[i] + sl) * no + m], h = orbtc::tf32_hi(v);
-          fhi[(size_t)m * Kq + kpos[i] + sl] = h;
-          flo[(size_t)m * Kq + kpos[i] + sl] = orbtc::tf32_lo(v, h);
-        }
-    }
-    c->tc_b[sp][0] = dalloc<float>(c, hi.size());
-    c->tc_b[sp][1] = dalloc<float>(c, lo.size());
-    c->tc_bf[sp][0] = dalloc<float>(c, fhi.size());
-    c->tc_bf[sp][1] = dalloc<float>(c, flo.size());
+    c->tc_b[sp][0] = dalloc<float>(c, (size_t)Np * Kp);
+    c->tc_b[sp][1] = dalloc<float>(c, (size_t)Np * Kp);
+    c->tc_bf[sp][0] = dalloc<float>(c, (size_t)Np * Kq);
+    c->tc_bf[sp][1] = dalloc<float>(c, (size_t)Np * Kq);
     if (!c->tc_b[sp][0] || !c->tc_b[sp][1] || !c->tc_bf[sp][0] || !c->tc_bf[sp][1])
       return fail(CHAMP_ENOMEM, "device allocation failed");
-    CK(cudaMemcpy(c->tc_b[sp][0], hi.data(), sizeof(float) * hi.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->tc_b[sp][1], lo.data(), sizeof(float) * lo.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->tc_bf[sp][0], fhi.data(), sizeof(float) * fhi.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->tc_bf[sp][1], flo.data(), sizeof(float) * flo.size(), cudaMemcpyHostToDevice));
   }
+  c->tc_kpos_h = kpos;
+  c->tc_b0_h = b0;
   c->tc_kq = Kq;
+  {
+    int rc = tc_upload_split(c);
+    if (rc) return rc;
+  }
   c->tc_nkb = nkb;
   c->tc_blk_sh = dalloc<int>(c, nkb + 1);
   c->tc_kpos = dalloc<int>(c, c->nshell);
@@ -1215,16 +1270,32 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
     int rc0 = build_radial_tables(d, c);
     if (rc0) { delete c; return rc0; }
   }
-  // e-e-n coefficients with the cusp conditions applied
+  // e-e-n terms; the optimisable parameters kept for later updates
   int nt = 0;
   for (int n = 2; n <= d->nordc; n++)
     for (int k = n - 1; k >= 0; k--) {
       int l_hi = (k == 0) ? n - k - 2 : n - k;
       for (int l = l_hi; l >= 0; l--) if (((n - k - l) & 1) == 0) nt++;
     }
-  std::vector<double> cfull((size_t)d->nctype * std::max(nt, 1), 0.0);
-  if (nt) memcpy(cfull.data(), d->c, sizeof(double) * d->nctype * nt);
-  if (d->een_cusp) host_een_cusp(d->nordc, d->nctype, nt, cfull);
+  {
+    Params &q = c->par;
+    q.norda = d->norda; q.nordb = d->nordb; q.nordc = d->nordc; q.nspin2b = d->nspin2b; q.een_cusp = d->een_cusp;
+    q.nterms = nt; q.scalek = d->scalek;
+    q.a4.assign(d->a4, d->a4 + (size_t)d->nctype * (d->norda + 1));
+    q.b.assign(d->b, d->b + (size_t)d->nspin2b * (d->nordb + 1));
+    q.c.assign((size_t)d->nctype * nt, 0.0);
+    if (nt) memcpy(q.c.data(), d->c, sizeof(double) * d->nctype * nt);
+    q.csf.assign(d->csf_coef, d->csf_coef + d->ncsf);
+    q.csf_ndet.assign(d->csf_ndet, d->csf_ndet + d->ncsf);
+    size_t ncd = 0;
+    for (int i = 0; i < d->ncsf; i++) ncd += d->csf_ndet[i];
+    q.csf_det.assign(d->csf_det, d->csf_det + ncd);
+    q.csf_det_coef.assign(d->csf_det_coef, d->csf_det_coef + ncd);
+    q.coef.assign(d->coef, d->coef + (size_t)d->norb * d->nbasis);
+  }
+  std::vector<double> cfull;
+  double asa[MAXCT] = {0}, asb[2] = {0, 0};
+  derive_jastrow(c, cfull, asa, asb);
   // free e-e-n coefficients and d c / d c_free (the cusp map is linear, so unit vectors give
   // its columns exactly)
   {
@@ -1237,34 +1308,19 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
     for (int ll = 0; ll < nt; ll++)
       if (std::find(dep.begin(), dep.end(), ll) == dep.end()) fr.push_back(ll);
     c->ncfree = (d->nordc > 1) ? (int)fr.size() : 0;
+    c->par.cfree = fr;
     c->cproj.assign((size_t)std::max(nt, 1) * std::max(c->ncfree, 1), 0.0);
     for (int f = 0; f < c->ncfree; f++) {
       std::vector<double> u(nt, 0.0);
       u[fr[f]] = 1.0;
-      if (d->een_cusp) host_een_cusp(d->nordc, 1, nt, u);
+      if (d->een_cusp) host_een_cusp(d->nordc, 1, nt, u, nullptr);
       for (int ll = 0; ll < nt; ll++) c->cproj[(size_t)ll * c->ncfree + f] = u[ll];
     }
     int na = d->nctype * std::max(0, d->norda - 1), nb = d->nspin2b * d->nordb;
     c->np_raw = na + nb + (d->nordc > 1 ? d->nctype * nt : 0);
     c->nparm_jas = na + nb + d->nctype * c->ncfree;
   }
-  if (nt == 0) cfull.assign(d->nctype, 0.0);
-  // asymptotic values for isc=4 (set_scale_dist, scale_dist.f90:147-225)
-  double ar = 1.0 / d->scalek, asa[MAXCT] = {0}, asb[2] = {0, 0};
-  for (int it = 0; it < d->nctype; it++) {
-    const double *a = d->a4 + it * (d->norda + 1);
-    double v = a[0] * ar / (1 + a[1] * ar);
-    for (int k = 2; k <= d->norda; k++) v += a[k] * std::pow(ar, k);
-    asa[it] = v;
-  }
-  for (int i = 0; i < 2; i++) {
-    double ss = (i == 1 && d->nspin2b == 1) ? 0.5 : 1.0;
-    int isp = (i == 1) ? d->nspin2b - 1 : 0;
-    const double *b = d->b + isp * (d->nordb + 1);
-    double v = ss * b[0] * ar / (1 + b[1] * ar);
-    for (int k = 2; k <= d->nordb; k++) v += b[k] * std::pow(ar, k);
-    asb[i] = v;
-  }
+
   // pseudopotential and quadrature (rotqua.f90 icosahedral rule)
   EcpPar ecp;
   memset(&ecp, 0, sizeof ecp);
@@ -1497,6 +1553,125 @@ int champ_param_grad(champ_ctx *c, double *dlnpsi, double *deloc, double *eloc) 
   if (dlnpsi || deloc || eloc) CK(cudaStreamSynchronize(c->stream));
   c->have_pgrad = true;
   return CHAMP_OK;
+}
+
+}  // extern "C"
+
+// Re-derives and uploads everything the kernels take from the optimisable parameters: the Jastrow
+// parameters (cusp-fixed e-e-n coefficients, asymptotic values), the determinant coefficients with
+// the CSF coefficients folded in, the orbital coefficients in every layout the kernels read, and
+// the tensor-core splits.  Writes into the buffers champ_create allocated.
+template <class T>
+static int upload_params(champ_ctx *c, Sys<T> &s) {
+  const Params &q = c->par;
+  std::vector<double> cfull;
+  double asa[MAXCT], asb[2];
+  derive_jastrow(c, cfull, asa, asb);
+  JasPar<T> J;
+  fill_jaspar<T>(c, cfull, asa, asb, J);
+  CK(cudaMemcpy((void *)s.jas, &J, sizeof J, cudaMemcpyHostToDevice));
+  std::vector<double> cc(c->md.ndet, 0.0);
+  for (size_t icsf = 0, off = 0; icsf < q.csf.size(); icsf++)
+    for (int i = 0; i < q.csf_ndet[icsf]; i++, off++) cc[q.csf_det[off]] += q.csf_det_coef[off] * q.csf[icsf];
+  if (!c->md.multidet && cc[0] == 0.0) return fail(CHAMP_EINVAL, "zero determinant coefficient");
+  c->md.ccoef = cc;
+  CK(cudaMemcpy((void *)s.ccoef, cc.data(), sizeof(double) * cc.size(), cudaMemcpyHostToDevice));
+  const int B = c->nbasis, M = c->norb;
+  for (int sp = 0; sp < 2; sp++) {
+    const int no = c->md.nocc[sp];
+    if (no == 0) continue;
+    std::vector<T> cr((size_t)B * no), ct((size_t)no * B);
+    for (int k = 0; k < no; k++)
+      for (int b = 0; b < B; b++) {
+        const T v = (T)q.coef[(size_t)c->md.occ[sp][k] * B + c->perm_b[b]];
+        cr[(size_t)b * no + k] = v;
+        ct[(size_t)k * B + b] = v;
+      }
+    CK(cudaMemcpy((void *)s.cocc[sp], cr.data(), sizeof(T) * cr.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((void *)s.coccT[sp], ct.data(), sizeof(T) * ct.size(), cudaMemcpyHostToDevice));
+    if constexpr (std::is_same<T, float>::value) c->tc_coef[sp] = cr;
+  }
+  std::vector<T> ca((size_t)B * M);
+  std::vector<double> cd((size_t)B * M);
+  for (int m = 0; m < M; m++)
+    for (int b = 0; b < B; b++) ca[(size_t)b * M + m] = (T)(cd[(size_t)b * M + m] = q.coef[(size_t)m * B + c->perm_b[b]]);
+  CK(cudaMemcpy((void *)s.call, ca.data(), sizeof(T) * ca.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->call_d, cd.data(), sizeof(double) * cd.size(), cudaMemcpyHostToDevice));
+  if constexpr (std::is_same<T, float>::value)
+    if (c->tc_ok) return tc_upload_split(c);
+  return CHAMP_OK;
+}
+
+static int reload_params(champ_ctx *c) {
+  int rc = CHAMP_OK;
+  if (c->prec != CHAMP_PREC_FP32) rc = upload_params<double>(c, c->sd);
+  if (!rc && c->prec != CHAMP_PREC_FP64) rc = upload_params<float>(c, c->sf);
+  if (rc) return rc;
+  c->have_pgrad = c->have_tape = false;
+  if (c->have_walkers) {  // the walkers' tables and inverses for the new wave function
+    rc = launch(c, Op::Eval);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  return CHAMP_OK;
+}
+
+extern "C" {
+
+int champ_set_params(champ_ctx *c, const double *a4, const double *b, const double *cc, const double *csf_coef,
+                     const double *coef) {
+  if (!c) return fail(CHAMP_EINVAL, "null context");
+  Params &q = c->par;
+  if (a4) std::copy(a4, a4 + q.a4.size(), q.a4.begin());
+  if (b) std::copy(b, b + q.b.size(), q.b.begin());
+  if (cc) std::copy(cc, cc + q.c.size(), q.c.begin());
+  if (csf_coef) std::copy(csf_coef, csf_coef + q.csf.size(), q.csf.begin());
+  if (coef) std::copy(coef, coef + q.coef.size(), q.coef.begin());
+  return reload_params(c);
+}
+
+int champ_get_params(const champ_ctx *c, double *a4, double *b, double *cc, double *csf_coef, double *coef) {
+  if (!c) return fail(CHAMP_EINVAL, "null context");
+  const Params &q = c->par;
+  if (a4) std::copy(q.a4.begin(), q.a4.end(), a4);
+  if (b) std::copy(q.b.begin(), q.b.end(), b);
+  if (cc) {
+    std::vector<double> cfull;
+    double asa[MAXCT], asb[2];
+    derive_jastrow(c, cfull, asa, asb);
+    std::copy(cfull.begin(), cfull.begin() + q.c.size(), cc);
+  }
+  if (csf_coef) std::copy(q.csf.begin(), q.csf.end(), csf_coef);
+  if (coef) std::copy(q.coef.begin(), q.coef.end(), coef);
+  return CHAMP_OK;
+}
+
+int champ_apply_param_step(champ_ctx *c, const double *dp) {
+  if (!c || !dp) return fail(CHAMP_EINVAL, "null argument");
+  Params &q = c->par;
+  int k = 0;
+  for (int i = 1; i <= c->ncsfp; i++) q.csf[i] += dp[k++];
+  if (c->norbp) {
+    const std::vector<double> old = q.coef;
+    const int B = c->nbasis;
+    for (int r = 0; r < c->norbp; r++) {
+      const int4 o = c->orbp[r];
+      const double d = dp[k++];
+      for (int bb = 0; bb < B; bb++) {
+        q.coef[(size_t)o.x * B + bb] += d * old[(size_t)o.y * B + bb];
+        if (o.z) q.coef[(size_t)o.y * B + bb] -= d * old[(size_t)o.x * B + bb];
+      }
+    }
+  }
+  for (int it = 0; it < c->nct; it++)
+    for (int kk = 2; kk <= q.norda; kk++) q.a4[(size_t)it * (q.norda + 1) + kk] += dp[k++];
+  for (int is = 0; is < q.nspin2b; is++)
+    for (int kk = 1; kk <= q.nordb; kk++) q.b[(size_t)is * (q.nordb + 1) + kk] += dp[k++];
+  if (q.nordc > 1)
+    for (int it = 0; it < c->nct; it++)
+      for (int f = 0; f < c->ncfree; f++) q.c[(size_t)it * q.nterms + q.cfree[f]] += dp[k++];
+  if (k != c->nfree) return fail(CHAMP_EINVAL, "internal: parameter count mismatch");
+  return reload_params(c);
 }
 
 int champ_oh_buffers(const champ_ctx *c, const double **S, const double **H) {

@@ -24,7 +24,7 @@ EXPORTED_SYMBOLS = [
     "champ_walker_status", "champ_synchronize", "champ_param_grad", "champ_accumulate_oh",
     "champ_dmc_init", "champ_dmc_steps", "champ_num_walkers", "champ_eval_energy_noalloc", "champ_set_option",
     "champ_get_option", "champ_oh_buffers", "champ_phase_times", "champ_param_grad_fwd", "champ_param_grad_bwd",
-    "champ_linear_update",
+    "champ_linear_update", "champ_set_params", "champ_get_params", "champ_apply_param_step",
 ]
 
 PREC = {"fp64": 0, "mixed": 1, "fp32": 2}
@@ -83,6 +83,9 @@ def load_library(path: str = LIB_PATH):
     L.champ_param_grad_fwd.argtypes = [vp, dp]
     L.champ_param_grad_bwd.argtypes = [vp, dp, dp]
     L.champ_linear_update.argtypes = [i32, i32, dp, dp, C.c_double, C.c_double, i32, dp, dp]
+    L.champ_set_params.argtypes = [vp, dp, dp, dp, dp, dp]
+    L.champ_get_params.argtypes = [vp, dp, dp, dp, dp, dp]
+    L.champ_apply_param_step.argtypes = [vp, dp]
     for n in EXPORTED_SYMBOLS:
         if n not in ("champ_last_error", "champ_version"):
             getattr(L, n).restype = C.c_int
@@ -229,6 +232,26 @@ class Engine:
         dl, de = np.zeros((self.nw, P)), np.zeros((self.nw, P))
         self._check(self.lib.champ_param_grad_bwd(self.h, _p(dl), _p(de)))
         return dl, de
+
+    def get_params(self):
+        """Current parameters: a4, b, c (cusp conditions applied), csf_coef, coef."""
+        s = self.system
+        from .system import nterms4
+        a = np.zeros_like(s.a4, dtype=float)
+        b = np.zeros_like(s.b, dtype=float)
+        c = np.zeros((s.nctype, nterms4(s.nordc)))
+        csf = np.zeros(len(s.csf_coef))
+        coef = np.zeros_like(s.coef, dtype=float)
+        self._check(self.lib.champ_get_params(self.h, _p(a), _p(b), _p(c) if c.size else None, _p(csf), _p(coef)))
+        return dict(a4=a, b=b, c=c, csf_coef=csf, coef=coef)
+
+    def set_params(self, a4=None, b=None, c=None, csf_coef=None, coef=None):
+        arr = [None if v is None else np.ascontiguousarray(v, np.float64) for v in (a4, b, c, csf_coef, coef)]
+        self._check(self.lib.champ_set_params(self.h, *[None if v is None or v.size == 0 else _p(v) for v in arr]))
+
+    def apply_param_step(self, dp):
+        dp = np.ascontiguousarray(dp, np.float64)
+        self._check(self.lib.champ_apply_param_step(self.h, _p(dp)))
 
     def accumulate_oh(self, weights=None):
         P1 = sum(self.nparam()) + 1

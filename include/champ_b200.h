@@ -253,6 +253,22 @@ int champ_accumulate_oh(champ_ctx *ctx, const double *weights /* [nw] or NULL */
    deriv_mod.f90:683,898,1375) without copying them to the host. */
 int champ_oh_buffers(const champ_ctx *ctx, const double **S, const double **H);
 
+/* Wave-function parameters of a live context (no counterpart as one call in the reference, whose
+   optimiser writes the new parameters into its global arrays; the layouts are champ_system's):
+   a4 [nctype][norda+1], b [nspin2b][nordb+1], c [nctype][nterms4(nordc)], csf_coef [ncsf],
+   coef [norb][nbasis].  NULL arrays are left as they are.  The e-e-n coefficients the cusp
+   conditions fix are re-derived from the others (champ_get_params returns them derived).  The
+   current walkers are re-evaluated for the new wave function (as champ_set_walkers does); the
+   tape of champ_param_grad_fwd and the results of champ_param_grad are invalidated. */
+int champ_set_params(champ_ctx *ctx, const double *a4, const double *b, const double *c, const double *csf_coef,
+                     const double *coef);
+int champ_get_params(const champ_ctx *ctx, double *a4, double *b, double *c, double *csf_coef, double *coef);
+/* Adds a step dp[P] in the order of champ_param_grad's parameters (CSF coefficients 2..ncsf,
+   orbital rotations: coefficients of orbital i += dp times those of orbital j, and those of j -=
+   dp times those of i for a rotation between two active orbitals, then the free Jastrow
+   parameters) -- the update the linear method's delta_lin makes -- and re-evaluates the walkers. */
+int champ_apply_param_step(champ_ctx *ctx, const double *dp /* [P] */);
+
 /* Linear-method update (ovlp_lin_bld, ham_lin_energy_bld, ham_lin_renorm_stab_bld and
    delta_lin_bld, qmc/opt_lin_mod.f90:249-1265; host code, no context or GPU needed).  S and H are
    the (nparm+1)^2 sums of champ_accumulate_oh (possibly summed over ranks); the first ncsf
