@@ -79,7 +79,7 @@ bool eig_real(int n, const std::vector<double> &A, std::vector<cd> &lam, std::ve
     for (; l > 0; l--) {
       double sc = std::abs(t(l - 1, l - 1)) + std::abs(t(l, l));
       if (sc == 0.0) sc = tnorm;
-      if (std::abs(t(l, l - 1)) <= eps * sc) {
+      if (std::abs(t(l, l - 1)) <= eps * sc || std::abs(t(l, l - 1)) <= 1e-3 * eps * tnorm) {
         t(l, l - 1) = 0.0;
         break;
       }
@@ -89,7 +89,7 @@ bool eig_real(int n, const std::vector<double> &A, std::vector<cd> &lam, std::ve
       iter = 0;
       continue;
     }
-    if (++iter > 60 || ++total > 60 * n) return false;
+    if (++iter > 200 || ++total > 100 * n + 1000) return false;
     const cd a = t(hi - 1, hi - 1), b = t(hi - 1, hi), c = t(hi, hi - 1), d = t(hi, hi);
     const cd disc = std::sqrt(0.25 * (a - d) * (a - d) + b * c);
     const cd m1 = 0.5 * (a + d) + disc, m2 = 0.5 * (a + d) - disc;
@@ -161,6 +161,10 @@ extern "C" int champ_linear_update(int32_t nparm, int32_t ncsf, const double *S,
                                    double diag_stab, int32_t select, double *dp, double *info) {
   if (nparm < 1 || ncsf < 0 || ncsf > nparm || !S || !H || !dp) return champ_fail(CHAMP_EINVAL, "linear update: bad argument");
   const int P = nparm, n1 = P + 1;
+  for (size_t i = 0; i < (size_t)n1 * n1; i++)
+    if (!std::isfinite(S[i]) || !std::isfinite(H[i]))
+      return champ_fail(CHAMP_EINVAL, "linear update: non-finite entries in S or H (a walker with a non-finite E_L "
+                                      "or derivative entered the sums)");
   const double W = S[0];
   if (!(W > 0)) return champ_fail(CHAMP_EINVAL, "linear update: the summed weight S[0][0] must be positive");
   auto s = [&](int a, int b) { return S[(size_t)a * n1 + b] / W; };

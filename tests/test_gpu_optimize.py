@@ -48,7 +48,7 @@ def test_linear_method_descends_like_the_transcript(prec):
             Ssum += Sk
             Hsum += Hk
         idx = np.concatenate([[0], jas + 1])
-        dpj, info = linear_update(Ssum[np.ix_(idx, idx)], Hsum[np.ix_(idx, idx)], ncsf=0, sigma=sigma, diag_stab=1e-3)
+        dpj, info = linear_update(Ssum[np.ix_(idx, idx)], Hsum[np.ix_(idx, idx)], ncsf=0, sigma=sigma, diag_stab=1e-2)
         dp = np.zeros(P)
         dp[jas] = dpj
         print(f"iteration {it}: E = {e:.5f} +- {err:.5f}, sigma {sigma:.4f}; eigenvalue {info[0]:.5f}, "
