@@ -25,6 +25,11 @@
 
 using namespace champ;
 
+// The limits the header publishes are the ones the kernels are compiled for.
+static_assert(CHAMP_MAX_CTYPE == MAXCT, "centre types");
+static_assert(CHAMP_MAX_LCHAN == MAXLCH, "pseudopotential channels");
+static_assert(CHAMP_MAX_QUAD == MAXQ, "quadrature points");
+
 // ---------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------

@@ -25,6 +25,7 @@ EXPORTED_SYMBOLS = [
     "champ_dmc_init", "champ_dmc_steps", "champ_num_walkers", "champ_eval_energy_noalloc", "champ_set_option",
     "champ_get_option", "champ_oh_buffers", "champ_phase_times", "champ_param_grad_fwd", "champ_param_grad_bwd",
     "champ_linear_update", "champ_set_params", "champ_get_params", "champ_apply_param_step",
+    "champ_check_param_step", "champ_eval_param_step", "champ_linear_method_step",
 ]
 
 PREC = {"fp64": 0, "mixed": 1, "fp32": 2}
@@ -86,6 +87,9 @@ def load_library(path: str = LIB_PATH):
     L.champ_set_params.argtypes = [vp, dp, dp, dp, dp, dp]
     L.champ_get_params.argtypes = [vp, dp, dp, dp, dp, dp]
     L.champ_apply_param_step.argtypes = [vp, dp]
+    L.champ_check_param_step.argtypes = [vp, dp, C.c_double, C.POINTER(i32)]
+    L.champ_eval_param_step.argtypes = [vp, dp, dp, dp]
+    L.champ_linear_method_step.argtypes = [vp, i32, C.POINTER(i32), dp, dp, C.c_double, C.c_double, dp, dp, dp]
     for n in EXPORTED_SYMBOLS:
         if n not in ("champ_last_error", "champ_version"):
             getattr(L, n).restype = C.c_int
@@ -252,6 +256,39 @@ class Engine:
     def apply_param_step(self, dp):
         dp = np.ascontiguousarray(dp, np.float64)
         self._check(self.lib.champ_apply_param_step(self.h, _p(dp)))
+
+    def check_param_step(self, dp, psi_lin_var_norm=0.0):
+        """champ_check_param_step: 0 (good), 1 (bad) or 2 (bad for any stabilisation)."""
+        dp = np.ascontiguousarray(dp, np.float64)
+        bad = C.c_int32()
+        self._check(self.lib.champ_check_param_step(self.h, _p(dp), psi_lin_var_norm, C.byref(bad)))
+        return bad.value
+
+    def eval_param_step(self, dp):
+        """Correlated sampling of a trial step: (E_L, ln|psi_new| - ln|psi_old|) of every walker."""
+        dp = np.ascontiguousarray(dp, np.float64)
+        el, dl = np.zeros(self.nw), np.zeros(self.nw)
+        self._check(self.lib.champ_eval_param_step(self.h, _p(dp), _p(el), _p(dl)))
+        return el, dl
+
+    def linear_method_step(self, S, H, sigma, diag_stab, sel=None, p_var=0.0):
+        """champ_linear_method_step: one stabilised linear-method iteration on the parameters sel
+        (S, H: the sums over those parameters).  Returns (dp, final diag_stab, info[8])."""
+        S = np.ascontiguousarray(S, np.float64)
+        H = np.ascontiguousarray(H, np.float64)
+        P = sum(self.nparam())
+        dp, info = np.zeros(P), np.zeros(8)
+        st = C.c_double(diag_stab)
+        if sel is None:
+            nsel, psel = P, None
+        else:
+            sel = np.ascontiguousarray(sel, np.int32)
+            nsel, psel = len(sel), sel.ctypes.data_as(C.POINTER(C.c_int32))
+        if S.shape != (nsel + 1, nsel + 1) or H.shape != S.shape:
+            raise ValueError("S and H must be (nsel+1)^2")
+        self._check(self.lib.champ_linear_method_step(self.h, nsel, psel, _p(S), _p(H), sigma, p_var, C.byref(st),
+                                                      _p(dp), _p(info)))
+        return dp, st.value, info
 
     def accumulate_oh(self, weights=None):
         P1 = sum(self.nparam()) + 1

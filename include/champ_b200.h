@@ -65,7 +65,7 @@ extern "C" {
 #define CHAMP_MAX_ELEC 256
 #define CHAMP_MAX_SPIN 64      /* electrons of one spin */
 #define CHAMP_MAX_L 4
-#define CHAMP_MAX_CTYPE 8
+#define CHAMP_MAX_CTYPE 4      /* nuclear (centre) types */
 #define CHAMP_MAX_NORD 7
 #define CHAMP_MAX_LCHAN 5      /* pseudopotential l channels (npotd) */
 #define CHAMP_MAX_QUAD 86      /* nonlocal quadrature points */
@@ -285,6 +285,37 @@ int champ_apply_param_step(champ_ctx *ctx, const double *dp /* [P] */);
    variation of the selection, parameters kept]. */
 int champ_linear_update(int32_t nparm, int32_t ncsf, const double *S, const double *H, double sigma,
                         double diag_stab, int32_t select, double *dp, double *info /* [4] or NULL */);
+
+/* The checks the reference's optimisation driver makes on a step before it keeps it
+   (wf_update_and_check, qmc/optimization_mod.f90:1730-1840): *bad = 1 if the root-mean-square
+   variation of the CSF coefficients exceeds 1, of the Jastrow parameters max(10, 5/scalek), of all
+   parameters 10 (each over the parameters the step changes), or psi_lin_var_norm (info[2] of
+   champ_linear_update) exceeds 10, or b2 (a2) would exceed 100; *bad = 2 if b2 or a2 would fall
+   below -scalek (a pole of the Pade form) or dp is not finite; else 0. */
+int champ_check_param_step(const champ_ctx *ctx, const double *dp /* [P] */, double psi_lin_var_norm, int32_t *bad);
+
+/* Correlated sampling of a trial step on the current walkers: E_L of every walker for the
+   parameters + dp, and ln|psi_new| - ln|psi_old| (the walkers' reweighting is exp(2 dlnpsi)).
+   The context's parameters and walker state are unchanged afterwards. */
+int champ_eval_param_step(champ_ctx *ctx, const double *dp /* [P] */, double *eloc /* [nw] or NULL */,
+                          double *dlnpsi /* [nw] or NULL */);
+
+/* One linear-method iteration with the reference's stabilisation search (adjust_diag_stab and
+   wf_update_and_check_and_stab, qmc/optimization_mod.f90:1845-2250; quad_min.f90): steps for
+   add_diag, add_diag/10 and 10 add_diag (*diag_stab = add_diag on input) from the sums S, H over
+   the parameters sel[nsel] (increasing indices; sel NULL: all P parameters); bad steps multiply
+   add_diag by 10^(sum of the bad codes, at most 3); the three trial wave functions' energies by
+   correlated sampling on the current walkers (reweighted; a trial whose weights' effective sample
+   size falls below 1/50 of the walkers is not reliable); if all three are much worse than the
+   current energy (sigma above (2.5 - p_var) times, or the energy above 3 (1 + p_var) combined
+   errors) add_diag is multiplied by 1000; then the objective (1 - p_var) E + p_var sigma^2 fitted
+   by a parabola in log10(add_diag) gives the final constant (bounded to two decades), which is
+   raised by factors of 10 until the step passes champ_check_param_step.  Applies that step to the
+   context and returns it in dp (host [P] or NULL), the final constant in *diag_stab and info
+   (host [8] or NULL): [eigenvalue, wave-function variation, current energy, its error, correlated
+   energies of the three trial constants, search iterations]. */
+int champ_linear_method_step(champ_ctx *ctx, int32_t nsel, const int32_t *sel, const double *S, const double *H,
+                             double sigma, double p_var, double *diag_stab, double *dp, double *info);
 
 /* Diffusion Monte Carlo (rundmc, qmc/rundmc_mod.f90:17-422).  champ_dmc_init starts from the
    current walkers (weight 1); w_target is the target population and the trial energy follows

@@ -7,14 +7,16 @@ first 'Final results' block of its transcript examples/be_vb1_jcas24_vmc_j_opt_l
 the parsed wave function and the reference's printed averages, so that the VMC energy
 of this wave function can be compared with the reference's without the reference tree.
 
-Usage: python tests/golden/make_be_fixture.py [/path/to/CHAMP]
+Usage: python tests/golden/make_be_fixture.py /path/to/CHAMP
 """
 import json
 import os
 import re
 import sys
 
-ROOT = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_be_fixture.py /path/to/CHAMP")
+ROOT = sys.argv[1]
 INP = os.path.join(ROOT, "examples", "be_vb1_jcas24_vmc_j_opt_lin.inp")
 OUT = os.path.join(ROOT, "examples", "be_vb1_jcas24_vmc_j_opt_lin.out")
 

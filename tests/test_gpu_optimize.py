@@ -1,12 +1,12 @@
 """The linear-method optimisation loop through the C ABI: champ_param_grad (forward pass + reverse
-sweep), champ_accumulate_oh, champ_linear_update and champ_apply_param_step, and the parameter
-setters of a live context.
+sweep), champ_accumulate_oh, champ_linear_method_step (built on champ_linear_update,
+champ_check_param_step and champ_eval_param_step), and the parameter setters of a live context.
 
 The reference's C2 pseudopotential example optimises its 24 Jastrow parameters with the linear
 method from the input's Jastrow (examples/c2_bfd_vtz_rhf_vmc_new.out: -10.7749 +- 0.0124 Ha, then
 -10.9807 +- 0.0062, -11.0008 +- 0.0031, -11.0061 +- 0.0016 after iterations 1-3).  The same loop
-here (Jastrow parameters only, 8192 walkers) must descend to below -10.99 Ha within four
-iterations, which is where the transcript is after two.
+here (Jastrow parameters only, 8192 walkers, champ_linear_method_step's stabilisation search) must
+descend to below -10.99 Ha within four iterations, which is where the transcript is after two.
 """
 import numpy as np
 import pytest
@@ -26,7 +26,10 @@ def vmc_energy(eng, s, seed, neq=30, ns=60):
 
 @pytest.mark.parametrize("prec", ["mixed"])
 def test_linear_method_descends_like_the_transcript(prec):
-    from champ_b200.engine import Engine, linear_update
+    """champ_linear_method_step with the reference's stabilisation search from add_diag = 1e-8 each
+    iteration (its add_diag_reset_value): the first steps put b2 below -scalek (the transcript
+    rejects add_diag 1e-9 ... 1e-4 for that reason and settles on 1e-2)."""
+    from champ_b200.engine import Engine
     s = S.c2_bfd_example(0)
     nw = 8192
     eng = Engine(s, nw, prec)
@@ -34,7 +37,7 @@ def test_linear_method_descends_like_the_transcript(prec):
     nj, ncsf, norb = eng.nparam()
     P = nj + ncsf + norb
     jas = np.arange(ncsf + norb, P)  # the Jastrow parameters come last
-    energies = []
+    energies, stabs = [], []
     for it in range(4):
         e, err, sigma = vmc_energy(eng, s, seed=300 + it)
         energies.append((e, err))
@@ -48,18 +51,71 @@ def test_linear_method_descends_like_the_transcript(prec):
             Ssum += Sk
             Hsum += Hk
         idx = np.concatenate([[0], jas + 1])
-        dpj, info = linear_update(Ssum[np.ix_(idx, idx)], Hsum[np.ix_(idx, idx)], ncsf=0, sigma=sigma, diag_stab=1e-2)
-        dp = np.zeros(P)
-        dp[jas] = dpj
-        print(f"iteration {it}: E = {e:.5f} +- {err:.5f}, sigma {sigma:.4f}; eigenvalue {info[0]:.5f}, "
-              f"|dp| {np.abs(dpj).max():.3f}")
-        eng.apply_param_step(dp)
+        dp, stab, info = eng.linear_method_step(Ssum[np.ix_(idx, idx)], Hsum[np.ix_(idx, idx)], sigma, 1e-8, sel=jas)
+        stabs.append(stab)
+        assert np.all(dp[:ncsf + norb] == 0)
+        assert eng.check_param_step(np.zeros(P)) == 0
+        b2 = eng.get_params()["b"][0, 1]
+        assert b2 >= -s.scalek
+        print(f"iteration {it}: E = {e:.5f} +- {err:.5f}, sigma {sigma:.4f}; add_diag {stab:.1e}, eigenvalue "
+              f"{info[0]:.5f}, correlated {info[4]:.5f} {info[5]:.5f} {info[6]:.5f}, |dp| {np.abs(dp).max():.3f}, "
+              f"b2 {b2:.3f}")
     e, err, sigma = vmc_energy(eng, s, seed=400)
     energies.append((e, err))
     print("energies:", energies)
     assert energies[0][0] > -10.80 and energies[0][0] < -10.74  # the input's Jastrow (-10.7749 +- 0.0124)
+    assert stabs[0] > 1e-5  # the unstabilised first step is rejected, as in the transcript
     assert min(e for e, _ in energies[1:]) < -10.99
     assert energies[-1][0] < energies[0][0] - 0.2
+
+
+def test_check_param_step_flags_the_references_bad_moves():
+    """wf_update_and_check's criteria: b2 below -scalek (2), large Jastrow or total variations (1)."""
+    from champ_b200.engine import Engine
+    s = S.c2_bfd_example(0)
+    eng = Engine(s, 64, "fp64")
+    eng.set_walkers(S.initial_walkers(s, 64, seed=1))
+    nj, ncsf, norb = eng.nparam()
+    P = nj + ncsf + norb
+    jb = ncsf + norb + s.nctype * (s.norda - 1)  # b2 of the first spin set
+    b2 = eng.get_params()["b"][0, 1]
+    assert eng.check_param_step(np.zeros(P)) == 0
+    dp = np.zeros(P)
+    dp[jb] = -s.scalek - b2 - 0.01
+    assert eng.check_param_step(dp) == 2
+    dp[jb] = -s.scalek - b2 + 0.01
+    assert eng.check_param_step(dp) == 0
+    dp = np.zeros(P)
+    dp[ncsf + norb:] = 11.0 if s.scalek > 0.5 else 1e3
+    assert eng.check_param_step(dp) == 1
+    assert eng.check_param_step(np.zeros(P), psi_lin_var_norm=11.0) == 1
+    dp = np.zeros(P)
+    dp[-1] = np.nan
+    assert eng.check_param_step(dp) == 2
+
+
+def test_eval_param_step_is_correlated_sampling():
+    """E_L and ln|psi| ratios of a trial step equal a context created with the stepped parameters,
+    and the context is unchanged afterwards."""
+    from champ_b200.engine import Engine
+    s = S.c2_bfd_example(0)
+    nw = 128
+    x = S.initial_walkers(s, nw, seed=4)
+    a = Engine(s, nw, "fp64")
+    a.set_walkers(x)
+    e0 = a.eval_full()
+    P = sum(a.nparam())
+    dp = np.zeros(P)
+    dp[-3:] = [0.05, -0.02, 0.01]
+    el, dl = a.eval_param_step(dp)
+    after = a.eval_full()
+    assert np.array_equal(after["energy"], e0["energy"]) and np.array_equal(after["lnpsi"], e0["lnpsi"])
+    b = Engine(s, nw, "fp64")
+    b.set_walkers(x)
+    b.apply_param_step(dp)
+    e1 = b.eval_full()
+    assert np.allclose(el, e1["energy"], rtol=1e-12, atol=1e-10)
+    assert np.allclose(dl, e1["lnpsi"] - e0["lnpsi"], rtol=1e-12, atol=1e-12)
 
 
 def test_set_params_matches_a_new_context():
