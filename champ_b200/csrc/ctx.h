@@ -77,6 +77,13 @@ struct champ_ctx {
   double rot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
   bool have_walkers = false;
   KCfg kf, kd;  // FP32 and FP64 kernels (a mixed-precision context uses both)
+  // staged evaluation (elstage.cuh) of the FP64 state when it lives in HBM: on/off (option
+  // "staged_eval"), warps per block and dynamic shared memory of k_el_jas, k_el_orb, k_el_fin,
+  // and the pseudopotential scratch of k_el_fin (elements)
+  int el_staged = 0;
+  int el_wpb[3] = {4, 4, 4};
+  size_t el_smem[3] = {0, 0, 0};
+  int el_nscr = 0;
   // device staging for per-call host arrays
   double *d_in = nullptr, *d_out = nullptr;
   uint8_t *d_mask = nullptr;

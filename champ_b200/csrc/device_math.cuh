@@ -606,14 +606,15 @@ __host__ __device__ constexpr int mixed_index(const MixedPQ &x, int p, int q) {
   return -1;
 }
 
-// X sums of one pair: a[2c+1] = a_c (stride 2), r[2c+1] = r_c; mixed products only.
+// X sums of one pair: a[sa c] = a_c, r[sr c] = r_c (the scaled e-n distances of the two
+// electrons, strided); mixed products only.
 template <class T, int NORD>
-__device__ __forceinline__ void een_xsums(int C, const T *a, const T *r, T *X) {
+__device__ __forceinline__ void een_xsums(int C, const T *a, int sa, const T *r, int sr, T *X) {
   constexpr MixedPQ mx = make_mixed(NORD);
 #pragma unroll
   for (int i = 0; i < mx.n; i++) X[i] = T(0);
   for (int c = 0; c < C; c++) {
-    T ac = a[2 * c + 1], rc = r[2 * c + 1];
+    T ac = a[sa * c], rc = r[sr * c];
     T ap[NORD + 1], rp[NORD + 1];
     ap[0] = rp[0] = T(1);
 #pragma unroll

@@ -723,6 +723,29 @@ static int build_state(champ_ctx *c, State<T> &st) {
   return CHAMP_OK;
 }
 
+// The staged evaluation of an FP64 state in HBM (elstage.cuh): per-warp shared memory and warps
+// per block of its parts (up to 4 warps, at most 96 KB a block), and its per-walker scratch.
+static int setup_el_staged(champ_ctx *c) {
+  const size_t bytes[3] = {el_jas_bytes(c->N), el_orb_bytes<double>(c->nbasis),
+                           el_fin_bytes<double>(c->N, el_fin_scratch(c->N, c->C))};
+  for (int k = 0; k < 3; k++) {
+    int wpb = 4;
+    while (wpb > 1 && bytes[k] * wpb > 96 * 1024) wpb >>= 1;
+    if (bytes[k] * wpb > 200 * 1024) return CHAMP_OK;  // too large: the single-kernel evaluation
+    c->el_wpb[k] = wpb;
+    c->el_smem[k] = bytes[k] * wpb;
+  }
+  c->el_nscr = el_fin_scratch(c->N, c->C);
+  const size_t W = c->wmax, N = c->N;
+  State<double> &st = c->std_;
+  st.el_vj = dalloc<double>(c, W * 4 * N);
+  st.el_sc = dalloc<double>(c, W * 8);
+  st.el_rt = dalloc<double>(c, W * 2 * c->C * N);
+  if (!st.el_vj || !st.el_sc || !st.el_rt) return fail(CHAMP_ENOMEM, "allocation of the staged-evaluation scratch failed");
+  c->el_staged = 1;
+  return CHAMP_OK;
+}
+
 // Mixed precision: the FP32 state of the single-electron moves shares every FP64 buffer with the
 // FP64 state (positions, inverses, log-det, determinant tables, outputs, statistics) and owns
 // only the FP32 Jastrow pair table, distances and power sums, which every FP64 full evaluation
@@ -776,6 +799,29 @@ static int ev_mark(champ_ctx *c, int phase, bool start) {
 }
 
 static int launch(champ_ctx *c, Op op, const OpArgs &a = OpArgs()) {
+  if (op == Op::Vmc && a.phase < 0 && c->prec == CHAMP_PREC_FP64 && c->el_staged) {
+    // moves, then the staged E_L, per sweep (the E_L re-inverts the Slater matrices every sweep)
+    const State<double> &st = c->std_;
+    CK(cudaMemsetAsync(st.s_esum, 0, sizeof(double) * c->W, c->stream));
+    CK(cudaMemsetAsync(st.s_e2sum, 0, sizeof(double) * c->W, c->stream));
+    CK(cudaMemsetAsync(st.s_acc, 0, sizeof(double) * c->W, c->stream));
+    OpArgs b = a;
+    b.nsweep = 1;
+    for (int isw = 0; isw < a.nsweep; isw++) {
+      b.sweep0 = a.sweep0 + (uint64_t)isw;
+      b.phase = 1;
+      int rc = ev_mark(c, PH_MOVES, true);
+      if (!rc) rc = launch_f64(c, op, b);
+      if (!rc) rc = ev_mark(c, PH_MOVES, false);
+      if (rc) return rc;
+      b.phase = 3;
+      rc = ev_mark(c, PH_EVAL, true);
+      if (!rc) rc = launch_f64(c, op, b);
+      if (!rc) rc = ev_mark(c, PH_EVAL, false);
+      if (rc) return rc;
+    }
+    return CHAMP_OK;
+  }
   if (op == Op::Vmc && a.phase < 0 && c->prec != CHAMP_PREC_MIXED && !c->tc_on) {
     // the fused sweep kernel: moves and E_L in one launch
     int rc = ev_mark(c, PH_SWEEP, true);
@@ -1377,6 +1423,8 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
     c->kd.lay = make_layout<double>(c->N, c->C, c->nbasis, c->nmax, c->nomax, c->std_.astride, c->std_.tvstride,
                                     c->std_.gstride, c->std_.wstride, c->nloc > 0, RESIDENT_LIMIT);
     if (!rc) rc = finish_cfg(c->kd);
+    // walker state in HBM: the full evaluation as the four kernels of elstage.cuh
+    if (!rc && !c->kd.lay.resident) rc = setup_el_staged(c);
   }
   if (use32 && !rc) {
     rc = build_sys<float>(c, d, pcn, cfull, asa, asb, ecp, pecent, c->sf);
@@ -2005,6 +2053,12 @@ int champ_set_option(champ_ctx *c, const char *name, int64_t value) {
     c->pg_mode = (int)value;
     return CHAMP_OK;
   }
+  if (!strcmp(name, "staged_eval")) {
+    if (value && !c->std_.el_vj)
+      return fail(CHAMP_EINVAL, "staged_eval: needs an FP64 or mixed context whose walker state lives in HBM");
+    c->el_staged = value ? 1 : 0;
+    return CHAMP_OK;
+  }
   return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);
 }
 
@@ -2030,7 +2084,9 @@ int champ_get_option(const champ_ctx *c, const char *name, int64_t *value) {
   if (!strcmp(name, "orbital_tc")) { *value = c->tc_on ? c->tc_mode : 0; return CHAMP_OK; }
   if (!strcmp(name, "launches_per_sweep")) {
     int spins = (c->nup > 0) + (c->ndn > 0);
-    *value = c->tc_on ? 2 + spins + (c->tc_mode == 2 ? 1 : 0) : (c->prec == CHAMP_PREC_MIXED ? 2 : 1);
+    *value = c->tc_on                                     ? 2 + spins + (c->tc_mode == 2 ? 1 : 0)
+             : (c->el_staged && c->prec != CHAMP_PREC_FP32) ? 5
+             : (c->prec == CHAMP_PREC_MIXED ? 2 : 1);
     return CHAMP_OK;
   }
   if (!strcmp(name, "reinvert_every")) { *value = c->reinv_every; return CHAMP_OK; }
@@ -2038,6 +2094,7 @@ int champ_get_option(const champ_ctx *c, const char *name, int64_t *value) {
   if (!strcmp(name, "orbital_tc_chunk")) { *value = c->tc_kchunk; return CHAMP_OK; }
   if (!strcmp(name, "phase_timing")) { *value = c->ptime; return CHAMP_OK; }
   if (!strcmp(name, "param_grad_mode")) { *value = c->pg_mode; return CHAMP_OK; }
+  if (!strcmp(name, "staged_eval")) { *value = c->el_staged; return CHAMP_OK; }
   return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);
 }
 

@@ -56,6 +56,12 @@ struct State {
   // mixed precision: the FP32 tables of the single-electron moves ([W][N][N], [W][N][C][2],
   // [W][N][ZQ]), refreshed from the FP64 tables by every full evaluation; null otherwise
   float *m_fso, *m_ren, *m_zq;
+  // intermediates of the staged evaluation (elstage.cuh) of a state in HBM; null otherwise:
+  // per walker grad ln J and div of the Jastrow velocity [4N], scalars [8] (J, its Laplacian
+  // sum, e-e and e-n Coulomb energies, ln|D| and sign(D) of each spin), and the e-n distances
+  // as [2][C][N] planes
+  double *el_vj, *el_sc;
+  T *el_rt;
 };
 constexpr int NLT = 2 + MAXLCH;  // task record: (e*C+c), r, vps[0..MAXLCH-1]
 constexpr int ZQ = 8;            // stride of the per-electron power sums zq
@@ -86,13 +92,17 @@ struct View {
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
 
+// Elements of the per-warp basis scratch: the 5 channels of every basis function, and at least
+// 32 per centre (the pseudopotential points' distances to the centres reuse it).
+__host__ __device__ inline int phi_count(int nbasis, int C) { return nbasis * 5 > 32 * C ? nbasis * 5 : 32 * C; }
+
 template <class T>
 static Layout make_layout(int N, int C, int nbasis, int nmax, int nomax, int astride, int tvstride, int gstride,
                           int wstride, bool nl, size_t resident_limit) {
   Layout L;
   size_t o = 0;
   auto take = [&](size_t b) { size_t r = o; o += align16(b); return r; };
-  L.phi = take(sizeof(T) * nbasis * 5);
+  L.phi = take(sizeof(T) * phi_count(nbasis, C));
   L.arow = take(sizeof(T) * 5 * nomax);
   L.xs = take(sizeof(double) * N * 3);
   L.vacc = take(sizeof(double) * N * 3);
@@ -335,7 +345,7 @@ __device__ __forceinline__ T pair_value(const Sys<T> &s, const JasPar<T> &J, int
   if (NORD > 1 && !GRAD && J.nct == 1 && s.C <= MAXC_NL) {
     // value only, one centre type: X sums (see een_xsums)
     T X[make_mixed(NORD).n > 0 ? make_mixed(NORD).n : 1];
-    een_xsums<T, NORD>(s.C, re, rj, X);
+    een_xsums<T, NORD>(s.C, re + 1, 2, rj + 1, 2, X);
     f += een_from_x<T, NORD>(J.c[0], du, ae, zj, X);
   } else if (NORD > 1) {
     for (int c = 0; c < s.C; c++) {
@@ -507,11 +517,36 @@ template <class T, int NORD, bool SLOTS>
 __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const View<T> &v, int e, const double *xn,
                                    double coeff, const PGBuf &pg, const T *tsum_pre);
 
-template <class T, int NORD, bool MD, bool PG = false>
-__device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, const State<T> &st, int w,
-                          const View<T> &v, const double *R, int lane, bool outputs, EvalRes &res,
-                          const PGBuf *pg = nullptr, bool orbs_ready = false, bool reinvert = true) {
-  const int N = s.N, C = s.C, nomax = s.nomax;
+// Multi-determinant tables of one walker from the inverses of the reference determinant:
+// T = Ainv Atilde on the virtual columns (t_bld, deriv_fast_mod.f90:367-398), then Y and G
+// (build_gamma).  Returns ln|chi| and sign(chi).
+template <class T>
+__device__ void md_tables(const Sys<T> &s, const View<T> &v, int lane, double &lc, double &sc) {
+  const int nomax = s.nomax;
+  for (int sp = 0; sp < 2; sp++) {
+    const int n = sp ? s.ndn : s.nup, nv = s.nvirt[sp], e0 = sp ? s.nup : 0;
+    const double *A = v.ainv + (sp ? s.nup * s.nup : 0);
+    double *Tv = v.tv + (sp ? s.nup * s.nvirt[0] : 0);
+    for (int i = lane; i < n * nv; i += 32) {
+      int k = i / nv, p = i - k * nv;
+      double acc = 0;
+      for (int e = 0; e < n; e++) acc += A[k * n + e] * (double)v.orb5[(size_t)(e0 + e) * 5 * nomax + n + p];
+      Tv[i] = acc;
+    }
+  }
+  __syncwarp();
+  build_gamma(s, v, lane, lc, sc);
+}
+
+// Distances to the centres (ren, zq), the Jastrow factor with its gradient (v.vacc) and the
+// divergence of its velocity (v.divj) per electron, the pair table fso (jastrow4.f90,
+// distances.f90) and the e-e (and, all-electron, e-n) Coulomb energies of one walker.  TR: the
+// e-n distances are also written to, and the pair and e-n terms read from, rt = [2][C][N]
+// (distance plane, then scaled-distance plane; consecutive electrons adjacent).
+template <class T, int NORD, bool TR>
+__device__ void jastrow_tables(const Sys<T> &s, const JasPar<T> &J, const View<T> &v, T *rt, int lane, double &fsum,
+                               double &d2j, double &pe_ee, double &pe_en) {
+  const int N = s.N, C = s.C;
   const double *xs = v.xs;
   T *fso = v.fso;
   const T sk = J.scalek;
@@ -522,6 +557,10 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
     cen_dist(s, sk, xs + 3 * e, c, r, d);
     v.ren[2 * i] = r;
     v.ren[2 * i + 1] = d;
+    if (TR) {
+      rt[c * N + e] = r;
+      rt[(C + c) * N + e] = d;
+    }
   }
   __syncwarp();
   for (int e = lane; e < N; e += 32) {
@@ -538,7 +577,10 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
   for (int i = lane; i < N; i += 32) v.divj[i] = 0;
   __syncwarp();
   // --- Jastrow (jastrow4.f90) and e-e Coulomb (distances.f90:131-158)
-  double fsum = 0, d2j = 0, pe_ee = 0, pe_en = 0;
+  fsum = 0, d2j = 0, pe_ee = 0, pe_en = 0;
+  // distance of electron e to centre c and its scaled form (TR: from the transposed planes)
+  auto rof = [&](int e, int c) -> T { return TR ? rt[c * N + e] : v.ren[2 * (e * C + c)]; };
+  auto dof = [&](int e, int c) -> T { return TR ? rt[(C + c) * N + e] : v.ren[2 * (e * C + c) + 1]; };
   const int npair = N * (N - 1) / 2;
   for (int p = lane; p < npair; p += 32) {
     int i = (int)((1.0 + sqrt(1.0 + 8.0 * (double)p)) * 0.5);
@@ -562,12 +604,11 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
     for (int k = 0; k < 3; k++) { gi[k] = fu * rv[k]; gj[k] = -fu * rv[k]; }
     T d2 = 2 * (fuu + 2 * fu);
     if (NORD > 1) {
-      const T *ri_ = v.ren + 2 * C * i, *rj_ = v.ren + 2 * C * j;
       for (int c = 0; c < C; c++) {
         const double *cc = s.cent + 3 * c;
-        T ri = ri_[2 * c], rj = rj_[2 * c];
+        T ri = rof(i, c), rj = rof(j, c);
         Een<T> o;
-        jas_een<T, NORD, 2>(J, s.ctype[c], rij, du, ri, ri_[2 * c + 1], rj, rj_[2 * c + 1], o);
+        jas_een<T, NORD, 2>(J, s.ctype[c], rij, du, ri, dof(i, c), rj, dof(j, c), o);
         f += o.fc;
 #pragma unroll
         for (int k = 0; k < 3; k++) {
@@ -597,7 +638,7 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
     T f = 0, d2 = 0, g[3] = {0, 0, 0};
     for (int c = 0; c < C; c++) {
       const double *cc = s.cent + 3 * c;
-      T r = v.ren[2 * (i * C + c)], dn = v.ren[2 * (i * C + c) + 1];
+      T r = rof(i, c), dn = dof(i, c);
       T fi, fii;
       f += jas_en<T, true>(J, s.ctype[c], r, dn, fi, fii);
 #pragma unroll
@@ -621,60 +662,16 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
   pe_ee = warp_sum(pe_ee);
   pe_en = warp_sum(pe_en);
   __syncwarp();
+}
 
-  // --- orbitals of every electron, Slater matrices (determinant.f90:36-42, t_bld); with
-  // orbs_ready they were computed for all walkers by the tensor-core contraction
-  double *ainv = v.ainv;
-  T *orb5 = v.orb5;
-  for (int e = 0; e < N; e++) {
-    int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
-    double *A = ainv + (sp ? s.nup * s.nup : 0);
-    T *oe = orb5 + (size_t)e * 5 * nomax;
-    if (!orbs_ready) {
-      warp_basis<T, 5>(s, xs + 3 * e, v.phi, lane);
-      warp_orbitals<T, 5>(v.phi, s.cocc[sp], s.nbasis, s.nocc[sp], oe, nomax, lane);
-    }
-    if (reinvert)
-      for (int k = lane; k < n; k += 32) A[eo * n + k] = (double)oe[k];
-  }
-  __syncwarp();
-  double lnd = 0, sgn = 1;
-  bool ok = true;
-  if (!reinvert) {
-    // inverses, T and G as kept current by the accepted moves' updates; ln|psi_D| likewise
-    lnd = st.lnd[w];
-    sgn = st.sgn[w];
-    ok = isfinite(lnd) && sgn != 0.0;
-  }
-  for (int sp = 0; sp < 2 && reinvert; sp++) {
-    int n = sp ? s.ndn : s.nup;
-    if (n == 0) continue;
-    double l1, s1;
-    bool o1 = warp_gj(ainv + (sp ? s.nup * s.nup : 0), n, v.perm, l1, s1, lane);
-    ok = ok && o1;
-    lnd += l1;
-    sgn *= s1;
-  }
-  if (MD && ok && reinvert) {
-    // T = Ainv Atilde on the virtual columns (t_bld, deriv_fast_mod.f90:367-398)
-    for (int sp = 0; sp < 2; sp++) {
-      const int n = sp ? s.ndn : s.nup, nv = s.nvirt[sp], e0 = sp ? s.nup : 0;
-      const double *A = ainv + (sp ? s.nup * s.nup : 0);
-      double *Tv = v.tv + (sp ? s.nup * s.nvirt[0] : 0);
-      for (int i = lane; i < n * nv; i += 32) {
-        int k = i / nv, p = i - k * nv;
-        double acc = 0;
-        for (int e = 0; e < n; e++) acc += A[k * n + e] * (double)orb5[(size_t)(e0 + e) * 5 * nomax + n + p];
-        Tv[i] = acc;
-      }
-    }
-    __syncwarp();
-    double lc, sc;
-    build_gamma(s, v, lane, lc, sc);
-    lnd += lc;
-    sgn *= sc;
-  }
-  // --- grad ln D, lap D / D per electron (determinant.f90:96-150)
+// grad ln D and lap D / D of every electron (determinant.f90:96-150) from G and the orbitals'
+// gradients and Laplacians; with the Jastrow velocities in v.vacc gives the velocities, |v|^2
+// and sum lap ln D.
+template <class T, bool MD, bool PG>
+__device__ void det_velocities(const Sys<T> &s, const State<T> &st, int w, const View<T> &v, int lane, bool outputs,
+                               const PGBuf *pg, double &d2lnd_o, double &v2_o) {
+  const int N = s.N, nomax = s.nomax;
+  const T *orb5 = v.orb5;
   double d2lnd = 0, v2 = 0;
   for (int e = 0; e < N; e++) {
     int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
@@ -702,233 +699,255 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
       st.o_divv[(size_t)w * N + e] = v.divj[e] + dvd;
     }
   }
+  d2lnd_o = d2lnd;
+  v2_o = v2;
+}
 
-  // --- pseudopotential (nonloc_pot.f90, nonloc.f90), quadrature rotated by R
+// Nonlocal pseudopotential energy of one walker (nonloc_pot.f90, nonloc.f90), quadrature rotated
+// by R.  scr: nscr elements of per-warp shared scratch, holding the radial parts of the tasks'
+// centres' shells and, on the one-centre-type path, each lane's scaled point-centre distances
+// (stored [centre][lane], 32 C elements at the end).  Returns the local and nonlocal parts and
+// the number of (electron, centre) tasks.
+template <class T, int NORD, bool MD, bool PG>
+__device__ void nlpp_energy(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, const View<T> &v, const double *R,
+                            int lane, const PGBuf *pg, T *scr, int nscr, double &vloc_o, double &vnl_o, int &ntask_o) {
+  const int N = s.N, C = s.C, B = s.nbasis;
+  const double *xs = v.xs;
+  const T *fso = v.fso;
+  const T sk = J.scalek;
+  const bool fast = (NORD > 1) && J.nct == 1 && C <= MAXC_NL;
+  const int nrown = nscr - (fast ? 32 * C : 0);
+  T *const prs = fast ? scr + nrown + lane : nullptr;  // this lane's point-centre distances, stride 32
   double vloc = 0, vnl = 0;
-  int ntask_all = 0;
-  if (s.nloc > 0 && ok) {
-    const int B = s.nbasis;
-    T *gp = v.gproj;
-    // G projected onto the basis: g_e[b] = sum_k coef[b][k] G[k][e] (psp_nonloc_pot_bld), one
-    // [nbasis x nocc] x [nocc x n] product per spin in compute precision: lanes along b over
-    // rows of the transposed coefficients (coalesced), 4 electrons x 4 basis functions per lane.
-    for (int sp = 0; sp < 2; sp++) {
-      const int n = sp ? s.ndn : s.nup, e0 = sp ? s.nup : 0, no = s.nocc[sp];
-      const double *G = gam_ptr<T, MD>(s, v, sp);
-      const T *ct = s.coccT[sp];
-      for (int eo0 = 0; eo0 < n; eo0 += 4) {
-        const int ne = min(4, n - eo0);
-        for (int b0 = 0; b0 < B; b0 += 128) {
-          T acc[4][4];
+  T *gp = v.gproj;
+  // G projected onto the basis: g_e[b] = sum_k coef[b][k] G[k][e] (psp_nonloc_pot_bld), one
+  // [nbasis x nocc] x [nocc x n] product per spin in compute precision: lanes along b over
+  // rows of the transposed coefficients (coalesced), 4 electrons x 4 basis functions per lane.
+  for (int sp = 0; sp < 2; sp++) {
+    const int n = sp ? s.ndn : s.nup, e0 = sp ? s.nup : 0, no = s.nocc[sp];
+    const double *G = gam_ptr<T, MD>(s, v, sp);
+    const T *ct = s.coccT[sp];
+    for (int eo0 = 0; eo0 < n; eo0 += 4) {
+      const int ne = min(4, n - eo0);
+      for (int b0 = 0; b0 < B; b0 += 128) {
+        T acc[4][4];
 #pragma unroll
-          for (int i = 0; i < 4; i++)
+        for (int i = 0; i < 4; i++)
 #pragma unroll
-            for (int j = 0; j < 4; j++) acc[i][j] = T(0);
-          for (int k = 0; k < no; k++) {
-            T g[4];
+          for (int j = 0; j < 4; j++) acc[i][j] = T(0);
+        for (int k = 0; k < no; k++) {
+          T g[4];
 #pragma unroll
-            for (int i = 0; i < 4; i++) g[i] = (i < ne) ? (T)G[k * n + eo0 + i] : T(0);
-            const T *row = ct + (size_t)k * B + b0 + lane;
+          for (int i = 0; i < 4; i++) g[i] = (i < ne) ? (T)G[k * n + eo0 + i] : T(0);
+          const T *row = ct + (size_t)k * B + b0 + lane;
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-              T cf = (b0 + lane + 32 * j < B) ? row[32 * j] : T(0);
+          for (int j = 0; j < 4; j++) {
+            T cf = (b0 + lane + 32 * j < B) ? row[32 * j] : T(0);
 #pragma unroll
-              for (int i = 0; i < 4; i++) acc[i][j] += cf * g[i];
-            }
-          }
-#pragma unroll
-          for (int i = 0; i < 4; i++)
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-              int b = b0 + lane + 32 * j;
-              if (i < ne && b < B) gp[(size_t)(e0 + eo0 + i) * B + b] = acc[i][j];
-            }
-        }
-      }
-    }
-    double *tl = v.nlt;
-    int ntask = 0;
-    // tasks in centre-major order, so that the points of one round of 32 lanes mostly share
-    // their centre (and with it the shells whose radial parts are precomputed per task)
-    for (int base = 0; base < N * C; base += 32) {
-      const int j = base + lane;
-      int idx = j;
-      bool nl = false;
-      double vps[MAXLCH], r = 0;
-      int c = 0;
-      if (j < N * C) {
-        c = j / N;
-        const int e = j - c * N;
-        idx = e * C + c;
-        const double *cc = s.cent + 3 * c, *xe = xs + 3 * e;
-        r = sqrt((xe[0] - cc[0]) * (xe[0] - cc[0]) + (xe[1] - cc[1]) * (xe[1] - cc[1]) +
-                 (xe[2] - cc[2]) * (xe[2] - cc[2]));
-        int it = s.ctype[c];
-        ecp_vps(E, it, r, vps);
-        vloc += vps[E.lpotp1[it] - 1];
-        for (int l = 0; l < E.npotd[it]; l++)
-          if (l + 1 != E.lpotp1[it] && fabs(vps[l]) > 1e-4) nl = true;
-      }
-      unsigned m = __ballot_sync(0xffffffffu, nl);
-      if (nl) {
-        int pos = ntask + __popc(m & ((1u << lane) - 1u));
-        double *rec = tl + (size_t)pos * NLT;
-        rec[0] = (double)idx;
-        rec[1] = r;
-        for (int l = 0; l < MAXLCH; l++) rec[2 + l] = (l < E.npotd[s.ctype[c]]) ? vps[l] : 0.0;
-      }
-      ntask += __popc(m);
-    }
-    vloc = warp_sum(vloc);
-    ntask_all = ntask;
-    __syncwarp();
-    const int nq = E.nquad;
-    // The points of an (electron, centre) task lie at the task's distance r from that centre, so
-    // the radial parts of the centre's own shells are evaluated once per task (into the per-warp
-    // basis scratch, unused in this phase) when the table fits there.
-    const int nshc = (s.nshc > 0 && ntask * s.nshc <= B * 5) ? s.nshc : 0;
-    T *rown = v.phi;  // [ntask][nshc]
-    if (nshc > 0) {
-      for (int i = lane; i < ntask * nshc; i += 32) {
-        const int tk = i / nshc, k = i - tk * nshc;
-        const double *rc = tl + (size_t)tk * NLT;
-        const int ci = (int)rc[0] % C, ish = s.cshell0[ci] + k;
-        if (ish < s.cshell0[ci + 1]) {
-          T R3[3];
-          shell_radial<T, false>(s, ish, (T)rc[1], R3);
-          rown[i] = R3[0];
-        }
-      }
-      __syncwarp();
-    }
-    for (int t = lane; t < ntask * nq; t += 32) {
-      int task = t / nq, q = t - task * nq;
-      const double *rec = tl + (size_t)task * NLT;
-      int idx = (int)rec[0], e = idx / C, c = idx - (idx / C) * C;
-      double r = rec[1];
-      const double *cc = s.cent + 3 * c, *xe = xs + 3 * e;
-      double qv[3];
-#pragma unroll
-      for (int k = 0; k < 3; k++) qv[k] = R[3 * k] * s.quad->q0[q][0] + R[3 * k + 1] * s.quad->q0[q][1] + R[3 * k + 2] * s.quad->q0[q][2];
-      double costh = ((xe[0] - cc[0]) * qv[0] + (xe[1] - cc[1]) * qv[1] + (xe[2] - cc[2]) * qv[2]) / r;
-      double xn[3] = {cc[0] + r * qv[0], cc[1] + r * qv[1], cc[2] + r * qv[2]};
-      // determinant ratio: orbitals at the point contracted with G
-      const T *ge = gp + (size_t)e * B;
-      T dr = 0;
-      const int c0 = nshc > 0 ? s.cshell0[c] : 0, c1 = nshc > 0 ? s.cshell0[c + 1] : 0;
-      const T *ro = rown + task * nshc - c0;
-      // with the nonlocal B-matrix sums wanted, the basis values at the point are formed once,
-      // after the Jastrow ratio, for both the ratio and those sums
-      const bool merged = PG && pg->phis != nullptr;
-      if (!merged)
-        for (int ish = 0; ish < s.nshell; ish++)
-          dr += shell_dot_r<T>(s, ish, xn, ge, (ish >= c0 && ish < c1) ? ro + ish : nullptr);
-      // Jastrow ratio (nonlocj, nonloc.f90:432-522): point-centre distances once per point
-      double dj = 0;
-      const bool fast = (NORD > 1) && J.nct == 1 && C <= MAXC_NL;
-      T pr[2 * MAXC_NL], asum[ZQ];
-      {
-        T f = 0;
-        for (int q2 = 0; q2 < ZQ; q2++) asum[q2] = (q2 == 0) ? T(C) : T(0);
-        for (int c2 = 0; c2 < C; c2++) {
-          T ri, di, fi, fii;
-          cen_dist(s, sk, xn, c2, ri, di);
-          f += jas_en<T, false>(J, s.ctype[c2], ri, di, fi, fii);
-          if (fast) {
-            pr[2 * c2] = ri;
-            pr[2 * c2 + 1] = di;
-            T p = di;
-            for (int q2 = 1; q2 < ZQ; q2++) { asum[q2] += p; p *= di; }
+            for (int i = 0; i < 4; i++) acc[i][j] += cf * g[i];
           }
         }
-        dj += (double)f - (double)fso[e * N + e];
-      }
-      // FP32 derivative run: the e-e-n parameter basis functions at the point, summed over the
-      // other electrons from the same X sums as the value (handed to point_param_values).  The
-      // FP64 run forms them there instead: 13 more FP64 registers here cost it more in spills.
-      constexpr bool SHARE = PG && std::is_same<T, float>::value;
-      constexpr int NT = make_terms(NORD).n > 0 ? make_terms(NORD).n : 1;
-      T tsum[SHARE ? NT : 1];
-      if (SHARE)
 #pragma unroll
-        for (int ll = 0; ll < NT; ll++) tsum[ll] = T(0);
-      for (int j = 0; j < N; j++) {
-        if (j == e) continue;
-        int isb, ipar;
-        T ss;
-        pair_class(J, s.nup, e, j, isb, ss, ipar);
-        const double *xj = xs + 3 * j;
-        T a0 = T(xn[0] - xj[0]), a1 = T(xn[1] - xj[1]), a2 = T(xn[2] - xj[2]);
-        T rij = tsqrt(a0 * a0 + a1 * a1 + a2 * a2);
-        T du = T(1) / (T(1) + sk * rij);
-        T fu, fuu;
-        T f = jas_ee<T, false>(J, isb, ss, ipar, rij, du, fu, fuu);
-        if (fast) {
-          T X[make_mixed(NORD).n > 0 ? make_mixed(NORD).n : 1];
-          een_xsums<T, NORD>(C, pr, v.ren + 2 * C * j, X);
-          if (SHARE) {
-            constexpr Terms tl = make_terms(NORD);
-            constexpr XIdx xi = make_xidx(NORD);
-            const T *zj = v.zq + ZQ * j;
-            T uu[NORD + 1];
-            uu[0] = T(1);
+        for (int i = 0; i < 4; i++)
 #pragma unroll
-            for (int q2 = 1; q2 <= NORD; q2++) uu[q2] = uu[q2 - 1] * du;
-#pragma unroll
-            for (int ll = 0; ll < tl.n; ll++) {
-              const T t = uu[tl.k[ll]] * (xsel(xi.a1[ll], asum, zj, X) + xsel(xi.a2[ll], asum, zj, X));
-              f += J.c[0][ll] * t;
-              tsum[ll] += t;
-            }
-          } else {
-            f += een_from_x<T, NORD>(J.c[0], du, asum, v.zq + ZQ * j, X);
+          for (int j = 0; j < 4; j++) {
+            int b = b0 + lane + 32 * j;
+            if (i < ne && b < B) gp[(size_t)(e0 + eo0 + i) * B + b] = acc[i][j];
           }
-        } else if (NORD > 1) {
-          const T *rj_ = v.ren + 2 * C * j;
-          for (int c2 = 0; c2 < C; c2++) {
-            T ri, di;
-            cen_dist(s, sk, xn, c2, ri, di);
-            Een<T> o;
-            jas_een<T, NORD, 0>(J, s.ctype[c2], rij, du, ri, di, rj_[2 * c2], rj_[2 * c2 + 1], o);
-            f += o.fc;
-          }
-        }
-        dj += (double)f - (double)fso[e * N + j];
       }
-      int it = s.ctype[c];
-      double vp = 0;
-      for (int l = 0; l < E.npotd[it]; l++)
-        if (l + 1 != E.lpotp1[it]) vp += rec[2 + l] * yl0(l, costh);
-      if (merged) {
-        const double c2 = s.quad->wq[q] * exp(dj) * vp;
-        double *ph = pg->phis + (size_t)e * s.nbasis;
-        for (int ish = 0; ish < s.nshell; ish++)
-          dr += shell_dot_acc<T>(s, ish, xn, ge, (ish >= c0 && ish < c1) ? ro + ish : nullptr, c2, ph);
-      }
-      vnl += s.quad->wq[q] * exp(dj) * vp * (double)dr;
-      if (PG) {
-        double coeff = s.quad->wq[q] * exp(dj) * vp * (double)dr;
-        atomicAdd(&pg->csum[e], coeff);
-        if (pg->tape) {
-          pg->tape[t] = coeff;  // the backward pass forms the parameter sums at this point
-        } else {
-          const T *ts = (SHARE && fast) ? tsum : nullptr;
-          if (pg->dvl) point_param_values<T, NORD, true>(s, J, v, e, xn, coeff, *pg, ts);
-          else point_param_values<T, NORD, false>(s, J, v, e, xn, coeff, *pg, ts);
-        }
-      }
-    }
-    vnl = warp_sum(vnl);
-    if (PG && pg->dvl) {
-      __syncwarp();
-      for (int p = lane; p < pg->P; p += 32) {
-        double a = 0;
-        for (int l = 0; l < 32; l++) a += pg->dvl[p * 32 + l];
-        pg->dvn[p] += a;
-      }
-      __syncwarp();
     }
   }
+  double *tl = v.nlt;
+  int ntask = 0;
+  // tasks in centre-major order, so that the points of one round of 32 lanes mostly share
+  // their centre (and with it the shells whose radial parts are precomputed per task)
+  for (int base = 0; base < N * C; base += 32) {
+    const int j = base + lane;
+    int idx = j;
+    bool nl = false;
+    double vps[MAXLCH], r = 0;
+    int c = 0;
+    if (j < N * C) {
+      c = j / N;
+      const int e = j - c * N;
+      idx = e * C + c;
+      const double *cc = s.cent + 3 * c, *xe = xs + 3 * e;
+      r = sqrt((xe[0] - cc[0]) * (xe[0] - cc[0]) + (xe[1] - cc[1]) * (xe[1] - cc[1]) +
+               (xe[2] - cc[2]) * (xe[2] - cc[2]));
+      int it = s.ctype[c];
+      ecp_vps(E, it, r, vps);
+      vloc += vps[E.lpotp1[it] - 1];
+      for (int l = 0; l < E.npotd[it]; l++)
+        if (l + 1 != E.lpotp1[it] && fabs(vps[l]) > 1e-4) nl = true;
+    }
+    unsigned m = __ballot_sync(0xffffffffu, nl);
+    if (nl) {
+      int pos = ntask + __popc(m & ((1u << lane) - 1u));
+      double *rec = tl + (size_t)pos * NLT;
+      rec[0] = (double)idx;
+      rec[1] = r;
+      for (int l = 0; l < MAXLCH; l++) rec[2 + l] = (l < E.npotd[s.ctype[c]]) ? vps[l] : 0.0;
+    }
+    ntask += __popc(m);
+  }
+  vloc = warp_sum(vloc);
+  ntask_o = ntask;
+  __syncwarp();
+  const int nq = E.nquad;
+  // The points of an (electron, centre) task lie at the task's distance r from that centre, so
+  // the radial parts of the centre's own shells are evaluated once per task (into the per-warp
+  // basis scratch, unused in this phase) when the table fits there.
+  const int nshc = (s.nshc > 0 && ntask * s.nshc <= nrown) ? s.nshc : 0;
+  T *rown = scr;  // [ntask][nshc]
+  if (nshc > 0) {
+    for (int i = lane; i < ntask * nshc; i += 32) {
+      const int tk = i / nshc, k = i - tk * nshc;
+      const double *rc = tl + (size_t)tk * NLT;
+      const int ci = (int)rc[0] % C, ish = s.cshell0[ci] + k;
+      if (ish < s.cshell0[ci + 1]) {
+        T R3[3];
+        shell_radial<T, false>(s, ish, (T)rc[1], R3);
+        rown[i] = R3[0];
+      }
+    }
+    __syncwarp();
+  }
+  for (int t = lane; t < ntask * nq; t += 32) {
+    int task = t / nq, q = t - task * nq;
+    const double *rec = tl + (size_t)task * NLT;
+    int idx = (int)rec[0], e = idx / C, c = idx - (idx / C) * C;
+    double r = rec[1];
+    const double *cc = s.cent + 3 * c, *xe = xs + 3 * e;
+    double qv[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) qv[k] = R[3 * k] * s.quad->q0[q][0] + R[3 * k + 1] * s.quad->q0[q][1] + R[3 * k + 2] * s.quad->q0[q][2];
+    double costh = ((xe[0] - cc[0]) * qv[0] + (xe[1] - cc[1]) * qv[1] + (xe[2] - cc[2]) * qv[2]) / r;
+    double xn[3] = {cc[0] + r * qv[0], cc[1] + r * qv[1], cc[2] + r * qv[2]};
+    // determinant ratio: orbitals at the point contracted with G
+    const T *ge = gp + (size_t)e * B;
+    T dr = 0;
+    const int c0 = nshc > 0 ? s.cshell0[c] : 0, c1 = nshc > 0 ? s.cshell0[c + 1] : 0;
+    const T *ro = rown + task * nshc - c0;
+    // with the nonlocal B-matrix sums wanted, the basis values at the point are formed once,
+    // after the Jastrow ratio, for both the ratio and those sums
+    const bool merged = PG && pg->phis != nullptr;
+    if (!merged)
+      for (int ish = 0; ish < s.nshell; ish++)
+        dr += shell_dot_r<T>(s, ish, xn, ge, (ish >= c0 && ish < c1) ? ro + ish : nullptr);
+    // Jastrow ratio (nonlocj, nonloc.f90:432-522): point-centre distances once per point
+    double dj = 0;
+    T asum[ZQ];
+    {
+      T f = 0;
+      for (int q2 = 0; q2 < ZQ; q2++) asum[q2] = (q2 == 0) ? T(C) : T(0);
+      for (int c2 = 0; c2 < C; c2++) {
+        T ri, di, fi, fii;
+        cen_dist(s, sk, xn, c2, ri, di);
+        f += jas_en<T, false>(J, s.ctype[c2], ri, di, fi, fii);
+        if (fast) {
+          prs[32 * c2] = di;
+          T p = di;
+          for (int q2 = 1; q2 < ZQ; q2++) { asum[q2] += p; p *= di; }
+        }
+      }
+      dj += (double)f - (double)fso[e * N + e];
+    }
+    // FP32 derivative run: the e-e-n parameter basis functions at the point, summed over the
+    // other electrons from the same X sums as the value (handed to point_param_values).  The
+    // FP64 run forms them there instead: 13 more FP64 registers here cost it more in spills.
+    constexpr bool SHARE = PG && std::is_same<T, float>::value;
+    constexpr int NT = make_terms(NORD).n > 0 ? make_terms(NORD).n : 1;
+    T tsum[SHARE ? NT : 1];
+    if (SHARE)
+#pragma unroll
+      for (int ll = 0; ll < NT; ll++) tsum[ll] = T(0);
+    for (int j = 0; j < N; j++) {
+      if (j == e) continue;
+      int isb, ipar;
+      T ss;
+      pair_class(J, s.nup, e, j, isb, ss, ipar);
+      const double *xj = xs + 3 * j;
+      T a0 = T(xn[0] - xj[0]), a1 = T(xn[1] - xj[1]), a2 = T(xn[2] - xj[2]);
+      T rij = tsqrt(a0 * a0 + a1 * a1 + a2 * a2);
+      T du = T(1) / (T(1) + sk * rij);
+      T fu, fuu;
+      T f = jas_ee<T, false>(J, isb, ss, ipar, rij, du, fu, fuu);
+      if (fast) {
+        T X[make_mixed(NORD).n > 0 ? make_mixed(NORD).n : 1];
+        een_xsums<T, NORD>(C, prs, 32, v.ren + 2 * C * j + 1, 2, X);
+        if (SHARE) {
+          constexpr Terms tl = make_terms(NORD);
+          constexpr XIdx xi = make_xidx(NORD);
+          const T *zj = v.zq + ZQ * j;
+          T uu[NORD + 1];
+          uu[0] = T(1);
+#pragma unroll
+          for (int q2 = 1; q2 <= NORD; q2++) uu[q2] = uu[q2 - 1] * du;
+#pragma unroll
+          for (int ll = 0; ll < tl.n; ll++) {
+            const T t = uu[tl.k[ll]] * (xsel(xi.a1[ll], asum, zj, X) + xsel(xi.a2[ll], asum, zj, X));
+            f += J.c[0][ll] * t;
+            tsum[ll] += t;
+          }
+        } else {
+          f += een_from_x<T, NORD>(J.c[0], du, asum, v.zq + ZQ * j, X);
+        }
+      } else if (NORD > 1) {
+        const T *rj_ = v.ren + 2 * C * j;
+        for (int c2 = 0; c2 < C; c2++) {
+          T ri, di;
+          cen_dist(s, sk, xn, c2, ri, di);
+          Een<T> o;
+          jas_een<T, NORD, 0>(J, s.ctype[c2], rij, du, ri, di, rj_[2 * c2], rj_[2 * c2 + 1], o);
+          f += o.fc;
+        }
+      }
+      dj += (double)f - (double)fso[e * N + j];
+    }
+    int it = s.ctype[c];
+    double vp = 0;
+    for (int l = 0; l < E.npotd[it]; l++)
+      if (l + 1 != E.lpotp1[it]) vp += rec[2 + l] * yl0(l, costh);
+    if (merged) {
+      const double c2 = s.quad->wq[q] * exp(dj) * vp;
+      double *ph = pg->phis + (size_t)e * s.nbasis;
+      for (int ish = 0; ish < s.nshell; ish++)
+        dr += shell_dot_acc<T>(s, ish, xn, ge, (ish >= c0 && ish < c1) ? ro + ish : nullptr, c2, ph);
+    }
+    vnl += s.quad->wq[q] * exp(dj) * vp * (double)dr;
+    if (PG) {
+      double coeff = s.quad->wq[q] * exp(dj) * vp * (double)dr;
+      atomicAdd(&pg->csum[e], coeff);
+      if (pg->tape) {
+        pg->tape[t] = coeff;  // the backward pass forms the parameter sums at this point
+      } else {
+        const T *ts = (SHARE && fast) ? tsum : nullptr;
+        if (pg->dvl) point_param_values<T, NORD, true>(s, J, v, e, xn, coeff, *pg, ts);
+        else point_param_values<T, NORD, false>(s, J, v, e, xn, coeff, *pg, ts);
+      }
+    }
+  }
+  vnl = warp_sum(vnl);
+  if (PG && pg->dvl) {
+    __syncwarp();
+    for (int p = lane; p < pg->P; p += 32) {
+      double a = 0;
+      for (int l = 0; l < 32; l++) a += pg->dvl[p * 32 + l];
+      pg->dvn[p] += a;
+    }
+    __syncwarp();
+  }
+  vloc_o = vloc;
+  vnl_o = vnl;
+}
+
+// E_L and the outputs of one walker's full evaluation from its parts (hpsi.f90:336-344): the
+// walker's log-determinant, Jastrow, status and, with outputs, the per-walker output arrays.
+template <class T>
+__device__ void finish_eval(const Sys<T> &s, const State<T> &st, int w, const View<T> &v, int lane, bool outputs,
+                            bool ok, double lnd, double sgn, double fsum, double d2j, double pe_ee, double pe_en,
+                            double d2lnd, double v2, double vloc, double vnl, int ntask_all, EvalRes &res) {
+  const int N = s.N;
   double pe = s.pecent + pe_ee + (s.nloc > 0 ? vloc + vnl : pe_en);
   double d2lnpsi = d2lnd + d2j;
   double eloc = pe - HB * (d2lnpsi + v2);
@@ -968,6 +987,66 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
       st.o_eloc[w] = eloc;
     }
   }
+  __syncwarp();
+}
+
+template <class T, int NORD, bool MD, bool PG = false>
+__device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, const State<T> &st, int w,
+                          const View<T> &v, const double *R, int lane, bool outputs, EvalRes &res,
+                          const PGBuf *pg = nullptr, bool orbs_ready = false, bool reinvert = true) {
+  const int N = s.N, C = s.C, nomax = s.nomax;
+  const double *xs = v.xs;
+  double fsum, d2j, pe_ee, pe_en;
+  jastrow_tables<T, NORD, false>(s, J, v, nullptr, lane, fsum, d2j, pe_ee, pe_en);
+
+  // --- orbitals of every electron, Slater matrices (determinant.f90:36-42, t_bld); with
+  // orbs_ready they were computed for all walkers by the tensor-core contraction
+  double *ainv = v.ainv;
+  T *orb5 = v.orb5;
+  for (int e = 0; e < N; e++) {
+    int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
+    double *A = ainv + (sp ? s.nup * s.nup : 0);
+    T *oe = orb5 + (size_t)e * 5 * nomax;
+    if (!orbs_ready) {
+      warp_basis<T, 5>(s, xs + 3 * e, v.phi, lane);
+      warp_orbitals<T, 5>(v.phi, s.cocc[sp], s.nbasis, s.nocc[sp], oe, nomax, lane);
+    }
+    if (reinvert)
+      for (int k = lane; k < n; k += 32) A[eo * n + k] = (double)oe[k];
+  }
+  __syncwarp();
+  double lnd = 0, sgn = 1;
+  bool ok = true;
+  if (!reinvert) {
+    // inverses, T and G as kept current by the accepted moves' updates; ln|psi_D| likewise
+    lnd = st.lnd[w];
+    sgn = st.sgn[w];
+    ok = isfinite(lnd) && sgn != 0.0;
+  }
+  for (int sp = 0; sp < 2 && reinvert; sp++) {
+    int n = sp ? s.ndn : s.nup;
+    if (n == 0) continue;
+    double l1, s1;
+    bool o1 = warp_gj(ainv + (sp ? s.nup * s.nup : 0), n, v.perm, l1, s1, lane);
+    ok = ok && o1;
+    lnd += l1;
+    sgn *= s1;
+  }
+  if (MD && ok && reinvert) {
+    double lc, sc;
+    md_tables(s, v, lane, lc, sc);
+    lnd += lc;
+    sgn *= sc;
+  }
+  double d2lnd = 0, v2 = 0;
+  det_velocities<T, MD, PG>(s, st, w, v, lane, outputs, pg, d2lnd, v2);
+
+  // --- pseudopotential (nonloc_pot.f90, nonloc.f90), quadrature rotated by R
+  double vloc = 0, vnl = 0;
+  int ntask_all = 0;
+  if (s.nloc > 0 && ok)
+    nlpp_energy<T, NORD, MD, PG>(s, J, E, v, R, lane, pg, v.phi, phi_count(s.nbasis, C), vloc, vnl, ntask_all);
+  finish_eval(s, st, w, v, lane, outputs, ok, lnd, sgn, fsum, d2j, pe_ee, pe_en, d2lnd, v2, vloc, vnl, ntask_all, res);
   __syncwarp();
 }
 
@@ -1284,6 +1363,7 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
   }
 }
 
+#include "elstage.cuh"
 #include "pgrad.cuh"
 #include "dmc.cuh"
 #include "orbtc.cuh"

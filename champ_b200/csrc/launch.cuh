@@ -34,6 +34,12 @@ static int set_smem_attrs(champ_ctx *c) {
     CK(cudaFuncSetAttribute(k_basis_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)std::min<size_t>(4 * (size_t)c->nbasis * 5 * sizeof(float), 227 * 1024)));
   }
+  if (!rc && c->el_staged && std::is_same<T, double>::value) {
+    rc = set_attrs(c, k_el_jas<T, NORD>, c->el_smem[0]);
+    if (!rc) rc = set_attrs(c, k_el_orb<T>, c->el_smem[1]);
+    if (!rc) rc = set_attrs(c, k_el_fin<T, NORD, MD>, c->el_smem[2]);
+    if (!rc) rc = set_attrs(c, k_el_inv, sizeof(double) * CHAMP_MAX_SPIN * CHAMP_MAX_SPIN);
+  }
   if (!rc && c->smem_pg > 0) {
     for (auto kern : {k_pgrad<T, NORD, MD, 1>, k_pgrad<T, NORD, MD, 2>, k_pgrad<T, NORD, MD, 3>, k_pgrad<T, NORD, MD, 4>}) {
       CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_pg));
@@ -117,6 +123,31 @@ static int run_orb_tc(champ_ctx *c, const State<T> &st) {
   }
 }
 
+// The full evaluation of every walker as the four parts of elstage.cuh (FP64 state in HBM).
+template <class T, int NORD, bool MD>
+static int run_el_staged(champ_ctx *c, const State<T> &st, bool outputs, bool stats, const ElRot &rot) {
+  if constexpr (!std::is_same<T, double>::value) {
+    return fail(CHAMP_EINVAL, "internal: the staged evaluation is an FP64 path");
+  } else {
+    Sys<T> &s = sysof<T>(c);
+    const int W = st.W, sm = c->num_sms > 0 ? c->num_sms : 148;
+    const int w0 = c->el_wpb[0], w1 = c->el_wpb[1], w2 = c->el_wpb[2];
+    k_el_jas<T, NORD><<<(W + w0 - 1) / w0, 32 * w0, c->el_smem[0], c->stream>>>(s, st);
+    CK(cudaGetLastError());
+    const long long items = (long long)W * c->N;
+    const long long g1 = std::min<long long>((items + w1 - 1) / w1, (long long)sm * 64);
+    k_el_orb<T><<<(unsigned)std::max<long long>(g1, 1), 32 * w1, c->el_smem[1], c->stream>>>(s, st);
+    CK(cudaGetLastError());
+    const int nmax = std::max(c->nup, c->ndn);
+    k_el_inv<<<2 * W, 128, sizeof(double) * nmax * nmax, c->stream>>>(st.ainv, st.astride, c->nup, c->ndn, W, st.el_sc);
+    CK(cudaGetLastError());
+    k_el_fin<T, NORD, MD><<<(W + w2 - 1) / w2, 32 * w2, c->el_smem[2], c->stream>>>(s, st, c->el_nscr, outputs ? 1 : 0,
+                                                                                stats ? 1 : 0, rot);
+    CK(cudaGetLastError());
+    return CHAMP_OK;
+  }
+}
+
 template <class T, int NORD, bool MD>
 static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
   Sys<T> &s = sysof<T>(c);
@@ -129,6 +160,11 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
   case Op::Eval:
   case Op::EvalOut: {
     const bool tc = c->tc_on && !a.st_override;  // only FP32 contexts turn it on
+    if (c->el_staged && std::is_same<T, double>::value && !a.st_override) {
+      ElRot rot{};
+      for (int i = 0; i < 9; i++) rot.R[i] = R[i];
+      return run_el_staged<T, NORD, MD>(c, st, op == Op::EvalOut, false, rot);
+    }
     if (tc) {
       int rc = run_orb_tc<T>(c, st);
       if (rc) return rc;
@@ -162,6 +198,14 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
     break;
   }
   case Op::Vmc: {
+    if (a.phase == 3 && c->el_staged && std::is_same<T, double>::value && !a.st_override) {
+      // the E_L half of a sweep whose moves ran as phase 1
+      ElRot rot{};
+      rot.random = 1;
+      rot.seed = a.seed;
+      rot.sweep = a.sweep0;
+      return run_el_staged<T, NORD, MD>(c, st, false, true, rot);
+    }
     if (a.phase >= 0) {
       auto kern = a.phase == 1 ? k_vmc<T, NORD, MD, 1> : a.phase == 2 ? k_vmc<T, NORD, MD, 2>
                 : a.phase == 3 ? k_vmc<T, NORD, MD, 3> : k_vmc<T, NORD, MD, 0>;

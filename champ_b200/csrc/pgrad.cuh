@@ -113,7 +113,7 @@ __device__ void point_param_values(const Sys<T> &s, const JasPar<T> &J, const Vi
     }
     if (xsums) {
       T X[make_mixed(NORD).n > 0 ? make_mixed(NORD).n : 1];
-      een_xsums<T, NORD>(C, pr, v.ren + 2 * C * j, X);
+      een_xsums<T, NORD>(C, pr + 1, 2, v.ren + 2 * C * j + 1, 2, X);
       const T *zj = v.zq + ZQ * j;
       constexpr XIdx xi = make_xidx(NORD);
       T uu[NORD + 1];

@@ -370,17 +370,25 @@ int champ_synchronize(champ_ctx *ctx);
    ceil(100 / nelec), i.e. a re-inversion about every 100 single-electron moves.
    "dmc_graph": 1 (default) replays pairs of DMC steps as a captured CUDA graph, 0 launches the
    kernels of every step from the host.
-   "phase_timing": 1 records CUDA events around the VMC sweep kernels (champ_phase_times). */
+   "phase_timing": 1 records CUDA events around the VMC sweep kernels (champ_phase_times).
+   "staged_eval": 1 (default when the walker state of an FP64 or mixed context lives in HBM)
+   runs the FP64 full evaluation as four kernels sized for their own parts (Jastrow and
+   distances; basis and orbitals per electron; Slater-matrix inversion in shared memory;
+   velocities, pseudopotential and E_L), and a VMC sweep of an FP64 context as its moves followed
+   by that evaluation; 0 runs the single-kernel evaluation (and the fused FP64 sweep kernel). */
 int champ_set_option(champ_ctx *ctx, const char *name, int64_t value);
 /* Device time of the VMC sweep kernels launched since option "phase_timing" was set to 1 or
    since the previous call (no counterpart in the reference: instrumentation for benchmarks),
    from CUDA events on the context's stream: ms[0] the fused sweep kernel (moves and E_L in one
-   launch: FP64, and FP32 without the tensor-core orbitals), ms[1] the FP32 move kernel and ms[2]
-   the FP64 full-evaluation kernel of a mixed-precision sweep, ms[3] unused; launches[] (may be
-   NULL) the launch counts.  Synchronises the stream and resets the sums. */
+   launch: FP64 with "staged_eval" 0, and FP32 without the tensor-core orbitals), ms[1] the move
+   kernel and ms[2] the FP64 full evaluation of a sweep made of the two (mixed precision, and FP64
+   with "staged_eval" 1), ms[3] unused; launches[] (may be NULL) the counts of timed sections.
+   Synchronises the stream and resets the sums. */
 int champ_phase_times(champ_ctx *ctx, double *ms /* [4] */, int32_t *launches /* [4] or NULL */);
-/* Current value of an option ("orbital_tc", "orbital_tc_chunk", "reinvert_every", "dmc_graph"); kernel launches per champ_vmc_sweeps sweep
-   ("launches_per_sweep": 1 for the fused sweep kernel, 5 with the tensor-core orbitals). */
+/* Current value of an option ("orbital_tc", "orbital_tc_chunk", "reinvert_every", "dmc_graph",
+   "phase_timing", "param_grad_mode", "staged_eval"); kernel launches per champ_vmc_sweeps sweep
+   ("launches_per_sweep": 1 for the fused sweep kernel, 2 for moves + single-kernel evaluation,
+   5 for moves + staged evaluation or with the tensor-core orbitals). */
 int champ_get_option(const champ_ctx *ctx, const char *name, int64_t *value);
 
 #ifdef __cplusplus
