@@ -225,7 +225,8 @@ __global__ void __launch_bounds__(128, 4) k_el_fin(Sys<T> s, State<T> st, int ns
       if (rot.random) random_rotation(rot.seed, (uint32_t)w, rot.sweep, R);
       else
         for (int i = 0; i < 9; i++) R[i] = rot.R[i];
-      nlpp_energy<T, NORD, MD, false>(s, J, E, v, R, lane, nullptr, scr, nscr, vloc, vnl, ntask);
+      nlpp_energy<T, NORD, MD, false>(s, J, E, v, R, lane, nullptr, scr, nscr, st.el_rt + (size_t)w * 2 * C * N, vloc,
+                                      vnl, ntask);
     }
     EvalRes res;
     finish_eval(s, st, w, v, lane, outputs != 0, ok, lnd, sgn, fsum, d2j, pe_ee, pe_en, d2lnd, v2, vloc, vnl, ntask,

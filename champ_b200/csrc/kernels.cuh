@@ -703,14 +703,96 @@ __device__ void det_velocities(const Sys<T> &s, const State<T> &st, int w, const
   v2_o = v2;
 }
 
+// FP64 tensor-core product D += A B of one 8x8 tile with k = 4 (mma m8n8k4, one element of A and
+// of B and two of D per lane: A[lane/4][lane%4], B[lane%4][lane/4], D[lane/4][2(lane%4) + 0, 1]).
+__device__ __forceinline__ void dmma_884(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// Jastrow ratio terms of 32 quadrature points (one per lane; act false for a lane without one):
+// the sum over the other electrons j of the pair term at the point (e-e, and e-e-n from the X
+// sums) minus the pair table entry u(e, j) (nonlocj, nonloc.f90:432-522).  The X sums
+// X_pq(point, j) = sum_c d_c^p(point) d_c^q(j) of the round are FP64 tensor-core products over
+// the centres: 4 row tiles of 8 points, column tiles of 8 electrons, k-steps of 4 centres.
+// pd: the points' scaled distances to the centres, [c][32]; bd: the electrons' scaled
+// distances, element (c, j) at bd[c sbc + j sbj]; asum: this lane's point's power sums.
+template <int NORD>
+__device__ double nl_pairs_mma(const Sys<double> &s, const JasPar<double> &J, const View<double> &v,
+                               const double *pd, const double *bd, int sbc, int sbj, const double *asum,
+                               const double *xn, int e, bool act, int lane) {
+  constexpr MixedPQ mx = make_mixed(NORD);
+  constexpr int NM = mx.n > 0 ? mx.n : 1;
+  const int N = s.N, C = s.C;
+  const double sk = J.scalek;
+  const unsigned full = 0xffffffffu, am = __ballot_sync(full, act);
+  double mine = 0;
+  for (int mt = 0; mt < 4; mt++) {
+    if (((am >> (8 * mt)) & 0xffu) == 0u) continue;  // no point in this row tile (uniform)
+    const int prow = mt * 8 + (lane >> 2);  // the point (lane) of this lane's fragment row
+    const double px = __shfl_sync(full, xn[0], prow), py = __shfl_sync(full, xn[1], prow),
+                 pz = __shfl_sync(full, xn[2], prow);
+    const int pe = __shfl_sync(full, e, prow);
+    const bool pact = (am >> prow) & 1u;
+    double pas[NORD + 1];
+#pragma unroll
+    for (int q = 0; q <= NORD; q++) pas[q] = __shfl_sync(full, asum[q], prow);
+    double dsum = 0;
+    for (int j0 = 0; j0 < N; j0 += 8) {
+      double acc[NM][2];
+#pragma unroll
+      for (int i = 0; i < NM; i++) acc[i][0] = acc[i][1] = 0.0;
+      const int jb = j0 + (lane >> 2);
+      for (int k0 = 0; k0 < C; k0 += 4) {
+        const int ck = k0 + (lane & 3);
+        const double a1 = ck < C ? pd[ck * 32 + prow] : 0.0;
+        const double b1 = (ck < C && jb < N) ? bd[(size_t)ck * sbc + (size_t)jb * sbj] : 0.0;
+        double ap[NORD + 1], bp[NORD + 1];
+        ap[0] = bp[0] = 1.0;
+#pragma unroll
+        for (int q = 1; q <= NORD; q++) { ap[q] = ap[q - 1] * a1; bp[q] = bp[q - 1] * b1; }
+#pragma unroll
+        for (int i = 0; i < mx.n; i++) dmma_884(acc[i][0], acc[i][1], ap[mx.p[i]], bp[mx.q[i]]);
+      }
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int j = j0 + 2 * (lane & 3) + h;
+        if (!pact || j >= N || j == pe) continue;
+        int isb, ipar;
+        double ss;
+        pair_class(J, s.nup, pe, j, isb, ss, ipar);
+        const double *xj = v.xs + 3 * j;
+        const double a0 = px - xj[0], a1 = py - xj[1], a2 = pz - xj[2];
+        const double rij = sqrt(a0 * a0 + a1 * a1 + a2 * a2);
+        const double du = 1.0 / (1.0 + sk * rij);
+        double fu, fuu;
+        double f = jas_ee<double, false>(J, isb, ss, ipar, rij, du, fu, fuu);
+        double X[NM];
+#pragma unroll
+        for (int i = 0; i < NM; i++) X[i] = acc[i][h];
+        f += een_from_x<double, NORD>(J.c[0], du, pas, v.zq + ZQ * j, X);
+        dsum += f - v.fso[pe * N + j];
+      }
+    }
+    dsum += __shfl_xor_sync(full, dsum, 1);
+    dsum += __shfl_xor_sync(full, dsum, 2);
+    const double got = __shfl_sync(full, dsum, 4 * (lane & 7));
+    if ((lane >> 3) == mt) mine = got;
+  }
+  return mine;
+}
+
 // Nonlocal pseudopotential energy of one walker (nonloc_pot.f90, nonloc.f90), quadrature rotated
 // by R.  scr: nscr elements of per-warp shared scratch, holding the radial parts of the tasks'
 // centres' shells and, on the one-centre-type path, each lane's scaled point-centre distances
-// (stored [centre][lane], 32 C elements at the end).  Returns the local and nonlocal parts and
-// the number of (electron, centre) tasks.
+// (stored [centre][lane], 32 C elements at the end).  st_rt: the walker's e-n distance planes
+// (State::el_rt) or null.  Returns the local and nonlocal parts and the number of (electron,
+// centre) tasks.
 template <class T, int NORD, bool MD, bool PG>
 __device__ void nlpp_energy(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, const View<T> &v, const double *R,
-                            int lane, const PGBuf *pg, T *scr, int nscr, double &vloc_o, double &vnl_o, int &ntask_o) {
+                            int lane, const PGBuf *pg, T *scr, int nscr, const T *st_rt, double &vloc_o, double &vnl_o,
+                            int &ntask_o) {
   const int N = s.N, C = s.C, B = s.nbasis;
   const double *xs = v.xs;
   const T *fso = v.fso;
@@ -812,7 +894,12 @@ __device__ void nlpp_energy(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E
     }
     __syncwarp();
   }
-  for (int t = lane; t < ntask * nq; t += 32) {
+  // rounds of 32 points, one per lane (lanes past the last point repeat the round's first point
+  // in the parts that all lanes run together and skip the rest)
+  const int npts = ntask * nq;
+  for (int t0 = 0; t0 < npts; t0 += 32) {
+    const bool act = t0 + lane < npts;
+    const int t = act ? t0 + lane : t0;
     int task = t / nq, q = t - task * nq;
     const double *rec = tl + (size_t)task * NLT;
     int idx = (int)rec[0], e = idx / C, c = idx - (idx / C) * C;
@@ -831,7 +918,7 @@ __device__ void nlpp_energy(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E
     // with the nonlocal B-matrix sums wanted, the basis values at the point are formed once,
     // after the Jastrow ratio, for both the ratio and those sums
     const bool merged = PG && pg->phis != nullptr;
-    if (!merged)
+    if (!merged && act)
       for (int ish = 0; ish < s.nshell; ish++)
         dr += shell_dot_r<T>(s, ish, xn, ge, (ish >= c0 && ish < c1) ? ro + ish : nullptr);
     // Jastrow ratio (nonlocj, nonloc.f90:432-522): point-centre distances once per point
@@ -861,7 +948,14 @@ __device__ void nlpp_energy(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E
     if (SHARE)
 #pragma unroll
       for (int ll = 0; ll < NT; ll++) tsum[ll] = T(0);
-    for (int j = 0; j < N; j++) {
+    constexpr bool MMA = std::is_same<T, double>::value && !SHARE;
+    if (MMA && fast) {
+      if constexpr (MMA) {
+        const double *bd = st_rt ? st_rt + (size_t)C * N : v.ren + 1;
+        dj += nl_pairs_mma<NORD>(s, J, v, prs - lane, bd, st_rt ? N : 2, st_rt ? 1 : 2 * C, asum, xn, e, act, lane);
+      }
+    }
+    for (int j = 0; j < N && act && !(MMA && fast); j++) {
       if (j == e) continue;
       int isb, ipar;
       T ss;
@@ -904,6 +998,7 @@ __device__ void nlpp_energy(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E
       }
       dj += (double)f - (double)fso[e * N + j];
     }
+    if (!act) continue;
     int it = s.ctype[c];
     double vp = 0;
     for (int l = 0; l < E.npotd[it]; l++)
@@ -1045,7 +1140,7 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
   double vloc = 0, vnl = 0;
   int ntask_all = 0;
   if (s.nloc > 0 && ok)
-    nlpp_energy<T, NORD, MD, PG>(s, J, E, v, R, lane, pg, v.phi, phi_count(s.nbasis, C), vloc, vnl, ntask_all);
+    nlpp_energy<T, NORD, MD, PG>(s, J, E, v, R, lane, pg, v.phi, phi_count(s.nbasis, C), nullptr, vloc, vnl, ntask_all);
   finish_eval(s, st, w, v, lane, outputs, ok, lnd, sgn, fsum, d2j, pe_ee, pe_en, d2lnd, v2, vloc, vnl, ntask_all, res);
   __syncwarp();
 }
