@@ -19,9 +19,13 @@ template <class T>
 __host__ __device__ inline size_t el_orb_bytes(int nbasis) { return align16(sizeof(T) * nbasis * 5); }
 template <class T>
 __host__ __device__ inline size_t el_fin_bytes(int N, int nscr) { return align16(sizeof(double) * 3 * N) + align16(sizeof(T) * nscr); }
-// Scratch of the pseudopotential part: the points' distances to the centres (one-centre-type
-// path) and the radial table of the tasks' centres.
-__host__ __device__ inline int el_fin_scratch(int N, int C) { return 32 * C + (4 * N > 512 ? 4 * N : 512); }
+// Scratch of the pseudopotential part (FP64): the radial table of the tasks' centres, as large as
+// keeps a warp's shared memory within 13 KB (16 warps per SM) but at least 256 elements, and
+// beyond 32 centres each lane's distances to the centres.
+__host__ __device__ inline int el_fin_scratch(int N, int C) {
+  const int room = (int)((13 * 1024 - align16(sizeof(double) * 3 * N)) / sizeof(double));
+  return (room > 256 ? room : 256) + (C > 32 ? 32 * C : 0);
+}
 
 template <class T, int NORD>
 __global__ void __launch_bounds__(128, 4) k_el_jas(Sys<T> s, State<T> st) {

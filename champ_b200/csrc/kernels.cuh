@@ -715,22 +715,24 @@ __device__ __forceinline__ void dmma_884(double &d0, double &d1, double a, doubl
 // the sum over the other electrons j of the pair term at the point (e-e, and e-e-n from the X
 // sums) minus the pair table entry u(e, j) (nonlocj, nonloc.f90:432-522).  The X sums
 // X_pq(point, j) = sum_c d_c^p(point) d_c^q(j) of the round are FP64 tensor-core products over
-// the centres: 4 row tiles of 8 points, column tiles of 8 electrons, k-steps of 4 centres.
-// pd: the points' scaled distances to the centres, [c][32]; bd: the electrons' scaled
-// distances, element (c, j) at bd[c sbc + j sbj]; asum: this lane's point's power sums.
-template <int NORD>
+// the centres (KS k-steps of 4 centres, 4 KS >= C): row tiles of 8 points, whose A fragments (the points'
+// scaled distances to the centres) each lane forms in registers; column tiles of 8 electrons,
+// B fragments from bd (element (c, j) at bd[c sbc + j sbj]).
+template <int NORD, int KS>
 __device__ double nl_pairs_mma(const Sys<double> &s, const JasPar<double> &J, const View<double> &v,
-                               const double *pd, const double *bd, int sbc, int sbj, const double *asum,
-                               const double *xn, int e, bool act, int lane) {
+                               const double *bd, int sbc, int sbj, const double *asum, const double *xn, int e,
+                               bool act, int lane) {
   constexpr MixedPQ mx = make_mixed(NORD);
   constexpr int NM = mx.n > 0 ? mx.n : 1;
   const int N = s.N, C = s.C;
   const double sk = J.scalek;
   const unsigned full = 0xffffffffu, am = __ballot_sync(full, act);
+  const int kq = lane & 3, rr = lane >> 2;
   double mine = 0;
+#pragma unroll 1
   for (int mt = 0; mt < 4; mt++) {
     if (((am >> (8 * mt)) & 0xffu) == 0u) continue;  // no point in this row tile (uniform)
-    const int prow = mt * 8 + (lane >> 2);  // the point (lane) of this lane's fragment row
+    const int prow = mt * 8 + rr;  // the point (lane) of this lane's fragment row
     const double px = __shfl_sync(full, xn[0], prow), py = __shfl_sync(full, xn[1], prow),
                  pz = __shfl_sync(full, xn[2], prow);
     const int pe = __shfl_sync(full, e, prow);
@@ -738,33 +740,51 @@ __device__ double nl_pairs_mma(const Sys<double> &s, const JasPar<double> &J, co
     double pas[NORD + 1];
 #pragma unroll
     for (int q = 0; q <= NORD; q++) pas[q] = __shfl_sync(full, asum[q], prow);
+    double a1[KS];
+#pragma unroll
+    for (int ks = 0; ks < KS; ks++) {
+      const int ck = 4 * ks + kq;
+      a1[ks] = 0.0;
+      if (ck < C) {
+        const double *cc = s.cent + 3 * ck;
+        const double dx = px - cc[0], dy = py - cc[1], dz = pz - cc[2];
+        a1[ks] = 1.0 / (1.0 + sk * sqrt(dx * dx + dy * dy + dz * dz));
+      }
+    }
     double dsum = 0;
     for (int j0 = 0; j0 < N; j0 += 8) {
+      const int jb = j0 + rr, ja = j0 + 2 * kq;
+      double b1[KS];
+#pragma unroll
+      for (int ks = 0; ks < KS; ks++) {
+        const int ck = 4 * ks + kq;
+        b1[ks] = (ck < C && jb < N) ? bd[(size_t)ck * sbc + (size_t)jb * sbj] : 0.0;
+      }
+      double fo[2];
+#pragma unroll
+      for (int h = 0; h < 2; h++) fo[h] = (pact && ja + h < N) ? v.fso[pe * N + ja + h] : 0.0;
       double acc[NM][2];
 #pragma unroll
       for (int i = 0; i < NM; i++) acc[i][0] = acc[i][1] = 0.0;
-      const int jb = j0 + (lane >> 2);
-      for (int k0 = 0; k0 < C; k0 += 4) {
-        const int ck = k0 + (lane & 3);
-        const double a1 = ck < C ? pd[ck * 32 + prow] : 0.0;
-        const double b1 = (ck < C && jb < N) ? bd[(size_t)ck * sbc + (size_t)jb * sbj] : 0.0;
+#pragma unroll
+      for (int ks = 0; ks < KS; ks++) {
         double ap[NORD + 1], bp[NORD + 1];
         ap[0] = bp[0] = 1.0;
 #pragma unroll
-        for (int q = 1; q <= NORD; q++) { ap[q] = ap[q - 1] * a1; bp[q] = bp[q - 1] * b1; }
+        for (int q = 1; q <= NORD; q++) { ap[q] = ap[q - 1] * a1[ks]; bp[q] = bp[q - 1] * b1[ks]; }
 #pragma unroll
         for (int i = 0; i < mx.n; i++) dmma_884(acc[i][0], acc[i][1], ap[mx.p[i]], bp[mx.q[i]]);
       }
 #pragma unroll
       for (int h = 0; h < 2; h++) {
-        const int j = j0 + 2 * (lane & 3) + h;
+        const int j = ja + h;
         if (!pact || j >= N || j == pe) continue;
         int isb, ipar;
         double ss;
         pair_class(J, s.nup, pe, j, isb, ss, ipar);
         const double *xj = v.xs + 3 * j;
-        const double a0 = px - xj[0], a1 = py - xj[1], a2 = pz - xj[2];
-        const double rij = sqrt(a0 * a0 + a1 * a1 + a2 * a2);
+        const double d0 = px - xj[0], d1 = py - xj[1], d2 = pz - xj[2];
+        const double rij = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
         const double du = 1.0 / (1.0 + sk * rij);
         double fu, fuu;
         double f = jas_ee<double, false>(J, isb, ss, ipar, rij, du, fu, fuu);
@@ -772,7 +792,7 @@ __device__ double nl_pairs_mma(const Sys<double> &s, const JasPar<double> &J, co
 #pragma unroll
         for (int i = 0; i < NM; i++) X[i] = acc[i][h];
         f += een_from_x<double, NORD>(J.c[0], du, pas, v.zq + ZQ * j, X);
-        dsum += f - v.fso[pe * N + j];
+        dsum += f - fo[h];
       }
     }
     dsum += __shfl_xor_sync(full, dsum, 1);
@@ -785,8 +805,8 @@ __device__ double nl_pairs_mma(const Sys<double> &s, const JasPar<double> &J, co
 
 // Nonlocal pseudopotential energy of one walker (nonloc_pot.f90, nonloc.f90), quadrature rotated
 // by R.  scr: nscr elements of per-warp shared scratch, holding the radial parts of the tasks'
-// centres' shells and, on the one-centre-type path, each lane's scaled point-centre distances
-// (stored [centre][lane], 32 C elements at the end).  st_rt: the walker's e-n distance planes
+// centres' shells and, on the one-centre-type path in FP32, each lane's scaled point-centre
+// distances (stored [centre][lane], 32 C elements at the end).  st_rt: the walker's e-n distance planes
 // (State::el_rt) or null.  Returns the local and nonlocal parts and the number of (electron,
 // centre) tasks.
 template <class T, int NORD, bool MD, bool PG>
@@ -797,9 +817,12 @@ __device__ void nlpp_energy(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E
   const double *xs = v.xs;
   const T *fso = v.fso;
   const T sk = J.scalek;
-  const bool fast = (NORD > 1) && J.nct == 1 && C <= MAXC_NL;
-  const int nrown = nscr - (fast ? 32 * C : 0);
-  T *const prs = fast ? scr + nrown + lane : nullptr;  // this lane's point-centre distances, stride 32
+  // FP64 with up to 32 centres: the X sums on the tensor cores, without the per-lane distances in
+  // shared memory; else in each lane from those distances (scratch permitting)
+  const bool mma = std::is_same<T, double>::value && NORD > 1 && J.nct == 1 && C <= 32;
+  const bool fast = mma || ((NORD > 1) && J.nct == 1 && C <= MAXC_NL && nscr >= 32 * C);
+  const int nrown = nscr - (fast && !mma ? 32 * C : 0);
+  T *const prs = fast && !mma ? scr + nrown + lane : nullptr;  // this lane's point-centre distances, stride 32
   double vloc = 0, vnl = 0;
   T *gp = v.gproj;
   // G projected onto the basis: g_e[b] = sum_k coef[b][k] G[k][e] (psp_nonloc_pot_bld), one
@@ -932,7 +955,7 @@ __device__ void nlpp_energy(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E
         cen_dist(s, sk, xn, c2, ri, di);
         f += jas_en<T, false>(J, s.ctype[c2], ri, di, fi, fii);
         if (fast) {
-          prs[32 * c2] = di;
+          if (!mma) prs[32 * c2] = di;
           T p = di;
           for (int q2 = 1; q2 < ZQ; q2++) { asum[q2] += p; p *= di; }
         }
@@ -949,13 +972,14 @@ __device__ void nlpp_energy(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E
 #pragma unroll
       for (int ll = 0; ll < NT; ll++) tsum[ll] = T(0);
     constexpr bool MMA = std::is_same<T, double>::value && !SHARE;
-    if (MMA && fast) {
+    if (MMA && mma) {
       if constexpr (MMA) {
         const double *bd = st_rt ? st_rt + (size_t)C * N : v.ren + 1;
-        dj += nl_pairs_mma<NORD>(s, J, v, prs - lane, bd, st_rt ? N : 2, st_rt ? 1 : 2 * C, asum, xn, e, act, lane);
+        const int sbc = st_rt ? N : 2, sbj = st_rt ? 1 : 2 * C;
+        dj += nl_pairs_mma<NORD, 8>(s, J, v, bd, sbc, sbj, asum, xn, e, act, lane);
       }
     }
-    for (int j = 0; j < N && act && !(MMA && fast); j++) {
+    for (int j = 0; j < N && act && !(MMA && mma); j++) {
       if (j == e) continue;
       int isb, ipar;
       T ss;
