@@ -162,6 +162,8 @@ __global__ void k_dmc_copy(State<T> a, State<T> b, DmcData Da, DmcData Db, int N
       for (int i = lane; i < N * N; i += 32) b.fso[(size_t)d * N * N + i] = a.fso[(size_t)w * N * N + i];
       for (int i = lane; i < N * C * 2; i += 32) b.ren[(size_t)d * N * C * 2 + i] = a.ren[(size_t)w * N * C * 2 + i];
       for (int i = lane; i < N * ZQ; i += 32) b.zq[(size_t)d * N * ZQ + i] = a.zq[(size_t)w * N * ZQ + i];
+      if (a.rtd)
+        for (int i = lane; i < N * C; i += 32) b.rtd[(size_t)d * N * C + i] = a.rtd[(size_t)w * N * C + i];
       for (int i = lane; i < a.tvstride; i += 32) b.tv[(size_t)d * a.tvstride + i] = a.tv[(size_t)w * a.tvstride + i];
       for (int i = lane; i < a.gstride; i += 32) b.gam[(size_t)d * a.gstride + i] = a.gam[(size_t)w * a.gstride + i];
       if (lane == 0) {

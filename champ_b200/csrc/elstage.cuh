@@ -240,6 +240,6 @@ __global__ void __launch_bounds__(128, 4) k_el_fin(Sys<T> s, State<T> st, int ns
       st.s_e2sum[w] += res.eloc * res.eloc;
       st.s_elast[w] = res.eloc;
     }
-    mirror_store(v, st, w, N, C, lane);
+    mirror_store(v, st, w, N, C, lane, st.el_rt ? st.el_rt + (size_t)w * 2 * C * N : nullptr);
   }
 }

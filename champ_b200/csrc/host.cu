@@ -751,7 +751,7 @@ static int setup_el_staged(champ_ctx *c) {
 // only the FP32 Jastrow pair table, distances and power sums, which every FP64 full evaluation
 // refreshes (State::m_fso, m_ren, m_zq).
 static void link_move_state(State<double> &d, State<float> &f) {
-  float *fso = f.fso, *ren = f.ren, *zq = f.zq, *pf = f.pf;
+  float *fso = f.fso, *ren = f.ren, *zq = f.zq, *pf = f.pf, *rtd = f.rtd;
   f.W = d.W;
   f.x = d.x; f.ainv = d.ainv; f.fsum = d.fsum; f.lnd = d.lnd; f.sgn = d.sgn; f.status = d.status;
   f.pa = d.pa; f.pdj = d.pdj; f.prho = d.prho; f.pxn = d.pxn; f.piel = d.piel;
@@ -761,9 +761,12 @@ static void link_move_state(State<double> &d, State<float> &f) {
   f.o_lnpsi = d.o_lnpsi; f.o_sign = d.o_sign; f.o_psij = d.o_psij; f.o_vel = d.o_vel; f.o_divv = d.o_divv;
   f.o_d2 = d.o_d2; f.o_pe = d.o_pe; f.o_peee = d.o_peee; f.o_penl = d.o_penl; f.o_eloc = d.o_eloc;
   f.s_esum = d.s_esum; f.s_e2sum = d.s_e2sum; f.s_acc = d.s_acc; f.s_elast = d.s_elast;
-  f.fso = fso; f.ren = ren; f.zq = zq; f.pf = pf;
+  f.fso = fso; f.ren = ren; f.zq = zq; f.pf = pf; f.rtd = rtd;
   f.m_fso = f.m_ren = f.m_zq = nullptr;
   d.m_fso = fso; d.m_ren = ren; d.m_zq = zq;
+  f.m_rtd = nullptr;
+  d.m_rtd = f.rtd;
+  d.rtd = nullptr;
 }
 
 static int build_move_state(champ_ctx *c, State<double> &d, State<float> &f) {
@@ -774,6 +777,11 @@ static int build_move_state(champ_ctx *c, State<double> &d, State<float> &f) {
   f.zq = dalloc<float>(c, W * N * ZQ);
   f.pf = dalloc<float>(c, W * N);
   if (!f.fso || !f.ren || !f.zq || !f.pf) return fail(CHAMP_ENOMEM, "device allocation of the FP32 move tables failed");
+  f.rtd = nullptr;
+  if (!c->kd.lay.resident) {  // walker state in HBM: the transposed distances of the pair loads
+    f.rtd = dalloc<float>(c, W * N * c->C);
+    if (!f.rtd) return fail(CHAMP_ENOMEM, "device allocation of the FP32 move tables failed");
+  }
   link_move_state(d, f);
   return CHAMP_OK;
 }
@@ -921,6 +929,10 @@ static int alloc_state_copy(champ_ctx *c, const State<T> &a, State<T> &b) {
   b.sgn = dalloc<double>(c, W);
   if (!b.x || !b.ainv || !b.fso || !b.ren || !b.zq || !b.tv || !b.gam || !b.fsum || !b.lnd || !b.sgn)
     return fail(CHAMP_ENOMEM, "allocation of the DMC state buffer failed");
+  if (a.rtd) {
+    b.rtd = dalloc<T>(c, W * N * c->C);
+    if (!b.rtd) return fail(CHAMP_ENOMEM, "allocation of the DMC state buffer failed");
+  }
   return CHAMP_OK;
 }
 
@@ -1003,6 +1015,10 @@ static size_t noalloc_carve(const champ_ctx *c, const State<T> &ref, int nw, cha
   st.o_penl = (double *)take(sizeof(double) * W);
   st.o_eloc = eloc;  // written straight into the caller's buffer
   st.m_fso = st.m_ren = st.m_zq = nullptr;  // the context's own move tables stay untouched
+  st.m_rtd = nullptr;
+  st.rtd = nullptr;
+  st.el_vj = st.el_sc = nullptr;
+  st.el_rt = nullptr;
   return o <= NOALLOC_BYTES ? o : 0;
 }
 
@@ -1776,7 +1792,7 @@ int champ_dmc_init(champ_ctx *c, int32_t w_target, double tau, double gpop) {
         const State<float> &f2 = c->stf2;
         d2.x = f2.x; d2.ainv = f2.ainv; d2.tv = f2.tv; d2.gam = f2.gam;
         d2.fsum = f2.fsum; d2.lnd = f2.lnd; d2.sgn = f2.sgn;
-        d2.m_fso = f2.fso; d2.m_ren = f2.ren; d2.m_zq = f2.zq;
+        d2.m_fso = f2.fso; d2.m_ren = f2.ren; d2.m_zq = f2.zq; d2.m_rtd = f2.rtd;
       }
     }
     if (rc) return rc;

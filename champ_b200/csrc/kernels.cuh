@@ -56,6 +56,11 @@ struct State {
   // mixed precision: the FP32 tables of the single-electron moves ([W][N][N], [W][N][C][2],
   // [W][N][ZQ]), refreshed from the FP64 tables by every full evaluation; null otherwise
   float *m_fso, *m_ren, *m_zq;
+  // the moves' scaled e-n distances transposed, [W][C][N] (the pair loads of a proposal read
+  // consecutive electrons), kept by the accepted moves; null when unused.  m_rtd: its FP32
+  // mirror, refreshed by the full evaluation of a mixed-precision state
+  T *rtd;
+  float *m_rtd;
   // intermediates of the staged evaluation (elstage.cuh) of a state in HBM; null otherwise:
   // per walker grad ln J and div of the Jastrow velocity [4N], scalars [8] (J, its Laplacian
   // sum, e-e and e-n Coulomb energies, ln|D| and sign(D) of each spin), and the e-n distances
@@ -88,6 +93,7 @@ struct View {
   double *ainv;
   T *fso, *ren, *zq, *pf, *orb5, *gproj;
   double *nlt, *tv, *gam, *ymd, *wdet;
+  T *rtd;          // [C][N] transposed scaled e-n distances (State::rtd) or null
 };
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
@@ -172,6 +178,7 @@ __device__ inline View<T> make_view(char *base, const Layout &L, const State<T> 
     v.ymd = st.ymd + (size_t)w * st.tvstride;
     v.wdet = st.wdet + (size_t)w * st.wstride;
   }
+  v.rtd = (st.rtd && !resident) ? st.rtd + (size_t)w * C * N : nullptr;
   return v;
 }
 
@@ -190,12 +197,24 @@ __device__ inline void view_load(const View<T> &v, const State<T> &st, int w, in
 // Mixed precision: after an FP64 full evaluation, the FP32 copies of the Jastrow pair table,
 // the e-n distances and the power sums that the single-electron moves read.
 template <class T>
-__device__ inline void mirror_store(const View<T> &v, const State<T> &st, int w, int N, int C, int lane) {
+__device__ inline void mirror_store(const View<T> &v, const State<T> &st, int w, int N, int C, int lane,
+                                    const T *rt = nullptr) {
   if (!st.m_fso) return;
   __syncwarp();
   for (int i = lane; i < N * N; i += 32) st.m_fso[(size_t)w * N * N + i] = (float)v.fso[i];
   for (int i = lane; i < N * C * 2; i += 32) st.m_ren[(size_t)w * N * C * 2 + i] = (float)v.ren[i];
   for (int i = lane; i < N * ZQ; i += 32) st.m_zq[(size_t)w * N * ZQ + i] = (float)v.zq[i];
+  if (st.m_rtd) {
+    // from the transposed planes when the evaluation has them ([2][C][N], scaled plane second)
+    float *m = st.m_rtd + (size_t)w * C * N;
+    if (rt)
+      for (int i = lane; i < N * C; i += 32) m[i] = (float)rt[(size_t)C * N + i];
+    else
+      for (int i = lane; i < N * C; i += 32) {
+        const int c = i / N, e = i - c * N;
+        m[i] = (float)v.ren[2 * (e * C + c) + 1];
+      }
+  }
   __syncwarp();
 }
 // The persistent state a full evaluation produces, from a resident view back to HBM: the FP64
@@ -332,7 +351,7 @@ __device__ __forceinline__ void cen_dist(const Sys<T> &s, T sk, const double *p,
 template <class T, int NORD, bool GRAD>
 __device__ __forceinline__ T pair_value(const Sys<T> &s, const JasPar<T> &J, int e, int j, const double *xe,
                                         const T *re, const double *xj, const T *rj, T *g, const T *ae = nullptr,
-                                        const T *zj = nullptr) {
+                                        const T *zj = nullptr, const T *dj = nullptr, int sdj = 0) {
   int isb, ipar;
   T ss;
   pair_class(J, s.nup, e, j, isb, ss, ipar);
@@ -345,7 +364,8 @@ __device__ __forceinline__ T pair_value(const Sys<T> &s, const JasPar<T> &J, int
   if (NORD > 1 && !GRAD && J.nct == 1 && s.C <= MAXC_NL) {
     // value only, one centre type: X sums (see een_xsums)
     T X[make_mixed(NORD).n > 0 ? make_mixed(NORD).n : 1];
-    een_xsums<T, NORD>(s.C, re + 1, 2, rj + 1, 2, X);
+    if (dj) een_xsums<T, NORD>(s.C, re + 1, 2, dj, sdj, X);
+    else een_xsums<T, NORD>(s.C, re + 1, 2, rj + 1, 2, X);
     f += een_from_x<T, NORD>(J.c[0], du, ae, zj, X);
   } else if (NORD > 1) {
     for (int c = 0; c < s.C; c++) {
@@ -1214,7 +1234,7 @@ __device__ void propose(const Sys<T> &s, const JasPar<T> &J, const State<T> &st,
     if (j == e) continue;
     T g[3];
     T f = pair_value<T, NORD, GRAD>(s, J, e, j, xn, v.rnew, v.xs + 3 * j, v.ren + 2 * C * j, g, v.asum,
-                                    v.zq + ZQ * j);
+                                    v.zq + ZQ * j, v.rtd ? v.rtd + j : nullptr, N);
     d += (double)f - (double)fso[e * N + j];
     pf[j] = f;
     if (GRAD) { gj0 += g[0]; gj1 += g[1]; gj2 += g[2]; }
@@ -1296,6 +1316,8 @@ __device__ void accept_move(const Sys<T> &s, const State<T> &st, int w, const Vi
     fso[j * N + e] = f;
   }
   for (int i = lane; i < 2 * C; i += 32) v.ren[2 * C * e + i] = v.rnew[i];
+  if (v.rtd)
+    for (int c = lane; c < C; c += 32) v.rtd[c * N + e] = v.rnew[2 * c + 1];
   for (int q = lane; q < ZQ; q += 32) v.zq[ZQ * e + q] = v.asum[q];
   if (lane < 3) v.xs[3 * e + lane] = xn[lane];
   if (lane == 0) {
