@@ -39,23 +39,23 @@ SEED = 20261203
 NSM = 148                       # B200 streaming multiprocessors
 FMA_PER_SM_CLK = {"fp64": 64, "fp32": 128}  # FP64 / FP32 fused multiply-adds per SM per clock
 
-# Executed floating-point operations per walker of one launch (2 per FMA, 1 per add/mul), counted
-# by ncu (smsp__sass_thread_inst_executed_op_{d,f}{fma,add,mul}_pred_on.sum) on a 256-walker
-# launch of the same kernel and divided by the walkers (profiles/flops_cluster128.md).  None
-# until counted: the roofline's achieved figure is then left out.
+# Executed floating-point operations per walker of one sweep phase (2 per FMA, 1 per add/mul, 512
+# per DMMA m8n8k4 warp instruction), counted by ncu (smsp__sass_thread_inst_executed_op_{d,f}{fma,
+# add,mul}_pred_on.sum, sm__inst_executed_pipe_tensor_subpipe_dmma.sum) on a 256-walker sweep of
+# the same kernels and divided by the walkers (profiles/flops_cluster128.md).  "eval" is the FP64
+# full evaluation (k_el_jas, k_el_orb, k_el_inv, k_el_fin); None until counted: the roofline's
+# achieved figure is then left out.
 FLOPS_PER_WALKER = {
-    ("cluster128", "eval", "fp64"): 259.2128e6,   # FP64: 2 x 25.636e9 FMA + 3.871e9 add + 11.216e9 mul / 256
-    ("cluster128", "moves", "fp32"): 18.5268e6,   # FP32: 2 x 1.927e9 FMA + 0.0898e9 add + 0.798e9 mul / 256
-                                                  # (plus 2.855e6 FP64 per walker: the Sherman-Morrison updates)
+    ("cluster128", "eval", "fp64"): 250.86e6,     # CUDA cores 216.31 M + DMMA 34.55 M
+    ("cluster128", "moves", "fp32"): 18.54e6,     # FP32 (plus 2.85 M FP64: the Sherman-Morrison updates)
     ("cluster128", "sweep", "fp64"): None,
 }
 # DRAM bytes per walker of the same launches (dram__bytes_read.sum + dram__bytes_write.sum).
 DRAM_PER_WALKER = {
-    ("cluster128", "eval", "fp64"): 1672818.0,    # 141.1 MB read + 287.1 MB written / 256
-    ("cluster128", "moves", "fp32"): 182891.0,    # 43.9 MB read + 2.9 MB written / 256
+    ("cluster128", "eval", "fp64"): 1555342.0,    # 218.0 MB read + 180.3 MB written / 256
+    ("cluster128", "moves", "fp32"): 162209.0,    # 39.8 MB read + 1.8 MB written / 256
     ("cluster128", "sweep", "fp64"): None,
 }
-
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -323,14 +323,17 @@ def roofline_for(system, nw, arm, clocks, prec):
     if not ks:
         return None
     kern = max(ks, key=ks.get)
-    kprec = {"moves": "fp32", "eval": "fp64", "sweep": "fp64" if prec == "fp64" else "fp32"}[kern]
+    kprec = {"moves": "fp64" if prec == "fp64" else "fp32", "eval": "fp64",
+             "sweep": "fp64" if prec == "fp64" else "fp32"}[kern]
     key = (system.name, kern, kprec)
     mhz = (clocks or {}).get("sm_mhz") or measured_peaks()[0].get("sm_max_mhz", 1965.0)
     peak = 2 * NSM * FMA_PER_SM_CLK[kprec] * mhz * 1e6 / 1e12
     fpw, dpw = FLOPS_PER_WALKER.get(key), DRAM_PER_WALKER.get(key)
     t = ks[kern] * 1e-3
-    name = {"eval": "k_vmc<double> E_L phase", "moves": "k_vmc<float> move phase", "sweep": "k_vmc (fused sweep)"}[kern]
-    out = {"bound": f"{kprec} CUDA-core FMA pipe", "kernel": name, "unit": "TFLOP/s", "peak": peak,
+    name = {"eval": "FP64 full evaluation (k_el_jas, k_el_orb, k_el_inv, k_el_fin)", "moves": "k_vmc<float> move phase",
+            "sweep": "k_vmc (fused sweep)"}[kern]
+    out = {"bound": f"{kprec} FMA rate (CUDA cores; FP64 tensor cores run at the same rate)", "kernel": name,
+           "unit": "TFLOP/s", "peak": peak,
            "peak_source": f"{FMA_PER_SM_CLK[kprec]} {kprec.upper()} FMA/clk/SM x {NSM} SMs x 2 x {mhz:.0f} MHz (median "
                           f"SM clock measured in the timed region)",
            "share_of_step": ks[kern] / arm["ms_per_step"], "kernel_ms": ks[kern]}
