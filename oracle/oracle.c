@@ -97,6 +97,7 @@ struct orc_sys {
   double *c; /* [nct][nterms] */
   int tk[64], tl[64], tm[64];
   double asymp_r, asymp_jasa[CHAMP_MAX_CTYPE], asymp_jasb[2];
+  int een_cusp;
   /* pseudopotential */
   int nloc, nquad, mgauss;
   int npotd[CHAMP_MAX_CTYPE], lpotp1[CHAMP_MAX_CTYPE];
@@ -143,7 +144,7 @@ static double basis_anorm(int kind, int n, int l, double z) {
 
 /* Cusp conditions on the e-e-n coefficients (qmc/fit/cuspinit4.f90:1-60 builds d and
    iwc4; qmc/fit/cuspexact4.f90:14-40 solves for the dependent coefficients). */
-static void apply_een_cusp(orc_sys *s) {
+static void een_cusp(orc_sys *s, int *dep_out) {
   int nordc = s->nordc, nt = s->nterms;
   if (nordc <= 1) return;
   int neq = 2 * (nordc - 1);
@@ -167,6 +168,8 @@ static void apply_een_cusp(orc_sys *s) {
         if (m > 0) { iord = nordc - 1 + k + l + m; d[iord - 1][i - 1] -= m; }
       }
     }
+  if (dep_out)
+    for (int e = 0; e < neq; e++) dep_out[e] = iwc4[e] - 1;
   for (int it = 0; it < s->nct; it++) {
     double *c = s->c + (size_t)it * nt;
     int order[2 * MAXORD], no = 0;
@@ -181,6 +184,30 @@ static void apply_een_cusp(orc_sys *s) {
         if (j != jd) sum += d[e - 1][j - 1] * c[j - 1];
       c[jd - 1] = -sum / d[e - 1][jd - 1];
     }
+  }
+}
+static void apply_een_cusp(orc_sys *s) { een_cusp(s, NULL); }
+
+/* asymptotic values of the e-n and e-e terms (set_scale_dist, qmc/vmc/scale_dist.f90:147-225,
+   isc=4 branch) */
+static void set_asymptotes(orc_sys *s) {
+  s->asymp_r = 1.0 / s->scalek;
+  double ar = s->asymp_r;
+  for (int it = 0; it < s->nct; it++) {
+    double v = s->a4[it][0] * ar / (1 + s->a4[it][1] * ar);
+    for (int iord = 2; iord <= s->norda; iord++) v += s->a4[it][iord] * pow(ar, iord);
+    s->asymp_jasa[it] = v;
+  }
+  for (int i = 0; i < 2; i++) {
+    double sspinn = 1;
+    int isp = 0;
+    if (i == 1) {
+      sspinn = (s->nspin2b == 1) ? 0.5 : 1.0;
+      isp = s->nspin2b - 1;
+    }
+    double v = sspinn * s->b[isp][0] * ar / (1 + s->b[isp][1] * ar);
+    for (int iord = 2; iord <= s->nordb; iord++) v += s->b[isp][iord] * pow(ar, iord);
+    s->asymp_jasb[i] = v;
   }
 }
 
@@ -516,28 +543,9 @@ orc_sys *orc_create(const champ_system *d) {
         }
       }
   }
+  s->een_cusp = d->een_cusp;
   if (d->een_cusp) apply_een_cusp(s);
-  /* asymptotic values (set_scale_dist, qmc/vmc/scale_dist.f90:147-225, isc=4 branch) */
-  s->asymp_r = 1.0 / s->scalek;
-  {
-    double ar = s->asymp_r;
-    for (int it = 0; it < s->nct; it++) {
-      double v = s->a4[it][0] * ar / (1 + s->a4[it][1] * ar);
-      for (int iord = 2; iord <= s->norda; iord++) v += s->a4[it][iord] * pow(ar, iord);
-      s->asymp_jasa[it] = v;
-    }
-    for (int i = 0; i < 2; i++) {
-      double sspinn = 1;
-      int isp = 0;
-      if (i == 1) {
-        sspinn = (s->nspin2b == 1) ? 0.5 : 1.0;
-        isp = s->nspin2b - 1;
-      }
-      double v = sspinn * s->b[isp][0] * ar / (1 + s->b[isp][1] * ar);
-      for (int iord = 2; iord <= s->nordb; iord++) v += s->b[isp][iord] * pow(ar, iord);
-      s->asymp_jasb[i] = v;
-    }
-  }
+  set_asymptotes(s);
   /* pseudopotential */
   s->nloc = d->nloc;
   s->nquad = d->nquad > 0 ? d->nquad : 12;
@@ -1381,6 +1389,183 @@ int orc_eval_full(const orc_sys *s, const double *x, orc_eval *out) {
   int r = eval_full_ws(s, x, out, &w);
   wstate_free(&w);
   return r;
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* Jastrow parameter derivatives (deriv_jastrow4, qmc/vmc/deriv_jastrow4.f90: gvalue, g, d2g;  */
+/* the nonlocal part as deriv_nonloc_pot / deriv_nonloc, qmc/fit/deriv_nonloc_pot.f90)          */
+/* ------------------------------------------------------------------------------------ */
+/* The free Jastrow parameters in the engine's order: a_k (k = 2..norda) per centre type, b_k
+   (k = 1..nordb, i.e. b_2 first) per spin set, then the e-e-n terms not fixed by the cusp
+   conditions per centre type.  J is linear in all of them except b_2 (the Pade denominator), so
+   the Jastrow of a system whose only non-zero free parameter is p = 1 (its dependent e-e-n terms
+   solved from the cusp equations, the asymptotes recomputed) is dJ/dp with all its derivatives.
+   Returns 0 for such a parameter (t set up), 1 for b_2 of spin set *isb, -1 past the last. */
+static int unit_param_sys(const orc_sys *s, int p, orc_sys *t, double *cbuf, int *isb) {
+  *t = *s;
+  memset(t->a4, 0, sizeof t->a4);
+  memset(t->b, 0, sizeof t->b);
+  const int nt = s->nterms;
+  t->c = cbuf;
+  if (nt > 0) memset(cbuf, 0, sizeof(double) * s->nct * nt);
+  const int na = s->nct * (s->norda > 1 ? s->norda - 1 : 0), nb = s->nspin2b * s->nordb;
+  if (p < na) {
+    t->a4[p / (s->norda - 1)][2 + p % (s->norda - 1)] = 1.0;
+    set_asymptotes(t);
+    return 0;
+  }
+  p -= na;
+  if (p < nb) {
+    const int is = p / s->nordb, k = 1 + p % s->nordb;
+    if (k == 1) { *isb = is; return 1; }
+    t->b[is][k] = 1.0;
+    set_asymptotes(t);
+    return 0;
+  }
+  p -= nb;
+  if (s->nordc <= 1 || nt == 0) return -1;
+  int dep[2 * MAXORD], ndep = 0, fr[64], nfr = 0;
+  if (s->een_cusp) {
+    orc_sys u = *s;
+    double tmp[64];
+    memset(tmp, 0, sizeof tmp);
+    u.c = tmp;
+    u.nct = 1;
+    een_cusp(&u, dep);
+    ndep = 2 * (s->nordc - 1);
+  }
+  for (int ll = 0; ll < nt; ll++) {
+    int isdep = 0;
+    for (int q = 0; q < ndep; q++) isdep |= dep[q] == ll;
+    if (!isdep) fr[nfr++] = ll;
+  }
+  if (p >= s->nct * nfr) return -1;
+  cbuf[(p / nfr) * nt + fr[p % nfr]] = 1.0;
+  if (s->een_cusp) een_cusp(t, NULL);
+  set_asymptotes(t);
+  return 0;
+}
+
+/* d/d b_2 of the e-e term of pair (i, j) when it belongs to spin set isb_p: the value, its radial
+   derivative divided by r and f'' + 2 f'/r's pieces in jas_ee's form. */
+static void jas_ee_db2(const orc_sys *s, int i, int j, double rij, int isb_p, double *g, double *gu, double *guu) {
+  int isb, ipar;
+  double ss;
+  pair_spin(s, i, j, &isb, &ss, &ipar);
+  *g = *gu = *guu = 0;
+  if (isb != isb_p) return;
+  double u, dd1, dd2;
+  scale_dist2(s->scalek, rij, &u, &dd1, &dd2);
+  const double b1 = s->b[isb][0], b2 = s->b[isb][1], bot = 1 + b2 * u, ar = s->asymp_r, bota = 1 + b2 * ar;
+  const double v = -ss * b1 * u * u / (bot * bot) + ss * b1 * ar * ar / (bota * bota);
+  const double vu = -2 * ss * b1 * u / (bot * bot * bot);
+  const double vuu = -2 * ss * b1 * (1 - 2 * b2 * u) / (bot * bot * bot * bot);
+  *g = v;
+  *guu = vuu * dd1 * dd1 + vu * dd2;
+  *gu = vu * dd1 / rij;
+}
+
+/* Per free Jastrow parameter p at configuration x: gval[p] = dJ/dp and (when not NULL)
+   gvel[p][N][3] = d grad_i J/dp, d2[p] = d sum_i lap_i J/dp.  Returns the parameter count. */
+int orc_jastrow_pderiv(const orc_sys *s, const double *x, double *gval, double *gvel, double *d2) {
+  const int N = s->N;
+  double *cbuf = (double *)calloc((size_t)(s->nct * (s->nterms > 0 ? s->nterms : 1)), sizeof(double));
+  double v[3 * CHAMP_MAX_ELEC];
+  int p = 0;
+  for (;; p++) {
+    orc_sys t;
+    int isb = 0;
+    const int kind = unit_param_sys(s, p, &t, cbuf, &isb);
+    if (kind < 0) break;
+    double val = 0, dd = 0;
+    if (kind == 0) {
+      val = jastrow_full(&t, x, v, &dd, NULL, NULL);
+    } else {
+      for (int k = 0; k < 3 * N; k++) v[k] = 0;
+      for (int i = 1; i < N; i++)
+        for (int j = 0; j < i; j++) {
+          double rv[3], rij = 0;
+          for (int k = 0; k < 3; k++) { rv[k] = x[3 * i + k] - x[3 * j + k]; rij += rv[k] * rv[k]; }
+          rij = sqrt(rij);
+          double g, gu, guu;
+          jas_ee_db2(s, i, j, rij, isb, &g, &gu, &guu);
+          val += g;
+          for (int k = 0; k < 3; k++) { v[3 * i + k] += gu * rv[k]; v[3 * j + k] -= gu * rv[k]; }
+          dd += 2 * (guu + 2 * gu);
+        }
+    }
+    gval[p] = val;
+    if (gvel) memcpy(gvel + (size_t)p * 3 * N, v, sizeof(double) * 3 * N);
+    if (d2) d2[p] = dd;
+  }
+  free(cbuf);
+  return p;
+}
+
+/* d ln psi/dp and d E_L/dp of the free Jastrow parameters at x: the local part
+   -1/2 (d2g_p + 2 v . g_p) (hpsi's kinetic energy differentiated), and for a pseudopotential each
+   quadrature point's term w e^dJ v_l P_l (D'/D) times dJ(x with the electron at the point)/dp -
+   dJ(x)/dp.  Returns the parameter count, or -1 for a singular configuration. */
+int orc_jastrow_param_grad(const orc_sys *s, const double *x, double *dlnpsi, double *deloc) {
+  const int N = s->N, C = s->C, no = s->norb;
+  wstate_t w;
+  wstate_alloc(s, &w);
+  double vel[3 * CHAMP_MAX_ELEC];
+  orc_eval e;
+  memset(&e, 0, sizeof e);
+  e.vel = vel;
+  int sing = eval_full_ws(s, x, &e, &w);
+  const int np = orc_jastrow_pderiv(s, x, dlnpsi, NULL, NULL);
+  double *gvel = (double *)malloc(sizeof(double) * (size_t)(np > 0 ? np : 1) * 3 * N);
+  double *d2 = (double *)malloc(sizeof(double) * (np > 0 ? np : 1));
+  double *gq = (double *)malloc(sizeof(double) * (np > 0 ? np : 1));
+  orc_jastrow_pderiv(s, x, dlnpsi, gvel, d2);
+  for (int p = 0; p < np; p++) {
+    double vg = 0;
+    for (int k = 0; k < 3 * N; k++) vg += vel[k] * gvel[(size_t)p * 3 * N + k];
+    deloc[p] = -HB * (d2[p] + 2 * vg);
+  }
+  if (s->nloc > 0 && !sing) {
+    double *phi = (double *)malloc(sizeof(double) * 5 * s->nbasis);
+    double *ov = (double *)malloc(sizeof(double) * no);
+    double *xq = (double *)malloc(sizeof(double) * 3 * N);
+    for (int i = 0; i < N; i++) {
+      int sp = i < s->nup ? 0 : 1;
+      for (int ic = 0; ic < C; ic++) {
+        int ict = s->ctype[ic];
+        double rv[3], r = 0;
+        for (int k = 0; k < 3; k++) { rv[k] = x[3 * i + k] - s->cent[3 * ic + k]; r += rv[k] * rv[k]; }
+        r = sqrt(r);
+        double vps[MAXLCH];
+        orc_vps(s, ict, r, vps);
+        int iskip = 1;
+        for (int l = 0; l < s->npotd[ict]; l++)
+          if (l + 1 != s->lpotp1[ict] && fabs(vps[l]) > 1e-4) iskip = 0;
+        if (iskip) continue;
+        for (int iq = 0; iq < s->nquad; iq++) {
+          double costh = (rv[0] * s->q[iq][0] + rv[1] * s->q[iq][1] + rv[2] * s->q[iq][2]) / r;
+          double xn[3];
+          for (int k = 0; k < 3; k++) xn[k] = r * s->q[iq][k] + s->cent[3 * ic + k];
+          orbitals_val(s, xn, sp, ov, phi);
+          double dr = 0;
+          for (int j = 0; j < s->nocc[sp]; j++) dr += w.G[((size_t)sp * no + s->occ[sp][j]) * N + i] * ov[j];
+          double dj = nonlocj(s, x, i, xn, w.jt.fso);
+          double vp = 0;
+          for (int l = 0; l < s->npotd[ict]; l++)
+            if (l + 1 != s->lpotp1[ict]) vp += vps[l] * yl0(l, costh);
+          const double tq = s->wq[iq] * exp(dj) * vp * dr;
+          memcpy(xq, x, sizeof(double) * 3 * N);
+          for (int k = 0; k < 3; k++) xq[3 * i + k] = xn[k];
+          orc_jastrow_pderiv(s, xq, gq, NULL, NULL);
+          for (int p = 0; p < np; p++) deloc[p] += tq * (gq[p] - dlnpsi[p]);
+        }
+      }
+    }
+    free(phi); free(ov); free(xq);
+  }
+  free(gvel); free(d2); free(gq);
+  wstate_free(&w);
+  return sing ? -1 : np;
 }
 
 /* ------------------------------------------------------------------------------------ */

@@ -59,6 +59,11 @@ void orc_vps(const orc_sys *s, int ict, double r, double *vps /* [npotd] */);
 /* hpsie for one walker: psi(new)/psi(old) with electron iel at xnew, and grad ln psi
    of electron iel at xnew (grad may be NULL). */
 double orc_ratio_1e(const orc_sys *s, const double *x, int iel, const double *xnew, double *grad);
+/* Free Jastrow parameters (engine order): dJ/dp, d grad J/dp [np][N][3], d sum lap J/dp at x
+   (gvel, d2 may be NULL); returns np. */
+int orc_jastrow_pderiv(const orc_sys *s, const double *x, double *gval, double *gvel, double *d2);
+/* d ln psi/dp and d E_L/dp of the free Jastrow parameters at x; np, or -1 when singular. */
+int orc_jastrow_param_grad(const orc_sys *s, const double *x, double *dlnpsi, double *deloc);
 
 /* Counter-based random numbers shared in definition with the engine (Philox4x32-10). */
 void orc_philox(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t *out4);

@@ -53,6 +53,10 @@ def lib():
         L.orc_ratio_1e.argtypes = [vp, dp, ip, dp, dp]
         L.orc_philox.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32)]
         L.orc_random_rotation.argtypes = [C.c_uint64, C.c_uint32, C.c_uint64, dp]
+        L.orc_jastrow_param_grad.restype = ip
+        L.orc_jastrow_param_grad.argtypes = [vp, dp, dp, dp]
+        L.orc_jastrow_pderiv.restype = ip
+        L.orc_jastrow_pderiv.argtypes = [vp, dp, dp, dp, dp]
         L.orc_vmc.restype = ip
         L.orc_vmc.argtypes = [vp, ip, dp, ip, C.c_uint64, C.c_uint64, C.c_double, dp, dp, dp, dp, ip]
         _lib = L
@@ -106,6 +110,22 @@ class Oracle:
         out = {n: getattr(e, n) for n, _ in OrcEval._fields_[:13]}
         out.update(vel=vel, vj=vj, vd=vd, div_v=dv, singular=bool(sing))
         return out
+
+    def jastrow_param_grad(self, x):
+        """Analytic d ln psi/dp and d E_L/dp of the free Jastrow parameters (engine order)."""
+        x = np.ascontiguousarray(x, float).reshape(self.N, 3)
+        dl, de = np.zeros(4096), np.zeros(4096)
+        n = lib().orc_jastrow_param_grad(self.h, _p(x), _p(dl), _p(de))
+        if n < 0:
+            raise ValueError("singular configuration")
+        return dl[:n].copy(), de[:n].copy()
+
+    def jastrow_pderiv(self, x):
+        """dJ/dp, d grad_i J/dp [np][N][3] and d sum_i lap_i J/dp of the free Jastrow parameters."""
+        x = np.ascontiguousarray(x, float).reshape(self.N, 3)
+        g, v, d2 = np.zeros(4096), np.zeros(4096 * 3 * self.N), np.zeros(4096)
+        n = lib().orc_jastrow_pderiv(self.h, _p(x), _p(g), _p(v), _p(d2))
+        return g[:n].copy(), v[:n * 3 * self.N].reshape(n, self.N, 3).copy(), d2[:n].copy()
 
     def basis(self, pt):
         pt = np.ascontiguousarray(pt, float)

@@ -218,3 +218,32 @@ def test_oh_device_buffers_match_host_copy():
     assert np.array_equal(Sd.cpu().numpy(), Sh) and np.array_equal(Hd.cpu().numpy(), Hh)
     Sr, Hr = reduce_oh(eng)  # one rank: unchanged
     assert np.array_equal(Sr.cpu().numpy(), Sh)
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, "c2bfd", "be"])
+def test_jastrow_derivatives_match_oracle_analytic(oracle_mod, k):
+    """The Jastrow block of champ_param_grad (forward pass + reverse sweep, FP64) against the
+    oracle's analytic restatement of deriv_jastrow4 and deriv_nonloc_pot
+    (orc_jastrow_param_grad, itself pinned to finite differences in
+    tests/test_oracle_jastrow_derivs.py): 1e-9 of max(1, |value|) for d ln psi/dp and of
+    max(1, |E_L|) for dE_L/dp."""
+    from champ_b200.engine import Engine
+    if k == "c2bfd":
+        s = S.c2_bfd_example(10)
+    elif k == "be":
+        s = S.be_example()
+    else:
+        s = S.get_system(k)
+    nw = 8
+    x = S.initial_walkers(s, nw, seed=77)
+    eng = Engine(s, nw, "fp64")
+    eng.set_walkers(x)
+    nj, ncsf, norb = eng.nparam()
+    dl, de, el = eng.param_grad()
+    o = oracle_mod.Oracle(s)
+    for w in range(nw):
+        rl, re_ = o.jastrow_param_grad(x[w])
+        assert len(rl) == nj
+        gl, ge = dl[w, ncsf + norb:], de[w, ncsf + norb:]
+        assert np.all(np.abs(gl - rl) <= 1e-9 * np.maximum(1.0, np.abs(rl))), np.abs(gl - rl).max()
+        assert np.all(np.abs(ge - re_) <= 1e-9 * max(1.0, abs(el[w]))), np.abs(ge - re_).max()
