@@ -270,6 +270,8 @@ def vmc_arm(system, nw, prec, steps, warmup, flush, torch, rank, world, x0=None,
     eng.set_walkers(x0 if x0 is not None else system_walkers(system, nw, seed=1000 + rank))
     if x0 is None:
         eng.vmc_sweeps(10, SEED + rank, sweep0=0, step=step_size(system), stats=False)  # equilibration
+    # launch options that change only the speed (champ_autotune), chosen before the timed region
+    tuned = eng.autotune(nsweep=2, seed=SEED + 7, step=step_size(system))
     torch.cuda.synchronize()
     if world > 1:
         import torch.distributed as dist
@@ -286,7 +288,7 @@ def vmc_arm(system, nw, prec, steps, warmup, flush, torch, rank, world, x0=None,
     out = {"value": nw * world * system.nelec * steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps,
            "steps": steps, "precision": prec, "wall_s_timed_region": tw,
            "kernels_ms_per_step": {k: v[0] / steps for k, v in ph.items() if v[1]},
-           "launches_per_step": eng.get_option("launches_per_sweep")}
+           "launches_per_step": eng.get_option("launches_per_sweep"), "autotune": tuned}
     if cl:
         out["clocks"] = cl
     if pg_steps:
@@ -487,7 +489,8 @@ def main():
                 "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": {"mixed": "f32 moves + f64 E_L", "fp64": "f64", "fp32": "f32+f64"}[prec],
-                "data": "synthetic", "config": config_of(system, nw, prec), "clocks": head.get("clocks"),
+                "data": "synthetic", "config": dict(config_of(system, nw, prec), autotune=head.get("autotune")),
+                "clocks": head.get("clocks"),
                 "gpu_launches": launches, "kernels_ms_per_step": head["kernels_ms_per_step"],
                 "roofline": roof, "param_grad": head.get("param_grad"), "mixed_error": err,
                 "arms": arms, "fp32_error": fp32_err, "e2e": e2e, "cpu_baseline": cpu,

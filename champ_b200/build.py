@@ -14,7 +14,7 @@ from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-UNITS = ["host.cu", "linear.cu", "optimize.cu"] + [f"inst_{t}_n{n}.cu" for t in ("f32", "f64") for n in (0, 4, 5)]
+UNITS = ["host.cu", "linear.cu", "optimize.cu", "tune.cu"] + [f"inst_{t}_n{n}.cu" for t in ("f32", "f64") for n in (0, 4, 5)]
 DEPS = [os.path.join(HERE, "..", "include", "champ_b200.h")] + glob.glob(os.path.join(CSRC, "*"))
 LIB = os.path.join(HERE, "libchamp_b200.so")
 OBJDIR = os.path.join(HERE, "_build")

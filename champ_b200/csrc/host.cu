@@ -746,6 +746,18 @@ static int setup_el_staged(champ_ctx *c) {
   return CHAMP_OK;
 }
 
+// Delayed inverse updates of the moves (struct Delay) for a walker state in HBM: room for up to
+// DELAY_MAX pending terms per spin; option "delay_rank" picks how many are folded in at a time.
+static constexpr int DELAY_MAX = 32, DELAY_DEFAULT = 4;
+static int setup_delay(champ_ctx *c) {
+  State<double> &st = c->std_;
+  st.dly = dalloc<double>(c, (size_t)c->wmax * 4 * DELAY_MAX * c->nmax);
+  if (!st.dly) return fail(CHAMP_ENOMEM, "allocation of the delayed-update buffer failed");
+  st.dlk = DELAY_DEFAULT;
+  st.dlk_max = DELAY_MAX;
+  return CHAMP_OK;
+}
+
 // Mixed precision: the FP32 state of the single-electron moves shares every FP64 buffer with the
 // FP64 state (positions, inverses, log-det, determinant tables, outputs, statistics) and owns
 // only the FP32 Jastrow pair table, distances and power sums, which every FP64 full evaluation
@@ -767,6 +779,9 @@ static void link_move_state(State<double> &d, State<float> &f) {
   f.m_rtd = nullptr;
   d.m_rtd = f.rtd;
   d.rtd = nullptr;
+  f.dly = d.dly;
+  f.dlk = d.dlk;
+  f.dlk_max = d.dlk_max;
 }
 
 static int build_move_state(champ_ctx *c, State<double> &d, State<float> &f) {
@@ -1017,6 +1032,7 @@ static size_t noalloc_carve(const champ_ctx *c, const State<T> &ref, int nw, cha
   st.m_fso = st.m_ren = st.m_zq = nullptr;  // the context's own move tables stay untouched
   st.m_rtd = nullptr;
   st.rtd = nullptr;
+  st.dly = nullptr;
   st.el_vj = st.el_sc = nullptr;
   st.el_rt = nullptr;
   return o <= NOALLOC_BYTES ? o : 0;
@@ -1441,6 +1457,7 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
     if (!rc) rc = finish_cfg(c->kd);
     // walker state in HBM: the full evaluation as the four kernels of elstage.cuh
     if (!rc && !c->kd.lay.resident) rc = setup_el_staged(c);
+    if (!rc && !c->kd.lay.resident && !c->md.multidet) rc = setup_delay(c);
   }
   if (use32 && !rc) {
     rc = build_sys<float>(c, d, pcn, cfull, asa, asb, ecp, pecent, c->sf);
@@ -2069,6 +2086,14 @@ int champ_set_option(champ_ctx *c, const char *name, int64_t value) {
     c->pg_mode = (int)value;
     return CHAMP_OK;
   }
+  if (!strcmp(name, "delay_rank")) {
+    if (value < 0 || value > DELAY_MAX) return fail(CHAMP_EINVAL, "delay_rank: 0 .. 32");
+    if (value > 1 && !c->std_.dly)
+      return fail(CHAMP_EINVAL, "delay_rank: needs a single-determinant FP64 or mixed context whose walker state "
+                                "lives in HBM");
+    c->std_.dlk = c->stf.dlk = (int)value;
+    return CHAMP_OK;
+  }
   if (!strcmp(name, "staged_eval")) {
     if (value && !c->std_.el_vj)
       return fail(CHAMP_EINVAL, "staged_eval: needs an FP64 or mixed context whose walker state lives in HBM");
@@ -2111,6 +2136,7 @@ int champ_get_option(const champ_ctx *c, const char *name, int64_t *value) {
   if (!strcmp(name, "phase_timing")) { *value = c->ptime; return CHAMP_OK; }
   if (!strcmp(name, "param_grad_mode")) { *value = c->pg_mode; return CHAMP_OK; }
   if (!strcmp(name, "staged_eval")) { *value = c->el_staged; return CHAMP_OK; }
+  if (!strcmp(name, "delay_rank")) { *value = c->std_.dly ? c->std_.dlk : 0; return CHAMP_OK; }
   return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);
 }
 

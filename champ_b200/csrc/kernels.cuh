@@ -67,6 +67,10 @@ struct State {
   // as [2][C][N] planes
   double *el_vj, *el_sc;
   T *el_rt;
+  // delayed inverse updates of the moves (struct Delay): [W][2][2][dlk_max][nmax] pending terms,
+  // dlk terms per flush; null / 0 when the updates are applied at once
+  double *dly;
+  int dlk, dlk_max;
 };
 constexpr int NLT = 2 + MAXLCH;  // task record: (e*C+c), r, vps[0..MAXLCH-1]
 constexpr int ZQ = 8;            // stride of the per-electron power sums zq
@@ -1192,12 +1196,64 @@ __device__ void full_eval(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, 
 // ---------------------------------------------------------------------------------------
 // single-electron proposal (hpsie, qmc/vmc/hpsie.f90) and acceptance (jassav/detsav)
 // ---------------------------------------------------------------------------------------
+// Delayed Sherman-Morrison updates of the reference inverse (single determinant, walker state in
+// HBM; dete_update, dete_mod.f90:165-190, applied lazily): the accepted moves of a spin are kept as
+// rank-1 terms, A = A_0 - sum_i u_i w_i^T (u_i the inverse's column of the moved electron over the
+// ratio, w_i the moved row times the inverse minus the unit row), and folded into A_0 as one
+// rank-K product on the FP64 tensor cores every K accepted moves of the spin and at the end of the
+// moves.  Proposals read the current column of A from A_0 and the pending terms.
+struct Delay {
+  double *buf;  // this walker's [2 spins][u rows, w rows][K][nmax]; null: updates applied at once
+  int K, nmax;
+  int m[2];     // pending terms per spin
+  __device__ double *u(int sp, int i) const { return buf + ((size_t)(2 * sp) * K + i) * nmax; }
+  __device__ double *wr(int sp, int i) const { return buf + ((size_t)(2 * sp + 1) * K + i) * nmax; }
+};
+
+// Column eo of the current inverse of spin sp into col[n].
+__device__ inline void delay_column(const Delay &d, const double *A0, int n, int sp, int eo, double *col, int lane) {
+  for (int k = lane; k < n; k += 32) {
+    double a = A0[k * n + eo];
+    for (int i = 0; i < d.m[sp]; i++) a -= d.u(sp, i)[k] * d.wr(sp, i)[eo];
+    col[k] = a;
+  }
+  __syncwarp();
+}
+
+// A_0 -= sum_{i < m} u_i w_i^T for spin sp: 8 x 8 tiles of A_0, k-steps of 4 pending terms
+// (mma m8n8k4, FP64; terms past m read as zero).
+__device__ inline void delay_flush(Delay &d, double *A0, int n, int sp, int lane) {
+  const int m = d.m[sp];
+  if (m == 0) return;
+  __syncwarp();
+  const int r = lane >> 2, q = lane & 3;
+  for (int k0 = 0; k0 < n; k0 += 8)
+    for (int j0 = 0; j0 < n; j0 += 8) {
+      const int kr = k0 + r, jc = j0 + 2 * q;
+      double c0 = (kr < n && jc < n) ? A0[kr * n + jc] : 0.0;
+      double c1 = (kr < n && jc + 1 < n) ? A0[kr * n + jc + 1] : 0.0;
+      for (int i0 = 0; i0 < m; i0 += 4) {
+        const int i = i0 + q;
+        const double a = (i < m && kr < n) ? -d.u(sp, i)[kr] : 0.0;        // A[row k][col i]
+        const double b = (i < m && j0 + r < n) ? d.wr(sp, i)[j0 + r] : 0.0;  // B[row i][col j]
+        dmma_884(c0, c1, a, b);
+      }
+      if (kr < n && jc < n) A0[kr * n + jc] = c0;
+      if (kr < n && jc + 1 < n) A0[kr * n + jc + 1] = c1;
+    }
+  d.m[sp] = 0;
+  __syncwarp();
+}
+
 template <class T, int NORD, bool MD, bool GRAD>
 __device__ void propose(const Sys<T> &s, const JasPar<T> &J, const State<T> &st, int w, const View<T> &v, int e,
-                        const double *xn, int lane, double &rho, double &dj, double *grad) {
+                        const double *xn, int lane, double &rho, double &dj, double *grad, const Delay *dl = nullptr) {
   const int N = s.N, C = s.C, nomax = s.nomax;
   int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
   const double *A = gam_ptr<T, MD>(s, v, sp);
+  // with delayed updates the column of the current inverse goes to v.colb (accept_move reuses it)
+  const bool dcol = !MD && dl && dl->buf;
+  if (dcol) delay_column(*dl, A, n, sp, eo, v.colb, lane);
   const int no = s.nocc[sp];
   constexpr int NCH = GRAD ? 5 : 1;
   for (int c = lane; c < C; c += 32) {
@@ -1218,7 +1274,7 @@ __device__ void propose(const Sys<T> &s, const JasPar<T> &J, const State<T> &st,
   // the wave function is linear in the moved electron's orbital row: ratio = sum_m G[m][e] phi_m
   double r0 = 0, g0 = 0, g1 = 0, g2 = 0;
   for (int k = lane; k < no; k += 32) {
-    double a = A[k * n + eo];
+    double a = dcol ? v.colb[k] : A[k * n + eo];
     r0 += a * (double)v.arow[k];
     if (GRAD) {
       g0 += a * (double)v.arow[nomax + k];
@@ -1271,18 +1327,42 @@ __device__ void propose(const Sys<T> &s, const JasPar<T> &J, const State<T> &st,
 // row is v.arow (channel 0), the proposed pair values v.pf, distances v.rnew.
 template <class T, bool MD>
 __device__ void accept_move(const Sys<T> &s, const State<T> &st, int w, const View<T> &v, int e, const double *xn,
-                            double dj, double rho, int lane) {
+                            double dj, double rho, int lane, Delay *dl = nullptr) {
   const int N = s.N, C = s.C;
   int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
   double *A = v.ainv + (sp ? s.nup * s.nup : 0);
-  for (int k = lane; k < n; k += 32) v.colb[k] = A[k * n + eo];
+  const bool delayed = !MD && dl && dl->buf;
+  if (!delayed)
+    for (int k = lane; k < n; k += 32) v.colb[k] = A[k * n + eo];
   for (int j = lane; j < n; j += 32) {
     double a = 0;
     for (int k = 0; k < n; k++) a += (double)v.arow[k] * A[k * n + j];
     v.vb[j] = a - (j == eo ? 1.0 : 0.0);
   }
+  if (delayed) {
+    // the pending terms: vb -= sum_i (arow . u_i) w_i
+    const int m = dl->m[sp];
+    for (int i = 0; i < m; i++) {
+      const double *ui = dl->u(sp, i);
+      double p = 0;
+      for (int k = lane; k < n; k += 32) p += (double)v.arow[k] * ui[k];
+      p = warp_sum(p);
+      const double *wi = dl->wr(sp, i);
+      for (int j = lane; j < n; j += 32) v.vb[j] -= p * wi[j];
+    }
+  }
   __syncwarp();
   double rinv = 1.0 / (v.vb[eo] + 1.0);
+  if (delayed) {
+    const int m = dl->m[sp];
+    double *um = dl->u(sp, m), *wm = dl->wr(sp, m);
+    for (int k = lane; k < n; k += 32) {
+      um[k] = v.colb[k] * rinv;
+      wm[k] = v.vb[k];
+    }
+    dl->m[sp] = m + 1;
+    if (m + 1 == dl->K) delay_flush(*dl, A, n, sp, lane);
+  }
   if (MD) {
     // T update: T += Ainv[:,e] (atilde'_virt - a'^T T) / rho_ref (dete_update, dete_mod.f90:186-190)
     const int nv = s.nvirt[sp];
@@ -1300,10 +1380,11 @@ __device__ void accept_move(const Sys<T> &s, const State<T> &st, int w, const Vi
     }
     __syncwarp();
   }
-  for (int idx = lane; idx < n * n; idx += 32) {
-    int k = idx / n, j = idx - k * n;
-    A[idx] -= v.colb[k] * v.vb[j] * rinv;
-  }
+  if (!delayed)
+    for (int idx = lane; idx < n * n; idx += 32) {
+      int k = idx / n, j = idx - k * n;
+      A[idx] -= v.colb[k] * v.vb[j] * rinv;
+    }
   if (MD) {
     __syncwarp();
     double lc, sc;
@@ -1460,6 +1541,11 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
       __syncwarp();
     }
     double es = 0, e2 = 0, acc = 0, el = 0;
+    Delay dl{};
+    dl.buf = (moves && !MD && !L.resident && st.dly && st.dlk > 1)
+                 ? st.dly + (size_t)w * 4 * st.dlk_max * s.nmax : nullptr;
+    dl.K = st.dlk;
+    dl.nmax = s.nmax;
     for (int isw = 0; isw < nsweep; isw++) {
       uint64_t sweep = sweep0 + (uint64_t)isw;
       for (int e = 0; moves && e < N; e++) {
@@ -1467,12 +1553,16 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
         move_randoms(seed, (uint32_t)w, sweep, (uint32_t)e, g, &ua);
         double xn[3] = {v.xs[3 * e] + step * g[0], v.xs[3 * e + 1] + step * g[1], v.xs[3 * e + 2] + step * g[2]};
         double rho, dj, gr[3];
-        propose<T, NORD, MD, false>(s, J, st, w, v, e, xn, lane, rho, dj, gr);
+        propose<T, NORD, MD, false>(s, J, st, w, v, e, xn, lane, rho, dj, gr, &dl);
         double p = rho * rho * exp(2.0 * dj);
         if (ua < p) {
-          accept_move<T, MD>(s, st, w, v, e, xn, dj, rho, lane);
+          accept_move<T, MD>(s, st, w, v, e, xn, dj, rho, lane, &dl);
           acc += 1;
         }
+      }
+      if (dl.buf) {  // the sweep's pending inverse updates, before anything else reads the inverse
+        delay_flush(dl, v.ainv, s.nup, 0, lane);
+        delay_flush(dl, v.ainv + s.nup * s.nup, s.ndn, 1, lane);
       }
       if constexpr (!eval) continue;
       double R[9];

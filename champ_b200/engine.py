@@ -25,7 +25,7 @@ EXPORTED_SYMBOLS = [
     "champ_dmc_init", "champ_dmc_steps", "champ_num_walkers", "champ_eval_energy_noalloc", "champ_set_option",
     "champ_get_option", "champ_oh_buffers", "champ_phase_times", "champ_param_grad_fwd", "champ_param_grad_bwd",
     "champ_linear_update", "champ_set_params", "champ_get_params", "champ_apply_param_step",
-    "champ_check_param_step", "champ_eval_param_step", "champ_linear_method_step",
+    "champ_check_param_step", "champ_eval_param_step", "champ_linear_method_step", "champ_autotune",
 ]
 
 PREC = {"fp64": 0, "mixed": 1, "fp32": 2}
@@ -90,6 +90,7 @@ def load_library(path: str = LIB_PATH):
     L.champ_check_param_step.argtypes = [vp, dp, C.c_double, C.POINTER(i32)]
     L.champ_eval_param_step.argtypes = [vp, dp, dp, dp]
     L.champ_linear_method_step.argtypes = [vp, i32, C.POINTER(i32), dp, dp, C.c_double, C.c_double, dp, dp, dp]
+    L.champ_autotune.argtypes = [vp, i32, u64, C.c_double, C.c_char_p, C.c_char_p, i32]
     for n in EXPORTED_SYMBOLS:
         if n not in ("champ_last_error", "champ_version"):
             getattr(L, n).restype = C.c_int
@@ -256,6 +257,14 @@ class Engine:
     def apply_param_step(self, dp):
         dp = np.ascontiguousarray(dp, np.float64)
         self._check(self.lib.champ_apply_param_step(self.h, _p(dp)))
+
+    def autotune(self, nsweep=2, seed=1, step=None, cache=None):
+        """champ_autotune: picks the fastest launch options on the current walkers; returns the
+        one-line report."""
+        buf = C.create_string_buffer(1024)
+        st = self.system.step if step is None else step
+        self._check(self.lib.champ_autotune(self.h, nsweep, seed, st, cache.encode() if cache else None, buf, 1024))
+        return buf.value.decode()
 
     def check_param_step(self, dp, psi_lin_var_norm=0.0):
         """champ_check_param_step: 0 (good), 1 (bad) or 2 (bad for any stabilisation)."""

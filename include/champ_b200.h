@@ -375,7 +375,12 @@ int champ_synchronize(champ_ctx *ctx);
    runs the FP64 full evaluation as four kernels sized for their own parts (Jastrow and
    distances; basis and orbitals per electron; Slater-matrix inversion in shared memory;
    velocities, pseudopotential and E_L), and a VMC sweep of an FP64 context as its moves followed
-   by that evaluation; 0 runs the single-kernel evaluation (and the fused FP64 sweep kernel). */
+   by that evaluation; 0 runs the single-kernel evaluation (and the fused FP64 sweep kernel).
+   "delay_rank": K >= 2 (default 4 when the walker state of a single-determinant FP64 or mixed
+   context lives in HBM) keeps the accepted moves' Sherman-Morrison terms of a spin aside and
+   folds K of them at a time into the inverse as one FP64 tensor-core product (proposals use the
+   inverse with the pending terms; all are folded in at the end of a sweep's moves); 0 or 1
+   applies each update at once. */
 int champ_set_option(champ_ctx *ctx, const char *name, int64_t value);
 /* Device time of the VMC sweep kernels launched since option "phase_timing" was set to 1 or
    since the previous call (no counterpart in the reference: instrumentation for benchmarks),
@@ -385,8 +390,21 @@ int champ_set_option(champ_ctx *ctx, const char *name, int64_t value);
    with "staged_eval" 1), ms[3] unused; launches[] (may be NULL) the counts of timed sections.
    Synchronises the stream and resets the sums. */
 int champ_phase_times(champ_ctx *ctx, double *ms /* [4] */, int32_t *launches /* [4] or NULL */);
+/* Autotuning of the launch shapes (no counterpart in the reference): for the options that change
+   only the speed of a VMC sweep -- "delay_rank" (0, 4, 8, 16), "staged_eval" (1, 0), and with the
+   tensor-core orbitals of an FP32 context "orbital_tc" (1, 2) and "orbital_tc_chunk" (2, 4, 8) --
+   one option at a time, in that order, times nsweep sweeps of the context's walkers (step size
+   step, after one untimed sweep; device time from CUDA events) for each value it accepts, and
+   keeps the fastest.  The probe sweeps move the walkers as equilibration sweeps would.  With
+   cache_path (may be NULL) the choice is appended to that text file under a key of the system's
+   shape (electrons, centres, basis functions, orbitals, determinants, e-e-n order, pseudopotential,
+   precision, walkers), and a later call with the same key applies it without timing.  report
+   (may be NULL) receives a one-line summary: the chosen values and the ms per sweep of each
+   candidate. */
+int champ_autotune(champ_ctx *ctx, int32_t nsweep, uint64_t seed, double step, const char *cache_path, char *report,
+                   int32_t report_len);
 /* Current value of an option ("orbital_tc", "orbital_tc_chunk", "reinvert_every", "dmc_graph",
-   "phase_timing", "param_grad_mode", "staged_eval"); kernel launches per champ_vmc_sweeps sweep
+   "phase_timing", "param_grad_mode", "staged_eval", "delay_rank"); kernel launches per champ_vmc_sweeps sweep
    ("launches_per_sweep": 1 for the fused sweep kernel, 2 for moves + single-kernel evaluation,
    5 for moves + staged evaluation or with the tensor-core orbitals). */
 int champ_get_option(const champ_ctx *ctx, const char *name, int64_t *value);
