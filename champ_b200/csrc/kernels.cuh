@@ -841,9 +841,11 @@ __device__ void nlpp_energy(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E
   const double *xs = v.xs;
   const T *fso = v.fso;
   const T sk = J.scalek;
-  // FP64 with up to 32 centres: the X sums on the tensor cores, without the per-lane distances in
-  // shared memory; else in each lane from those distances (scratch permitting)
-  const bool mma = std::is_same<T, double>::value && NORD > 1 && J.nct == 1 && C <= 32;
+  // FP64 with 16 to 32 centres and at least 16 electrons: the X sums on the tensor cores (whose
+  // tiles of 8 electrons and k-steps of 4 centres smaller systems would mostly leave empty),
+  // without the per-lane distances in shared memory; else in each lane from those distances
+  // (scratch permitting)
+  const bool mma = std::is_same<T, double>::value && NORD > 1 && J.nct == 1 && C >= 16 && C <= 32 && N >= 16;
   const bool fast = mma || ((NORD > 1) && J.nct == 1 && C <= MAXC_NL && nscr >= 32 * C);
   const int nrown = nscr - (fast && !mma ? 32 * C : 0);
   T *const prs = fast && !mma ? scr + nrown + lane : nullptr;  // this lane's point-centre distances, stride 32
