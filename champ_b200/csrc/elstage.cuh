@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(128, 4) k_el_fin(Sys<T> s, State<T> st, int ns
       if (rot.random) random_rotation(rot.seed, (uint32_t)w, rot.sweep, R);
       else
         for (int i = 0; i < 9; i++) R[i] = rot.R[i];
-      nlpp_energy<T, NORD, MD, false>(s, J, E, v, R, lane, nullptr, scr, nscr, st.el_rt + (size_t)w * 2 * C * N, vloc,
+      nlpp_energy<T, NORD, MD, false, true>(s, J, E, v, R, lane, nullptr, scr, nscr, st.el_rt + (size_t)w * 2 * C * N, vloc,
                                       vnl, ntask);
     }
     EvalRes res;

@@ -829,11 +829,13 @@ __device__ double nl_pairs_mma(const Sys<double> &s, const JasPar<double> &J, co
 
 // Nonlocal pseudopotential energy of one walker (nonloc_pot.f90, nonloc.f90), quadrature rotated
 // by R.  scr: nscr elements of per-warp shared scratch, holding the radial parts of the tasks'
-// centres' shells and, on the one-centre-type path in FP32, each lane's scaled point-centre
-// distances (stored [centre][lane], 32 C elements at the end).  st_rt: the walker's e-n distance planes
+// centres' shells and, on the one-centre-type path without the tensor cores, each lane's scaled
+// point-centre distances (stored [centre][lane], 32 C elements at the end).  TC: the FP64 X sums
+// may run on the tensor cores (compiled only into the staged evaluation, whose registers the
+// single-kernel evaluation of small systems does not have to carry).  st_rt: the walker's e-n distance planes
 // (State::el_rt) or null.  Returns the local and nonlocal parts and the number of (electron,
 // centre) tasks.
-template <class T, int NORD, bool MD, bool PG>
+template <class T, int NORD, bool MD, bool PG, bool TC = false>
 __device__ void nlpp_energy(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, const View<T> &v, const double *R,
                             int lane, const PGBuf *pg, T *scr, int nscr, const T *st_rt, double &vloc_o, double &vnl_o,
                             int &ntask_o) {
@@ -845,7 +847,7 @@ __device__ void nlpp_energy(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E
   // tiles of 8 electrons and k-steps of 4 centres smaller systems would mostly leave empty),
   // without the per-lane distances in shared memory; else in each lane from those distances
   // (scratch permitting)
-  const bool mma = std::is_same<T, double>::value && NORD > 1 && J.nct == 1 && C >= 16 && C <= 32 && N >= 16;
+  const bool mma = TC && std::is_same<T, double>::value && NORD > 1 && J.nct == 1 && C >= 16 && C <= 32 && N >= 16;
   const bool fast = mma || ((NORD > 1) && J.nct == 1 && C <= MAXC_NL && nscr >= 32 * C);
   const int nrown = nscr - (fast && !mma ? 32 * C : 0);
   T *const prs = fast && !mma ? scr + nrown + lane : nullptr;  // this lane's point-centre distances, stride 32
@@ -997,7 +999,7 @@ __device__ void nlpp_energy(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E
     if (SHARE)
 #pragma unroll
       for (int ll = 0; ll < NT; ll++) tsum[ll] = T(0);
-    constexpr bool MMA = std::is_same<T, double>::value && !SHARE;
+    constexpr bool MMA = TC && std::is_same<T, double>::value && !SHARE;
     if (MMA && mma) {
       if constexpr (MMA) {
         const double *bd = st_rt ? st_rt + (size_t)C * N : v.ren + 1;
