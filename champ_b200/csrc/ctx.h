@@ -80,6 +80,8 @@ struct champ_ctx {
   // staged evaluation (elstage.cuh) of the FP64 state when it lives in HBM: on/off (option
   // "staged_eval"), warps per block and dynamic shared memory of k_el_jas, k_el_orb, k_el_fin,
   // and the pseudopotential scratch of k_el_fin (elements)
+  // the VMC mover (champ_set_mover): Gaussian displacements, or the accelerated Metropolis method
+  Mover mover{1, 5.0, 1.0, 1.0};
   int el_staged = 0;
   int el_wpb[3] = {4, 4, 4};
   size_t el_smem[3] = {0, 0, 0};

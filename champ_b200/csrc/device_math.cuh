@@ -166,6 +166,262 @@ __device__ inline void move_randoms(uint64_t seed, uint32_t w, uint64_t sweep, u
   *ua = u32d(b[3]);
 }
 
+// ---------------------------------------------------------------------------------------
+// Accelerated Metropolis proposal (imetro = 6; metrop_slat_mov1.f90:82-546, Umrigar's
+// accelerated Metropolis): the electron moves in spherical coordinates about its nearest
+// nucleus -- the new radius drawn between r/deltar and r deltar from sqrt(r)|1 + co r| e^-zeta r,
+// whose shape follows the radial drift and the cusp, the polar angle within a cone that narrows
+// near the nucleus, the azimuth biased by the tangential drift -- and the forward and reverse
+// transition probabilities enter the acceptance.  Scalar FP64 code that every lane of a warp runs
+// alike on the same random numbers.
+// ---------------------------------------------------------------------------------------
+struct Mover {
+  int kind;  // 1: Gaussian displacements of size step; 6: accelerated Metropolis
+  double deltar, deltat, fbias;
+};
+
+// The uniforms of one accelerated move: Philox keyed by (walker, sweep) with the electron and a
+// draw counter in the last counter word (bit 31 set, apart from the words of move_randoms and
+// random_rotation); draws past 2^15 per move reuse the last pair.
+struct MoveRng {
+  uint64_t seed;
+  uint32_t w, s0, s1, e, ctr;
+  double u[2];
+  int left;
+  __host__ __device__ double next() {
+    if (left == 0) {
+      uint32_t o[4];
+      philox(seed, w, s0, s1, 0x80000000u | (e << 15) | (ctr < 32767u ? ctr : 32767u), o);
+      ctr++;
+      u[0] = u53(o[0], o[1]);
+      u[1] = u53(o[2], o[3]);
+      left = 2;
+    }
+    return u[2 - left--];
+  }
+};
+
+// Incomplete gamma function of order a at x times x^a e^-x / x^a e^-x supplied as xae (gammai.f90):
+// the lower function by its series below a + 4 (iflag = 1), minus the upper one by its continued
+// fraction above (iflag = -1), with the reference's iteration counts.
+__host__ __device__ inline double slat_gammai(double a, double x, double xae, int &iflag) {
+  if (x < a + 4) {
+    iflag = 1;
+    double ap = a, sum = 1 / a, del = sum;
+    const int iter = (int)(21 + 3 * (x - a));
+    for (int n = 1; n <= iter; n++) {
+      ap += 1;
+      del *= x / ap;
+      sum += del;
+    }
+    return sum * xae;
+  }
+  iflag = -1;
+  double a0 = 1, a1 = x, b0 = 0, b1 = 1, fac = 1, g = 0;
+  const long na = lround(a - x);
+  const int iter = (int)(20 + na > 7 ? 20 + na : 7);
+  for (int n = 1; n <= iter; n++) {
+    const double an = (double)n, ana = an - a;
+    a0 = (a1 + a0 * ana) * fac;
+    b0 = (b1 + b0 * ana) * fac;
+    const double anf = an * fac;
+    a1 = x * a0 + anf * a1;
+    b1 = x * b0 + anf * b1;
+    fac = 1 / a1;
+    g = b1 * fac;
+  }
+  return -g * xae;
+}
+
+// Shape of the radial distribution about a nucleus at distance r with radial drift vr and cusp
+// zcusp: zeta and co of sqrt(r)|1 + co r| e^-zeta r.
+__host__ __device__ inline void slat_shape(double zcusp, double vr, double r, double &zeta, double &co) {
+  const double eps = 1e-10;
+  double root = (zcusp + vr) * (zcusp + vr - 4 / r);
+  if (root >= 0) {
+    root = sqrt(root);
+    zeta = 0.5 * (zcusp - vr - root);
+    if (zeta <= 0) zeta = 0.5 * (zcusp - vr + root);
+    if (zeta <= 0) zeta = eps;
+  } else {
+    zeta = vr < 0 ? -vr - eps : 1.0;
+  }
+  co = (zeta + vr) / (1 - (zeta + vr) * r);
+}
+
+// Integral of that distribution over [rbot, rtop] divided by its value bot at the current radius.
+__host__ __device__ inline double slat_area(double zeta, double co, double rbot, double rtop, double bot) {
+  const double g5b2 = 1.329340388179137, d2b3 = 0.666666666666667;
+  const double rzero = -1 / co, zrbot = zeta * rbot, zrtop = zeta * rtop;
+  const double zebot = sqrt(zrbot * zrbot * zrbot) * exp(-zrbot), zetop = sqrt(zrtop * zrtop * zrtop) * exp(-zrtop);
+  int fb, ft, fz;
+  const double gbot = slat_gammai(2.5, zrbot, zrbot * zebot, fb), gtop = slat_gammai(2.5, zrtop, zrtop * zetop, ft);
+  const double norm = bot * sqrt(zeta * zeta * zeta);
+  if (rzero < rbot || rzero > rtop) {
+    const double g52 = (fb * ft == 1) ? gtop - gbot : gtop - gbot + g5b2;
+    const double g32 = d2b3 * (g52 + zetop - zebot);
+    return fabs(g32 + co * g52 / zeta) / norm;
+  }
+  const double zrzer = zeta * rzero, zezer = sqrt(zrzer * zrzer * zrzer) * exp(-zrzer);
+  const double gzer = slat_gammai(2.5, zrzer, zrzer * zezer, fz);
+  const double g521 = (fb * fz == 1) ? gzer - gbot : gzer - gbot + g5b2;
+  const double g321 = d2b3 * (g521 + zezer - zebot);
+  const double g522 = (ft * fz == 1) ? gtop - gzer : gtop - gzer + g5b2;
+  const double g322 = d2b3 * (g522 + zetop - zezer);
+  return (fabs(g321 + co * g521 / zeta) + fabs(g322 + co * g522 / zeta)) / norm;
+}
+
+__host__ __device__ inline double slat_thetamx(const Mover &m, double r, double z) {
+  return m.deltat + (2 - m.deltat) / (1 + (z * r) * (z * r));
+}
+
+// Nearest centre of point p and the vector from it.
+template <class SysT>
+__host__ __device__ inline int slat_nearest(const SysT &s, const double *p, double *rv, double &r) {
+  int best = 0;
+  double bd = 1e300;
+  for (int c = 0; c < s.C; c++) {
+    const double d0 = p[0] - s.cent[3 * c], d1 = p[1] - s.cent[3 * c + 1], d2 = p[2] - s.cent[3 * c + 2];
+    const double d = d0 * d0 + d1 * d1 + d2 * d2;
+    if (d < bd) { bd = d; best = c; }
+  }
+  for (int k = 0; k < 3; k++) rv[k] = p[k] - s.cent[3 * best + k];
+  r = sqrt(bd);
+  return best;
+}
+
+// Local frame about the direction zaxis with the component of v perpendicular to it as xaxis:
+// returns that component's length (eps-regularised as the reference does).
+__host__ __device__ inline double slat_frame(const double *v, const double *zaxis, double vr, double *xaxis) {
+  const double eps = 1e-10;
+  double vp = 0;
+  for (int k = 0; k < 3; k++) {
+    xaxis[k] = v[k] - vr * zaxis[k];
+    vp += xaxis[k] * xaxis[k];
+  }
+  vp = sqrt(vp);
+  if (vp < eps) {
+    xaxis[0] = eps * (1 - zaxis[0] * zaxis[0]);
+    xaxis[1] = eps * (-zaxis[0] * zaxis[1]);
+    xaxis[2] = eps * (-zaxis[0] * zaxis[2]);
+    vp = eps * sqrt(1 - zaxis[0] * zaxis[0]);
+  }
+  for (int k = 0; k < 3; k++) xaxis[k] /= vp;
+  return vp;
+}
+
+// Forward half of an accelerated move of the electron at xo with drift vold: the new position
+// xn, and the forward transition factors fxop (the sampled densities relative to the current
+// point) and areao (their normalisations), the sampled radius rtry.
+template <class SysT>
+__host__ __device__ inline void slat_forward(const SysT &s, const Mover &m, const double *xo, const double *vold,
+                                             MoveRng &rng, double *xn, double &fxop, double &areao, double &rtry) {
+  double rv[3], r;
+  const int near = slat_nearest(s, xo, rv, r);
+  const double zn = s.zc[near], zcusp = s.nloc == 0 ? zn : 0.0;
+  const double deltri = 1 / m.deltar, rbot = r * deltri, rtop = r * m.deltar;
+  double zaxis[3], xaxis[3], yaxis[3];
+  for (int k = 0; k < 3; k++) zaxis[k] = rv[k] / r;
+  double vr = (vold[0] * rv[0] + vold[1] * rv[1] + vold[2] * rv[2]) / r;
+  double vp = slat_frame(vold, zaxis, vr, xaxis);
+  if (vr < -2 * zn) vr = -2 * zn;
+  yaxis[0] = zaxis[1] * xaxis[2] - zaxis[2] * xaxis[1];
+  yaxis[1] = zaxis[2] * xaxis[0] - zaxis[0] * xaxis[2];
+  yaxis[2] = zaxis[0] * xaxis[1] - zaxis[1] * xaxis[0];
+  vp *= m.fbias;
+  double zeta, co;
+  slat_shape(zcusp, vr, r, zeta, co);
+  // maximum of the radial density on [rbot, rtop] for the rejection sampling
+  const double root = sqrt((1.5 * co - zeta) * (1.5 * co - zeta) + 2 * zeta * co);
+  double rmax1 = co != 0 ? (1.5 * co - zeta + root) / (2 * zeta * co) : rtop;
+  rmax1 = rmax1 < rbot ? rbot : (rmax1 > rtop ? rtop : rmax1);
+  double fmx = sqrt(rmax1) * fabs(1 + co * rmax1) * exp(-zeta * rmax1);
+  if (co < 0) {
+    double rmax2 = (1.5 * co - zeta - root) / (2 * zeta * co);
+    rmax2 = rmax2 < rbot ? rbot : (rmax2 > rtop ? rtop : rmax2);
+    const double f2 = sqrt(rmax2) * fabs(1 + co * rmax2) * exp(-zeta * rmax2);
+    if (f2 > fmx) fmx = f2;
+  }
+  const double bot = sqrt(r) * fabs(1 + co * r) * exp(-zeta * r);
+  double top = 0;
+  for (int it = 0; it < 10000; it++) {  // bounded: the acceptance per try is far from zero
+    rtry = ((m.deltar - deltri) * rng.next() + deltri) * r;
+    top = sqrt(rtry) * fabs(1 + co * rtry) * exp(-zeta * rtry);
+    if (top / fmx > rng.next()) break;
+  }
+  fxop = top / bot;
+  areao = slat_area(zeta, co, rbot, rtop, bot);
+  const double raver = 0.5 * (r + rtry), deltt = slat_thetamx(m, raver, zn);
+  const double costht = 1 - deltt * rng.next(), zprime = rtry * costht, sintht = sqrt(1 - costht * costht);
+  areao *= deltt;
+  const double term = fmin(vp * raver * sintht, 1.0), fm = 1 + term;
+  double phitry = 0, topp = 1;
+  for (int it = 0; it < 10000; it++) {
+    phitry = 3.141592653589793 * rng.next();
+    topp = 1 + term * cos(phitry);
+    if (topp > rng.next() * fm) break;
+  }
+  fxop *= topp;
+  const double xprime = rtry * sintht * cos(phitry);
+  double yprime = sqrt(fmax(0.0, rtry * rtry - xprime * xprime - zprime * zprime));
+  if (rng.next() < 0.5) yprime = -yprime;
+  for (int k = 0; k < 3; k++) xn[k] = xaxis[k] * xprime + yaxis[k] * yprime + zaxis[k] * zprime + s.cent[3 * near + k];
+}
+
+// The reverse geometry of a move xo -> xn about the new point's nearest centre; false when the
+// reverse move could not be proposed (the move is rejected without evaluating psi).
+struct SlatBack {
+  int near;
+  double rminn, rminon, costht, sintht, ravern, delttn, rvn[3], rvo[3];
+};
+template <class SysT>
+__host__ __device__ inline bool slat_geometry(const SysT &s, const Mover &m, const double *xo, const double *xn,
+                                              SlatBack &b) {
+  b.near = slat_nearest(s, xn, b.rvn, b.rminn);
+  double r2 = 0, dot = 0;
+  for (int k = 0; k < 3; k++) {
+    b.rvo[k] = xo[k] - s.cent[3 * b.near + k];
+    r2 += b.rvo[k] * b.rvo[k];
+    dot += b.rvn[k] * b.rvo[k];
+  }
+  b.rminon = sqrt(r2);
+  dot /= b.rminn * b.rminon;
+  b.costht = dot;
+  b.sintht = sqrt(1 - dot * dot);
+  b.ravern = 0.5 * (b.rminn + b.rminon);
+  b.delttn = slat_thetamx(m, b.ravern, s.zc[b.near]);
+  return !(b.rminon > b.rminn * m.deltar || dot < 1 - b.delttn);
+}
+
+// Reverse transition factors fxnp, arean of the move back from xn (drift vnew there) to xo.
+template <class SysT>
+__host__ __device__ inline void slat_reverse(const SysT &s, const Mover &m, const SlatBack &b, const double *vnew,
+                                             double &fxnp, double &arean) {
+  const double zn = s.zc[b.near], zcusp = s.nloc == 0 ? zn : 0.0;
+  const double rbot = b.rminn / m.deltar, rtop = b.rminn * m.deltar;
+  double zaxis[3], xaxis[3];
+  for (int k = 0; k < 3; k++) zaxis[k] = b.rvn[k] / b.rminn;
+  double vr = (vnew[0] * b.rvn[0] + vnew[1] * b.rvn[1] + vnew[2] * b.rvn[2]) / b.rminn;
+  double vp = slat_frame(vnew, zaxis, vr, xaxis);
+  if (vr < -2 * zn) vr = -2 * zn;
+  vp *= m.fbias;
+  double zeta, co;
+  slat_shape(zcusp, vr, b.rminn, zeta, co);
+  const double bot = sqrt(b.rminn) * fabs(1 + co * b.rminn) * exp(-zeta * b.rminn);
+  const double top = sqrt(b.rminon) * fabs(1 + co * b.rminon) * exp(-zeta * b.rminon);
+  fxnp = top / bot;
+  arean = slat_area(zeta, co, rbot, rtop, bot) * b.delttn;
+  const double term = fmin(vp * b.ravern * b.sintht, 1.0);
+  double cosphi = 0, rnorm = 0;
+  for (int k = 0; k < 3; k++) {
+    const double t2 = b.rvo[k] / b.rminon - b.costht * b.rvn[k] / b.rminn;
+    rnorm += t2 * t2;
+    cosphi += t2 * xaxis[k];
+  }
+  cosphi /= sqrt(rnorm);
+  fxnp *= 1 + term * cosphi;
+}
+
 // Uniform random rotation (Shoemake's quaternion method) for (seed, walker, sweep).
 __device__ inline void random_rotation(uint64_t seed, uint32_t w, uint64_t sweep, double *R) {
   uint32_t o[4];

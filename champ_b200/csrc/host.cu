@@ -2046,6 +2046,17 @@ int champ_walker_status(champ_ctx *c, uint32_t *flags) {
   return tc_check(c);
 }
 
+int champ_set_mover(champ_ctx *c, int32_t imetro, double deltar, double deltat, double fbias) {
+  if (!c) return fail(CHAMP_EINVAL, "null context");
+  if (imetro != 1 && imetro != 6) return fail(CHAMP_EINVAL, "imetro must be 1 or 6 (accelerated Metropolis)");
+  // the reference's corrections of out-of-range values (control_mod.f90:375-385)
+  if (!(deltar >= 1.0)) deltar = 2.0;
+  if (!(deltat >= 0.0 && deltat <= 2.0)) deltat = 2.0;
+  fbias = std::min(2.0, std::max(0.0, fbias));
+  c->mover = Mover{imetro, deltar, deltat, fbias};
+  return CHAMP_OK;
+}
+
 int champ_set_option(champ_ctx *c, const char *name, int64_t value) {
   if (!c || !name) return fail(CHAMP_EINVAL, "null argument");
   if (!strcmp(name, "orbital_tc")) {

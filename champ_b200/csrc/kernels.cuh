@@ -1524,10 +1524,11 @@ __global__ void __launch_bounds__(128, 4) k_accept(Sys<T> s, State<T> st, Layout
 // (tensor-core contraction).  Phase 3 runs only the E_L, from the positions alone (re-inverting,
 // and refreshing the FP32 move tables when the state has them): the FP64 half of a mixed-precision
 // sweep whose moves ran in FP32.  Statistics are added to st.s_*.
-// (One kernel per phase, PH, so that each holds only the code it runs.)
-template <class T, int NORD, bool MD, int PH>
+// (One kernel per phase, PH, so that each holds only the code it runs; MV: the mover, 1 Gaussian
+// displacements, 6 the accelerated Metropolis method.)
+template <class T, int NORD, bool MD, int PH, int MV = 1>
 __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L, int nsweep, uint64_t seed,
-                                                uint64_t sweep0, double step, int reinv_every) {
+                                                uint64_t sweep0, double step, int reinv_every, Mover mv) {
   __shared__ JasPar<T> J;
   __shared__ EcpPar E;
   extern __shared__ __align__(16) char dsm[];
@@ -1553,6 +1554,31 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
     for (int isw = 0; isw < nsweep; isw++) {
       uint64_t sweep = sweep0 + (uint64_t)isw;
       for (int e = 0; moves && e < N; e++) {
+        if constexpr (MV == 6) {
+          // accelerated Metropolis (metrop_slat_mov1.f90:82-546): the drift at the current position,
+          // the spherical-polar proposal about the nearest nucleus, psi and the drift at the new
+          // position, both transition probabilities
+          const double xo[3] = {v.xs[3 * e], v.xs[3 * e + 1], v.xs[3 * e + 2]};
+          double r0, d0, go[3];
+          propose<T, NORD, MD, true>(s, J, st, w, v, e, xo, lane, r0, d0, go, &dl);
+          MoveRng rng{seed, (uint32_t)w, (uint32_t)sweep, (uint32_t)(sweep >> 32), (uint32_t)e, 0u, {0.0, 0.0}, 0};
+          double xn[3], fxop, areao, rtry;
+          slat_forward(s, mv, xo, go, rng, xn, fxop, areao, rtry);
+          SlatBack b;
+          double p = 0, rho = 0, dj = 0;
+          if (slat_geometry(s, mv, xo, xn, b)) {
+            double gn[3], fxnp, arean;
+            propose<T, NORD, MD, true>(s, J, st, w, v, e, xn, lane, rho, dj, gn, &dl);
+            slat_reverse(s, mv, b, gn, fxnp, arean);
+            const double rr = rtry / b.rminon;
+            p = rr * rr * rho * rho * exp(2.0 * dj) * fabs((fxnp * areao) / (fxop * arean));
+          }
+          if (rng.next() < p) {
+            accept_move<T, MD>(s, st, w, v, e, xn, dj, rho, lane, &dl);
+            acc += 1;
+          }
+          continue;
+        } else {
         double g[3], ua;
         move_randoms(seed, (uint32_t)w, sweep, (uint32_t)e, g, &ua);
         double xn[3] = {v.xs[3 * e] + step * g[0], v.xs[3 * e + 1] + step * g[1], v.xs[3 * e + 2] + step * g[2]};
@@ -1562,6 +1588,7 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
         if (ua < p) {
           accept_move<T, MD>(s, st, w, v, e, xn, dj, rho, lane, &dl);
           acc += 1;
+        }
         }
       }
       if (dl.buf) {  // the sweep's pending inverse updates, before anything else reads the inverse

@@ -23,6 +23,8 @@ static int set_smem_attrs(champ_ctx *c) {
   if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD, 1>, sm);
   if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD, 2>, sm);
   if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD, 3>, sm);
+  if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD, 0, 6>, sm);
+  if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD, 1, 6>, sm);
   if (!rc) rc = set_attrs(c, k_dmc_move<T, NORD, MD>, sm);
   if (!rc && std::is_same<T, float>::value && c->prec == CHAMP_PREC_FP32) {
     CK(cudaFuncSetAttribute(orbtc::k_orb_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024 + 128));
@@ -207,9 +209,11 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
       return run_el_staged<T, NORD, MD>(c, st, false, true, rot);
     }
     if (a.phase >= 0) {
-      auto kern = a.phase == 1 ? k_vmc<T, NORD, MD, 1> : a.phase == 2 ? k_vmc<T, NORD, MD, 2>
-                : a.phase == 3 ? k_vmc<T, NORD, MD, 3> : k_vmc<T, NORD, MD, 0>;
-      kern<<<grid, block, K.smem, c->stream>>>(s, st, K.lay, a.nsweep, a.seed, a.sweep0, a.step, c->reinv_every);
+      const bool acc6 = c->mover.kind == 6;
+      auto kern = a.phase == 1 ? (acc6 ? k_vmc<T, NORD, MD, 1, 6> : k_vmc<T, NORD, MD, 1>)
+                : a.phase == 2 ? k_vmc<T, NORD, MD, 2>
+                : a.phase == 3 ? k_vmc<T, NORD, MD, 3> : (acc6 ? k_vmc<T, NORD, MD, 0, 6> : k_vmc<T, NORD, MD, 0>);
+      kern<<<grid, block, K.smem, c->stream>>>(s, st, K.lay, a.nsweep, a.seed, a.sweep0, a.step, c->reinv_every, c->mover);
       break;
     }
     CK(cudaMemsetAsync(st.s_esum, 0, sizeof(double) * st.W, c->stream));
@@ -217,19 +221,21 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
     CK(cudaMemsetAsync(st.s_acc, 0, sizeof(double) * st.W, c->stream));
     const bool tc = c->tc_on && !a.st_override;  // only FP32 contexts turn it on
     if (!tc) {
-      k_vmc<T, NORD, MD, 0><<<grid, block, K.smem, c->stream>>>(s, st, K.lay, a.nsweep, a.seed, a.sweep0, a.step,
-                                                                  c->reinv_every);
+      auto kern = c->mover.kind == 6 ? k_vmc<T, NORD, MD, 0, 6> : k_vmc<T, NORD, MD, 0>;
+      kern<<<grid, block, K.smem, c->stream>>>(s, st, K.lay, a.nsweep, a.seed, a.sweep0, a.step, c->reinv_every,
+                                               c->mover);
       break;
     }
     // per sweep: moves, orbitals of all walkers on the tensor cores, E_L
     for (int isw = 0; isw < a.nsweep; isw++) {
-      k_vmc<T, NORD, MD, 1><<<grid, block, K.smem, c->stream>>>(s, st, K.lay, 1, a.seed, a.sweep0 + isw, a.step,
-                                                                  c->reinv_every);
+      auto kmv = c->mover.kind == 6 ? k_vmc<T, NORD, MD, 1, 6> : k_vmc<T, NORD, MD, 1>;
+      kmv<<<grid, block, K.smem, c->stream>>>(s, st, K.lay, 1, a.seed, a.sweep0 + isw, a.step, c->reinv_every,
+                                              c->mover);
       CK(cudaGetLastError());
       int rc = run_orb_tc<T>(c, st);
       if (rc) return rc;
       k_vmc<T, NORD, MD, 2><<<grid, block, K.smem, c->stream>>>(s, st, K.lay, 1, a.seed, a.sweep0 + isw, a.step,
-                                                                  c->reinv_every);
+                                                                  c->reinv_every, c->mover);
       CK(cudaGetLastError());
     }
     break;

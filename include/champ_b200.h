@@ -349,6 +349,20 @@ int champ_eval_energy_noalloc(champ_ctx *ctx, int32_t nw, const double *x, doubl
 /* Waits for the context's stream; also reports a tensor-core contraction that gave up. */
 int champ_synchronize(champ_ctx *ctx);
 
+/* The VMC mover of champ_vmc_sweeps and champ_vmc_run_host (imetro of the reference's control
+   menu, control_mod.f90:78-82 and 375-385, default there 6).  imetro 1: Gaussian displacements
+   of the step size those calls take (the engine's default).  imetro 6: the accelerated
+   Metropolis method of metrop_slat_mov1.f90:82-546 -- each electron moves in spherical
+   coordinates about its nearest nucleus, its new radius drawn between r/deltar and r*deltar from a
+   Slater-like distribution shaped by the radial drift (and by the nuclear cusp in all-electron
+   systems), its polar angle within a cone of 1 - cos(theta) up to deltat + (2 - deltat)/(1 +
+   (Z r)^2), its azimuth biased by the tangential drift times fbias, the forward and reverse
+   transition probabilities in the acceptance; the step size is then unused.  Out-of-range values
+   are corrected as the reference does (deltar < 1 -> 2, deltat outside [0, 2] -> 2, fbias clamped
+   to [0, 2]); the reference's defaults are deltar 5, deltat 1, fbias 1.  The random numbers come
+   from the same counter-based generator, keyed by (seed, walker, sweep, electron, draw). */
+int champ_set_mover(champ_ctx *ctx, int32_t imetro, double deltar, double deltat, double fbias);
+
 /* Engine options (no counterpart in the reference, which has one code path).
    "orbital_tc": 1 computes the orbitals of the full evaluation (value, gradient, Laplacian of
    every electron of every walker) as one tcgen05 tensor-core contraction per spin with a

@@ -1738,3 +1738,244 @@ int orc_vmc(const orc_sys *s, int nw, double *xall, int nsweep, uint64_t seed, u
   }
   return 0;
 }
+
+/* ------------------------------------------------------------------------------------ */
+/* Accelerated Metropolis VMC (imetro = 6, qmc/vmc/metrop_slat_mov1.f90:82-546; gammai.f90)   */
+/* ------------------------------------------------------------------------------------ */
+typedef struct { uint64_t seed; uint32_t w, s0, s1, e, ctr; double u[2]; int left; } mrng_t;
+static double mrng_next(mrng_t *r) {
+  if (r->left == 0) {
+    uint32_t o[4];
+    orc_philox(r->seed, r->w, r->s0, r->s1, 0x80000000u | (r->e << 15) | (r->ctr < 32767u ? r->ctr : 32767u), o);
+    r->ctr++;
+    r->u[0] = u53(o[0], o[1]);
+    r->u[1] = u53(o[2], o[3]);
+    r->left = 2;
+  }
+  return r->u[2 - r->left--];
+}
+
+/* gammai(a, x, xae, iflag) (gammai.f90:1-46): lower incomplete gamma by its series (x < a + 4,
+   iflag 1), minus the upper one by its continued fraction (iflag -1), times xae = x^a e^-x */
+static double gammai_ref(double a, double x, double xae, int *iflag) {
+  if (x < a + 4) {
+    *iflag = 1;
+    double ap = a, sum = 1 / a, del = sum;
+    int iter = (int)(21 + 3 * (x - a));
+    for (int n = 1; n <= iter; n++) { ap += 1; del *= x / ap; sum += del; }
+    return sum * xae;
+  }
+  *iflag = -1;
+  double a0 = 1, a1 = x, b0 = 0, b1 = 1, fac = 1, g = 0;
+  long na = lround(a - x);
+  int iter = (int)(20 + na > 7 ? 20 + na : 7);
+  for (int n = 1; n <= iter; n++) {
+    double an = n, ana = an - a;
+    a0 = (a1 + a0 * ana) * fac;
+    b0 = (b1 + b0 * ana) * fac;
+    double anf = an * fac;
+    a1 = x * a0 + anf * a1;
+    b1 = x * b0 + anf * b1;
+    fac = 1 / a1;
+    g = b1 * fac;
+  }
+  return -g * xae;
+}
+
+/* zeta and co of the radial density sqrt(r)|1 + co r| e^(-zeta r) (metrop_slat_mov1.f90:136-152) */
+static void slat_zeta(double zcusp, double vr, double r, double *zeta, double *co) {
+  const double eps = 1e-10;
+  double root = (zcusp + vr) * (zcusp + vr - 4 / r);
+  if (root >= 0) {
+    root = sqrt(root);
+    *zeta = 0.5 * (zcusp - vr - root);
+    if (*zeta <= 0) *zeta = 0.5 * (zcusp - vr + root);
+    if (*zeta <= 0) *zeta = eps;
+  } else {
+    *zeta = vr < 0 ? -vr - eps : 1.0;
+  }
+  *co = (*zeta + vr) / (1 - (*zeta + vr) * r);
+}
+
+/* normalisation of that density on [rbot, rtop] over its value bot (metrop_slat_mov1.f90:183-214) */
+static double slat_norm(double zeta, double co, double rbot, double rtop, double bot) {
+  const double g5b2 = 1.329340388179137, d2b3 = 0.666666666666667;
+  double rzero = -1 / co, zrbot = zeta * rbot, zrtop = zeta * rtop;
+  double zebot = sqrt(pow(zrbot, 3)) * exp(-zrbot), zetop = sqrt(pow(zrtop, 3)) * exp(-zrtop);
+  int ib, it, iz;
+  double g52bot = gammai_ref(2.5, zrbot, zrbot * zebot, &ib), g52top = gammai_ref(2.5, zrtop, zrtop * zetop, &it);
+  if (rzero < rbot || rzero > rtop) {
+    double g52dif = (ib * it == 1) ? g52top - g52bot : g52top - g52bot + g5b2;
+    double g32dif = d2b3 * (g52dif + zetop - zebot);
+    return fabs(g32dif + co * g52dif / zeta) / (bot * sqrt(pow(zeta, 3)));
+  }
+  double zrzer = zeta * rzero, zezer = sqrt(pow(zrzer, 3)) * exp(-zrzer);
+  double g52zer = gammai_ref(2.5, zrzer, zrzer * zezer, &iz);
+  double d1 = (ib * iz == 1) ? g52zer - g52bot : g52zer - g52bot + g5b2;
+  double c1 = d2b3 * (d1 + zezer - zebot);
+  double d2 = (it * iz == 1) ? g52top - g52zer : g52top - g52zer + g5b2;
+  double c2 = d2b3 * (d2 + zetop - zezer);
+  return (fabs(c1 + co * d1 / zeta) + fabs(c2 + co * d2 / zeta)) / (bot * sqrt(pow(zeta, 3)));
+}
+
+static int nearest_centre(const orc_sys *s, const double *p, double *rv, double *r) {
+  int best = 0;
+  double bd = 1e300;
+  for (int c = 0; c < s->C; c++) {
+    double d = 0;
+    for (int k = 0; k < 3; k++) d += (p[k] - s->cent[3 * c + k]) * (p[k] - s->cent[3 * c + k]);
+    if (d < bd) { bd = d; best = c; }
+  }
+  for (int k = 0; k < 3; k++) rv[k] = p[k] - s->cent[3 * best + k];
+  *r = sqrt(bd);
+  return best;
+}
+
+/* unit vector along the part of v perpendicular to the unit vector z; returns that part's length */
+static double perp_axis(const double *v, const double *z, double vr, double *x) {
+  const double eps = 1e-10;
+  double vp = 0;
+  for (int k = 0; k < 3; k++) { x[k] = v[k] - vr * z[k]; vp += x[k] * x[k]; }
+  vp = sqrt(vp);
+  if (vp < eps) {
+    x[0] = eps * (1 - z[0] * z[0]); x[1] = eps * (-z[0] * z[1]); x[2] = eps * (-z[0] * z[2]);
+    vp = eps * sqrt(1 - z[0] * z[0]);
+  }
+  for (int k = 0; k < 3; k++) x[k] /= vp;
+  return vp;
+}
+
+static double thetamx(double deltat, double r, double z) { return deltat + (2 - deltat) / (1 + (z * r) * (z * r)); }
+
+/* One accelerated Metropolis move of electron e (metrop_slat_mov1.f90:82-546); returns 1 if
+   accepted (x updated). */
+static int slat_move(const orc_sys *s, double *x, int e, uint64_t seed, uint32_t iw, uint64_t sweep,
+                     double deltar, double deltat, double fbias) {
+  mrng_t rng = {seed, iw, (uint32_t)sweep, (uint32_t)(sweep >> 32), (uint32_t)e, 0u, {0, 0}, 0};
+  double xo[3] = {x[3 * e], x[3 * e + 1], x[3 * e + 2]}, vold[3];
+  orc_ratio_1e(s, x, e, xo, vold);
+  double rv[3], r;
+  int near = nearest_centre(s, xo, rv, &r);
+  double zn = s->znuc[s->ctype[near]], zcusp = s->nloc == 0 ? zn : 0.0;
+  double deltri = 1 / deltar, rbot = r * deltri, rtop = r * deltar;
+  double z[3], xa[3], ya[3];
+  for (int k = 0; k < 3; k++) z[k] = rv[k] / r;
+  double vr = (vold[0] * rv[0] + vold[1] * rv[1] + vold[2] * rv[2]) / r;
+  double vp = perp_axis(vold, z, vr, xa);
+  if (vr < -2 * zn) vr = -2 * zn;
+  ya[0] = z[1] * xa[2] - z[2] * xa[1]; ya[1] = z[2] * xa[0] - z[0] * xa[2]; ya[2] = z[0] * xa[1] - z[1] * xa[0];
+  vp *= fbias;
+  double zeta, co;
+  slat_zeta(zcusp, vr, r, &zeta, &co);
+  double root = sqrt((1.5 * co - zeta) * (1.5 * co - zeta) + 2 * zeta * co);
+  double rmax1 = co != 0 ? (1.5 * co - zeta + root) / (2 * zeta * co) : rtop;
+  if (rmax1 < rbot) rmax1 = rbot;
+  if (rmax1 > rtop) rmax1 = rtop;
+  double fmx = sqrt(rmax1) * fabs(1 + co * rmax1) * exp(-zeta * rmax1);
+  if (co < 0) {
+    double rmax2 = (1.5 * co - zeta - root) / (2 * zeta * co);
+    if (rmax2 < rbot) rmax2 = rbot;
+    if (rmax2 > rtop) rmax2 = rtop;
+    double f2 = sqrt(rmax2) * fabs(1 + co * rmax2) * exp(-zeta * rmax2);
+    if (f2 > fmx) fmx = f2;
+  }
+  double bot = sqrt(r) * fabs(1 + co * r) * exp(-zeta * r), rtry = r, top = bot;
+  for (int it = 0; it < 10000; it++) {
+    rtry = ((deltar - deltri) * mrng_next(&rng) + deltri) * r;
+    top = sqrt(rtry) * fabs(1 + co * rtry) * exp(-zeta * rtry);
+    if (top / fmx > mrng_next(&rng)) break;
+  }
+  double fxop = top / bot, areao = slat_norm(zeta, co, rbot, rtop, bot);
+  double raver = 0.5 * (r + rtry), deltt = thetamx(deltat, raver, zn);
+  double costht = 1 - deltt * mrng_next(&rng), zprime = rtry * costht, sintht = sqrt(1 - costht * costht);
+  areao *= deltt;
+  double term = fmin(vp * raver * sintht, 1.0), fm = 1 + term, phitry = 0, tp = 1;
+  for (int it = 0; it < 10000; it++) {
+    phitry = 3.141592653589793 * mrng_next(&rng);
+    tp = 1 + term * cos(phitry);
+    if (tp > mrng_next(&rng) * fm) break;
+  }
+  fxop *= tp;
+  double xprime = rtry * sintht * cos(phitry);
+  double yprime = sqrt(fmax(0.0, rtry * rtry - xprime * xprime - zprime * zprime));
+  if (mrng_next(&rng) < 0.5) yprime = -yprime;
+  double xn[3];
+  for (int k = 0; k < 3; k++) xn[k] = xa[k] * xprime + ya[k] * yprime + z[k] * zprime + s->cent[3 * near + k];
+  /* the reverse move about the new point's nearest nucleus (metrop_slat_mov1.f90:216-250) */
+  double rvn[3], rn;
+  int nn = nearest_centre(s, xn, rvn, &rn);
+  double rvo[3], ro = 0, dot = 0;
+  for (int k = 0; k < 3; k++) { rvo[k] = xo[k] - s->cent[3 * nn + k]; ro += rvo[k] * rvo[k]; dot += rvn[k] * rvo[k]; }
+  ro = sqrt(ro);
+  dot /= rn * ro;
+  double costn = dot, sintn = sqrt(1 - dot * dot), ravern = 0.5 * (rn + ro);
+  double zn2 = s->znuc[s->ctype[nn]], delttn = thetamx(deltat, ravern, zn2);
+  double p = 0;
+  if (!(ro > rn * deltar || dot < 1 - delttn)) {
+    double vnew[3];
+    double ratio = orc_ratio_1e(s, x, e, xn, vnew);
+    double zc2 = s->nloc == 0 ? zn2 : 0.0, rb2 = rn / deltar, rt2 = rn * deltar, zz[3], xb[3];
+    for (int k = 0; k < 3; k++) zz[k] = rvn[k] / rn;
+    double vnr = (vnew[0] * rvn[0] + vnew[1] * rvn[1] + vnew[2] * rvn[2]) / rn;
+    double vnp = perp_axis(vnew, zz, vnr, xb);
+    if (vnr < -2 * zn2) vnr = -2 * zn2;
+    vnp *= fbias;
+    double z2, c2;
+    slat_zeta(zc2, vnr, rn, &z2, &c2);
+    double bot2 = sqrt(rn) * fabs(1 + c2 * rn) * exp(-z2 * rn);
+    double top2 = sqrt(ro) * fabs(1 + c2 * ro) * exp(-z2 * ro);
+    double fxnp = top2 / bot2, arean = slat_norm(z2, c2, rb2, rt2, bot2) * delttn;
+    double t2 = fmin(vnp * ravern * sintn, 1.0), cosphi = 0, rnorm = 0;
+    for (int k = 0; k < 3; k++) {
+      double q = rvo[k] / ro - costn * rvn[k] / rn;
+      rnorm += q * q;
+      cosphi += q * xb[k];
+    }
+    cosphi /= sqrt(rnorm);
+    fxnp *= 1 + t2 * cosphi;
+    double rr = rtry / ro;
+    p = rr * rr * ratio * ratio * fabs((fxnp * areao) / (fxop * arean));
+  }
+  if (mrng_next(&rng) < p) {
+    for (int k = 0; k < 3; k++) x[3 * e + k] = xn[k];
+    return 1;
+  }
+  return 0;
+}
+
+/* VMC with the accelerated Metropolis mover: nsweep sweeps of moves of every electron, E_L after
+   each sweep with the quadrature rotated per sweep, as orc_vmc. */
+int orc_vmc_accel(const orc_sys *s, int nw, double *xall, int nsweep, uint64_t seed, uint64_t sweep0, double deltar,
+                  double deltat, double fbias, double *esum, double *e2sum, double *accept, double *elast,
+                  int nthreads) {
+  int N = s->N;
+  if (deltar < 1) deltar = 2;
+  if (deltat < 0 || deltat > 2) deltat = 2;
+  fbias = fmin(2.0, fmax(0.0, fbias));
+#ifdef _OPENMP
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+#endif
+  for (int iw = 0; iw < nw; iw++) {
+    orc_sys sl = *s;
+    double *x = xall + (size_t)iw * 3 * N;
+    double es = 0, e2 = 0, acc = 0, el = 0;
+    for (int isw = 0; isw < nsweep; isw++) {
+      uint64_t sweep = sweep0 + (uint64_t)isw;
+      for (int e = 0; e < N; e++) acc += slat_move(&sl, x, e, seed, (uint32_t)iw, sweep, deltar, deltat, fbias);
+      double R[9];
+      orc_random_rotation(seed, (uint32_t)iw, sweep, R);
+      orc_set_rotation(&sl, R);
+      orc_eval ev;
+      memset(&ev, 0, sizeof ev);
+      orc_eval_full(&sl, x, &ev);
+      el = ev.energy;
+      es += el; e2 += el * el;
+    }
+    if (esum) esum[iw] = es;
+    if (e2sum) e2sum[iw] = e2;
+    if (accept) accept[iw] = acc;
+    if (elast) elast[iw] = el;
+  }
+  return 0;
+}

@@ -57,6 +57,9 @@ def lib():
         L.orc_jastrow_param_grad.argtypes = [vp, dp, dp, dp]
         L.orc_jastrow_pderiv.restype = ip
         L.orc_jastrow_pderiv.argtypes = [vp, dp, dp, dp, dp]
+        L.orc_vmc_accel.restype = ip
+        L.orc_vmc_accel.argtypes = [vp, ip, dp, ip, C.c_uint64, C.c_uint64, C.c_double, C.c_double, C.c_double,
+                                    dp, dp, dp, dp, ip]
         L.orc_vmc.restype = ip
         L.orc_vmc.argtypes = [vp, ip, dp, ip, C.c_uint64, C.c_uint64, C.c_double, dp, dp, dp, dp, ip]
         _lib = L
@@ -162,6 +165,15 @@ class Oracle:
         nw = x.shape[0]
         es, e2, acc, el = (np.zeros(nw) for _ in range(4))
         lib().orc_vmc(self.h, nw, _p(x), nsweep, seed, sweep0, step, _p(es), _p(e2), _p(acc), _p(el), nthreads)
+        return dict(x=x, esum=es, e2sum=e2, accept=acc, elast=el)
+
+    def vmc_accel(self, x, nsweep, seed, sweep0=0, deltar=5.0, deltat=1.0, fbias=1.0, nthreads=0):
+        """VMC with the accelerated Metropolis mover (imetro = 6)."""
+        x = np.ascontiguousarray(x, float).copy()
+        nw = x.shape[0]
+        es, e2, acc, el = (np.zeros(nw) for _ in range(4))
+        lib().orc_vmc_accel(self.h, nw, _p(x), nsweep, seed, sweep0, deltar, deltat, fbias, _p(es), _p(e2), _p(acc),
+                            _p(el), nthreads)
         return dict(x=x, esum=es, e2sum=e2, accept=acc, elast=el)
 
 
