@@ -264,10 +264,13 @@ def time_param_grad(eng, system, nsteps, flush, torch):
     return tpg
 
 
-def vmc_arm(system, nw, prec, steps, warmup, flush, torch, rank, world, x0=None, pg_steps=0, clocks=False):
+def vmc_arm(system, nw, prec, steps, warmup, flush, torch, rank, world, x0=None, pg_steps=0, clocks=False,
+            mover=1):
     from champ_b200.engine import Engine
     eng = Engine(system, nw, prec)
     eng.set_walkers(x0 if x0 is not None else system_walkers(system, nw, seed=1000 + rank))
+    if mover != 1:
+        eng.set_mover(mover)
     if x0 is None:
         eng.vmc_sweeps(10, SEED + rank, sweep0=0, step=step_size(system), stats=False)  # equilibration
     # launch options that change only the speed (champ_autotune), chosen before the timed region
@@ -442,6 +445,11 @@ def main():
                             pg_steps=max(2, pg_steps // 2) if p2 == "fp64" else 0)
             e2.close()
             arms[p2] = a
+        # the reference's default mover (accelerated Metropolis, imetro 6): drift before and after
+        # each proposal, so more work per move than the Gaussian steps of the headline
+        a6, e6 = vmc_arm(system, nw, prec, max(3, args.steps // 2), 2, flush, torch, rank, world, x0=xw, mover=6)
+        e6.close()
+        arms[f"{prec}_imetro6"] = {k: a6[k] for k in ("value", "unit", "ms_per_step", "kernels_ms_per_step")}
         if prec == "mixed":
             arms["mixed_over_fp64"] = {"e-moves/s": head["value"] / arms["fp64"]["value"],
                                        "param-grad samples/s": head["param_grad"]["value"] /
