@@ -126,6 +126,7 @@ struct champ_ctx {
   int dmc_step = 0;
   // CUDA graph of two DMC steps (A->B->A buffers), captured on a private stream, replayed per pair
   int dmc_graph_on = 1;
+  int dmc_ene_int = 1;  // DMC energy integration over the step: 1 ene_int_v9, 0 none (option "dmc_ene_int")
   void *dmc_graph = nullptr, *dmc_exec = nullptr;  // cudaGraph_t, cudaGraphExec_t
   uint64_t dmc_graph_seed = 0;
   cudaStream_t cap_stream = nullptr;
@@ -175,7 +176,7 @@ inline KCfg &kcfg<double>(champ_ctx *c) { return c->kd; }
 template <>
 inline KCfg &kcfg<float>(champ_ctx *c) { return c->kf; }
 
-enum class Op { Eval, EvalOut, Propose, ProposeGrad, Accept, Vmc, PGrad, PGradBwd, DmcMove, DmcCopy };
+enum class Op { Eval, EvalOut, Propose, ProposeGrad, Accept, Vmc, PGrad, PGradBwd, DmcMove, DmcCopy, Tmove };
 struct OpArgs {
   int e = 0;
   const double *xnew = nullptr;
@@ -189,6 +190,12 @@ struct OpArgs {
   const void *st_override = nullptr;  // State<T> to use instead of the context's (and its walker count)
   int nw_override = 0;
   int phase = -1;  // Vmc: one k_vmc launch of this phase (no statistics reset); DmcMove: k_dmc_move phase
+  // Tmove: time step, variant (1 casula1, 2 det_balance1), per-walker counts of accepted T-moves
+  // (device, may be null), and whether the walker count and step number come from the DMC state
+  double tau = 0;
+  int variant = 0;
+  int *moved = nullptr;
+  bool dmc = false;
 };
 
 

@@ -4,7 +4,12 @@
 // proposal x' = x + tau vbar(x) + sqrt(tau) chi with the averaged drift of
 // averaged_1e_velocity (green_functions_mod.f90:598-633, n_drift_param = 2), accepted with
 // min(1, |psi'/psi|^2 G(x<-x')/G(x'<-x)) (sample_1e_prob), node crossings rejected; then the
-// full E_L, and the weight is multiplied by exp(-tau ((E_L,old + E_L,new)/2 - E_T)).
+// full E_L, and the weight is multiplied by exp(-tau_eff (E_int - E_T)), with the energy integrated
+// over the step as ene_int_rewt does for the default ene_int_v9 (green_functions_mod.f90:382-472):
+// each end's E_L - E_est is damped by (sqrt(pi)/2) erf(f)/f, f = |grad ln psi| / sqrt(N) tau_eff c_rewt,
+// which removes the locality approximation's negative spikes near the nodes; E_int is floored at
+// E_est - limit_rewt_dmc sigma_E / tau^(1/4); tau_eff = tau sum_i p_i chi_i^2 / sum_i chi_i^2 over
+// the electrons' acceptance probabilities and diffusion steps (itau_eff = 1, rundmc_mod.f90:203-210).
 // Branching (split_join, dmc/dmc_elec/split_join_mod.f90): each walker is copied
 // floor(w + u) times with weight 1 into a second state buffer (exclusive scan for the
 // destinations); the trial energy follows the population: E_T = E_est - ln(W/W_target)/(g tau).
@@ -12,14 +17,20 @@
 #pragma once
 
 struct DmcPar {
-  double tau, adrift, gpop, ecut;
+  double tau, adrift, gpop;
+  double rewt_limit, c_rewt;  // limit_rewt_dmc, c_rewt (control_mod.f90:16)
+  int ene_int;                // 1: ene_int_v9 (the reference's default), 0: no_ene_int
   int wtarget, wmax;
   uint64_t seed;
+  int tmove;  // T-moves before each step's drift-diffusion moves: 0 off, 1 casula1, 2 det_balance1
 };
 
 // per-walker DMC data (weights, E_L at the last step) and device scalars
 struct DmcData {
   double *wt, *el;        // [wmax]
+  double *v2;             // [wmax] |grad ln psi|^2 at the last step
+  double *teff;           // [wmax] the step's effective time step (written by the moves)
+  double *esg;            // [4] (device) generations, sum sw, sum sw E, sum sw E^2 since the start
   int *nw;                // current population (device)
   double *et;             // trial energy (device)
   double *eest;           // running estimate of the energy (device)
@@ -37,6 +48,36 @@ __device__ __forceinline__ void avg_drift(const double *g, double tau, double a,
   vb[0] = f * g[0]; vb[1] = f * g[1]; vb[2] = f * g[2];
 }
 
+// sigma of E_L for the reweighting floor (rundmc_mod.f90:238-244): 0.2 sqrt(N) for the first
+// max(10, 10/tau) generations, then sqrt(W_target) times the weighted standard deviation of the
+// generations' mixed estimators (stats_sigma, stats_type_mod.f90:270-280)
+__device__ inline double energy_sigma(const DmcPar &P, const double *esg, int N) {
+  const double ngen = esg[0], nmin = fmax(10.0, rint(10.0 / P.tau));
+  if (ngen <= nmin || esg[1] <= 0) return 0.2 * sqrt((double)N);
+  const double avg = esg[2] / esg[1], var = esg[3] / esg[1] - avg * avg;
+  return sqrt((double)P.wtarget) * sqrt(var > 0 ? var : 0.0);
+}
+
+// E_int - E_T of one walker's step (ene_int_rewt, green_functions_mod.f90:382-472): the old and new
+// local energies, each damped towards E_est by (sqrt(pi)/2) erf(f)/f with
+// f = max(|grad ln psi| / N^pow_rewt tau_int c_rewt, 1e-9), pow_rewt = 1/2, tau_int = tau_eff
+// (itau_integ = 1); their mean minus E_T, floored at E_est - E_T - limit_rewt_dmc sigma / tau^(1/4).
+__device__ inline double integrated_energy(const DmcPar &P, double eo, double v2o, double en, double v2n, int N,
+                                           double eest, double et, double esigma, double tauint) {
+  double ewo = eo, ewn = en;
+  if (P.ene_int == 1) {
+    const double spi = 0.886226925452758;  // sqrt(pi) / 2
+    const double rn = 1.0 / sqrt((double)N);
+    const double fo = fmax(sqrt(v2o) * rn * tauint * P.c_rewt, 1e-9);
+    const double fn = fmax(sqrt(v2n) * rn * tauint * P.c_rewt, 1e-9);
+    ewo = eest + (eo - eest) * spi * erf(fo) / fo;
+    ewn = eest + (en - eest) * spi * erf(fn) / fn;
+  }
+  const double eint = 0.5 * (ewo + ewn) - et;
+  const double emin = eest - et - P.rewt_limit * esigma / sqrt(sqrt(P.tau));
+  return eint < emin ? emin : eint;
+}
+
 // phase 0: moves, E_L and reweighting in one pass; 1: the moves only; 2: E_L (from the positions,
 // re-inverting, refreshing the FP32 move tables when the state has them) and reweighting only --
 // the FP32 and FP64 halves of a mixed-precision step.
@@ -48,7 +89,8 @@ __global__ void __launch_bounds__(128, 4) k_dmc_move(Sys<T> s, State<T> st, Layo
   load_params(s, J, E);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   const int N = s.N, W = *D.nw;
-  const double et = *D.et, sqt = sqrt(P.tau);
+  const double et = *D.et, eest = *D.eest, sqt = sqrt(P.tau);
+  const double esigma = energy_sigma(P, D.esg, N);
   const uint64_t step = (uint64_t)D.ctr[0];
   for (int w = blockIdx.x * wpb + wib; w < W; w += gridDim.x * wpb) {
     View<T> v = make_view<T>(dsm + L.bytes * wib, L, st, w, s.N, s.C, s.nbasis, s.nomax, L.resident != 0);
@@ -59,6 +101,7 @@ __global__ void __launch_bounds__(128, 4) k_dmc_move(Sys<T> s, State<T> st, Layo
       __syncwarp();
     }
     int acc = 0;
+    double sdd = 0, spd = 0;  // sum_i chi_i^2 tau and sum_i p_i chi_i^2 tau over the electrons
     for (int e = 0; e < N && phase != 2; e++) {
       double xo[3] = {v.xs[3 * e], v.xs[3 * e + 1], v.xs[3 * e + 2]};
       double r0, d0, go[3], gn[3], vo[3], vn[3];
@@ -75,10 +118,20 @@ __global__ void __launch_bounds__(128, 4) k_dmc_move(Sys<T> s, State<T> st, Layo
       double db[3] = {xo[0] - xn[0] - P.tau * vn[0], xo[1] - xn[1] - P.tau * vn[1], xo[2] - xn[2] - P.tau * vn[2]};
       double lgb = -(db[0] * db[0] + db[1] * db[1] + db[2] * db[2]) / (2 * P.tau);
       double p = (rho > 0) ? rho * rho * exp(2.0 * dj + lgb - lgf) : 0.0;  // fixed node
+      const double dd = P.tau * (g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+      sdd += dd;
+      spd += (p < 1.0 ? p : 1.0) * dd;
       if (ua < p) {
         accept_move<T, MD>(s, st, w, v, e, xn, dj, rho, lane);
         acc++;
       }
+    }
+    double teff = P.tau;
+    if (phase != 2) {
+      teff = sdd > 0 ? P.tau * spd / sdd : P.tau;
+      if (phase == 1 && lane == 0) D.teff[w] = teff;
+    } else {
+      teff = D.teff[w];
     }
     if (phase == 1) {
       if (L.resident) view_store(v, st, w, N, s.C, lane);
@@ -101,14 +154,148 @@ __global__ void __launch_bounds__(128, 4) k_dmc_move(Sys<T> s, State<T> st, Layo
       __syncwarp();
     }
     if (lane == 0) {
-      double eo = D.el[w], en = res.eloc;
-      double de = 0.5 * (eo + en) - et;
-      de = de > P.ecut ? P.ecut : (de < -P.ecut ? -P.ecut : de);  // reweighting cut-off
-      double wn = D.wt[w] * exp(-P.tau * de);
+      const double eo = D.el[w], en = res.eloc;
+      const double eint = integrated_energy(P, eo, D.v2[w], en, res.v2, N, eest, et, esigma, teff);
+      double wn = D.wt[w] * exp(-eint * teff);
       if (!isfinite(wn) || !isfinite(en)) wn = 0.0;  // a walker with a non-finite energy dies
       D.wt[w] = wn;
       D.el[w] = en;
+      D.v2[w] = res.v2;
     }
+    __syncwarp();
+  }
+}
+
+// Uniform random rotation (Shoemake's quaternion method) from three draws of a move's stream.
+__device__ inline void rotation_from(MoveRng &rng, double *R) {
+  const double u1 = rng.next(), u2 = rng.next(), u3 = rng.next();
+  const double tp = 6.283185307179586, s1 = sqrt(1.0 - u1), s2 = sqrt(u1);
+  double sa, ca, sb, cb;
+  sincos(tp * u2, &sa, &ca);
+  sincos(tp * u3, &sb, &cb);
+  const double qx = s1 * sa, qy = s1 * ca, qz = s2 * sb, qw = s2 * cb;
+  R[0] = 1 - 2 * (qy * qy + qz * qz); R[1] = 2 * (qx * qy - qz * qw); R[2] = 2 * (qx * qz + qy * qw);
+  R[3] = 2 * (qx * qy + qz * qw); R[4] = 1 - 2 * (qx * qx + qz * qz); R[5] = 2 * (qy * qz - qx * qw);
+  R[6] = 2 * (qx * qz - qy * qw); R[7] = 2 * (qy * qz + qx * qw); R[8] = 1 - 2 * (qx * qx + qy * qy);
+}
+
+// T-move of electron e (tmove.f90:1-192, Casula's size-consistent T-moves): the nonlocal
+// pseudopotential's off-diagonal elements to the quadrature points of every centre in range,
+// T(q) = sum_{l nonlocal} w_q (exp(-tau v_l(r)) - 1) P_l(cos theta) psi(x_q)/psi(x), sampled by heat
+// bath against weight 1 for staying (positive T only); with det_balance1 (variant 2) the move is
+// then accepted with min(1, sum_forward / sum_backward), the backward sum over the chosen centre's
+// points about the new position (fresh rotation).  The point grid is rotated at random per
+// (walker, step, electron); the draws come from that move's own stream.  Returns whether the
+// electron moved (its state updated as by an accepted single-electron move).
+template <class T, int NORD, bool MD>
+__device__ bool tmove_electron(const Sys<T> &s, const JasPar<T> &J, const EcpPar &E, const State<T> &st, int w,
+                               const View<T> &v, int e, double tau, int variant, uint64_t seed, uint64_t step,
+                               int lane) {
+  MoveRng rng{seed, (uint32_t)w, (uint32_t)step, (uint32_t)(step >> 32), 256u + (uint32_t)e, 0u, {0.0, 0.0}, 0};
+  double R[9];
+  rotation_from(rng, R);
+  const double xo[3] = {v.xs[3 * e], v.xs[3 * e + 1], v.xs[3 * e + 2]};
+  double S = 1.0, pratio = 0.0;
+  int pc = -1, pq = -1;
+  for (int c = 0; c < s.C; c++) {
+    const double *cc = s.cent + 3 * c;
+    const double rv[3] = {xo[0] - cc[0], xo[1] - cc[1], xo[2] - cc[2]};
+    const double r = sqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
+    const int it = s.ctype[c];
+    double vps[MAXLCH];
+    ecp_vps(E, it, r, vps);
+    bool skip = true;
+    for (int l = 0; l < E.npotd[it]; l++)
+      if (l + 1 != E.lpotp1[it] && fabs(vps[l]) > 1e-4) skip = false;
+    if (skip) continue;
+    for (int q = 0; q < E.nquad; q++) {
+      double qv[3];
+      for (int k = 0; k < 3; k++)
+        qv[k] = R[3 * k] * s.quad->q0[q][0] + R[3 * k + 1] * s.quad->q0[q][1] + R[3 * k + 2] * s.quad->q0[q][2];
+      const double costh = (rv[0] * qv[0] + rv[1] * qv[1] + rv[2] * qv[2]) / r;
+      const double xq[3] = {cc[0] + r * qv[0], cc[1] + r * qv[1], cc[2] + r * qv[2]};
+      double rho, dj, g[3];
+      propose<T, NORD, MD, false>(s, J, st, w, v, e, xq, lane, rho, dj, g);
+      const double ratio = rho * exp(dj);
+      double gp = 0;
+      for (int l = 0; l < E.npotd[it]; l++)
+        if (l + 1 != E.lpotp1[it]) gp += s.quad->wq[q] * (exp(-tau * vps[l]) - 1) * yl0(l, costh) * ratio;
+      if (gp > 0) {
+        S += gp;
+        if (rng.next() < gp / S) { pc = c; pq = q; pratio = ratio; }
+      }
+    }
+  }
+  if (pc < 0) return false;
+  const double *cc = s.cent + 3 * pc;
+  const double r = sqrt((xo[0] - cc[0]) * (xo[0] - cc[0]) + (xo[1] - cc[1]) * (xo[1] - cc[1]) +
+                        (xo[2] - cc[2]) * (xo[2] - cc[2]));
+  double xn[3];
+  for (int k = 0; k < 3; k++)
+    xn[k] = cc[k] + r * (R[3 * k] * s.quad->q0[pq][0] + R[3 * k + 1] * s.quad->q0[pq][1] +
+                         R[3 * k + 2] * s.quad->q0[pq][2]);
+  double p = 1.0;
+  if (variant == 2) {
+    const int it = s.ctype[pc];
+    double vps[MAXLCH];
+    ecp_vps(E, it, r, vps);
+    double R2[9];
+    rotation_from(rng, R2);
+    const double xe[3] = {xn[0] - cc[0], xn[1] - cc[1], xn[2] - cc[2]};
+    double Sb = 1.0;
+    for (int q = 0; q < E.nquad; q++) {
+      double qv[3];
+      for (int k = 0; k < 3; k++)
+        qv[k] = R2[3 * k] * s.quad->q0[q][0] + R2[3 * k + 1] * s.quad->q0[q][1] + R2[3 * k + 2] * s.quad->q0[q][2];
+      const double costh = (xe[0] * qv[0] + xe[1] * qv[1] + xe[2] * qv[2]) / r;
+      const double xq[3] = {cc[0] + r * qv[0], cc[1] + r * qv[1], cc[2] + r * qv[2]};
+      double rho, dj, g[3];
+      propose<T, NORD, MD, false>(s, J, st, w, v, e, xq, lane, rho, dj, g);
+      const double ratio = rho * exp(dj) / pratio;
+      double gp = 0;
+      for (int l = 0; l < E.npotd[it]; l++)
+        if (l + 1 != E.lpotp1[it]) gp += s.quad->wq[q] * (exp(-tau * vps[l]) - 1) * yl0(l, costh) * ratio;
+      if (gp > 0) Sb += gp;
+    }
+    p = S / Sb < 1.0 ? S / Sb : 1.0;
+  }
+  if (rng.next() >= p) return false;
+  double rho, dj, g[3];
+  propose<T, NORD, MD, false>(s, J, st, w, v, e, xn, lane, rho, dj, g);
+  accept_move<T, MD>(s, st, w, v, e, xn, dj, rho, lane);
+  return true;
+}
+
+// T-moves of every electron of walkers [0, W) (W from *nw when not null): the first part of a DMC
+// step with T-moves (rundmc_mod.f90:137, do_tmoves), or on its own (champ_tmoves).  moved (may be
+// null) receives the accepted T-moves per walker.
+template <class T, int NORD, bool MD>
+__global__ void __launch_bounds__(128, 4) k_dmc_tmove(Sys<T> s, State<T> st, Layout L, int W_host, const int *nw,
+                                                      double tau, int variant, uint64_t seed, const long long *step_dev,
+                                                      uint64_t step_host, int *moved) {
+  __shared__ JasPar<T> J;
+  __shared__ EcpPar E;
+  extern __shared__ __align__(16) char dsm[];
+  load_params(s, J, E);
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  const int N = s.N, W = nw ? *nw : W_host;
+  const uint64_t step = step_dev ? (uint64_t)step_dev[0] : step_host;
+  for (int w = blockIdx.x * wpb + wib; w < W; w += gridDim.x * wpb) {
+    View<T> v = make_view<T>(dsm + L.bytes * wib, L, st, w, s.N, s.C, s.nbasis, s.nomax, L.resident != 0);
+    if (L.resident) {
+      view_load(v, st, w, N, s.C, lane);
+    } else {
+      for (int i = lane; i < 3 * N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * N + i];
+      __syncwarp();
+    }
+    int nmv = 0;
+    for (int e = 0; e < N; e++) nmv += tmove_electron<T, NORD, MD>(s, J, E, st, w, v, e, tau, variant, seed, step, lane);
+    if (L.resident) view_store(v, st, w, N, s.C, lane);
+    else {
+      for (int i = lane; i < 3 * N; i += 32) st.x[(size_t)w * 3 * N + i] = v.xs[i];
+      __syncwarp();
+    }
+    if (moved && lane == 0) moved[w] = nmv;
     __syncwarp();
   }
 }
@@ -172,6 +359,7 @@ __global__ void k_dmc_copy(State<T> a, State<T> b, DmcData Da, DmcData Db, int N
         b.sgn[d] = a.sgn[w];
         Db.wt[d] = 1.0;
         Db.el[d] = Da.el[w];
+        Db.v2[d] = Da.v2[w];
       }
     }
   }
@@ -195,6 +383,12 @@ static __global__ void k_dmc_finish(DmcData Da, DmcData Db, DmcPar P) {
   *Db.et = et;
   *Da.eest = eest;
   *Da.et = et;
+  if (sw > 0) {  // the generation's mixed estimator, for sigma_E (stats_accuest)
+    Da.esg[0] += 1.0;
+    Da.esg[1] += sw;
+    Da.esg[2] += swe;
+    Da.esg[3] += sw * emix * emix;
+  }
   double *st = Da.stat + 4 * (size_t)istat;
   st[0] = (double)W;
   st[1] = sw;

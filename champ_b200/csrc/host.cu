@@ -863,6 +863,7 @@ static int launch(champ_ctx *c, Op op, const OpArgs &a = OpArgs()) {
   case Op::Propose:
   case Op::ProposeGrad:
   case Op::Accept:
+  case Op::Tmove:  // T-moves, like the other moves, on the FP32 tables
   case Op::DmcCopy:
   case Op::PGradBwd:  // the parameter derivatives' reverse sweep in FP32 (E_L stays FP64)
     return launch_f32(c, op, a);
@@ -1185,7 +1186,17 @@ static int tc_setup(champ_ctx *c) {
 // their prefix sum, the branching copy into the other state buffer, population and E_T update;
 // then the buffers swap roles.  Reads its step number from the device counter.
 static int dmc_one_step(champ_ctx *c) {
-  int rc = launch(c, Op::DmcMove);
+  int rc;
+  if (c->dpar.tmove && c->nloc > 0) {  // T-moves first (rundmc_mod.f90:137)
+    OpArgs t;
+    t.tau = c->dpar.tau;
+    t.variant = c->dpar.tmove;
+    t.seed = c->dpar.seed;
+    t.dmc = true;
+    rc = launch(c, Op::Tmove, t);
+    if (rc) return rc;
+  }
+  rc = launch(c, Op::DmcMove);
   if (rc) return rc;
   k_dmc_sums<<<148, 256, 0, c->stream>>>(c->dA, c->dpar.wmax);
   k_dmc_count<<<(c->dpar.wmax + 255) / 256, 256, 0, c->stream>>>(c->dA, c->dpar);
@@ -1815,18 +1826,22 @@ int champ_dmc_init(champ_ctx *c, int32_t w_target, double tau, double gpop) {
     if (rc) return rc;
     size_t W = c->wmax;
     int *nw = dalloc<int>(c, 1);
-    double *sc = dalloc<double>(c, 4);
+    double *sc = dalloc<double>(c, 8);
     int *nc = dalloc<int>(c, W), *off = dalloc<int>(c, W);
     double *stat = dalloc<double>(c, 4 * (size_t)DMC_STAT_CAP);
     double *w0 = dalloc<double>(c, W), *w1 = dalloc<double>(c, W), *e0 = dalloc<double>(c, W), *e1 = dalloc<double>(c, W);
+    double *v0 = dalloc<double>(c, W), *v1 = dalloc<double>(c, W), *te = dalloc<double>(c, W);
     long long *ctr = dalloc<long long>(c, 2);
-    if (!nw || !sc || !nc || !off || !stat || !w0 || !w1 || !e0 || !e1 || !ctr)
+    if (!nw || !sc || !nc || !off || !stat || !w0 || !w1 || !e0 || !e1 || !v0 || !v1 || !te || !ctr)
       return fail(CHAMP_ENOMEM, "DMC allocation failed");
     c->dA.ctr = c->dB.ctr = ctr;
     c->dA.nw = c->dB.nw = nw;
     c->dA.et = c->dB.et = sc;
     c->dA.eest = c->dB.eest = sc + 1;
     c->dA.red = c->dB.red = sc + 2;
+    c->dA.esg = c->dB.esg = sc + 4;
+    c->dA.teff = c->dB.teff = te;
+    c->dA.v2 = v0; c->dB.v2 = v1;
     c->dA.ncopy = c->dB.ncopy = nc;
     c->dA.off = c->dB.off = off;
     c->dA.stat = c->dB.stat = stat;
@@ -1841,26 +1856,33 @@ int champ_dmc_init(champ_ctx *c, int32_t w_target, double tau, double gpop) {
   c->dpar.tau = tau;
   c->dpar.adrift = 0.5;  // adrift_default (control_mod.f90:16)
   c->dpar.gpop = gpop;
-  c->dpar.ecut = 10.0 / std::sqrt(tau);
+  c->dpar.rewt_limit = 10.0;  // limit_rewt_dmc (control_mod.f90:16)
+  c->dpar.c_rewt = 3.5;       // c_rewt (control_mod.f90:16)
+  c->dpar.ene_int = c->dmc_ene_int;
   c->dpar.wtarget = w_target;
   c->dpar.wmax = c->wmax;
   // initial population: the current walkers, weight 1, with their local energies
   int rc = launch(c, Op::EvalOut);
   if (rc) return rc;
   double *el = c->prec == CHAMP_PREC_FP32 ? c->stf.o_eloc : c->std_.o_eloc;
-  std::vector<double> elh(c->W), one(c->W, 1.0);
+  double *vel = c->prec == CHAMP_PREC_FP32 ? c->stf.o_vel : c->std_.o_vel;
+  std::vector<double> elh(c->W), one(c->W, 1.0), velh((size_t)c->W * c->N * 3), v2h(c->W, 0.0);
   CK(cudaMemcpyAsync(elh.data(), el, sizeof(double) * c->W, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(velh.data(), vel, sizeof(double) * velh.size(), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  for (int w = 0; w < c->W; w++)
+    for (int i = 0; i < 3 * c->N; i++) v2h[w] += velh[(size_t)w * 3 * c->N + i] * velh[(size_t)w * 3 * c->N + i];
   double em = 0;
   int nf = 0;
   for (double e : elh)
     if (std::isfinite(e)) { em += e; nf++; }
   em = nf ? em / nf : 0.0;
-  double sc[4] = {em, em, 0.0, 0.0};
+  double sc[8] = {em, em, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   int nw = c->W;
   CK(cudaMemcpyAsync(c->dA.el, elh.data(), sizeof(double) * c->W, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->dA.v2, v2h.data(), sizeof(double) * c->W, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->dA.wt, one.data(), sizeof(double) * c->W, cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(c->dA.et, sc, sizeof(double) * 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->dA.et, sc, sizeof(double) * 8, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->dA.nw, &nw, sizeof(int), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->dmc_step = 0;
@@ -2046,6 +2068,25 @@ int champ_walker_status(champ_ctx *c, uint32_t *flags) {
   return tc_check(c);
 }
 
+int champ_tmoves(champ_ctx *c, uint64_t seed, uint64_t step, double tau, int32_t variant, int32_t *moved) {
+  if (!c) return fail(CHAMP_EINVAL, "null context");
+  if (!c->have_walkers) return fail(CHAMP_ESTATE, "no walkers set");
+  if (variant != 1 && variant != 2) return fail(CHAMP_EINVAL, "T-move variant: 1 (casula1) or 2 (det_balance1)");
+  if (!(tau > 0)) return fail(CHAMP_EINVAL, "tau must be positive");
+  if (c->nloc == 0) return fail(CHAMP_EINVAL, "T-moves need a nonlocal pseudopotential");
+  OpArgs t;
+  t.tau = tau;
+  t.variant = variant;
+  t.seed = seed;
+  t.sweep0 = step;
+  t.moved = moved ? (int *)c->d_out : nullptr;  // the staging buffer holds [w_max][4 nelec] doubles
+  int rc = launch(c, Op::Tmove, t);
+  if (rc) return rc;
+  if (moved) CK(cudaMemcpyAsync(moved, t.moved, sizeof(int) * c->W, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return CHAMP_OK;
+}
+
 int champ_set_mover(champ_ctx *c, int32_t imetro, double deltar, double deltat, double fbias) {
   if (!c) return fail(CHAMP_EINVAL, "null context");
   if (imetro != 1 && imetro != 6) return fail(CHAMP_EINVAL, "imetro must be 1 or 6 (accelerated Metropolis)");
@@ -2095,6 +2136,18 @@ int champ_set_option(champ_ctx *c, const char *name, int64_t value) {
   if (!strcmp(name, "param_grad_mode")) {
     if (value < 0 || value > 1) return fail(CHAMP_EINVAL, "param_grad_mode: 0 or 1");
     c->pg_mode = (int)value;
+    return CHAMP_OK;
+  }
+  if (!strcmp(name, "dmc_ene_int")) {
+    if (value < 0 || value > 1) return fail(CHAMP_EINVAL, "dmc_ene_int: 0 (no_ene_int) or 1 (ene_int_v9)");
+    c->dmc_ene_int = c->dpar.ene_int = (int)value;
+    dmc_graph_release(c);
+    return CHAMP_OK;
+  }
+  if (!strcmp(name, "tmoves")) {
+    if (value < 0 || value > 2) return fail(CHAMP_EINVAL, "tmoves: 0 (off), 1 (casula1) or 2 (det_balance1)");
+    c->dpar.tmove = (int)value;
+    dmc_graph_release(c);  // the captured steps carry the old setting
     return CHAMP_OK;
   }
   if (!strcmp(name, "delay_rank")) {
@@ -2148,6 +2201,8 @@ int champ_get_option(const champ_ctx *c, const char *name, int64_t *value) {
   if (!strcmp(name, "param_grad_mode")) { *value = c->pg_mode; return CHAMP_OK; }
   if (!strcmp(name, "staged_eval")) { *value = c->el_staged; return CHAMP_OK; }
   if (!strcmp(name, "delay_rank")) { *value = c->std_.dly ? c->std_.dlk : 0; return CHAMP_OK; }
+  if (!strcmp(name, "tmoves")) { *value = c->dpar.tmove; return CHAMP_OK; }
+  if (!strcmp(name, "dmc_ene_int")) { *value = c->dmc_ene_int; return CHAMP_OK; }
   return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);
 }
 

@@ -515,6 +515,7 @@ __device__ void build_gamma(const Sys<T> &s, const View<T> &v, int lane, double 
 // ---------------------------------------------------------------------------------------
 struct EvalRes {
   double lnpsi, sign, psij, d2lnpsi, pe, pe_ee, pe_nl, eloc, d2j, vj2;
+  double v2;  // |grad ln psi|^2 summed over the electrons
   bool singular;
   int ntask;  // (electron, centre) pairs inside the nonlocal range (task records in the view's nlt)
 };
@@ -1108,6 +1109,7 @@ __device__ void finish_eval(const Sys<T> &s, const State<T> &st, int w, const Vi
   res.pe_nl = vnl;
   res.eloc = eloc;
   res.d2j = d2j;
+  res.v2 = v2;
   {
     double vj2 = 0;
     for (int i = lane; i < 3 * N; i += 32) vj2 += v.vacc[i] * v.vacc[i];

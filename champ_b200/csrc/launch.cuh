@@ -26,6 +26,7 @@ static int set_smem_attrs(champ_ctx *c) {
   if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD, 0, 6>, sm);
   if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD, 1, 6>, sm);
   if (!rc) rc = set_attrs(c, k_dmc_move<T, NORD, MD>, sm);
+  if (!rc) rc = set_attrs(c, k_dmc_tmove<T, NORD, MD>, sm);
   if (!rc && std::is_same<T, float>::value && c->prec == CHAMP_PREC_FP32) {
     CK(cudaFuncSetAttribute(orbtc::k_orb_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024 + 128));
     CK(cudaFuncSetAttribute(orbtc::k_orb_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024 + 128));
@@ -195,6 +196,13 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
     k_dmc_move<T, NORD, MD><<<dim3((c->dpar.wmax + K.wpb - 1) / K.wpb), block, K.smem, c->stream>>>(
         s, st, K.lay, c->dpar, c->dA, a.phase < 0 ? 0 : a.phase);
     break;
+  case Op::Tmove: {
+    const int wl = a.dmc ? c->dpar.wmax : st.W;
+    k_dmc_tmove<T, NORD, MD><<<dim3((wl + K.wpb - 1) / K.wpb), block, K.smem, c->stream>>>(
+        s, st, K.lay, st.W, a.dmc ? c->dA.nw : nullptr, a.tau, a.variant, a.seed, a.dmc ? c->dA.ctr : nullptr,
+        a.sweep0, a.moved);
+    break;
+  }
   case Op::DmcCopy: {
     k_dmc_copy<T><<<592, 128, 0, c->stream>>>(st, st2of<T>(c), c->dA, c->dB, c->N, c->C, c->dpar.wmax);
     break;

@@ -26,7 +26,7 @@ EXPORTED_SYMBOLS = [
     "champ_get_option", "champ_oh_buffers", "champ_phase_times", "champ_param_grad_fwd", "champ_param_grad_bwd",
     "champ_linear_update", "champ_set_params", "champ_get_params", "champ_apply_param_step",
     "champ_check_param_step", "champ_eval_param_step", "champ_linear_method_step", "champ_autotune",
-    "champ_set_mover",
+    "champ_set_mover", "champ_tmoves",
 ]
 
 PREC = {"fp64": 0, "mixed": 1, "fp32": 2}
@@ -93,6 +93,7 @@ def load_library(path: str = LIB_PATH):
     L.champ_linear_method_step.argtypes = [vp, i32, C.POINTER(i32), dp, dp, C.c_double, C.c_double, dp, dp, dp]
     L.champ_autotune.argtypes = [vp, i32, u64, C.c_double, C.c_char_p, C.c_char_p, i32]
     L.champ_set_mover.argtypes = [vp, i32, C.c_double, C.c_double, C.c_double]
+    L.champ_tmoves.argtypes = [vp, u64, u64, C.c_double, i32, C.POINTER(i32)]
     for n in EXPORTED_SYMBOLS:
         if n not in ("champ_last_error", "champ_version"):
             getattr(L, n).restype = C.c_int
@@ -259,6 +260,12 @@ class Engine:
     def apply_param_step(self, dp):
         dp = np.ascontiguousarray(dp, np.float64)
         self._check(self.lib.champ_apply_param_step(self.h, _p(dp)))
+
+    def tmoves(self, seed, step, tau, variant=2):
+        """champ_tmoves: T-moves of every electron; returns the accepted moves per walker."""
+        moved = np.zeros(self.nw, np.int32)
+        self._check(self.lib.champ_tmoves(self.h, seed, step, tau, variant, moved.ctypes.data_as(C.POINTER(C.c_int32))))
+        return moved
 
     def set_mover(self, imetro, deltar=5.0, deltat=1.0, fbias=1.0):
         """champ_set_mover: 1 Gaussian steps, 6 the accelerated Metropolis method."""

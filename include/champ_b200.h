@@ -325,7 +325,10 @@ int champ_linear_method_step(champ_ctx *ctx, int32_t nsel, const int32_t *sel, c
    returns per step {population, sum w, sum w E_L, E_T} in stats (host [nstep][4] or NULL).
    Afterwards the context's walker count is the new population.  Pairs of steps run as one
    CUDA graph (captured on first use and whenever the seed changes; option "dmc_graph" 0 launches
-   step by step); the step number that keys the random numbers is kept on the device. */
+   step by step); the step number that keys the random numbers is kept on the device.  The
+   reweighting integrates the energy over the step as the reference's default ene_int_v9 does
+   (green_functions_mod.f90:382-472, limit_rewt_dmc 10, c_rewt 3.5, effective time step of
+   itau_eff 1); option "dmc_ene_int" 0 uses the plain local energies (no_ene_int). */
 int champ_dmc_init(champ_ctx *ctx, int32_t w_target, double tau, double gpop);
 int champ_dmc_steps(champ_ctx *ctx, int32_t nstep, uint64_t seed, double *stats);
 
@@ -348,6 +351,18 @@ int champ_num_walkers(const champ_ctx *ctx, int32_t *nw);
 int champ_eval_energy_noalloc(champ_ctx *ctx, int32_t nw, const double *x, double *eloc);
 /* Waits for the context's stream; also reports a tensor-core contraction that gave up. */
 int champ_synchronize(champ_ctx *ctx);
+
+/* T-moves (tmove.f90:1-192, Casula's size-consistent T-moves; psi_utils_mod.f90:390 do_tmoves) of
+   every electron of every walker, in order: the off-diagonal elements of the nonlocal
+   pseudopotential to the quadrature points of each centre in range, T(q) = sum over the nonlocal
+   channels of w_q (exp(-tau v_l(r)) - 1) P_l(cos theta) psi(x_q)/psi(x), sampled by heat bath
+   against weight 1 for staying (positive elements only); variant 1 (casula1) moves the electron
+   there, variant 2 (det_balance1, the reference's default) accepts with min(1, forward sum /
+   backward sum over the chosen centre's points about the new position).  The points are rotated
+   at random per (walker, step, electron).  moved (host [nw] or NULL) receives the accepted
+   T-moves per walker.  A DMC run makes them at the start of every step when option "tmoves" is 1
+   or 2 (rundmc_mod.f90:137). */
+int champ_tmoves(champ_ctx *ctx, uint64_t seed, uint64_t step, double tau, int32_t variant, int32_t *moved);
 
 /* The VMC mover of champ_vmc_sweeps and champ_vmc_run_host (imetro of the reference's control
    menu, control_mod.f90:78-82 and 375-385, default there 6).  imetro 1: Gaussian displacements
@@ -390,6 +405,9 @@ int champ_set_mover(champ_ctx *ctx, int32_t imetro, double deltar, double deltat
    distances; basis and orbitals per electron; Slater-matrix inversion in shared memory;
    velocities, pseudopotential and E_L), and a VMC sweep of an FP64 context as its moves followed
    by that evaluation; 0 runs the single-kernel evaluation (and the fused FP64 sweep kernel).
+   "tmoves": 0 (default), 1 or 2 -- T-moves of the variant of champ_tmoves at the start of every
+   DMC step (champ_dmc_steps).
+   "dmc_ene_int": 1 (default) ene_int_v9 energy integration in the DMC reweighting, 0 none.
    "delay_rank": K >= 2 (default 4 when the walker state of a single-determinant FP64 or mixed
    context lives in HBM) keeps the accepted moves' Sherman-Morrison terms of a spin aside and
    folds K of them at a time into the inverse as one FP64 tensor-core product (proposals use the
@@ -418,7 +436,8 @@ int champ_phase_times(champ_ctx *ctx, double *ms /* [4] */, int32_t *launches /*
 int champ_autotune(champ_ctx *ctx, int32_t nsweep, uint64_t seed, double step, const char *cache_path, char *report,
                    int32_t report_len);
 /* Current value of an option ("orbital_tc", "orbital_tc_chunk", "reinvert_every", "dmc_graph",
-   "phase_timing", "param_grad_mode", "staged_eval", "delay_rank"); kernel launches per champ_vmc_sweeps sweep
+   "phase_timing", "param_grad_mode", "staged_eval", "delay_rank", "tmoves", "dmc_ene_int"); kernel launches per
+   champ_vmc_sweeps sweep
    ("launches_per_sweep": 1 for the fused sweep kernel, 2 for moves + single-kernel evaluation,
    5 for moves + staged evaluation or with the tensor-core orbitals). */
 int champ_get_option(const champ_ctx *ctx, const char *name, int64_t *value);

@@ -1979,3 +1979,93 @@ int orc_vmc_accel(const orc_sys *s, int nw, double *xall, int nsweep, uint64_t s
   }
   return 0;
 }
+
+/* ------------------------------------------------------------------------------------ */
+/* T-moves (qmc/dmc/dmc_elec/tmove.f90:1-192; psi_utils_mod.f90:390 do_tmoves)            */
+/* ------------------------------------------------------------------------------------ */
+static void rotation_draws(mrng_t *r, double *R) {
+  double u1 = mrng_next(r), u2 = mrng_next(r), u3 = mrng_next(r);
+  const double tp = 6.283185307179586;
+  double s1 = sqrt(1.0 - u1), s2 = sqrt(u1);
+  double qx = s1 * sin(tp * u2), qy = s1 * cos(tp * u2), qz = s2 * sin(tp * u3), qw = s2 * cos(tp * u3);
+  R[0] = 1 - 2 * (qy * qy + qz * qz); R[1] = 2 * (qx * qy - qz * qw); R[2] = 2 * (qx * qz + qy * qw);
+  R[3] = 2 * (qx * qy + qz * qw); R[4] = 1 - 2 * (qx * qx + qz * qz); R[5] = 2 * (qy * qz - qx * qw);
+  R[6] = 2 * (qx * qz - qy * qw); R[7] = 2 * (qy * qz + qx * qw); R[8] = 1 - 2 * (qx * qx + qy * qy);
+}
+
+/* the T-matrix element of one quadrature point: sum over the nonlocal channels of
+   w_q (exp(-tau v_l) - 1) P_l(cos) times the wave-function ratio */
+static double tmove_element(const orc_sys *s, int ict, const double *vps, double wq, double costh, double tau,
+                            double ratio) {
+  double g = 0;
+  for (int l = 0; l < s->npotd[ict]; l++)
+    if (l + 1 != s->lpotp1[ict]) g += wq * (exp(-tau * vps[l]) - 1) * yl0(l, costh) * ratio;
+  return g;
+}
+
+/* T-moves of every electron of one walker at x (in place), with the draws of the engine's
+   per-(walker, step, electron) streams; variant 1 casula1, 2 det_balance1.  Returns the number of
+   accepted moves. */
+int orc_tmoves(const orc_sys *s, double *x, uint64_t seed, uint32_t iw, uint64_t step, double tau, int variant) {
+  int N = s->N, nmv = 0;
+  for (int e = 0; e < N; e++) {
+    mrng_t rng = {seed, iw, (uint32_t)step, (uint32_t)(step >> 32), 256u + (uint32_t)e, 0u, {0, 0}, 0};
+    double R[9];
+    rotation_draws(&rng, R);
+    double xo[3] = {x[3 * e], x[3 * e + 1], x[3 * e + 2]};
+    double S = 1.0, pratio = 0.0;
+    int pc = -1, pq = -1;
+    for (int c = 0; c < s->C; c++) {
+      const double *cc = s->cent + 3 * c;
+      double rv[3] = {xo[0] - cc[0], xo[1] - cc[1], xo[2] - cc[2]};
+      double r = sqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
+      int ict = s->ctype[c];
+      double vps[MAXLCH];
+      orc_vps(s, ict, r, vps);
+      int skip = 1;
+      for (int l = 0; l < s->npotd[ict]; l++)
+        if (l + 1 != s->lpotp1[ict] && fabs(vps[l]) > 1e-4) skip = 0;
+      if (skip) continue;
+      for (int q = 0; q < s->nquad; q++) {
+        double qv[3];
+        for (int k = 0; k < 3; k++) qv[k] = R[3 * k] * s->q0[q][0] + R[3 * k + 1] * s->q0[q][1] + R[3 * k + 2] * s->q0[q][2];
+        double costh = (rv[0] * qv[0] + rv[1] * qv[1] + rv[2] * qv[2]) / r;
+        double xq[3] = {cc[0] + r * qv[0], cc[1] + r * qv[1], cc[2] + r * qv[2]};
+        double ratio = orc_ratio_1e(s, x, e, xq, NULL);
+        double g = tmove_element(s, ict, vps, s->wq[q], costh, tau, ratio);
+        if (g > 0) {
+          S += g;
+          if (mrng_next(&rng) < g / S) { pc = c; pq = q; pratio = ratio; }
+        }
+      }
+    }
+    if (pc < 0) continue;
+    const double *cc = s->cent + 3 * pc;
+    double r = sqrt((xo[0] - cc[0]) * (xo[0] - cc[0]) + (xo[1] - cc[1]) * (xo[1] - cc[1]) + (xo[2] - cc[2]) * (xo[2] - cc[2]));
+    double xn[3];
+    for (int k = 0; k < 3; k++)
+      xn[k] = cc[k] + r * (R[3 * k] * s->q0[pq][0] + R[3 * k + 1] * s->q0[pq][1] + R[3 * k + 2] * s->q0[pq][2]);
+    double p = 1.0;
+    if (variant == 2) {
+      int ict = s->ctype[pc];
+      double vps[MAXLCH], R2[9];
+      orc_vps(s, ict, r, vps);
+      rotation_draws(&rng, R2);
+      double xe[3] = {xn[0] - cc[0], xn[1] - cc[1], xn[2] - cc[2]}, Sb = 1.0;
+      for (int q = 0; q < s->nquad; q++) {
+        double qv[3];
+        for (int k = 0; k < 3; k++) qv[k] = R2[3 * k] * s->q0[q][0] + R2[3 * k + 1] * s->q0[q][1] + R2[3 * k + 2] * s->q0[q][2];
+        double costh = (xe[0] * qv[0] + xe[1] * qv[1] + xe[2] * qv[2]) / r;
+        double xq[3] = {cc[0] + r * qv[0], cc[1] + r * qv[1], cc[2] + r * qv[2]};
+        double ratio = orc_ratio_1e(s, x, e, xq, NULL) / pratio;
+        double g = tmove_element(s, ict, vps, s->wq[q], costh, tau, ratio);
+        if (g > 0) Sb += g;
+      }
+      p = S / Sb < 1.0 ? S / Sb : 1.0;
+    }
+    if (mrng_next(&rng) >= p) continue;
+    for (int k = 0; k < 3; k++) x[3 * e + k] = xn[k];
+    nmv++;
+  }
+  return nmv;
+}

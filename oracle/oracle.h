@@ -74,6 +74,8 @@ void orc_random_rotation(uint64_t seed, uint32_t walker, uint64_t sweep, double 
    Metropolis accept on |psi ratio|^2, full E_L after each sweep with the quadrature
    rotated per (walker, sweep).  Incremental single-electron updates as in
    metrop_mov1/hpsie/jassav/detsav.  x is updated in place.  nthreads <= 0: all cores. */
+/* T-moves of every electron of one walker (in place); returns the accepted moves. */
+int orc_tmoves(const orc_sys *s, double *x, uint64_t seed, uint32_t iw, uint64_t step, double tau, int variant);
 /* VMC with the accelerated Metropolis mover (imetro = 6). */
 int orc_vmc_accel(const orc_sys *s, int nw, double *x, int nsweep, uint64_t seed, uint64_t sweep0, double deltar,
                   double deltat, double fbias, double *esum, double *e2sum, double *accept, double *elast,

@@ -57,6 +57,8 @@ def lib():
         L.orc_jastrow_param_grad.argtypes = [vp, dp, dp, dp]
         L.orc_jastrow_pderiv.restype = ip
         L.orc_jastrow_pderiv.argtypes = [vp, dp, dp, dp, dp]
+        L.orc_tmoves.restype = ip
+        L.orc_tmoves.argtypes = [vp, dp, C.c_uint64, C.c_uint32, C.c_uint64, C.c_double, ip]
         L.orc_vmc_accel.restype = ip
         L.orc_vmc_accel.argtypes = [vp, ip, dp, ip, C.c_uint64, C.c_uint64, C.c_double, C.c_double, C.c_double,
                                     dp, dp, dp, dp, ip]
@@ -166,6 +168,12 @@ class Oracle:
         es, e2, acc, el = (np.zeros(nw) for _ in range(4))
         lib().orc_vmc(self.h, nw, _p(x), nsweep, seed, sweep0, step, _p(es), _p(e2), _p(acc), _p(el), nthreads)
         return dict(x=x, esum=es, e2sum=e2, accept=acc, elast=el)
+
+    def tmoves(self, x, seed, iw, step, tau, variant=2):
+        """T-moves of every electron of one walker; returns (new positions, accepted moves)."""
+        x = np.ascontiguousarray(x, float).reshape(self.N, 3).copy()
+        n = lib().orc_tmoves(self.h, _p(x), seed, iw, step, tau, variant)
+        return x, n
 
     def vmc_accel(self, x, nsweep, seed, sweep0=0, deltar=5.0, deltat=1.0, fbias=1.0, nthreads=0):
         """VMC with the accelerated Metropolis mover (imetro = 6)."""
