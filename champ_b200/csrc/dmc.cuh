@@ -12,7 +12,8 @@
 // the electrons' acceptance probabilities and diffusion steps (itau_eff = 1, rundmc_mod.f90:203-210).
 // Branching (split_join, dmc/dmc_elec/split_join_mod.f90): each walker is copied
 // floor(w + u) times with weight 1 into a second state buffer (exclusive scan for the
-// destinations); the trial energy follows the population: E_T = E_est - ln(W/W_target)/(g tau).
+// destinations); the trial energy follows the population: E_T = E_g - ln(W/W_target)/(g tau),
+// E_g a running average of the growth energy.
 // The walker count lives on the device, so steps need no host synchronisation.
 #pragma once
 
@@ -31,6 +32,7 @@ struct DmcData {
   double *v2;             // [wmax] |grad ln psi|^2 at the last step
   double *teff;           // [wmax] the step's effective time step (written by the moves)
   double *esg;            // [4] (device) generations, sum sw, sum sw E, sum sw E^2 since the start
+  double *egr;            // (device) running growth energy, the reference of the trial energy
   int *nw;                // current population (device)
   double *et;             // trial energy (device)
   double *eest;           // running estimate of the energy (device)
@@ -377,7 +379,12 @@ static __global__ void k_dmc_finish(DmcData Da, DmcData Db, DmcPar P) {
   double emix = sw > 0 ? swe / sw : *Da.eest;
   // running energy estimate: exponential average of the mixed estimator
   double eest = 0.95 * (*Da.eest) + 0.05 * emix;
-  double et = eest - log((tot > 0 ? (double)tot : 1.0) / (double)P.wtarget) / (P.gpop * P.tau);
+  // running growth energy E_T - ln(sum w_new / sum w_old) / tau (every weight is 1 after branching,
+  // so sum w_old is the population); the trial energy is set from it, so that the population
+  // settles at the target even where the integrated energy that drives the weights differs from
+  // the mixed estimator
+  if (sw > 0 && W > 0) *Da.egr = 0.95 * (*Da.egr) + 0.05 * (*Da.et - log(sw / (double)W) / P.tau);
+  double et = *Da.egr - log((tot > 0 ? (double)tot : 1.0) / (double)P.wtarget) / (P.gpop * P.tau);
   *Db.nw = tot;
   *Db.eest = eest;
   *Db.et = et;

@@ -1826,7 +1826,7 @@ int champ_dmc_init(champ_ctx *c, int32_t w_target, double tau, double gpop) {
     if (rc) return rc;
     size_t W = c->wmax;
     int *nw = dalloc<int>(c, 1);
-    double *sc = dalloc<double>(c, 8);
+    double *sc = dalloc<double>(c, 10);
     int *nc = dalloc<int>(c, W), *off = dalloc<int>(c, W);
     double *stat = dalloc<double>(c, 4 * (size_t)DMC_STAT_CAP);
     double *w0 = dalloc<double>(c, W), *w1 = dalloc<double>(c, W), *e0 = dalloc<double>(c, W), *e1 = dalloc<double>(c, W);
@@ -1840,6 +1840,7 @@ int champ_dmc_init(champ_ctx *c, int32_t w_target, double tau, double gpop) {
     c->dA.eest = c->dB.eest = sc + 1;
     c->dA.red = c->dB.red = sc + 2;
     c->dA.esg = c->dB.esg = sc + 4;
+    c->dA.egr = c->dB.egr = sc + 8;
     c->dA.teff = c->dB.teff = te;
     c->dA.v2 = v0; c->dB.v2 = v1;
     c->dA.ncopy = c->dB.ncopy = nc;
@@ -1877,12 +1878,12 @@ int champ_dmc_init(champ_ctx *c, int32_t w_target, double tau, double gpop) {
   for (double e : elh)
     if (std::isfinite(e)) { em += e; nf++; }
   em = nf ? em / nf : 0.0;
-  double sc[8] = {em, em, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  double sc[10] = {em, em, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, em, 0.0};
   int nw = c->W;
   CK(cudaMemcpyAsync(c->dA.el, elh.data(), sizeof(double) * c->W, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->dA.v2, v2h.data(), sizeof(double) * c->W, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->dA.wt, one.data(), sizeof(double) * c->W, cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(c->dA.et, sc, sizeof(double) * 8, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->dA.et, sc, sizeof(double) * 10, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->dA.nw, &nw, sizeof(int), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->dmc_step = 0;

@@ -319,7 +319,7 @@ int champ_linear_method_step(champ_ctx *ctx, int32_t nsel, const int32_t *sel, c
 
 /* Diffusion Monte Carlo (rundmc, qmc/rundmc_mod.f90:17-422).  champ_dmc_init starts from the
    current walkers (weight 1); w_target is the target population and the trial energy follows
-   E_T = E_est - ln(W / w_target) / (gpop * tau).  The population may range up to w_max.
+   E_T = E_g - ln(W / w_target) / (gpop * tau), E_g a running average of the growth energy.  The population may range up to w_max.
    champ_dmc_steps runs nstep steps (drift-diffusion moves with the Green's-function acceptance
    of green_functions_mod.f90, E_L, reweighting, branching) without host synchronisation and
    returns per step {population, sum w, sum w E_L, E_T} in stats (host [nstep][4] or NULL).
