@@ -117,7 +117,7 @@ struct champ_ctx {
   void *cublas = nullptr;
   // DMC: second state buffer for branching, per-walker weights/energies, device scalars
   bool dmc_ready = false;
-  DmcPar dpar;
+  DmcPar dpar{};
   DmcData dA, dB;
   State<double> std2;
   State<float> stf2;

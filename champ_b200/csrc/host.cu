@@ -1196,10 +1196,8 @@ static int dmc_one_step(champ_ctx *c) {
     rc = launch(c, Op::Tmove, t);
     if (rc) return rc;
   }
-  rc = launch(c, Op::DmcMove);
+  rc = launch(c, Op::DmcMove);  // moves, E_L, reweighting, weight sums, copy counts
   if (rc) return rc;
-  k_dmc_sums<<<148, 256, 0, c->stream>>>(c->dA, c->dpar.wmax);
-  k_dmc_count<<<(c->dpar.wmax + 255) / 256, 256, 0, c->stream>>>(c->dA, c->dpar);
   if (cub::DeviceScan::ExclusiveSum(c->scan_tmp, c->scan_bytes, c->dA.ncopy, c->dA.off, c->dpar.wmax, c->stream) !=
       cudaSuccess)
     return fail(CHAMP_ECUDA, "DMC scan failed");
@@ -1826,21 +1824,23 @@ int champ_dmc_init(champ_ctx *c, int32_t w_target, double tau, double gpop) {
     if (rc) return rc;
     size_t W = c->wmax;
     int *nw = dalloc<int>(c, 1);
-    double *sc = dalloc<double>(c, 10);
+    double *sc = dalloc<double>(c, 12);
     int *nc = dalloc<int>(c, W), *off = dalloc<int>(c, W);
     double *stat = dalloc<double>(c, 4 * (size_t)DMC_STAT_CAP);
     double *w0 = dalloc<double>(c, W), *w1 = dalloc<double>(c, W), *e0 = dalloc<double>(c, W), *e1 = dalloc<double>(c, W);
     double *v0 = dalloc<double>(c, W), *v1 = dalloc<double>(c, W), *te = dalloc<double>(c, W);
     long long *ctr = dalloc<long long>(c, 2);
-    if (!nw || !sc || !nc || !off || !stat || !w0 || !w1 || !e0 || !e1 || !v0 || !v1 || !te || !ctr)
+    int *nx = dalloc<int>(c, 2);
+    if (!nw || !sc || !nc || !off || !stat || !w0 || !w1 || !e0 || !e1 || !v0 || !v1 || !te || !ctr || !nx)
       return fail(CHAMP_ENOMEM, "DMC allocation failed");
     c->dA.ctr = c->dB.ctr = ctr;
     c->dA.nw = c->dB.nw = nw;
     c->dA.et = c->dB.et = sc;
     c->dA.eest = c->dB.eest = sc + 1;
     c->dA.red = c->dB.red = sc + 2;
-    c->dA.esg = c->dB.esg = sc + 4;
-    c->dA.egr = c->dB.egr = sc + 8;
+    c->dA.esg = c->dB.esg = sc + 5;
+    c->dA.egr = c->dB.egr = sc + 9;
+    c->dA.next = c->dB.next = nx;
     c->dA.teff = c->dB.teff = te;
     c->dA.v2 = v0; c->dB.v2 = v1;
     c->dA.ncopy = c->dB.ncopy = nc;
@@ -1873,18 +1873,24 @@ int champ_dmc_init(champ_ctx *c, int32_t w_target, double tau, double gpop) {
   CK(cudaStreamSynchronize(c->stream));
   for (int w = 0; w < c->W; w++)
     for (int i = 0; i < 3 * c->N; i++) v2h[w] += velh[(size_t)w * 3 * c->N + i] * velh[(size_t)w * 3 * c->N + i];
-  double em = 0;
-  int nf = 0;
+  // the initial energy estimate: the median of the finite local energies (a mean would follow the
+  // rare near-node outliers of a short equilibration)
+  std::vector<double> fin;
   for (double e : elh)
-    if (std::isfinite(e)) { em += e; nf++; }
-  em = nf ? em / nf : 0.0;
-  double sc[10] = {em, em, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, em, 0.0};
+    if (std::isfinite(e)) fin.push_back(e);
+  double em = 0.0;
+  if (!fin.empty()) {
+    std::nth_element(fin.begin(), fin.begin() + fin.size() / 2, fin.end());
+    em = fin[fin.size() / 2];
+  }
+  double sc[12] = {em, em, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, em, 0.0, 0.0};
   int nw = c->W;
   CK(cudaMemcpyAsync(c->dA.el, elh.data(), sizeof(double) * c->W, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->dA.v2, v2h.data(), sizeof(double) * c->W, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->dA.wt, one.data(), sizeof(double) * c->W, cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(c->dA.et, sc, sizeof(double) * 10, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->dA.et, sc, sizeof(double) * 12, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->dA.nw, &nw, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->dA.next, 0, 2 * sizeof(int), c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->dmc_step = 0;
   dmc_graph_release(c);
@@ -2139,6 +2145,12 @@ int champ_set_option(champ_ctx *c, const char *name, int64_t value) {
     c->pg_mode = (int)value;
     return CHAMP_OK;
   }
+  if (!strcmp(name, "dmc_persistent")) {
+    if (value < 0 || value > 1) return fail(CHAMP_EINVAL, "dmc_persistent: 0 or 1");
+    c->dpar.persist = (int)value;
+    dmc_graph_release(c);
+    return CHAMP_OK;
+  }
   if (!strcmp(name, "dmc_ene_int")) {
     if (value < 0 || value > 1) return fail(CHAMP_EINVAL, "dmc_ene_int: 0 (no_ene_int) or 1 (ene_int_v9)");
     c->dmc_ene_int = c->dpar.ene_int = (int)value;
@@ -2204,6 +2216,7 @@ int champ_get_option(const champ_ctx *c, const char *name, int64_t *value) {
   if (!strcmp(name, "delay_rank")) { *value = c->std_.dly ? c->std_.dlk : 0; return CHAMP_OK; }
   if (!strcmp(name, "tmoves")) { *value = c->dpar.tmove; return CHAMP_OK; }
   if (!strcmp(name, "dmc_ene_int")) { *value = c->dmc_ene_int; return CHAMP_OK; }
+  if (!strcmp(name, "dmc_persistent")) { *value = c->dpar.persist; return CHAMP_OK; }
   return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);
 }
 

@@ -192,10 +192,16 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
     kern<<<pgrid, pblock, c->smem_pg, c->stream>>>(s, st, K.lay, a.pgout, R[0], R[1], R[2], R[3], R[4], R[5], R[6], R[7], R[8]);
     break;
   }
-  case Op::DmcMove:
-    k_dmc_move<T, NORD, MD><<<dim3((c->dpar.wmax + K.wpb - 1) / K.wpb), block, K.smem, c->stream>>>(
-        s, st, K.lay, c->dpar, c->dA, a.phase < 0 ? 0 : a.phase);
+  case Op::DmcMove: {
+    // persistent: as many blocks as the SMs can hold at once (at most 16 per SM; a block that
+    // finds the work counter exhausted exits at once), no more than the walkers need
+    const int sm = c->num_sms > 0 ? c->num_sms : 148;
+    const int need = (c->dpar.wmax + K.wpb - 1) / K.wpb;
+    const int grid = c->dpar.persist ? std::max(1, std::min(need, sm * 16)) : need;
+    k_dmc_move<T, NORD, MD><<<dim3(grid), block, K.smem, c->stream>>>(s, st, K.lay, c->dpar, c->dA,
+                                                                     a.phase < 0 ? 0 : a.phase);
     break;
+  }
   case Op::Tmove: {
     const int wl = a.dmc ? c->dpar.wmax : st.W;
     k_dmc_tmove<T, NORD, MD><<<dim3((wl + K.wpb - 1) / K.wpb), block, K.smem, c->stream>>>(

@@ -319,7 +319,9 @@ int champ_linear_method_step(champ_ctx *ctx, int32_t nsel, const int32_t *sel, c
 
 /* Diffusion Monte Carlo (rundmc, qmc/rundmc_mod.f90:17-422).  champ_dmc_init starts from the
    current walkers (weight 1); w_target is the target population and the trial energy follows
-   E_T = E_g - ln(W / w_target) / (gpop * tau), E_g a running average of the growth energy.  The population may range up to w_max.
+   E_T = E_g - ln(W / w_target) / (gpop * tau), E_g a running average of the growth energy
+   E_T - ln(sum w_new / W) / tau, seeded with the median local energy.  The population may range
+   up to w_max.
    champ_dmc_steps runs nstep steps (drift-diffusion moves with the Green's-function acceptance
    of green_functions_mod.f90, E_L, reweighting, branching) without host synchronisation and
    returns per step {population, sum w, sum w E_L, E_T} in stats (host [nstep][4] or NULL).
@@ -408,6 +410,8 @@ int champ_set_mover(champ_ctx *ctx, int32_t imetro, double deltar, double deltat
    "tmoves": 0 (default), 1 or 2 -- T-moves of the variant of champ_tmoves at the start of every
    DMC step (champ_dmc_steps).
    "dmc_ene_int": 1 (default) ene_int_v9 energy integration in the DMC reweighting, 0 none.
+   "dmc_persistent": 1 runs the DMC step kernel persistent (resident blocks taking walkers from a
+   work counter), 0 (default) a warp per walker; the results are the same.
    "delay_rank": K >= 2 (default 4 when the walker state of a single-determinant FP64 or mixed
    context lives in HBM) keeps the accepted moves' Sherman-Morrison terms of a spin aside and
    folds K of them at a time into the inverse as one FP64 tensor-core product (proposals use the
@@ -436,7 +440,8 @@ int champ_phase_times(champ_ctx *ctx, double *ms /* [4] */, int32_t *launches /*
 int champ_autotune(champ_ctx *ctx, int32_t nsweep, uint64_t seed, double step, const char *cache_path, char *report,
                    int32_t report_len);
 /* Current value of an option ("orbital_tc", "orbital_tc_chunk", "reinvert_every", "dmc_graph",
-   "phase_timing", "param_grad_mode", "staged_eval", "delay_rank", "tmoves", "dmc_ene_int"); kernel launches per
+   "phase_timing", "param_grad_mode", "staged_eval", "delay_rank", "tmoves", "dmc_ene_int",
+   "dmc_persistent"); kernel launches per
    champ_vmc_sweeps sweep
    ("launches_per_sweep": 1 for the fused sweep kernel, 2 for moves + single-kernel evaluation,
    5 for moves + staged evaluation or with the tensor-core orbitals). */

@@ -71,3 +71,41 @@ def test_dmc_graph_replay_matches_step_by_step_launches():
     assert np.array_equal(st0[:, 0], st1[:, 0])
     assert np.allclose(st0[:, 1:], st1[:, 1:], rtol=1e-10, atol=1e-10)
     assert np.allclose(out[0][1], out[1][1], rtol=0, atol=1e-12)
+
+
+def test_dmc_persistent_kernel_matches_warp_per_walker():
+    """The persistent DMC step kernel (walkers taken from a work counter) follows the same trajectory
+    as the warp-per-walker launch: same populations, weights and energies to summation order."""
+    from champ_b200.engine import Engine
+    s = S.c2_dmc()
+    out = {}
+    for persist in (0, 1):
+        eng = Engine(s, 4096, "fp64")
+        eng.set_option("dmc_persistent", persist)
+        assert eng.get_option("dmc_persistent") == persist
+        eng.set_walkers(S.initial_walkers(s, 2048, seed=9))
+        eng.vmc_sweeps(10, seed=9, sweep0=0, step=0.4, stats=False)
+        eng.dmc_init(2048, 0.01)
+        out[persist] = (eng.dmc_steps(9, seed=31), eng.get_walkers())
+    assert np.array_equal(out[0][0][:, 0], out[1][0][:, 0])
+    assert np.allclose(out[0][0][:, 1:], out[1][0][:, 1:], rtol=1e-10, atol=1e-10)
+    assert np.allclose(out[0][1], out[1][1], rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("nvmc", [5, 40])
+def test_dmc_population_control_from_short_equilibration(nvmc):
+    """Population control from a barely equilibrated start (a few VMC sweeps, near-node outliers
+    among the initial local energies): the population stays within a factor of 2 of the target and
+    ends within 15 % of it."""
+    from champ_b200.engine import Engine
+    s = S.c2_dmc()
+    target = 8192
+    eng = Engine(s, 2 * target, "mixed")
+    eng.set_walkers(S.initial_walkers(s, target, seed=11))
+    eng.vmc_sweeps(nvmc, seed=5, sweep0=0, step=s.step, stats=False)
+    eng.dmc_init(target, 0.01)
+    st = eng.dmc_steps(300, seed=3)
+    pop = st[:, 0]
+    print(f"{nvmc} VMC sweeps: population {pop.min():.0f}..{pop.max():.0f}, last 100 steps {pop[-100:].mean():.0f}")
+    assert pop.min() > 0.5 * target and pop.max() < 2 * target
+    assert abs(pop[-100:].mean() / target - 1) < 0.15
