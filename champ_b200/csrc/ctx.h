@@ -77,6 +77,8 @@ struct champ_ctx {
   double rot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
   bool have_walkers = false;
   KCfg kf, kd;  // FP32 and FP64 kernels (a mixed-precision context uses both)
+  KCfg kfm;     // FP32 Gaussian moves of a state in HBM sharing the coefficient stream (kfm.lay.coop)
+  int move_coop = 0;  // option "move_coop": 1 runs those moves with kfm
   // staged evaluation (elstage.cuh) of the FP64 state when it lives in HBM: on/off (option
   // "staged_eval"), warps per block and dynamic shared memory of k_el_jas, k_el_orb, k_el_fin,
   // and the pseudopotential scratch of k_el_fin (elements)

@@ -1476,6 +1476,21 @@ int champ_create(const champ_system *d, int32_t w_max, int32_t precision, void *
                                    c->stf.gstride, c->stf.wstride, c->nloc > 0 && precision == CHAMP_PREC_FP32,
                                    RESIDENT_LIMIT);
     if (!rc) rc = finish_cfg(c->kf);
+    // Gaussian moves of a state in HBM: a move-only layout (one basis channel) and the block's
+    // warps sharing the proposals' coefficient stream (block_orbitals: more than 16 and at most 128
+    // orbitals per spin, the lane mapping of warp_orbitals, so the sums are the same)
+    const int no0 = c->sf.nocc[0], no1 = c->sf.nocc[1];
+    if (!rc && !c->kf.lay.resident && !c->md.multidet && no0 > 16 && no1 > 16 && no0 <= 128 && no1 <= 128) {
+      KCfg &m = c->kfm;
+      m.lay = make_layout<float>(c->N, c->C, c->nbasis, c->nmax, c->nomax, c->stf.astride, c->stf.tvstride,
+                                 c->stf.gstride, c->stf.wstride, false, RESIDENT_LIMIT, true);
+      m.wpb = 4;
+      m.lay.stage = align16(m.lay.bytes * m.wpb);
+      m.smem = m.lay.stage + sizeof(float) * COOP_STAGES * COOP_KB * (size_t)std::max(no0, no1);
+      m.lay.coop = 1;
+      if (m.smem <= 200 * 1024) c->move_coop = 1;
+      else m = KCfg{};
+    }
   }
   if (rc) { champ_destroy(c); return rc; }
   c->nfree = c->ncsfp + c->norbp + c->nparm_jas;
@@ -2145,6 +2160,14 @@ int champ_set_option(champ_ctx *c, const char *name, int64_t value) {
     c->pg_mode = (int)value;
     return CHAMP_OK;
   }
+  if (!strcmp(name, "move_coop")) {
+    if (value < 0 || value > 1) return fail(CHAMP_EINVAL, "move_coop: 0 or 1");
+    if (value && !c->kfm.lay.coop)
+      return fail(CHAMP_EINVAL, "move_coop: needs an FP32 or mixed single-determinant context whose walker state "
+                                "lives in HBM, with 17 to 128 orbitals per spin");
+    c->move_coop = (int)value;
+    return CHAMP_OK;
+  }
   if (!strcmp(name, "dmc_persistent")) {
     if (value < 0 || value > 1) return fail(CHAMP_EINVAL, "dmc_persistent: 0 or 1");
     c->dpar.persist = (int)value;
@@ -2217,6 +2240,7 @@ int champ_get_option(const champ_ctx *c, const char *name, int64_t *value) {
   if (!strcmp(name, "tmoves")) { *value = c->dpar.tmove; return CHAMP_OK; }
   if (!strcmp(name, "dmc_ene_int")) { *value = c->dmc_ene_int; return CHAMP_OK; }
   if (!strcmp(name, "dmc_persistent")) { *value = c->dpar.persist; return CHAMP_OK; }
+  if (!strcmp(name, "move_coop")) { *value = c->move_coop; return CHAMP_OK; }
   return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);
 }
 

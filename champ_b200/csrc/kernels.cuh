@@ -84,6 +84,8 @@ struct Layout {
   size_t ainv, fso, ren, zq, pf, orb5, gproj, nlt, tv, gam, ymd, wdet;  // resident mode only
   size_t bytes, base;  // total bytes per warp; bytes of the always-shared part
   int resident;
+  int coop;            // the FP32 move kernel's warps share the coefficient stream (block_orbitals)
+  size_t stage;        // offset of that stream's double buffer in the block's shared memory
 };
 
 // Per-walker view: where this walker's arrays live for the current kernel.
@@ -108,15 +110,17 @@ __host__ __device__ inline int phi_count(int nbasis, int C) { return nbasis * 5 
 
 template <class T>
 static Layout make_layout(int N, int C, int nbasis, int nmax, int nomax, int astride, int tvstride, int gstride,
-                          int wstride, bool nl, size_t resident_limit) {
-  Layout L;
+                          int wstride, bool nl, size_t resident_limit, bool moves_only = false) {
+  // moves_only: the Gaussian single-electron moves of a state in HBM (one basis channel, no
+  // velocities); vacc and divj then share phi's place and must not be used
+  Layout L{};
   size_t o = 0;
   auto take = [&](size_t b) { size_t r = o; o += align16(b); return r; };
-  L.phi = take(sizeof(T) * phi_count(nbasis, C));
+  L.phi = take(sizeof(T) * (moves_only ? (size_t)nbasis : (size_t)phi_count(nbasis, C)));
   L.arow = take(sizeof(T) * 5 * nomax);
   L.xs = take(sizeof(double) * N * 3);
-  L.vacc = take(sizeof(double) * N * 3);
-  L.divj = take(sizeof(double) * N);
+  L.vacc = moves_only ? L.phi : take(sizeof(double) * N * 3);
+  L.divj = moves_only ? L.phi : take(sizeof(double) * N);
   L.colb = take(sizeof(double) * nmax);
   L.vb = take(sizeof(double) * nmax);
   L.perm = take(sizeof(int) * nmax);
@@ -136,7 +140,7 @@ static Layout make_layout(int N, int C, int nbasis, int nmax, int nomax, int ast
   L.ymd = take(sizeof(double) * tvstride);
   L.wdet = take(sizeof(double) * wstride);
   L.base = base;
-  L.resident = (o <= resident_limit) ? 1 : 0;
+  L.resident = (!moves_only && o <= resident_limit) ? 1 : 0;
   L.bytes = L.resident ? o : base;
   return L;
 }
@@ -1253,7 +1257,8 @@ __device__ inline void delay_flush(Delay &d, double *A0, int n, int sp, int lane
 
 template <class T, int NORD, bool MD, bool GRAD>
 __device__ void propose(const Sys<T> &s, const JasPar<T> &J, const State<T> &st, int w, const View<T> &v, int e,
-                        const double *xn, int lane, double &rho, double &dj, double *grad, const Delay *dl = nullptr) {
+                        const double *xn, int lane, double &rho, double &dj, double *grad, const Delay *dl = nullptr,
+                        T *coop = nullptr) {
   const int N = s.N, C = s.C, nomax = s.nomax;
   int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
   const double *A = gam_ptr<T, MD>(s, v, sp);
@@ -1276,7 +1281,12 @@ __device__ void propose(const Sys<T> &s, const JasPar<T> &J, const State<T> &st,
     v.asum[lane] = z;
   }
   warp_basis<T, NCH>(s, xn, v.phi, lane);
-  warp_orbitals<T, NCH>(v.phi, s.cocc[sp], s.nbasis, no, v.arow, nomax, lane);
+  if constexpr (!GRAD && sizeof(T) == 4) {
+    if (coop) block_orbitals<T>(v.phi, s.cocc[sp], s.nbasis, no, v.arow, lane, coop, true);
+    else warp_orbitals<T, NCH>(v.phi, s.cocc[sp], s.nbasis, no, v.arow, nomax, lane);
+  } else {
+    warp_orbitals<T, NCH>(v.phi, s.cocc[sp], s.nbasis, no, v.arow, nomax, lane);
+  }
   // the wave function is linear in the moved electron's orbital row: ratio = sum_m G[m][e] phi_m
   double r0 = 0, g0 = 0, g1 = 0, g2 = 0;
   for (int k = lane; k < no; k += 32) {
@@ -1539,7 +1549,27 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
   const int N = s.N;
   constexpr int phase = PH;
   constexpr bool moves = phase == 0 || phase == 1, eval = phase != 1;
-  for (int w = blockIdx.x * wpb + wib; w < st.W; w += gridDim.x * wpb) {
+  // FP32 Gaussian moves of a state in HBM with L.coop: the block's warps move their walkers'
+  // electrons in step and share the coefficient stream of the proposals (block_orbitals)
+  T *coop = nullptr;
+  if constexpr (PH == 1 && MV == 1 && sizeof(T) == 4)
+    if (L.coop) coop = (T *)(dsm + L.stage);
+  for (int wb = blockIdx.x * wpb; wb < st.W; wb += gridDim.x * wpb) {
+    const int w = wb + wib;
+    if (w >= st.W) {
+      if constexpr (PH == 1 && MV == 1 && sizeof(T) == 4) {
+        if (coop) {
+          // no walker for this warp: take part in the block's coefficient stream, no sums
+          for (int isw = 0; isw < nsweep; isw++)
+            for (int e = 0; e < N; e++) {
+              const int sp = e < s.nup ? 0 : 1;
+              block_orbitals<T>((const T *)nullptr, s.cocc[sp], s.nbasis, s.nocc[sp], (T *)nullptr, lane, coop, false);
+            }
+          continue;
+        }
+      }
+      break;
+    }
     View<T> v = make_view<T>(dsm + L.bytes * wib, L, st, w, s.N, s.C, s.nbasis, s.nomax, L.resident != 0);
     if (L.resident && phase != 3) {
       view_load(v, st, w, N, s.C, lane);
@@ -1585,7 +1615,7 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
         move_randoms(seed, (uint32_t)w, sweep, (uint32_t)e, g, &ua);
         double xn[3] = {v.xs[3 * e] + step * g[0], v.xs[3 * e + 1] + step * g[1], v.xs[3 * e + 2] + step * g[2]};
         double rho, dj, gr[3];
-        propose<T, NORD, MD, false>(s, J, st, w, v, e, xn, lane, rho, dj, gr, &dl);
+        propose<T, NORD, MD, false>(s, J, st, w, v, e, xn, lane, rho, dj, gr, &dl, coop);
         double p = rho * rho * exp(2.0 * dj);
         if (ua < p) {
           accept_move<T, MD>(s, st, w, v, e, xn, dj, rho, lane, &dl);

@@ -20,7 +20,7 @@ static int set_smem_attrs(champ_ctx *c) {
   if (!rc) rc = set_attrs(c, k_propose<T, NORD, MD>, sm);
   if (!rc) rc = set_attrs(c, k_accept<T, MD>, sm);
   if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD, 0>, sm);
-  if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD, 1>, sm);
+  if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD, 1>, std::is_same<T, float>::value ? std::max(sm, c->kfm.smem) : sm);
   if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD, 2>, sm);
   if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD, 3>, sm);
   if (!rc) rc = set_attrs(c, k_vmc<T, NORD, MD, 0, 6>, sm);
@@ -227,6 +227,13 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
       auto kern = a.phase == 1 ? (acc6 ? k_vmc<T, NORD, MD, 1, 6> : k_vmc<T, NORD, MD, 1>)
                 : a.phase == 2 ? k_vmc<T, NORD, MD, 2>
                 : a.phase == 3 ? k_vmc<T, NORD, MD, 3> : (acc6 ? k_vmc<T, NORD, MD, 0, 6> : k_vmc<T, NORD, MD, 0>);
+      if (std::is_same<T, float>::value && a.phase == 1 && !acc6 && c->move_coop && c->kfm.lay.coop) {
+        // the block's warps share the proposals' coefficient stream (move-only layout)
+        const KCfg &M = c->kfm;
+        kern<<<dim3((st.W + M.wpb - 1) / M.wpb), dim3(32 * M.wpb), M.smem, c->stream>>>(
+            s, st, M.lay, a.nsweep, a.seed, a.sweep0, a.step, c->reinv_every, c->mover);
+        break;
+      }
       kern<<<grid, block, K.smem, c->stream>>>(s, st, K.lay, a.nsweep, a.seed, a.sweep0, a.step, c->reinv_every, c->mover);
       break;
     }

@@ -84,10 +84,11 @@ def test_autotune_picks_and_caches(tmp_path):
     eng.set_walkers(S.initial_walkers(s, 64, seed=3))
     cache = str(tmp_path / "tune.txt")
     rep = eng.autotune(nsweep=1, cache=cache)
-    assert "delay_rank=" in rep and "staged_eval=" in rep, rep
+    assert "delay_rank=" in rep and "staged_eval=" in rep and "move_coop=" in rep, rep
     chosen = dict(kv.split("=") for kv in rep.split(" (")[0].split())
     assert int(chosen["delay_rank"]) == eng.get_option("delay_rank")
     assert int(chosen["staged_eval"]) == eng.get_option("staged_eval")
+    assert int(chosen["move_coop"]) == eng.get_option("move_coop")
     # a second context of the same shape takes the choice from the cache, without timing
     e2 = Engine(s, 64, "mixed")
     e2.set_walkers(S.initial_walkers(s, 64, seed=4))

@@ -1,0 +1,40 @@
+"""FP32 Gaussian moves whose block shares the proposals' coefficient stream (option "move_coop",
+block_orbitals) against the same moves with each warp streaming the coefficients itself: the sums
+run in the same order, so the walks are identical -- positions, acceptances and energies -- also
+when the walker count leaves warps of the last block without a walker."""
+import numpy as np
+import pytest
+
+from champ_b200 import system as S
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("nw", [256, 254])
+def test_cooperative_moves_walk_the_same_chain(nw):
+    from champ_b200.engine import Engine
+    s = S.cluster128(ncent=8)
+    x = S.initial_walkers(s, nw, seed=17)
+    out = {}
+    for coop in (1, 0):
+        eng = Engine(s, nw, "mixed")
+        assert eng.get_option("move_coop") == 1  # on by default for this shape
+        eng.set_option("move_coop", coop)
+        assert eng.get_option("move_coop") == coop
+        eng.set_walkers(x)
+        st = eng.vmc_sweeps(3, seed=23, sweep0=0, step=s.step)
+        out[coop] = (eng.get_walkers(), st)
+        eng.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    for k in ("accept", "esum", "elast"):
+        assert np.array_equal(out[0][1][k], out[1][1][k]), k
+    assert out[1][1]["accept"].mean() > 0.1
+
+
+def test_cooperative_moves_option_bounds():
+    from champ_b200.engine import Engine, ChampError
+    s = S.get_system(2)  # walker state resident in shared memory: no cooperative moves
+    eng = Engine(s, 64, "mixed")
+    assert eng.get_option("move_coop") == 0
+    with pytest.raises(ChampError):
+        eng.set_option("move_coop", 1)
