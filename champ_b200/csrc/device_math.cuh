@@ -809,14 +809,13 @@ __device__ __forceinline__ void warp_orbitals(const T *phi, const T *coef, int n
   __syncwarp();
 }
 
-// Block: the same contraction as warp_orbitals (one channel, n > 16), for every warp of the block at
-// once, each with its own phi, sharing the coefficient stream: chunks of COOP_KB coefficient rows
-// (contiguous in [nbasis][n]) go through COOP_STAGES shared-memory buffers (stage, COOP_STAGES x
-// COOP_KB x n elements) by cp.async, COOP_STAGES - 1 chunks in flight while one is summed.  Each
-// orbital is summed over b in order, as warp_orbitals does, so the results are the same.  Every warp
-// of the block must make the call (a warp without a walker passes active = false: it copies and
-// waits, no sums).  Without 16-byte alignment of the rows the chunks are copied by plain loads.
-constexpr int COOP_KB = 32, COOP_STAGES = 3;
+// Block: the same contraction as warp_orbitals (n > 16), for every warp of the block at once, each
+// with its own phi ([nbasis][NCH]), sharing the coefficient stream: chunks of KB coefficient rows
+// (contiguous in [nbasis][n]) go through STG shared-memory buffers (stage, STG x KB x n elements)
+// by cp.async, STG - 1 chunks in flight while one is summed.  Each orbital and channel is summed
+// over b in order, as warp_orbitals does, so the results are the same.  Every warp of the block
+// must make the call with the same n and coefficients (a warp without work passes active = false:
+// it copies and waits, no sums).  Without 16-byte alignment the chunks are copied by plain loads.
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
@@ -825,20 +824,21 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int K>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(K) : "memory"); }
 
-template <class T, class O>
-__device__ __forceinline__ void block_orbitals(const T *phi, const T *coef, int nbasis, int n, O *out, int lane,
-                                               T *stage, bool active) {
-  static_assert(sizeof(T) == 4, "staged coefficient chunks are FP32");
+template <class T, int NCH, int KB, int STG, class O>
+__device__ __forceinline__ void block_orbitals(const T *phi, const T *coef, int nbasis, int n, O *out, int ostride,
+                                               int lane, T *stage, bool active) {
+  static_assert(STG >= 2 && 16 % sizeof(T) == 0, "pipeline of at least two 16-byte-copyable buffers");
+  constexpr int EV = 16 / sizeof(T);  // elements per 16-byte copy
   const int tid = threadIdx.x, nt = blockDim.x;
-  const int nchunk = (nbasis + COOP_KB - 1) / COOP_KB;
-  const bool vec = (n & 3) == 0 && (reinterpret_cast<uintptr_t>(coef) & 15) == 0;
-  auto issue = [&](int k) {  // chunk k into buffer k % COOP_STAGES (this thread's share)
+  const int nchunk = (nbasis + KB - 1) / KB;
+  const bool vec = n % EV == 0 && (reinterpret_cast<uintptr_t>(coef) & 15) == 0;
+  auto issue = [&](int k) {  // chunk k into buffer k % STG (this thread's share)
     if (k >= nchunk) return;
-    const int len = min(COOP_KB, nbasis - k * COOP_KB) * n;
-    const T *src = coef + (size_t)k * COOP_KB * n;
-    T *dst = stage + (size_t)(k % COOP_STAGES) * COOP_KB * n;
+    const int len = min(KB, nbasis - k * KB) * n;
+    const T *src = coef + (size_t)k * KB * n;
+    T *dst = stage + (size_t)(k % STG) * KB * n;
     if (vec) {
-      for (int q = tid; 4 * q < len; q += nt) cp_async16(dst + 4 * q, src + 4 * q);
+      for (int q = tid; EV * q < len; q += nt) cp_async16(dst + EV * q, src + EV * q);
     } else {
       for (int i = tid; i < len; i += nt) dst[i] = src[i];
     }
@@ -846,37 +846,47 @@ __device__ __forceinline__ void block_orbitals(const T *phi, const T *coef, int 
   for (int m0 = 0; m0 < n; m0 += 64) {
     const int ma = m0 + lane, mb = m0 + 32 + lane;
     const bool ha = ma < n, hb = mb < n;
-    T aa = T(0), ab = T(0);
+    T aa[NCH], ab[NCH];
+#pragma unroll
+    for (int ch = 0; ch < NCH; ch++) aa[ch] = ab[ch] = T(0);
     __syncthreads();  // earlier readers of the buffers are done
 #pragma unroll
-    for (int k = 0; k < COOP_STAGES - 1; k++) {
+    for (int k = 0; k < STG - 1; k++) {
       issue(k);
       cp_async_commit();
     }
     for (int k = 0; k < nchunk; k++) {
-      cp_async_wait<COOP_STAGES - 2>();  // this thread's copies of chunk k have landed
-      __syncthreads();                   // everyone's have; chunk k - 1 is no longer read
-      issue(k + COOP_STAGES - 1);        // into chunk k - 1's buffer
+      cp_async_wait<STG - 2>();  // this thread's copies of chunk k have landed
+      __syncthreads();           // everyone's have; chunk k - 1 is no longer read
+      issue(k + STG - 1);        // into chunk k - 1's buffer
       cp_async_commit();
       if (active) {
-        const T *cs = stage + (size_t)(k % COOP_STAGES) * COOP_KB * n;
-        const int b0 = k * COOP_KB, kb = min(COOP_KB, nbasis - b0);
+        const T *cs = stage + (size_t)(k % STG) * KB * n;
+        const int b0 = k * KB, kb = min(KB, nbasis - b0);
         for (int u = 0; u < kb; u++) {
-          const T p = phi[b0 + u];
           const T ca = ha ? cs[u * n + ma] : T(0), cb = hb ? cs[u * n + mb] : T(0);
-          aa += ca * p;
-          ab += cb * p;
+#pragma unroll
+          for (int ch = 0; ch < NCH; ch++) {
+            const T p = phi[(b0 + u) * NCH + ch];
+            aa[ch] += ca * p;
+            ab[ch] += cb * p;
+          }
         }
       }
     }
     cp_async_wait<0>();
     if (active) {
-      if (ha) out[ma] = (O)aa;
-      if (hb) out[mb] = (O)ab;
+#pragma unroll
+      for (int ch = 0; ch < NCH; ch++) {
+        if (ha) out[ch * ostride + ma] = (O)aa[ch];
+        if (hb) out[ch * ostride + mb] = (O)ab[ch];
+      }
     }
   }
   __syncwarp();
 }
+// the FP32 single-electron moves' pipeline: 32-row chunks, three buffers
+constexpr int COOP_KB = 32, COOP_STAGES = 3;
 
 // ---------------------------------------------------------------------------------------
 // Jastrow ijas=4, isc=4 (jastrow4.f90, scale_dist.f90:644-648, 857-884)

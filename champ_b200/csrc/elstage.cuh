@@ -63,19 +63,37 @@ __global__ void __launch_bounds__(128, 4) k_el_jas(Sys<T> s, State<T> st) {
   }
 }
 
+// Orbital coefficients shared by the block (coop): the block's warps take consecutive (walker,
+// electron) items of one spin (the host checks that N and nup are multiples of the warps per
+// block) and stream the coefficient rows through shared memory once for all of them
+// (block_orbitals, 8-row chunks, two buffers at stage_off); otherwise every warp streams them.
+constexpr int EL_ORB_KB = 8, EL_ORB_STG = 2;
 template <class T>
-__global__ void __launch_bounds__(128, 4) k_el_orb(Sys<T> s, State<T> st) {
+__global__ void __launch_bounds__(128, 4) k_el_orb(Sys<T> s, State<T> st, int coop, size_t stage_off) {
   extern __shared__ __align__(16) char dsm[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   const int N = s.N, nomax = s.nomax;
   T *phi = (T *)(dsm + el_orb_bytes<T>(s.nbasis) * wib);
+  T *stage = (T *)(dsm + stage_off);
   const long long items = (long long)st.W * N;
-  for (long long it = (long long)blockIdx.x * wpb + wib; it < items; it += (long long)gridDim.x * wpb) {
+  for (long long ib = (long long)blockIdx.x * wpb; ib < items; ib += (long long)gridDim.x * wpb) {
+    const long long it = ib + wib;
+    if (it >= items) {
+      if (!coop) break;
+      // no item for this warp: take part in the block's coefficient stream
+      const int e0 = (int)(ib % N), sp0 = e0 < s.nup ? 0 : 1;
+      block_orbitals<T, 5, EL_ORB_KB, EL_ORB_STG>((const T *)nullptr, s.cocc[sp0], s.nbasis, s.nocc[sp0], (T *)nullptr,
+                                                 0, lane, stage, false);
+      continue;
+    }
     const int w = (int)(it / N), e = (int)(it - (long long)w * N);
     const int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
     T *oe = st.orb5 + ((size_t)w * N + e) * 5 * nomax;
     warp_basis<T, 5>(s, st.x + ((size_t)w * N + e) * 3, phi, lane);
-    warp_orbitals<T, 5>(phi, s.cocc[sp], s.nbasis, s.nocc[sp], oe, nomax, lane);
+    if (coop)
+      block_orbitals<T, 5, EL_ORB_KB, EL_ORB_STG>(phi, s.cocc[sp], s.nbasis, s.nocc[sp], oe, nomax, lane, stage, true);
+    else
+      warp_orbitals<T, 5>(phi, s.cocc[sp], s.nbasis, s.nocc[sp], oe, nomax, lane);
     __syncwarp();
     double *A = st.ainv + (size_t)w * st.astride + (sp ? s.nup * s.nup : 0);
     for (int k = lane; k < n; k += 32) A[eo * n + k] = (double)oe[k];

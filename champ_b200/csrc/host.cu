@@ -736,6 +736,20 @@ static int setup_el_staged(champ_ctx *c) {
     c->el_smem[k] = bytes[k] * wpb;
   }
   c->el_nscr = el_fin_scratch(c->N, c->C);
+  // the orbital part's warps share the coefficient stream when a block's items are always of one
+  // spin (N and nup multiples of its warps) and the orbitals take warp_orbitals' lane mapping (> 16)
+  {
+    const int wpb = c->el_wpb[1], n0 = c->sd.nocc[0], n1 = c->sd.nocc[1];
+    if (wpb == 4 && c->N % wpb == 0 && c->nup % wpb == 0 && n0 > 16 && n1 > 16) {
+      const size_t st_bytes = sizeof(double) * EL_ORB_STG * EL_ORB_KB * (size_t)std::max(n0, n1);
+      const size_t off = align16(c->el_smem[1]);
+      if (off + st_bytes <= 200 * 1024) {
+        c->orb_stage = off;
+        c->el_smem[1] = off + st_bytes;
+        c->orb_coop_ok = c->orb_coop = 1;
+      }
+    }
+  }
   const size_t W = c->wmax, N = c->N;
   State<double> &st = c->std_;
   st.el_vj = dalloc<double>(c, W * 4 * N);
@@ -2160,6 +2174,14 @@ int champ_set_option(champ_ctx *c, const char *name, int64_t value) {
     c->pg_mode = (int)value;
     return CHAMP_OK;
   }
+  if (!strcmp(name, "orb_coop")) {
+    if (value < 0 || value > 1) return fail(CHAMP_EINVAL, "orb_coop: 0 or 1");
+    if (value && !c->orb_coop_ok)
+      return fail(CHAMP_EINVAL, "orb_coop: needs the staged evaluation with electrons and up electrons in multiples "
+                                "of 4 and more than 16 orbitals per spin");
+    c->orb_coop = (int)value;
+    return CHAMP_OK;
+  }
   if (!strcmp(name, "move_coop")) {
     if (value < 0 || value > 1) return fail(CHAMP_EINVAL, "move_coop: 0 or 1");
     if (value && !c->kfm.lay.coop)
@@ -2241,6 +2263,7 @@ int champ_get_option(const champ_ctx *c, const char *name, int64_t *value) {
   if (!strcmp(name, "dmc_ene_int")) { *value = c->dmc_ene_int; return CHAMP_OK; }
   if (!strcmp(name, "dmc_persistent")) { *value = c->dpar.persist; return CHAMP_OK; }
   if (!strcmp(name, "move_coop")) { *value = c->move_coop; return CHAMP_OK; }
+  if (!strcmp(name, "orb_coop")) { *value = c->orb_coop_ok ? c->orb_coop : 0; return CHAMP_OK; }
   return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);
 }
 

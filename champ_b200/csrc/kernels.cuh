@@ -1282,7 +1282,7 @@ __device__ void propose(const Sys<T> &s, const JasPar<T> &J, const State<T> &st,
   }
   warp_basis<T, NCH>(s, xn, v.phi, lane);
   if constexpr (!GRAD && sizeof(T) == 4) {
-    if (coop) block_orbitals<T>(v.phi, s.cocc[sp], s.nbasis, no, v.arow, lane, coop, true);
+    if (coop) block_orbitals<T, 1, COOP_KB, COOP_STAGES>(v.phi, s.cocc[sp], s.nbasis, no, v.arow, nomax, lane, coop, true);
     else warp_orbitals<T, NCH>(v.phi, s.cocc[sp], s.nbasis, no, v.arow, nomax, lane);
   } else {
     warp_orbitals<T, NCH>(v.phi, s.cocc[sp], s.nbasis, no, v.arow, nomax, lane);
@@ -1563,7 +1563,8 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
           for (int isw = 0; isw < nsweep; isw++)
             for (int e = 0; e < N; e++) {
               const int sp = e < s.nup ? 0 : 1;
-              block_orbitals<T>((const T *)nullptr, s.cocc[sp], s.nbasis, s.nocc[sp], (T *)nullptr, lane, coop, false);
+              block_orbitals<T, 1, COOP_KB, COOP_STAGES>((const T *)nullptr, s.cocc[sp], s.nbasis, s.nocc[sp],
+                                                         (T *)nullptr, 0, lane, coop, false);
             }
           continue;
         }

@@ -139,7 +139,8 @@ static int run_el_staged(champ_ctx *c, const State<T> &st, bool outputs, bool st
     CK(cudaGetLastError());
     const long long items = (long long)W * c->N;
     const long long g1 = std::min<long long>((items + w1 - 1) / w1, (long long)sm * 64);
-    k_el_orb<T><<<(unsigned)std::max<long long>(g1, 1), 32 * w1, c->el_smem[1], c->stream>>>(s, st);
+    k_el_orb<T><<<(unsigned)std::max<long long>(g1, 1), 32 * w1, c->el_smem[1], c->stream>>>(
+        s, st, c->orb_coop && c->orb_coop_ok, c->orb_stage);
     CK(cudaGetLastError());
     const int nmax = std::max(c->nup, c->ndn);
     k_el_inv<<<2 * W, 128, sizeof(double) * nmax * nmax, c->stream>>>(st.ainv, st.astride, c->nup, c->ndn, W, st.el_sc);

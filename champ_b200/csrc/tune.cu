@@ -1,7 +1,7 @@
 // tune.cu -- autotuning of the engine's launch shapes (host code).
 //
 // The options that change only the speed of a VMC sweep, never its results beyond rounding --
-// "delay_rank", "staged_eval", "move_coop", and for the tensor-core orbitals of FP32 contexts
+// "delay_rank", "staged_eval", "move_coop", "orb_coop", and for the tensor-core orbitals of FP32 contexts
 // "orbital_tc" and "orbital_tc_chunk" -- are timed one at a time over a few sweeps of the context's own walkers
 // (device time from CUDA events on the context's stream), and each keeps its fastest value.  The
 // result can be stored in a text file under a key of the system's shape and reused.
@@ -80,7 +80,7 @@ int champ_autotune(champ_ctx *c, int32_t nsweep, uint64_t seed, double step, con
   if (!c) return champ_fail(CHAMP_EINVAL, "null context");
   if (!c->have_walkers) return champ_fail(CHAMP_ESTATE, "no walkers set");
   if (nsweep < 1) return champ_fail(CHAMP_EINVAL, "nsweep < 1");
-  const std::vector<Knob> knobs = {{"delay_rank", {0, 4, 8, 16}}, {"staged_eval", {1, 0}}, {"move_coop", {1, 0}},
+  const std::vector<Knob> knobs = {{"delay_rank", {0, 4, 8, 16}}, {"staged_eval", {1, 0}}, {"move_coop", {1, 0}}, {"orb_coop", {1, 0}},
                                    {"orbital_tc", {1, 2}}, {"orbital_tc_chunk", {2, 4, 8}}};
   const std::string key = shape_key(c);
   std::string out, cached;
@@ -110,6 +110,7 @@ int champ_autotune(champ_ctx *c, int32_t nsweep, uint64_t seed, double step, con
       if (!strcmp(k.name, "delay_rank") && !c->std_.dly) continue;
       if (!strcmp(k.name, "staged_eval") && !c->std_.el_vj) continue;
       if (!strcmp(k.name, "move_coop") && !c->kfm.lay.coop) continue;
+      if (!strcmp(k.name, "orb_coop") && !(c->orb_coop_ok && c->el_staged)) continue;
       int64_t best = cur;
       float best_ms = 1e30f;
       char line[160];

@@ -415,6 +415,9 @@ int champ_set_mover(champ_ctx *ctx, int32_t imetro, double deltar, double deltat
    a block sharing the proposals' orbital-coefficient stream through shared memory (cp.async), in
    step electron by electron; 0 lets every warp stream the coefficients itself.  The walks are the
    same.
+   "orb_coop": 1 (default where available: the staged evaluation with electrons and up electrons in
+   multiples of 4 and more than 16 orbitals per spin) lets the warps of a block of its orbital part
+   share the coefficient stream through shared memory; 0 lets every warp stream it.  Same results.
    "dmc_persistent": 1 runs the DMC step kernel persistent (resident blocks taking walkers from a
    work counter), 0 (default) a warp per walker; the results are the same.
    "delay_rank": K >= 2 (default 4 when the walker state of a single-determinant FP64 or mixed
@@ -433,7 +436,7 @@ int champ_set_option(champ_ctx *ctx, const char *name, int64_t value);
 int champ_phase_times(champ_ctx *ctx, double *ms /* [4] */, int32_t *launches /* [4] or NULL */);
 /* Autotuning of the launch shapes (no counterpart in the reference): for the options that change
    only the speed of a VMC sweep -- "delay_rank" (0, 4, 8, 16), "staged_eval" (1, 0), "move_coop"
-   (1, 0), and with the
+   (1, 0), "orb_coop" (1, 0), and with the
    tensor-core orbitals of an FP32 context "orbital_tc" (1, 2) and "orbital_tc_chunk" (2, 4, 8) --
    one option at a time, in that order, times nsweep sweeps of the context's walkers (step size
    step, after one untimed sweep; device time from CUDA events) for each value it accepts, and
@@ -447,7 +450,7 @@ int champ_autotune(champ_ctx *ctx, int32_t nsweep, uint64_t seed, double step, c
                    int32_t report_len);
 /* Current value of an option ("orbital_tc", "orbital_tc_chunk", "reinvert_every", "dmc_graph",
    "phase_timing", "param_grad_mode", "staged_eval", "delay_rank", "tmoves", "dmc_ene_int",
-   "dmc_persistent", "move_coop"); kernel launches per
+   "dmc_persistent", "move_coop", "orb_coop"); kernel launches per
    champ_vmc_sweeps sweep
    ("launches_per_sweep": 1 for the fused sweep kernel, 2 for moves + single-kernel evaluation,
    5 for moves + staged evaluation or with the tensor-core orbitals). */

@@ -38,3 +38,23 @@ def test_cooperative_moves_option_bounds():
     assert eng.get_option("move_coop") == 0
     with pytest.raises(ChampError):
         eng.set_option("move_coop", 1)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_cooperative_orbital_stage_gives_the_same_evaluation(prec):
+    """The staged evaluation's orbital part with the block sharing the coefficient stream (option
+    "orb_coop") gives the same orbitals, hence bit-identical local energies, as every warp
+    streaming the coefficients itself."""
+    from champ_b200.engine import Engine
+    s = S.cluster128(ncent=8)
+    x = S.initial_walkers(s, 96, seed=5)
+    out = {}
+    for coop in (1, 0):
+        eng = Engine(s, 96, prec)
+        assert eng.get_option("orb_coop") == 1
+        eng.set_option("orb_coop", coop)
+        eng.set_walkers(x)
+        out[coop] = eng.eval_full()
+        eng.close()
+    for k in ("energy", "lnpsi", "d2lnpsi", "pe_nonloc", "velocity"):
+        assert np.array_equal(out[0][k], out[1][k]), k
