@@ -409,7 +409,7 @@ def e2e_of(eng, system, nw, nsteps, world, torch):
     te = allmax(time.perf_counter() - t0)
     return {"value": nw * world * system.nelec * nsteps / te, "unit": UNIT,
             "h2d_bytes_per_step": nw * system.nelec * 3 * 8, "d2h_bytes_per_step": nw * system.nelec * 3 * 8 + nw * 8,
-            "call": "champ_vmc_run_host (walkers host->device, FP64 state rebuild, 1 sweep, E_L and walkers device->host)"}
+            "call": "champ_vmc_run_host (walkers host->device, FP64 state rebuild without E_L (inverse, log-det, move tables), 1 sweep, E_L and walkers device->host)"}
 
 
 def main():

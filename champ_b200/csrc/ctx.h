@@ -194,6 +194,7 @@ struct OpArgs {
   const void *st_override = nullptr;  // State<T> to use instead of the context's (and its walker count)
   int nw_override = 0;
   int phase = -1;  // Vmc: one k_vmc launch of this phase (no statistics reset); DmcMove: k_dmc_move phase
+  bool rebuild = false;  // Eval: only the state the moves need (inverse, log-det, move tables), no E_L
   // Tmove: time step, variant (1 casula1, 2 det_balance1), per-walker counts of accepted T-moves
   // (device, may be null), and whether the walker count and step number come from the DMC state
   double tau = 0;

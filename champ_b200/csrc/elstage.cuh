@@ -200,7 +200,11 @@ struct ElRot {
 };
 
 template <class T, int NORD, bool MD>
-__global__ void __launch_bounds__(128, 4) k_el_fin(Sys<T> s, State<T> st, int nscr, int outputs, int stats, ElRot rot) {
+// tables_only: the state the single-electron moves start from (log-determinant, sign, Jastrow sum,
+// the FP32 move tables) without velocities, pseudopotential and E_L (the status flags then see
+// no E_L; the next full evaluation sets them)
+__global__ void __launch_bounds__(128, 4) k_el_fin(Sys<T> s, State<T> st, int nscr, int outputs, int stats, ElRot rot,
+                                                   int tables_only) {
   __shared__ JasPar<T> J;
   __shared__ EcpPar E;
   extern __shared__ __align__(16) char dsm[];
@@ -239,10 +243,10 @@ __global__ void __launch_bounds__(128, 4) k_el_fin(Sys<T> s, State<T> st, int ns
       sgn *= sgc;
     }
     double d2lnd = 0, v2 = 0;
-    det_velocities<T, MD, false>(s, st, w, v, lane, outputs != 0, nullptr, d2lnd, v2);
+    if (!tables_only) det_velocities<T, MD, false>(s, st, w, v, lane, outputs != 0, nullptr, d2lnd, v2);
     double vloc = 0, vnl = 0;
     int ntask = 0;
-    if (s.nloc > 0 && ok) {
+    if (s.nloc > 0 && ok && !tables_only) {
       double R[9];
       if (rot.random) random_rotation(rot.seed, (uint32_t)w, rot.sweep, R);
       else

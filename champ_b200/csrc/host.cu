@@ -2083,7 +2083,9 @@ int champ_vmc_run_host(champ_ctx *c, int32_t nw, double *x, int32_t nsweep, uint
   if (nw < 1 || nw > c->wmax) return fail(CHAMP_EINVAL, "nw out of range");
   c->W = nw;
   CK(cudaMemcpyAsync(state_x(c), x, sizeof(double) * nw * 3 * c->N, cudaMemcpyHostToDevice, c->stream));
-  int rc = launch(c, Op::Eval);
+  OpArgs rb;
+  rb.rebuild = true;  // the sweeps need the inverses and move tables; their E_L comes after the moves
+  int rc = launch(c, Op::Eval, rb);
   if (rc) return rc;
   c->have_walkers = true;
   champ_vmc_stats st = {nullptr, nullptr, nullptr, nullptr};  // champ_vmc_sweeps reports a tensor-core give-up

@@ -128,7 +128,8 @@ static int run_orb_tc(champ_ctx *c, const State<T> &st) {
 
 // The full evaluation of every walker as the four parts of elstage.cuh (FP64 state in HBM).
 template <class T, int NORD, bool MD>
-static int run_el_staged(champ_ctx *c, const State<T> &st, bool outputs, bool stats, const ElRot &rot) {
+static int run_el_staged(champ_ctx *c, const State<T> &st, bool outputs, bool stats, const ElRot &rot,
+                         bool rebuild = false) {
   if constexpr (!std::is_same<T, double>::value) {
     return fail(CHAMP_EINVAL, "internal: the staged evaluation is an FP64 path");
   } else {
@@ -145,8 +146,8 @@ static int run_el_staged(champ_ctx *c, const State<T> &st, bool outputs, bool st
     const int nmax = std::max(c->nup, c->ndn);
     k_el_inv<<<2 * W, 128, sizeof(double) * nmax * nmax, c->stream>>>(st.ainv, st.astride, c->nup, c->ndn, W, st.el_sc);
     CK(cudaGetLastError());
-    k_el_fin<T, NORD, MD><<<(W + w2 - 1) / w2, 32 * w2, c->el_smem[2], c->stream>>>(s, st, c->el_nscr, outputs ? 1 : 0,
-                                                                                stats ? 1 : 0, rot);
+    k_el_fin<T, NORD, MD><<<(W + w2 - 1) / w2, 32 * w2, c->el_smem[2], c->stream>>>(
+        s, st, c->el_nscr, outputs ? 1 : 0, stats ? 1 : 0, rot, rebuild && !outputs && !stats ? 1 : 0);
     CK(cudaGetLastError());
     return CHAMP_OK;
   }
@@ -167,7 +168,7 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
     if (c->el_staged && std::is_same<T, double>::value && !a.st_override) {
       ElRot rot{};
       for (int i = 0; i < 9; i++) rot.R[i] = R[i];
-      return run_el_staged<T, NORD, MD>(c, st, op == Op::EvalOut, false, rot);
+      return run_el_staged<T, NORD, MD>(c, st, op == Op::EvalOut, false, rot, a.rebuild);
     }
     if (tc) {
       int rc = run_orb_tc<T>(c, st);

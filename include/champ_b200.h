@@ -213,7 +213,9 @@ int champ_vmc_sweeps(champ_ctx *ctx, int32_t nsweep, uint64_t seed, uint64_t swe
                      double step, const champ_vmc_stats *stats);
 
 /* Same as champ_vmc_sweeps, but the walkers come from and go back to host memory and
-   the per-walker E_L of the last sweep is copied back (the call a host driver makes). */
+   the per-walker E_L of the last sweep is copied back (the call a host driver makes).  The state
+   the moves start from (inverses, log-determinants, move tables) is rebuilt from the incoming
+   positions without an E_L evaluation of them. */
 int champ_vmc_run_host(champ_ctx *ctx, int32_t nw, double *x /* host [nw][nelec][3], in/out */,
                        int32_t nsweep, uint64_t seed, uint64_t sweep0, double step,
                        double *eloc /* host [nw] */);

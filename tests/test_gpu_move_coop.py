@@ -58,3 +58,22 @@ def test_cooperative_orbital_stage_gives_the_same_evaluation(prec):
         eng.close()
     for k in ("energy", "lnpsi", "d2lnpsi", "pe_nonloc", "velocity"):
         assert np.array_equal(out[0][k], out[1][k]), k
+
+
+@pytest.mark.parametrize("k,prec", [(5, "mixed"), (5, "fp64"), (2, "mixed")])
+def test_vmc_run_host_matches_device_sweeps(k, prec):
+    """champ_vmc_run_host (walkers from host memory, the state rebuilt without an E_L -- only the
+    inverse, log-determinant and move tables for the staged evaluation -- one call of sweeps,
+    E_L and walkers back) walks the same chain as set_walkers + champ_vmc_sweeps."""
+    from champ_b200.engine import Engine
+    s = S.cluster128(ncent=8) if k == 5 else S.get_system(k)
+    nw = 64
+    x = S.initial_walkers(s, nw, seed=8)
+    a = Engine(s, nw, prec)
+    a.set_walkers(x)
+    st = a.vmc_sweeps(2, seed=13, sweep0=4, step=s.step)
+    xa = a.get_walkers()
+    b = Engine(s, nw, prec)
+    xb, eb = b.vmc_run_host(x, 2, seed=13, sweep0=4, step=s.step)
+    assert np.array_equal(xa, xb)
+    assert np.array_equal(st["elast"], eb)
