@@ -81,6 +81,8 @@ struct champ_ctx {
   int move_coop = 0;  // option "move_coop": 1 runs those moves with kfm
   int orb_coop_ok = 0, orb_coop = 0;  // k_el_orb's warps share the coefficient stream (option "orb_coop")
   size_t orb_stage = 0;               // offset of its double buffer in the block's shared memory
+  bool orb5_valid = false;  // the FP64 state's orbital rows are current for the walkers' positions
+  int mover_cache = 1;      // option "mover_cache": the accelerated mover's drift from those rows
   // staged evaluation (elstage.cuh) of the FP64 state when it lives in HBM: on/off (option
   // "staged_eval"), warps per block and dynamic shared memory of k_el_jas, k_el_orb, k_el_fin,
   // and the pseudopotential scratch of k_el_fin (elements)

@@ -1745,6 +1745,7 @@ extern "C" {
 int champ_set_params(champ_ctx *c, const double *a4, const double *b, const double *cc, const double *csf_coef,
                      const double *coef) {
   if (!c) return fail(CHAMP_EINVAL, "null context");
+  c->orb5_valid = false;  // orbital rows of the old coefficients
   Params &q = c->par;
   if (a4) std::copy(a4, a4 + q.a4.size(), q.a4.begin());
   if (b) std::copy(b, b + q.b.size(), q.b.begin());
@@ -1772,6 +1773,7 @@ int champ_get_params(const champ_ctx *c, double *a4, double *b, double *cc, doub
 
 int champ_apply_param_step(champ_ctx *c, const double *dp) {
   if (!c || !dp) return fail(CHAMP_EINVAL, "null argument");
+  c->orb5_valid = false;
   Params &q = c->par;
   int k = 0;
   for (int i = 1; i <= c->ncsfp; i++) q.csf[i] += dp[k++];
@@ -2176,6 +2178,11 @@ int champ_set_option(champ_ctx *c, const char *name, int64_t value) {
     c->pg_mode = (int)value;
     return CHAMP_OK;
   }
+  if (!strcmp(name, "mover_cache")) {
+    if (value < 0 || value > 1) return fail(CHAMP_EINVAL, "mover_cache: 0 or 1");
+    c->mover_cache = (int)value;
+    return CHAMP_OK;
+  }
   if (!strcmp(name, "orb_coop")) {
     if (value < 0 || value > 1) return fail(CHAMP_EINVAL, "orb_coop: 0 or 1");
     if (value && !c->orb_coop_ok)
@@ -2266,6 +2273,7 @@ int champ_get_option(const champ_ctx *c, const char *name, int64_t *value) {
   if (!strcmp(name, "dmc_persistent")) { *value = c->dpar.persist; return CHAMP_OK; }
   if (!strcmp(name, "move_coop")) { *value = c->move_coop; return CHAMP_OK; }
   if (!strcmp(name, "orb_coop")) { *value = c->orb_coop_ok ? c->orb_coop : 0; return CHAMP_OK; }
+  if (!strcmp(name, "mover_cache")) { *value = c->mover_cache; return CHAMP_OK; }
   return fail(CHAMP_EINVAL, std::string("unknown option: ") + name);
 }
 

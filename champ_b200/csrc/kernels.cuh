@@ -31,6 +31,10 @@ template <class T>
 struct State {
   int W;
   double *x;       // [W][N][3]
+  // the FP64 state's orbital rows [W][N][5][nomax] (value, gradient, Laplacian at each electron's
+  // position), current for the positions, for the accelerated mover's drift at the current
+  // position (kept current by its accepted moves); null when not current
+  double *orb_cache = nullptr;
   double *ainv;    // [W][astride]; spin-up block at 0 (nup x nup), spin-down at nup*nup
   T *fso;          // [W][N][N]
   T *ren;          // [W][N][C][2]: r_en and 1/(1 + scalek r_en)
@@ -1258,7 +1262,9 @@ __device__ inline void delay_flush(Delay &d, double *A0, int n, int sp, int lane
 template <class T, int NORD, bool MD, bool GRAD>
 __device__ void propose(const Sys<T> &s, const JasPar<T> &J, const State<T> &st, int w, const View<T> &v, int e,
                         const double *xn, int lane, double &rho, double &dj, double *grad, const Delay *dl = nullptr,
-                        T *coop = nullptr) {
+                        T *coop = nullptr, const double *orow = nullptr) {
+  // orow (may be null): the electron's orbital row at xn ([5][nomax], FP64) when it is known
+  // already (its current position): no basis functions or contraction then
   const int N = s.N, C = s.C, nomax = s.nomax;
   int sp = e < s.nup ? 0 : 1, n = sp ? s.ndn : s.nup, eo = sp ? e - s.nup : e;
   const double *A = gam_ptr<T, MD>(s, v, sp);
@@ -1280,22 +1286,25 @@ __device__ void propose(const Sys<T> &s, const JasPar<T> &J, const State<T> &st,
       for (int c = 0; c < C; c++) z += ipow(v.rnew[2 * c + 1], lane);
     v.asum[lane] = z;
   }
-  warp_basis<T, NCH>(s, xn, v.phi, lane);
-  if constexpr (!GRAD && sizeof(T) == 4) {
+  if (orow) {
+    // the row is given
+  } else if constexpr (!GRAD && sizeof(T) == 4) {
+    warp_basis<T, NCH>(s, xn, v.phi, lane);
     if (coop) block_orbitals<T, 1, COOP_KB, COOP_STAGES>(v.phi, s.cocc[sp], s.nbasis, no, v.arow, nomax, lane, coop, true);
     else warp_orbitals<T, NCH>(v.phi, s.cocc[sp], s.nbasis, no, v.arow, nomax, lane);
   } else {
+    warp_basis<T, NCH>(s, xn, v.phi, lane);
     warp_orbitals<T, NCH>(v.phi, s.cocc[sp], s.nbasis, no, v.arow, nomax, lane);
   }
   // the wave function is linear in the moved electron's orbital row: ratio = sum_m G[m][e] phi_m
   double r0 = 0, g0 = 0, g1 = 0, g2 = 0;
   for (int k = lane; k < no; k += 32) {
     double a = dcol ? v.colb[k] : A[k * n + eo];
-    r0 += a * (double)v.arow[k];
+    r0 += a * (orow ? orow[k] : (double)v.arow[k]);
     if (GRAD) {
-      g0 += a * (double)v.arow[nomax + k];
-      g1 += a * (double)v.arow[2 * nomax + k];
-      g2 += a * (double)v.arow[3 * nomax + k];
+      g0 += a * (orow ? orow[nomax + k] : (double)v.arow[nomax + k]);
+      g1 += a * (orow ? orow[2 * nomax + k] : (double)v.arow[2 * nomax + k]);
+      g2 += a * (orow ? orow[3 * nomax + k] : (double)v.arow[3 * nomax + k]);
     }
   }
   rho = warp_sum(r0);
@@ -1593,7 +1602,8 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
           // position, both transition probabilities
           const double xo[3] = {v.xs[3 * e], v.xs[3 * e + 1], v.xs[3 * e + 2]};
           double r0, d0, go[3];
-          propose<T, NORD, MD, true>(s, J, st, w, v, e, xo, lane, r0, d0, go, &dl);
+          double *orow = st.orb_cache ? st.orb_cache + ((size_t)w * N + e) * 5 * s.nomax : nullptr;
+          propose<T, NORD, MD, true>(s, J, st, w, v, e, xo, lane, r0, d0, go, &dl, nullptr, orow);
           MoveRng rng{seed, (uint32_t)w, (uint32_t)sweep, (uint32_t)(sweep >> 32), (uint32_t)e, 0u, {0.0, 0.0}, 0};
           double xn[3], fxop, areao, rtry;
           slat_forward(s, mv, xo, go, rng, xn, fxop, areao, rtry);
@@ -1607,6 +1617,10 @@ __global__ void __launch_bounds__(128, 4) k_vmc(Sys<T> s, State<T> st, Layout L,
             p = rr * rr * rho * rho * exp(2.0 * dj) * fabs((fxnp * areao) / (fxop * arean));
           }
           if (rng.next() < p) {
+            if (orow) {  // the electron's new orbital row becomes its cached row
+              for (int i = lane; i < 5 * s.nomax; i += 32) orow[i] = (double)v.arow[i];
+              __syncwarp();
+            }
             accept_move<T, MD>(s, st, w, v, e, xn, dj, rho, lane, &dl);
             acc += 1;
           }

@@ -149,6 +149,7 @@ static int run_el_staged(champ_ctx *c, const State<T> &st, bool outputs, bool st
     k_el_fin<T, NORD, MD><<<(W + w2 - 1) / w2, 32 * w2, c->el_smem[2], c->stream>>>(
         s, st, c->el_nscr, outputs ? 1 : 0, stats ? 1 : 0, rot, rebuild && !outputs && !stats ? 1 : 0);
     CK(cudaGetLastError());
+    c->orb5_valid = st.orb5 == c->std_.orb5;  // k_el_orb wrote every electron's row
     return CHAMP_OK;
   }
 }
@@ -160,6 +161,9 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
   st.W = a.st_override ? a.nw_override : c->W;
   const KCfg &K = kcfg<T>(c);
   dim3 grid((st.W + K.wpb - 1) / K.wpb), block(32 * K.wpb);
+  // the FP64 state's orbital rows stay current only through evaluations and the accelerated
+  // mover's sweeps, which update them (run_el_staged marks them current)
+  if (op != Op::Eval && op != Op::EvalOut && op != Op::Vmc) c->orb5_valid = false;
   const double *R = c->rot;
   switch (op) {
   case Op::Eval:
@@ -170,6 +174,7 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
       for (int i = 0; i < 9; i++) rot.R[i] = R[i];
       return run_el_staged<T, NORD, MD>(c, st, op == Op::EvalOut, false, rot, a.rebuild);
     }
+    c->orb5_valid = false;
     if (tc) {
       int rc = run_orb_tc<T>(c, st);
       if (rc) return rc;
@@ -229,6 +234,18 @@ static int launch_t(champ_ctx *c, Op op, const OpArgs &a) {
       auto kern = a.phase == 1 ? (acc6 ? k_vmc<T, NORD, MD, 1, 6> : k_vmc<T, NORD, MD, 1>)
                 : a.phase == 2 ? k_vmc<T, NORD, MD, 2>
                 : a.phase == 3 ? k_vmc<T, NORD, MD, 3> : (acc6 ? k_vmc<T, NORD, MD, 0, 6> : k_vmc<T, NORD, MD, 0>);
+      // the accelerated mover of a mixed context takes the drift at the current position from the
+      // FP64 state's orbital rows while they are current, and keeps them current
+      const bool cache = std::is_same<T, float>::value && a.phase == 1 && acc6 && c->mover_cache && c->orb5_valid &&
+                         c->prec == CHAMP_PREC_MIXED && !c->md.multidet && c->el_staged;
+      if (!cache) c->orb5_valid = false;
+      if (cache) {
+        State<T> sc = st;
+        sc.orb_cache = c->std_.orb5;
+        kern<<<grid, block, K.smem, c->stream>>>(s, sc, K.lay, a.nsweep, a.seed, a.sweep0, a.step, c->reinv_every,
+                                                 c->mover);
+        break;
+      }
       if (std::is_same<T, float>::value && a.phase == 1 && !acc6 && c->move_coop && c->kfm.lay.coop) {
         // the block's warps share the proposals' coefficient stream (move-only layout)
         const KCfg &M = c->kfm;

@@ -420,6 +420,10 @@ int champ_set_mover(champ_ctx *ctx, int32_t imetro, double deltar, double deltat
    "orb_coop": 1 (default where available: the staged evaluation with electrons and up electrons in
    multiples of 4 and more than 16 orbitals per spin) lets the warps of a block of its orbital part
    share the coefficient stream through shared memory; 0 lets every warp stream it.  Same results.
+   "mover_cache": 1 (default) lets the accelerated mover of a mixed single-determinant context
+   whose walker state lives in HBM take the drift at an electron's current position from the
+   orbital rows of the last FP64 evaluation (updated by its accepted moves) instead of evaluating
+   the basis functions and orbitals there again; 0 evaluates them.  The two differ at FP32 rounding.
    "dmc_persistent": 1 runs the DMC step kernel persistent (resident blocks taking walkers from a
    work counter), 0 (default) a warp per walker; the results are the same.
    "delay_rank": K >= 2 (default 4 when the walker state of a single-determinant FP64 or mixed
@@ -452,7 +456,7 @@ int champ_autotune(champ_ctx *ctx, int32_t nsweep, uint64_t seed, double step, c
                    int32_t report_len);
 /* Current value of an option ("orbital_tc", "orbital_tc_chunk", "reinvert_every", "dmc_graph",
    "phase_timing", "param_grad_mode", "staged_eval", "delay_rank", "tmoves", "dmc_ene_int",
-   "dmc_persistent", "move_coop", "orb_coop"); kernel launches per
+   "dmc_persistent", "move_coop", "orb_coop", "mover_cache"); kernel launches per
    champ_vmc_sweeps sweep
    ("launches_per_sweep": 1 for the fused sweep kernel, 2 for moves + single-kernel evaluation,
    5 for moves + staged evaluation or with the tensor-core orbitals). */

@@ -95,3 +95,34 @@ def test_set_mover_validates_and_corrects():
     eng.set_walkers(S.initial_walkers(S.get_system(2), 8, seed=1))
     st = eng.vmc_sweeps(2, seed=1, sweep0=0, step=0.5)
     assert np.all(np.isfinite(st["elast"]))
+
+
+def test_accelerated_mover_drift_from_cached_orbital_rows():
+    """Mixed precision, walker state in HBM: the accelerated mover's drift at the current position
+    from the last FP64 evaluation's orbital rows (option "mover_cache", kept current by the accepted
+    moves) against evaluating the orbitals there again.  The drifts differ at FP32 rounding; the
+    accelerated proposal follows the drift and each move changes the next electron's drift, so the
+    difference grows through a sweep (first electron: 1e-7 bohr) without changing the sampling:
+    after one sweep most walkers agree to 1e-3 bohr and the acceptances agree."""
+    from champ_b200.engine import Engine
+    s = S.cluster128(ncent=8)
+    nw = 128
+    x = S.initial_walkers(s, nw, seed=21)
+    out = {}
+    for cache in (1, 0):
+        eng = Engine(s, nw, "mixed")
+        eng.set_mover(6)
+        eng.set_option("mover_cache", cache)
+        assert eng.get_option("mover_cache") == cache
+        eng.set_walkers(x)
+        st = eng.vmc_sweeps(1, seed=9, sweep0=0, step=s.step)
+        out[cache] = (eng.get_walkers(), st)
+        eng.close()
+    d = np.abs(out[1][0] - out[0][0]).reshape(nw, -1, 3).max(axis=2)
+    close = d.max(axis=1) < 1e-3
+    acc1, acc0 = out[1][1]["accept"].sum(), out[0][1]["accept"].sum()
+    print(f"mover_cache: first electron max {d[:, 0].max():.2e} bohr, {close.mean():.3f} of walkers within "
+          f"1e-3 bohr, acceptances {acc1:.0f} / {acc0:.0f}")
+    assert np.median(d[:, 0]) < 1e-5
+    assert close.mean() >= 0.6
+    assert abs(acc1 - acc0) <= 0.02 * acc0
