@@ -367,7 +367,7 @@ def measure_dmc(system, target, nstep, torch, prec):
     eng.set_walkers(system_walkers(system, target, seed=11))
     eng.vmc_sweeps(20, SEED, sweep0=0, step=step_size(system), stats=False)
     eng.dmc_init(target, 0.01)
-    eng.dmc_steps(100, seed=SEED)  # equilibration (the population settles in about 60 steps), graph capture
+    eng.dmc_steps(250, seed=SEED)  # equilibration (the population settles within about 250 steps), graph capture
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
