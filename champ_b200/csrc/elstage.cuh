@@ -27,7 +27,8 @@ __host__ __device__ inline int el_fin_scratch(int N, int C) {
   return (room > 256 ? room : 256) + (C > 32 ? 32 * C : 0);
 }
 
-template <class T, int NORD>
+// VO: the tables and the Jastrow sum only (the rebuild of the state the moves start from)
+template <class T, int NORD, bool VO = false>
 __global__ void __launch_bounds__(128, 4) k_el_jas(Sys<T> s, State<T> st) {
   __shared__ JasPar<T> J;
   __shared__ EcpPar E;
@@ -48,7 +49,7 @@ __global__ void __launch_bounds__(128, 4) k_el_jas(Sys<T> s, State<T> st) {
     for (int i = lane; i < 3 * N; i += 32) v.xs[i] = st.x[(size_t)w * 3 * N + i];
     __syncwarp();
     double fsum, d2j, pe_ee, pe_en;
-    jastrow_tables<T, NORD, true>(s, J, v, rt, lane, fsum, d2j, pe_ee, pe_en);
+    jastrow_tables<T, NORD, true, VO>(s, J, v, rt, lane, fsum, d2j, pe_ee, pe_en);
     double *vj = st.el_vj + (size_t)w * 4 * N;
     for (int i = lane; i < 3 * N; i += 32) vj[i] = v.vacc[i];
     for (int i = lane; i < N; i += 32) vj[3 * N + i] = v.divj[i];

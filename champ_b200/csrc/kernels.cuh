@@ -576,7 +576,9 @@ __device__ void md_tables(const Sys<T> &s, const View<T> &v, int lane, double &l
 // distances.f90) and the e-e (and, all-electron, e-n) Coulomb energies of one walker.  TR: the
 // e-n distances are also written to, and the pair and e-n terms read from, rt = [2][C][N]
 // (distance plane, then scaled-distance plane; consecutive electrons adjacent).
-template <class T, int NORD, bool TR>
+// VO: values only -- the tables and the Jastrow sum without the gradient and Laplacian terms (v.vacc
+// and v.divj stay zero), for rebuilding the state the moves start from.
+template <class T, int NORD, bool TR, bool VO = false>
 __device__ void jastrow_tables(const Sys<T> &s, const JasPar<T> &J, const View<T> &v, T *rt, int lane, double &fsum,
                                double &d2j, double &pe_ee, double &pe_en) {
   const int N = s.N, C = s.C;
@@ -631,37 +633,43 @@ __device__ void jastrow_tables(const Sys<T> &s, const JasPar<T> &J, const View<T
     T rij = tsqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
     T du = T(1) / (T(1) + sk * rij);
     T fu, fuu;
-    T f = jas_ee<T, true>(J, isb, ss, ipar, rij, du, fu, fuu);
-    T gi[3], gj[3];
+    T f = jas_ee<T, !VO>(J, isb, ss, ipar, rij, du, fu, fuu);
+    T gi[3] = {0, 0, 0}, gj[3] = {0, 0, 0}, d2 = 0;
+    if constexpr (!VO) {
 #pragma unroll
-    for (int k = 0; k < 3; k++) { gi[k] = fu * rv[k]; gj[k] = -fu * rv[k]; }
-    T d2 = 2 * (fuu + 2 * fu);
+      for (int k = 0; k < 3; k++) { gi[k] = fu * rv[k]; gj[k] = -fu * rv[k]; }
+      d2 = 2 * (fuu + 2 * fu);
+    }
     if (NORD > 1) {
       for (int c = 0; c < C; c++) {
         const double *cc = s.cent + 3 * c;
         T ri = rof(i, c), rj = rof(j, c);
         Een<T> o;
-        jas_een<T, NORD, 2>(J, s.ctype[c], rij, du, ri, dof(i, c), rj, dof(j, c), o);
+        jas_een<T, NORD, VO ? 0 : 2>(J, s.ctype[c], rij, du, ri, dof(i, c), rj, dof(j, c), o);
         f += o.fc;
+        if constexpr (!VO) {
 #pragma unroll
-        for (int k = 0; k < 3; k++) {
-          gi[k] += o.fi * T(xi[k] - cc[k]) + o.fu * rv[k];
-          gj[k] += o.fj * T(xj[k] - cc[k]) - o.fu * rv[k];
+          for (int k = 0; k < 3; k++) {
+            gi[k] += o.fi * T(xi[k] - cc[k]) + o.fu * rv[k];
+            gj[k] += o.fj * T(xj[k] - cc[k]) - o.fu * rv[k];
+          }
+          T sp = ri + rj, tm = ri - rj;
+          d2 += 2 * (2 * o.fu + o.fi + o.fj) + 2 * o.fuu + o.fii + o.fjj + o.fui * (rij * rij + sp * tm) / (ri * rij) +
+                o.fuj * (rij * rij - sp * tm) / (rj * rij);
         }
-        T sp = ri + rj, tm = ri - rj;
-        d2 += 2 * (2 * o.fu + o.fi + o.fj) + 2 * o.fuu + o.fii + o.fjj + o.fui * (rij * rij + sp * tm) / (ri * rij) +
-              o.fuj * (rij * rij - sp * tm) / (rj * rij);
       }
     }
     fsum += (double)f;
-    d2j += (double)d2;
+    if constexpr (!VO) {
+      d2j += (double)d2;
 #pragma unroll
-    for (int k = 0; k < 3; k++) {
-      atomicAdd(&v.vacc[3 * i + k], (double)gi[k]);
-      atomicAdd(&v.vacc[3 * j + k], (double)gj[k]);
+      for (int k = 0; k < 3; k++) {
+        atomicAdd(&v.vacc[3 * i + k], (double)gi[k]);
+        atomicAdd(&v.vacc[3 * j + k], (double)gj[k]);
+      }
+      atomicAdd(&v.divj[i], 0.5 * (double)d2);
+      atomicAdd(&v.divj[j], 0.5 * (double)d2);
     }
-    atomicAdd(&v.divj[i], 0.5 * (double)d2);
-    atomicAdd(&v.divj[j], 0.5 * (double)d2);
     fso[i * N + j] = f;
     fso[j * N + i] = f;
   }
@@ -672,11 +680,13 @@ __device__ void jastrow_tables(const Sys<T> &s, const JasPar<T> &J, const View<T
     for (int c = 0; c < C; c++) {
       const double *cc = s.cent + 3 * c;
       T r = rof(i, c), dn = dof(i, c);
-      T fi, fii;
-      f += jas_en<T, true>(J, s.ctype[c], r, dn, fi, fii);
+      T fi = 0, fii = 0;
+      f += jas_en<T, !VO>(J, s.ctype[c], r, dn, fi, fii);
+      if constexpr (!VO) {
 #pragma unroll
-      for (int k = 0; k < 3; k++) g[k] += fi * T(xi[k] - cc[k]);
-      d2 += fii + 2 * fi;
+        for (int k = 0; k < 3; k++) g[k] += fi * T(xi[k] - cc[k]);
+        d2 += fii + 2 * fi;
+      }
       if (s.nloc == 0) {
         double rd = sqrt((xi[0] - cc[0]) * (xi[0] - cc[0]) + (xi[1] - cc[1]) * (xi[1] - cc[1]) +
                          (xi[2] - cc[2]) * (xi[2] - cc[2]));

@@ -39,6 +39,7 @@ static int set_smem_attrs(champ_ctx *c) {
   }
   if (!rc && c->el_staged && std::is_same<T, double>::value) {
     rc = set_attrs(c, k_el_jas<T, NORD>, c->el_smem[0]);
+    if (!rc) rc = set_attrs(c, k_el_jas<T, NORD, true>, c->el_smem[0]);
     if (!rc) rc = set_attrs(c, k_el_orb<T>, c->el_smem[1]);
     if (!rc) rc = set_attrs(c, k_el_fin<T, NORD, MD>, c->el_smem[2]);
     if (!rc) rc = set_attrs(c, k_el_inv, sizeof(double) * CHAMP_MAX_SPIN * CHAMP_MAX_SPIN);
@@ -136,7 +137,9 @@ static int run_el_staged(champ_ctx *c, const State<T> &st, bool outputs, bool st
     Sys<T> &s = sysof<T>(c);
     const int W = st.W, sm = c->num_sms > 0 ? c->num_sms : 148;
     const int w0 = c->el_wpb[0], w1 = c->el_wpb[1], w2 = c->el_wpb[2];
-    k_el_jas<T, NORD><<<(W + w0 - 1) / w0, 32 * w0, c->el_smem[0], c->stream>>>(s, st);
+    const bool vo = rebuild && !outputs && !stats;  // the moves' state only: no velocities, no E_L
+    if (vo) k_el_jas<T, NORD, true><<<(W + w0 - 1) / w0, 32 * w0, c->el_smem[0], c->stream>>>(s, st);
+    else k_el_jas<T, NORD><<<(W + w0 - 1) / w0, 32 * w0, c->el_smem[0], c->stream>>>(s, st);
     CK(cudaGetLastError());
     const long long items = (long long)W * c->N;
     const long long g1 = std::min<long long>((items + w1 - 1) / w1, (long long)sm * 64);
@@ -147,7 +150,7 @@ static int run_el_staged(champ_ctx *c, const State<T> &st, bool outputs, bool st
     k_el_inv<<<2 * W, 128, sizeof(double) * nmax * nmax, c->stream>>>(st.ainv, st.astride, c->nup, c->ndn, W, st.el_sc);
     CK(cudaGetLastError());
     k_el_fin<T, NORD, MD><<<(W + w2 - 1) / w2, 32 * w2, c->el_smem[2], c->stream>>>(
-        s, st, c->el_nscr, outputs ? 1 : 0, stats ? 1 : 0, rot, rebuild && !outputs && !stats ? 1 : 0);
+        s, st, c->el_nscr, outputs ? 1 : 0, stats ? 1 : 0, rot, vo ? 1 : 0);
     CK(cudaGetLastError());
     c->orb5_valid = st.orb5 == c->std_.orb5;  // k_el_orb wrote every electron's row
     return CHAMP_OK;
